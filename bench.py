@@ -1,0 +1,340 @@
+#!/usr/bin/env python3
+"""Benchmark of the sm_100a volume raycast on render3d's scale workload.
+
+Workload: a 1024^3 u8 seeded scroll phantom split into 128^3 bricks with a
+4-level (sum+4)/8 pyramid and render3d's page table, rendered at 1920x1080
+with full gradient shading, ray-cone LOD (bias 0) and early termination at
+opacity 0.99, along the 120-frame scripted orbit (frame i at phase
+(i mod 120)/120).  One step = one frame.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+value: Gsamples/s (sum of per-ray march iterations / device time), inputs
+resident in HBM.  e2e: the same metric through the render3d-facing API
+(r3d_frame + r3d_read_frame into pinned host memory, params host->device and
+the RGBA8 frame device->host every step), host wall clock.  --impl reference
+times the CPU restatement of the reference shader (the reference's Slang
+shader cannot be compiled here) on the host cores.  With --gpus N > 1 every
+rank renders the orbit independently (the path has no exchange step:
+replicas).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+W, H = 1920, 1080
+N_EDGE = 1024
+NLEV = 4
+SEED = 1234
+CUTOFF = 0.99
+STEP_VOXELS = 0.5
+ORBIT_FRAMES = 120
+WORKLOAD = "scroll phantom 1024^3 u8, 128^3 bricks x 4 LOD levels, 1920x1080 full shading"
+
+
+def measured_peaks() -> tuple[float, str]:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi SM clocks and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+        self.t = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            if self.t:
+                self.t.join(timeout=2)
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def orbit_params(rb, lut, i: int, brick_mode: int, mode: int = 0):
+    p = rb.orbit_view((i % ORBIT_FRAMES) / ORBIT_FRAMES, W, H, lut, step_voxels=STEP_VOXELS,
+                      mode=mode, frame_index=i)
+    p.brick_mode = brick_mode
+    return p
+
+
+def algorithmic_bytes(cnt: np.ndarray, pixels: int) -> float:
+    """Bytes the march must read/write: 8 per trilinear sample, 6x8 for the
+    gradient taps of a shaded sample, 8 per TF lookup (2 RGBA8 texels), 4
+    per page-table walk and 4 per output pixel."""
+    samples, tf, grad, walks = (float(x) for x in cnt)
+    return 8.0 * samples + 48.0 * grad + 8.0 * tf + 4.0 * walks + 4.0 * pixels
+
+
+def cpu_baseline(rb, orc, vol_pages, lut, frames: list[int], threads: int) -> dict:
+    """The oracle (FP32 CPU restatement of the reference shader) on a bounded
+    sample of the same workload: whole 1920x1080 frames of the orbit."""
+    page, pool, brick_mode = vol_pages
+    sc = orc.BrickScene(page, pool)
+    total, t0 = 0, time.perf_counter()
+    for i in frames:
+        p = orbit_params(rb, lut, i, brick_mode)
+        _, _, _, tot, _ = orc.render(p, sc, lut, W, H, cutoff=CUTOFF, threads=threads,
+                                     want_aux=False)
+        total += tot
+    dt = time.perf_counter() - t0
+    return {"value": total / dt / 1e9, "unit": "Gsamples/s", "cores": threads, "kind": "port",
+            "sample": f"{len(frames)} full 1920x1080 orbit frames (phases "
+                      f"{', '.join(str(i) for i in frames)} of 120), {total} samples, "
+                      f"{dt:.1f} s", "fps": len(frames) / dt}
+
+
+def run_reference(args) -> None:
+    """CPU arm: the oracle on all host threads; each step traces a bounded,
+    evenly strided 1/16 of the rays of one orbit frame (every 4th pixel of
+    every 4th row), so the whole run takes minutes."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import render3d_b200 as rb
+    import oracle as orc
+    threads = os.cpu_count() or 1
+    vol = rb.phantom(N_EDGE, seed=SEED)
+    sc = orc.BrickScene.build(vol, NLEV)  # the oracle's own brick builder
+    del vol
+    lut = rb.scroll_ramp_tf()
+    brick_mode = 9 | (NLEV << 8) | rb.BRICK_LOD_FLAG
+    ys, xs = np.mgrid[0:H:4, 0:W:4]
+    xy = np.stack([xs.ravel(), ys.ravel()], axis=1).astype(np.uint32)
+    times, samples = [], []
+    for s in range(args.warmup + args.steps):
+        p = orbit_params(rb, lut, s, brick_mode)
+        t0 = time.perf_counter()
+        _, st, _ = orc.render_pixels(p, sc, lut, xy, cutoff=CUTOFF, threads=threads)
+        dt = time.perf_counter() - t0
+        if s >= args.warmup:
+            times.append(dt)
+            samples.append(float(st.sum()))
+    t = sum(times)
+    v = sum(samples) / t / 1e9
+    sample = (f"per step: {xy.shape[0]} rays (every 4th pixel of every 4th row) of one "
+              "1920x1080 orbit frame")
+    out = {"impl": "reference", "metric": "raycast Gsamples/s @1024^3 1080p (full shading)",
+           "value": v, "unit": "Gsamples/s", "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": 1000.0 * t / len(times),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic",
+           "config": {"workload": WORKLOAD, "cutoff": CUTOFF, "step_voxels": STEP_VOXELS,
+                      "sample": sample},
+           "cpu_baseline": {"value": v, "unit": "Gsamples/s", "cores": threads, "kind": "port",
+                            "sample": sample},
+           "e2e": {"value": v, "unit": "Gsamples/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def run_ours(args) -> None:
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(local)
+    import render3d_b200 as rb
+
+    lut = rb.scroll_ramp_tf()
+    vol = rb.phantom(N_EDGE, seed=SEED)
+    ctx = rb.Context(local)
+    ctx.set_transfer(lut)
+    ctx.set_quality(rb.QUALITY_FULL)
+    ctx.set_alpha_cutoff(CUTOFF)
+    ctx.bricks_build(vol, NLEV)
+    bm = ctx.brick_mode
+    info = ctx.bricks_info()
+    stream = torch.cuda.ExternalStream(ctx.stream, device=local)
+    img = torch.zeros((H, W, 4), dtype=torch.uint8, device=f"cuda:{local}")
+    total = torch.zeros(1, dtype=torch.int64, device=f"cuda:{local}")
+    K, Wm = args.steps, args.warmup
+
+    def frame(i, counters=None):
+        ctx.raycast(orbit_params(rb, lut, i, bm), W, H, out=img, total=total,
+                    counters=counters, stream=ctx.stream)
+
+    # untimed counting pass over the same frames: algorithmic work per frame
+    cnt = torch.zeros(4, dtype=torch.int64, device=f"cuda:{local}")
+    for i in range(Wm, Wm + K):
+        frame(i, counters=cnt)
+    torch.cuda.synchronize()
+    counts = cnt.cpu().numpy().astype(np.float64)
+
+    for i in range(Wm):
+        frame(i)
+    total.zero_()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for i in range(Wm, Wm + K):
+            frame(i)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    samples = float(total.item())
+    assert abs(samples - counts[0]) < 0.5, "counting pass and timed pass disagree"
+    t = torch.tensor([ms], device=f"cuda:{local}")
+    s_all = torch.tensor([samples], device=f"cuda:{local}", dtype=torch.float64)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(s_all, op=dist.ReduceOp.SUM)
+    ms_max = float(t.item())
+    value = float(s_all.item()) / (ms_max * 1e-3) / 1e9
+    fps = K * world / (ms_max * 1e-3)
+
+    # end to end through the render3d-facing API: r3d_frame + r3d_read_frame
+    r = rb.Renderer(W, H)
+    r.set_transfer(lut)
+    r.set_alpha_cutoff(CUTOFF)
+    r.bricks_begin_volume(vol, NLEV)
+    host = torch.empty((H, W, 4), dtype=torch.uint8, pin_memory=True).numpy()
+    for i in range(Wm):
+        p = orbit_params(rb, lut, i, 0)
+        r.bricks_params(p)
+        r.frame(p)
+        r.read_frame(host)
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for i in range(Wm, Wm + K):
+        p = orbit_params(rb, lut, i, 0)
+        r.bricks_params(p)
+        r.frame(p)
+        r.read_frame(host)
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], device=f"cuda:{local}")
+    if dist:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = float(s_all.item()) / float(te.item()) / 1e9
+    r.close()
+
+    peak, peak_kind = measured_peaks()
+    alg = algorithmic_bytes(counts, W * H * K)
+    achieved = alg / (ms * 1e-3) / 1e9
+    out = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            import oracle as orc
+            page, pool = ctx.bricks_read()
+            cpu = cpu_baseline(rb, orc, (page, pool, bm), lut, [0, 30],
+                               os.cpu_count() or 1)
+            del pool
+        out = {"metric": "raycast Gsamples/s @1024^3 1080p (full shading)", "value": value,
+               "unit": "Gsamples/s", "n_gpus": world, "steps": K, "warmup": Wm,
+               "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+               "config": {"workload": WORKLOAD, "frames_per_step": 1, "cutoff": CUTOFF,
+                          "step_voxels": STEP_VOXELS, "lod_bias": 0.0,
+                          "slots": info["nslots"], "l2": "inputs larger than L2 "
+                          f"(brick pool {info['nslots'] * 2} MiB)",
+                          "parallelism": f"replicas x{world}"},
+               "fps": fps, "mrays_per_s": W * H * K * world / (ms_max * 1e-3) / 1e6,
+               "samples_per_frame": counts[0] / K,
+               "e2e": {"value": e2e_value, "unit": "Gsamples/s", "h2d_bytes_per_step": 248,
+                       "d2h_bytes_per_step": W * H * 4, "fps": K * world / float(te.item())},
+               "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
+                            "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                            "peak_kind": peak_kind,
+                            "algorithmic_bytes_per_frame": alg / K},
+               "gpu_launches": K,
+               "clocks": clk.summary(),
+               "cpu_baseline": cpu}
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=120)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

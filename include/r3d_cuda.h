@@ -1,0 +1,147 @@
+/* C-ABI of the sm_100a volume-raycast library (libr3d_b200.so).
+ *
+ * This is the layer beneath render3d's render-backend interface
+ * (reference src/render/render.h): render3d's Vulkan backend records one
+ * raycast dispatch per view (src/vk/vkbackend.c:7121-7173) of the compute
+ * shader src/shaders/raycast.slang; this library replaces that dispatch and
+ * the resources it samples with hand-written CUDA kernels.  r3d_render.h
+ * builds the headless render.h subset on top of these calls.
+ *
+ * Conventions: every call returns R3D_OK (0) or a negative R3D_E_* code and
+ * leaves a message in r3d_cuda_last_error(ctx); nothing aborts or throws.
+ * Calls are stream-ordered on the stream passed (NULL = the context's own
+ * stream); a context is used by one host thread at a time.  Output buffers
+ * may be device pointers (asynchronous) or host pointers (the call copies to
+ * them and synchronizes).  No CUDA types appear here: streams are void *. */
+#ifndef R3D_CUDA_H
+#define R3D_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "r3d_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct r3d_cuda_ctx r3d_cuda_ctx;
+
+enum {
+  R3D_OK = 0,
+  R3D_E_INVALID = -1,     /* bad argument */
+  R3D_E_CUDA = -2,        /* CUDA runtime error (message names it) */
+  R3D_E_NOMEM = -3,       /* device or host allocation failed */
+  R3D_E_UNSUPPORTED = -4, /* a feature this library does not implement */
+  R3D_E_STATE = -5,       /* no volume / bricks / TF uploaded yet */
+  R3D_E_DEVICE = -6,      /* a kernel reported a data error (see status) */
+  R3D_E_TIMEOUT = -7,     /* a bounded device wait ran out */
+};
+
+/* Device status bits (r3d_cuda_status). */
+#define R3D_STATUS_PAGE_RANGE 1u  /* page word or slot index out of range */
+#define R3D_STATUS_QUEUE 2u       /* batched queue descriptor rejected */
+#define R3D_STATUS_WAIT 4u        /* a bounded spin-wait gave up */
+
+/* --- context ----------------------------------------------------------- */
+
+/* Creates a context on CUDA device `device` with its own stream. */
+int r3d_cuda_create(int device, r3d_cuda_ctx **out);
+void r3d_cuda_destroy(r3d_cuda_ctx *ctx);
+const char *r3d_cuda_last_error(const r3d_cuda_ctx *ctx);
+/* The context's stream (a cudaStream_t). */
+void *r3d_cuda_stream(r3d_cuda_ctx *ctx);
+/* Synchronizes, returns and (if clear) resets the device status bits. */
+int r3d_cuda_status(r3d_cuda_ctx *ctx, uint32_t *bits, int clear);
+
+/* --- scene state --------------------------------------------------------- */
+
+/* Cube volume: copies nx*ny*nz u8 voxels (x fastest; host or device
+ * pointer), builds the full mip chain (2x box, (sum+4)/8) and the dilated
+ * 8^3 occupancy grid on the device.  Replaces r3d_upload_volume
+ * (reference src/render/render.h:20, src/vk/vkbackend.c:1508-1672). */
+int r3d_cuda_upload_volume(r3d_cuda_ctx *ctx, const r3d_volume_desc *d, const uint8_t *voxels);
+
+/* 256-entry RGBA8 transfer function (reference src/render/render.h:240). */
+int r3d_cuda_set_transfer(r3d_cuda_ctx *ctx, const uint8_t rgba[256][4]);
+
+/* R3D_QUALITY_FULL (six-tap) or R3D_QUALITY_FAST (four-tap) gradients
+ * (reference src/render/render.h:242). */
+int r3d_cuda_set_quality(r3d_cuda_ctx *ctx, uint32_t quality);
+
+/* Front-to-back termination opacity, default 0.98 (the reference's
+ * ALPHA_CUTOFF constant, src/shaders/raycast.slang:124).  (0, 1]. */
+int r3d_cuda_set_alpha_cutoff(r3d_cuda_ctx *ctx, float cutoff);
+
+/* LOD brick cache built on the device from a raw volume: nlev levels of the
+ * (sum+4)/8 box pyramid over 128^3 bricks, zero-padded at the far edges; a
+ * brick is resident when its maximum is >= min_max (0: all resident).
+ * Writes render3d's page table (64-word header + one word per brick, entry
+ * = slot | max << 24, 0xFFFFFFFF absent; src/vk/vkbackend.c:4184-4206).
+ * voxels may be a host or device pointer. */
+int r3d_cuda_bricks_build(r3d_cuda_ctx *ctx, const r3d_volume_desc *d, const uint8_t *voxels,
+                          uint32_t nlev, uint32_t min_max);
+
+/* Brick cache from an existing page table and slot pool (host pointers):
+ * page_words u32 words in render3d's LOD format and nslots 128^3 slots,
+ * x fastest.  The header is validated; scales must be powers of two. */
+int r3d_cuda_bricks_load(r3d_cuda_ctx *ctx, const uint32_t *page, uint32_t page_words,
+                         const uint8_t *slots, uint32_t nslots);
+
+/* brick_mode word for r3d_frame_params (abpa | nlev << 8 | 0x20000;
+ * reference src/vk/vkbackend.c:4511-4517), 0 when no bricks are loaded. */
+uint32_t r3d_cuda_brick_mode(const r3d_cuda_ctx *ctx);
+
+/* Sizes of the loaded brick cache; and a copy of it (host pointers, either
+ * may be NULL) for inspection and tests. */
+int r3d_cuda_bricks_info(const r3d_cuda_ctx *ctx, uint32_t *page_words, uint32_t *nslots,
+                         uint32_t shape[3], uint32_t *nlev);
+int r3d_cuda_bricks_read(r3d_cuda_ctx *ctx, uint32_t *page, uint8_t *slots);
+
+/* Copy of cube mip level `level` or (level == -1) the occupancy grid into a
+ * host buffer; dims receives its size. */
+int r3d_cuda_cube_read(r3d_cuda_ctx *ctx, int level, uint8_t *out, uint32_t dims[3]);
+
+/* --- forward raycast ------------------------------------------------------ */
+
+/* Optional per-pixel outputs of a forward raycast, in the same memory kind
+ * (device or host) as the image. */
+typedef struct r3d_cuda_aux {
+  uint32_t *steps;     /* out_w*out_h: march iterations of the ray */
+  uint32_t *mip_index; /* out_w*out_h: step at which the MIP max last rose */
+  unsigned long long *total_steps; /* one counter: += sum of steps */
+  /* R3D_COUNTERS counters, += per frame: samples (= steps), composited TF
+   * lookups, gradient-shaded samples, page-table walks.  Counting runs a
+   * separate kernel build; NULL for the plain one. */
+  unsigned long long *counters;
+} r3d_cuda_aux;
+#define R3D_COUNTERS 4
+
+/* Raycasts nviews (1..64) views into the RGBA8 image rgba_out of
+ * out_w x out_h pixels (row-major, 4 bytes per pixel).  Each view renders
+ * its viewport rect at view_org, clipped to the image like render3d's
+ * r3d_frame_views sanitize pass (src/vk/vkbackend.c:6871-6900); views whose
+ * rect is empty are skipped.  A cube view needs r3d_cuda_upload_volume, a
+ * brick view (brick_mode != 0) r3d_cuda_bricks_*.  Replaces the per-view
+ * vkCmdDispatch of src/vk/vkbackend.c:7121-7173. */
+int r3d_cuda_raycast_fwd(r3d_cuda_ctx *ctx, const r3d_frame_params *views, uint32_t nviews,
+                         uint8_t *rgba_out, uint32_t out_w, uint32_t out_h,
+                         const r3d_cuda_aux *aux, void *stream);
+
+/* CUDA-event time of the last r3d_cuda_raycast_fwd's kernels in ns
+ * (synchronizes the events). */
+int r3d_cuda_last_kernel_ns(r3d_cuda_ctx *ctx, uint64_t *ns);
+
+/* --- diagnostics ----------------------------------------------------------- */
+
+/* Evaluates the raycast's log2, exp2, pow(x, y) and x^24 on the device for n
+ * inputs (host pointers); out receives 4 floats per input in that order.
+ * Used to check the device build of r3d_fmath.h bit for bit. */
+int r3d_cuda_fmath_eval(r3d_cuda_ctx *ctx, const float *x, const float *y, float *out,
+                        uint32_t n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* R3D_CUDA_H */

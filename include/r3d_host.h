@@ -1,0 +1,88 @@
+/* Host-side inputs of the raycast: camera basis, turntable orbit, volume
+ * rotation, transfer-function LUTs and presets, the skip gate, the LOD
+ * policy, the scripted benchmark orbit, and the seeded scroll phantom.
+ *
+ * These restate render3d's core helpers (src/core/camera.c:5-75,
+ * src/core/mathx.h:34-43, src/core/transfer.c:5-50, src/core/lod.h:8-26,
+ * src/main.c:1238-1242,3932-3946,6788-6824) under an r3d_host_ prefix so
+ * that they link beside the reference's own core library without clashing.
+ * With -ffp-contract=off they produce the same bits as the reference's. */
+#ifndef R3D_HOST_H
+#define R3D_HOST_H
+
+#include <stdint.h>
+
+#include "r3d_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct r3d_host_camera {
+  float pos[3];
+  float yaw, pitch, fov_y; /* radians; fov defaults to 60 degrees */
+  float target[3];
+  float dist;
+} r3d_host_camera;
+
+void r3d_host_camera_init(r3d_host_camera *c, const float pos[3]);
+void r3d_host_camera_look(r3d_host_camera *c, float dyaw, float dpitch);
+void r3d_host_camera_move(r3d_host_camera *c, const float local[3], float dist);
+void r3d_host_camera_orbit_set(r3d_host_camera *c, const float target[3], float dist);
+void r3d_host_camera_orbit_drag(r3d_host_camera *c, float dyaw, float dpitch);
+void r3d_host_camera_orbit_zoom(r3d_host_camera *c, float factor);
+/* right/up pre-scaled by tan(fov/2)*aspect and tan(fov/2). */
+void r3d_host_camera_basis(const r3d_host_camera *c, float aspect, float right[3], float up[3],
+                           float fwd[3]);
+/* rows of R = Ry(yaw) Rx(pitch) Rz(roll) */
+void r3d_host_m3_ypr(float yaw, float pitch, float roll, float rows[3][3]);
+
+/* Piecewise-linear TF points -> LUT with render3d's integer lerp. */
+void r3d_host_tf_build(const uint8_t *values, const uint8_t (*rgba)[4], uint32_t npts,
+                       uint8_t lut[256][4]);
+/* Presets 0 grey ramp, 1 scroll, 2 high-pass; returns idx, or the preset
+ * count (3) when idx is out of range (lut untouched). */
+uint32_t r3d_host_tf_preset(uint32_t idx, uint8_t lut[256][4]);
+/* First value with nonzero alpha (255 if none). */
+float r3d_host_tf_min_visible(const uint8_t lut[256][4]);
+/* skip_gate = max(low_cut, tf_min_visible - 0.5) / 255. */
+float r3d_host_skip_gate(float low_cut, const uint8_t lut[256][4]);
+
+uint32_t r3d_host_lod_pick(float distance, float pixel_cone, float base_voxels,
+                           uint32_t nlevels);
+uint32_t r3d_host_lod_fallback(uint32_t desired, uint32_t ordinal, uint32_t nlevels);
+
+/* A view of the scripted "orbit" benchmark at phase ph in [0,1): yaw = 2 pi ph,
+ * pitch = 0.5 sin(4 pi ph), distance 2 around target (src/main.c:3932-3946),
+ * identity volume transform, viewport w x h.  Other fields: step_voxels,
+ * density, lod_bias as given, max_mip 10, threshold / skip_gate from
+ * low_cut and the LUT. */
+void r3d_host_orbit_view(r3d_frame_params *p, float ph, const float target[3], uint32_t w,
+                         uint32_t h, float step_voxels, float density, float lod_bias,
+                         uint32_t mode, uint32_t frame_index, float low_cut,
+                         const uint8_t lut[256][4]);
+
+/* Seeded scroll phantom: papyrus sheets along an Archimedean spiral about
+ * the z axis through the volume centre, r(theta) = r0 + pitch*theta/(2 pi).
+ * A voxel is papyrus when its radial distance to the nearest wrap is below
+ * sheet_half and r0 <= r < radius.  Papyrus ~ N(in_mean, in_sd), air
+ * ~ N(air_mean, air_sd), plus N(0, noise_sd), rounded and clamped to u8.
+ * Normals come from splitmix64 of (seed, voxel index) through Box-Muller,
+ * so every voxel is independent of the thread count. */
+typedef struct r3d_phantom_desc {
+  uint64_t seed;
+  float pitch, radius, r0, sheet_half;
+  float in_mean, in_sd, air_mean, air_sd, noise_sd;
+} r3d_phantom_desc;
+
+/* The configuration used for a volume of edge n: pitch 14 and radius 110
+ * at 256, pitch 18 and radius 110/256 of the edge above 256. */
+void r3d_host_phantom_default(uint32_t n, uint64_t seed, r3d_phantom_desc *d);
+int r3d_host_phantom(uint8_t *vox, uint32_t nx, uint32_t ny, uint32_t nz,
+                     const r3d_phantom_desc *d, int threads);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* R3D_HOST_H */

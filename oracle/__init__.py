@@ -1,0 +1,199 @@
+"""ctypes bindings for the CPU oracle (liboracle.so) and for the reference's
+own host code compiled from the reference tree (_ref/libr3dref.so).
+
+Test infrastructure: only the test suite, the smoke check and the CPU
+baseline of the benchmark import this package.  The oracle restates the
+reference raycast on the CPU in FP32 (r3d_oracle.c); the renderer library
+never calls it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_LIB_PATH = os.path.join(HERE, "_ref", "libr3dref.so")
+REF_TEST_GPU = os.path.join(HERE, "_ref", "test_gpu")
+CLI_PATH = os.path.join(HERE, "r3d_oracle_cli")
+
+
+def build() -> None:
+    """Builds liboracle.so, the oracle CLI and (when the reference tree is
+    present) _ref/ with the system gcc."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+class Cube(C.Structure):
+    _fields_ = [("nlevels", C.c_uint32), ("dim", (C.c_uint32 * 3) * 16),
+                ("level", C.c_void_p * 16), ("occ", C.c_void_p), ("odim", C.c_uint32 * 3)]
+
+
+class Bricks(C.Structure):
+    _fields_ = [("page", C.c_void_p), ("page_words", C.c_uint32), ("pool", C.c_void_p),
+                ("nslots", C.c_uint32)]
+
+
+class Opts(C.Structure):
+    _fields_ = [("alpha_cutoff", C.c_float), ("quality", C.c_uint32), ("threads", C.c_int)]
+
+
+class Aux(C.Structure):
+    _fields_ = [("steps", C.c_void_p), ("mip_index", C.c_void_p),
+                ("total_steps", C.c_uint64), ("status", C.c_uint32)]
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        build()
+    lib = C.CDLL(LIB_PATH)
+    P, U32, F = C.c_void_p, C.c_uint32, C.c_float
+    lib.orc_render_view.restype = C.c_int
+    lib.orc_render_view.argtypes = [P, C.POINTER(Cube), C.POINTER(Bricks), P, C.POINTER(Opts), P,
+                                    U32, U32, C.POINTER(Aux)]
+    lib.orc_render_pixels.restype = C.c_int
+    lib.orc_render_pixels.argtypes = [P, C.POINTER(Cube), C.POINTER(Bricks), P, C.POINTER(Opts),
+                                      P, U32, P, P, P]
+    lib.orc_mip_levels.restype = U32
+    lib.orc_mip_levels.argtypes = [U32, U32, U32, P]
+    lib.orc_downsample.restype = None
+    lib.orc_downsample.argtypes = [P, U32, U32, U32, P, U32, U32, U32]
+    lib.orc_occupancy.restype = None
+    lib.orc_occupancy.argtypes = [P, U32, U32, U32, P]
+    lib.orc_build_lod_bricks.restype = C.c_int64
+    lib.orc_build_lod_bricks.argtypes = [P, U32, U32, U32, U32, U32, P, U32, P, C.c_uint64]
+    lib.orc_lod_page_words.restype = U32
+    lib.orc_lod_page_words.argtypes = [U32, U32, U32, U32]
+    lib.orc_camera_basis.restype = None
+    lib.orc_camera_basis.argtypes = [F, F, F, F, P, P, P]
+    lib.orc_orbit_pos.restype = None
+    lib.orc_orbit_pos.argtypes = [F, F, P, F, P]
+    lib.orc_tf_build.restype = None
+    lib.orc_tf_build.argtypes = [P, P, U32, P]
+    lib.orc_lod_pick.restype = U32
+    lib.orc_lod_pick.argtypes = [F, F, F, U32]
+    lib.orc_lod_fallback.restype = U32
+    lib.orc_lod_fallback.argtypes = [U32, U32, U32]
+    lib.orc_fmath_eval.restype = None
+    lib.orc_fmath_eval.argtypes = [P, P, P, U32]
+    lib.orc_m3_ypr.restype = None
+    lib.orc_m3_ypr.argtypes = [F, F, F, P]
+    return lib
+
+
+lib = _load()
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+class CubeScene:
+    """A cube volume with the oracle's own mip chain and occupancy grid."""
+
+    def __init__(self, vol: np.ndarray):
+        vol = np.ascontiguousarray(vol, np.uint8)
+        nz, ny, nx = vol.shape
+        self.c = Cube()
+        dims = ((C.c_uint32 * 3) * 16)()
+        self.c.nlevels = lib.orc_mip_levels(nx, ny, nz, dims)
+        self.levels = [vol]
+        for m in range(1, self.c.nlevels):
+            d = tuple(dims[m])
+            dst = np.empty((d[2], d[1], d[0]), np.uint8)
+            s = self.levels[-1]
+            lib.orc_downsample(_p(s), s.shape[2], s.shape[1], s.shape[0], _p(dst), *d)
+            self.levels.append(dst)
+        for m, lv in enumerate(self.levels):
+            self.c.dim[m][:] = (lv.shape[2], lv.shape[1], lv.shape[0])
+            self.c.level[m] = lv.ctypes.data
+        od = ((nx + 7) // 8, (ny + 7) // 8, (nz + 7) // 8)
+        self.occ = np.empty((od[2], od[1], od[0]), np.uint8)
+        lib.orc_occupancy(_p(vol), nx, ny, nz, _p(self.occ))
+        self.c.occ = self.occ.ctypes.data
+        self.c.odim[:] = od
+
+
+class BrickScene:
+    """A LOD brick cache: page table + slot pool (x fastest)."""
+
+    def __init__(self, page: np.ndarray, pool: np.ndarray):
+        self.page = np.ascontiguousarray(page, np.uint32)
+        self.pool = np.ascontiguousarray(pool, np.uint8)
+        self.b = Bricks(self.page.ctypes.data, self.page.size, self.pool.ctypes.data,
+                        self.pool.size // 128 ** 3)
+
+    @classmethod
+    def build(cls, vol: np.ndarray, nlev: int, min_max: int = 0) -> "BrickScene":
+        vol = np.ascontiguousarray(vol, np.uint8)
+        nz, ny, nx = vol.shape
+        words = lib.orc_lod_page_words(nx, ny, nz, nlev)
+        page = np.empty(words, np.uint32)
+        n = lib.orc_build_lod_bricks(_p(vol), nx, ny, nz, nlev, min_max, _p(page), words, None, 0)
+        if n < 0:
+            raise ValueError("orc_build_lod_bricks failed")
+        pool = np.empty(max(n, 1) * 128 ** 3, np.uint8)
+        n2 = lib.orc_build_lod_bricks(_p(vol), nx, ny, nz, nlev, min_max, _p(page), words,
+                                      _p(pool), n)
+        assert n2 == n
+        return cls(page, pool[: n * 128 ** 3] if n else pool[:0])
+
+
+def render(params, scene, lut: np.ndarray, img_w: int, img_h: int, cutoff: float = 0.98,
+           quality: int = 0, threads: int = 0, img: np.ndarray | None = None,
+           want_aux: bool = True):
+    """Renders one view; returns (img (h, w, 4) u8, steps, mip_index, total, status)."""
+    if img is None:
+        img = np.zeros((img_h, img_w, 4), np.uint8)
+    lut = np.ascontiguousarray(lut, np.uint8)
+    steps = np.zeros((img_h, img_w), np.uint32) if want_aux else None
+    mipi = np.zeros((img_h, img_w), np.uint32) if want_aux else None
+    aux = Aux(_p(steps), _p(mipi), 0, 0)
+    cube = C.byref(scene.c) if isinstance(scene, CubeScene) else None
+    br = C.byref(scene.b) if isinstance(scene, BrickScene) else None
+    rc = lib.orc_render_view(C.byref(params), cube, br, _p(lut), C.byref(Opts(cutoff, quality,
+                             threads)), _p(img), img_w, img_h, C.byref(aux))
+    if rc != 0:
+        raise ValueError("orc_render_view rejected the view")
+    return img, steps, mipi, aux.total_steps, aux.status
+
+
+def render_pixels(params, scene, lut: np.ndarray, xy: np.ndarray, cutoff: float = 0.98,
+                  quality: int = 0, threads: int = 0):
+    """Rays of the listed dispatch-thread coordinates xy (n, 2); returns
+    (rgba (n, 4), steps (n,), mip_index (n,))."""
+    xy = np.ascontiguousarray(xy, np.uint32)
+    n = xy.shape[0]
+    rgba = np.zeros((n, 4), np.uint8)
+    steps = np.zeros(n, np.uint32)
+    mipi = np.zeros(n, np.uint32)
+    lut = np.ascontiguousarray(lut, np.uint8)
+    cube = C.byref(scene.c) if isinstance(scene, CubeScene) else None
+    br = C.byref(scene.b) if isinstance(scene, BrickScene) else None
+    rc = lib.orc_render_pixels(C.byref(params), cube, br, _p(lut),
+                               C.byref(Opts(cutoff, quality, threads)), _p(xy), n, _p(rgba),
+                               _p(steps), _p(mipi))
+    if rc != 0:
+        raise ValueError("orc_render_pixels rejected the view")
+    return rgba, steps, mipi
+
+
+def fmath_eval(x: np.ndarray, y: np.ndarray) -> np.ndarray:
+    """CPU log2, exp2, pow and x^24 of the shared header, (n, 4) float32."""
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.ascontiguousarray(y, np.float32)
+    out = np.empty((x.size, 4), np.float32)
+    lib.orc_fmath_eval(_p(x), _p(y), _p(out), x.size)
+    return out
+
+
+def ref_lib():
+    """The reference's camera.c / transfer.c / lod.h / mathx.h, or None when
+    _ref/ has not been built (no reference tree at build time)."""
+    if not os.path.exists(REF_LIB_PATH):
+        return None
+    r = C.CDLL(REF_LIB_PATH)
+    return r

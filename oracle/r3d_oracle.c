@@ -1,0 +1,889 @@
+/* CPU oracle for the volume raycast (test infrastructure; see r3d_oracle.h).
+ *
+ * Build with -ffp-contract=off: every multiply-add that is fused is written
+ * as fmaf, every other operation rounds on its own, in the order written.
+ * Line references are to the reference tree (src/shaders/raycast.slang
+ * unless another file is named). */
+#include "r3d_oracle.h"
+
+#include <math.h>
+#include <omp.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "r3d_fmath.h"
+
+/* ---------------------------------------------------------------- helpers */
+
+typedef struct v3f {
+  float x, y, z;
+} v3f;
+
+static inline v3f mk3(float x, float y, float z) {
+  v3f r = {x, y, z};
+  return r;
+}
+/* dot product, evaluated as fma(z, fma(y, x*x)) */
+static inline float dot3(v3f a, v3f b) { return fmaf(a.z, b.z, fmaf(a.y, b.y, a.x * b.x)); }
+static inline float lerpf_(float a, float b, float t) { return fmaf(t, b - a, a); }
+static inline float clampf_(float x, float lo, float hi) { return fminf(fmaxf(x, lo), hi); }
+static inline float satf(float x) { return clampf_(x, 0.0f, 1.0f); }
+static inline v3f norm3(v3f a) {
+  float inv = 1.0f / sqrtf(dot3(a, a));
+  return mk3(a.x * inv, a.y * inv, a.z * inv);
+}
+
+#define INV255 (1.0f / 255.0f)
+#define MAX_STEPS 4096u   /* :123 */
+#define OCC_BLOCK 8.0f    /* :125 */
+#define BR_SLOT 128.0f    /* :156 */
+
+static const float BG_R = 0.02f, BG_G = 0.02f, BG_B = 0.03f; /* :716 */
+
+/* hash12, src/shaders/common.slang:57-61 */
+static float hash12(uint32_t px, uint32_t py, uint32_t frame) {
+  uint32_t h = px * 374761393u + py * 668265263u + frame * 2246822519u;
+  h = (h ^ (h >> 13)) * 1274126177u;
+  return (float)(h >> 8) * (1.0f / 16777216.0f);
+}
+
+static inline uint8_t unorm8(float x) { return (uint8_t)(int)fmaf(satf(x), 255.0f, 0.5f); }
+
+/* ------------------------------------------------------------ sampling */
+
+/* clamp-to-edge trilinear at texel centres on one u8 grid; the 8 taps are
+ * blended in 0..255 space (x, then y, then z) and scaled by 1/255 */
+static float tri_u8(const uint8_t *g, uint32_t dx, uint32_t dy, uint32_t dz, float tx, float ty,
+                    float tz) {
+  tx = clampf_(tx, 0.0f, (float)(dx - 1u));
+  ty = clampf_(ty, 0.0f, (float)(dy - 1u));
+  tz = clampf_(tz, 0.0f, (float)(dz - 1u));
+  uint32_t x0 = (uint32_t)tx, y0 = (uint32_t)ty, z0 = (uint32_t)tz;
+  float fx = tx - (float)x0, fy = ty - (float)y0, fz = tz - (float)z0;
+  uint32_t x1 = x0 + 1u < dx ? x0 + 1u : dx - 1u;
+  uint32_t y1 = y0 + 1u < dy ? y0 + 1u : dy - 1u;
+  uint32_t z1 = z0 + 1u < dz ? z0 + 1u : dz - 1u;
+  size_t sx = 1, sy = dx, sz = (size_t)dx * dy;
+  const uint8_t *b = g;
+#define T(X, Y, Z) ((float)b[(size_t)(X) * sx + (size_t)(Y) * sy + (size_t)(Z) * sz])
+  float c00 = lerpf_(T(x0, y0, z0), T(x1, y0, z0), fx);
+  float c10 = lerpf_(T(x0, y1, z0), T(x1, y1, z0), fx);
+  float c01 = lerpf_(T(x0, y0, z1), T(x1, y0, z1), fx);
+  float c11 = lerpf_(T(x0, y1, z1), T(x1, y1, z1), fx);
+#undef T
+  float c0 = lerpf_(c00, c10, fy), c1 = lerpf_(c01, c11, fy);
+  return lerpf_(c0, c1, fz) * INV255;
+}
+
+/* volumes[0].SampleLevel(p, lod) with the trilinear + linear-mip sampler of
+ * src/vk/vkbackend.c:1058-1069 (:409-416) */
+static float cube_sample(const orc_cube *c, v3f p, float lod) {
+  float fl = floorf(lod);
+  uint32_t m0 = (uint32_t)fl;
+  if (m0 > c->nlevels - 1u) m0 = c->nlevels - 1u;
+  float fr = lod - fl;
+  const uint32_t *d = c->dim[m0];
+  float v = tri_u8(c->level[m0], d[0], d[1], d[2], fmaf(p.x, (float)d[0], -0.5f),
+                   fmaf(p.y, (float)d[1], -0.5f), fmaf(p.z, (float)d[2], -0.5f));
+  if (fr > 0.0f && m0 + 1u < c->nlevels) {
+    const uint32_t *e = c->dim[m0 + 1u];
+    float v1 = tri_u8(c->level[m0 + 1u], e[0], e[1], e[2], fmaf(p.x, (float)e[0], -0.5f),
+                      fmaf(p.y, (float)e[1], -0.5f), fmaf(p.z, (float)e[2], -0.5f));
+    v = lerpf_(v, v1, fr);
+  }
+  return v;
+}
+
+/* occ.SampleLevel(p, 0) with the nearest sampler */
+static float occ_sample(const uint8_t *occ, const uint32_t od[3], v3f p) {
+  float q[3] = {floorf(p.x * (float)od[0]), floorf(p.y * (float)od[1]), floorf(p.z * (float)od[2])};
+  uint32_t i[3];
+  for (int a = 0; a < 3; a++) {
+    float m = (float)(od[a] - 1u);
+    i[a] = !(q[a] >= 0.0f) ? 0u : (q[a] > m ? od[a] - 1u : (uint32_t)q[a]);
+  }
+  return (float)occ[((size_t)i[2] * od[1] + i[1]) * od[0] + i[0]] * INV255;
+}
+
+/* tf.SampleLevel(v, 0): 256-texel linear sampler, clamp (:894) */
+static void tf_sample(const uint8_t lut[256][4], float v, float s[4]) {
+  float t = clampf_(fmaf(v, 256.0f, -0.5f), 0.0f, 255.0f);
+  uint32_t i0 = (uint32_t)t;
+  uint32_t i1 = i0 + 1u < 256u ? i0 + 1u : 255u;
+  float f = t - (float)i0;
+  for (int c = 0; c < 4; c++) s[c] = lerpf_((float)lut[i0][c], (float)lut[i1][c], f) * INV255;
+}
+
+/* ------------------------------------------------------------- bricks */
+
+typedef struct brick_ctx { /* BrickCtx, :144-152 */
+  int ok;
+  float maxv;
+  v3f bl;
+  uint32_t slot;
+  float grad_vox;
+  float world_brick;
+} brick_ctx;
+
+typedef struct lod_cache { /* LodCache, :190-196 */
+  int valid;
+  int desired;
+  uint32_t scale;
+  uint32_t bc[3];
+  brick_ctx c;
+} lod_cache;
+
+typedef struct scene {
+  const orc_cube *cube;
+  const orc_bricks *br;
+  uint32_t *status;
+} scene;
+
+static inline uint32_t page_rd(const scene *s, uint32_t i) {
+  if (i >= s->br->page_words) {
+    *s->status |= 1u;
+    return 0xFFFFFFFFu;
+  }
+  return s->br->page[i];
+}
+
+/* bricks_lod_locate_ex, :198-247 */
+static brick_ctx lod_locate_ex(const scene *s, v3f p, float lod, uint32_t *scale_out,
+                               uint32_t bc_out[3]) {
+  brick_ctx c;
+  *scale_out = 1u;
+  bc_out[0] = bc_out[1] = bc_out[2] = 0u;
+  c.ok = 0;
+  c.maxv = 0.0f;
+  c.bl = mk3(0, 0, 0);
+  c.slot = 0;
+  c.grad_vox = 1.0f;
+  uint32_t nlev = page_rd(s, 0);
+  float bs[3] = {(float)page_rd(s, 1), (float)page_rd(s, 2), (float)page_rd(s, 3)};
+  float md = fmaxf(bs[0], fmaxf(bs[1], bs[2]));
+  c.world_brick = (BR_SLOT * (float)(1u << (nlev - 1u))) / md;
+  float base_v[3] = {clampf_(p.x * md, 0.0f, fmaxf(bs[0] - 0.001f, 0.0f)),
+                     clampf_(p.y * md, 0.0f, fmaxf(bs[1] - 0.001f, 0.0f)),
+                     clampf_(p.z * md, 0.0f, fmaxf(bs[2] - 0.001f, 0.0f))};
+  int desired = (int)clampf_(floorf(lod), 0.0f, (float)(nlev - 1u));
+  int last = (int)nlev - 1;
+  for (uint32_t step = 0; step < 4u; step++) {
+    int li = step < 3u ? desired + (int)step : last;
+    if (li < 0 || li > last || (step == 3u && li <= desired + 2)) continue;
+    uint32_t h = 4u + (uint32_t)li * 4u;
+    uint32_t off = page_rd(s, h), packed = page_rd(s, h + 1u), scale = page_rd(s, h + 2u);
+    uint32_t bd[3] = {packed & 1023u, (packed >> 10) & 1023u, packed >> 20};
+    float lv[3];
+    uint32_t bc[3];
+    for (int a = 0; a < 3; a++) {
+      lv[a] = base_v[a] / (float)scale;
+      uint32_t q = (uint32_t)lv[a] >> 7;
+      bc[a] = q < bd[a] - 1u ? q : bd[a] - 1u;
+    }
+    uint32_t bi = off + (bc[2] * bd[1] + bc[1]) * bd[0] + bc[0];
+    uint32_t e = page_rd(s, bi);
+    if (e == 0xFFFFFFFFu) continue;
+    uint32_t slot = e & 0xFFFFFFu;
+    if (slot >= s->br->nslots) {
+      *s->status |= 1u;
+      continue;
+    }
+    c.ok = 1;
+    c.maxv = (float)(e >> 24) / 255.0f;
+    c.slot = slot;
+    c.bl = mk3(lv[0] - (float)(bc[0] << 7), lv[1] - (float)(bc[1] << 7),
+               lv[2] - (float)(bc[2] << 7));
+    c.grad_vox = r3d_exp2f(lod) / (float)scale;
+    c.world_brick = (BR_SLOT * (float)scale) / md;
+    *scale_out = scale;
+    bc_out[0] = bc[0];
+    bc_out[1] = bc[1];
+    bc_out[2] = bc[2];
+    return c;
+  }
+  return c;
+}
+
+/* bricks_lod_locate_cached, :255-279 */
+static brick_ctx lod_locate_cached(const scene *s, v3f p, float lod, lod_cache *lc) {
+  uint32_t nlev = page_rd(s, 0);
+  int desired = (int)clampf_(floorf(lod), 0.0f, (float)(nlev - 1u));
+  if (lc->valid && lc->desired == desired) {
+    float bs[3] = {(float)page_rd(s, 1), (float)page_rd(s, 2), (float)page_rd(s, 3)};
+    float md = fmaxf(bs[0], fmaxf(bs[1], bs[2]));
+    float pv[3] = {p.x, p.y, p.z};
+    float lv[3];
+    uint32_t bc[3];
+    for (int a = 0; a < 3; a++) {
+      float base_v = clampf_(pv[a] * md, 0.0f, fmaxf(bs[a] - 0.001f, 0.0f));
+      lv[a] = base_v / (float)lc->scale;
+      bc[a] = (uint32_t)lv[a] >> 7;
+    }
+    if (bc[0] == lc->bc[0] && bc[1] == lc->bc[1] && bc[2] == lc->bc[2]) {
+      brick_ctx c = lc->c;
+      c.bl = mk3(lv[0] - (float)(bc[0] << 7), lv[1] - (float)(bc[1] << 7),
+                 lv[2] - (float)(bc[2] << 7));
+      return c;
+    }
+  }
+  uint32_t scale, bc[3];
+  brick_ctx c = lod_locate_ex(s, p, lod, &scale, bc);
+  lc->valid = c.ok;
+  lc->desired = desired;
+  lc->scale = scale;
+  lc->bc[0] = bc[0];
+  lc->bc[1] = bc[1];
+  lc->bc[2] = bc[2];
+  lc->c = c;
+  return c;
+}
+
+/* bricks_fetch at atlas lod 0 (:284-288): clamp to [0.5, 127.5] inside the
+ * brick (no cross-brick filtering), trilinear in the slot */
+static float brick_fetch(const scene *s, uint32_t slot, v3f bl) {
+  const uint8_t *g = s->br->pool + (size_t)slot * (128u * 128u * 128u);
+  float lx = clampf_(bl.x, 0.5f, 127.5f), ly = clampf_(bl.y, 0.5f, 127.5f),
+        lz = clampf_(bl.z, 0.5f, 127.5f);
+  return tri_u8(g, 128u, 128u, 128u, lx - 0.5f, ly - 0.5f, lz - 0.5f);
+}
+
+/* ------------------------------------------------------------ the march */
+
+typedef struct ray_out {
+  float rgb[3];
+  uint32_t steps;
+  uint32_t mip_index;
+  int store; /* 0: pixel outside the viewport */
+} ray_out;
+
+/* main(), :505-1038, for one dispatch thread (tx, ty) of the view */
+static void march(const r3d_frame_params *pc, const scene *s, const uint8_t lut[256][4],
+                  const orc_opts *o, uint32_t tx, uint32_t ty, ray_out *out) {
+  int half = (pc->view_flags & R3D_VIEW_HALF) != 0u;
+  uint32_t px = half ? tx * 2u : tx, py = half ? ty * 2u : ty;
+  out->steps = 0;
+  out->mip_index = 0;
+  out->store = 0;
+  if (px >= pc->viewport[0] || py >= pc->viewport[1]) return;
+  out->store = 1;
+  int ortho = (pc->view_flags & R3D_VIEW_ORTHO) != 0u;
+  int bricks = pc->brick_mode != 0u;
+  int lodb = bricks && (pc->brick_mode & R3D_BRICK_LOD_FLAG) != 0u;
+
+  /* pix_ndc / ray_dir / ray_origin, :469-486 */
+  float ux = ((float)px + 0.5f) / (float)pc->viewport[0];
+  float uy = ((float)py + 0.5f) / (float)pc->viewport[1];
+  float nx = ux * 2.0f - 1.0f, ny = 1.0f - uy * 2.0f;
+  v3f fwd = mk3(pc->cam_forward[0], pc->cam_forward[1], pc->cam_forward[2]);
+  v3f rt = mk3(pc->cam_right[0], pc->cam_right[1], pc->cam_right[2]);
+  v3f up = mk3(pc->cam_up[0], pc->cam_up[1], pc->cam_up[2]);
+  v3f dir;
+  if (ortho)
+    dir = norm3(fwd);
+  else
+    dir = norm3(mk3(fmaf(ny, up.x, fmaf(nx, rt.x, fwd.x)), fmaf(ny, up.y, fmaf(nx, rt.y, fwd.y)),
+                    fmaf(ny, up.z, fmaf(nx, rt.z, fwd.z))));
+  if (pc->mode == R3D_MODE_RAYDIR) {
+    out->rgb[0] = fmaf(dir.x, 0.5f, 0.5f);
+    out->rgb[1] = fmaf(dir.y, 0.5f, 0.5f);
+    out->rgb[2] = fmaf(dir.z, 0.5f, 0.5f);
+    return;
+  }
+  v3f org = mk3(pc->cam_origin[0], pc->cam_origin[1], pc->cam_origin[2]);
+  if (ortho)
+    org = mk3(fmaf(ny, up.x, fmaf(nx, rt.x, org.x)), fmaf(ny, up.y, fmaf(nx, rt.y, org.y)),
+              fmaf(ny, up.z, fmaf(nx, rt.z, org.z)));
+
+  /* voxel pitch, LOD ceiling, extent (:647-683, :305-314); the ray-cone
+   * footprint is measured in voxels by multiplying with vox_inv = 1/voxel */
+  float voxel, vox_inv, max_lod;
+  v3f ext = mk3(1.0f, 1.0f, 1.0f);
+  uint32_t nlev = 0;
+  float md = 0.0f; /* bricks: largest base dimension */
+  if (lodb) {
+    nlev = page_rd(s, 0);
+    float bs[3] = {(float)page_rd(s, 1), (float)page_rd(s, 2), (float)page_rd(s, 3)};
+    md = fmaxf(bs[0], fmaxf(bs[1], bs[2]));
+    voxel = 1.0f / md;
+    vox_inv = md;
+    max_lod = (float)(nlev - 1u);
+    ext = mk3(bs[0] / md, bs[1] / md, bs[2] / md);
+  } else {
+    const uint32_t *d = s->cube->dim[0];
+    uint32_t cm = d[0] > d[1] ? d[0] : d[1];
+    if (d[2] > cm) cm = d[2];
+    voxel = 1.0f / (float)cm;
+    vox_inv = (float)cm;
+    max_lod = fminf(pc->max_mip, (float)(s->cube->nlevels - 1u));
+  }
+  /* model transform, common.slang:45-52 */
+  v3f c = mk3(ext.x * 0.5f, ext.y * 0.5f, ext.z * 0.5f);
+  v3f r0 = mk3(pc->vol_r0[0], pc->vol_r0[1], pc->vol_r0[2]);
+  v3f r1 = mk3(pc->vol_r1[0], pc->vol_r1[1], pc->vol_r1[2]);
+  v3f r2 = mk3(pc->vol_r2[0], pc->vol_r2[1], pc->vol_r2[2]);
+  v3f q = mk3((org.x - pc->vol_tx) - c.x, (org.y - pc->vol_ty) - c.y, (org.z - pc->vol_tz) - c.z);
+  v3f ro = mk3(fmaf(r2.x, q.z, fmaf(r1.x, q.y, r0.x * q.x)) + c.x,
+               fmaf(r2.y, q.z, fmaf(r1.y, q.y, r0.y * q.x)) + c.y,
+               fmaf(r2.z, q.z, fmaf(r1.z, q.y, r0.z * q.x)) + c.z);
+  dir = mk3(fmaf(r2.x, dir.z, fmaf(r1.x, dir.y, r0.x * dir.x)),
+            fmaf(r2.y, dir.z, fmaf(r1.y, dir.y, r0.y * dir.x)),
+            fmaf(r2.z, dir.z, fmaf(r1.z, dir.y, r0.z * dir.x)));
+
+  /* clip boxes and t range, :686-714 */
+  float lo[3] = {0.0f, 0.0f, 0.0f}, hi[3] = {ext.x, ext.y, ext.z};
+  float t_lo = 0.0f, t_hi = 1e30f;
+  if (lodb && (pc->view_flags & R3D_VIEW_CROP) != 0u) {
+    float clo[3] = {pc->slab_x0 / md, pc->slab_y0 / md, pc->slab_z0 / md};
+    float cx[3] = {pc->slab_px / md, pc->slab_py / md, pc->slab_nx / md};
+    for (int a = 0; a < 3; a++) {
+      lo[a] = clampf_(clo[a], 0.0f, hi[a]);
+      hi[a] = clampf_(clo[a] + cx[a], lo[a], hi[a]);
+    }
+  } else if (lodb && pc->slab_depth > 0u) {
+    if ((pc->view_flags & R3D_VIEW_OBLIQUE) != 0u) {
+      t_lo = pc->slab_z0 / md;
+      t_hi = (pc->slab_z0 + (float)pc->slab_depth) / md;
+    } else {
+      uint32_t axc = (pc->view_flags >> 8) & 3u;
+      int a = axc == 1u ? 0 : (axc == 2u ? 1 : 2);
+      float e = hi[a];
+      lo[a] = clampf_(pc->slab_z0 / md, 0.0f, e);
+      hi[a] = clampf_((pc->slab_z0 + (float)pc->slab_depth) / md, lo[a], e);
+    }
+  }
+  /* box_hit, :489-495 */
+  float dv[3] = {dir.x, dir.y, dir.z}, ov[3] = {ro.x, ro.y, ro.z};
+  float tmn[3], tmx[3];
+  for (int a = 0; a < 3; a++) {
+    float inv = 1.0f / dv[a];
+    float t0 = (lo[a] - ov[a]) * inv, t1 = (hi[a] - ov[a]) * inv;
+    tmn[a] = fminf(t0, t1);
+    tmx[a] = fmaxf(t0, t1);
+  }
+  float hx = fmaxf(fmaxf(tmn[0], tmn[1]), tmn[2]);
+  float hy = fminf(fminf(tmx[0], tmx[1]), tmx[2]);
+  float tn = fmaxf(hx, t_lo), tf_ = fminf(hy, t_hi);
+  if (tn >= tf_) {
+    out->rgb[0] = BG_R;
+    out->rgb[1] = BG_G;
+    out->rgb[2] = BG_B;
+    return;
+  }
+
+  /* cone, step, jitter, budget, gates (:722-762) */
+  float cone = (2.0f * sqrtf(dot3(up, up))) / (float)pc->viewport[1];
+  float dt = pc->step_voxels * voxel;
+  float jitter = hash12(px, py, pc->frame_index);
+  float t = fmaf(jitter, dt, tn);
+  float mip_max = 0.0f, first_hit = -1.0f;
+  float acc[4] = {0, 0, 0, 0};
+  uint32_t steps = 0, mip_index = 0;
+  int composite = pc->mode == R3D_MODE_FULL || pc->mode == R3D_MODE_FLAT;
+  int shaded = pc->mode == R3D_MODE_FULL;
+  uint32_t ray_budget = lodb ? (shaded ? 192u : 256u) : MAX_STEPS;
+  float span_step = fmaxf((tf_ - tn) / ((float)ray_budget * dt), 1.0f);
+  float bs = OCC_BLOCK * voxel;
+  float occ_gate = fmaxf(pc->skip_gate, 0.5f / 255.0f);
+  float opac_k = pc->density * pc->step_voxels;
+
+  /* shading constants (:988-998): key light, headlight l = -dir and its
+   * half vector normalize(l - dir) are per-ray constants */
+  v3f key = norm3(mk3(0.4f, 0.8f, -0.4f));
+  v3f l = mk3(-dir.x, -dir.y, -dir.z);
+  v3f hv = norm3(mk3(l.x - dir.x, l.y - dir.y, l.z - dir.z));
+
+  lod_cache lc;
+  memset(&lc, 0, sizeof lc);
+  lc.valid = 0;
+  lc.desired = -1;
+  lc.scale = 1u;
+  lc.bc[0] = lc.bc[1] = lc.bc[2] = 0u;
+  brick_ctx b;
+  memset(&b, 0, sizeof b);
+  b.world_brick = 128.0f * voxel;
+
+  while (t < tf_ && steps < ray_budget) {
+    steps++;
+    /* LOD and step (:772-779) */
+    float foot = ortho ? cone : t * cone;
+    float lod = clampf_(r3d_log2f(fmaxf(foot * vox_inv, 1.0f)) + pc->lod_bias, 0.0f, max_lod);
+    float lod_step = fmaxf(r3d_exp2f(lod), span_step);
+    v3f p = mk3(fmaf(t, dir.x, ro.x), fmaf(t, dir.y, ro.y), fmaf(t, dir.z, ro.z));
+
+    float v;
+    if (lodb) {
+      b = lod_locate_cached(s, p, lod, &lc);
+      v = b.ok ? brick_fetch(s, b.slot, b.bl) : 0.0f;
+    } else {
+      v = cube_sample(s->cube, p, lod);
+    }
+    int cut = v < pc->threshold; /* :826-827 */
+    if (cut) v = 0.0f;
+
+    /* empty-space skip (:829-869) */
+    int void_blk = 0;
+    float bsz = bs;
+    if (lodb) {
+      float bgate = fmaxf(occ_gate, 4.5f / 255.0f);
+      if (pc->mode == R3D_MODE_MIP && b.ok && b.maxv <= mip_max) {
+        void_blk = 1;
+        bsz = b.world_brick;
+      } else if (v < bgate && b.maxv < bgate) {
+        void_blk = 1;
+        bsz = b.world_brick;
+      }
+    } else if (v < occ_gate && occ_sample(s->cube->occ, s->cube->odim, p) < occ_gate) {
+      void_blk = 1;
+    }
+    if (void_blk) {
+      float pv[3] = {p.x, p.y, p.z};
+      float tex[3];
+      for (int a = 0; a < 3; a++) {
+        float nextp = (floorf(pv[a] / bsz) + (dv[a] > 0.0f ? 1.0f : 0.0f)) * bsz;
+        tex[a] = fabsf(dv[a]) > 1e-8f ? (nextp - ov[a]) / dv[a] : 1e30f;
+      }
+      t = fmaxf(fminf(fminf(tex[0], tex[1]), tex[2]), t) + bsz * 0.01f;
+      continue;
+    }
+
+    if (v > mip_max) { /* :871 */
+      mip_max = v;
+      mip_index = steps;
+    }
+    if (pc->mode == R3D_MODE_MIP && mip_max >= 0.999f) break; /* :888 */
+    if (first_hit < 0.0f && v > 0.05f) first_hit = t;         /* :891 */
+
+    if (composite && !cut) {
+      float sm[4];
+      tf_sample(lut, v, sm);
+      /* opacity correction (:906) */
+      float a = 1.0f - r3d_powf(1.0f - sm[3], opac_k * lod_step);
+      if (a > 0.003f) {
+        float col[3] = {sm[0], sm[1], sm[2]};
+        if (shaded) {
+          float g[3];
+          if (o->quality == R3D_QUALITY_FAST) { /* :919-955 */
+            const float ir3 = 0.57735026919f, renorm = 0.86602540378f;
+            float q0, q1, q2, q3;
+            if (lodb) {
+              float ev = b.grad_vox * ir3;
+              q0 = brick_fetch(s, b.slot, mk3(b.bl.x + ev, b.bl.y - ev, b.bl.z - ev));
+              q1 = brick_fetch(s, b.slot, mk3(b.bl.x - ev, b.bl.y - ev, b.bl.z + ev));
+              q2 = brick_fetch(s, b.slot, mk3(b.bl.x - ev, b.bl.y + ev, b.bl.z - ev));
+              q3 = brick_fetch(s, b.slot, mk3(b.bl.x + ev, b.bl.y + ev, b.bl.z + ev));
+            } else {
+              float ee = (voxel * lod_step) * ir3;
+              q0 = cube_sample(s->cube, mk3(p.x + ee, p.y - ee, p.z - ee), lod);
+              q1 = cube_sample(s->cube, mk3(p.x - ee, p.y - ee, p.z + ee), lod);
+              q2 = cube_sample(s->cube, mk3(p.x - ee, p.y + ee, p.z - ee), lod);
+              q3 = cube_sample(s->cube, mk3(p.x + ee, p.y + ee, p.z + ee), lod);
+            }
+            g[0] = (((q0 - q1) - q2) + q3) * renorm;
+            g[1] = (((-q0 - q1) + q2) + q3) * renorm;
+            g[2] = (((-q0 + q1) - q2) + q3) * renorm;
+          } else { /* :957-986 */
+            if (lodb) {
+              float ev = b.grad_vox;
+              v3f u = b.bl;
+              g[0] = brick_fetch(s, b.slot, mk3(u.x + ev, u.y, u.z)) -
+                     brick_fetch(s, b.slot, mk3(u.x - ev, u.y, u.z));
+              g[1] = brick_fetch(s, b.slot, mk3(u.x, u.y + ev, u.z)) -
+                     brick_fetch(s, b.slot, mk3(u.x, u.y - ev, u.z));
+              g[2] = brick_fetch(s, b.slot, mk3(u.x, u.y, u.z + ev)) -
+                     brick_fetch(s, b.slot, mk3(u.x, u.y, u.z - ev));
+            } else {
+              float e = voxel * lod_step;
+              g[0] = cube_sample(s->cube, mk3(p.x + e, p.y, p.z), lod) -
+                     cube_sample(s->cube, mk3(p.x - e, p.y, p.z), lod);
+              g[1] = cube_sample(s->cube, mk3(p.x, p.y + e, p.z), lod) -
+                     cube_sample(s->cube, mk3(p.x, p.y - e, p.z), lod);
+              g[2] = cube_sample(s->cube, mk3(p.x, p.y, p.z + e), lod) -
+                     cube_sample(s->cube, mk3(p.x, p.y, p.z - e), lod);
+            }
+          }
+          v3f gv = mk3(g[0], g[1], g[2]);
+          float gm = sqrtf(dot3(gv, gv));
+          if (gm > 1e-4f) { /* :988-998 */
+            float inv = 1.0f / gm;
+            v3f n = mk3(gv.x * inv, gv.y * inv, gv.z * inv);
+            float diff = fmaf(0.3f, fabsf(dot3(n, key)), 0.7f * fabsf(dot3(n, l)));
+            float spec = r3d_powi24f(fabsf(dot3(n, hv))) * 0.3f;
+            float lit = fmaf(0.75f, diff, 0.25f);
+            float w = satf(gm * 6.0f);
+            float lm = fmaf(w, lit - 1.0f, 1.0f);
+            float sw = spec * w;
+            for (int k = 0; k < 3; k++) col[k] = fmaf(col[k], lm, sw);
+          }
+        }
+        /* front-to-back compositing and early termination (:1015-1017) */
+        float wgt = (1.0f - acc[3]) * a;
+        for (int k = 0; k < 3; k++) acc[k] = fmaf(wgt, col[k], acc[k]);
+        acc[3] = acc[3] + wgt;
+        if (acc[3] >= o->alpha_cutoff) break;
+      }
+    }
+    t = fmaf(dt, lod_step, t); /* :1020 */
+  }
+
+  /* finalize (:1023-1038) */
+  out->steps = steps;
+  out->mip_index = mip_index;
+  if (pc->mode == R3D_MODE_HEATMAP) {
+    float x = (float)steps / 1024.0f;
+    out->rgb[0] = x;
+    out->rgb[1] = 1.0f - fabsf(x - 0.5f) * 2.0f;
+    out->rgb[2] = 1.0f - x;
+  } else if (pc->mode == R3D_MODE_DEPTH) {
+    float d = first_hit < 0.0f ? 0.0f : 1.0f - satf(first_hit * 0.5f);
+    out->rgb[0] = out->rgb[1] = out->rgb[2] = d;
+  } else if (composite) {
+    float tr = 1.0f - acc[3];
+    out->rgb[0] = fmaf(tr, BG_R, acc[0]);
+    out->rgb[1] = fmaf(tr, BG_G, acc[1]);
+    out->rgb[2] = fmaf(tr, BG_B, acc[2]);
+  } else {
+    float m = mip_max * pc->density;
+    out->rgb[0] = out->rgb[1] = out->rgb[2] = m;
+  }
+}
+
+static int check_view(const r3d_frame_params *p, const orc_cube *cube, const orc_bricks *br) {
+  if (p->slab_grid || p->clip_valid || p->overlay_flags ||
+      (p->view_flags & (R3D_VIEW_SURF | R3D_VIEW_STRETCH)) || p->mode >= R3D_MODE_COUNT)
+    return -1;
+  if (p->brick_mode) {
+    if (!(p->brick_mode & R3D_BRICK_LOD_FLAG) || !br || !br->page || br->page_words < 64u)
+      return -1;
+    uint32_t nlev = br->page[0];
+    if (nlev < 1u || nlev > 15u) return -1;
+  } else if (!cube || !cube->nlevels || !cube->occ) {
+    return -1;
+  }
+  return 0;
+}
+
+int orc_render_view(const r3d_frame_params *p, const orc_cube *cube, const orc_bricks *bricks,
+                    const uint8_t lut[256][4], const orc_opts *o, uint8_t *img, uint32_t img_w,
+                    uint32_t img_h, orc_aux *aux) {
+  if (check_view(p, cube, bricks) != 0) return -1;
+  uint32_t vw = p->viewport[0], vh = p->viewport[1];
+  uint32_t ox = p->view_org & 0xffffu, oy = p->view_org >> 16;
+  if (ox + vw > img_w || oy + vh > img_h) return -1;
+  int half = (p->view_flags & R3D_VIEW_HALF) != 0u;
+  uint32_t gw = half ? (vw + 1u) / 2u : vw, gh = half ? (vh + 1u) / 2u : vh;
+  uint64_t total = 0;
+  uint32_t status = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : total) reduction(| : status) \
+    num_threads(o->threads > 0 ? o->threads : omp_get_max_threads())
+  for (uint32_t ty = 0; ty < gh; ty++) {
+    uint32_t st = 0;
+    scene s = {cube, bricks, &st};
+    for (uint32_t tx = 0; tx < gw; tx++) {
+      ray_out r;
+      march(p, &s, lut, o, tx, ty, &r);
+      if (!r.store) continue;
+      total += r.steps;
+      uint32_t lx = half ? tx * 2u : tx, ly = half ? ty * 2u : ty;
+      uint8_t px[4] = {unorm8(r.rgb[0]), unorm8(r.rgb[1]), unorm8(r.rgb[2]), 255};
+      for (uint32_t k = 0; k < (half ? 4u : 1u); k++) {
+        uint32_t ax = lx + (k & 1u), ay = ly + (k >> 1);
+        if (ax >= vw || ay >= vh) continue;
+        size_t i = (size_t)(oy + ay) * img_w + (ox + ax);
+        memcpy(img + i * 4u, px, 4);
+        if (aux && aux->steps) aux->steps[i] = r.steps;
+        if (aux && aux->mip_index) aux->mip_index[i] = r.mip_index;
+      }
+    }
+    status |= st;
+  }
+  if (aux) {
+    aux->total_steps = total;
+    aux->status = status;
+  }
+  return 0;
+}
+
+int orc_render_pixels(const r3d_frame_params *p, const orc_cube *cube, const orc_bricks *bricks,
+                      const uint8_t lut[256][4], const orc_opts *o, const uint32_t *xy,
+                      uint32_t n, uint8_t *out_rgba, uint32_t *steps, uint32_t *mip_index) {
+  if (check_view(p, cube, bricks) != 0) return -1;
+#pragma omp parallel for schedule(dynamic, 16) \
+    num_threads(o->threads > 0 ? o->threads : omp_get_max_threads())
+  for (uint32_t i = 0; i < n; i++) {
+    uint32_t st = 0;
+    scene s = {cube, bricks, &st};
+    ray_out r;
+    march(p, &s, lut, o, xy[2 * i], xy[2 * i + 1], &r);
+    uint8_t px[4] = {0, 0, 0, 0};
+    if (r.store) {
+      px[0] = unorm8(r.rgb[0]);
+      px[1] = unorm8(r.rgb[1]);
+      px[2] = unorm8(r.rgb[2]);
+      px[3] = 255;
+    }
+    memcpy(out_rgba + (size_t)i * 4u, px, 4);
+    if (steps) steps[i] = r.steps;
+    if (mip_index) mip_index[i] = r.mip_index;
+  }
+  return 0;
+}
+
+/* log2 / exp2 / pow / x^24 of the shared header, for the device bit check */
+void orc_fmath_eval(const float *x, const float *y, float *out, uint32_t n) {
+  for (uint32_t i = 0; i < n; i++) {
+    out[4 * i + 0] = r3d_log2f(x[i]);
+    out[4 * i + 1] = r3d_exp2f(x[i]);
+    out[4 * i + 2] = r3d_powf(x[i], y[i]);
+    out[4 * i + 3] = r3d_powi24f(x[i]);
+  }
+}
+
+/* ------------------------------------------------------- data builders */
+
+uint32_t orc_mip_levels(uint32_t nx, uint32_t ny, uint32_t nz, uint32_t dims[][3]) {
+  uint32_t maxdim = nx > ny ? nx : ny;
+  if (nz > maxdim) maxdim = nz;
+  uint32_t mips = 1;
+  while ((maxdim >> mips) >= 1u && mips < 16u) mips++;
+  for (uint32_t m = 0; m < mips; m++) {
+    dims[m][0] = nx >> m ? nx >> m : 1u;
+    dims[m][1] = ny >> m ? ny >> m : 1u;
+    dims[m][2] = nz >> m ? nz >> m : 1u;
+  }
+  return mips;
+}
+
+void orc_downsample(const uint8_t *src, uint32_t sx, uint32_t sy, uint32_t sz, uint8_t *dst,
+                    uint32_t dx, uint32_t dy, uint32_t dz) {
+  for (uint32_t z = 0; z < dz; z++)
+    for (uint32_t y = 0; y < dy; y++)
+      for (uint32_t x = 0; x < dx; x++) {
+        uint32_t sum = 4u;
+        for (uint32_t k = 0; k < 8u; k++) {
+          uint32_t xx = 2u * x + (k & 1u), yy = 2u * y + ((k >> 1) & 1u), zz = 2u * z + (k >> 2);
+          if (xx >= sx) xx = sx - 1u;
+          if (yy >= sy) yy = sy - 1u;
+          if (zz >= sz) zz = sz - 1u;
+          sum += src[((size_t)zz * sy + yy) * sx + xx];
+        }
+        dst[((size_t)z * dy + y) * dx + x] = (uint8_t)(sum / 8u);
+      }
+}
+
+void orc_occupancy(const uint8_t *vox, uint32_t nx, uint32_t ny, uint32_t nz, uint8_t *out) {
+  uint32_t ox = (nx + 7u) / 8u, oy = (ny + 7u) / 8u, oz = (nz + 7u) / 8u;
+  size_t n = (size_t)ox * oy * oz;
+  uint8_t *raw = malloc(n);
+  if (!raw) return;
+  for (uint32_t bz = 0; bz < oz; bz++)
+    for (uint32_t by = 0; by < oy; by++)
+      for (uint32_t bx = 0; bx < ox; bx++) {
+        uint8_t m = 0;
+        for (uint32_t z = bz * 8u; z < bz * 8u + 8u && z < nz; z++)
+          for (uint32_t y = by * 8u; y < by * 8u + 8u && y < ny; y++)
+            for (uint32_t x = bx * 8u; x < bx * 8u + 8u && x < nx; x++) {
+              uint8_t v = vox[((size_t)z * ny + y) * nx + x];
+              if (v > m) m = v;
+            }
+        raw[((size_t)bz * oy + by) * ox + bx] = m;
+      }
+  for (uint32_t z = 0; z < oz; z++)
+    for (uint32_t y = 0; y < oy; y++)
+      for (uint32_t x = 0; x < ox; x++) {
+        uint8_t m = 0;
+        for (int dz = -1; dz <= 1; dz++)
+          for (int dy = -1; dy <= 1; dy++)
+            for (int dx = -1; dx <= 1; dx++) {
+              int zz = (int)z + dz, yy = (int)y + dy, xx = (int)x + dx;
+              if (zz < 0 || yy < 0 || xx < 0 || zz >= (int)oz || yy >= (int)oy || xx >= (int)ox)
+                continue;
+              uint8_t v = raw[((size_t)zz * oy + (size_t)yy) * ox + (size_t)xx];
+              if (v > m) m = v;
+            }
+        out[((size_t)z * oy + y) * ox + x] = m;
+      }
+  free(raw);
+}
+
+static uint32_t ceil_div(uint32_t a, uint32_t b) { return (a + b - 1u) / b; }
+
+uint32_t orc_lod_page_words(uint32_t nx, uint32_t ny, uint32_t nz, uint32_t nlev) {
+  uint32_t w = R3D_BRICK_PAGE_HEADER;
+  for (uint32_t l = 0; l < nlev; l++) {
+    uint32_t s = 1u << l;
+    w += ceil_div(ceil_div(nx, s), 128u) * ceil_div(ceil_div(ny, s), 128u) *
+         ceil_div(ceil_div(nz, s), 128u);
+  }
+  return w;
+}
+
+int64_t orc_build_lod_bricks(const uint8_t *vox, uint32_t nx, uint32_t ny, uint32_t nz,
+                             uint32_t nlev, uint32_t min_max, uint32_t *page,
+                             uint32_t page_words, uint8_t *pool, uint64_t pool_slots) {
+  if (nlev < 1u || nlev > 15u || page_words != orc_lod_page_words(nx, ny, nz, nlev)) return -1;
+  /* padded level grids: E[l] = 128 * bricks per axis; level 0 reads vox */
+  uint32_t bd[16][3], E[16][3];
+  uint8_t *lev[16] = {0};
+  for (uint32_t l = 0; l < nlev; l++) {
+    uint32_t s = 1u << l;
+    bd[l][0] = ceil_div(ceil_div(nx, s), 128u);
+    bd[l][1] = ceil_div(ceil_div(ny, s), 128u);
+    bd[l][2] = ceil_div(ceil_div(nz, s), 128u);
+    for (int a = 0; a < 3; a++) E[l][a] = bd[l][a] * 128u;
+  }
+#define L0(X, Y, Z) \
+  ((X) < nx && (Y) < ny && (Z) < nz ? vox[((size_t)(Z) * ny + (Y)) * nx + (X)] : (uint8_t)0)
+  for (uint32_t l = 1; l < nlev; l++) {
+    lev[l] = malloc((size_t)E[l][0] * E[l][1] * E[l][2]);
+    if (!lev[l]) goto fail;
+    for (uint32_t z = 0; z < E[l][2]; z++)
+      for (uint32_t y = 0; y < E[l][1]; y++)
+        for (uint32_t x = 0; x < E[l][0]; x++) {
+          uint32_t sum = 4u;
+          for (uint32_t k = 0; k < 8u; k++) {
+            uint32_t xx = 2u * x + (k & 1u), yy = 2u * y + ((k >> 1) & 1u),
+                     zz = 2u * z + (k >> 2);
+            if (l == 1u)
+              sum += L0(xx, yy, zz);
+            else if (xx < E[l - 1][0] && yy < E[l - 1][1] && zz < E[l - 1][2])
+              sum += lev[l - 1][((size_t)zz * E[l - 1][1] + yy) * E[l - 1][0] + xx];
+          }
+          lev[l][((size_t)z * E[l][1] + y) * E[l][0] + x] = (uint8_t)(sum / 8u);
+        }
+  }
+  memset(page, 0, R3D_BRICK_PAGE_HEADER * sizeof *page);
+  page[0] = nlev;
+  page[1] = nx;
+  page[2] = ny;
+  page[3] = nz;
+  uint32_t off = 0;
+  int64_t slot = 0;
+  for (uint32_t l = 0; l < nlev; l++) {
+    page[4u + l * 4u] = R3D_BRICK_PAGE_HEADER + off;
+    page[5u + l * 4u] = bd[l][0] | (bd[l][1] << 10) | (bd[l][2] << 20);
+    page[6u + l * 4u] = 1u << l;
+    for (uint32_t bz = 0; bz < bd[l][2]; bz++)
+      for (uint32_t by = 0; by < bd[l][1]; by++)
+        for (uint32_t bx = 0; bx < bd[l][0]; bx++) {
+          uint32_t m = 0;
+          for (uint32_t z = 0; z < 128u; z++)
+            for (uint32_t y = 0; y < 128u; y++)
+              for (uint32_t x = 0; x < 128u; x++) {
+                uint32_t X = bx * 128u + x, Y = by * 128u + y, Z = bz * 128u + z;
+                uint32_t v = l == 0u ? L0(X, Y, Z)
+                                     : lev[l][((size_t)Z * E[l][1] + Y) * E[l][0] + X];
+                if (v > m) m = v;
+              }
+          uint32_t idx = R3D_BRICK_PAGE_HEADER + off + (bz * bd[l][1] + by) * bd[l][0] + bx;
+          if (m >= min_max) {
+            page[idx] = (uint32_t)slot | (m << 24);
+            if (pool && (uint64_t)slot < pool_slots) {
+              uint8_t *dst = pool + (size_t)slot * (128u * 128u * 128u);
+              for (uint32_t z = 0; z < 128u; z++)
+                for (uint32_t y = 0; y < 128u; y++)
+                  for (uint32_t x = 0; x < 128u; x++) {
+                    uint32_t X = bx * 128u + x, Y = by * 128u + y, Z = bz * 128u + z;
+                    dst[((size_t)z * 128u + y) * 128u + x] =
+                        l == 0u ? L0(X, Y, Z) : lev[l][((size_t)Z * E[l][1] + Y) * E[l][0] + X];
+                  }
+            }
+            slot++;
+          } else {
+            page[idx] = R3D_BRICK_ABSENT;
+          }
+        }
+    off += bd[l][0] * bd[l][1] * bd[l][2];
+  }
+#undef L0
+  for (uint32_t l = 1; l < nlev; l++) free(lev[l]);
+  return slot;
+fail:
+  for (uint32_t l = 1; l < nlev; l++) free(lev[l]);
+  return -1;
+}
+
+/* ------------------------------------------------- host-side helpers */
+
+/* forward_of + r3d_camera_basis, src/core/camera.c:12-15,65-75 */
+void orc_camera_basis(float yaw, float pitch, float fov_y, float aspect, float right[3],
+                      float up[3], float fwd[3]) {
+  float cp = cosf(pitch);
+  float f[3] = {sinf(yaw) * cp, sinf(pitch), cosf(yaw) * cp};
+  /* cross(f, (0,1,0)) = (-f.z, 0, f.x) */
+  float r[3] = {f[1] * 0.0f - f[2] * 1.0f, f[2] * 0.0f - f[0] * 0.0f, f[0] * 1.0f - f[1] * 0.0f};
+  float rl = sqrtf(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+  if (rl > 0.0f) {
+    float inv = 1.0f / rl;
+    r[0] *= inv, r[1] *= inv, r[2] *= inv;
+  } else {
+    r[0] = r[1] = r[2] = 0.0f;
+  }
+  if (sqrtf(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]) == 0.0f) {
+    r[0] = 1.0f;
+    r[1] = r[2] = 0.0f;
+  }
+  float u[3] = {r[1] * f[2] - r[2] * f[1], r[2] * f[0] - r[0] * f[2], r[0] * f[1] - r[1] * f[0]};
+  float t = tanf(fov_y * 0.5f);
+  for (int a = 0; a < 3; a++) {
+    right[a] = r[a] * (t * aspect);
+    up[a] = u[a] * t;
+    fwd[a] = f[a];
+  }
+}
+
+/* orbit_sync, src/core/camera.c:32-34 */
+void orc_orbit_pos(float yaw, float pitch, const float target[3], float dist, float pos[3]) {
+  float cp = cosf(pitch);
+  float f[3] = {sinf(yaw) * cp, sinf(pitch), cosf(yaw) * cp};
+  for (int a = 0; a < 3; a++) pos[a] = target[a] - f[a] * dist;
+}
+
+/* r3d_tf_build, src/core/transfer.c:5-23 */
+void orc_tf_build(const uint8_t *values, const uint8_t (*rgba)[4], uint32_t npts,
+                  uint8_t lut[256][4]) {
+  for (uint32_t i = 0; i < 256u; i++) {
+    uint32_t lo = 0, hi = npts - 1u;
+    for (uint32_t k = 0; k + 1u < npts; k++)
+      if (values[k] <= i && i <= values[k + 1u]) {
+        lo = k;
+        hi = k + 1u;
+        break;
+      }
+    uint32_t span = (uint32_t)(values[hi] - values[lo]);
+    uint32_t tn = span ? i - values[lo] : 0u, td = span ? span : 1u;
+    for (int c = 0; c < 4; c++)
+      lut[i][c] = (uint8_t)(((uint32_t)rgba[lo][c] * (td - tn) + (uint32_t)rgba[hi][c] * tn) / td);
+  }
+}
+
+/* r3d_lod_pick / r3d_lod_fallback, src/core/lod.h:8-26 */
+uint32_t orc_lod_pick(float distance, float pixel_cone, float base_voxels, uint32_t nlevels) {
+  if (!nlevels) return 0;
+  float fp = fmaxf(distance * pixel_cone * base_voxels, 1.0f);
+  int level = (int)floorf(log2f(fp));
+  if (level < 0) level = 0;
+  if (level >= (int)nlevels) level = (int)nlevels - 1;
+  return (uint32_t)level;
+}
+
+uint32_t orc_lod_fallback(uint32_t desired, uint32_t ordinal, uint32_t nlevels) {
+  if (!nlevels || desired >= nlevels || ordinal >= nlevels) return UINT32_MAX;
+  uint32_t coarse = nlevels - desired;
+  if (ordinal < coarse) return desired + ordinal;
+  return desired - 1u - (ordinal - coarse);
+}
+
+/* m3_ypr, src/core/mathx.h:34-43 (rows; M = Ry * Rx * Rz) */
+void orc_m3_ypr(float yaw, float pitch, float roll, float rows[3][3]) {
+  float cy = cosf(yaw), sy = sinf(yaw), cp = cosf(pitch), sp = sinf(pitch), cr = cosf(roll),
+        sr = sinf(roll);
+  rows[0][0] = cy * cr + sy * sp * sr;
+  rows[0][1] = -cy * sr + sy * sp * cr;
+  rows[0][2] = sy * cp;
+  rows[1][0] = cp * sr;
+  rows[1][1] = cp * cr;
+  rows[1][2] = -sp;
+  rows[2][0] = -sy * cr + cy * sp * sr;
+  rows[2][1] = sy * sr + cy * sp * cr;
+  rows[2][2] = cy * cp;
+}

@@ -1,0 +1,119 @@
+/* CPU oracle for the volume raycast: test infrastructure, not product code.
+ *
+ * A plain-C restatement of render3d's raycast compute shader
+ * (src/shaders/raycast.slang:117-295,409-416,457-495,505-1039 and
+ * src/shaders/common.slang:44-61) plus the data the shader samples: mip chain,
+ * 8^3 occupancy grid (src/vk/vkbackend.c:794-870,944-983), LOD brick pyramid
+ * and page table (src/vk/vkbackend.c:4184-4206, tools/lodpack/main.c:203-230).
+ *
+ * Texture units are restated as exact FP32 arithmetic: clamp-to-edge
+ * trilinear at texel centres, linear blending between mip floor(lod) and
+ * floor(lod)+1, 1-D linear TF lookup at v*256-0.5, and round-to-nearest RGBA8
+ * stores.  Every floating-point step is written out in a fixed order with
+ * explicit fmaf and no contraction, so that the sm_100a kernels, which follow
+ * the same arithmetic, reproduce it bit for bit.
+ *
+ * Only the test suite, the smoke check and the CPU baseline of the benchmark
+ * use this code; the renderer library never links it. */
+#ifndef R3D_ORACLE_H
+#define R3D_ORACLE_H
+
+#include <stdint.h>
+
+#include "r3d_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ORC_MAX_LEVELS 16
+
+/* Cube volume with its mip chain (level 0 = the volume, x fastest). */
+typedef struct orc_cube {
+  uint32_t nlevels;
+  uint32_t dim[ORC_MAX_LEVELS][3];
+  const uint8_t *level[ORC_MAX_LEVELS];
+  const uint8_t *occ; /* dilated 8^3 block maxima, x fastest */
+  uint32_t odim[3];
+} orc_cube;
+
+/* Brick cache: the page table in render3d's word format and a pool of
+ * 128^3 slots (slot s at pool + s * 128^3, x fastest). */
+typedef struct orc_bricks {
+  const uint32_t *page;
+  uint32_t page_words;
+  const uint8_t *pool;
+  uint32_t nslots;
+} orc_bricks;
+
+typedef struct orc_opts {
+  float alpha_cutoff; /* front-to-back termination opacity; reference 0.98 */
+  uint32_t quality;   /* R3D_QUALITY_FULL / R3D_QUALITY_FAST */
+  int threads;        /* OpenMP threads over rows; <= 0: all */
+} orc_opts;
+
+/* Per-pixel auxiliary outputs (all nullable, img_w * img_h each). */
+typedef struct orc_aux {
+  uint32_t *steps;     /* loop iterations of the ray (heatmap counter) */
+  uint32_t *mip_index; /* step index at which the MIP maximum was last raised */
+  uint64_t total_steps; /* sum over rays (out) */
+  uint32_t status;      /* bit 0: a page entry or slot was out of range */
+} orc_aux;
+
+/* Renders one view into the RGBA8 image (img_w x img_h, the view's rect at
+ * view_org, already sanitized to lie inside the image).  The scene pointer
+ * matching p->brick_mode must be non-NULL.  Returns 0 or -1 on bad input. */
+int orc_render_view(const r3d_frame_params *p, const orc_cube *cube, const orc_bricks *bricks,
+                    const uint8_t lut[256][4], const orc_opts *o, uint8_t *img, uint32_t img_w,
+                    uint32_t img_h, orc_aux *aux);
+
+/* Renders only the rays of the listed pixels (view-local thread coordinates,
+ * 2 * n entries); colours go to out_rgba (4 * n), steps / mip_index to the
+ * nullable arrays (n).  Used for sampled parity checks at full resolution. */
+int orc_render_pixels(const r3d_frame_params *p, const orc_cube *cube, const orc_bricks *bricks,
+                      const uint8_t lut[256][4], const orc_opts *o, const uint32_t *xy,
+                      uint32_t n, uint8_t *out_rgba, uint32_t *steps, uint32_t *mip_index);
+
+/* CPU build of the shared log2 / exp2 / pow / x^24 (4 outputs per input). */
+void orc_fmath_eval(const float *x, const float *y, float *out, uint32_t n);
+
+/* Mip level sizes for a cube: level m is max(1, dim >> m); returns the level
+ * count floor(log2(maxdim)) + 1 (src/vk/vkbackend.c:1517-1518). */
+uint32_t orc_mip_levels(uint32_t nx, uint32_t ny, uint32_t nz, uint32_t dims[][3]);
+
+/* One 2x box reduction: dst = (sum of the 8 children + 4) / 8 with source
+ * coordinates clamped to the source extent. */
+void orc_downsample(const uint8_t *src, uint32_t sx, uint32_t sy, uint32_t sz, uint8_t *dst,
+                    uint32_t dx, uint32_t dy, uint32_t dz);
+
+/* 8^3 block maxima followed by 26-neighbour max dilation
+ * (src/vk/vkbackend.c:794-870).  out holds ceil(n/8) per axis. */
+void orc_occupancy(const uint8_t *vox, uint32_t nx, uint32_t ny, uint32_t nz, uint8_t *out);
+
+/* LOD brick cache from a raw volume: level l is the (sum+4)/8 box pyramid
+ * over the zero-padded brick grid, levels [0, nlev); a brick is resident when
+ * its maximum is >= min_max.  Slots are assigned in (level, z, y, x) order.
+ * Writes the page table (page_words = 64 + total bricks) and, if pool is not
+ * NULL, the slot contents.  Returns the number of resident bricks, or -1. */
+int64_t orc_build_lod_bricks(const uint8_t *vox, uint32_t nx, uint32_t ny, uint32_t nz,
+                             uint32_t nlev, uint32_t min_max, uint32_t *page,
+                             uint32_t page_words, uint8_t *pool, uint64_t pool_slots);
+uint32_t orc_lod_page_words(uint32_t nx, uint32_t ny, uint32_t nz, uint32_t nlev);
+
+/* Host-side camera / TF helpers restated from src/core/camera.c:5-75,
+ * src/core/transfer.c:5-50, src/core/lod.h:8-26 and src/core/mathx.h:34-43,
+ * for checking the library's own versions against the reference. */
+void orc_camera_basis(float yaw, float pitch, float fov_y, float aspect, float right[3],
+                      float up[3], float fwd[3]);
+void orc_orbit_pos(float yaw, float pitch, const float target[3], float dist, float pos[3]);
+void orc_tf_build(const uint8_t *values, const uint8_t (*rgba)[4], uint32_t npts,
+                  uint8_t lut[256][4]);
+uint32_t orc_lod_pick(float distance, float pixel_cone, float base_voxels, uint32_t nlevels);
+uint32_t orc_lod_fallback(uint32_t desired, uint32_t ordinal, uint32_t nlevels);
+void orc_m3_ypr(float yaw, float pitch, float roll, float rows[3][3]);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* R3D_ORACLE_H */

@@ -1,0 +1,470 @@
+"""Python bindings (ctypes) for libr3d_b200.so, the sm_100a volume raycaster.
+
+The library is C: CUDA kernels behind the C-ABI in include/r3d_cuda.h, the
+headless render3d interface in include/r3d_render.h and host helpers in
+include/r3d_host.h.  This module mirrors those calls for tests, benchmarks
+and Python callers.  It never falls back to another implementation: if the
+shared library is missing or fails to load, importing it raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libr3d_b200.so")
+ROOT = os.path.dirname(HERE)
+
+R3D_OK = 0
+ERRORS = {-1: "R3D_E_INVALID", -2: "R3D_E_CUDA", -3: "R3D_E_NOMEM", -4: "R3D_E_UNSUPPORTED",
+          -5: "R3D_E_STATE", -6: "R3D_E_DEVICE", -7: "R3D_E_TIMEOUT"}
+
+MODE_FULL, MODE_MIP, MODE_DEPTH, MODE_HEATMAP, MODE_RAYDIR, MODE_FLAT = range(6)
+QUALITY_FULL, QUALITY_FAST = 0, 1
+VIEW_ORTHO, VIEW_SURF, VIEW_OBLIQUE, VIEW_STRETCH, VIEW_CROP, VIEW_HALF = 1, 2, 4, 8, 16, 32
+BRICK_LOD_FLAG = 0x20000
+
+
+def VIEW_AXIS(a: int) -> int:
+    """Bricks slab axis bits of view_flags: 0 = z, 1 = x, 2 = y."""
+    return (a & 3) << 8
+
+
+class FrameParams(C.Structure):
+    """r3d_frame_params: 248 bytes, the reference's layout
+    (src/render/render_types.h:47-94)."""
+    _fields_ = [
+        ("cam_origin", C.c_float * 3), ("step_voxels", C.c_float),
+        ("cam_right", C.c_float * 3), ("density", C.c_float),
+        ("cam_up", C.c_float * 3), ("lod_bias", C.c_float),
+        ("cam_forward", C.c_float * 3), ("max_mip", C.c_float),
+        ("viewport", C.c_uint32 * 2), ("mode", C.c_uint32), ("frame_index", C.c_uint32),
+        ("threshold", C.c_float), ("slab_grid", C.c_uint32), ("slab_wz", C.c_uint32),
+        ("slab_z0", C.c_float), ("slab_nx", C.c_float), ("slab_ny", C.c_float),
+        ("slab_px", C.c_float), ("slab_py", C.c_float), ("slab_depth", C.c_uint32),
+        ("clip_valid", C.c_uint32), ("clip_orig", (C.c_float * 2) * 6),
+        ("vol_r0", C.c_float * 3), ("vol_tx", C.c_float),
+        ("vol_r1", C.c_float * 3), ("vol_ty", C.c_float),
+        ("vol_r2", C.c_float * 3), ("vol_tz", C.c_float),
+        ("brick_mode", C.c_uint32), ("skip_gate", C.c_float),
+        ("slab_x0", C.c_float), ("slab_y0", C.c_float),
+        ("view_org", C.c_uint32), ("view_flags", C.c_uint32),
+        ("overlay_gain", C.c_float), ("overlay_flags", C.c_uint32),
+    ]
+
+    def copy(self) -> "FrameParams":
+        p = FrameParams()
+        C.memmove(C.byref(p), C.byref(self), C.sizeof(FrameParams))
+        return p
+
+
+assert C.sizeof(FrameParams) == 248
+
+
+class VolumeDesc(C.Structure):
+    _fields_ = [("nx", C.c_uint32), ("ny", C.c_uint32), ("nz", C.c_uint32),
+                ("brick_dim", C.c_uint32), ("voxel_um", C.c_float)]
+
+
+class CudaAux(C.Structure):
+    _fields_ = [("steps", C.c_void_p), ("mip_index", C.c_void_p),
+                ("total_steps", C.c_void_p), ("counters", C.c_void_p)]
+
+
+class PhantomDesc(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("pitch", C.c_float), ("radius", C.c_float),
+                ("r0", C.c_float), ("sheet_half", C.c_float), ("in_mean", C.c_float),
+                ("in_sd", C.c_float), ("air_mean", C.c_float), ("air_sd", C.c_float),
+                ("noise_sd", C.c_float)]
+
+
+class HostCamera(C.Structure):
+    _fields_ = [("pos", C.c_float * 3), ("yaw", C.c_float), ("pitch", C.c_float),
+                ("fov_y", C.c_float), ("target", C.c_float * 3), ("dist", C.c_float)]
+
+
+class RenderConfig(C.Structure):
+    _fields_ = [("validate", C.c_bool), ("vsync", C.c_bool), ("spv_dir", C.c_char_p),
+                ("gpu_budget_bytes", C.c_uint64), ("headless", C.c_bool),
+                ("headless_w", C.c_uint32), ("headless_h", C.c_uint32)]
+
+
+class FrameStats(C.Structure):
+    _fields_ = [("gpu_ns", C.c_uint64), ("gpu_raycast_ns", C.c_uint64),
+                ("gpu_blit_ns", C.c_uint64), ("gpu_gui_ns", C.c_uint64),
+                ("panes_drawn", C.c_uint32), ("cpu_wait_ns", C.c_uint64),
+                ("cpu_acquire_ns", C.c_uint64), ("cpu_record_ns", C.c_uint64),
+                ("cpu_submit_ns", C.c_uint64)]
+
+
+def _load() -> C.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is not built; run python render3d_b200/build.py")
+    lib = C.CDLL(LIB_PATH)
+    P, U32, F, I = C.c_void_p, C.c_uint32, C.c_float, C.c_int
+    sig = {
+        "r3d_cuda_create": (I, [I, C.POINTER(P)]),
+        "r3d_cuda_destroy": (None, [P]),
+        "r3d_cuda_last_error": (C.c_char_p, [P]),
+        "r3d_cuda_stream": (P, [P]),
+        "r3d_cuda_status": (I, [P, C.POINTER(U32), I]),
+        "r3d_cuda_upload_volume": (I, [P, C.POINTER(VolumeDesc), P]),
+        "r3d_cuda_set_transfer": (I, [P, P]),
+        "r3d_cuda_set_quality": (I, [P, U32]),
+        "r3d_cuda_set_alpha_cutoff": (I, [P, F]),
+        "r3d_cuda_bricks_build": (I, [P, C.POINTER(VolumeDesc), P, U32, U32]),
+        "r3d_cuda_bricks_load": (I, [P, P, U32, P, U32]),
+        "r3d_cuda_brick_mode": (U32, [P]),
+        "r3d_cuda_bricks_info": (I, [P, C.POINTER(U32), C.POINTER(U32), P, C.POINTER(U32)]),
+        "r3d_cuda_bricks_read": (I, [P, P, P]),
+        "r3d_cuda_cube_read": (I, [P, I, P, P]),
+        "r3d_cuda_raycast_fwd": (I, [P, P, U32, P, U32, U32, C.POINTER(CudaAux), P]),
+        "r3d_cuda_last_kernel_ns": (I, [P, C.POINTER(C.c_uint64)]),
+        "r3d_cuda_fmath_eval": (I, [P, P, P, P, U32]),
+        "r3d_create": (I, [P, C.POINTER(RenderConfig), C.POINTER(P)]),
+        "r3d_destroy": (None, [P]),
+        "r3d_upload_volume": (I, [P, C.POINTER(VolumeDesc), P]),
+        "r3d_set_transfer": (I, [P, P]),
+        "r3d_set_quality": (None, [P, U32]),
+        "r3d_set_alpha_cutoff": (I, [P, F]),
+        "r3d_renderer_cuda": (P, [P]),
+        "r3d_bricks_begin_volume": (I, [P, C.POINTER(VolumeDesc), P, U32, U32]),
+        "r3d_bricks_end": (I, [P]),
+        "r3d_bricks_params": (None, [P, C.POINTER(FrameParams)]),
+        "r3d_bricks_extent": (None, [P, P]),
+        "r3d_bricks_shape": (None, [P, P]),
+        "r3d_frame": (I, [P, C.POINTER(FrameParams), C.POINTER(FrameStats)]),
+        "r3d_frame_views": (I, [P, P, U32, C.POINTER(FrameStats)]),
+        "r3d_read_frame": (I, [P, P, C.POINTER(U32), C.POINTER(U32)]),
+        "r3d_host_camera_init": (None, [C.POINTER(HostCamera), P]),
+        "r3d_host_camera_look": (None, [C.POINTER(HostCamera), F, F]),
+        "r3d_host_camera_move": (None, [C.POINTER(HostCamera), P, F]),
+        "r3d_host_camera_orbit_set": (None, [C.POINTER(HostCamera), P, F]),
+        "r3d_host_camera_orbit_drag": (None, [C.POINTER(HostCamera), F, F]),
+        "r3d_host_camera_orbit_zoom": (None, [C.POINTER(HostCamera), F]),
+        "r3d_host_camera_basis": (None, [C.POINTER(HostCamera), F, P, P, P]),
+        "r3d_host_m3_ypr": (None, [F, F, F, P]),
+        "r3d_host_tf_build": (None, [P, P, U32, P]),
+        "r3d_host_tf_preset": (U32, [U32, P]),
+        "r3d_host_tf_min_visible": (F, [P]),
+        "r3d_host_skip_gate": (F, [F, P]),
+        "r3d_host_lod_pick": (U32, [F, F, F, U32]),
+        "r3d_host_lod_fallback": (U32, [U32, U32, U32]),
+        "r3d_host_orbit_view": (None, [C.POINTER(FrameParams), F, P, U32, U32, F, F, F, U32,
+                                       U32, F, P]),
+        "r3d_host_phantom_default": (None, [U32, C.c_uint64, C.POINTER(PhantomDesc)]),
+        "r3d_host_phantom": (I, [P, U32, U32, U32, C.POINTER(PhantomDesc), I]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+class R3DError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+def _ptr(a) -> int:
+    """Address of a numpy array or a torch tensor (host or device)."""
+    if a is None:
+        return 0
+    if isinstance(a, np.ndarray):
+        assert a.flags["C_CONTIGUOUS"]
+        return a.ctypes.data
+    return int(a.data_ptr())
+
+
+# ------------------------------------------------------------------ host
+
+def tf_preset(idx: int) -> np.ndarray:
+    lut = np.zeros((256, 4), np.uint8)
+    if lib.r3d_host_tf_preset(idx, _ptr(lut)) != idx:
+        raise ValueError(f"no TF preset {idx}")
+    return lut
+
+
+def tf_build(points: list[tuple[int, tuple[int, int, int, int]]]) -> np.ndarray:
+    vals = np.array([p[0] for p in points], np.uint8)
+    cols = np.array([p[1] for p in points], np.uint8).reshape(-1, 4)
+    lut = np.zeros((256, 4), np.uint8)
+    lib.r3d_host_tf_build(_ptr(vals), _ptr(cols), len(points), _ptr(lut))
+    return lut
+
+
+def grey_ramp() -> np.ndarray:
+    return np.repeat(np.arange(256, dtype=np.uint8)[:, None], 4, axis=1).copy()
+
+
+def scroll_ramp_tf() -> np.ndarray:
+    """The benchmark TF: alpha 0 below 40, rising to 0.9 (230) at 200 and
+    flat to 255, grey RGB ramp."""
+    return tf_build([(0, (0, 0, 0, 0)), (40, (40, 40, 40, 0)), (200, (200, 200, 200, 230)),
+                     (255, (255, 255, 255, 230))])
+
+
+def skip_gate(low_cut: float, lut: np.ndarray) -> float:
+    return float(lib.r3d_host_skip_gate(low_cut, _ptr(np.ascontiguousarray(lut))))
+
+
+def phantom(n: int | tuple[int, int, int], seed: int = 1234, threads: int = 0,
+            desc: PhantomDesc | None = None) -> np.ndarray:
+    """Seeded scroll phantom as a (nz, ny, nx) u8 array."""
+    nx, ny, nz = (n, n, n) if isinstance(n, int) else n
+    if desc is None:
+        desc = PhantomDesc()
+        lib.r3d_host_phantom_default(max(nx, ny, nz), seed, C.byref(desc))
+    vol = np.empty((nz, ny, nx), np.uint8)
+    if threads <= 0:
+        threads = os.cpu_count() or 8
+    if lib.r3d_host_phantom(_ptr(vol), nx, ny, nz, C.byref(desc), threads) != 0:
+        raise ValueError("phantom: bad parameters")
+    return vol
+
+
+def orbit_view(ph: float, w: int, h: int, lut: np.ndarray, target=(0.5, 0.5, 0.5),
+               step_voxels: float = 1.0, density: float = 1.0, lod_bias: float = 0.0,
+               mode: int = MODE_FULL, frame_index: int = 0, low_cut: float = 0.0
+               ) -> FrameParams:
+    """View of the scripted orbit benchmark at phase ph (src/main.c:3932-3946)."""
+    p = FrameParams()
+    t = (C.c_float * 3)(*target)
+    lib.r3d_host_orbit_view(C.byref(p), ph, t, w, h, step_voxels, density, lod_bias, mode,
+                            frame_index, low_cut, _ptr(np.ascontiguousarray(lut)))
+    return p
+
+
+def camera_view(yaw: float, pitch: float, dist: float, w: int, h: int, lut: np.ndarray,
+                target=(0.5, 0.5, 0.5), step_voxels: float = 1.0, density: float = 1.0,
+                lod_bias: float = 0.0, mode: int = MODE_FULL, frame_index: int = 0,
+                low_cut: float = 0.0, max_mip: float = 10.0) -> FrameParams:
+    """Turntable orbit view at (yaw, pitch) radians; pitch < 0 looks down."""
+    cam = HostCamera()
+    lib.r3d_host_camera_init(C.byref(cam), (C.c_float * 3)(0.5, 0.5, -1.5))
+    cam.yaw, cam.pitch = yaw, pitch
+    lib.r3d_host_camera_orbit_set(C.byref(cam), (C.c_float * 3)(*target), dist)
+    p = FrameParams()
+    p.cam_origin[:] = cam.pos[:]
+    lib.r3d_host_camera_basis(C.byref(cam), C.c_float(w / h), p.cam_right, p.cam_up,
+                              p.cam_forward)
+    p.step_voxels, p.density, p.lod_bias, p.max_mip = step_voxels, density, lod_bias, max_mip
+    p.viewport[0], p.viewport[1] = w, h
+    p.mode, p.frame_index = mode, frame_index
+    p.threshold = low_cut / 255.0
+    p.skip_gate = skip_gate(low_cut, lut)
+    p.vol_r0[:] = (1.0, 0.0, 0.0)
+    p.vol_r1[:] = (0.0, 1.0, 0.0)
+    p.vol_r2[:] = (0.0, 0.0, 1.0)
+    return p
+
+
+def set_rotation(p: FrameParams, yaw: float, pitch: float, roll: float,
+                 t=(0.0, 0.0, 0.0)) -> None:
+    m = (C.c_float * 9)()
+    lib.r3d_host_m3_ypr(yaw, pitch, roll, m)
+    p.vol_r0[:] = m[0:3]
+    p.vol_r1[:] = m[3:6]
+    p.vol_r2[:] = m[6:9]
+    p.vol_tx, p.vol_ty, p.vol_tz = t
+
+
+# ---------------------------------------------------------------- device
+
+class Context:
+    """An r3d_cuda_ctx: scene state on one GPU plus the forward raycast."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        rc = lib.r3d_cuda_create(device, C.byref(h))
+        if rc != R3D_OK:
+            raise R3DError(rc, "r3d_cuda_create failed (no CUDA device?)")
+        self.h = h
+
+    def close(self) -> None:
+        if self.h:
+            lib.r3d_cuda_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int) -> None:
+        if rc != R3D_OK:
+            raise R3DError(rc, lib.r3d_cuda_last_error(self.h).decode())
+
+    @property
+    def stream(self) -> int:
+        return lib.r3d_cuda_stream(self.h) or 0
+
+    def upload_volume(self, vol) -> None:
+        nz, ny, nx = vol.shape
+        d = VolumeDesc(nx, ny, nz, 128, 1.0)
+        self._check(lib.r3d_cuda_upload_volume(self.h, C.byref(d), _ptr(vol)))
+
+    def set_transfer(self, lut: np.ndarray) -> None:
+        lut = np.ascontiguousarray(lut, dtype=np.uint8)
+        assert lut.shape == (256, 4)
+        self._check(lib.r3d_cuda_set_transfer(self.h, _ptr(lut)))
+
+    def set_quality(self, q: int) -> None:
+        self._check(lib.r3d_cuda_set_quality(self.h, q))
+
+    def set_alpha_cutoff(self, c: float) -> None:
+        self._check(lib.r3d_cuda_set_alpha_cutoff(self.h, c))
+
+    def bricks_build(self, vol, nlev: int, min_max: int = 0) -> None:
+        nz, ny, nx = vol.shape
+        d = VolumeDesc(nx, ny, nz, 128, 1.0)
+        self._check(lib.r3d_cuda_bricks_build(self.h, C.byref(d), _ptr(vol), nlev, min_max))
+
+    def bricks_load(self, page: np.ndarray, slots: np.ndarray) -> None:
+        page = np.ascontiguousarray(page, np.uint32)
+        slots = np.ascontiguousarray(slots, np.uint8)
+        nslots = slots.size // (128 ** 3)
+        self._check(lib.r3d_cuda_bricks_load(self.h, _ptr(page), page.size, _ptr(slots), nslots))
+
+    @property
+    def brick_mode(self) -> int:
+        return int(lib.r3d_cuda_brick_mode(self.h))
+
+    def bricks_info(self) -> dict:
+        w, n, nl = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        shape = (C.c_uint32 * 3)()
+        self._check(lib.r3d_cuda_bricks_info(self.h, C.byref(w), C.byref(n), shape,
+                                             C.byref(nl)))
+        return {"page_words": w.value, "nslots": n.value, "shape": tuple(shape),
+                "nlev": nl.value}
+
+    def bricks_read(self, slots: bool = True) -> tuple[np.ndarray, np.ndarray | None]:
+        info = self.bricks_info()
+        page = np.empty(info["page_words"], np.uint32)
+        pool = np.empty(info["nslots"] * 128 ** 3, np.uint8) if slots else None
+        self._check(lib.r3d_cuda_bricks_read(self.h, _ptr(page), _ptr(pool)))
+        return page, pool
+
+    def cube_read(self, level: int) -> np.ndarray:
+        dims = (C.c_uint32 * 3)()
+        self._check(lib.r3d_cuda_cube_read(self.h, level, None, dims))
+        out = np.empty((dims[2], dims[1], dims[0]), np.uint8)
+        self._check(lib.r3d_cuda_cube_read(self.h, level, _ptr(out), dims))
+        return out
+
+    def status(self, clear: bool = True) -> int:
+        b = C.c_uint32()
+        self._check(lib.r3d_cuda_status(self.h, C.byref(b), int(clear)))
+        return b.value
+
+    def raycast(self, views, out_w: int, out_h: int, out=None, steps=None, mip_index=None,
+                total=None, counters=None, stream: int = 0):
+        """Raycasts views into out (host numpy (h, w, 4) u8 or a device tensor);
+        returns out.  steps / mip_index: same kind, (h, w) u32; total: one
+        u64 counter, counters: four u64 counters (samples, TF lookups,
+        shaded samples, page walks), both accumulated."""
+        if isinstance(views, FrameParams):
+            views = [views]
+        arr = (FrameParams * len(views))(*views)
+        if out is None:
+            out = np.zeros((out_h, out_w, 4), np.uint8)
+        aux = None
+        if any(a is not None for a in (steps, mip_index, total, counters)):
+            aux = CudaAux(_ptr(steps) or None, _ptr(mip_index) or None, _ptr(total) or None,
+                          _ptr(counters) or None)
+        self._check(lib.r3d_cuda_raycast_fwd(self.h, arr, len(views), _ptr(out), out_w, out_h,
+                                             C.byref(aux) if aux else None, stream or None))
+        return out
+
+    def fmath_eval(self, x: np.ndarray, y: np.ndarray) -> np.ndarray:
+        """Device log2, exp2, pow and x^24 of the inputs, (n, 4) float32."""
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        out = np.empty((x.size, 4), np.float32)
+        self._check(lib.r3d_cuda_fmath_eval(self.h, _ptr(x), _ptr(y), _ptr(out), x.size))
+        return out
+
+    def last_kernel_ns(self) -> int:
+        ns = C.c_uint64()
+        self._check(lib.r3d_cuda_last_kernel_ns(self.h, C.byref(ns)))
+        return ns.value
+
+
+class Renderer:
+    """The headless render3d interface (r3d_render.h)."""
+
+    def __init__(self, w: int, h: int):
+        cfg = RenderConfig(False, False, None, 0, True, w, h)
+        r = C.c_void_p()
+        if lib.r3d_create(None, C.byref(cfg), C.byref(r)) != 0:
+            raise RuntimeError("r3d_create failed")
+        self.r = r
+        self.w, self.h = w, h
+
+    def close(self) -> None:
+        if self.r:
+            lib.r3d_destroy(self.r)
+            self.r = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ok(self, rc: int, what: str) -> None:
+        if rc != 0:
+            raise RuntimeError(f"{what} failed ({rc})")
+
+    def upload_volume(self, vol) -> None:
+        nz, ny, nx = vol.shape
+        self._ok(lib.r3d_upload_volume(self.r, C.byref(VolumeDesc(nx, ny, nz, 128, 1.0)),
+                                       _ptr(vol)), "r3d_upload_volume")
+
+    def bricks_begin_volume(self, vol, nlev: int, min_max: int = 0) -> None:
+        nz, ny, nx = vol.shape
+        self._ok(lib.r3d_bricks_begin_volume(self.r, C.byref(VolumeDesc(nx, ny, nz, 128, 1.0)),
+                                             _ptr(vol), nlev, min_max), "r3d_bricks_begin")
+
+    def bricks_params(self, p: FrameParams) -> None:
+        lib.r3d_bricks_params(self.r, C.byref(p))
+
+    def set_transfer(self, lut: np.ndarray) -> None:
+        self._ok(lib.r3d_set_transfer(self.r, _ptr(np.ascontiguousarray(lut, np.uint8))),
+                 "r3d_set_transfer")
+
+    def set_quality(self, q: int) -> None:
+        lib.r3d_set_quality(self.r, q)
+
+    def set_alpha_cutoff(self, c: float) -> None:
+        self._ok(lib.r3d_set_alpha_cutoff(self.r, c), "r3d_set_alpha_cutoff")
+
+    def frame(self, p: FrameParams, stats: FrameStats | None = None) -> None:
+        self._ok(lib.r3d_frame(self.r, C.byref(p), C.byref(stats) if stats else None),
+                 "r3d_frame")
+
+    def frame_views(self, views, stats: FrameStats | None = None) -> None:
+        arr = (FrameParams * len(views))(*views)
+        self._ok(lib.r3d_frame_views(self.r, arr, len(views),
+                                     C.byref(stats) if stats else None), "r3d_frame_views")
+
+    def read_frame(self, out=None):
+        w, h = C.c_uint32(), C.c_uint32()
+        lib.r3d_read_frame(self.r, None, C.byref(w), C.byref(h))
+        if out is None:
+            out = np.empty((h.value, w.value, 4), np.uint8)
+        self._ok(lib.r3d_read_frame(self.r, _ptr(out), C.byref(w), C.byref(h)),
+                 "r3d_read_frame")
+        return out
+
+    @property
+    def cuda(self) -> int:
+        return lib.r3d_renderer_cuda(self.r)

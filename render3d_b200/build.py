@@ -1,0 +1,110 @@
+"""Builds libr3d_b200.so (sm_100a CUDA kernels + C-ABI + C23 host code) and
+the r3d_headless command-line tool in place, next to this file.
+
+    python render3d_b200/build.py [--force] [--verbose]
+
+(run as a script: importing the package loads the library it builds)
+
+Kernels are compiled with -fmad=false and IEEE division / square root: the
+raycast's arithmetic is written out operation by operation (explicit fmaf)
+and must not be contracted or approximated, so that the CPU oracle used by
+the tests reproduces it bit for bit.  ptxas register / spill reports go to
+_build/ptxas.log.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+INC = os.path.join(ROOT, "include")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libr3d_b200.so")
+CLI = os.path.join(HERE, "r3d_headless")
+
+CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
+GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = GENCODE + [
+    "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+    "-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false",
+    "-Xptxas", "-v", "-I" + INC, "-I" + CSRC,
+]
+# the image's CC points at a gcc build without libgomp; the system gcc is used
+CC = shutil.which("gcc", path="/usr/bin:/bin") or "gcc"
+C_FLAGS = ["-O2", "-std=c2x", "-D_GNU_SOURCE", "-fPIC", "-ffp-contract=off", "-Wall",
+           "-Wextra", "-I" + INC, "-I" + os.path.join(CUDA_HOME, "include")]
+
+CU_SOURCES = ["r3d_ctx.cu", "r3d_fwd.cu", "r3d_diag.cu"]
+C_SOURCES = ["r3d_render.c", "r3d_host.c"]
+CLI_SOURCES = ["r3d_headless.c"]
+
+
+def _newer(target: str, deps: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def _headers() -> list[str]:
+    hs = []
+    for d in (CSRC, INC):
+        hs += [os.path.join(d, f) for f in os.listdir(d) if f.endswith((".h", ".cuh"))]
+    return hs
+
+
+def _run(cmd: list[str], log=None, verbose=False) -> None:
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    if log is not None:
+        log.write(" ".join(cmd) + "\n" + r.stdout + "\n")
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout)
+        raise RuntimeError("build step failed: " + " ".join(cmd[:3]))
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    """Compiles whatever is out of date; returns the library path."""
+    os.makedirs(BUILD, exist_ok=True)
+    hdrs = _headers()
+    objs = []
+    with open(os.path.join(BUILD, "ptxas.log"), "a") as log:
+        for src in CU_SOURCES:
+            s = os.path.join(CSRC, src)
+            o = os.path.join(BUILD, src + ".o")
+            if force or _newer(o, [s] + hdrs):
+                _run([NVCC] + NVCC_FLAGS + ["-c", s, "-o", o], log, verbose)
+            objs.append(o)
+        for src in C_SOURCES:
+            s = os.path.join(CSRC, src)
+            o = os.path.join(BUILD, src + ".o")
+            if force or _newer(o, [s] + hdrs):
+                _run([CC] + C_FLAGS + ["-c", s, "-o", o], log, verbose)
+            objs.append(o)
+        if force or _newer(LIB, objs):
+            _run([NVCC] + GENCODE + ["-shared", "-o", LIB] + objs +
+                 ["-lcudart", "-lpthread", "-lm"], log, verbose)
+        cli_src = [os.path.join(CSRC, s) for s in CLI_SOURCES]
+        if force or _newer(CLI, cli_src + [LIB] + hdrs):
+            _run([CC] + C_FLAGS + ["-o", CLI] + cli_src +
+                 ["-L" + HERE, "-lr3d_b200", "-Wl,-rpath,$ORIGIN", "-lm"], log, verbose)
+    return LIB
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--verbose", action="store_true")
+    a = ap.parse_args()
+    print(build(a.force, a.verbose))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,774 @@
+// C-ABI entry points: context, scene uploads and device-side builders (mip
+// chain, occupancy grid, LOD brick pyramid and page table), forward raycast.
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <vector>
+
+#include "r3d_internal.h"
+
+namespace r3d {
+
+int fail(r3d_cuda_ctx *c, int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return code;
+}
+
+int cuda_fail(r3d_cuda_ctx *c, cudaError_t e, const char *what) {
+  return fail(c, e == cudaErrorMemoryAllocation ? R3D_E_NOMEM : R3D_E_CUDA, "%s: %s (%s)", what,
+              cudaGetErrorName(e), cudaGetErrorString(e));
+}
+
+bool is_device_ptr(const void *p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// ------------------------------------------------------------- builders
+
+// 2x box reduction with clamped source coordinates: (sum + 4) / 8
+__global__ void k_downsample_clamp(const uint8_t *__restrict__ src, uint32_t sx, uint32_t sy,
+                                   uint32_t sz, uint8_t *__restrict__ dst, uint32_t dx,
+                                   uint32_t dy, uint32_t dz) {
+  size_t n = (size_t)dx * dy * dz;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    uint32_t x = (uint32_t)(i % dx), y = (uint32_t)((i / dx) % dy), z = (uint32_t)(i / dx / dy);
+    uint32_t sum = 4u;
+#pragma unroll
+    for (uint32_t k = 0; k < 8u; k++) {
+      uint32_t xx = min(2u * x + (k & 1u), sx - 1u), yy = min(2u * y + ((k >> 1) & 1u), sy - 1u),
+               zz = min(2u * z + (k >> 2), sz - 1u);
+      sum += src[((size_t)zz * sy + yy) * sx + xx];
+    }
+    dst[i] = (uint8_t)(sum >> 3);
+  }
+}
+
+// 2x box reduction reading zeros outside the source extent (brick pyramid)
+__global__ void k_downsample_zero(const uint8_t *__restrict__ src, uint32_t sx, uint32_t sy,
+                                  uint32_t sz, uint8_t *__restrict__ dst, uint32_t dx,
+                                  uint32_t dy, uint32_t dz) {
+  size_t n = (size_t)dx * dy * dz;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    uint32_t x = (uint32_t)(i % dx), y = (uint32_t)((i / dx) % dy), z = (uint32_t)(i / dx / dy);
+    uint32_t sum = 4u;
+#pragma unroll
+    for (uint32_t k = 0; k < 8u; k++) {
+      uint32_t xx = 2u * x + (k & 1u), yy = 2u * y + ((k >> 1) & 1u), zz = 2u * z + (k >> 2);
+      if (xx < sx && yy < sy && zz < sz) sum += src[((size_t)zz * sy + yy) * sx + xx];
+    }
+    dst[i] = (uint8_t)(sum >> 3);
+  }
+}
+
+// 8^3 block maxima (src/vk/vkbackend.c:794-824)
+__global__ void k_occ_raw(const uint8_t *__restrict__ vox, uint32_t nx, uint32_t ny, uint32_t nz,
+                          uint8_t *__restrict__ raw, uint32_t ox, uint32_t oy, uint32_t oz) {
+  size_t n = (size_t)ox * oy * oz;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    uint32_t bx = (uint32_t)(i % ox), by = (uint32_t)((i / ox) % oy), bz = (uint32_t)(i / ox / oy);
+    uint32_t m = 0;
+    for (uint32_t z = bz * 8u; z < min(bz * 8u + 8u, nz); z++)
+      for (uint32_t y = by * 8u; y < min(by * 8u + 8u, ny); y++) {
+        const uint8_t *row = vox + ((size_t)z * ny + y) * nx;
+        for (uint32_t x = bx * 8u; x < min(bx * 8u + 8u, nx); x++) m = max(m, (uint32_t)row[x]);
+      }
+    raw[i] = (uint8_t)m;
+  }
+}
+
+// 26-neighbour max dilation (src/vk/vkbackend.c:845-860)
+__global__ void k_occ_dilate(const uint8_t *__restrict__ raw, uint8_t *__restrict__ dil,
+                             uint32_t ox, uint32_t oy, uint32_t oz) {
+  size_t n = (size_t)ox * oy * oz;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    int x = (int)(i % ox), y = (int)((i / ox) % oy), z = (int)(i / ox / oy);
+    uint32_t m = 0;
+    for (int dz = -1; dz <= 1; dz++)
+      for (int dy = -1; dy <= 1; dy++)
+        for (int dx = -1; dx <= 1; dx++) {
+          int zz = z + dz, yy = y + dy, xx = x + dx;
+          if (zz < 0 || yy < 0 || xx < 0 || zz >= (int)oz || yy >= (int)oy || xx >= (int)ox)
+            continue;
+          m = max(m, (uint32_t)raw[((size_t)zz * oy + yy) * ox + xx]);
+        }
+    dil[i] = (uint8_t)m;
+  }
+}
+
+// Maximum of each 128^3 brick of a level (zero outside the level's extent).
+// One block per brick.
+__global__ void k_brick_max(const uint8_t *__restrict__ lev, uint32_t ex, uint32_t ey,
+                            uint32_t ez, uint32_t bdx, uint32_t bdy, uint32_t *__restrict__ out) {
+  uint32_t bi = blockIdx.x;
+  uint32_t bx = bi % bdx, by = (bi / bdx) % bdy, bz = bi / bdx / bdy;
+  uint32_t m = 0;
+  for (uint32_t r = threadIdx.x; r < 128u * 128u; r += blockDim.x) {
+    uint32_t y = by * 128u + (r & 127u), z = bz * 128u + (r >> 7);
+    if (y >= ey || z >= ez) continue;
+    const uint8_t *row = lev + ((size_t)z * ey + y) * ex;
+    uint32_t x0 = bx * 128u, x1 = min(x0 + 128u, ex);
+    for (uint32_t x = x0; x < x1; x++) m = max(m, (uint32_t)row[x]);
+  }
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  __shared__ uint32_t wm[32];
+  if ((threadIdx.x & 31u) == 0) wm[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t r = 0;
+    for (uint32_t w = 0; w < blockDim.x / 32u; w++) r = max(r, wm[w]);
+    out[bi] = r;
+  }
+}
+
+// Copies bricks into their slots: job j copies brick src_brick[j] (linear
+// index in the level's brick grid) into slot dst_slot[j]; zero outside the
+// level's extent.  Grid: (128 z-slices, jobs).
+__global__ void k_brick_copy(const uint8_t *__restrict__ lev, uint32_t ex, uint32_t ey,
+                             uint32_t ez, uint32_t bdx, uint32_t bdy,
+                             const uint32_t *__restrict__ src_brick,
+                             const uint32_t *__restrict__ dst_slot, uint8_t *__restrict__ pool) {
+  uint32_t j = blockIdx.y, zl = blockIdx.x;
+  uint32_t bi = src_brick[j];
+  uint32_t bx = bi % bdx, by = (bi / bdx) % bdy, bz = bi / bdx / bdy;
+  uint8_t *dst = pool + (size_t)dst_slot[j] * (128u * 128u * 128u) + (size_t)zl * 16384u;
+  uint32_t z = bz * 128u + zl;
+  for (uint32_t r = threadIdx.x; r < 128u * 128u; r += blockDim.x) {
+    uint32_t yl = r >> 7, xl = r & 127u;
+    uint32_t y = by * 128u + yl, x = bx * 128u + xl;
+    uint8_t v = 0;
+    if (x < ex && y < ey && z < ez) v = lev[((size_t)z * ey + y) * ex + x];
+    dst[r] = v;
+  }
+}
+
+static unsigned grid_for(size_t n) {
+  size_t b = (n + 255) / 256;
+  return (unsigned)(b < 148u * 64u ? (b ? b : 1) : 148u * 64u);
+}
+
+}  // namespace r3d
+
+using namespace r3d;
+
+r3d::DevScene r3d_cuda_ctx::scene() const {
+  DevScene s;
+  memset(&s, 0, sizeof s);
+  s.cube = cube;
+  s.br = br;
+  s.status = status;
+  s.alpha_cutoff = alpha_cutoff;
+  s.tf_zero_t = tf_zero_t;
+  return s;
+}
+
+extern "C" {
+
+int r3d_cuda_create(int device, r3d_cuda_ctx **out) {
+  if (!out) return R3D_E_INVALID;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+    cudaGetLastError();
+    return R3D_E_CUDA;
+  }
+  r3d_cuda_ctx *c = new (std::nothrow) r3d_cuda_ctx();
+  if (!c) return R3D_E_NOMEM;
+  c->device = device;
+  if (cudaSetDevice(device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&c->status, sizeof(uint32_t)) != cudaSuccess ||
+      cudaMalloc(&c->lut, 256 * sizeof(uchar4)) != cudaSuccess ||
+      cudaMalloc(&c->total, (R3D_COUNTERS + 1) * sizeof(unsigned long long)) != cudaSuccess ||
+      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+    cudaGetLastError();
+    r3d_cuda_destroy(c);
+    return R3D_E_CUDA;
+  }
+  cudaMemset(c->status, 0, sizeof(uint32_t));
+  // default transfer function: grey ramp with alpha = value
+  // (src/vk/vkbackend.c:1100-1114)
+  uint8_t ramp[256][4];
+  for (int i = 0; i < 256; i++) ramp[i][0] = ramp[i][1] = ramp[i][2] = ramp[i][3] = (uint8_t)i;
+  if (r3d_cuda_set_transfer(c, ramp) != R3D_OK) {
+    r3d_cuda_destroy(c);
+    return R3D_E_CUDA;
+  }
+  *out = c;
+  return R3D_OK;
+}
+
+void r3d_cuda_destroy(r3d_cuda_ctx *c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  cudaFree(c->cube_buf);
+  cudaFree(c->page);
+  cudaFree(c->pool);
+  cudaFree(c->lut);
+  cudaFree(c->status);
+  cudaFree(c->img);
+  cudaFree(c->aux_buf);
+  cudaFree(c->total);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+const char *r3d_cuda_last_error(const r3d_cuda_ctx *c) { return c ? c->err.c_str() : "no ctx"; }
+
+void *r3d_cuda_stream(r3d_cuda_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+int r3d_cuda_status(r3d_cuda_ctx *c, uint32_t *bits, int clear) {
+  if (!c) return R3D_E_INVALID;
+  cudaSetDevice(c->device);
+  uint32_t v = 0;
+  R3D_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  R3D_CUDA_TRY(c, cudaMemcpy(&v, c->status, 4, cudaMemcpyDeviceToHost));
+  if (clear) R3D_CUDA_TRY(c, cudaMemset(c->status, 0, 4));
+  if (bits) *bits = v;
+  return R3D_OK;
+}
+
+int r3d_cuda_upload_volume(r3d_cuda_ctx *c, const r3d_volume_desc *d, const uint8_t *voxels) {
+  if (!c || !d || !voxels || !d->nx || !d->ny || !d->nz)
+    return fail(c, R3D_E_INVALID, "upload_volume: bad arguments");
+  cudaSetDevice(c->device);
+  uint32_t nx = d->nx, ny = d->ny, nz = d->nz;
+  uint32_t maxdim = max(nx, max(ny, nz));
+  if (maxdim > 65535u) return fail(c, R3D_E_INVALID, "upload_volume: dimension > 65535");
+  uint32_t mips = 1;
+  while ((maxdim >> mips) >= 1u && mips < 16u) mips++;
+  DevCube cube;
+  memset(&cube, 0, sizeof cube);
+  cube.nlevels = mips;
+  cube.maxdim = maxdim;
+  size_t off[17];
+  off[0] = 0;
+  for (uint32_t m = 0; m < mips; m++) {
+    cube.dim[m][0] = nx >> m ? nx >> m : 1u;
+    cube.dim[m][1] = ny >> m ? ny >> m : 1u;
+    cube.dim[m][2] = nz >> m ? nz >> m : 1u;
+    size_t b = (size_t)cube.dim[m][0] * cube.dim[m][1] * cube.dim[m][2];
+    off[m + 1] = off[m] + ((b + 255) & ~(size_t)255);
+  }
+  for (int a = 0; a < 3; a++) cube.odim[a] = ((a == 0 ? nx : a == 1 ? ny : nz) + 7u) / 8u;
+  size_t onb = (size_t)cube.odim[0] * cube.odim[1] * cube.odim[2];
+  size_t total = off[mips] + ((onb + 255) & ~(size_t)255);
+  uint8_t *buf = nullptr, *raw = nullptr;
+  R3D_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  cudaError_t e = cudaMalloc(&buf, total + onb);
+  if (e != cudaSuccess) return cuda_fail(c, e, "upload_volume: cudaMalloc");
+  raw = buf + total;
+  e = cudaMemcpyAsync(buf, voxels, (size_t)nx * ny * nz, cudaMemcpyDefault, c->stream);
+  for (uint32_t m = 1; m < mips && e == cudaSuccess; m++) {
+    size_t n = (size_t)cube.dim[m][0] * cube.dim[m][1] * cube.dim[m][2];
+    k_downsample_clamp<<<grid_for(n), 256, 0, c->stream>>>(
+        buf + off[m - 1], cube.dim[m - 1][0], cube.dim[m - 1][1], cube.dim[m - 1][2], buf + off[m],
+        cube.dim[m][0], cube.dim[m][1], cube.dim[m][2]);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) {
+    k_occ_raw<<<grid_for(onb), 256, 0, c->stream>>>(buf, nx, ny, nz, raw, cube.odim[0],
+                                                    cube.odim[1], cube.odim[2]);
+    k_occ_dilate<<<grid_for(onb), 256, 0, c->stream>>>(raw, buf + off[mips], cube.odim[0],
+                                                       cube.odim[1], cube.odim[2]);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) {
+    cudaFree(buf);
+    return cuda_fail(c, e, "upload_volume");
+  }
+  for (uint32_t m = 0; m < mips; m++) cube.lev[m] = buf + off[m];
+  cube.occ = buf + off[mips];
+  cudaFree(c->cube_buf);
+  c->cube_buf = buf;
+  c->cube_bytes = total;
+  c->have_cube = true;
+  c->cube = cube;
+  return R3D_OK;
+}
+
+int r3d_cuda_set_transfer(r3d_cuda_ctx *c, const uint8_t rgba[256][4]) {
+  if (!c || !rgba) return fail(c, R3D_E_INVALID, "set_transfer: bad arguments");
+  cudaSetDevice(c->device);
+  memcpy(c->lut_host, rgba, sizeof c->lut_host);
+  int imin = 256;
+  for (int i = 0; i < 256; i++)
+    if (rgba[i][3]) {
+      imin = i;
+      break;
+    }
+  // TF coordinate t < imin - 1 interpolates two zero-alpha texels
+  c->tf_zero_t = (float)(imin - 1);
+  R3D_CUDA_TRY(c, cudaMemcpyAsync(c->lut, c->lut_host, sizeof c->lut_host, cudaMemcpyHostToDevice,
+                                  c->stream));
+  R3D_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return R3D_OK;
+}
+
+int r3d_cuda_set_quality(r3d_cuda_ctx *c, uint32_t quality) {
+  if (!c || quality >= R3D_QUALITY_COUNT) return fail(c, R3D_E_INVALID, "set_quality: %u", quality);
+  c->quality = quality;
+  return R3D_OK;
+}
+
+int r3d_cuda_set_alpha_cutoff(r3d_cuda_ctx *c, float cutoff) {
+  if (!c || !(cutoff > 0.0f && cutoff <= 1.0f))
+    return fail(c, R3D_E_INVALID, "set_alpha_cutoff: %g not in (0, 1]", (double)cutoff);
+  c->alpha_cutoff = cutoff;
+  return R3D_OK;
+}
+
+}  // extern "C"
+
+// Validates a LOD page-table header and decodes it into the kernel's form.
+static int decode_header(r3d_cuda_ctx *c, const uint32_t *page, uint32_t words, uint32_t nslots,
+                         DevBricks &b) {
+  memset(&b, 0, sizeof b);
+  if (words < R3D_BRICK_PAGE_HEADER) return fail(c, R3D_E_INVALID, "page table < 64 words");
+  uint32_t nlev = page[0];
+  if (nlev < 1u || nlev > 15u) return fail(c, R3D_E_INVALID, "page header: %u levels", nlev);
+  if (!page[1] || !page[2] || !page[3] || page[1] > 65535u || page[2] > 65535u ||
+      page[3] > 65535u)
+    return fail(c, R3D_E_INVALID, "page header: bad base shape");
+  b.nlev = nlev;
+  for (int a = 0; a < 3; a++) b.bs[a] = (float)page[1 + a];
+  b.md = fmaxf(b.bs[0], fmaxf(b.bs[1], b.bs[2]));
+  for (uint32_t l = 0; l < nlev; l++) {
+    uint32_t off = page[4 + 4 * l], packed = page[5 + 4 * l], scale = page[6 + 4 * l];
+    uint32_t bd[3] = {packed & 1023u, (packed >> 10) & 1023u, packed >> 20};
+    if (!scale || (scale & (scale - 1u)) || scale > (1u << 20))
+      return fail(c, R3D_E_INVALID, "page header: level %u scale %u not a power of two", l, scale);
+    if (!bd[0] || !bd[1] || !bd[2] || bd[2] > 1023u)
+      return fail(c, R3D_E_INVALID, "page header: level %u empty brick grid", l);
+    uint64_t end = (uint64_t)off + (uint64_t)bd[0] * bd[1] * bd[2];
+    if (off < R3D_BRICK_PAGE_HEADER || end > words)
+      return fail(c, R3D_E_INVALID, "page header: level %u entries out of range", l);
+    b.off[l] = off;
+    b.scale[l] = scale;
+    b.inv_scale[l] = 1.0f / (float)scale;
+    for (int a = 0; a < 3; a++) b.bd[l][a] = bd[a];
+  }
+  b.page_words = words;
+  b.nslots = nslots;
+  return R3D_OK;
+}
+
+static uint32_t atlas_bpa(uint32_t nslots) {
+  uint32_t a = 1;
+  while ((uint64_t)a * a * a < nslots) a++;
+  return a;
+}
+
+extern "C" {
+
+int r3d_cuda_bricks_build(r3d_cuda_ctx *c, const r3d_volume_desc *d, const uint8_t *voxels,
+                          uint32_t nlev, uint32_t min_max) {
+  if (!c || !d || !voxels || !d->nx || !d->ny || !d->nz || nlev < 1u || nlev > 15u)
+    return fail(c, R3D_E_INVALID, "bricks_build: bad arguments");
+  uint32_t nx = d->nx, ny = d->ny, nz = d->nz;
+  if (max(nx, max(ny, nz)) > 65535u) return fail(c, R3D_E_INVALID, "bricks_build: too large");
+  cudaSetDevice(c->device);
+  cudaStream_t st = c->stream;
+  R3D_CUDA_TRY(c, cudaStreamSynchronize(st));
+  // level extents: level 0 is the volume itself, level l >= 1 the zero-
+  // padded brick grid 128 * ceil(ceil(n / 2^l) / 128)
+  uint32_t E[16][3], bd[16][3];
+  size_t lev_off[16] = {0}, lev_total = 0;
+  uint32_t nb_total = 0;
+  for (uint32_t l = 0; l < nlev; l++) {
+    uint32_t n3[3] = {nx, ny, nz};
+    for (int a = 0; a < 3; a++) {
+      uint32_t dl = (n3[a] + (1u << l) - 1u) >> l;
+      bd[l][a] = (dl + 127u) / 128u;
+      E[l][a] = l == 0 ? n3[a] : bd[l][a] * 128u;
+    }
+    if (bd[l][0] > 1023u || bd[l][1] > 1023u || bd[l][2] > 1023u)
+      return fail(c, R3D_E_INVALID, "bricks_build: brick grid too large");
+    lev_off[l] = lev_total;
+    lev_total += ((size_t)E[l][0] * E[l][1] * E[l][2] + 255) & ~(size_t)255;
+    nb_total += bd[l][0] * bd[l][1] * bd[l][2];
+  }
+  uint32_t words = R3D_BRICK_PAGE_HEADER + nb_total;
+  uint8_t *lev = nullptr;
+  uint32_t *dmax = nullptr, *jobs = nullptr;
+  uint8_t *pool = nullptr;
+  uint32_t *page = nullptr;
+  std::vector<uint32_t> hmax(nb_total), hpage(words, R3D_BRICK_ABSENT);
+  std::vector<uint32_t> src_brick, dst_slot;
+  int rc = R3D_OK;
+  cudaError_t e = cudaMalloc(&lev, lev_total);
+  if (e == cudaSuccess) e = cudaMalloc(&dmax, (size_t)nb_total * 4);
+  if (e != cudaSuccess) {
+    rc = cuda_fail(c, e, "bricks_build: cudaMalloc levels");
+    goto out;
+  }
+  e = cudaMemcpyAsync(lev, voxels, (size_t)nx * ny * nz, cudaMemcpyDefault, st);
+  for (uint32_t l = 1; l < nlev && e == cudaSuccess; l++) {
+    size_t n = (size_t)E[l][0] * E[l][1] * E[l][2];
+    k_downsample_zero<<<grid_for(n), 256, 0, st>>>(lev + lev_off[l - 1], E[l - 1][0], E[l - 1][1],
+                                                   E[l - 1][2], lev + lev_off[l], E[l][0], E[l][1],
+                                                   E[l][2]);
+    e = cudaGetLastError();
+  }
+  {
+    uint32_t moff = 0;
+    for (uint32_t l = 0; l < nlev && e == cudaSuccess; l++) {
+      uint32_t nb = bd[l][0] * bd[l][1] * bd[l][2];
+      k_brick_max<<<nb, 256, 0, st>>>(lev + lev_off[l], E[l][0], E[l][1], E[l][2], bd[l][0],
+                                      bd[l][1], dmax + moff);
+      e = cudaGetLastError();
+      moff += nb;
+    }
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(hmax.data(), dmax, (size_t)nb_total * 4, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    rc = cuda_fail(c, e, "bricks_build: pyramid");
+    goto out;
+  }
+  {
+    // page table in render3d's format (src/vk/vkbackend.c:4184-4206)
+    memset(hpage.data(), 0, R3D_BRICK_PAGE_HEADER * 4);
+    hpage[0] = nlev;
+    hpage[1] = nx;
+    hpage[2] = ny;
+    hpage[3] = nz;
+    uint32_t off = 0, slot = 0;
+    for (uint32_t l = 0; l < nlev; l++) {
+      uint32_t nb = bd[l][0] * bd[l][1] * bd[l][2];
+      hpage[4 + 4 * l] = R3D_BRICK_PAGE_HEADER + off;
+      hpage[5 + 4 * l] = bd[l][0] | (bd[l][1] << 10) | (bd[l][2] << 20);
+      hpage[6 + 4 * l] = 1u << l;
+      for (uint32_t bi = 0; bi < nb; bi++) {
+        uint32_t m = hmax[off + bi];
+        if (m >= min_max) {
+          hpage[R3D_BRICK_PAGE_HEADER + off + bi] = slot | (m << 24);
+          slot++;
+        }
+      }
+      off += nb;
+    }
+    if (slot >= (1u << 24)) {
+      rc = fail(c, R3D_E_INVALID, "bricks_build: %u slots exceed the 24-bit slot field", slot);
+      goto out;
+    }
+    uint32_t nslots = slot;
+    size_t pool_bytes = (size_t)(nslots ? nslots : 1u) * (128u * 128u * 128u);
+    e = cudaMalloc(&pool, pool_bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&page, (size_t)words * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&jobs, (size_t)(nslots ? nslots : 1u) * 8);
+    if (e != cudaSuccess) {
+      rc = cuda_fail(c, e, "bricks_build: cudaMalloc pool");
+      goto out;
+    }
+    off = 0;
+    uint32_t joff = 0;
+    std::vector<uint32_t> hj;
+    hj.reserve((size_t)nslots * 2);
+    std::vector<uint32_t> lvl_count(nlev, 0);
+    for (uint32_t l = 0; l < nlev; l++) {
+      uint32_t nb = bd[l][0] * bd[l][1] * bd[l][2];
+      for (uint32_t bi = 0; bi < nb; bi++) {
+        uint32_t en = hpage[R3D_BRICK_PAGE_HEADER + off + bi];
+        if (en != R3D_BRICK_ABSENT) {
+          src_brick.push_back(bi);
+          dst_slot.push_back(en & 0xFFFFFFu);
+          lvl_count[l]++;
+        }
+      }
+      off += nb;
+    }
+    if (nslots) {
+      e = cudaMemcpyAsync(jobs, src_brick.data(), (size_t)nslots * 4, cudaMemcpyHostToDevice, st);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(jobs + nslots, dst_slot.data(), (size_t)nslots * 4,
+                            cudaMemcpyHostToDevice, st);
+    }
+    for (uint32_t l = 0; l < nlev && e == cudaSuccess; l++) {
+      uint32_t n = lvl_count[l];
+      if (!n) continue;
+      for (uint32_t j0 = 0; j0 < n && e == cudaSuccess; j0 += 65535u) {
+        uint32_t nj = min(n - j0, 65535u);
+        k_brick_copy<<<dim3(128, nj), 256, 0, st>>>(lev + lev_off[l], E[l][0], E[l][1], E[l][2],
+                                                    bd[l][0], bd[l][1], jobs + joff + j0,
+                                                    jobs + nslots + joff + j0, pool);
+        e = cudaGetLastError();
+      }
+      joff += n;
+    }
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(page, hpage.data(), (size_t)words * 4, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+      rc = cuda_fail(c, e, "bricks_build: slot copy");
+      goto out;
+    }
+    DevBricks b;
+    rc = decode_header(c, hpage.data(), words, nslots, b);
+    if (rc != R3D_OK) goto out;
+    b.page = page;
+    b.pool = pool;
+    cudaFree(c->page);
+    cudaFree(c->pool);
+    c->page = page;
+    c->pool = pool;
+    page = nullptr;
+    pool = nullptr;
+    c->page_words = words;
+    c->nslots = nslots;
+    c->abpa = atlas_bpa(nslots);
+    c->shape[0] = nx;
+    c->shape[1] = ny;
+    c->shape[2] = nz;
+    c->have_bricks = true;
+    c->br = b;
+  }
+out:
+  cudaFree(lev);
+  cudaFree(dmax);
+  cudaFree(jobs);
+  cudaFree(pool);
+  cudaFree(page);
+  return rc;
+}
+
+int r3d_cuda_bricks_load(r3d_cuda_ctx *c, const uint32_t *page, uint32_t page_words,
+                         const uint8_t *slots, uint32_t nslots) {
+  if (!c || !page || (!slots && nslots)) return fail(c, R3D_E_INVALID, "bricks_load: bad args");
+  if (nslots >= (1u << 24)) return fail(c, R3D_E_INVALID, "bricks_load: too many slots");
+  DevBricks b;
+  int rc = decode_header(c, page, page_words, nslots, b);
+  if (rc != R3D_OK) return rc;
+  cudaSetDevice(c->device);
+  R3D_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  uint32_t *dpage = nullptr;
+  uint8_t *dpool = nullptr;
+  size_t pool_bytes = (size_t)(nslots ? nslots : 1u) * (128u * 128u * 128u);
+  cudaError_t e = cudaMalloc(&dpage, (size_t)page_words * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&dpool, pool_bytes);
+  if (e == cudaSuccess) e = cudaMemcpy(dpage, page, (size_t)page_words * 4, cudaMemcpyDefault);
+  if (e == cudaSuccess && nslots)
+    e = cudaMemcpy(dpool, slots, (size_t)nslots * (128u * 128u * 128u), cudaMemcpyDefault);
+  if (e != cudaSuccess) {
+    cudaFree(dpage);
+    cudaFree(dpool);
+    return cuda_fail(c, e, "bricks_load");
+  }
+  b.page = dpage;
+  b.pool = dpool;
+  cudaFree(c->page);
+  cudaFree(c->pool);
+  c->page = dpage;
+  c->pool = dpool;
+  c->page_words = page_words;
+  c->nslots = nslots;
+  c->abpa = atlas_bpa(nslots);
+  c->shape[0] = page[1];
+  c->shape[1] = page[2];
+  c->shape[2] = page[3];
+  c->have_bricks = true;
+  c->br = b;
+  return R3D_OK;
+}
+
+uint32_t r3d_cuda_brick_mode(const r3d_cuda_ctx *c) {
+  if (!c || !c->have_bricks) return 0u;
+  return c->abpa | (c->br.nlev << 8) | R3D_BRICK_LOD_FLAG;
+}
+
+int r3d_cuda_bricks_info(const r3d_cuda_ctx *c, uint32_t *page_words, uint32_t *nslots,
+                         uint32_t shape[3], uint32_t *nlev) {
+  if (!c) return R3D_E_INVALID;
+  if (!c->have_bricks) return R3D_E_STATE;
+  if (page_words) *page_words = c->page_words;
+  if (nslots) *nslots = c->nslots;
+  if (shape) memcpy(shape, c->shape, sizeof c->shape);
+  if (nlev) *nlev = c->br.nlev;
+  return R3D_OK;
+}
+
+int r3d_cuda_bricks_read(r3d_cuda_ctx *c, uint32_t *page, uint8_t *slots) {
+  if (!c) return R3D_E_INVALID;
+  if (!c->have_bricks) return fail(c, R3D_E_STATE, "bricks_read: no bricks");
+  cudaSetDevice(c->device);
+  R3D_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  if (page) R3D_CUDA_TRY(c, cudaMemcpy(page, c->page, (size_t)c->page_words * 4, cudaMemcpyDefault));
+  if (slots && c->nslots)
+    R3D_CUDA_TRY(c, cudaMemcpy(slots, c->pool, (size_t)c->nslots * (128u * 128u * 128u),
+                               cudaMemcpyDefault));
+  return R3D_OK;
+}
+
+int r3d_cuda_cube_read(r3d_cuda_ctx *c, int level, uint8_t *out, uint32_t dims[3]) {
+  if (!c) return R3D_E_INVALID;
+  if (!c->have_cube) return fail(c, R3D_E_STATE, "cube_read: no volume");
+  const DevCube &cb = c->cube;
+  const uint8_t *src;
+  uint32_t d[3];
+  if (level < 0) {
+    src = cb.occ;
+    memcpy(d, cb.odim, sizeof d);
+  } else {
+    if ((uint32_t)level >= cb.nlevels) return fail(c, R3D_E_INVALID, "cube_read: level");
+    src = cb.lev[level];
+    memcpy(d, cb.dim[level], sizeof d);
+  }
+  if (dims) memcpy(dims, d, sizeof d);
+  if (out) {
+    cudaSetDevice(c->device);
+    R3D_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    R3D_CUDA_TRY(c, cudaMemcpy(out, src, (size_t)d[0] * d[1] * d[2], cudaMemcpyDefault));
+  }
+  return R3D_OK;
+}
+
+}  // extern "C"
+
+// Validates and sanitizes one view against the image (the rectangle rule of
+// src/vk/vkbackend.c:6871-6900).  Returns 1 to render, 0 to skip, < 0 error.
+static int prepare_view(r3d_cuda_ctx *c, const r3d_frame_params &in, uint32_t out_w,
+                        uint32_t out_h, r3d_frame_params &pc) {
+  pc = in;
+  if (in.mode >= R3D_MODE_COUNT) return fail(c, R3D_E_INVALID, "view: mode %u", in.mode);
+  if (in.slab_grid || in.clip_valid)
+    return fail(c, R3D_E_UNSUPPORTED, "view: slab / clipmap sampling is not implemented");
+  if (in.view_flags & (R3D_VIEW_SURF | R3D_VIEW_STRETCH))
+    return fail(c, R3D_E_UNSUPPORTED, "view: flattened-surface views are not implemented");
+  if (in.overlay_flags & 0x1Du)
+    return fail(c, R3D_E_UNSUPPORTED, "view: overlay atlases are not implemented");
+  if (!(in.max_mip >= 0.0f)) return fail(c, R3D_E_INVALID, "view: max_mip must be >= 0");
+  if (!(in.step_voxels > 0.0f)) return fail(c, R3D_E_INVALID, "view: step_voxels must be > 0");
+  if (in.brick_mode) {
+    if (!(in.brick_mode & R3D_BRICK_LOD_FLAG))
+      return fail(c, R3D_E_UNSUPPORTED, "view: single-level brick atlases are not implemented");
+    if (!c->have_bricks) return fail(c, R3D_E_STATE, "view: no brick cache loaded");
+  } else if (!c->have_cube) {
+    return fail(c, R3D_E_STATE, "view: no volume uploaded");
+  }
+  uint32_t ox = in.view_org & 0xffffu, oy = (in.view_org >> 16) & 0xffffu;
+  uint32_t vw = in.viewport[0] ? in.viewport[0] : out_w;
+  uint32_t vh = in.viewport[1] ? in.viewport[1] : out_h;
+  bool ok = ox < out_w && oy < out_h;
+  if (ok) {
+    vw = min(vw, out_w - ox);
+    vh = min(vh, out_h - oy);
+    ok = vw && vh;
+  }
+  pc.view_org = ox | (oy << 16);
+  pc.viewport[0] = ok ? vw : 0u;
+  pc.viewport[1] = ok ? vh : 0u;
+  return ok ? 1 : 0;
+}
+
+extern "C" {
+
+int r3d_cuda_raycast_fwd(r3d_cuda_ctx *c, const r3d_frame_params *views, uint32_t nviews,
+                         uint8_t *rgba_out, uint32_t out_w, uint32_t out_h,
+                         const r3d_cuda_aux *aux, void *stream) {
+  if (!c || !views || !nviews || nviews > 64u || !rgba_out || !out_w || !out_h ||
+      out_w > 65535u || out_h > 65535u)
+    return fail(c, R3D_E_INVALID, "raycast_fwd: bad arguments");
+  cudaSetDevice(c->device);
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  r3d_frame_params pcs[64];
+  int render[64];
+  for (uint32_t v = 0; v < nviews; v++) {
+    render[v] = prepare_view(c, views[v], out_w, out_h, pcs[v]);
+    if (render[v] < 0) return render[v];
+  }
+  bool host = !is_device_ptr(rgba_out);
+  size_t npix = (size_t)out_w * out_h;
+  uint8_t *img = rgba_out;
+  uint32_t *steps = aux ? aux->steps : nullptr, *mip = aux ? aux->mip_index : nullptr;
+  unsigned long long *total = aux ? aux->total_steps : nullptr;
+  unsigned long long *counters = aux ? aux->counters : nullptr;
+  if (host) {
+    if (c->img_cap < npix * 4) {
+      cudaFree(c->img);
+      c->img = nullptr;
+      c->img_cap = 0;
+      R3D_CUDA_TRY(c, cudaMalloc(&c->img, npix * 4));
+      c->img_cap = npix * 4;
+    }
+    img = c->img;
+    // pixels outside every view keep the caller's contents
+    R3D_CUDA_TRY(c, cudaMemcpyAsync(img, rgba_out, npix * 4, cudaMemcpyHostToDevice, st));
+    if (steps || mip) {
+      if (c->aux_cap < npix * 2) {
+        cudaFree(c->aux_buf);
+        c->aux_buf = nullptr;
+        c->aux_cap = 0;
+        R3D_CUDA_TRY(c, cudaMalloc(&c->aux_buf, npix * 2 * 4));
+        c->aux_cap = npix * 2;
+      }
+      steps = steps ? c->aux_buf : nullptr;
+      mip = mip ? c->aux_buf + npix : nullptr;
+      if (steps)
+        R3D_CUDA_TRY(c, cudaMemcpyAsync(steps, aux->steps, npix * 4, cudaMemcpyHostToDevice, st));
+      if (mip)
+        R3D_CUDA_TRY(c,
+                     cudaMemcpyAsync(mip, aux->mip_index, npix * 4, cudaMemcpyHostToDevice, st));
+    }
+    if (total || counters) {
+      R3D_CUDA_TRY(c, cudaMemsetAsync(c->total, 0, (R3D_COUNTERS + 1) * 8, st));
+      total = total ? c->total : nullptr;
+      counters = counters ? c->total + 1 : nullptr;
+    }
+  }
+  R3D_CUDA_TRY(c, cudaEventRecord(c->ev0, st));
+  for (uint32_t v = 0; v < nviews; v++) {
+    if (!render[v]) continue;
+    cudaError_t e = launch_view(c, pcs[v], img, out_w, steps, mip, total, counters, st);
+    if (e != cudaSuccess) return cuda_fail(c, e, "raycast_fwd: launch");
+  }
+  R3D_CUDA_TRY(c, cudaEventRecord(c->ev1, st));
+  c->timed = true;
+  if (host) {
+    R3D_CUDA_TRY(c, cudaMemcpyAsync(rgba_out, img, npix * 4, cudaMemcpyDeviceToHost, st));
+    if (steps)
+      R3D_CUDA_TRY(c, cudaMemcpyAsync(aux->steps, steps, npix * 4, cudaMemcpyDeviceToHost, st));
+    if (mip)
+      R3D_CUDA_TRY(c, cudaMemcpyAsync(aux->mip_index, mip, npix * 4, cudaMemcpyDeviceToHost, st));
+    unsigned long long tsum[R3D_COUNTERS + 1] = {0};
+    if (total || counters)
+      R3D_CUDA_TRY(c, cudaMemcpyAsync(tsum, c->total, sizeof tsum, cudaMemcpyDeviceToHost, st));
+    R3D_CUDA_TRY(c, cudaStreamSynchronize(st));
+    if (total) *aux->total_steps += tsum[0];
+    if (counters)
+      for (int k = 0; k < R3D_COUNTERS; k++) aux->counters[k] += tsum[1 + k];
+  }
+  return R3D_OK;
+}
+
+int r3d_cuda_last_kernel_ns(r3d_cuda_ctx *c, uint64_t *ns) {
+  if (!c || !ns) return R3D_E_INVALID;
+  if (!c->timed) return fail(c, R3D_E_STATE, "last_kernel_ns: nothing timed");
+  cudaSetDevice(c->device);
+  R3D_CUDA_TRY(c, cudaEventSynchronize(c->ev1));
+  float ms = 0.0f;
+  R3D_CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  *ns = (uint64_t)((double)ms * 1e6);
+  return R3D_OK;
+}
+
+}  // extern "C"
+

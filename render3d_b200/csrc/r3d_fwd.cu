@@ -1,0 +1,128 @@
+// Forward raycast kernels: one thread per ray, 128-thread blocks covering
+// 16x8 dispatch threads as four 8x4 warp tiles whose lanes follow a Morton
+// (Z-order) curve, so a warp's rays stay spatially compact and share cache
+// lines.  Mode, sampling path and gradient quality are template parameters
+// (the reference specializes its shader per path for the same reason:
+// src/shaders/raycast.slang:127-130).
+#include "r3d_internal.h"
+
+namespace r3d {
+
+template <int PATH, int MODE, bool FAST, bool COUNT>
+__global__ void __launch_bounds__(128) k_raycast(const __grid_constant__ r3d_frame_params pc,
+                                                 const __grid_constant__ DevScene s,
+                                                 const uchar4 *__restrict__ lut,
+                                                 uchar4 *__restrict__ img, uint32_t out_w,
+                                                 uint32_t *__restrict__ steps_out,
+                                                 uint32_t *__restrict__ mip_out,
+                                                 unsigned long long *__restrict__ total,
+                                                 unsigned long long *__restrict__ counters) {
+  __shared__ float4 tf[256];
+  for (uint32_t i = threadIdx.x; i < 256u; i += blockDim.x) {
+    uchar4 u = lut[i];
+    tf[i] = make_float4((float)u.x, (float)u.y, (float)u.z, (float)u.w);
+  }
+  __syncthreads();
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t lx = (lane & 1u) | ((lane >> 1) & 2u) | ((lane >> 2) & 4u);
+  const uint32_t ly = ((lane >> 1) & 1u) | ((lane >> 2) & 2u);
+  const uint32_t tx = blockIdx.x * 16u + (warp & 1u) * 8u + lx;
+  const uint32_t ty = blockIdx.y * 8u + (warp >> 1) * 4u + ly;
+  const bool half = (pc.view_flags & R3D_VIEW_HALF) != 0u;
+  const uint32_t px = half ? tx * 2u : tx, py = half ? ty * 2u : ty;
+  const uint32_t vw = pc.viewport[0], vh = pc.viewport[1];
+  uint32_t my_steps = 0, my_tf = 0, my_grad = 0, my_walk = 0;
+  if (px < vw && py < vh) {
+    RayResult r;
+    march<PATH, MODE, FAST, COUNT>(pc, s, tf, px, py, r);
+    my_tf = r.n_tf;
+    my_grad = r.n_grad;
+    my_walk = r.n_walk;
+    const uchar4 col = make_uchar4(unorm8(r.rgb[0]), unorm8(r.rgb[1]), unorm8(r.rgb[2]), 255);
+    const uint32_t ox = pc.view_org & 0xffffu, oy = pc.view_org >> 16;
+    const uint32_t n = half ? 4u : 1u;
+    for (uint32_t k = 0; k < n; k++) {
+      uint32_t ax = px + (k & 1u), ay = py + (k >> 1);
+      if (ax >= vw || ay >= vh) continue;
+      size_t i = (size_t)(oy + ay) * out_w + (ox + ax);
+      img[i] = col;
+      if (steps_out) steps_out[i] = r.steps;
+      if (mip_out) mip_out[i] = r.mip_index;
+    }
+    my_steps = r.steps;
+  }
+  if (total) {
+    uint32_t sum = my_steps;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (lane == 0 && sum) atomicAdd(total, (unsigned long long)sum);
+  }
+  if (COUNT) {
+    uint32_t v[4] = {my_steps, my_tf, my_grad, my_walk};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      uint32_t sum = v[k];
+      for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+      if (lane == 0 && sum) atomicAdd(counters + k, (unsigned long long)sum);
+    }
+  }
+}
+
+template <int PATH, int MODE, bool FAST>
+static cudaError_t launch_t(const r3d_frame_params &pc, const DevScene &s, const uchar4 *lut,
+                            uint8_t *img, uint32_t out_w, uint32_t *steps, uint32_t *mip,
+                            unsigned long long *total, unsigned long long *counters,
+                            cudaStream_t stream) {
+  const bool half = (pc.view_flags & R3D_VIEW_HALF) != 0u;
+  uint32_t gw = half ? (pc.viewport[0] + 1u) / 2u : pc.viewport[0];
+  uint32_t gh = half ? (pc.viewport[1] + 1u) / 2u : pc.viewport[1];
+  dim3 grid((gw + 15u) / 16u, (gh + 7u) / 8u);
+  if (counters)
+    k_raycast<PATH, MODE, FAST, true><<<grid, 128, 0, stream>>>(pc, s, lut, (uchar4 *)img, out_w,
+                                                                steps, mip, total, counters);
+  else
+    k_raycast<PATH, MODE, FAST, false><<<grid, 128, 0, stream>>>(pc, s, lut, (uchar4 *)img, out_w,
+                                                                 steps, mip, total, nullptr);
+  return cudaGetLastError();
+}
+
+template <int PATH>
+static cudaError_t launch_p(const r3d_frame_params &pc, const DevScene &s, bool fast,
+                            const uchar4 *lut, uint8_t *img, uint32_t out_w, uint32_t *steps,
+                            uint32_t *mip, unsigned long long *total,
+                            unsigned long long *cnt, cudaStream_t st) {
+  switch (pc.mode) {
+    case R3D_MODE_FULL:
+      return fast ? launch_t<PATH, R3D_MODE_FULL, true>(pc, s, lut, img, out_w, steps, mip, total, cnt,
+                                                        st)
+                  : launch_t<PATH, R3D_MODE_FULL, false>(pc, s, lut, img, out_w, steps, mip,
+                                                         total, cnt, st);
+    case R3D_MODE_MIP:
+      return launch_t<PATH, R3D_MODE_MIP, false>(pc, s, lut, img, out_w, steps, mip, total, cnt, st);
+    case R3D_MODE_DEPTH:
+      return launch_t<PATH, R3D_MODE_DEPTH, false>(pc, s, lut, img, out_w, steps, mip, total, cnt, st);
+    case R3D_MODE_HEATMAP:
+      return launch_t<PATH, R3D_MODE_HEATMAP, false>(pc, s, lut, img, out_w, steps, mip, total, cnt,
+                                                     st);
+    case R3D_MODE_RAYDIR:
+      return launch_t<PATH, R3D_MODE_RAYDIR, false>(pc, s, lut, img, out_w, steps, mip, total, cnt,
+                                                    st);
+    default:
+      return launch_t<PATH, R3D_MODE_FLAT, false>(pc, s, lut, img, out_w, steps, mip, total, cnt, st);
+  }
+}
+
+cudaError_t launch_view(const r3d_cuda_ctx *c, const r3d_frame_params &pc, uint8_t *img,
+                        uint32_t out_w, uint32_t *steps, uint32_t *mip_index,
+                        unsigned long long *total, unsigned long long *counters,
+                        cudaStream_t stream) {
+  DevScene s = c->scene();
+  bool fast = c->quality == R3D_QUALITY_FAST;
+  if (pc.brick_mode != 0u)
+    return launch_p<PATH_LOD_BRICKS>(pc, s, fast, c->lut, img, out_w, steps, mip_index, total,
+                                     counters, stream);
+  return launch_p<PATH_CUBE>(pc, s, fast, c->lut, img, out_w, steps, mip_index, total, counters,
+                             stream);
+}
+
+}  // namespace r3d

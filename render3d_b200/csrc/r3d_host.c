@@ -1,0 +1,330 @@
+/* Host-side raycast inputs (camera, TF, LOD policy, bench orbit) and the
+ * seeded scroll phantom.  Compiled with -ffp-contract=off so the float
+ * results equal the reference core's (src/core/camera.c, transfer.c,
+ * lod.h, mathx.h) bit for bit. */
+#include "r3d_host.h"
+
+#include <math.h>
+#include <pthread.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ---- vector helpers in the evaluation order of src/core/mathx.h ---- */
+
+static float dot3(const float a[3], const float b[3]) {
+  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+static void cross3(const float a[3], const float b[3], float o[3]) {
+  float x = a[1] * b[2] - a[2] * b[1], y = a[2] * b[0] - a[0] * b[2], z = a[0] * b[1] - a[1] * b[0];
+  o[0] = x, o[1] = y, o[2] = z;
+}
+static void norm3(float a[3]) {
+  float l = sqrtf(dot3(a, a));
+  if (l > 0.0f) {
+    float s = 1.0f / l;
+    a[0] *= s, a[1] *= s, a[2] *= s;
+  } else {
+    a[0] = a[1] = a[2] = 0.0f;
+  }
+}
+static float clampf_(float x, float lo, float hi) { return x < lo ? lo : (x > hi ? hi : x); }
+
+/* ---- camera (src/core/camera.c) ---- */
+
+#define PITCH_LIMIT 1.55334303f /* pi/2 - 1 degree */
+
+void r3d_host_camera_init(r3d_host_camera *c, const float pos[3]) {
+  memset(c, 0, sizeof *c);
+  memcpy(c->pos, pos, sizeof c->pos);
+  c->fov_y = 1.04719755f; /* 60 degrees */
+}
+
+static void forward_of(const r3d_host_camera *c, float f[3]) {
+  float cp = cosf(c->pitch);
+  f[0] = sinf(c->yaw) * cp;
+  f[1] = sinf(c->pitch);
+  f[2] = cosf(c->yaw) * cp;
+}
+
+static void flat_right(const float fwd[3], float r[3]) {
+  static const float wup[3] = {0.0f, 1.0f, 0.0f};
+  cross3(fwd, wup, r);
+  norm3(r);
+  if (sqrtf(dot3(r, r)) == 0.0f) r[0] = 1.0f, r[1] = 0.0f, r[2] = 0.0f;
+}
+
+void r3d_host_camera_move(r3d_host_camera *c, const float local[3], float dist) {
+  float f[3], r[3];
+  forward_of(c, f);
+  flat_right(f, r);
+  for (int a = 0; a < 3; a++) {
+    float up = a == 1 ? 1.0f : 0.0f;
+    float d = (r[a] * local[0] + up * local[1]) + f[a] * local[2];
+    c->pos[a] = c->pos[a] + d * dist;
+  }
+}
+
+void r3d_host_camera_look(r3d_host_camera *c, float dyaw, float dpitch) {
+  c->yaw += dyaw;
+  c->pitch = clampf_(c->pitch + dpitch, -PITCH_LIMIT, PITCH_LIMIT);
+}
+
+static void orbit_sync(r3d_host_camera *c) {
+  float f[3];
+  forward_of(c, f);
+  for (int a = 0; a < 3; a++) c->pos[a] = c->target[a] - f[a] * c->dist;
+}
+
+void r3d_host_camera_orbit_set(r3d_host_camera *c, const float target[3], float dist) {
+  memcpy(c->target, target, sizeof c->target);
+  c->dist = dist;
+  orbit_sync(c);
+}
+
+void r3d_host_camera_orbit_drag(r3d_host_camera *c, float dyaw, float dpitch) {
+  r3d_host_camera_look(c, dyaw, dpitch);
+  orbit_sync(c);
+}
+
+void r3d_host_camera_orbit_zoom(r3d_host_camera *c, float factor) {
+  c->dist = clampf_(c->dist * factor, 0.0005f, 20.0f);
+  orbit_sync(c);
+}
+
+void r3d_host_camera_basis(const r3d_host_camera *c, float aspect, float right[3], float up[3],
+                           float fwd[3]) {
+  float f[3], r[3], u[3];
+  forward_of(c, f);
+  flat_right(f, r);
+  cross3(r, f, u);
+  float t = tanf(c->fov_y * 0.5f);
+  float ta = t * aspect;
+  for (int a = 0; a < 3; a++) {
+    right[a] = r[a] * ta;
+    up[a] = u[a] * t;
+    fwd[a] = f[a];
+  }
+}
+
+/* src/core/mathx.h:34-43 */
+void r3d_host_m3_ypr(float yaw, float pitch, float roll, float m[3][3]) {
+  float cy = cosf(yaw), sy = sinf(yaw), cp = cosf(pitch), sp = sinf(pitch), cr = cosf(roll),
+        sr = sinf(roll);
+  m[0][0] = cy * cr + sy * sp * sr;
+  m[0][1] = -cy * sr + sy * sp * cr;
+  m[0][2] = sy * cp;
+  m[1][0] = cp * sr;
+  m[1][1] = cp * cr;
+  m[1][2] = -sp;
+  m[2][0] = -sy * cr + cy * sp * sr;
+  m[2][1] = sy * sr + cy * sp * cr;
+  m[2][2] = cy * cp;
+}
+
+/* ---- transfer function (src/core/transfer.c) ---- */
+
+void r3d_host_tf_build(const uint8_t *values, const uint8_t (*rgba)[4], uint32_t npts,
+                       uint8_t lut[256][4]) {
+  if (!npts) return;
+  for (uint32_t i = 0; i < 256u; i++) {
+    uint32_t lo = 0, hi = npts - 1u;
+    for (uint32_t k = 0; k + 1u < npts; k++) {
+      if (values[k] <= i && i <= values[k + 1u]) {
+        lo = k;
+        hi = k + 1u;
+        break;
+      }
+    }
+    uint32_t span = (uint32_t)values[hi] - (uint32_t)values[lo];
+    uint32_t num = span ? i - values[lo] : 0u, den = span ? span : 1u;
+    for (int ch = 0; ch < 4; ch++) {
+      uint32_t a = rgba[lo][ch], b = rgba[hi][ch];
+      lut[i][ch] = (uint8_t)((a * (den - num) + b * num) / den);
+    }
+  }
+}
+
+typedef struct preset_pt {
+  uint8_t v, c[4];
+} preset_pt;
+
+static const preset_pt P_GREY[] = {{0, {0, 0, 0, 0}}, {255, {255, 255, 255, 255}}};
+static const preset_pt P_SCROLL[] = {{0, {0, 0, 0, 0}},
+                                     {40, {0, 0, 0, 0}},
+                                     {90, {150, 110, 70, 40}},
+                                     {160, {230, 190, 130, 160}},
+                                     {255, {255, 250, 240, 255}}};
+static const preset_pt P_HIGHPASS[] = {{0, {0, 0, 0, 0}},
+                                       {120, {0, 0, 0, 0}},
+                                       {180, {200, 200, 255, 120}},
+                                       {255, {255, 255, 255, 255}}};
+
+uint32_t r3d_host_tf_preset(uint32_t idx, uint8_t lut[256][4]) {
+  const preset_pt *p;
+  uint32_t n;
+  switch (idx) {
+    case 0: p = P_GREY, n = 2; break;
+    case 1: p = P_SCROLL, n = 5; break;
+    case 2: p = P_HIGHPASS, n = 4; break;
+    default: return 3u;
+  }
+  uint8_t vals[8], cols[8][4];
+  for (uint32_t k = 0; k < n; k++) {
+    vals[k] = p[k].v;
+    memcpy(cols[k], p[k].c, 4);
+  }
+  r3d_host_tf_build(vals, (const uint8_t(*)[4])cols, n, lut);
+  return idx;
+}
+
+float r3d_host_tf_min_visible(const uint8_t lut[256][4]) {
+  for (uint32_t i = 0; i < 256u; i++)
+    if (lut[i][3] != 0) return (float)i;
+  return 255.0f;
+}
+
+float r3d_host_skip_gate(float low_cut, const uint8_t lut[256][4]) {
+  return fmaxf(low_cut, r3d_host_tf_min_visible(lut) - 0.5f) / 255.0f;
+}
+
+/* ---- LOD policy (src/core/lod.h) ---- */
+
+uint32_t r3d_host_lod_pick(float distance, float pixel_cone, float base_voxels,
+                           uint32_t nlevels) {
+  if (!nlevels) return 0;
+  float footprint = fmaxf(distance * pixel_cone * base_voxels, 1.0f);
+  int level = (int)floorf(log2f(footprint));
+  if (level < 0) level = 0;
+  if (level >= (int)nlevels) level = (int)nlevels - 1;
+  return (uint32_t)level;
+}
+
+uint32_t r3d_host_lod_fallback(uint32_t desired, uint32_t ordinal, uint32_t nlevels) {
+  if (!nlevels || desired >= nlevels || ordinal >= nlevels) return UINT32_MAX;
+  uint32_t coarse = nlevels - desired;
+  if (ordinal < coarse) return desired + ordinal;
+  return desired - 1u - (ordinal - coarse);
+}
+
+/* ---- scripted orbit view (src/main.c:3932-3946, 6788-6824) ---- */
+
+void r3d_host_orbit_view(r3d_frame_params *p, float ph, const float target[3], uint32_t w,
+                         uint32_t h, float step_voxels, float density, float lod_bias,
+                         uint32_t mode, uint32_t frame_index, float low_cut,
+                         const uint8_t lut[256][4]) {
+  const float tau = 6.2831853f;
+  static const float origin0[3] = {0.5f, 0.5f, -1.5f};
+  r3d_host_camera cam;
+  r3d_host_camera_init(&cam, origin0);
+  cam.yaw = ph * tau;
+  cam.pitch = 0.5f * sinf(ph * tau * 2.0f);
+  r3d_host_camera_orbit_set(&cam, target, 2.0f);
+  memset(p, 0, sizeof *p);
+  memcpy(p->cam_origin, cam.pos, sizeof cam.pos);
+  r3d_host_camera_basis(&cam, (float)w / (float)h, p->cam_right, p->cam_up, p->cam_forward);
+  p->step_voxels = step_voxels;
+  p->density = density;
+  p->lod_bias = lod_bias;
+  p->max_mip = 10.0f;
+  p->viewport[0] = w;
+  p->viewport[1] = h;
+  p->mode = mode;
+  p->frame_index = frame_index;
+  p->threshold = low_cut / 255.0f;
+  p->skip_gate = r3d_host_skip_gate(low_cut, lut);
+  float m[3][3];
+  r3d_host_m3_ypr(0.0f, 0.0f, 0.0f, m);
+  memcpy(p->vol_r0, m[0], 12);
+  memcpy(p->vol_r1, m[1], 12);
+  memcpy(p->vol_r2, m[2], 12);
+}
+
+/* ---- seeded scroll phantom ---- */
+
+void r3d_host_phantom_default(uint32_t n, uint64_t seed, r3d_phantom_desc *d) {
+  memset(d, 0, sizeof *d);
+  d->seed = seed;
+  d->pitch = n <= 256u ? 14.0f : 18.0f;
+  d->radius = 110.0f * (float)n / 256.0f;
+  d->r0 = 8.0f;
+  d->sheet_half = 3.0f;
+  d->in_mean = 130.0f;
+  d->in_sd = 15.0f;
+  d->air_mean = 12.0f;
+  d->air_sd = 4.0f;
+  d->noise_sd = 6.0f;
+}
+
+static inline uint64_t splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+typedef struct phantom_job {
+  uint8_t *vox;
+  const uint8_t *mask;
+  uint32_t nx, ny, z0, z1;
+  const r3d_phantom_desc *d;
+} phantom_job;
+
+static void *phantom_worker(void *arg) {
+  phantom_job *j = arg;
+  const r3d_phantom_desc *d = j->d;
+  const double two_pi = 6.283185307179586;
+  for (uint32_t z = j->z0; z < j->z1; z++)
+    for (uint32_t y = 0; y < j->ny; y++)
+      for (uint32_t x = 0; x < j->nx; x++) {
+        uint64_t idx = ((uint64_t)z * j->ny + y) * j->nx + x;
+        uint64_t h1 = splitmix64(d->seed ^ (idx * 2u));
+        uint64_t h2 = splitmix64(d->seed ^ (idx * 2u + 1u));
+        double u1 = ((double)(h1 >> 11) + 1.0) * 0x1.0p-53; /* (0, 1] */
+        double u2 = (double)(h2 >> 11) * 0x1.0p-53;
+        double rad = sqrt(-2.0 * log(u1));
+        double g0 = rad * cos(two_pi * u2), g1 = rad * sin(two_pi * u2);
+        int pap = j->mask[(size_t)y * j->nx + x];
+        double mean = pap ? d->in_mean : d->air_mean, sd = pap ? d->in_sd : d->air_sd;
+        double v = mean + sd * g0 + d->noise_sd * g1;
+        v = floor(v + 0.5);
+        j->vox[idx] = (uint8_t)(v < 0.0 ? 0.0 : (v > 255.0 ? 255.0 : v));
+      }
+  return NULL;
+}
+
+int r3d_host_phantom(uint8_t *vox, uint32_t nx, uint32_t ny, uint32_t nz,
+                     const r3d_phantom_desc *d, int threads) {
+  if (!vox || !d || !nx || !ny || !nz || !(d->pitch > 0.0f)) return -1;
+  uint8_t *mask = malloc((size_t)nx * ny);
+  if (!mask) return -1;
+  /* papyrus mask of one z slice: the spiral is a prism along z */
+  const double two_pi = 6.283185307179586;
+  double cx = 0.5 * nx, cy = 0.5 * ny;
+  for (uint32_t y = 0; y < ny; y++)
+    for (uint32_t x = 0; x < nx; x++) {
+      double dx = x + 0.5 - cx, dy = y + 0.5 - cy;
+      double r = sqrt(dx * dx + dy * dy);
+      double th = atan2(dy, dx);
+      if (th < 0.0) th += two_pi;
+      double m = fmod(r - d->r0 - d->pitch * th / two_pi, d->pitch);
+      if (m < 0.0) m += d->pitch;
+      double dist = m < d->pitch - m ? m : d->pitch - m;
+      mask[(size_t)y * nx + x] = dist < d->sheet_half && r >= d->r0 && r < d->radius;
+    }
+  if (threads <= 0) threads = 8;
+  if (threads > 256) threads = 256;
+  if ((uint32_t)threads > nz) threads = (int)nz;
+  pthread_t tid[256];
+  phantom_job jobs[256];
+  int live[256];
+  for (int i = 0; i < threads; i++) {
+    jobs[i] = (phantom_job){vox, mask, nx, ny, (uint32_t)((uint64_t)nz * (uint64_t)i / threads),
+                            (uint32_t)((uint64_t)nz * (uint64_t)(i + 1) / threads), d};
+    live[i] = pthread_create(&tid[i], NULL, phantom_worker, &jobs[i]) == 0;
+    if (!live[i]) phantom_worker(&jobs[i]);
+  }
+  for (int i = 0; i < threads; i++)
+    if (live[i]) pthread_join(tid[i], NULL);
+  free(mask);
+  return 0;
+}

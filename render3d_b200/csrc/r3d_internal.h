@@ -1,0 +1,72 @@
+// Internal state of a raycast context (not part of the C-ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "r3d_cuda.h"
+#include "r3d_march.cuh"
+
+struct r3d_cuda_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+
+  // cube volume: all mip levels in one allocation, then the occupancy grid
+  uint8_t *cube_buf = nullptr;
+  size_t cube_bytes = 0;
+  bool have_cube = false;
+  r3d::DevCube cube{};
+
+  // LOD brick cache
+  uint32_t *page = nullptr;
+  uint8_t *pool = nullptr;
+  uint32_t page_words = 0;
+  uint32_t nslots = 0;
+  uint32_t abpa = 0;
+  uint32_t shape[3] = {0, 0, 0};
+  bool have_bricks = false;
+  r3d::DevBricks br{};
+
+  // transfer function
+  uchar4 *lut = nullptr;
+  uint8_t lut_host[256][4];
+  float tf_zero_t = -1.0f;
+
+  uint32_t quality = R3D_QUALITY_FULL;
+  float alpha_cutoff = 0.98f;
+  uint32_t *status = nullptr;
+
+  // device staging for host-pointer outputs
+  uint8_t *img = nullptr;
+  size_t img_cap = 0;
+  uint32_t *aux_buf = nullptr;
+  size_t aux_cap = 0;
+  unsigned long long *total = nullptr;  // R3D_COUNTERS + 1 device counters
+
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  bool timed = false;
+
+  r3d::DevScene scene() const;
+};
+
+namespace r3d {
+
+int fail(r3d_cuda_ctx *c, int code, const char *fmt, ...);
+int cuda_fail(r3d_cuda_ctx *c, cudaError_t e, const char *what);
+bool is_device_ptr(const void *p);
+
+// Forward launch of one sanitized view into a device image.
+cudaError_t launch_view(const r3d_cuda_ctx *c, const r3d_frame_params &pc, uint8_t *img,
+                        uint32_t out_w, uint32_t *steps, uint32_t *mip_index,
+                        unsigned long long *total, unsigned long long *counters,
+                        cudaStream_t stream);
+
+}  // namespace r3d
+
+#define R3D_CUDA_TRY(ctx, expr)                                  \
+  do {                                                           \
+    cudaError_t e_ = (expr);                                     \
+    if (e_ != cudaSuccess) return r3d::cuda_fail(ctx, e_, #expr); \
+  } while (0)

@@ -1,0 +1,616 @@
+// Device-side ray march shared by the forward, batched and adjoint kernels.
+//
+// Restates render3d's raycast compute shader (src/shaders/raycast.slang) for
+// sm_100a: one thread per ray, trilinear u8 sampling in FP32 in software, the
+// 256-entry TF from shared memory, ray-cone LOD, empty-space skipping, six-
+// or four-tap gradient shading and front-to-back compositing.  Arithmetic is
+// fixed operation by operation (explicit fmaf, compiled with -fmad=false,
+// IEEE division and square root, project-written log2/exp2/pow) so that the
+// CPU restatement used as the test oracle reproduces every bit, including
+// the early-termination step counts and MIP indices.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "r3d_cuda.h"
+#include "r3d_fmath.h"
+#include "r3d_types.h"
+
+namespace r3d {
+
+constexpr int kMaxLevels = 16;
+constexpr uint32_t kMaxSteps = 4096u;  // raycast.slang:123
+constexpr float kInv255 = 1.0f / 255.0f;
+
+enum Path { PATH_CUBE = 0, PATH_LOD_BRICKS = 1 };
+
+struct DevCube {
+  const uint8_t *lev[kMaxLevels];
+  uint32_t dim[kMaxLevels][3];
+  uint32_t nlevels;
+  uint32_t maxdim;
+  const uint8_t *occ;
+  uint32_t odim[3];
+};
+
+// LOD brick cache.  The page-table header is validated and decoded on the
+// host when the cache is loaded; entries are read from device memory.
+struct DevBricks {
+  const uint32_t *page;
+  uint32_t page_words;
+  const uint8_t *pool;  // slot s at pool + s * 128^3, x fastest
+  uint32_t nslots;
+  uint32_t nlev;
+  float bs[3];  // base shape
+  float md;     // max(base shape)
+  uint32_t off[kMaxLevels];
+  uint32_t bd[kMaxLevels][3];
+  uint32_t scale[kMaxLevels];
+  float inv_scale[kMaxLevels];  // exact: scales are powers of two
+};
+
+struct DevScene {
+  DevCube cube;
+  DevBricks br;
+  uint32_t *status;
+  float alpha_cutoff;
+  float tf_zero_t;  // TF coordinates below this have alpha exactly 0
+};
+
+struct RayResult {
+  float rgb[3];
+  uint32_t steps;
+  uint32_t mip_index;
+  uint32_t n_tf;    // composited TF lookups
+  uint32_t n_grad;  // gradient-shaded samples
+  uint32_t n_walk;  // page-table walks
+};
+
+__device__ __forceinline__ float lerp_(float a, float b, float t) { return fmaf(t, b - a, a); }
+__device__ __forceinline__ float clamp_(float x, float lo, float hi) {
+  return fminf(fmaxf(x, lo), hi);
+}
+__device__ __forceinline__ float sat_(float x) { return clamp_(x, 0.0f, 1.0f); }
+__device__ __forceinline__ float dot3(float3 a, float3 b) {
+  return fmaf(a.z, b.z, fmaf(a.y, b.y, a.x * b.x));
+}
+__device__ __forceinline__ float3 norm3(float3 a) {
+  float inv = 1.0f / sqrtf(dot3(a, a));
+  return make_float3(a.x * inv, a.y * inv, a.z * inv);
+}
+
+// common.slang:57-61
+__device__ __forceinline__ float hash12(uint32_t px, uint32_t py, uint32_t frame) {
+  uint32_t h = px * 374761393u + py * 668265263u + frame * 2246822519u;
+  h = (h ^ (h >> 13)) * 1274126177u;
+  return (float)(h >> 8) * (1.0f / 16777216.0f);
+}
+
+__device__ __forceinline__ uint8_t unorm8(float x) {
+  return (uint8_t)(int)fmaf(sat_(x), 255.0f, 0.5f);
+}
+
+// Clamp-to-edge trilinear at texel centres on a u8 grid: x, then y, then z
+// lerps in 0..255 space, scaled by 1/255 at the end.
+__device__ __forceinline__ float tri_u8(const uint8_t *__restrict__ g, uint32_t dx, uint32_t dy,
+                                        uint32_t dz, float tx, float ty, float tz) {
+  tx = clamp_(tx, 0.0f, (float)(dx - 1u));
+  ty = clamp_(ty, 0.0f, (float)(dy - 1u));
+  tz = clamp_(tz, 0.0f, (float)(dz - 1u));
+  uint32_t x0 = (uint32_t)tx, y0 = (uint32_t)ty, z0 = (uint32_t)tz;
+  float fx = tx - (float)x0, fy = ty - (float)y0, fz = tz - (float)z0;
+  uint32_t x1 = min(x0 + 1u, dx - 1u), y1 = min(y0 + 1u, dy - 1u), z1 = min(z0 + 1u, dz - 1u);
+  size_t sy = dx, sz = (size_t)dx * dy;
+  const uint8_t *r00 = g + (size_t)y0 * sy + (size_t)z0 * sz;
+  const uint8_t *r10 = g + (size_t)y1 * sy + (size_t)z0 * sz;
+  const uint8_t *r01 = g + (size_t)y0 * sy + (size_t)z1 * sz;
+  const uint8_t *r11 = g + (size_t)y1 * sy + (size_t)z1 * sz;
+  float a0 = __ldg(r00 + x0), a1 = __ldg(r00 + x1);
+  float b0 = __ldg(r10 + x0), b1 = __ldg(r10 + x1);
+  float c0 = __ldg(r01 + x0), c1 = __ldg(r01 + x1);
+  float d0 = __ldg(r11 + x0), d1 = __ldg(r11 + x1);
+  float c00 = lerp_(a0, a1, fx), c10 = lerp_(b0, b1, fx);
+  float c01 = lerp_(c0, c1, fx), c11 = lerp_(d0, d1, fx);
+  float e0 = lerp_(c00, c10, fy), e1 = lerp_(c01, c11, fy);
+  return lerp_(e0, e1, fz) * kInv255;
+}
+
+// Trilinear inside one 128^3 slot at slot-local texel coordinates already
+// clamped to [0, 127].
+__device__ __forceinline__ float tri_slot(const uint8_t *__restrict__ g, float tx, float ty,
+                                          float tz) {
+  uint32_t x0 = (uint32_t)tx, y0 = (uint32_t)ty, z0 = (uint32_t)tz;
+  float fx = tx - (float)x0, fy = ty - (float)y0, fz = tz - (float)z0;
+  uint32_t dx1 = x0 < 127u ? 1u : 0u;
+  uint32_t dy1 = y0 < 127u ? 128u : 0u;
+  uint32_t dz1 = z0 < 127u ? 16384u : 0u;
+  const uint8_t *r00 = g + ((z0 << 14) | (y0 << 7) | x0);
+  float a0 = __ldg(r00), a1 = __ldg(r00 + dx1);
+  float b0 = __ldg(r00 + dy1), b1 = __ldg(r00 + dy1 + dx1);
+  float c0 = __ldg(r00 + dz1), c1 = __ldg(r00 + dz1 + dx1);
+  float d0 = __ldg(r00 + dz1 + dy1), d1 = __ldg(r00 + dz1 + dy1 + dx1);
+  float c00 = lerp_(a0, a1, fx), c10 = lerp_(b0, b1, fx);
+  float c01 = lerp_(c0, c1, fx), c11 = lerp_(d0, d1, fx);
+  float e0 = lerp_(c00, c10, fy), e1 = lerp_(c01, c11, fy);
+  return lerp_(e0, e1, fz) * kInv255;
+}
+
+// volumes[0].SampleLevel(p, lod): trilinear within a level, linear between
+// floor(lod) and floor(lod)+1 (raycast.slang:409-416, vkbackend.c:1058-1069)
+__device__ __forceinline__ float cube_sample(const DevCube &c, float3 p, float lod) {
+  float fl = floorf(lod);
+  uint32_t m0 = min((uint32_t)fl, c.nlevels - 1u);
+  float fr = lod - fl;
+  float v = tri_u8(c.lev[m0], c.dim[m0][0], c.dim[m0][1], c.dim[m0][2],
+                   fmaf(p.x, (float)c.dim[m0][0], -0.5f), fmaf(p.y, (float)c.dim[m0][1], -0.5f),
+                   fmaf(p.z, (float)c.dim[m0][2], -0.5f));
+  if (fr > 0.0f && m0 + 1u < c.nlevels) {
+    uint32_t m1 = m0 + 1u;
+    float v1 = tri_u8(c.lev[m1], c.dim[m1][0], c.dim[m1][1], c.dim[m1][2],
+                      fmaf(p.x, (float)c.dim[m1][0], -0.5f),
+                      fmaf(p.y, (float)c.dim[m1][1], -0.5f),
+                      fmaf(p.z, (float)c.dim[m1][2], -0.5f));
+    v = lerp_(v, v1, fr);
+  }
+  return v;
+}
+
+// occ.SampleLevel(p, 0) with a nearest sampler
+__device__ __forceinline__ float occ_sample(const DevCube &c, float3 p) {
+  float q[3] = {floorf(p.x * (float)c.odim[0]), floorf(p.y * (float)c.odim[1]),
+                floorf(p.z * (float)c.odim[2])};
+  uint32_t i[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    float m = (float)(c.odim[a] - 1u);
+    i[a] = !(q[a] >= 0.0f) ? 0u : (q[a] > m ? c.odim[a] - 1u : (uint32_t)q[a]);
+  }
+  return (float)__ldg(c.occ + ((size_t)i[2] * c.odim[1] + i[1]) * c.odim[0] + i[0]) * kInv255;
+}
+
+struct BrickCtx {  // raycast.slang:144-152
+  bool ok;
+  float maxv;
+  float3 bl;
+  uint32_t slot;
+  float grad_vox;
+  float world_brick;
+};
+
+struct LodCache {  // raycast.slang:190-196
+  bool valid;
+  int desired;
+  uint32_t scale;
+  float inv_scale;
+  uint32_t bc[3];
+  BrickCtx c;
+};
+
+__device__ __forceinline__ uint32_t page_entry(const DevScene &s, uint32_t i) {
+  if (i >= s.br.page_words) {
+    atomicOr(s.status, R3D_STATUS_PAGE_RANGE);
+    return 0xFFFFFFFFu;
+  }
+  return __ldcg(s.br.page + i);  // page table through L2
+}
+
+// bricks_lod_locate_ex, raycast.slang:198-247 (header pre-decoded)
+__device__ __forceinline__ BrickCtx lod_locate_ex(const DevScene &s, float3 p, float lod,
+                                               LodCache &lc, int desired) {
+  const DevBricks &b = s.br;
+  BrickCtx c;
+  c.ok = false;
+  c.maxv = 0.0f;
+  c.bl = make_float3(0.0f, 0.0f, 0.0f);
+  c.slot = 0;
+  c.grad_vox = 1.0f;
+  c.world_brick = (128.0f * (float)(1u << (b.nlev - 1u))) / b.md;
+  float base_v[3] = {clamp_(p.x * b.md, 0.0f, fmaxf(b.bs[0] - 0.001f, 0.0f)),
+                     clamp_(p.y * b.md, 0.0f, fmaxf(b.bs[1] - 0.001f, 0.0f)),
+                     clamp_(p.z * b.md, 0.0f, fmaxf(b.bs[2] - 0.001f, 0.0f))};
+  int last = (int)b.nlev - 1;
+  uint32_t scale_out = 1u;
+  float inv_out = 1.0f;
+  uint32_t bco[3] = {0u, 0u, 0u};
+  for (uint32_t step = 0; step < 4u; step++) {
+    int li = step < 3u ? desired + (int)step : last;
+    if (li < 0 || li > last || (step == 3u && li <= desired + 2)) continue;
+    float inv = b.inv_scale[li];
+    float lv[3];
+    uint32_t bc[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      lv[a] = base_v[a] * inv;
+      bc[a] = min((uint32_t)lv[a] >> 7, b.bd[li][a] - 1u);
+    }
+    uint32_t bi = b.off[li] + (bc[2] * b.bd[li][1] + bc[1]) * b.bd[li][0] + bc[0];
+    uint32_t e = page_entry(s, bi);
+    if (e == 0xFFFFFFFFu) continue;
+    uint32_t slot = e & 0xFFFFFFu;
+    if (slot >= b.nslots) {
+      atomicOr(s.status, R3D_STATUS_PAGE_RANGE);
+      continue;
+    }
+    c.ok = true;
+    c.maxv = (float)(e >> 24) / 255.0f;
+    c.slot = slot;
+    c.bl = make_float3(lv[0] - (float)(bc[0] << 7), lv[1] - (float)(bc[1] << 7),
+                       lv[2] - (float)(bc[2] << 7));
+    c.grad_vox = r3d_exp2f(lod) * inv;
+    c.world_brick = (128.0f * (float)b.scale[li]) / b.md;
+    scale_out = b.scale[li];
+    inv_out = inv;
+    bco[0] = bc[0];
+    bco[1] = bc[1];
+    bco[2] = bc[2];
+    break;
+  }
+  lc.valid = c.ok;
+  lc.desired = desired;
+  lc.scale = scale_out;
+  lc.inv_scale = inv_out;
+  lc.bc[0] = bco[0];
+  lc.bc[1] = bco[1];
+  lc.bc[2] = bco[2];
+  lc.c = c;
+  return c;
+}
+
+// bricks_lod_locate_cached, raycast.slang:255-279
+__device__ __forceinline__ BrickCtx lod_locate_cached(const DevScene &s, float3 p, float lod,
+                                                      LodCache &lc, bool &walked) {
+  const DevBricks &b = s.br;
+  int desired = (int)clamp_(floorf(lod), 0.0f, (float)(b.nlev - 1u));
+  if (lc.valid && lc.desired == desired) {
+    float lv[3];
+    uint32_t bc[3];
+    float pv[3] = {p.x, p.y, p.z};
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      float base_v = clamp_(pv[a] * b.md, 0.0f, fmaxf(b.bs[a] - 0.001f, 0.0f));
+      lv[a] = base_v * lc.inv_scale;
+      bc[a] = (uint32_t)lv[a] >> 7;
+    }
+    if (bc[0] == lc.bc[0] && bc[1] == lc.bc[1] && bc[2] == lc.bc[2]) {
+      BrickCtx c = lc.c;
+      c.bl = make_float3(lv[0] - (float)(bc[0] << 7), lv[1] - (float)(bc[1] << 7),
+                         lv[2] - (float)(bc[2] << 7));
+      return c;
+    }
+  }
+  walked = true;
+  return lod_locate_ex(s, p, lod, lc, desired);
+}
+
+// bricks_fetch at atlas lod 0 (raycast.slang:284-288): clamp to
+// [0.5, 127.5] inside the brick, no cross-brick filtering
+__device__ __forceinline__ float brick_fetch(const DevScene &s, uint32_t slot, float3 bl) {
+  const uint8_t *g = s.br.pool + (size_t)slot * (128u * 128u * 128u);
+  float lx = clamp_(bl.x, 0.5f, 127.5f), ly = clamp_(bl.y, 0.5f, 127.5f),
+        lz = clamp_(bl.z, 0.5f, 127.5f);
+  return tri_slot(g, lx - 0.5f, ly - 0.5f, lz - 0.5f);
+}
+
+// TF lookup (raycast.slang:894) from raw 0..255 RGBA values in shared memory
+__device__ __forceinline__ float4 tf_sample(const float4 *tf, float t) {
+  uint32_t i0 = (uint32_t)t;
+  uint32_t i1 = min(i0 + 1u, 255u);
+  float f = t - (float)i0;
+  float4 a = tf[i0], b = tf[i1];
+  return make_float4(lerp_(a.x, b.x, f) * kInv255, lerp_(a.y, b.y, f) * kInv255,
+                     lerp_(a.z, b.z, f) * kInv255, lerp_(a.w, b.w, f) * kInv255);
+}
+
+// One ray: raycast.slang main() for dispatch thread (px, py) (half mode
+// already applied), returning the final colour, steps and MIP index.
+template <int PATH, int MODE, bool FAST, bool COUNT = false>
+__device__ __forceinline__ void march(const r3d_frame_params &pc, const DevScene &s,
+                                      const float4 *tf, uint32_t px, uint32_t py,
+                                      RayResult &out) {
+  constexpr bool kLod = PATH == PATH_LOD_BRICKS;
+  constexpr bool kComposite = MODE == R3D_MODE_FULL || MODE == R3D_MODE_FLAT;
+  constexpr bool kShaded = MODE == R3D_MODE_FULL;
+  const bool ortho = (pc.view_flags & R3D_VIEW_ORTHO) != 0u;
+  out.steps = 0;
+  out.mip_index = 0;
+  out.n_tf = out.n_grad = out.n_walk = 0;
+  uint32_t n_tf = 0, n_grad = 0, n_walk = 0;
+
+  // pix_ndc / ray_dir / ray_origin (raycast.slang:469-486)
+  float ux = ((float)px + 0.5f) / (float)pc.viewport[0];
+  float uy = ((float)py + 0.5f) / (float)pc.viewport[1];
+  float nx = ux * 2.0f - 1.0f, ny = 1.0f - uy * 2.0f;
+  float3 fwd = make_float3(pc.cam_forward[0], pc.cam_forward[1], pc.cam_forward[2]);
+  float3 rt = make_float3(pc.cam_right[0], pc.cam_right[1], pc.cam_right[2]);
+  float3 up = make_float3(pc.cam_up[0], pc.cam_up[1], pc.cam_up[2]);
+  float3 dir;
+  if (ortho)
+    dir = norm3(fwd);
+  else
+    dir = norm3(make_float3(fmaf(ny, up.x, fmaf(nx, rt.x, fwd.x)),
+                            fmaf(ny, up.y, fmaf(nx, rt.y, fwd.y)),
+                            fmaf(ny, up.z, fmaf(nx, rt.z, fwd.z))));
+  if (MODE == R3D_MODE_RAYDIR) {
+    out.rgb[0] = fmaf(dir.x, 0.5f, 0.5f);
+    out.rgb[1] = fmaf(dir.y, 0.5f, 0.5f);
+    out.rgb[2] = fmaf(dir.z, 0.5f, 0.5f);
+    return;
+  }
+  float3 org = make_float3(pc.cam_origin[0], pc.cam_origin[1], pc.cam_origin[2]);
+  if (ortho)
+    org = make_float3(fmaf(ny, up.x, fmaf(nx, rt.x, org.x)), fmaf(ny, up.y, fmaf(nx, rt.y, org.y)),
+                      fmaf(ny, up.z, fmaf(nx, rt.z, org.z)));
+
+  // voxel pitch, LOD ceiling and extent (raycast.slang:647-683, 305-314)
+  float voxel, vox_inv, max_lod;
+  float3 ext = make_float3(1.0f, 1.0f, 1.0f);
+  if (kLod) {
+    voxel = 1.0f / s.br.md;
+    vox_inv = s.br.md;
+    max_lod = (float)(s.br.nlev - 1u);
+    ext = make_float3(s.br.bs[0] / s.br.md, s.br.bs[1] / s.br.md, s.br.bs[2] / s.br.md);
+  } else {
+    voxel = 1.0f / (float)s.cube.maxdim;
+    vox_inv = (float)s.cube.maxdim;
+    max_lod = fminf(pc.max_mip, (float)(s.cube.nlevels - 1u));
+  }
+  // model transform (common.slang:45-52)
+  float3 c = make_float3(ext.x * 0.5f, ext.y * 0.5f, ext.z * 0.5f);
+  float3 r0 = make_float3(pc.vol_r0[0], pc.vol_r0[1], pc.vol_r0[2]);
+  float3 r1 = make_float3(pc.vol_r1[0], pc.vol_r1[1], pc.vol_r1[2]);
+  float3 r2 = make_float3(pc.vol_r2[0], pc.vol_r2[1], pc.vol_r2[2]);
+  float3 q = make_float3((org.x - pc.vol_tx) - c.x, (org.y - pc.vol_ty) - c.y,
+                         (org.z - pc.vol_tz) - c.z);
+  float3 ro = make_float3(fmaf(r2.x, q.z, fmaf(r1.x, q.y, r0.x * q.x)) + c.x,
+                          fmaf(r2.y, q.z, fmaf(r1.y, q.y, r0.y * q.x)) + c.y,
+                          fmaf(r2.z, q.z, fmaf(r1.z, q.y, r0.z * q.x)) + c.z);
+  dir = make_float3(fmaf(r2.x, dir.z, fmaf(r1.x, dir.y, r0.x * dir.x)),
+                    fmaf(r2.y, dir.z, fmaf(r1.y, dir.y, r0.y * dir.x)),
+                    fmaf(r2.z, dir.z, fmaf(r1.z, dir.y, r0.z * dir.x)));
+
+  // clip boxes and t range (raycast.slang:686-714)
+  float lo[3] = {0.0f, 0.0f, 0.0f}, hi[3] = {ext.x, ext.y, ext.z};
+  float t_lo = 0.0f, t_hi = 1e30f;
+  if (kLod) {
+    float md = s.br.md;
+    if ((pc.view_flags & R3D_VIEW_CROP) != 0u) {
+      float clo[3] = {pc.slab_x0 / md, pc.slab_y0 / md, pc.slab_z0 / md};
+      float cx[3] = {pc.slab_px / md, pc.slab_py / md, pc.slab_nx / md};
+#pragma unroll
+      for (int a = 0; a < 3; a++) {
+        lo[a] = clamp_(clo[a], 0.0f, hi[a]);
+        hi[a] = clamp_(clo[a] + cx[a], lo[a], hi[a]);
+      }
+    } else if (pc.slab_depth > 0u) {
+      if ((pc.view_flags & R3D_VIEW_OBLIQUE) != 0u) {
+        t_lo = pc.slab_z0 / md;
+        t_hi = (pc.slab_z0 + (float)pc.slab_depth) / md;
+      } else {
+        uint32_t axc = (pc.view_flags >> 8) & 3u;
+        int a = axc == 1u ? 0 : (axc == 2u ? 1 : 2);
+        float e = a == 0 ? hi[0] : (a == 1 ? hi[1] : hi[2]);
+        float nlo = clamp_(pc.slab_z0 / md, 0.0f, e);
+        float nhi = clamp_((pc.slab_z0 + (float)pc.slab_depth) / md, nlo, e);
+        if (a == 0) { lo[0] = nlo; hi[0] = nhi; }
+        if (a == 1) { lo[1] = nlo; hi[1] = nhi; }
+        if (a == 2) { lo[2] = nlo; hi[2] = nhi; }
+      }
+    }
+  }
+  // box_hit (raycast.slang:489-495)
+  float dv[3] = {dir.x, dir.y, dir.z}, ov[3] = {ro.x, ro.y, ro.z};
+  float tmn[3], tmx[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    float inv = 1.0f / dv[a];
+    float t0 = (lo[a] - ov[a]) * inv, t1 = (hi[a] - ov[a]) * inv;
+    tmn[a] = fminf(t0, t1);
+    tmx[a] = fmaxf(t0, t1);
+  }
+  float tn = fmaxf(fmaxf(fmaxf(tmn[0], tmn[1]), tmn[2]), t_lo);
+  float tf_ = fminf(fminf(fminf(tmx[0], tmx[1]), tmx[2]), t_hi);
+  if (tn >= tf_) {
+    out.rgb[0] = 0.02f;
+    out.rgb[1] = 0.02f;
+    out.rgb[2] = 0.03f;
+    return;
+  }
+
+  // cone, step, jitter, budget, gates (raycast.slang:722-762)
+  const float cone = (2.0f * sqrtf(dot3(up, up))) / (float)pc.viewport[1];
+  const float dt = pc.step_voxels * voxel;
+  float t = fmaf(hash12(px, py, pc.frame_index), dt, tn);
+  float mip_max = 0.0f, first_hit = -1.0f;
+  float acc_r = 0.0f, acc_g = 0.0f, acc_b = 0.0f, acc_a = 0.0f;
+  uint32_t steps = 0, mip_index = 0;
+  const uint32_t ray_budget = kLod ? (kShaded ? 192u : 256u) : kMaxSteps;
+  const float span_step = fmaxf((tf_ - tn) / ((float)ray_budget * dt), 1.0f);
+  const float bs = 8.0f * voxel;
+  const float occ_gate = fmaxf(pc.skip_gate, 0.5f / 255.0f);
+  const float bgate = fmaxf(occ_gate, 4.5f / 255.0f);
+  const float opac_k = pc.density * pc.step_voxels;
+  const float3 key = norm3(make_float3(0.4f, 0.8f, -0.4f));
+  const float3 l = make_float3(-dir.x, -dir.y, -dir.z);
+  const float3 hv = norm3(make_float3(l.x - dir.x, l.y - dir.y, l.z - dir.z));
+  // with a zero LOD ceiling the clamp pins lod to 0 whatever log2 returns
+  const bool lod_on = max_lod != 0.0f;
+
+  LodCache lc;
+  lc.valid = false;
+  lc.desired = -1;
+  lc.scale = 1u;
+  lc.inv_scale = 1.0f;
+  lc.bc[0] = lc.bc[1] = lc.bc[2] = 0u;
+  BrickCtx b;
+  b.ok = false;
+  b.maxv = 0.0f;
+  b.slot = 0;
+  b.grad_vox = 1.0f;
+  b.world_brick = 128.0f * voxel;
+  b.bl = make_float3(0.0f, 0.0f, 0.0f);
+
+  while (t < tf_ && steps < ray_budget) {
+    steps++;
+    // LOD and step (raycast.slang:772-779)
+    float lod = 0.0f;
+    if (lod_on) {
+      float foot = ortho ? cone : t * cone;
+      lod = clamp_(r3d_log2f(fmaxf(foot * vox_inv, 1.0f)) + pc.lod_bias, 0.0f, max_lod);
+    }
+    float lod_step = fmaxf(lod == 0.0f ? 1.0f : r3d_exp2f(lod), span_step);
+    float3 p = make_float3(fmaf(t, dir.x, ro.x), fmaf(t, dir.y, ro.y), fmaf(t, dir.z, ro.z));
+
+    float v;
+    if (kLod) {
+      bool walked = false;
+      b = lod_locate_cached(s, p, lod, lc, walked);
+      if (COUNT) n_walk += walked ? 1u : 0u;
+      v = b.ok ? brick_fetch(s, b.slot, b.bl) : 0.0f;
+    } else {
+      v = cube_sample(s.cube, p, lod);
+    }
+    bool cut = v < pc.threshold;  // raycast.slang:826-827
+    if (cut) v = 0.0f;
+
+    // empty-space skip (raycast.slang:829-869)
+    bool void_blk = false;
+    float bsz = bs;
+    if (kLod) {
+      if (MODE == R3D_MODE_MIP && b.ok && b.maxv <= mip_max) {
+        void_blk = true;
+        bsz = b.world_brick;
+      } else if (v < bgate && b.maxv < bgate) {
+        void_blk = true;
+        bsz = b.world_brick;
+      }
+    } else if (v < occ_gate && occ_sample(s.cube, p) < occ_gate) {
+      void_blk = true;
+    }
+    if (void_blk) {
+      float pv[3] = {p.x, p.y, p.z};
+      float tex[3];
+#pragma unroll
+      for (int a = 0; a < 3; a++) {
+        float nextp = (floorf(pv[a] / bsz) + (dv[a] > 0.0f ? 1.0f : 0.0f)) * bsz;
+        tex[a] = fabsf(dv[a]) > 1e-8f ? (nextp - ov[a]) / dv[a] : 1e30f;
+      }
+      t = fmaxf(fminf(fminf(tex[0], tex[1]), tex[2]), t) + bsz * 0.01f;
+      continue;
+    }
+
+    if (v > mip_max) {
+      mip_max = v;
+      mip_index = steps;
+    }
+    if (MODE == R3D_MODE_MIP && mip_max >= 0.999f) break;
+    if (MODE == R3D_MODE_DEPTH && first_hit < 0.0f && v > 0.05f) first_hit = t;
+
+    if (kComposite && !cut) {
+      float tt = clamp_(fmaf(v, 256.0f, -0.5f), 0.0f, 255.0f);
+      // below tf_zero_t both TF texels have alpha 0, so the opacity is
+      // exactly 0 and the sample cannot contribute
+      if (tt >= s.tf_zero_t) {
+        if (COUNT) n_tf++;
+        float4 sm = tf_sample(tf, tt);
+        float a = 1.0f - r3d_powf(1.0f - sm.w, opac_k * lod_step);
+        if (a > 0.003f) {
+          float col_r = sm.x, col_g = sm.y, col_b = sm.z;
+          if (kShaded) {
+            if (COUNT) n_grad++;
+            float g0, g1, g2;
+            if (FAST) {  // raycast.slang:919-955
+              const float ir3 = 0.57735026919f, renorm = 0.86602540378f;
+              float q0, q1, q2, q3;
+              if (kLod) {
+                float ev = b.grad_vox * ir3;
+                float3 u = b.bl;
+                q0 = brick_fetch(s, b.slot, make_float3(u.x + ev, u.y - ev, u.z - ev));
+                q1 = brick_fetch(s, b.slot, make_float3(u.x - ev, u.y - ev, u.z + ev));
+                q2 = brick_fetch(s, b.slot, make_float3(u.x - ev, u.y + ev, u.z - ev));
+                q3 = brick_fetch(s, b.slot, make_float3(u.x + ev, u.y + ev, u.z + ev));
+              } else {
+                float ee = (voxel * lod_step) * ir3;
+                q0 = cube_sample(s.cube, make_float3(p.x + ee, p.y - ee, p.z - ee), lod);
+                q1 = cube_sample(s.cube, make_float3(p.x - ee, p.y - ee, p.z + ee), lod);
+                q2 = cube_sample(s.cube, make_float3(p.x - ee, p.y + ee, p.z - ee), lod);
+                q3 = cube_sample(s.cube, make_float3(p.x + ee, p.y + ee, p.z + ee), lod);
+              }
+              g0 = (((q0 - q1) - q2) + q3) * renorm;
+              g1 = (((-q0 - q1) + q2) + q3) * renorm;
+              g2 = (((-q0 + q1) - q2) + q3) * renorm;
+            } else {  // raycast.slang:957-986
+              if (kLod) {
+                float ev = b.grad_vox;
+                float3 u = b.bl;
+                g0 = brick_fetch(s, b.slot, make_float3(u.x + ev, u.y, u.z)) -
+                     brick_fetch(s, b.slot, make_float3(u.x - ev, u.y, u.z));
+                g1 = brick_fetch(s, b.slot, make_float3(u.x, u.y + ev, u.z)) -
+                     brick_fetch(s, b.slot, make_float3(u.x, u.y - ev, u.z));
+                g2 = brick_fetch(s, b.slot, make_float3(u.x, u.y, u.z + ev)) -
+                     brick_fetch(s, b.slot, make_float3(u.x, u.y, u.z - ev));
+              } else {
+                float e = voxel * lod_step;
+                g0 = cube_sample(s.cube, make_float3(p.x + e, p.y, p.z), lod) -
+                     cube_sample(s.cube, make_float3(p.x - e, p.y, p.z), lod);
+                g1 = cube_sample(s.cube, make_float3(p.x, p.y + e, p.z), lod) -
+                     cube_sample(s.cube, make_float3(p.x, p.y - e, p.z), lod);
+                g2 = cube_sample(s.cube, make_float3(p.x, p.y, p.z + e), lod) -
+                     cube_sample(s.cube, make_float3(p.x, p.y, p.z - e), lod);
+              }
+            }
+            float3 gv = make_float3(g0, g1, g2);
+            float gm = sqrtf(dot3(gv, gv));
+            if (gm > 1e-4f) {  // raycast.slang:988-998
+              float inv = 1.0f / gm;
+              float3 n = make_float3(gv.x * inv, gv.y * inv, gv.z * inv);
+              float diff = fmaf(0.3f, fabsf(dot3(n, key)), 0.7f * fabsf(dot3(n, l)));
+              float spec = r3d_powi24f(fabsf(dot3(n, hv))) * 0.3f;
+              float lit = fmaf(0.75f, diff, 0.25f);
+              float w = sat_(gm * 6.0f);
+              float lm = fmaf(w, lit - 1.0f, 1.0f);
+              float sw = spec * w;
+              col_r = fmaf(col_r, lm, sw);
+              col_g = fmaf(col_g, lm, sw);
+              col_b = fmaf(col_b, lm, sw);
+            }
+          }
+          // front-to-back compositing (raycast.slang:1015-1017)
+          float wgt = (1.0f - acc_a) * a;
+          acc_r = fmaf(wgt, col_r, acc_r);
+          acc_g = fmaf(wgt, col_g, acc_g);
+          acc_b = fmaf(wgt, col_b, acc_b);
+          acc_a = acc_a + wgt;
+          if (acc_a >= s.alpha_cutoff) break;
+        }
+      }
+    }
+    t = fmaf(dt, lod_step, t);  // raycast.slang:1020
+  }
+
+  // finalize (raycast.slang:1023-1038)
+  out.steps = steps;
+  out.mip_index = mip_index;
+  out.n_tf = n_tf;
+  out.n_grad = n_grad;
+  out.n_walk = n_walk;
+  if (MODE == R3D_MODE_HEATMAP) {
+    float x = (float)steps / 1024.0f;
+    out.rgb[0] = x;
+    out.rgb[1] = 1.0f - fabsf(x - 0.5f) * 2.0f;
+    out.rgb[2] = 1.0f - x;
+  } else if (MODE == R3D_MODE_DEPTH) {
+    float d = first_hit < 0.0f ? 0.0f : 1.0f - sat_(first_hit * 0.5f);
+    out.rgb[0] = out.rgb[1] = out.rgb[2] = d;
+  } else if (kComposite) {
+    float tr = 1.0f - acc_a;
+    out.rgb[0] = fmaf(tr, 0.02f, acc_r);
+    out.rgb[1] = fmaf(tr, 0.02f, acc_g);
+    out.rgb[2] = fmaf(tr, 0.03f, acc_b);
+  } else {
+    float m = mip_max * pc.density;
+    out.rgb[0] = out.rgb[1] = out.rgb[2] = m;
+  }
+}
+
+}  // namespace r3d
