@@ -30,13 +30,13 @@ def test_fmath_bits_match_cpu(ctx):
     x = x.astype(np.float32)
     y = rng.uniform(0.01, 20, x.size).astype(np.float32)
     dev = ctx.fmath_eval(x, y)
-    import ctypes as C
-    from oracle import HERE
-    # the CPU build of the same header, through a tiny helper in liboracle
     import oracle
-    cpu = oracle.fmath_eval(x, y)
-    assert np.array_equal(dev.view(np.uint32), cpu.view(np.uint32)), \
-        f"{np.sum(dev.view(np.uint32) != cpu.view(np.uint32))} mismatching results"
+    cpu = oracle.fmath_eval(x, y)  # the CPU build of the same header
+    # NaN payloads differ between CUDA and glibc; every other result is
+    # compared bit for bit
+    both_nan = np.isnan(dev) & np.isnan(cpu)
+    diff = (dev.view(np.uint32) != cpu.view(np.uint32)) & ~both_nan
+    assert not diff.any(), f"{diff.sum()} mismatching results, e.g. x={x[diff.any(1)][:4]}"
 
 
 @pytest.fixture(scope="module")
