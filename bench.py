@@ -60,8 +60,9 @@ class ClockSampler:
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device: int):
+    def __init__(self, device: int, period_ms: int = 50):
         self.device = device
+        self.period_ms = period_ms
         self.proc = None
         self.lines: list[str] = []
         self.t = None
@@ -70,10 +71,11 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", str(self.period_ms)],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            time.sleep(1.0)  # nvidia-smi's own start-up; sampling runs before the region
         except Exception:
             self.proc = None
         return self
@@ -229,16 +231,16 @@ def run_ours(args) -> None:
     torch.cuda.synchronize()
     counts = cnt.cpu().numpy().astype(np.float64)
 
-    for i in range(Wm):
-        frame(i)
-    torch.cuda.synchronize()  # the frames run on the context's own stream
-    total.zero_()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # clocks are sampled across the warm-up and the timed frames
     with ClockSampler(local) as clk:
+        for i in range(Wm):
+            frame(i)
+        torch.cuda.synchronize()  # the frames run on the context's own stream
+        total.zero_()
         torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
         e0.record(stream)
         for i in range(Wm, Wm + K):
             frame(i)
@@ -323,6 +325,26 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
 
 
+def run_profile(args) -> None:
+    """Renders args.profile frames of the workload with no timing: the
+    command line that ncu captures."""
+    import torch
+    import render3d_b200 as rb
+    lut = rb.scroll_ramp_tf()
+    vol = rb.phantom(args.profile_size, seed=SEED)
+    ctx = rb.Context(0)
+    ctx.set_transfer(lut)
+    ctx.set_alpha_cutoff(CUTOFF)
+    ctx.bricks_build(vol, NLEV)
+    img = torch.zeros((H, W, 4), dtype=torch.uint8, device="cuda")
+    for i in range(args.profile):
+        ctx.raycast(orbit_params(rb, lut, i, ctx.brick_mode, args.profile_mode), W, H, out=img,
+                    stream=ctx.stream)
+    torch.cuda.synchronize()
+    print("profile frames done:", args.profile)
+    ctx.close()
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -332,7 +354,14 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=400)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", type=int, default=0, metavar="N",
+                    help="only build the workload and render N orbit frames (for ncu)")
+    ap.add_argument("--profile-mode", type=int, default=0)
+    ap.add_argument("--profile-size", type=int, default=N_EDGE)
     args = ap.parse_args()
+    if args.profile:
+        run_profile(args)
+        return
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -30,7 +30,8 @@ CLI = os.path.join(HERE, "r3d_headless")
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = GENCODE + [
+# R3D_NVCC_EXTRA: extra nvcc flags (tuning experiments)
+NVCC_FLAGS = GENCODE + os.environ.get("R3D_NVCC_EXTRA", "").split() + [
     "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
     "-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false",
     "-Xptxas", "-v", "-I" + INC, "-I" + CSRC,

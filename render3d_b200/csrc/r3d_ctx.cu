@@ -156,6 +156,24 @@ __global__ void k_brick_copy(const uint8_t *__restrict__ lev, uint32_t ex, uint3
   }
 }
 
+// Per-slot table of dilated 8^3 block maxima: entry (bz, by, bx) of slot s
+// is the max over voxels [8b, min(8b+8, 127)] on each axis.  One block per
+// slot, one thread per table entry.
+__global__ void k_slot_blockmax(const uint8_t *__restrict__ pool, uint8_t *__restrict__ out) {
+  const uint8_t *g = pool + (size_t)blockIdx.x * (128u * 128u * 128u);
+  for (uint32_t e = threadIdx.x; e < 4096u; e += blockDim.x) {
+    uint32_t bx = e & 15u, by = (e >> 4) & 15u, bz = e >> 8;
+    uint32_t m = 0;
+    for (uint32_t z = bz * 8u; z <= min(bz * 8u + 8u, 127u); z++)
+      for (uint32_t y = by * 8u; y <= min(by * 8u + 8u, 127u); y++) {
+        const uint8_t *row = g + ((size_t)z << 14) + ((size_t)y << 7);
+        for (uint32_t x = bx * 8u; x <= min(bx * 8u + 8u, 127u); x++)
+          m = max(m, (uint32_t)row[x]);
+      }
+    out[(size_t)blockIdx.x * 4096u + e] = (uint8_t)m;
+  }
+}
+
 static unsigned grid_for(size_t n) {
   size_t b = (n + 255) / 256;
   return (unsigned)(b < 148u * 64u ? (b ? b : 1) : 148u * 64u);
@@ -219,6 +237,7 @@ void r3d_cuda_destroy(r3d_cuda_ctx *c) {
   cudaFree(c->cube_buf);
   cudaFree(c->page);
   cudaFree(c->pool);
+  cudaFree(c->bmax);
   cudaFree(c->lut);
   cudaFree(c->status);
   cudaFree(c->img);
@@ -368,6 +387,22 @@ static int decode_header(r3d_cuda_ctx *c, const uint32_t *page, uint32_t words, 
   }
   b.page_words = words;
   b.nslots = nslots;
+  return R3D_OK;
+}
+
+// (Re)builds the block-maximum table of the context's slot pool.
+static int build_blockmax(r3d_cuda_ctx *c) {
+  cudaFree(c->bmax);
+  c->bmax = nullptr;
+  size_t n = (size_t)(c->nslots ? c->nslots : 1u) * 4096u;
+  R3D_CUDA_TRY(c, cudaMalloc(&c->bmax, n));
+  R3D_CUDA_TRY(c, cudaMemsetAsync(c->bmax, 0, n, c->stream));
+  if (c->nslots) {
+    k_slot_blockmax<<<c->nslots, 256, 0, c->stream>>>(c->pool, c->bmax);
+    R3D_CUDA_TRY(c, cudaGetLastError());
+  }
+  R3D_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  c->br.bmax = c->bmax;
   return R3D_OK;
 }
 
@@ -539,8 +574,11 @@ int r3d_cuda_bricks_build(r3d_cuda_ctx *c, const r3d_volume_desc *d, const uint8
     c->shape[0] = nx;
     c->shape[1] = ny;
     c->shape[2] = nz;
-    c->have_bricks = true;
     c->br = b;
+    c->have_bricks = false;
+    rc = build_blockmax(c);
+    if (rc != R3D_OK) goto out;
+    c->have_bricks = true;
   }
 out:
   cudaFree(lev);
@@ -585,8 +623,11 @@ int r3d_cuda_bricks_load(r3d_cuda_ctx *c, const uint32_t *page, uint32_t page_wo
   c->shape[0] = page[1];
   c->shape[1] = page[2];
   c->shape[2] = page[3];
-  c->have_bricks = true;
   c->br = b;
+  c->have_bricks = false;
+  rc = build_blockmax(c);
+  if (rc != R3D_OK) return rc;
+  c->have_bricks = true;
   return R3D_OK;
 }
 

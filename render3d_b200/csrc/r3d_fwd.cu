@@ -6,10 +6,15 @@
 // src/shaders/raycast.slang:127-130).
 #include "r3d_internal.h"
 
+// Minimum resident 128-thread blocks per SM the register allocator targets.
+#ifndef R3D_FWD_MIN_BLOCKS
+#define R3D_FWD_MIN_BLOCKS 1
+#endif
+
 namespace r3d {
 
 template <int PATH, int MODE, bool FAST, bool COUNT>
-__global__ void __launch_bounds__(128) k_raycast(const __grid_constant__ r3d_frame_params pc,
+__global__ void __launch_bounds__(128, R3D_FWD_MIN_BLOCKS) k_raycast(const __grid_constant__ r3d_frame_params pc,
                                                  const __grid_constant__ DevScene s,
                                                  const uchar4 *__restrict__ lut,
                                                  uchar4 *__restrict__ img, uint32_t out_w,

@@ -40,6 +40,10 @@ struct DevBricks {
   const uint32_t *page;
   uint32_t page_words;
   const uint8_t *pool;  // slot s at pool + s * 128^3, x fastest
+  // per slot, 16^3 entries: max of voxels [8b, 8b+8] per axis (clamped to
+  // the slot), an upper bound of any trilinear sample whose base texel lies
+  // in block b
+  const uint8_t *bmax;
   uint32_t nslots;
   uint32_t nlev;
   float bs[3];  // base shape
@@ -283,6 +287,40 @@ __device__ __forceinline__ BrickCtx lod_locate_cached(const DevScene &s, float3 
   return lod_locate_ex(s, p, lod, lc, desired);
 }
 
+// Slot-local texel coordinates of bricks_fetch (clamped, minus 0.5) and
+// their base texel.
+struct SlotCoord {
+  float tx, ty, tz;
+  uint32_t x0, y0, z0;
+};
+
+__device__ __forceinline__ SlotCoord slot_coord(float3 bl) {
+  SlotCoord q;
+  q.tx = clamp_(bl.x, 0.5f, 127.5f) - 0.5f;
+  q.ty = clamp_(bl.y, 0.5f, 127.5f) - 0.5f;
+  q.tz = clamp_(bl.z, 0.5f, 127.5f) - 0.5f;
+  q.x0 = (uint32_t)q.tx;
+  q.y0 = (uint32_t)q.ty;
+  q.z0 = (uint32_t)q.tz;
+  return q;
+}
+
+__device__ __forceinline__ float tri_slot_at(const uint8_t *__restrict__ g, const SlotCoord &q) {
+  float fx = q.tx - (float)q.x0, fy = q.ty - (float)q.y0, fz = q.tz - (float)q.z0;
+  uint32_t dx1 = q.x0 < 127u ? 1u : 0u;
+  uint32_t dy1 = q.y0 < 127u ? 128u : 0u;
+  uint32_t dz1 = q.z0 < 127u ? 16384u : 0u;
+  const uint8_t *r00 = g + ((q.z0 << 14) | (q.y0 << 7) | q.x0);
+  float a0 = __ldg(r00), a1 = __ldg(r00 + dx1);
+  float b0 = __ldg(r00 + dy1), b1 = __ldg(r00 + dy1 + dx1);
+  float c0 = __ldg(r00 + dz1), c1 = __ldg(r00 + dz1 + dx1);
+  float d0 = __ldg(r00 + dz1 + dy1), d1 = __ldg(r00 + dz1 + dy1 + dx1);
+  float c00 = lerp_(a0, a1, fx), c10 = lerp_(b0, b1, fx);
+  float c01 = lerp_(c0, c1, fx), c11 = lerp_(d0, d1, fx);
+  float e0 = lerp_(c00, c10, fy), e1 = lerp_(c01, c11, fy);
+  return lerp_(e0, e1, fz) * kInv255;
+}
+
 // bricks_fetch at atlas lod 0 (raycast.slang:284-288): clamp to
 // [0.5, 127.5] inside the brick, no cross-brick filtering
 __device__ __forceinline__ float brick_fetch(const DevScene &s, uint32_t slot, float3 bl) {
@@ -461,12 +499,51 @@ __device__ __forceinline__ void march(const r3d_frame_params &pc, const DevScene
     float lod_step = fmaxf(lod == 0.0f ? 1.0f : r3d_exp2f(lod), span_step);
     float3 p = make_float3(fmaf(t, dir.x, ro.x), fmaf(t, dir.y, ro.y), fmaf(t, dir.z, ro.z));
 
-    float v;
+    float v = 0.0f;
     if (kLod) {
       bool walked = false;
       b = lod_locate_cached(s, p, lod, lc, walked);
       if (COUNT) n_walk += walked ? 1u : 0u;
-      v = b.ok ? brick_fetch(s, b.slot, b.bl) : 0.0f;
+      if (b.ok) {
+        // Exact fetch elision: vub bounds the trilinear value from above
+        // (every tap lies in the dilated block and rounding is monotone).
+        // When vub already fixes every decision the sample feeds, the
+        // outcome equals the fetched one and the 8 loads are skipped.
+        const SlotCoord q = slot_coord(b.bl);
+        const uint32_t m = __ldg(s.br.bmax + (size_t)b.slot * 4096u +
+                                 (((q.z0 >> 3) << 8) | ((q.y0 >> 3) << 4) | (q.x0 >> 3)));
+        const float vub = (float)m * kInv255;
+        const bool cut_known = vub < pc.threshold;
+        const bool void_known = b.maxv >= bgate || vub < bgate || cut_known;
+        bool elide;
+        if (MODE == R3D_MODE_MIP)
+          elide = b.maxv <= mip_max || (void_known && (cut_known || vub <= mip_max));
+        else if (MODE == R3D_MODE_DEPTH)
+          elide = void_known && (cut_known || first_hit >= 0.0f || vub <= 0.05f);
+        else if (MODE == R3D_MODE_HEATMAP)
+          elide = void_known;
+        else
+          elide = void_known &&
+                  (cut_known || clamp_(fmaf(vub, 256.0f, -0.5f), 0.0f, 255.0f) < s.tf_zero_t);
+        if (elide) {
+          // the sample changes nothing but the march position
+          if ((MODE == R3D_MODE_MIP && b.maxv <= mip_max) || b.maxv < bgate) {
+            const float bsz = b.world_brick;
+            float pv[3] = {p.x, p.y, p.z};
+            float tex[3];
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+              float nextp = (floorf(pv[a] / bsz) + (dv[a] > 0.0f ? 1.0f : 0.0f)) * bsz;
+              tex[a] = fabsf(dv[a]) > 1e-8f ? (nextp - ov[a]) / dv[a] : 1e30f;
+            }
+            t = fmaxf(fminf(fminf(tex[0], tex[1]), tex[2]), t) + bsz * 0.01f;
+          } else {
+            t = fmaf(dt, lod_step, t);
+          }
+          continue;
+        }
+        v = tri_slot_at(s.br.pool + (size_t)b.slot * (128u * 128u * 128u), q);
+      }
     } else {
       v = cube_sample(s.cube, p, lod);
     }
