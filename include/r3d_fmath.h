@@ -6,7 +6,7 @@
  * so the CPU restatement and the sm_100a kernels must produce the same bits
  * for them.  Library transcendentals differ between glibc and CUDA; these do
  * not, because they use only IEEE-754 correctly rounded operations (+ - * /,
- * fmaf, rintf, exponent bit manipulation), evaluated in a fixed order.
+ * fmaf, exponent bit manipulation), evaluated in a fixed order.
  * Callers must compile without floating-point contraction
  * (gcc -ffp-contract=off, nvcc -fmad=false); every fused multiply-add
  * below is an explicit fmaf.
@@ -16,7 +16,8 @@
  *          ln m = 2 atanh(s), s = (m - 1) / (m + 1), |s| <= 0.1716, using the
  *          odd series 2 (s + s^3/3 + s^5/5 + s^7/7 + s^9/9) (Abramowitz &
  *          Stegun 4.1.28); truncation error < 3e-9 relative.
- *  - exp2: x = n + f with n = rint(x), |f| <= 1/2; 2^f = e^(f ln 2) by its
+ *  - exp2: x = n + f with n = rint(x) (round-half-even, by the 1.5*2^23
+ *          shift), |f| <= 1/2; 2^f = e^(f ln 2) by its
  *          Taylor series to degree 7 (truncation < 8e-9 relative); 2^n is
  *          applied by building the exponent field (two factors so that
  *          subnormal results round once).
@@ -93,7 +94,10 @@ R3D_FM_HD float r3d_exp2f(float x) {
   if (x != x) return x;
   if (x >= 128.0f) return R3D_FM_INF;
   if (x < -151.0f) return 0.0f;
-  float n = rintf(x);
+  /* n = rint(x): adding 1.5 * 2^23 rounds to the nearest even integer,
+   * which then sits in the low mantissa bits of big */
+  float big = x + 12582912.0f;
+  float n = big - 12582912.0f;
   float f = x - n; /* exact, |f| <= 0.5 */
   float p = fmaf(f, 1.52527338e-05f, 1.54035304e-04f);
   p = fmaf(f, p, 1.33335581e-03f);
@@ -102,7 +106,7 @@ R3D_FM_HD float r3d_exp2f(float x) {
   p = fmaf(f, p, 2.40226507e-01f);
   p = fmaf(f, p, 6.93147181e-01f);
   p = fmaf(f, p, 1.0f);
-  int ni = (int)n;
+  int ni = (int)(r3d_f2u(big) - 0x4B400000u);
   if (ni >= -126 && ni <= 127) return p * r3d_u2f((uint32_t)(ni + 127) << 23);
   /* split the scale so a subnormal result is rounded exactly once */
   int n1 = ni / 2, n2 = ni - n1;

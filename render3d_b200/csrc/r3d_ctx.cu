@@ -370,6 +370,7 @@ static int decode_header(r3d_cuda_ctx *c, const uint32_t *page, uint32_t words, 
   b.nlev = nlev;
   for (int a = 0; a < 3; a++) b.bs[a] = (float)page[1 + a];
   b.md = fmaxf(b.bs[0], fmaxf(b.bs[1], b.bs[2]));
+  for (int a = 0; a < 3; a++) b.bs_hi[a] = fmaxf(b.bs[a] - 0.001f, 0.0f);
   for (uint32_t l = 0; l < nlev; l++) {
     uint32_t off = page[4 + 4 * l], packed = page[5 + 4 * l], scale = page[6 + 4 * l];
     uint32_t bd[3] = {packed & 1023u, (packed >> 10) & 1023u, packed >> 20};

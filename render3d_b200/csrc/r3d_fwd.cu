@@ -1,20 +1,35 @@
-// Forward raycast kernels: one thread per ray, 128-thread blocks covering
-// 16x8 dispatch threads as four 8x4 warp tiles whose lanes follow a Morton
-// (Z-order) curve, so a warp's rays stay spatially compact and share cache
-// lines.  Mode, sampling path and gradient quality are template parameters
+// Forward raycast kernels: one thread per ray; each warp covers an 8x4 tile
+// of dispatch threads whose lanes follow a Morton (Z-order) curve, so a
+// warp's rays stay spatially compact and share cache lines; a block holds
+// 1, 2 or 4 warp tiles.  Mode, sampling path and gradient quality are template parameters
 // (the reference specializes its shader per path for the same reason:
 // src/shaders/raycast.slang:127-130).
 #include "r3d_internal.h"
 
-// Minimum resident 128-thread blocks per SM the register allocator targets.
+// Minimum resident 128-thread blocks per SM the register allocator targets
+// (0: no target).
 #ifndef R3D_FWD_MIN_BLOCKS
-#define R3D_FWD_MIN_BLOCKS 1
+#define R3D_FWD_MIN_BLOCKS 0
+#endif
+// Warps per block: 1, 2 or 4 8x4 warp tiles.
+#ifndef R3D_FWD_WARPS
+#define R3D_FWD_WARPS 4
+#endif
+#if R3D_FWD_MIN_BLOCKS > 0
+#define R3D_FWD_BOUNDS __launch_bounds__(R3D_FWD_WARPS * 32, R3D_FWD_MIN_BLOCKS)
+#else
+#define R3D_FWD_BOUNDS __launch_bounds__(R3D_FWD_WARPS * 32)
 #endif
 
 namespace r3d {
 
+constexpr uint32_t kFwdWarps = R3D_FWD_WARPS;
+constexpr uint32_t kBlockW = kFwdWarps >= 2 ? 16u : 8u;  // dispatch threads per block, x
+constexpr uint32_t kBlockH = kFwdWarps == 4 ? 8u : 4u;   // and y
+static_assert(kFwdWarps == 1 || kFwdWarps == 2 || kFwdWarps == 4, "1, 2 or 4 warps");
+
 template <int PATH, int MODE, bool FAST, bool COUNT>
-__global__ void __launch_bounds__(128, R3D_FWD_MIN_BLOCKS) k_raycast(const __grid_constant__ r3d_frame_params pc,
+__global__ void R3D_FWD_BOUNDS k_raycast(const __grid_constant__ r3d_frame_params pc,
                                                  const __grid_constant__ DevScene s,
                                                  const uchar4 *__restrict__ lut,
                                                  uchar4 *__restrict__ img, uint32_t out_w,
@@ -31,8 +46,8 @@ __global__ void __launch_bounds__(128, R3D_FWD_MIN_BLOCKS) k_raycast(const __gri
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   const uint32_t lx = (lane & 1u) | ((lane >> 1) & 2u) | ((lane >> 2) & 4u);
   const uint32_t ly = ((lane >> 1) & 1u) | ((lane >> 2) & 2u);
-  const uint32_t tx = blockIdx.x * 16u + (warp & 1u) * 8u + lx;
-  const uint32_t ty = blockIdx.y * 8u + (warp >> 1) * 4u + ly;
+  const uint32_t tx = blockIdx.x * kBlockW + (warp & 1u) * 8u + lx;
+  const uint32_t ty = blockIdx.y * kBlockH + (warp >> 1) * 4u + ly;
   const bool half = (pc.view_flags & R3D_VIEW_HALF) != 0u;
   const uint32_t px = half ? tx * 2u : tx, py = half ? ty * 2u : ty;
   const uint32_t vw = pc.viewport[0], vh = pc.viewport[1];
@@ -81,13 +96,14 @@ static cudaError_t launch_t(const r3d_frame_params &pc, const DevScene &s, const
   const bool half = (pc.view_flags & R3D_VIEW_HALF) != 0u;
   uint32_t gw = half ? (pc.viewport[0] + 1u) / 2u : pc.viewport[0];
   uint32_t gh = half ? (pc.viewport[1] + 1u) / 2u : pc.viewport[1];
-  dim3 grid((gw + 15u) / 16u, (gh + 7u) / 8u);
+  dim3 grid((gw + kBlockW - 1u) / kBlockW, (gh + kBlockH - 1u) / kBlockH);
+  const uint32_t threads = kFwdWarps * 32u;
   if (counters)
-    k_raycast<PATH, MODE, FAST, true><<<grid, 128, 0, stream>>>(pc, s, lut, (uchar4 *)img, out_w,
-                                                                steps, mip, total, counters);
+    k_raycast<PATH, MODE, FAST, true><<<grid, threads, 0, stream>>>(
+        pc, s, lut, (uchar4 *)img, out_w, steps, mip, total, counters);
   else
-    k_raycast<PATH, MODE, FAST, false><<<grid, 128, 0, stream>>>(pc, s, lut, (uchar4 *)img, out_w,
-                                                                 steps, mip, total, nullptr);
+    k_raycast<PATH, MODE, FAST, false><<<grid, threads, 0, stream>>>(
+        pc, s, lut, (uchar4 *)img, out_w, steps, mip, total, nullptr);
   return cudaGetLastError();
 }
 

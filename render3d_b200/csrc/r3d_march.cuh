@@ -46,8 +46,9 @@ struct DevBricks {
   const uint8_t *bmax;
   uint32_t nslots;
   uint32_t nlev;
-  float bs[3];  // base shape
-  float md;     // max(base shape)
+  float bs[3];     // base shape
+  float bs_hi[3];  // max(bs - 0.001, 0): upper clamp of base-level coordinates
+  float md;        // max(base shape)
   uint32_t off[kMaxLevels];
   uint32_t bd[kMaxLevels][3];
   uint32_t scale[kMaxLevels];
@@ -188,6 +189,7 @@ struct LodCache {  // raycast.slang:190-196
   uint32_t scale;
   float inv_scale;
   uint32_t bc[3];
+  float lo[3];  // 128 * bc: (uint)lv >> 7 == bc  <=>  lo <= lv < lo + 128
   BrickCtx c;
 };
 
@@ -210,9 +212,8 @@ __device__ __forceinline__ BrickCtx lod_locate_ex(const DevScene &s, float3 p, f
   c.slot = 0;
   c.grad_vox = 1.0f;
   c.world_brick = (128.0f * (float)(1u << (b.nlev - 1u))) / b.md;
-  float base_v[3] = {clamp_(p.x * b.md, 0.0f, fmaxf(b.bs[0] - 0.001f, 0.0f)),
-                     clamp_(p.y * b.md, 0.0f, fmaxf(b.bs[1] - 0.001f, 0.0f)),
-                     clamp_(p.z * b.md, 0.0f, fmaxf(b.bs[2] - 0.001f, 0.0f))};
+  float base_v[3] = {clamp_(p.x * b.md, 0.0f, b.bs_hi[0]), clamp_(p.y * b.md, 0.0f, b.bs_hi[1]),
+                     clamp_(p.z * b.md, 0.0f, b.bs_hi[2])};
   int last = (int)b.nlev - 1;
   uint32_t scale_out = 1u;
   float inv_out = 1.0f;
@@ -257,6 +258,9 @@ __device__ __forceinline__ BrickCtx lod_locate_ex(const DevScene &s, float3 p, f
   lc.bc[0] = bco[0];
   lc.bc[1] = bco[1];
   lc.bc[2] = bco[2];
+  lc.lo[0] = (float)(bco[0] << 7);
+  lc.lo[1] = (float)(bco[1] << 7);
+  lc.lo[2] = (float)(bco[2] << 7);
   lc.c = c;
   return c;
 }
@@ -268,18 +272,18 @@ __device__ __forceinline__ BrickCtx lod_locate_cached(const DevScene &s, float3 
   int desired = (int)clamp_(floorf(lod), 0.0f, (float)(b.nlev - 1u));
   if (lc.valid && lc.desired == desired) {
     float lv[3];
-    uint32_t bc[3];
+    bool same = true;
     float pv[3] = {p.x, p.y, p.z};
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-      float base_v = clamp_(pv[a] * b.md, 0.0f, fmaxf(b.bs[a] - 0.001f, 0.0f));
+      float base_v = clamp_(pv[a] * b.md, 0.0f, b.bs_hi[a]);
       lv[a] = base_v * lc.inv_scale;
-      bc[a] = (uint32_t)lv[a] >> 7;
+      // lv >= 0, so floor(lv) >> 7 == bc exactly when lo <= lv < lo + 128
+      same = same && lv[a] >= lc.lo[a] && lv[a] < lc.lo[a] + 128.0f;
     }
-    if (bc[0] == lc.bc[0] && bc[1] == lc.bc[1] && bc[2] == lc.bc[2]) {
+    if (same) {
       BrickCtx c = lc.c;
-      c.bl = make_float3(lv[0] - (float)(bc[0] << 7), lv[1] - (float)(bc[1] << 7),
-                         lv[2] - (float)(bc[2] << 7));
+      c.bl = make_float3(lv[0] - lc.lo[0], lv[1] - lc.lo[1], lv[2] - lc.lo[2]);
       return c;
     }
   }
@@ -290,23 +294,29 @@ __device__ __forceinline__ BrickCtx lod_locate_cached(const DevScene &s, float3 
 // Slot-local texel coordinates of bricks_fetch (clamped, minus 0.5) and
 // their base texel.
 struct SlotCoord {
-  float tx, ty, tz;
+  float fx, fy, fz;  // fractions
   uint32_t x0, y0, z0;
 };
 
+// floor of t in [0, 2^23) as an integer and its fraction, without the
+// conversion unit: adding 2^23 with truncation leaves floor(t) in the
+// mantissa.  Equal to (uint32_t)t and t - (float)(uint32_t)t.
+__device__ __forceinline__ uint32_t floor_frac(float t, float &frac) {
+  float r = __fadd_rz(t, 8388608.0f);
+  frac = t - (r - 8388608.0f);
+  return __float_as_uint(r) & 0x7fffffu;
+}
+
 __device__ __forceinline__ SlotCoord slot_coord(float3 bl) {
   SlotCoord q;
-  q.tx = clamp_(bl.x, 0.5f, 127.5f) - 0.5f;
-  q.ty = clamp_(bl.y, 0.5f, 127.5f) - 0.5f;
-  q.tz = clamp_(bl.z, 0.5f, 127.5f) - 0.5f;
-  q.x0 = (uint32_t)q.tx;
-  q.y0 = (uint32_t)q.ty;
-  q.z0 = (uint32_t)q.tz;
+  q.x0 = floor_frac(clamp_(bl.x, 0.5f, 127.5f) - 0.5f, q.fx);
+  q.y0 = floor_frac(clamp_(bl.y, 0.5f, 127.5f) - 0.5f, q.fy);
+  q.z0 = floor_frac(clamp_(bl.z, 0.5f, 127.5f) - 0.5f, q.fz);
   return q;
 }
 
 __device__ __forceinline__ float tri_slot_at(const uint8_t *__restrict__ g, const SlotCoord &q) {
-  float fx = q.tx - (float)q.x0, fy = q.ty - (float)q.y0, fz = q.tz - (float)q.z0;
+  const float fx = q.fx, fy = q.fy, fz = q.fz;
   uint32_t dx1 = q.x0 < 127u ? 1u : 0u;
   uint32_t dy1 = q.y0 < 127u ? 128u : 0u;
   uint32_t dz1 = q.z0 < 127u ? 16384u : 0u;
