@@ -114,6 +114,19 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def reduce_replicas(dist, samples: float, ms: float, device) -> tuple[float, float]:
+    """Whole-job totals of independent replicas: samples summed over ranks and
+    the device time of the slowest rank."""
+    import torch
+    if dist is None:
+        return samples, ms
+    s = torch.tensor([samples], dtype=torch.float64, device=device)
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(s, op=dist.ReduceOp.SUM)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(s.item()), float(t.item())
+
+
 def orbit_params(rb, lut, i: int, brick_mode: int, mode: int = 0):
     p = rb.orbit_view((i % ORBIT_FRAMES) / ORBIT_FRAMES, W, H, lut, step_voxels=STEP_VOXELS,
                       mode=mode, frame_index=i)
@@ -251,13 +264,8 @@ def run_ours(args) -> None:
     if abs(samples - counts[0]) > 0.5:
         print(f"warning: counting pass {counts[0]:.0f} samples, timed pass {samples:.0f}",
               file=sys.stderr)
-    t = torch.tensor([ms], device=f"cuda:{local}")
-    s_all = torch.tensor([samples], device=f"cuda:{local}", dtype=torch.float64)
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(s_all, op=dist.ReduceOp.SUM)
-    ms_max = float(t.item())
-    value = float(s_all.item()) / (ms_max * 1e-3) / 1e9
+    samples_all, ms_max = reduce_replicas(dist, samples, ms, torch.device(f"cuda:{local}"))
+    value = samples_all / (ms_max * 1e-3) / 1e9
     fps = K * world / (ms_max * 1e-3)
 
     # end to end through the render3d-facing API: r3d_frame + r3d_read_frame
@@ -283,7 +291,7 @@ def run_ours(args) -> None:
     te = torch.tensor([e2e_s], device=f"cuda:{local}")
     if dist:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = float(s_all.item()) / float(te.item()) / 1e9
+    e2e_value = samples_all / float(te.item()) / 1e9
     r.close()
 
     peak, peak_kind = measured_peaks()

@@ -128,6 +128,24 @@ int r3d_cuda_raycast_fwd(r3d_cuda_ctx *ctx, const r3d_frame_params *views, uint3
                          uint8_t *rgba_out, uint32_t out_w, uint32_t out_h,
                          const r3d_cuda_aux *aux, void *stream);
 
+/* How forward launches are scheduled.  persistent = 0: one thread per ray
+ * (one grid per view).  persistent = 1: resident warps drain a queue of
+ * 32-ray tiles covering all views of the call, refilling lanes whose rays
+ * have ended whenever at least refill_min lanes are idle; tile_shape 0/1/2
+ * = 8x4 / 16x2 / 32x1 rays; unroll = march steps between refill checks
+ * (1 or 2); blocks_per_sm = resident 128-thread blocks per SM (0: the
+ * occupancy limit).  Results are identical under every schedule. */
+typedef struct r3d_cuda_schedule {
+  uint32_t persistent;
+  uint32_t refill_min;
+  uint32_t tile_shape;
+  uint32_t unroll;
+  uint32_t blocks_per_sm;
+} r3d_cuda_schedule;
+
+int r3d_cuda_set_schedule(r3d_cuda_ctx *ctx, const r3d_cuda_schedule *sched);
+int r3d_cuda_get_schedule(const r3d_cuda_ctx *ctx, r3d_cuda_schedule *sched);
+
 /* CUDA-event time of the last r3d_cuda_raycast_fwd's kernels in ns
  * (synchronizes the events). */
 int r3d_cuda_last_kernel_ns(r3d_cuda_ctx *ctx, uint64_t *ns);

@@ -73,6 +73,13 @@ class CudaAux(C.Structure):
                 ("total_steps", C.c_void_p), ("counters", C.c_void_p)]
 
 
+class Schedule(C.Structure):
+    """r3d_cuda_schedule: forward launch scheduling (results never change)."""
+    _fields_ = [("persistent", C.c_uint32), ("refill_min", C.c_uint32),
+                ("tile_shape", C.c_uint32), ("unroll", C.c_uint32),
+                ("blocks_per_sm", C.c_uint32)]
+
+
 class PhantomDesc(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("pitch", C.c_float), ("radius", C.c_float),
                 ("r0", C.c_float), ("sheet_half", C.c_float), ("in_mean", C.c_float),
@@ -123,6 +130,8 @@ def _load() -> C.CDLL:
         "r3d_cuda_raycast_fwd": (I, [P, P, U32, P, U32, U32, C.POINTER(CudaAux), P]),
         "r3d_cuda_last_kernel_ns": (I, [P, C.POINTER(C.c_uint64)]),
         "r3d_cuda_fmath_eval": (I, [P, P, P, P, U32]),
+        "r3d_cuda_set_schedule": (I, [P, C.POINTER(Schedule)]),
+        "r3d_cuda_get_schedule": (I, [P, C.POINTER(Schedule)]),
         "r3d_create": (I, [P, C.POINTER(RenderConfig), C.POINTER(P)]),
         "r3d_destroy": (None, [P]),
         "r3d_upload_volume": (I, [P, C.POINTER(VolumeDesc), P]),
@@ -391,6 +400,16 @@ class Context:
         out = np.empty((x.size, 4), np.float32)
         self._check(lib.r3d_cuda_fmath_eval(self.h, _ptr(x), _ptr(y), _ptr(out), x.size))
         return out
+
+    def set_schedule(self, persistent: int = 0, refill_min: int = 16, tile_shape: int = 0,
+                     unroll: int = 1, blocks_per_sm: int = 0) -> None:
+        self._check(lib.r3d_cuda_set_schedule(
+            self.h, C.byref(Schedule(persistent, refill_min, tile_shape, unroll, blocks_per_sm))))
+
+    def schedule(self) -> dict:
+        sc = Schedule()
+        self._check(lib.r3d_cuda_get_schedule(self.h, C.byref(sc)))
+        return {f: getattr(sc, f) for f, _ in Schedule._fields_}
 
     def last_kernel_ns(self) -> int:
         ns = C.c_uint64()

@@ -212,12 +212,23 @@ int r3d_cuda_create(int device, r3d_cuda_ctx **out) {
       cudaMalloc(&c->status, sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&c->lut, 256 * sizeof(uchar4)) != cudaSuccess ||
       cudaMalloc(&c->total, (R3D_COUNTERS + 1) * sizeof(unsigned long long)) != cudaSuccess ||
-      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+      cudaMallocHost(&c->ring_host, sizeof(DevView) * kMaxBatchViews * r3d_cuda_ctx::kRing) !=
+          cudaSuccess ||
+      cudaMalloc(&c->ring_dev, sizeof(DevView) * kMaxBatchViews * r3d_cuda_ctx::kRing) !=
+          cudaSuccess ||
+      cudaMalloc(&c->ring_queue, sizeof(uint32_t) * kMaxBatchViews * r3d_cuda_ctx::kRing) !=
+          cudaSuccess) {
     cudaGetLastError();
     r3d_cuda_destroy(c);
     return R3D_E_CUDA;
   }
   cudaMemset(c->status, 0, sizeof(uint32_t));
+  for (int k = 0; k < r3d_cuda_ctx::kRing; k++)
+    if (cudaEventCreateWithFlags(&c->ring_ev[k], cudaEventDisableTiming) != cudaSuccess) {
+      r3d_cuda_destroy(c);
+      return R3D_E_CUDA;
+    }
   // default transfer function: grey ramp with alpha = value
   // (src/vk/vkbackend.c:1100-1114)
   uint8_t ramp[256][4];
@@ -245,6 +256,11 @@ void r3d_cuda_destroy(r3d_cuda_ctx *c) {
   cudaFree(c->total);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
+  for (int k = 0; k < r3d_cuda_ctx::kRing; k++)
+    if (c->ring_ev[k]) cudaEventDestroy(c->ring_ev[k]);
+  cudaFreeHost(c->ring_host);
+  cudaFree(c->ring_dev);
+  cudaFree(c->ring_queue);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -721,7 +737,106 @@ static int prepare_view(r3d_cuda_ctx *c, const r3d_frame_params &in, uint32_t ou
   return ok ? 1 : 0;
 }
 
+// Persistent launches for the renderable views of one call: views sharing a
+// sampling path and mode go into one launch (template parameters of the
+// kernel), in order of first appearance.
+static int launch_views_persistent(r3d_cuda_ctx *c, const r3d_frame_params *pcs,
+                                   const int *render, uint32_t nviews, uint8_t *img,
+                                   uint32_t out_w, uint32_t *steps, uint32_t *mip,
+                                   unsigned long long *total, unsigned long long *counters,
+                                   cudaStream_t st) {
+  const int k = c->ring_next;
+  c->ring_next = (k + 1) % r3d_cuda_ctx::kRing;
+  if (c->ring_used[k]) R3D_CUDA_TRY(c, cudaEventSynchronize(c->ring_ev[k]));
+  DevView *hv = c->ring_host + (size_t)k * kMaxBatchViews;
+  DevView *dv = c->ring_dev + (size_t)k * kMaxBatchViews;
+  uint32_t *queue = c->ring_queue + (size_t)k * kMaxBatchViews;
+  const r3d_cuda_schedule &sc = c->sched;
+  // group views by (path, mode)
+  uint32_t order[64], group_of[64], ngroups = 0, gkey[64], gstart[65], gcount[64];
+  uint32_t n = 0;
+  for (uint32_t v = 0; v < nviews; v++) {
+    if (!render[v]) continue;
+    uint32_t key = (pcs[v].brick_mode ? 8u : 0u) | pcs[v].mode;
+    uint32_t g = 0;
+    while (g < ngroups && gkey[g] != key) g++;
+    if (g == ngroups) {
+      gkey[ngroups] = key;
+      gcount[ngroups] = 0;
+      ngroups++;
+    }
+    group_of[n] = g;
+    order[n++] = v;
+    gcount[g]++;
+  }
+  if (!n) return R3D_OK;
+  gstart[0] = 0;
+  for (uint32_t g = 0; g < ngroups; g++) gstart[g + 1] = gstart[g] + gcount[g];
+  uint32_t fill[64] = {0}, ntiles[64] = {0};
+  for (uint32_t i = 0; i < n; i++) {
+    uint32_t g = group_of[i], slot = gstart[g] + fill[g]++;
+    DevView &d = hv[slot];
+    memset(&d, 0, sizeof d);
+    d.pc = pcs[order[i]];
+    d.img = (uchar4 *)img;
+    d.stride = out_w;
+    d.tile_begin = ntiles[g];
+    ntiles[g] += view_tiles(d, sc.tile_shape);
+  }
+  R3D_CUDA_TRY(c, cudaMemcpyAsync(dv, hv, sizeof(DevView) * n, cudaMemcpyHostToDevice, st));
+  R3D_CUDA_TRY(c, cudaEventRecord(c->ring_ev[k], st));
+  c->ring_used[k] = true;
+  R3D_CUDA_TRY(c, cudaMemsetAsync(queue, 0, sizeof(uint32_t) * ngroups, st));
+  int dev_sms = 148;
+  cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device);
+  const DevScene s = c->scene();
+  for (uint32_t g = 0; g < ngroups; g++) {
+    PersistLaunch L;
+    memset(&L, 0, sizeof L);
+    L.views = dv + gstart[g];
+    L.nviews = gcount[g];
+    L.ntiles = ntiles[g];
+    L.lut = c->lut;
+    L.queue = queue + g;
+    L.refill_min = sc.refill_min;
+    L.shape = sc.tile_shape;
+    L.unroll = sc.unroll;
+    L.steps = steps;
+    L.mip = mip;
+    L.total = total;
+    L.counters = counters;
+    L.mode = gkey[g] & 7u;
+    L.fast = c->quality == R3D_QUALITY_FAST;
+    L.lod_bricks = (gkey[g] & 8u) != 0u;
+    int per_sm = sc.blocks_per_sm
+                     ? (int)sc.blocks_per_sm
+                     : persist_blocks_per_sm(L.lod_bricks, L.mode, L.fast, L.unroll);
+    // no more blocks than there are tiles for their warps
+    uint32_t want = (uint32_t)per_sm * (uint32_t)dev_sms;
+    uint32_t cap = (L.ntiles + 3u) / 4u;
+    L.blocks = want < cap ? want : (cap ? cap : 1u);
+    cudaError_t e = launch_persist(L, s, st);
+    if (e != cudaSuccess) return cuda_fail(c, e, "raycast_fwd: persistent launch");
+  }
+  return R3D_OK;
+}
+
 extern "C" {
+
+int r3d_cuda_set_schedule(r3d_cuda_ctx *c, const r3d_cuda_schedule *sc) {
+  if (!c || !sc || sc->persistent > 1u || sc->refill_min < 1u || sc->refill_min > 32u ||
+      sc->tile_shape > 2u || (sc->unroll != 1u && sc->unroll != 2u) ||
+      sc->blocks_per_sm > 32u)
+    return fail(c, R3D_E_INVALID, "set_schedule: bad schedule");
+  c->sched = *sc;
+  return R3D_OK;
+}
+
+int r3d_cuda_get_schedule(const r3d_cuda_ctx *c, r3d_cuda_schedule *sc) {
+  if (!c || !sc) return R3D_E_INVALID;
+  *sc = c->sched;
+  return R3D_OK;
+}
 
 int r3d_cuda_raycast_fwd(r3d_cuda_ctx *c, const r3d_frame_params *views, uint32_t nviews,
                          uint8_t *rgba_out, uint32_t out_w, uint32_t out_h,
@@ -777,10 +892,16 @@ int r3d_cuda_raycast_fwd(r3d_cuda_ctx *c, const r3d_frame_params *views, uint32_
     }
   }
   R3D_CUDA_TRY(c, cudaEventRecord(c->ev0, st));
-  for (uint32_t v = 0; v < nviews; v++) {
-    if (!render[v]) continue;
-    cudaError_t e = launch_view(c, pcs[v], img, out_w, steps, mip, total, counters, st);
-    if (e != cudaSuccess) return cuda_fail(c, e, "raycast_fwd: launch");
+  if (c->sched.persistent) {
+    int rc = launch_views_persistent(c, pcs, render, nviews, img, out_w, steps, mip, total,
+                                     counters, st);
+    if (rc != R3D_OK) return rc;
+  } else {
+    for (uint32_t v = 0; v < nviews; v++) {
+      if (!render[v]) continue;
+      cudaError_t e = launch_view(c, pcs[v], img, out_w, steps, mip, total, counters, st);
+      if (e != cudaSuccess) return cuda_fail(c, e, "raycast_fwd: launch");
+    }
   }
   R3D_CUDA_TRY(c, cudaEventRecord(c->ev1, st));
   c->timed = true;

@@ -53,8 +53,9 @@ __global__ void R3D_FWD_BOUNDS k_raycast(const __grid_constant__ r3d_frame_param
   const uint32_t vw = pc.viewport[0], vh = pc.viewport[1];
   uint32_t my_steps = 0, my_tf = 0, my_grad = 0, my_walk = 0;
   if (px < vw && py < vh) {
+    const ViewConst vc = view_const<PATH>(pc, s);
     RayResult r;
-    march<PATH, MODE, FAST, COUNT>(pc, s, tf, px, py, r);
+    march<PATH, MODE, FAST, COUNT>(pc, s, vc, tf, px, py, r);
     my_tf = r.n_tf;
     my_grad = r.n_grad;
     my_walk = r.n_walk;

@@ -7,6 +7,7 @@
 
 #include "r3d_cuda.h"
 #include "r3d_march.cuh"
+#include "r3d_persist.h"
 
 struct r3d_cuda_ctx {
   int device = 0;
@@ -48,6 +49,18 @@ struct r3d_cuda_ctx {
 
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   bool timed = false;
+
+  // forward scheduling and the view-table ring of persistent launches:
+  // slot k holds one call's views (pinned host copy + device copy) and its
+  // tile counters; ring_ev[k] completes once the slot's upload has run
+  r3d_cuda_schedule sched = {0u, 16u, 0u, 1u, 0u};
+  static constexpr int kRing = 4;
+  r3d::DevView *ring_host = nullptr;
+  r3d::DevView *ring_dev = nullptr;
+  uint32_t *ring_queue = nullptr;
+  cudaEvent_t ring_ev[kRing] = {};
+  bool ring_used[kRing] = {};
+  int ring_next = 0;
 
   r3d::DevScene scene() const;
 };

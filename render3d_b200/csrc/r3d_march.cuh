@@ -183,13 +183,12 @@ struct BrickCtx {  // raycast.slang:144-152
   float world_brick;
 };
 
-struct LodCache {  // raycast.slang:190-196
+struct LodCache {  // raycast.slang:190-196 (the cached brick is kept as the
+                   // float origin lo = 128 * bc of its coordinates)
   bool valid;
   int desired;
-  uint32_t scale;
   float inv_scale;
-  uint32_t bc[3];
-  float lo[3];  // 128 * bc: (uint)lv >> 7 == bc  <=>  lo <= lv < lo + 128
+  float lo[3];  // (uint)lv >> 7 == bc  <=>  lo <= lv < lo + 128, for lv >= 0
   BrickCtx c;
 };
 
@@ -215,7 +214,6 @@ __device__ __forceinline__ BrickCtx lod_locate_ex(const DevScene &s, float3 p, f
   float base_v[3] = {clamp_(p.x * b.md, 0.0f, b.bs_hi[0]), clamp_(p.y * b.md, 0.0f, b.bs_hi[1]),
                      clamp_(p.z * b.md, 0.0f, b.bs_hi[2])};
   int last = (int)b.nlev - 1;
-  uint32_t scale_out = 1u;
   float inv_out = 1.0f;
   uint32_t bco[3] = {0u, 0u, 0u};
   for (uint32_t step = 0; step < 4u; step++) {
@@ -244,7 +242,6 @@ __device__ __forceinline__ BrickCtx lod_locate_ex(const DevScene &s, float3 p, f
                        lv[2] - (float)(bc[2] << 7));
     c.grad_vox = r3d_exp2f(lod) * inv;
     c.world_brick = (128.0f * (float)b.scale[li]) / b.md;
-    scale_out = b.scale[li];
     inv_out = inv;
     bco[0] = bc[0];
     bco[1] = bc[1];
@@ -253,11 +250,7 @@ __device__ __forceinline__ BrickCtx lod_locate_ex(const DevScene &s, float3 p, f
   }
   lc.valid = c.ok;
   lc.desired = desired;
-  lc.scale = scale_out;
   lc.inv_scale = inv_out;
-  lc.bc[0] = bco[0];
-  lc.bc[1] = bco[1];
-  lc.bc[2] = bco[2];
   lc.lo[0] = (float)(bco[0] << 7);
   lc.lo[1] = (float)(bco[1] << 7);
   lc.lo[2] = (float)(bco[2] << 7);
@@ -350,20 +343,68 @@ __device__ __forceinline__ float4 tf_sample(const float4 *tf, float t) {
                      lerp_(a.z, b.z, f) * kInv255, lerp_(a.w, b.w, f) * kInv255);
 }
 
-// One ray: raycast.slang main() for dispatch thread (px, py) (half mode
-// already applied), returning the final colour, steps and MIP index.
-template <int PATH, int MODE, bool FAST, bool COUNT = false>
-__device__ __forceinline__ void march(const r3d_frame_params &pc, const DevScene &s,
-                                      const float4 *tf, uint32_t px, uint32_t py,
-                                      RayResult &out) {
+// Per-view constants of the march (raycast.slang:647-683,722-762).
+struct ViewConst {
+  float voxel, vox_inv, max_lod, cone, dt, bs, occ_gate, bgate, opac_k;
+  float lod_bias, threshold, density;
+  float3 ext;
+  bool ortho, lod_on;
+};
+
+template <int PATH>
+__device__ __forceinline__ ViewConst view_const(const r3d_frame_params &pc, const DevScene &s) {
+  ViewConst v;
+  if (PATH == PATH_LOD_BRICKS) {
+    v.voxel = 1.0f / s.br.md;
+    v.vox_inv = s.br.md;
+    v.max_lod = (float)(s.br.nlev - 1u);
+    v.ext = make_float3(s.br.bs[0] / s.br.md, s.br.bs[1] / s.br.md, s.br.bs[2] / s.br.md);
+  } else {
+    v.voxel = 1.0f / (float)s.cube.maxdim;
+    v.vox_inv = (float)s.cube.maxdim;
+    v.max_lod = fminf(pc.max_mip, (float)(s.cube.nlevels - 1u));
+    v.ext = make_float3(1.0f, 1.0f, 1.0f);
+  }
+  const float3 up = make_float3(pc.cam_up[0], pc.cam_up[1], pc.cam_up[2]);
+  v.cone = (2.0f * sqrtf(dot3(up, up))) / (float)pc.viewport[1];
+  v.dt = pc.step_voxels * v.voxel;
+  v.bs = 8.0f * v.voxel;
+  v.occ_gate = fmaxf(pc.skip_gate, 0.5f / 255.0f);
+  v.bgate = fmaxf(v.occ_gate, 4.5f / 255.0f);
+  v.opac_k = pc.density * pc.step_voxels;
+  v.lod_bias = pc.lod_bias;
+  v.threshold = pc.threshold;
+  v.density = pc.density;
+  v.ortho = (pc.view_flags & R3D_VIEW_ORTHO) != 0u;
+  // with a zero LOD ceiling the clamp pins lod to 0 whatever log2 returns
+  v.lod_on = v.max_lod != 0.0f;
+  return v;
+}
+
+// State of one ray between march steps.
+struct RayState {
+  float3 ro, dir;  // volume space
+  float t, tf_, span_step;
+  bool span_dom;  // span_step >= every exp2(lod): lod_step is span_step
+  uint32_t steps, mip_index;
+  float mip_max, first_hit;
+  float acc_r, acc_g, acc_b, acc_a;
+  LodCache lc;
+  uint32_t n_tf, n_grad, n_walk;
+};
+
+// Ray setup of raycast.slang main() (:640-762) for dispatch thread (px, py)
+// (half mode already applied).  Returns false when the ray needs no march:
+// out.rgb then holds its final colour (ray-direction mode or background).
+template <int PATH, int MODE>
+__device__ __forceinline__ bool ray_begin(const r3d_frame_params &pc, const DevScene &s,
+                                          const ViewConst &vc, uint32_t px, uint32_t py,
+                                          RayState &st, RayResult &out) {
   constexpr bool kLod = PATH == PATH_LOD_BRICKS;
-  constexpr bool kComposite = MODE == R3D_MODE_FULL || MODE == R3D_MODE_FLAT;
   constexpr bool kShaded = MODE == R3D_MODE_FULL;
-  const bool ortho = (pc.view_flags & R3D_VIEW_ORTHO) != 0u;
   out.steps = 0;
   out.mip_index = 0;
   out.n_tf = out.n_grad = out.n_walk = 0;
-  uint32_t n_tf = 0, n_grad = 0, n_walk = 0;
 
   // pix_ndc / ray_dir / ray_origin (raycast.slang:469-486)
   float ux = ((float)px + 0.5f) / (float)pc.viewport[0];
@@ -373,7 +414,7 @@ __device__ __forceinline__ void march(const r3d_frame_params &pc, const DevScene
   float3 rt = make_float3(pc.cam_right[0], pc.cam_right[1], pc.cam_right[2]);
   float3 up = make_float3(pc.cam_up[0], pc.cam_up[1], pc.cam_up[2]);
   float3 dir;
-  if (ortho)
+  if (vc.ortho)
     dir = norm3(fwd);
   else
     dir = norm3(make_float3(fmaf(ny, up.x, fmaf(nx, rt.x, fwd.x)),
@@ -383,27 +424,15 @@ __device__ __forceinline__ void march(const r3d_frame_params &pc, const DevScene
     out.rgb[0] = fmaf(dir.x, 0.5f, 0.5f);
     out.rgb[1] = fmaf(dir.y, 0.5f, 0.5f);
     out.rgb[2] = fmaf(dir.z, 0.5f, 0.5f);
-    return;
+    return false;
   }
   float3 org = make_float3(pc.cam_origin[0], pc.cam_origin[1], pc.cam_origin[2]);
-  if (ortho)
+  if (vc.ortho)
     org = make_float3(fmaf(ny, up.x, fmaf(nx, rt.x, org.x)), fmaf(ny, up.y, fmaf(nx, rt.y, org.y)),
                       fmaf(ny, up.z, fmaf(nx, rt.z, org.z)));
 
-  // voxel pitch, LOD ceiling and extent (raycast.slang:647-683, 305-314)
-  float voxel, vox_inv, max_lod;
-  float3 ext = make_float3(1.0f, 1.0f, 1.0f);
-  if (kLod) {
-    voxel = 1.0f / s.br.md;
-    vox_inv = s.br.md;
-    max_lod = (float)(s.br.nlev - 1u);
-    ext = make_float3(s.br.bs[0] / s.br.md, s.br.bs[1] / s.br.md, s.br.bs[2] / s.br.md);
-  } else {
-    voxel = 1.0f / (float)s.cube.maxdim;
-    vox_inv = (float)s.cube.maxdim;
-    max_lod = fminf(pc.max_mip, (float)(s.cube.nlevels - 1u));
-  }
   // model transform (common.slang:45-52)
+  const float3 ext = vc.ext;
   float3 c = make_float3(ext.x * 0.5f, ext.y * 0.5f, ext.z * 0.5f);
   float3 r0 = make_float3(pc.vol_r0[0], pc.vol_r0[1], pc.vol_r0[2]);
   float3 r1 = make_float3(pc.vol_r1[0], pc.vol_r1[1], pc.vol_r1[2]);
@@ -462,242 +491,263 @@ __device__ __forceinline__ void march(const r3d_frame_params &pc, const DevScene
     out.rgb[0] = 0.02f;
     out.rgb[1] = 0.02f;
     out.rgb[2] = 0.03f;
-    return;
+    return false;
   }
 
-  // cone, step, jitter, budget, gates (raycast.slang:722-762)
-  const float cone = (2.0f * sqrtf(dot3(up, up))) / (float)pc.viewport[1];
-  const float dt = pc.step_voxels * voxel;
-  float t = fmaf(hash12(px, py, pc.frame_index), dt, tn);
-  float mip_max = 0.0f, first_hit = -1.0f;
-  float acc_r = 0.0f, acc_g = 0.0f, acc_b = 0.0f, acc_a = 0.0f;
-  uint32_t steps = 0, mip_index = 0;
+  // jitter, budget (raycast.slang:726-744)
   const uint32_t ray_budget = kLod ? (kShaded ? 192u : 256u) : kMaxSteps;
-  const float span_step = fmaxf((tf_ - tn) / ((float)ray_budget * dt), 1.0f);
-  const float bs = 8.0f * voxel;
-  const float occ_gate = fmaxf(pc.skip_gate, 0.5f / 255.0f);
-  const float bgate = fmaxf(occ_gate, 4.5f / 255.0f);
-  const float opac_k = pc.density * pc.step_voxels;
-  const float3 key = norm3(make_float3(0.4f, 0.8f, -0.4f));
-  const float3 l = make_float3(-dir.x, -dir.y, -dir.z);
-  const float3 hv = norm3(make_float3(l.x - dir.x, l.y - dir.y, l.z - dir.z));
-  // with a zero LOD ceiling the clamp pins lod to 0 whatever log2 returns
-  const bool lod_on = max_lod != 0.0f;
+  st.ro = ro;
+  st.dir = dir;
+  st.t = fmaf(hash12(px, py, pc.frame_index), vc.dt, tn);
+  st.tf_ = tf_;
+  st.span_step = fmaxf((tf_ - tn) / ((float)ray_budget * vc.dt), 1.0f);
+  // exp2(lod) <= 2^ceil(max_lod) for every lod the clamp admits (powers of
+  // two are exact and the margin covers the approximation), so beyond this
+  // bound max(exp2(lod), span_step) is span_step without evaluating exp2
+  st.span_dom = st.span_step >= r3d_exp2f(ceilf(vc.max_lod)) * 1.001f;
+  st.steps = 0;
+  st.mip_index = 0;
+  st.mip_max = 0.0f;
+  st.first_hit = -1.0f;
+  st.acc_r = st.acc_g = st.acc_b = st.acc_a = 0.0f;
+  st.lc.valid = false;
+  st.lc.desired = -1;
+  st.lc.inv_scale = 1.0f;
+  st.lc.lo[0] = st.lc.lo[1] = st.lc.lo[2] = 0.0f;
+  st.lc.c.ok = false;
+  st.lc.c.maxv = 0.0f;
+  st.lc.c.slot = 0;
+  st.lc.c.grad_vox = 1.0f;
+  st.lc.c.world_brick = 128.0f * vc.voxel;
+  st.lc.c.bl = make_float3(0.0f, 0.0f, 0.0f);
+  st.n_tf = st.n_grad = st.n_walk = 0;
+  return true;
+}
 
-  LodCache lc;
-  lc.valid = false;
-  lc.desired = -1;
-  lc.scale = 1u;
-  lc.inv_scale = 1.0f;
-  lc.bc[0] = lc.bc[1] = lc.bc[2] = 0u;
+// Block jump of the empty-space skip (raycast.slang:864-868).
+__device__ __forceinline__ float skip_block(const RayState &st, float3 p, float bsz) {
+  float pv[3] = {p.x, p.y, p.z}, dv[3] = {st.dir.x, st.dir.y, st.dir.z},
+        ov[3] = {st.ro.x, st.ro.y, st.ro.z};
+  float tex[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    float nextp = (floorf(pv[a] / bsz) + (dv[a] > 0.0f ? 1.0f : 0.0f)) * bsz;
+    tex[a] = fabsf(dv[a]) > 1e-8f ? (nextp - ov[a]) / dv[a] : 1e30f;
+  }
+  return fmaxf(fminf(fminf(tex[0], tex[1]), tex[2]), st.t) + bsz * 0.01f;
+}
+
+// One iteration of the hot loop (raycast.slang:767-1021).  Returns false
+// when the ray is finished (loop condition failed, saturation or opacity
+// cutoff).
+template <int PATH, int MODE, bool FAST, bool COUNT>
+__device__ __forceinline__ bool ray_step(const DevScene &s, const ViewConst &vc,
+                                         const float4 *tf, RayState &st) {
+  constexpr bool kLod = PATH == PATH_LOD_BRICKS;
+  constexpr bool kComposite = MODE == R3D_MODE_FULL || MODE == R3D_MODE_FLAT;
+  constexpr bool kShaded = MODE == R3D_MODE_FULL;
+  constexpr uint32_t ray_budget = kLod ? (kShaded ? 192u : 256u) : kMaxSteps;
+  if (!(st.t < st.tf_ && st.steps < ray_budget)) return false;
+  st.steps++;
+  const float t = st.t;
+  // LOD and step (raycast.slang:772-779)
+  float lod = 0.0f;
+  if (vc.lod_on) {
+    float foot = vc.ortho ? vc.cone : t * vc.cone;
+    lod = clamp_(r3d_log2f(fmaxf(foot * vc.vox_inv, 1.0f)) + vc.lod_bias, 0.0f, vc.max_lod);
+  }
+  const float lod_step =
+      st.span_dom ? st.span_step : fmaxf(lod == 0.0f ? 1.0f : r3d_exp2f(lod), st.span_step);
+  const float3 dir = st.dir;
+  const float3 p =
+      make_float3(fmaf(t, dir.x, st.ro.x), fmaf(t, dir.y, st.ro.y), fmaf(t, dir.z, st.ro.z));
+
+  float v = 0.0f;
   BrickCtx b;
-  b.ok = false;
-  b.maxv = 0.0f;
-  b.slot = 0;
-  b.grad_vox = 1.0f;
-  b.world_brick = 128.0f * voxel;
-  b.bl = make_float3(0.0f, 0.0f, 0.0f);
-
-  while (t < tf_ && steps < ray_budget) {
-    steps++;
-    // LOD and step (raycast.slang:772-779)
-    float lod = 0.0f;
-    if (lod_on) {
-      float foot = ortho ? cone : t * cone;
-      lod = clamp_(r3d_log2f(fmaxf(foot * vox_inv, 1.0f)) + pc.lod_bias, 0.0f, max_lod);
-    }
-    float lod_step = fmaxf(lod == 0.0f ? 1.0f : r3d_exp2f(lod), span_step);
-    float3 p = make_float3(fmaf(t, dir.x, ro.x), fmaf(t, dir.y, ro.y), fmaf(t, dir.z, ro.z));
-
-    float v = 0.0f;
-    if (kLod) {
-      bool walked = false;
-      b = lod_locate_cached(s, p, lod, lc, walked);
-      if (COUNT) n_walk += walked ? 1u : 0u;
-      if (b.ok) {
-        // Exact fetch elision: vub bounds the trilinear value from above
-        // (every tap lies in the dilated block and rounding is monotone).
-        // When vub already fixes every decision the sample feeds, the
-        // outcome equals the fetched one and the 8 loads are skipped.
-        const SlotCoord q = slot_coord(b.bl);
-        const uint32_t m = __ldg(s.br.bmax + (size_t)b.slot * 4096u +
-                                 (((q.z0 >> 3) << 8) | ((q.y0 >> 3) << 4) | (q.x0 >> 3)));
-        const float vub = (float)m * kInv255;
-        const bool cut_known = vub < pc.threshold;
-        const bool void_known = b.maxv >= bgate || vub < bgate || cut_known;
-        bool elide;
-        if (MODE == R3D_MODE_MIP)
-          elide = b.maxv <= mip_max || (void_known && (cut_known || vub <= mip_max));
-        else if (MODE == R3D_MODE_DEPTH)
-          elide = void_known && (cut_known || first_hit >= 0.0f || vub <= 0.05f);
-        else if (MODE == R3D_MODE_HEATMAP)
-          elide = void_known;
+  if (kLod) {
+    bool walked = false;
+    b = lod_locate_cached(s, p, lod, st.lc, walked);
+    if (COUNT) st.n_walk += walked ? 1u : 0u;
+    if (b.ok) {
+      // Exact fetch elision: vub bounds the trilinear value from above
+      // (every tap lies in the dilated block and rounding is monotone).
+      // When vub already fixes every decision the sample feeds, the outcome
+      // equals the fetched one and the 8 loads are skipped.
+      const SlotCoord q = slot_coord(b.bl);
+      const uint32_t m = __ldg(s.br.bmax + (size_t)b.slot * 4096u +
+                               (((q.z0 >> 3) << 8) | ((q.y0 >> 3) << 4) | (q.x0 >> 3)));
+      const float vub = (float)m * kInv255;
+      const bool cut_known = vub < vc.threshold;
+      const bool void_known = b.maxv >= vc.bgate || vub < vc.bgate || cut_known;
+      bool elide;
+      if (MODE == R3D_MODE_MIP)
+        elide = b.maxv <= st.mip_max || (void_known && (cut_known || vub <= st.mip_max));
+      else if (MODE == R3D_MODE_DEPTH)
+        elide = void_known && (cut_known || st.first_hit >= 0.0f || vub <= 0.05f);
+      else if (MODE == R3D_MODE_HEATMAP)
+        elide = void_known;
+      else
+        elide = void_known &&
+                (cut_known || clamp_(fmaf(vub, 256.0f, -0.5f), 0.0f, 255.0f) < s.tf_zero_t);
+      if (elide) {  // the sample changes nothing but the march position
+        if ((MODE == R3D_MODE_MIP && b.maxv <= st.mip_max) || b.maxv < vc.bgate)
+          st.t = skip_block(st, p, b.world_brick);
         else
-          elide = void_known &&
-                  (cut_known || clamp_(fmaf(vub, 256.0f, -0.5f), 0.0f, 255.0f) < s.tf_zero_t);
-        if (elide) {
-          // the sample changes nothing but the march position
-          if ((MODE == R3D_MODE_MIP && b.maxv <= mip_max) || b.maxv < bgate) {
-            const float bsz = b.world_brick;
-            float pv[3] = {p.x, p.y, p.z};
-            float tex[3];
-#pragma unroll
-            for (int a = 0; a < 3; a++) {
-              float nextp = (floorf(pv[a] / bsz) + (dv[a] > 0.0f ? 1.0f : 0.0f)) * bsz;
-              tex[a] = fabsf(dv[a]) > 1e-8f ? (nextp - ov[a]) / dv[a] : 1e30f;
-            }
-            t = fmaxf(fminf(fminf(tex[0], tex[1]), tex[2]), t) + bsz * 0.01f;
-          } else {
-            t = fmaf(dt, lod_step, t);
-          }
-          continue;
-        }
-        v = tri_slot_at(s.br.pool + (size_t)b.slot * (128u * 128u * 128u), q);
+          st.t = fmaf(vc.dt, lod_step, t);
+        return true;
       }
-    } else {
-      v = cube_sample(s.cube, p, lod);
+      v = tri_slot_at(s.br.pool + (size_t)b.slot * (128u * 128u * 128u), q);
     }
-    bool cut = v < pc.threshold;  // raycast.slang:826-827
-    if (cut) v = 0.0f;
+  } else {
+    v = cube_sample(s.cube, p, lod);
+  }
+  const bool cut = v < vc.threshold;  // raycast.slang:826-827
+  if (cut) v = 0.0f;
 
-    // empty-space skip (raycast.slang:829-869)
-    bool void_blk = false;
-    float bsz = bs;
-    if (kLod) {
-      if (MODE == R3D_MODE_MIP && b.ok && b.maxv <= mip_max) {
-        void_blk = true;
-        bsz = b.world_brick;
-      } else if (v < bgate && b.maxv < bgate) {
-        void_blk = true;
-        bsz = b.world_brick;
-      }
-    } else if (v < occ_gate && occ_sample(s.cube, p) < occ_gate) {
-      void_blk = true;
+  // empty-space skip (raycast.slang:829-869)
+  if (kLod) {
+    if ((MODE == R3D_MODE_MIP && b.ok && b.maxv <= st.mip_max) ||
+        (v < vc.bgate && b.maxv < vc.bgate)) {
+      st.t = skip_block(st, p, b.world_brick);
+      return true;
     }
-    if (void_blk) {
-      float pv[3] = {p.x, p.y, p.z};
-      float tex[3];
-#pragma unroll
-      for (int a = 0; a < 3; a++) {
-        float nextp = (floorf(pv[a] / bsz) + (dv[a] > 0.0f ? 1.0f : 0.0f)) * bsz;
-        tex[a] = fabsf(dv[a]) > 1e-8f ? (nextp - ov[a]) / dv[a] : 1e30f;
-      }
-      t = fmaxf(fminf(fminf(tex[0], tex[1]), tex[2]), t) + bsz * 0.01f;
-      continue;
-    }
-
-    if (v > mip_max) {
-      mip_max = v;
-      mip_index = steps;
-    }
-    if (MODE == R3D_MODE_MIP && mip_max >= 0.999f) break;
-    if (MODE == R3D_MODE_DEPTH && first_hit < 0.0f && v > 0.05f) first_hit = t;
-
-    if (kComposite && !cut) {
-      float tt = clamp_(fmaf(v, 256.0f, -0.5f), 0.0f, 255.0f);
-      // below tf_zero_t both TF texels have alpha 0, so the opacity is
-      // exactly 0 and the sample cannot contribute
-      if (tt >= s.tf_zero_t) {
-        if (COUNT) n_tf++;
-        float4 sm = tf_sample(tf, tt);
-        float a = 1.0f - r3d_powf(1.0f - sm.w, opac_k * lod_step);
-        if (a > 0.003f) {
-          float col_r = sm.x, col_g = sm.y, col_b = sm.z;
-          if (kShaded) {
-            if (COUNT) n_grad++;
-            float g0, g1, g2;
-            if (FAST) {  // raycast.slang:919-955
-              const float ir3 = 0.57735026919f, renorm = 0.86602540378f;
-              float q0, q1, q2, q3;
-              if (kLod) {
-                float ev = b.grad_vox * ir3;
-                float3 u = b.bl;
-                q0 = brick_fetch(s, b.slot, make_float3(u.x + ev, u.y - ev, u.z - ev));
-                q1 = brick_fetch(s, b.slot, make_float3(u.x - ev, u.y - ev, u.z + ev));
-                q2 = brick_fetch(s, b.slot, make_float3(u.x - ev, u.y + ev, u.z - ev));
-                q3 = brick_fetch(s, b.slot, make_float3(u.x + ev, u.y + ev, u.z + ev));
-              } else {
-                float ee = (voxel * lod_step) * ir3;
-                q0 = cube_sample(s.cube, make_float3(p.x + ee, p.y - ee, p.z - ee), lod);
-                q1 = cube_sample(s.cube, make_float3(p.x - ee, p.y - ee, p.z + ee), lod);
-                q2 = cube_sample(s.cube, make_float3(p.x - ee, p.y + ee, p.z - ee), lod);
-                q3 = cube_sample(s.cube, make_float3(p.x + ee, p.y + ee, p.z + ee), lod);
-              }
-              g0 = (((q0 - q1) - q2) + q3) * renorm;
-              g1 = (((-q0 - q1) + q2) + q3) * renorm;
-              g2 = (((-q0 + q1) - q2) + q3) * renorm;
-            } else {  // raycast.slang:957-986
-              if (kLod) {
-                float ev = b.grad_vox;
-                float3 u = b.bl;
-                g0 = brick_fetch(s, b.slot, make_float3(u.x + ev, u.y, u.z)) -
-                     brick_fetch(s, b.slot, make_float3(u.x - ev, u.y, u.z));
-                g1 = brick_fetch(s, b.slot, make_float3(u.x, u.y + ev, u.z)) -
-                     brick_fetch(s, b.slot, make_float3(u.x, u.y - ev, u.z));
-                g2 = brick_fetch(s, b.slot, make_float3(u.x, u.y, u.z + ev)) -
-                     brick_fetch(s, b.slot, make_float3(u.x, u.y, u.z - ev));
-              } else {
-                float e = voxel * lod_step;
-                g0 = cube_sample(s.cube, make_float3(p.x + e, p.y, p.z), lod) -
-                     cube_sample(s.cube, make_float3(p.x - e, p.y, p.z), lod);
-                g1 = cube_sample(s.cube, make_float3(p.x, p.y + e, p.z), lod) -
-                     cube_sample(s.cube, make_float3(p.x, p.y - e, p.z), lod);
-                g2 = cube_sample(s.cube, make_float3(p.x, p.y, p.z + e), lod) -
-                     cube_sample(s.cube, make_float3(p.x, p.y, p.z - e), lod);
-              }
-            }
-            float3 gv = make_float3(g0, g1, g2);
-            float gm = sqrtf(dot3(gv, gv));
-            if (gm > 1e-4f) {  // raycast.slang:988-998
-              float inv = 1.0f / gm;
-              float3 n = make_float3(gv.x * inv, gv.y * inv, gv.z * inv);
-              float diff = fmaf(0.3f, fabsf(dot3(n, key)), 0.7f * fabsf(dot3(n, l)));
-              float spec = r3d_powi24f(fabsf(dot3(n, hv))) * 0.3f;
-              float lit = fmaf(0.75f, diff, 0.25f);
-              float w = sat_(gm * 6.0f);
-              float lm = fmaf(w, lit - 1.0f, 1.0f);
-              float sw = spec * w;
-              col_r = fmaf(col_r, lm, sw);
-              col_g = fmaf(col_g, lm, sw);
-              col_b = fmaf(col_b, lm, sw);
-            }
-          }
-          // front-to-back compositing (raycast.slang:1015-1017)
-          float wgt = (1.0f - acc_a) * a;
-          acc_r = fmaf(wgt, col_r, acc_r);
-          acc_g = fmaf(wgt, col_g, acc_g);
-          acc_b = fmaf(wgt, col_b, acc_b);
-          acc_a = acc_a + wgt;
-          if (acc_a >= s.alpha_cutoff) break;
-        }
-      }
-    }
-    t = fmaf(dt, lod_step, t);  // raycast.slang:1020
+  } else if (v < vc.occ_gate && occ_sample(s.cube, p) < vc.occ_gate) {
+    st.t = skip_block(st, p, vc.bs);
+    return true;
   }
 
-  // finalize (raycast.slang:1023-1038)
-  out.steps = steps;
-  out.mip_index = mip_index;
-  out.n_tf = n_tf;
-  out.n_grad = n_grad;
-  out.n_walk = n_walk;
+  if (v > st.mip_max) {
+    st.mip_max = v;
+    st.mip_index = st.steps;
+  }
+  if (MODE == R3D_MODE_MIP && st.mip_max >= 0.999f) return false;
+  if (MODE == R3D_MODE_DEPTH && st.first_hit < 0.0f && v > 0.05f) st.first_hit = t;
+
+  if (kComposite && !cut) {
+    float tt = clamp_(fmaf(v, 256.0f, -0.5f), 0.0f, 255.0f);
+    // below tf_zero_t both TF texels have alpha 0, so the opacity is
+    // exactly 0 and the sample cannot contribute
+    if (tt >= s.tf_zero_t) {
+      if (COUNT) st.n_tf++;
+      float4 sm = tf_sample(tf, tt);
+      float a = 1.0f - r3d_powf(1.0f - sm.w, vc.opac_k * lod_step);
+      if (a > 0.003f) {
+        float col_r = sm.x, col_g = sm.y, col_b = sm.z;
+        if (kShaded) {
+          if (COUNT) st.n_grad++;
+          float g0, g1, g2;
+          if (FAST) {  // raycast.slang:919-955
+            const float ir3 = 0.57735026919f, renorm = 0.86602540378f;
+            float q0, q1, q2, q3;
+            if (kLod) {
+              float ev = b.grad_vox * ir3;
+              float3 u = b.bl;
+              q0 = brick_fetch(s, b.slot, make_float3(u.x + ev, u.y - ev, u.z - ev));
+              q1 = brick_fetch(s, b.slot, make_float3(u.x - ev, u.y - ev, u.z + ev));
+              q2 = brick_fetch(s, b.slot, make_float3(u.x - ev, u.y + ev, u.z - ev));
+              q3 = brick_fetch(s, b.slot, make_float3(u.x + ev, u.y + ev, u.z + ev));
+            } else {
+              float ee = (vc.voxel * lod_step) * ir3;
+              q0 = cube_sample(s.cube, make_float3(p.x + ee, p.y - ee, p.z - ee), lod);
+              q1 = cube_sample(s.cube, make_float3(p.x - ee, p.y - ee, p.z + ee), lod);
+              q2 = cube_sample(s.cube, make_float3(p.x - ee, p.y + ee, p.z - ee), lod);
+              q3 = cube_sample(s.cube, make_float3(p.x + ee, p.y + ee, p.z + ee), lod);
+            }
+            g0 = (((q0 - q1) - q2) + q3) * renorm;
+            g1 = (((-q0 - q1) + q2) + q3) * renorm;
+            g2 = (((-q0 + q1) - q2) + q3) * renorm;
+          } else {  // raycast.slang:957-986
+            if (kLod) {
+              float ev = b.grad_vox;
+              float3 u = b.bl;
+              g0 = brick_fetch(s, b.slot, make_float3(u.x + ev, u.y, u.z)) -
+                   brick_fetch(s, b.slot, make_float3(u.x - ev, u.y, u.z));
+              g1 = brick_fetch(s, b.slot, make_float3(u.x, u.y + ev, u.z)) -
+                   brick_fetch(s, b.slot, make_float3(u.x, u.y - ev, u.z));
+              g2 = brick_fetch(s, b.slot, make_float3(u.x, u.y, u.z + ev)) -
+                   brick_fetch(s, b.slot, make_float3(u.x, u.y, u.z - ev));
+            } else {
+              float e = vc.voxel * lod_step;
+              g0 = cube_sample(s.cube, make_float3(p.x + e, p.y, p.z), lod) -
+                   cube_sample(s.cube, make_float3(p.x - e, p.y, p.z), lod);
+              g1 = cube_sample(s.cube, make_float3(p.x, p.y + e, p.z), lod) -
+                   cube_sample(s.cube, make_float3(p.x, p.y - e, p.z), lod);
+              g2 = cube_sample(s.cube, make_float3(p.x, p.y, p.z + e), lod) -
+                   cube_sample(s.cube, make_float3(p.x, p.y, p.z - e), lod);
+            }
+          }
+          float3 gv = make_float3(g0, g1, g2);
+          float gm = sqrtf(dot3(gv, gv));
+          if (gm > 1e-4f) {  // raycast.slang:988-998
+            // key light, headlight l = -dir and its half vector normalize(l - dir)
+            const float3 key = norm3(make_float3(0.4f, 0.8f, -0.4f));
+            const float3 l = make_float3(-dir.x, -dir.y, -dir.z);
+            const float3 hv = norm3(make_float3(l.x - dir.x, l.y - dir.y, l.z - dir.z));
+            float inv = 1.0f / gm;
+            float3 n = make_float3(gv.x * inv, gv.y * inv, gv.z * inv);
+            float diff = fmaf(0.3f, fabsf(dot3(n, key)), 0.7f * fabsf(dot3(n, l)));
+            float spec = r3d_powi24f(fabsf(dot3(n, hv))) * 0.3f;
+            float lit = fmaf(0.75f, diff, 0.25f);
+            float w = sat_(gm * 6.0f);
+            float lm = fmaf(w, lit - 1.0f, 1.0f);
+            float sw = spec * w;
+            col_r = fmaf(col_r, lm, sw);
+            col_g = fmaf(col_g, lm, sw);
+            col_b = fmaf(col_b, lm, sw);
+          }
+        }
+        // front-to-back compositing (raycast.slang:1015-1017)
+        float wgt = (1.0f - st.acc_a) * a;
+        st.acc_r = fmaf(wgt, col_r, st.acc_r);
+        st.acc_g = fmaf(wgt, col_g, st.acc_g);
+        st.acc_b = fmaf(wgt, col_b, st.acc_b);
+        st.acc_a = st.acc_a + wgt;
+        if (st.acc_a >= s.alpha_cutoff) return false;
+      }
+    }
+  }
+  st.t = fmaf(vc.dt, lod_step, t);  // raycast.slang:1020
+  return true;
+}
+
+// Final colour of a marched ray (raycast.slang:1023-1038).
+template <int MODE>
+__device__ __forceinline__ void ray_end(const ViewConst &vc, const RayState &st, RayResult &out) {
+  constexpr bool kComposite = MODE == R3D_MODE_FULL || MODE == R3D_MODE_FLAT;
+  out.steps = st.steps;
+  out.mip_index = st.mip_index;
+  out.n_tf = st.n_tf;
+  out.n_grad = st.n_grad;
+  out.n_walk = st.n_walk;
   if (MODE == R3D_MODE_HEATMAP) {
-    float x = (float)steps / 1024.0f;
+    float x = (float)st.steps / 1024.0f;
     out.rgb[0] = x;
     out.rgb[1] = 1.0f - fabsf(x - 0.5f) * 2.0f;
     out.rgb[2] = 1.0f - x;
   } else if (MODE == R3D_MODE_DEPTH) {
-    float d = first_hit < 0.0f ? 0.0f : 1.0f - sat_(first_hit * 0.5f);
+    float d = st.first_hit < 0.0f ? 0.0f : 1.0f - sat_(st.first_hit * 0.5f);
     out.rgb[0] = out.rgb[1] = out.rgb[2] = d;
   } else if (kComposite) {
-    float tr = 1.0f - acc_a;
-    out.rgb[0] = fmaf(tr, 0.02f, acc_r);
-    out.rgb[1] = fmaf(tr, 0.02f, acc_g);
-    out.rgb[2] = fmaf(tr, 0.03f, acc_b);
+    float tr = 1.0f - st.acc_a;
+    out.rgb[0] = fmaf(tr, 0.02f, st.acc_r);
+    out.rgb[1] = fmaf(tr, 0.02f, st.acc_g);
+    out.rgb[2] = fmaf(tr, 0.03f, st.acc_b);
   } else {
-    float m = mip_max * pc.density;
+    float m = st.mip_max * vc.density;
     out.rgb[0] = out.rgb[1] = out.rgb[2] = m;
   }
+}
+
+// One ray start to finish: raycast.slang main() for dispatch thread (px, py).
+template <int PATH, int MODE, bool FAST, bool COUNT = false>
+__device__ __forceinline__ void march(const r3d_frame_params &pc, const DevScene &s,
+                                      const ViewConst &vc, const float4 *tf, uint32_t px,
+                                      uint32_t py, RayResult &out) {
+  RayState st;
+  if (!ray_begin<PATH, MODE>(pc, s, vc, px, py, st, out)) return;
+  while (ray_step<PATH, MODE, FAST, COUNT>(s, vc, tf, st)) {
+  }
+  ray_end<MODE>(vc, st, out);
 }
 
 }  // namespace r3d

@@ -1,0 +1,261 @@
+// Persistent raycast kernel: resident warps drain a queue of ray tiles.
+//
+// A one-thread-per-ray launch leaves lanes idle once their rays end (early
+// termination, background pixels) and SM slots idle while blocks wait for
+// their slowest warp.  Here every warp keeps its lanes busy: when at least
+// `refill_min` lanes are idle, it claims rays from its pending tile and, when
+// that is used up, pulls the next tile from a global counter (one atomic per
+// 32 rays).  Tiles are 32 dispatch threads (8x4, 16x2 or 32x1), ordered in
+// 8x8-tile supertiles, Morton order inside.  A launch may cover many views of
+// different sizes (the batched path): their tiles are numbered consecutively
+// and the per-view march constants sit in shared memory.
+//
+// Per-ray arithmetic is the same ray_begin / ray_step / ray_end as the
+// one-ray-per-thread kernel, so results are bit-identical to it and to the
+// CPU oracle; only the order in which rays are processed changes.
+#include "r3d_internal.h"
+#include "r3d_persist.h"
+
+namespace r3d {
+
+constexpr uint32_t kFull = 0xffffffffu;
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// mask without its lowest n set bits
+__device__ __forceinline__ uint32_t drop_low_bits(uint32_t mask, uint32_t n) {
+  if (n == 0u) return mask;
+  uint32_t p = __fns(mask, 0u, (int)n);
+  return p >= 31u ? 0u : mask & (~0u << (p + 1u));
+}
+
+// dispatch-thread coordinates of ray k (0..31) of tile `tile` of a view
+__host__ __device__ __forceinline__ void tile_ray(const DevView &v, uint32_t tile, uint32_t k,
+                                         uint32_t shape, uint32_t &tx, uint32_t &ty) {
+  const uint32_t tile_w = tile_w_of(shape);
+  const uint32_t tile_h = 32u / tile_w;
+  const uint32_t sup = tile >> 6, local = tile & 63u;
+  const uint32_t lx = (local & 1u) | ((local >> 1) & 2u) | ((local >> 2) & 4u);
+  const uint32_t ly = ((local >> 1) & 1u) | ((local >> 2) & 2u) | ((local >> 3) & 4u);
+  const uint32_t sx = sup % v.sup_x, sy = sup / v.sup_x;
+  const uint32_t tcx = sx * 8u + lx, tcy = sy * 8u + ly;  // tile coordinates
+  // within the tile: Morton order of the 32 rays for 8x4, row-major else
+  uint32_t ix, iy;
+  if (tile_w == 8u) {
+    ix = (k & 1u) | ((k >> 1) & 2u) | ((k >> 2) & 4u);
+    iy = ((k >> 1) & 1u) | ((k >> 2) & 2u);
+  } else {
+    ix = k % tile_w;
+    iy = k / tile_w;
+  }
+  tx = tcx * tile_w + ix;
+  ty = tcy * tile_h + iy;
+}
+
+// mask of the rays of a tile that fall inside the view's dispatch grid
+// (lane k tests ray k)
+__device__ __forceinline__ uint32_t tile_valid(const DevView &v, uint32_t tile, uint32_t shape,
+                                               uint32_t lane) {
+  uint32_t tx, ty;
+  tile_ray(v, tile, lane, shape, tx, ty);
+  return __ballot_sync(0xffffffffu, tx < v.grid_w && ty < v.grid_h);
+}
+
+template <int MODE>
+__device__ __forceinline__ void store_ray(const DevView &v, uint32_t px, uint32_t py,
+                                          const RayResult &r, uint32_t *steps_out,
+                                          uint32_t *mip_out) {
+  const uchar4 col = make_uchar4(unorm8(r.rgb[0]), unorm8(r.rgb[1]), unorm8(r.rgb[2]), 255);
+  const r3d_frame_params &pc = v.pc;
+  const bool half = (pc.view_flags & R3D_VIEW_HALF) != 0u;
+  const uint32_t vw = pc.viewport[0], vh = pc.viewport[1];
+  const uint32_t ox = pc.view_org & 0xffffu, oy = pc.view_org >> 16;
+  const uint32_t n = half ? 4u : 1u;
+  for (uint32_t k = 0; k < n; k++) {
+    uint32_t ax = px + (k & 1u), ay = py + (k >> 1);
+    if (ax >= vw || ay >= vh) continue;
+    size_t i = (size_t)(oy + ay) * v.stride + (ox + ax);
+    v.img[i] = col;
+    if (steps_out) steps_out[i] = r.steps;
+    if (mip_out) mip_out[i] = r.mip_index;
+  }
+}
+
+template <int PATH, int MODE, bool FAST, bool COUNT, int UNROLL>
+__global__ void __launch_bounds__(128) k_raycast_persist(
+    const DevView *__restrict__ views, uint32_t nviews, const __grid_constant__ DevScene s,
+    const uchar4 *__restrict__ lut, uint32_t *__restrict__ queue, uint32_t ntiles,
+    uint32_t refill_min, uint32_t shape, uint32_t *__restrict__ steps_out,
+    uint32_t *__restrict__ mip_out, unsigned long long *__restrict__ total,
+    unsigned long long *__restrict__ counters) {
+  __shared__ float4 tf[256];
+  __shared__ ViewConst vcs[kMaxBatchViews];
+  for (uint32_t i = threadIdx.x; i < 256u; i += blockDim.x) {
+    uchar4 u = lut[i];
+    tf[i] = make_float4((float)u.x, (float)u.y, (float)u.z, (float)u.w);
+  }
+  for (uint32_t i = threadIdx.x; i < nviews; i += blockDim.x)
+    vcs[i] = view_const<PATH>(views[i].pc, s);
+  __syncthreads();
+
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t lt = lanemask_lt();
+  RayState st;
+  bool active = false;
+  uint32_t my_view = 0, my_px = 0, my_py = 0;
+  uint32_t pend_tile = 0, pend_view = 0, avail = 0;  // warp-uniform
+  bool exhausted = false;
+  uint32_t acc_steps = 0, acc_tf = 0, acc_grad = 0, acc_walk = 0;
+
+  while (true) {
+    uint32_t idle = __ballot_sync(kFull, !active);
+    // refill rounds: assign rays to idle lanes until enough are busy
+    while (!exhausted && idle != 0u && (__popc(idle) >= (int)refill_min || idle == kFull)) {
+      if (avail == 0u) {
+        uint32_t t0 = 0;
+        if (lane == 0) t0 = atomicAdd(queue, 1u);
+        t0 = __shfl_sync(kFull, t0, 0);
+        if (t0 >= ntiles) {
+          exhausted = true;
+          break;
+        }
+        // view of global tile t0 (views are few: linear scan)
+        uint32_t vi = 0;
+        while (vi + 1u < nviews && views[vi + 1u].tile_begin <= t0) vi++;
+        pend_view = vi;
+        pend_tile = t0 - views[vi].tile_begin;
+        avail = tile_valid(views[vi], pend_tile, shape, lane);
+        continue;
+      }
+      const uint32_t n = min((uint32_t)__popc(idle), (uint32_t)__popc(avail));
+      const bool mine = ((idle >> lane) & 1u) != 0u;
+      const uint32_t rank = (uint32_t)__popc(idle & lt);
+      if (mine && rank < n) {
+        const uint32_t k = __fns(avail, 0u, (int)rank + 1);
+        const DevView &v = views[pend_view];
+        uint32_t tx, ty;
+        tile_ray(v, pend_tile, k, shape, tx, ty);
+        const bool half = (v.pc.view_flags & R3D_VIEW_HALF) != 0u;
+        const uint32_t px = half ? tx * 2u : tx, py = half ? ty * 2u : ty;
+        RayResult r;
+        if (ray_begin<PATH, MODE>(v.pc, s, vcs[pend_view], px, py, st, r)) {
+          active = true;
+          my_view = pend_view;
+          my_px = px;
+          my_py = py;
+        } else {
+          store_ray<MODE>(v, px, py, r, steps_out, mip_out);
+        }
+      }
+      idle = drop_low_bits(idle, n);
+      avail = drop_low_bits(avail, n);
+      idle = __ballot_sync(kFull, !active);
+    }
+    if (!__any_sync(kFull, active)) {
+      if (exhausted) break;
+      continue;
+    }
+    if (active) {
+      const ViewConst &vc = vcs[my_view];
+#pragma unroll
+      for (int u = 0; u < UNROLL; u++) {
+        if (!ray_step<PATH, MODE, FAST, COUNT>(s, vc, tf, st)) {
+          RayResult r;
+          ray_end<MODE>(vc, st, r);
+          store_ray<MODE>(views[my_view], my_px, my_py, r, steps_out, mip_out);
+          acc_steps += r.steps;
+          if (COUNT) {
+            acc_tf += r.n_tf;
+            acc_grad += r.n_grad;
+            acc_walk += r.n_walk;
+          }
+          active = false;
+          break;
+        }
+      }
+    }
+  }
+  if (total) {
+    uint32_t sum = acc_steps;
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
+    if (lane == 0 && sum) atomicAdd(total, (unsigned long long)sum);
+  }
+  if (COUNT) {
+    uint32_t v4[4] = {acc_steps, acc_tf, acc_grad, acc_walk};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      uint32_t sum = v4[k];
+      for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
+      if (lane == 0 && sum) atomicAdd(counters + k, (unsigned long long)sum);
+    }
+  }
+}
+
+template <int PATH, int MODE, bool FAST, bool COUNT, int UNROLL>
+static cudaError_t launch_pt(const PersistLaunch &L, const DevScene &s, cudaStream_t st) {
+  k_raycast_persist<PATH, MODE, FAST, COUNT, UNROLL><<<L.blocks, 128, 0, st>>>(
+      L.views, L.nviews, s, L.lut, L.queue, L.ntiles, L.refill_min, L.shape, L.steps, L.mip,
+      L.total, L.counters);
+  return cudaGetLastError();
+}
+
+template <int PATH, int MODE, bool FAST, bool COUNT>
+static cudaError_t launch_pu(const PersistLaunch &L, const DevScene &s, cudaStream_t st) {
+  return L.unroll == 2 ? launch_pt<PATH, MODE, FAST, COUNT, 2>(L, s, st)
+                       : launch_pt<PATH, MODE, FAST, COUNT, 1>(L, s, st);
+}
+
+template <int PATH, int MODE, bool FAST>
+static cudaError_t launch_pc(const PersistLaunch &L, const DevScene &s, cudaStream_t st) {
+  return L.counters ? launch_pu<PATH, MODE, FAST, true>(L, s, st)
+                    : launch_pu<PATH, MODE, FAST, false>(L, s, st);
+}
+
+template <int PATH>
+static cudaError_t launch_pm(const PersistLaunch &L, const DevScene &s, cudaStream_t st) {
+  switch (L.mode) {
+    case R3D_MODE_FULL:
+      return L.fast ? launch_pc<PATH, R3D_MODE_FULL, true>(L, s, st)
+                    : launch_pc<PATH, R3D_MODE_FULL, false>(L, s, st);
+    case R3D_MODE_MIP: return launch_pc<PATH, R3D_MODE_MIP, false>(L, s, st);
+    case R3D_MODE_DEPTH: return launch_pc<PATH, R3D_MODE_DEPTH, false>(L, s, st);
+    case R3D_MODE_HEATMAP: return launch_pc<PATH, R3D_MODE_HEATMAP, false>(L, s, st);
+    case R3D_MODE_RAYDIR: return launch_pc<PATH, R3D_MODE_RAYDIR, false>(L, s, st);
+    default: return launch_pc<PATH, R3D_MODE_FLAT, false>(L, s, st);
+  }
+}
+
+cudaError_t launch_persist(const PersistLaunch &L, const DevScene &s, cudaStream_t st) {
+  return L.lod_bricks ? launch_pm<PATH_LOD_BRICKS>(L, s, st) : launch_pm<PATH_CUBE>(L, s, st);
+}
+
+int persist_blocks_per_sm(bool lod_bricks, uint32_t mode, bool fast, uint32_t unroll) {
+  // occupancy of the instantiation that launch_persist would pick
+  int n = 0;
+  cudaError_t e = cudaSuccess;
+#define R3D_OCC(P, M, F, U)                                                            \
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_raycast_persist<P, M, F, false, U>, \
+                                                    128, 0)
+  if (lod_bricks) {
+    if (mode == R3D_MODE_FULL && !fast) {
+      if (unroll == 2) R3D_OCC(PATH_LOD_BRICKS, R3D_MODE_FULL, false, 2);
+      else R3D_OCC(PATH_LOD_BRICKS, R3D_MODE_FULL, false, 1);
+    } else {
+      R3D_OCC(PATH_LOD_BRICKS, R3D_MODE_MIP, false, 1);
+    }
+  } else {
+    R3D_OCC(PATH_CUBE, R3D_MODE_FULL, false, 1);
+  }
+#undef R3D_OCC
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return 4;
+  }
+  return n > 0 ? n : 1;
+}
+
+}  // namespace r3d

@@ -54,8 +54,20 @@ def test_cube_builders_bit_exact(ctx, cube256):
     assert np.array_equal(ctx.cube_read(-1), cube256.occ)
 
 
+SCHEDULES = {"grid": dict(persistent=0), "persist": dict(persistent=1, refill_min=8),
+             "persist_16x2_u2": dict(persistent=1, refill_min=4, tile_shape=1, unroll=2),
+             "persist_32x1": dict(persistent=1, refill_min=24, tile_shape=2, unroll=1)}
+
+
+@pytest.fixture(params=list(SCHEDULES))
+def sched(request, ctx):
+    ctx.set_schedule(**SCHEDULES[request.param])
+    yield request.param
+    ctx.set_schedule()
+
+
 @pytest.mark.parametrize("mode", [0, 1, 2, 3, 4, 5])
-def test_cube_config0_modes(rb, orc, ctx, cube256, scroll_tf, mode):
+def test_cube_config0_modes(rb, orc, ctx, cube256, scroll_tf, mode, sched):
     p = elev35(rb, scroll_tf, step_voxels=0.5, max_mip=0.0, mode=mode)
     steps = np.zeros((512, 512), np.uint32)
     mipi = np.zeros((512, 512), np.uint32)
@@ -80,7 +92,7 @@ def test_cube_fast_gradient(rb, orc, ctx, cube256, scroll_tf):
 
 
 @pytest.mark.parametrize("case", ["lod", "rot", "ortho", "half", "lowcut", "bias"])
-def test_cube_view_variants(rb, orc, ctx, cube256, scroll_tf, case):
+def test_cube_view_variants(rb, orc, ctx, cube256, scroll_tf, case, sched):
     w, h = 320, 200
     p = rb.camera_view(1.1, -0.3, 1.2, w, h, scroll_tf, step_voxels=1.0, max_mip=10.0,
                        frame_index=3)
@@ -108,7 +120,7 @@ def test_cube_view_variants(rb, orc, ctx, cube256, scroll_tf, case):
         assert np.array_equal(steps, rsteps), f"{case} mode {mode} steps"
 
 
-def test_multiview_rects(rb, orc, ctx, cube256, scroll_tf):
+def test_multiview_rects(rb, orc, ctx, cube256, scroll_tf, sched):
     W, H = 400, 300
     views = []
     for i, (yaw, mode) in enumerate([(0.2, 0), (1.2, 1), (2.2, 3), (3.2, 5)]):
@@ -168,7 +180,7 @@ def bricks256(ctx, orc, phantom256, scroll_tf):
 
 
 @pytest.mark.parametrize("mode", [0, 1, 2, 3, 5])
-def test_bricks_modes(rb, orc, ctx, bricks256, scroll_tf, mode):
+def test_bricks_modes(rb, orc, ctx, bricks256, scroll_tf, mode, sched):
     w, h = 384, 256
     p = rb.camera_view(0.9, -0.5, 1.6, w, h, scroll_tf, step_voxels=0.5, mode=mode)
     p.brick_mode = ctx.brick_mode
@@ -184,7 +196,7 @@ def test_bricks_modes(rb, orc, ctx, bricks256, scroll_tf, mode):
 
 
 @pytest.mark.parametrize("case", ["crop", "axis_slab", "oblique", "fast", "cutoff99"])
-def test_bricks_clips(rb, orc, ctx, bricks256, scroll_tf, case):
+def test_bricks_clips(rb, orc, ctx, bricks256, scroll_tf, case, sched):
     w, h = 256, 192
     p = rb.camera_view(2.0, -0.2, 1.4, w, h, scroll_tf, step_voxels=0.5)
     p.brick_mode = ctx.brick_mode
