@@ -128,6 +128,25 @@ int r3d_cuda_raycast_fwd(r3d_cuda_ctx *ctx, const r3d_frame_params *views, uint3
                          uint8_t *rgba_out, uint32_t out_w, uint32_t out_h,
                          const r3d_cuda_aux *aux, void *stream);
 
+/* Forward raycast that allocates no device memory.  No counterpart in the
+ * reference: it exists for callers that must not let the library allocate
+ * while they render -- applications that give the renderer a fixed device-
+ * memory budget at start-up, or real-time render threads for which an
+ * allocation (which can synchronize the device) is a frame hitch.  Same
+ * views, image rules and results as r3d_cuda_raycast_fwd with a device
+ * rgba_out (required here), without the auxiliary outputs; it always runs
+ * the persistent queue-draining kernel.  Its per-call scratch (the view
+ * table and tile counters) lives in a 32 KiB array of device memory inside
+ * the library, which every GPU that loads the library holds until the
+ * process exits; at most 64 views fit, larger calls fail with
+ * R3D_E_INVALID.  The first call on a device looks up that array's device
+ * address, so make it before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU (different streams, or different
+ * contexts on one device) race and must be serialized by the caller. */
+int r3d_cuda_raycast_fwd_noalloc(r3d_cuda_ctx *ctx, const r3d_frame_params *views,
+                                 uint32_t nviews, uint8_t *rgba_out, uint32_t out_w,
+                                 uint32_t out_h, void *stream);
+
 /* How forward launches are scheduled.  persistent = 0: one thread per ray
  * (one grid per view).  persistent = 1: resident warps drain a queue of
  * 32-ray tiles covering all views of the call, refilling lanes whose rays

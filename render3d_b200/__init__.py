@@ -131,6 +131,7 @@ def _load() -> C.CDLL:
         "r3d_cuda_last_kernel_ns": (I, [P, C.POINTER(C.c_uint64)]),
         "r3d_cuda_fmath_eval": (I, [P, P, P, P, U32]),
         "r3d_cuda_set_schedule": (I, [P, C.POINTER(Schedule)]),
+        "r3d_cuda_raycast_fwd_noalloc": (I, [P, P, U32, P, U32, U32, P]),
         "r3d_cuda_get_schedule": (I, [P, C.POINTER(Schedule)]),
         "r3d_create": (I, [P, C.POINTER(RenderConfig), C.POINTER(P)]),
         "r3d_destroy": (None, [P]),

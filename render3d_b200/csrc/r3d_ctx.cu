@@ -703,7 +703,7 @@ int r3d_cuda_cube_read(r3d_cuda_ctx *c, int level, uint8_t *out, uint32_t dims[3
 
 // Validates and sanitizes one view against the image (the rectangle rule of
 // src/vk/vkbackend.c:6871-6900).  Returns 1 to render, 0 to skip, < 0 error.
-static int prepare_view(r3d_cuda_ctx *c, const r3d_frame_params &in, uint32_t out_w,
+int prepare_view(r3d_cuda_ctx *c, const r3d_frame_params &in, uint32_t out_w,
                         uint32_t out_h, r3d_frame_params &pc) {
   pc = in;
   if (in.mode >= R3D_MODE_COUNT) return fail(c, R3D_E_INVALID, "view: mode %u", in.mode);

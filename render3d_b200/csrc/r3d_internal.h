@@ -79,6 +79,11 @@ cudaError_t launch_view(const r3d_cuda_ctx *c, const r3d_frame_params &pc, uint8
 
 }  // namespace r3d
 
+// Validates one view and clips its rect to the image (1: render, 0: empty
+// rect, < 0: error code).
+int prepare_view(r3d_cuda_ctx *c, const r3d_frame_params &in, uint32_t out_w, uint32_t out_h,
+                 r3d_frame_params &pc);
+
 #define R3D_CUDA_TRY(ctx, expr)                                  \
   do {                                                           \
     cudaError_t e_ = (expr);                                     \
