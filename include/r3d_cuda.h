@@ -169,6 +169,45 @@ int r3d_cuda_get_schedule(const r3d_cuda_ctx *ctx, r3d_cuda_schedule *sched);
  * (synchronizes the events). */
 int r3d_cuda_last_kernel_ns(r3d_cuda_ctx *ctx, uint64_t *ns);
 
+/* --- differentiable render and adjoint --------------------------------------- */
+
+/* No counterpart in the reference: render3d's emission-absorption
+ * compositing (the FLAT mode of src/shaders/raycast.slang:894-1017) made
+ * differentiable over an FP32 density grid and an FP32 256x4 TF.  The render
+ * is the cube path at level 0 with no empty-space skip; alpha is clamped to
+ * [0, 1]; density scale = r3d_frame_params.density; termination at the
+ * context's alpha cutoff.  All pointers are device memory. */
+typedef struct r3d_cuda_diff_scene {
+  const float *density; /* nx*ny*nz, x fastest */
+  uint32_t nx, ny, nz;
+  const float *lut; /* 256 x RGBA, any real values (alpha is clamped) */
+} r3d_cuda_diff_scene;
+
+typedef struct r3d_cuda_grads {
+  float *density;       /* nx*ny*nz: dL/dvoxel (overwritten) */
+  float *lut;           /* 256*4: dL/dLUT (overwritten) */
+  float *density_scale; /* 1: dL/ddensity (overwritten) */
+} r3d_cuda_grads;
+
+/* Renders nviews (1..64) views (explicit viewports, cube path, optionally
+ * orthographic) into rgb_out: per view, viewport[0]*viewport[1]*3 floats,
+ * views back to back.  total_steps (nullable) += march iterations. */
+int r3d_cuda_diff_forward(r3d_cuda_ctx *ctx, const r3d_cuda_diff_scene *scene,
+                          const r3d_frame_params *views, uint32_t nviews, float *rgb_out,
+                          unsigned long long *total_steps, void *stream);
+
+/* Adjoint of r3d_cuda_diff_forward: given dL/drgb in rgb_out's layout,
+ * writes dL/dvoxel, dL/dLUT and dL/ddensity.  The march is recomputed in
+ * reverse from checkpoints kept every ckpt_k (32, 64 or 128) samples.
+ * deterministic = 0: FP32 atomic accumulation (last bits depend on the
+ * execution order); 1: fixed-point accumulation (2^-32 resolution, int64),
+ * bit-identical from run to run, using a context-owned buffer of
+ * 8 * (nvox + 1025) bytes. */
+int r3d_cuda_raycast_bwd(r3d_cuda_ctx *ctx, const r3d_cuda_diff_scene *scene,
+                         const r3d_frame_params *views, uint32_t nviews, const float *dl_drgb,
+                         const r3d_cuda_grads *out, uint32_t ckpt_k, int deterministic,
+                         void *stream);
+
 /* --- diagnostics ----------------------------------------------------------- */
 
 /* Evaluates the raycast's log2, exp2, pow(x, y) and x^24 on the device for n

@@ -77,6 +77,10 @@ def _load():
     lib.orc_lod_pick.argtypes = [F, F, F, U32]
     lib.orc_lod_fallback.restype = U32
     lib.orc_lod_fallback.argtypes = [U32, U32, U32]
+    lib.orc_diff_forward32.restype = C.c_int
+    lib.orc_diff_forward32.argtypes = [P, P, P, P, F, P, P, C.c_int]
+    lib.orc_diff_grad64.restype = C.c_int
+    lib.orc_diff_grad64.argtypes = [P, P, P, P, F, P, C.c_int, P, P, P, P, P, P, C.c_int]
     lib.orc_fmath_eval.restype = None
     lib.orc_fmath_eval.argtypes = [P, P, P, U32]
     lib.orc_m3_ypr.restype = None
@@ -188,6 +192,49 @@ def fmath_eval(x: np.ndarray, y: np.ndarray) -> np.ndarray:
     out = np.empty((x.size, 4), np.float32)
     lib.orc_fmath_eval(_p(x), _p(y), _p(out), x.size)
     return out
+
+
+def diff_forward32(params, dens: np.ndarray, lut: np.ndarray, cutoff: float = 0.98,
+                   threads: int = 0):
+    """FP32 differentiable render of one view: (rgb (h, w, 3) float32, steps)."""
+    dens = np.ascontiguousarray(dens, np.float32)
+    lut = np.ascontiguousarray(lut, np.float32)
+    n = np.array(dens.shape[::-1], np.uint32)
+    w, h = params.viewport[0], params.viewport[1]
+    rgb = np.zeros((h, w, 3), np.float32)
+    steps = np.zeros((h, w), np.uint32)
+    rc = lib.orc_diff_forward32(C.byref(params), _p(dens), _p(n), _p(lut), cutoff, _p(rgb),
+                                _p(steps), threads)
+    if rc != 0:
+        raise ValueError("orc_diff_forward32 rejected the view")
+    return rgb, steps
+
+
+def diff_grad64(params, dens: np.ndarray, lut: np.ndarray, dl_drgb: np.ndarray,
+                cutoff: float = 0.98, decisions32: bool = True, threads: int = 0,
+                dec_dens: np.ndarray | None = None, dec_lut: np.ndarray | None = None):
+    """FP64 render and gradients: (rgb64, g_dens, g_lut (256, 4), g_density).
+    With decisions32, the contributing samples and termination come from the
+    FP32 render of (dec_dens, dec_lut) when given (frozen decisions)."""
+    if dec_dens is not None:
+        dec_dens = np.ascontiguousarray(dec_dens, np.float32)
+    if dec_lut is not None:
+        dec_lut = np.ascontiguousarray(dec_lut, np.float32)
+    dens = np.ascontiguousarray(dens, np.float32)
+    lut = np.ascontiguousarray(lut, np.float32)
+    g = np.ascontiguousarray(dl_drgb, np.float32)
+    n = np.array(dens.shape[::-1], np.uint32)
+    w, h = params.viewport[0], params.viewport[1]
+    rgb = np.zeros((h, w, 3), np.float64)
+    gd = np.zeros(dens.shape, np.float64)
+    gl = np.zeros((256, 4), np.float64)
+    gs = np.zeros(1, np.float64)
+    rc = lib.orc_diff_grad64(C.byref(params), _p(dens), _p(n), _p(lut), cutoff, _p(g),
+                             int(decisions32), _p(dec_dens), _p(dec_lut), _p(gd), _p(gl),
+                             _p(gs), _p(rgb), threads)
+    if rc != 0:
+        raise ValueError("orc_diff_grad64 rejected the view")
+    return rgb, gd, gl, float(gs[0])
 
 
 def ref_lib():

@@ -74,6 +74,23 @@ int orc_render_pixels(const r3d_frame_params *p, const orc_cube *cube, const orc
                       const uint8_t lut[256][4], const orc_opts *o, const uint32_t *xy,
                       uint32_t n, uint8_t *out_rgba, uint32_t *steps, uint32_t *mip_index);
 
+/* Differentiable emission-absorption render over an FP32 density grid
+ * (n[0] x n[1] x n[2], x fastest) and an FP32 256x4 TF (see
+ * r3d_oracle_diff.c).  orc_diff_forward32: FP32 RGB image (w*h*3) exactly as
+ * the kernel computes it, and the per-ray step counts (nullable).
+ * orc_diff_grad64: FP64 render (rgb64_out, nullable) and the gradients of
+ * sum(dl_drgb * rgb) with respect to the voxels (g_dens), the LUT (g_lut,
+ * 256*4) and the density scale (g_density), all accumulated (+=).
+ * decisions32: contributing samples and termination as in the FP32 render
+ * of (dec_dens, dec_lut), or of (dens, lut) when those are NULL. */
+int orc_diff_forward32(const r3d_frame_params *pc, const float *dens, const uint32_t n[3],
+                       const float *lut, float cutoff, float *rgb_out, uint32_t *steps_out,
+                       int threads);
+int orc_diff_grad64(const r3d_frame_params *pc, const float *dens, const uint32_t n[3],
+                    const float *lut, float cutoff, const float *dl_drgb, int decisions32,
+                    const float *dec_dens, const float *dec_lut, double *g_dens, double *g_lut,
+                    double *g_density, double *rgb64_out, int threads);
+
 /* CPU build of the shared log2 / exp2 / pow / x^24 (4 outputs per input). */
 void orc_fmath_eval(const float *x, const float *y, float *out, uint32_t n);
 

@@ -80,6 +80,15 @@ class Schedule(C.Structure):
                 ("blocks_per_sm", C.c_uint32)]
 
 
+class DiffScene(C.Structure):
+    _fields_ = [("density", C.c_void_p), ("nx", C.c_uint32), ("ny", C.c_uint32),
+                ("nz", C.c_uint32), ("lut", C.c_void_p)]
+
+
+class Grads(C.Structure):
+    _fields_ = [("density", C.c_void_p), ("lut", C.c_void_p), ("density_scale", C.c_void_p)]
+
+
 class PhantomDesc(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("pitch", C.c_float), ("radius", C.c_float),
                 ("r0", C.c_float), ("sheet_half", C.c_float), ("in_mean", C.c_float),
@@ -132,6 +141,9 @@ def _load() -> C.CDLL:
         "r3d_cuda_fmath_eval": (I, [P, P, P, P, U32]),
         "r3d_cuda_set_schedule": (I, [P, C.POINTER(Schedule)]),
         "r3d_cuda_raycast_fwd_noalloc": (I, [P, P, U32, P, U32, U32, P]),
+        "r3d_cuda_diff_forward": (I, [P, C.POINTER(DiffScene), P, U32, P, P, P]),
+        "r3d_cuda_raycast_bwd": (I, [P, C.POINTER(DiffScene), P, U32, P, C.POINTER(Grads), U32,
+                                     I, P]),
         "r3d_cuda_get_schedule": (I, [P, C.POINTER(Schedule)]),
         "r3d_create": (I, [P, C.POINTER(RenderConfig), C.POINTER(P)]),
         "r3d_destroy": (None, [P]),
@@ -393,6 +405,31 @@ class Context:
         self._check(lib.r3d_cuda_raycast_fwd(self.h, arr, len(views), _ptr(out), out_w, out_h,
                                              C.byref(aux) if aux else None, stream or None))
         return out
+
+    def diff_forward(self, density, lut, views, rgb_out, total=None, stream: int = 0):
+        """Differentiable render (device tensors): density (nz, ny, nx) f32,
+        lut (256, 4) f32, rgb_out f32 of sum(w*h*3) over the views."""
+        if isinstance(views, FrameParams):
+            views = [views]
+        arr = (FrameParams * len(views))(*views)
+        nz, ny, nx = density.shape
+        sc = DiffScene(_ptr(density), nx, ny, nz, _ptr(lut))
+        self._check(lib.r3d_cuda_diff_forward(self.h, C.byref(sc), arr, len(views),
+                                              _ptr(rgb_out), _ptr(total) or None,
+                                              stream or None))
+
+    def raycast_bwd(self, density, lut, views, dl_drgb, g_density, g_lut, g_scale,
+                    ckpt_k: int = 32, deterministic: bool = False, stream: int = 0):
+        """Adjoint of diff_forward into the given device gradient buffers."""
+        if isinstance(views, FrameParams):
+            views = [views]
+        arr = (FrameParams * len(views))(*views)
+        nz, ny, nx = density.shape
+        sc = DiffScene(_ptr(density), nx, ny, nz, _ptr(lut))
+        gr = Grads(_ptr(g_density), _ptr(g_lut), _ptr(g_scale))
+        self._check(lib.r3d_cuda_raycast_bwd(self.h, C.byref(sc), arr, len(views),
+                                             _ptr(dl_drgb), C.byref(gr), ckpt_k,
+                                             int(deterministic), stream or None))
 
     def fmath_eval(self, x: np.ndarray, y: np.ndarray) -> np.ndarray:
         """Device log2, exp2, pow and x^24 of the inputs, (n, 4) float32."""

@@ -254,6 +254,7 @@ void r3d_cuda_destroy(r3d_cuda_ctx *c) {
   cudaFree(c->img);
   cudaFree(c->aux_buf);
   cudaFree(c->total);
+  cudaFree(c->diff_q);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   for (int k = 0; k < r3d_cuda_ctx::kRing; k++)

@@ -1,0 +1,552 @@
+// Differentiable emission-absorption raycast: forward and adjoint.
+//
+// The render is render3d's compositing without shading (FLAT mode,
+// src/shaders/raycast.slang:894-1017) over an FP32 density grid and an FP32
+// 256x4 transfer function: ray setup of the cube path, trilinear density at
+// texel centres (level 0, clamp to edge, no empty-space skip), TF lookup at
+// v*256-0.5, alpha clamped to [0, 1], opacity correction
+// a = 1 - (1 - alpha)^(density * step * lod_step), samples with a <= 0.003
+// ignored, front-to-back compositing with termination at the cutoff, then
+// the background.  The forward kernel writes an FP32 RGB image per view;
+// its arithmetic equals the CPU oracle's bit for bit.
+//
+// The adjoint kernel (one thread per ray) returns the gradients of
+// L = sum(dL/drgb * rgb) with respect to every voxel, every LUT entry and the
+// density scale.  It first marches the ray forward, keeping a checkpoint
+// (position and accumulated opacity) every K samples in local memory, then
+// walks the segments from last to first: each segment is recomputed from its
+// checkpoint, its contributing samples are recorded, and they are visited in
+// reverse with the colour behind them S (S <- a c + (1 - a) S, starting from
+// the background).  Transmittance is never divided out, which would be
+// unstable as alpha approaches 1.
+//
+// Gradients: voxel contributions are summed per trilinear cell in registers
+// while consecutive samples stay in one cell, then flushed with global
+// atomics; LUT contributions go to a per-block shared-memory table flushed
+// once per block; the density-scale gradient is reduced per warp.  Atomic
+// mode adds FP32 (order-dependent rounding).  Deterministic mode adds
+// fixed-point integers (value * 2^32, rounded, in int64): integer addition
+// is associative, so the result is identical for any execution order.
+#include <string.h>
+
+#include "r3d_internal.h"
+
+namespace r3d {
+
+constexpr double kFix = 4294967296.0;  // 2^32, deterministic fixed point
+
+struct DiffView {
+  r3d_frame_params pc;
+  unsigned long long out_off;  // first float of the view's RGB image
+  uint32_t pad[2];
+};
+
+struct DiffGrid {
+  const float *dens;
+  uint32_t n[3];
+  uint32_t nmax;
+  const float *lut;  // 256 x 4
+  float cutoff;
+};
+
+struct DiffRay {
+  float ro[3], dir[3];
+  float t0, tf, dt, span;
+  bool hit;
+};
+
+// ray setup of the cube path (raycast.slang:640-748)
+__device__ __forceinline__ void diff_setup(const r3d_frame_params &pc, const DiffGrid &g,
+                                           uint32_t px, uint32_t py, DiffRay &r) {
+  const bool ortho = (pc.view_flags & R3D_VIEW_ORTHO) != 0u;
+  float ux = ((float)px + 0.5f) / (float)pc.viewport[0];
+  float uy = ((float)py + 0.5f) / (float)pc.viewport[1];
+  float nx = ux * 2.0f - 1.0f, ny = 1.0f - uy * 2.0f;
+  float3 fw = make_float3(pc.cam_forward[0], pc.cam_forward[1], pc.cam_forward[2]);
+  float3 rt = make_float3(pc.cam_right[0], pc.cam_right[1], pc.cam_right[2]);
+  float3 up = make_float3(pc.cam_up[0], pc.cam_up[1], pc.cam_up[2]);
+  float3 d = ortho ? fw
+                   : make_float3(fmaf(ny, up.x, fmaf(nx, rt.x, fw.x)),
+                                 fmaf(ny, up.y, fmaf(nx, rt.y, fw.y)),
+                                 fmaf(ny, up.z, fmaf(nx, rt.z, fw.z)));
+  d = norm3(d);
+  float3 o = make_float3(pc.cam_origin[0], pc.cam_origin[1], pc.cam_origin[2]);
+  if (ortho)
+    o = make_float3(fmaf(ny, up.x, fmaf(nx, rt.x, o.x)), fmaf(ny, up.y, fmaf(nx, rt.y, o.y)),
+                    fmaf(ny, up.z, fmaf(nx, rt.z, o.z)));
+  const float c = 0.5f;
+  float q[3] = {(o.x - pc.vol_tx) - c, (o.y - pc.vol_ty) - c, (o.z - pc.vol_tz) - c};
+  float dv[3] = {d.x, d.y, d.z};
+  const float *r0 = pc.vol_r0, *r1 = pc.vol_r1, *r2 = pc.vol_r2;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    r.ro[a] = fmaf(r2[a], q[2], fmaf(r1[a], q[1], r0[a] * q[0])) + c;
+    r.dir[a] = fmaf(r2[a], dv[2], fmaf(r1[a], dv[1], r0[a] * dv[0]));
+  }
+  float tmn[3], tmx[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    float iv = 1.0f / r.dir[a];
+    float t0 = (0.0f - r.ro[a]) * iv, t1 = (1.0f - r.ro[a]) * iv;
+    tmn[a] = fminf(t0, t1);
+    tmx[a] = fmaxf(t0, t1);
+  }
+  float tn = fmaxf(fmaxf(fmaxf(tmn[0], tmn[1]), tmn[2]), 0.0f);
+  float tf = fminf(fminf(fminf(tmx[0], tmx[1]), tmx[2]), 1e30f);
+  r.hit = !(tn >= tf);
+  float voxel = 1.0f / (float)g.nmax;
+  r.dt = pc.step_voxels * voxel;
+  r.t0 = fmaf(hash12(px, py, pc.frame_index), r.dt, tn);
+  r.tf = tf;
+  r.span = fmaxf((tf - tn) / (4096.0f * r.dt), 1.0f);
+}
+
+// One sample: density, TF, opacity.  Fills the trilinear cell for scatters.
+struct DiffSample {
+  float v, tt, f, s[4], alpha, a;
+  uint32_t i0, i1;
+  uint32_t base, sx, sy, sz;  // corner (x0,y0,z0) and strides to x1/y1/z1 (0 at edges)
+  float fx, fy, fz;
+};
+
+__device__ __forceinline__ void diff_sample(const DiffGrid &g, const DiffRay &r, float t,
+                                            DiffSample &o) {
+  float p[3] = {fmaf(t, r.dir[0], r.ro[0]), fmaf(t, r.dir[1], r.ro[1]),
+                fmaf(t, r.dir[2], r.ro[2])};
+  uint32_t i0[3];
+  float fr[3];
+  bool up[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    float tc = clamp_(fmaf(p[a], (float)g.n[a], -0.5f), 0.0f, (float)(g.n[a] - 1u));
+    i0[a] = (uint32_t)tc;
+    fr[a] = tc - (float)i0[a];
+    up[a] = i0[a] + 1u < g.n[a];
+  }
+  const uint32_t nx = g.n[0], nxy = g.n[0] * g.n[1];
+  o.base = i0[0] + i0[1] * nx + i0[2] * nxy;
+  o.sx = up[0] ? 1u : 0u;
+  o.sy = up[1] ? nx : 0u;
+  o.sz = up[2] ? nxy : 0u;
+  o.fx = fr[0];
+  o.fy = fr[1];
+  o.fz = fr[2];
+  const float *b = g.dens + o.base;
+  float c00 = lerp_(__ldg(b), __ldg(b + o.sx), fr[0]);
+  float c10 = lerp_(__ldg(b + o.sy), __ldg(b + o.sy + o.sx), fr[0]);
+  float c01 = lerp_(__ldg(b + o.sz), __ldg(b + o.sz + o.sx), fr[0]);
+  float c11 = lerp_(__ldg(b + o.sz + o.sy), __ldg(b + o.sz + o.sy + o.sx), fr[0]);
+  o.v = lerp_(lerp_(c00, c10, fr[1]), lerp_(c01, c11, fr[1]), fr[2]);
+}
+
+// TF and opacity of a sample (FP32, as the oracle)
+__device__ __forceinline__ void diff_tf(const DiffGrid &g, float k, DiffSample &o) {
+  o.tt = clamp_(fmaf(o.v, 256.0f, -0.5f), 0.0f, 255.0f);
+  o.i0 = (uint32_t)o.tt;
+  o.i1 = min(o.i0 + 1u, 255u);
+  o.f = o.tt - (float)o.i0;
+  const float4 l0 = __ldg((const float4 *)g.lut + o.i0), l1 = __ldg((const float4 *)g.lut + o.i1);
+  o.s[0] = lerp_(l0.x, l1.x, o.f);
+  o.s[1] = lerp_(l0.y, l1.y, o.f);
+  o.s[2] = lerp_(l0.z, l1.z, o.f);
+  o.s[3] = lerp_(l0.w, l1.w, o.f);
+  o.alpha = clamp_(o.s[3], 0.0f, 1.0f);
+  o.a = 1.0f - r3d_powf(1.0f - o.alpha, k);
+}
+
+__global__ void __launch_bounds__(128) k_diff_fwd(const DiffView *__restrict__ views,
+                                                  const __grid_constant__ DiffGrid g,
+                                                  float *__restrict__ rgb,
+                                                  unsigned long long *__restrict__ total) {
+  const DiffView &vw = views[blockIdx.z];
+  const r3d_frame_params &pc = vw.pc;
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t px = blockIdx.x * 16u + (warp & 1u) * 8u +
+                      ((lane & 1u) | ((lane >> 1) & 2u) | ((lane >> 2) & 4u));
+  const uint32_t py = blockIdx.y * 8u + (warp >> 1) * 4u + (((lane >> 1) & 1u) | ((lane >> 2) & 2u));
+  uint32_t steps = 0;
+  if (px < pc.viewport[0] && py < pc.viewport[1]) {
+    DiffRay r;
+    diff_setup(pc, g, px, py, r);
+    float acc_r = 0.0f, acc_g = 0.0f, acc_b = 0.0f, acc_a = 0.0f;
+    if (r.hit) {
+      const float k = (pc.density * pc.step_voxels) * r.span;
+      float t = r.t0;
+      while (t < r.tf && steps < 4096u) {
+        steps++;
+        DiffSample s;
+        diff_sample(g, r, t, s);
+        if (!(s.v < pc.threshold)) {
+          diff_tf(g, k, s);
+          if (s.a > 0.003f) {
+            float w = (1.0f - acc_a) * s.a;
+            acc_r = fmaf(w, s.s[0], acc_r);
+            acc_g = fmaf(w, s.s[1], acc_g);
+            acc_b = fmaf(w, s.s[2], acc_b);
+            acc_a = acc_a + w;
+            if (acc_a >= g.cutoff) break;
+          }
+        }
+        t = fmaf(r.dt, r.span, t);
+      }
+    }
+    float tr = 1.0f - acc_a;
+    float *o = rgb + vw.out_off + ((size_t)py * pc.viewport[0] + px) * 3u;
+    o[0] = fmaf(tr, 0.02f, acc_r);
+    o[1] = fmaf(tr, 0.02f, acc_g);
+    o[2] = fmaf(tr, 0.03f, acc_b);
+  }
+  if (total) {
+    uint32_t sum = steps;
+    for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
+    if (lane == 0 && sum) atomicAdd(total, (unsigned long long)sum);
+  }
+}
+
+// voxel gradient sink: FP32 atomics or 2^32 fixed point
+template <bool DET>
+__device__ __forceinline__ void vox_add(float *gf, unsigned long long *gq, uint32_t i, float x) {
+  if (x == 0.0f) return;
+  if (DET)
+    atomicAdd(gq + i, (unsigned long long)(long long)__double2ll_rn((double)x * kFix));
+  else
+    atomicAdd(gf + i, x);
+}
+
+template <int K, bool DET>
+__global__ void __launch_bounds__(128) k_diff_bwd(const DiffView *__restrict__ views,
+                                                  const __grid_constant__ DiffGrid g,
+                                                  const float *__restrict__ dl_drgb,
+                                                  float *__restrict__ g_dens,
+                                                  unsigned long long *__restrict__ q_dens,
+                                                  float *__restrict__ g_lut,
+                                                  unsigned long long *__restrict__ q_lut,
+                                                  float *__restrict__ g_scale,
+                                                  unsigned long long *__restrict__ q_scale) {
+  constexpr int kMaxCk = (4096 + K - 1) / K;
+  __shared__ float s_lut[DET ? 1 : 1024];
+  __shared__ unsigned long long s_qlut[DET ? 1024 : 1];
+  for (uint32_t i = threadIdx.x; i < 1024u; i += blockDim.x) {
+    if (DET)
+      s_qlut[i] = 0ull;
+    else
+      s_lut[i] = 0.0f;
+  }
+  __syncthreads();
+
+  const DiffView &vw = views[blockIdx.z];
+  const r3d_frame_params &pc = vw.pc;
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t px = blockIdx.x * 16u + (warp & 1u) * 8u +
+                      ((lane & 1u) | ((lane >> 1) & 2u) | ((lane >> 2) & 4u));
+  const uint32_t py = blockIdx.y * 8u + (warp >> 1) * 4u + (((lane >> 1) & 1u) | ((lane >> 2) & 2u));
+  float g_density = 0.0f;
+  if (px < pc.viewport[0] && py < pc.viewport[1]) {
+    DiffRay r;
+    diff_setup(pc, g, px, py, r);
+    const float *gp = dl_drgb + vw.out_off + ((size_t)py * pc.viewport[0] + px) * 3u;
+    const float gr = gp[0], gg = gp[1], gb = gp[2];
+    if (r.hit && (gr != 0.0f || gg != 0.0f || gb != 0.0f)) {
+      const float kstep = pc.step_voxels * r.span;
+      const float k = (pc.density * pc.step_voxels) * r.span;
+      // forward sweep: checkpoints (t, accumulated opacity) before steps
+      // 1, K+1, 2K+1, ...
+      float ck_t[kMaxCk], ck_a[kMaxCk];
+      uint32_t nsteps = 0;
+      {
+        float t = r.t0, acc_a = 0.0f;
+        while (t < r.tf && nsteps < 4096u) {
+          if (nsteps % K == 0u) {
+            ck_t[nsteps / K] = t;
+            ck_a[nsteps / K] = acc_a;
+          }
+          nsteps++;
+          DiffSample s;
+          diff_sample(g, r, t, s);
+          bool stop = false;
+          if (!(s.v < pc.threshold)) {
+            diff_tf(g, k, s);
+            if (s.a > 0.003f) {
+              acc_a = acc_a + (1.0f - acc_a) * s.a;
+              stop = acc_a >= g.cutoff;
+            }
+          }
+          if (stop) break;
+          t = fmaf(r.dt, r.span, t);
+        }
+      }
+      // reverse sweep over segments
+      float S_r = 0.02f, S_g = 0.02f, S_b = 0.03f;
+      // current trilinear cell of the voxel-gradient aggregation
+      uint32_t cell = 0xffffffffu, csx = 0, csy = 0, csz = 0;
+      float cw[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      float seg_t[K], seg_a[K];
+      const int nck = (int)((nsteps + K - 1) / K);
+      for (int j = nck - 1; j >= 0; j--) {
+        // recompute segment j, recording its contributing samples
+        int nseg = 0;
+        float t = ck_t[j], acc_a = ck_a[j];
+        const uint32_t s_end = min(nsteps, (uint32_t)(j + 1) * K);
+        for (uint32_t st = (uint32_t)j * K; st < s_end; st++) {
+          DiffSample s;
+          diff_sample(g, r, t, s);
+          if (!(s.v < pc.threshold)) {
+            diff_tf(g, k, s);
+            if (s.a > 0.003f) {
+              seg_t[nseg] = t;
+              seg_a[nseg] = acc_a;
+              nseg++;
+              acc_a = acc_a + (1.0f - acc_a) * s.a;
+            }
+          }
+          t = fmaf(r.dt, r.span, t);
+        }
+        for (int i = nseg - 1; i >= 0; i--) {
+          DiffSample s;
+          diff_sample(g, r, seg_t[i], s);
+          diff_tf(g, k, s);
+          const float tprev = 1.0f - seg_a[i];
+          const float dc_r = gr * tprev * s.a, dc_g = gg * tprev * s.a, dc_b = gb * tprev * s.a;
+          const float da = gr * tprev * (s.s[0] - S_r) + gg * tprev * (s.s[1] - S_g) +
+                           gb * tprev * (s.s[2] - S_b);
+          S_r = fmaf(s.a, s.s[0] - S_r, S_r);
+          S_g = fmaf(s.a, s.s[1] - S_g, S_g);
+          S_b = fmaf(s.a, s.s[2] - S_b, S_b);
+          float dalpha = 0.0f;
+          const bool alpha_free = s.s[3] > 0.0f && s.s[3] < 1.0f;
+          if (alpha_free) dalpha = da * k * r3d_powf(1.0f - s.alpha, k - 1.0f);
+          if (s.alpha < 1.0f)
+            g_density += da * (-(1.0f - s.a) * (r3d_log2f(1.0f - s.alpha) * 0.693147181f)) *
+                         kstep;
+          const float ds[4] = {dc_r, dc_g, dc_b, dalpha};
+          const float lf0 = 1.0f - s.f;
+          const float4 l0 = __ldg((const float4 *)g.lut + s.i0);
+          const float4 l1 = __ldg((const float4 *)g.lut + s.i1);
+          const float dl[4] = {l1.x - l0.x, l1.y - l0.y, l1.z - l0.z, l1.w - l0.w};
+          float dvv = 0.0f;
+#pragma unroll
+          for (int c = 0; c < 4; c++) {
+            if (DET) {
+              atomicAdd(&s_qlut[s.i0 * 4u + c],
+                        (unsigned long long)__double2ll_rn((double)(ds[c] * lf0) * kFix));
+              atomicAdd(&s_qlut[s.i1 * 4u + c],
+                        (unsigned long long)__double2ll_rn((double)(ds[c] * s.f) * kFix));
+            } else {
+              atomicAdd(&s_lut[s.i0 * 4u + c], ds[c] * lf0);
+              atomicAdd(&s_lut[s.i1 * 4u + c], ds[c] * s.f);
+            }
+            dvv = fmaf(ds[c], dl[c], dvv);
+          }
+          const bool tt_free = s.tt > 0.0f && s.tt < 255.0f;
+          const float dv = tt_free ? dvv * 256.0f : 0.0f;
+          // trilinear scatter, aggregated per cell
+          if (s.base != cell || s.sx != csx || s.sy != csy || s.sz != csz) {
+            if (cell != 0xffffffffu) {
+#pragma unroll
+              for (int c = 0; c < 8; c++)
+                vox_add<DET>(g_dens, q_dens,
+                             cell + ((c & 1) ? csx : 0u) + ((c & 2) ? csy : 0u) +
+                                 ((c & 4) ? csz : 0u),
+                             cw[c]);
+            }
+            cell = s.base;
+            csx = s.sx;
+            csy = s.sy;
+            csz = s.sz;
+#pragma unroll
+            for (int c = 0; c < 8; c++) cw[c] = 0.0f;
+          }
+          const float wx[2] = {1.0f - s.fx, s.fx}, wy[2] = {1.0f - s.fy, s.fy},
+                      wz[2] = {1.0f - s.fz, s.fz};
+#pragma unroll
+          for (int c = 0; c < 8; c++)
+            cw[c] = fmaf(dv, (wx[c & 1] * wy[(c >> 1) & 1]) * wz[c >> 2], cw[c]);
+        }
+      }
+      if (cell != 0xffffffffu) {
+#pragma unroll
+        for (int c = 0; c < 8; c++)
+          vox_add<DET>(g_dens, q_dens,
+                       cell + ((c & 1) ? csx : 0u) + ((c & 2) ? csy : 0u) + ((c & 4) ? csz : 0u),
+                       cw[c]);
+      }
+    }
+  }
+  // density scale: warp reduction, one global add per warp
+  float gs = g_density;
+  if (DET) {
+    long long q = __double2ll_rn((double)gs * kFix);
+    for (int off = 16; off > 0; off >>= 1) q += __shfl_xor_sync(0xffffffffu, q, off);
+    if (lane == 0 && q) atomicAdd(q_scale, (unsigned long long)q);
+  } else {
+    for (int off = 16; off > 0; off >>= 1) gs += __shfl_xor_sync(0xffffffffu, gs, off);
+    if (lane == 0 && gs != 0.0f) atomicAdd(g_scale, gs);
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < 1024u; i += blockDim.x) {
+    if (DET) {
+      if (s_qlut[i]) atomicAdd(q_lut + i, s_qlut[i]);
+    } else {
+      if (s_lut[i] != 0.0f) atomicAdd(g_lut + i, s_lut[i]);
+    }
+  }
+}
+
+static unsigned grid_blocks(size_t n) {
+  size_t b = (n + 255) / 256;
+  return (unsigned)(b < 148u * 32u ? (b ? b : 1) : 148u * 32u);
+}
+
+// fixed point -> float
+__global__ void k_fix_to_float(const unsigned long long *__restrict__ q, float *__restrict__ out,
+                               size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    out[i] = (float)((double)(long long)q[i] / kFix);
+}
+
+}  // namespace r3d
+
+using namespace r3d;
+
+// Validates the grid and views, uploads the view table; returns the grid
+// descriptor and total output floats.
+static int diff_prepare(r3d_cuda_ctx *c, const r3d_cuda_diff_scene *sc,
+                        const r3d_frame_params *views, uint32_t nviews, DiffGrid &g,
+                        DiffView *&dviews, uint32_t &maxw, uint32_t &maxh, size_t &nfloats,
+                        cudaStream_t st) {
+  if (!sc || !sc->density || !sc->lut || !sc->nx || !sc->ny || !sc->nz || !views || !nviews ||
+      nviews > kMaxBatchViews)
+    return fail(c, R3D_E_INVALID, "diff: bad arguments");
+  if ((uint64_t)sc->nx * sc->ny * sc->nz >= (1ull << 32))
+    return fail(c, R3D_E_INVALID, "diff: grid too large for 32-bit voxel indices");
+  g.dens = sc->density;
+  g.n[0] = sc->nx;
+  g.n[1] = sc->ny;
+  g.n[2] = sc->nz;
+  g.nmax = max(sc->nx, max(sc->ny, sc->nz));
+  g.lut = sc->lut;
+  g.cutoff = c->alpha_cutoff;
+  const int k = c->ring_next;
+  c->ring_next = (k + 1) % r3d_cuda_ctx::kRing;
+  if (c->ring_used[k]) R3D_CUDA_TRY(c, cudaEventSynchronize(c->ring_ev[k]));
+  static_assert(sizeof(DiffView) <= sizeof(DevView), "ring slot size");
+  DiffView *hv = (DiffView *)(c->ring_host + (size_t)k * kMaxBatchViews);
+  dviews = (DiffView *)(c->ring_dev + (size_t)k * kMaxBatchViews);
+  maxw = maxh = 0;
+  nfloats = 0;
+  for (uint32_t v = 0; v < nviews; v++) {
+    const r3d_frame_params &p = views[v];
+    if (!p.viewport[0] || !p.viewport[1] || p.viewport[0] > 16384u || p.viewport[1] > 16384u)
+      return fail(c, R3D_E_INVALID, "diff: view %u needs an explicit viewport", v);
+    if (p.brick_mode || p.slab_grid || p.clip_valid || p.overlay_flags ||
+        (p.view_flags & ~R3D_VIEW_ORTHO))
+      return fail(c, R3D_E_UNSUPPORTED, "diff: view %u uses a feature the differentiable "
+                                        "render does not have", v);
+    if (!(p.step_voxels > 0.0f)) return fail(c, R3D_E_INVALID, "diff: step_voxels");
+    memset(&hv[v], 0, sizeof hv[v]);
+    hv[v].pc = p;
+    hv[v].out_off = nfloats;
+    nfloats += (size_t)p.viewport[0] * p.viewport[1] * 3u;
+    maxw = max(maxw, p.viewport[0]);
+    maxh = max(maxh, p.viewport[1]);
+  }
+  R3D_CUDA_TRY(c, cudaMemcpyAsync(dviews, hv, sizeof(DiffView) * nviews, cudaMemcpyHostToDevice,
+                                  st));
+  R3D_CUDA_TRY(c, cudaEventRecord(c->ring_ev[k], st));
+  c->ring_used[k] = true;
+  return R3D_OK;
+}
+
+extern "C" int r3d_cuda_diff_forward(r3d_cuda_ctx *c, const r3d_cuda_diff_scene *sc,
+                                     const r3d_frame_params *views, uint32_t nviews,
+                                     float *rgb_out, unsigned long long *total_steps,
+                                     void *stream) {
+  if (!c || !rgb_out) return fail(c, R3D_E_INVALID, "diff_forward: bad arguments");
+  cudaSetDevice(c->device);
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  if (!is_device_ptr(rgb_out)) return fail(c, R3D_E_INVALID, "diff_forward: rgb_out not device");
+  DiffGrid g;
+  DiffView *dv;
+  uint32_t mw, mh;
+  size_t nf;
+  int rc = diff_prepare(c, sc, views, nviews, g, dv, mw, mh, nf, st);
+  if (rc != R3D_OK) return rc;
+  R3D_CUDA_TRY(c, cudaEventRecord(c->ev0, st));
+  dim3 grid((mw + 15u) / 16u, (mh + 7u) / 8u, nviews);
+  k_diff_fwd<<<grid, 128, 0, st>>>(dv, g, rgb_out, total_steps);
+  R3D_CUDA_TRY(c, cudaGetLastError());
+  R3D_CUDA_TRY(c, cudaEventRecord(c->ev1, st));
+  c->timed = true;
+  return R3D_OK;
+}
+
+template <int K, bool DET>
+static cudaError_t launch_bwd(dim3 grid, cudaStream_t st, const DiffView *dv, const DiffGrid &g,
+                              const float *dl, float *gd, unsigned long long *qd, float *gl,
+                              unsigned long long *ql, float *gs, unsigned long long *qs) {
+  k_diff_bwd<K, DET><<<grid, 128, 0, st>>>(dv, g, dl, gd, qd, gl, ql, gs, qs);
+  return cudaGetLastError();
+}
+
+extern "C" int r3d_cuda_raycast_bwd(r3d_cuda_ctx *c, const r3d_cuda_diff_scene *sc,
+                                    const r3d_frame_params *views, uint32_t nviews,
+                                    const float *dl_drgb, const r3d_cuda_grads *out,
+                                    uint32_t ckpt_k, int deterministic, void *stream) {
+  if (!c || !dl_drgb || !out || !out->density || !out->lut || !out->density_scale)
+    return fail(c, R3D_E_INVALID, "raycast_bwd: bad arguments");
+  if (ckpt_k != 32u && ckpt_k != 64u && ckpt_k != 128u)
+    return fail(c, R3D_E_INVALID, "raycast_bwd: checkpoint interval %u not 32, 64 or 128",
+                ckpt_k);
+  cudaSetDevice(c->device);
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  DiffGrid g;
+  DiffView *dv;
+  uint32_t mw, mh;
+  size_t nf;
+  int rc = diff_prepare(c, sc, views, nviews, g, dv, mw, mh, nf, st);
+  if (rc != R3D_OK) return rc;
+  const size_t nvox = (size_t)sc->nx * sc->ny * sc->nz;
+  unsigned long long *qd = nullptr, *ql = nullptr, *qs = nullptr;
+  if (deterministic) {
+    const size_t need = (nvox + 1024u + 1u) * sizeof(unsigned long long);
+    if (c->diff_q_bytes < need) {
+      cudaFree(c->diff_q);
+      c->diff_q = nullptr;
+      c->diff_q_bytes = 0;
+      R3D_CUDA_TRY(c, cudaMalloc(&c->diff_q, need));
+      c->diff_q_bytes = need;
+    }
+    qd = c->diff_q;
+    ql = qd + nvox;
+    qs = ql + 1024;
+    R3D_CUDA_TRY(c, cudaMemsetAsync(c->diff_q, 0, need, st));
+  } else {
+    R3D_CUDA_TRY(c, cudaMemsetAsync(out->density, 0, nvox * sizeof(float), st));
+    R3D_CUDA_TRY(c, cudaMemsetAsync(out->lut, 0, 1024 * sizeof(float), st));
+    R3D_CUDA_TRY(c, cudaMemsetAsync(out->density_scale, 0, sizeof(float), st));
+  }
+  R3D_CUDA_TRY(c, cudaEventRecord(c->ev0, st));
+  dim3 grid((mw + 15u) / 16u, (mh + 7u) / 8u, nviews);
+  cudaError_t e;
+  float *gd = out->density, *gl = out->lut, *gs = out->density_scale;
+  if (deterministic) {
+    e = ckpt_k == 32u ? launch_bwd<32, true>(grid, st, dv, g, dl_drgb, gd, qd, gl, ql, gs, qs)
+        : ckpt_k == 64u ? launch_bwd<64, true>(grid, st, dv, g, dl_drgb, gd, qd, gl, ql, gs, qs)
+                        : launch_bwd<128, true>(grid, st, dv, g, dl_drgb, gd, qd, gl, ql, gs, qs);
+  } else {
+    e = ckpt_k == 32u ? launch_bwd<32, false>(grid, st, dv, g, dl_drgb, gd, qd, gl, ql, gs, qs)
+        : ckpt_k == 64u ? launch_bwd<64, false>(grid, st, dv, g, dl_drgb, gd, qd, gl, ql, gs, qs)
+                        : launch_bwd<128, false>(grid, st, dv, g, dl_drgb, gd, qd, gl, ql, gs, qs);
+  }
+  if (e != cudaSuccess) return cuda_fail(c, e, "raycast_bwd: launch");
+  if (deterministic) {
+    k_fix_to_float<<<grid_blocks(nvox), 256, 0, st>>>(qd, gd, nvox);
+    k_fix_to_float<<<4, 256, 0, st>>>(ql, gl, 1024);
+    k_fix_to_float<<<1, 32, 0, st>>>(qs, gs, 1);
+    R3D_CUDA_TRY(c, cudaGetLastError());
+  }
+  R3D_CUDA_TRY(c, cudaEventRecord(c->ev1, st));
+  c->timed = true;
+  return R3D_OK;
+}

@@ -50,6 +50,10 @@ struct r3d_cuda_ctx {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   bool timed = false;
 
+  // fixed-point gradient accumulators of the deterministic adjoint
+  unsigned long long *diff_q = nullptr;
+  size_t diff_q_bytes = 0;
+
   // forward scheduling and the view-table ring of persistent launches:
   // slot k holds one call's views (pinned host copy + device copy) and its
   // tile counters; ring_ev[k] completes once the slot's upload has run
