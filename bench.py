@@ -42,6 +42,7 @@ CUTOFF = 0.99
 STEP_VOXELS = 0.5
 ORBIT_FRAMES = 120
 WORKLOAD = "scroll phantom 1024^3 u8, 128^3 bricks x 4 LOD levels, 1920x1080 full shading"
+METRIC = "raycast Gsamples/s & fps @1024^3 1080p; fwd+bwd Gsamples/s vs plain, same GPU"
 
 
 def measured_peaks() -> tuple[float, str]:
@@ -142,6 +143,89 @@ def algorithmic_bytes(cnt: np.ndarray, pixels: int) -> float:
     return 8.0 * samples + 48.0 * grad + 8.0 * tf + 4.0 * walks + 4.0 * pixels
 
 
+def fwd_bwd_bench(rb, ctx, torch, local: int, steps: int, adam_steps: int) -> dict:
+    """Differentiable workload: a 256^3 FP32 density grid (scroll phantom / 255
+    plus N(0, 10/255), seeded), the scroll TF as FP32, 64 orbit views of
+    256x256 at step 0.5; L2 loss against the unperturbed phantom's render.
+    Times forward + backward (deterministic fixed-point gradients, K = 64)
+    per step; Gsamples/s counts the forward march's samples."""
+    dev = f"cuda:{local}"
+    n, nv, w = 256, 64, 256
+    rng = np.random.default_rng(SEED)
+    clean = rb.phantom(n, seed=SEED).astype(np.float32) / 255.0
+    noisy = clean + rng.normal(0.0, 10.0 / 255.0, clean.shape).astype(np.float32)
+    lut8 = rb.scroll_ramp_tf()
+    lut = torch.tensor(lut8.astype(np.float32) / 255.0, device=dev)
+    views = [rb.orbit_view(i / nv, w, w, lut8, step_voxels=0.5, frame_index=i) for i in range(nv)]
+    for v in views:
+        v.max_mip = 0.0
+    nf = nv * w * w * 3
+    st = torch.cuda.ExternalStream(ctx.stream, device=local)
+    dclean = torch.tensor(clean, device=dev)
+    dens = torch.tensor(noisy, device=dev)
+    target = torch.empty(nf, device=dev)
+    rgb = torch.empty(nf, device=dev)
+    tot = torch.zeros(1, dtype=torch.int64, device=dev)
+    ctx.set_alpha_cutoff(0.98)
+    ctx.diff_forward(dclean, lut, views, target, stream=ctx.stream)
+    ctx.diff_forward(dens, lut, views, rgb, total=tot, stream=ctx.stream)
+    torch.cuda.synchronize()
+    samples = float(tot.item())
+    gd = torch.empty_like(dens)
+    gl = torch.empty_like(lut)
+    gs = torch.empty(1, device=dev)
+    grad = torch.empty(nf, device=dev)
+
+    def step():
+        ctx.diff_forward(dens, lut, views, rgb, stream=ctx.stream)
+        with torch.cuda.stream(st):
+            torch.sub(rgb, target, out=grad)
+            grad.mul_(2.0)
+        ctx.raycast_bwd(dens, lut, views, grad, gd, gl, gs, 64, True, stream=ctx.stream)
+
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(steps):
+        step()
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    # 100 Adam steps on the voxels, LUT and density scale
+    p_dens = dens.clone().requires_grad_(False)
+    opt_state = [torch.zeros_like(p_dens), torch.zeros_like(p_dens)]
+    loss0 = lossN = None
+    t0 = time.perf_counter()
+    b1, b2, lr, eps = 0.9, 0.999, 2e-3, 1e-8
+    for it in range(1, adam_steps + 1):
+        ctx.diff_forward(p_dens, lut, views, rgb, stream=ctx.stream)
+        with torch.cuda.stream(st):
+            torch.sub(rgb, target, out=grad)
+            loss = float((grad * grad).sum().item()) if it in (1, adam_steps) else None
+            grad.mul_(2.0)
+        ctx.raycast_bwd(p_dens, lut, views, grad, gd, gl, gs, 64, True, stream=ctx.stream)
+        with torch.cuda.stream(st):
+            m, v2 = opt_state
+            m.mul_(b1).add_(gd, alpha=1 - b1)
+            v2.mul_(b2).addcmul_(gd, gd, value=1 - b2)
+            den = (v2 / (1 - b2 ** it)).sqrt_().add_(eps)
+            p_dens.addcdiv_(m, den, value=-lr / (1 - b1 ** it))
+        if it == 1:
+            loss0 = loss
+        if it == adam_steps:
+            lossN = loss
+    torch.cuda.synchronize()
+    adam_s = time.perf_counter() - t0
+    return {"workload": "256^3 FP32 density (phantom/255 + N(0,10/255)), 64 orbit views 256x256, "
+                        "step 0.5, L2 loss, checkpoints every 64 samples, deterministic",
+            "value": samples / (ms * 1e-3) / 1e9, "unit": "Gsamples/s", "ms_per_step": ms,
+            "samples_per_step": samples, "steps": steps,
+            "adam": {"steps": adam_steps, "loss_first": loss0, "loss_last": lossN,
+                     "s_per_step": adam_s / adam_steps}}
+
+
 def cpu_baseline(rb, orc, vol_pages, lut, frames: list[int], threads: int) -> dict:
     """The oracle (FP32 CPU restatement of the reference shader) on a bounded
     sample of the same workload: whole 1920x1080 frames of the orbit."""
@@ -190,7 +274,7 @@ def run_reference(args) -> None:
     v = sum(samples) / t / 1e9
     sample = (f"per step: {xy.shape[0]} rays (every 4th pixel of every 4th row) of one "
               "1920x1080 orbit frame")
-    out = {"impl": "reference", "metric": "raycast Gsamples/s @1024^3 1080p (full shading)",
+    out = {"impl": "reference", "metric": METRIC,
            "value": v, "unit": "Gsamples/s", "n_gpus": args.gpus, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": 1000.0 * t / len(times),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -294,6 +378,11 @@ def run_ours(args) -> None:
     e2e_value = samples_all / float(te.item()) / 1e9
     r.close()
 
+    fb = None
+    if not args.no_fwd_bwd:
+        fb = fwd_bwd_bench(rb, ctx, torch, local, steps=20, adam_steps=100)
+        fb["ratio_vs_plain"] = fb["value"] / value
+
     peak, peak_kind = measured_peaks()
     alg = algorithmic_bytes(counts, W * H * K)
     achieved = alg / (ms * 1e-3) / 1e9
@@ -306,7 +395,7 @@ def run_ours(args) -> None:
             cpu = cpu_baseline(rb, orc, (page, pool, bm), lut, [0, 30],
                                os.cpu_count() or 1)
             del pool
-        out = {"metric": "raycast Gsamples/s @1024^3 1080p (full shading)", "value": value,
+        out = {"metric": METRIC, "value": value,
                "unit": "Gsamples/s", "n_gpus": world, "steps": K, "warmup": Wm,
                "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -323,6 +412,7 @@ def run_ours(args) -> None:
                             "unit": "GB/s", "frac": achieved / peak, "traffic": None,
                             "peak_kind": peak_kind,
                             "algorithmic_bytes_per_frame": alg / K},
+               "fwd_bwd": fb,
                "gpu_launches": K,
                "clocks": clk.summary(),
                "cpu_baseline": cpu}
@@ -331,6 +421,7 @@ def run_ours(args) -> None:
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+    return out
 
 
 def run_profile(args) -> None:
@@ -362,6 +453,7 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=400)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fwd-bwd", action="store_true")
     ap.add_argument("--profile", type=int, default=0, metavar="N",
                     help="only build the workload and render N orbit frames (for ncu)")
     ap.add_argument("--profile-mode", type=int, default=0)

@@ -13,12 +13,14 @@
 // The adjoint kernel (one thread per ray) returns the gradients of
 // L = sum(dL/drgb * rgb) with respect to every voxel, every LUT entry and the
 // density scale.  It first marches the ray forward, keeping a checkpoint
-// (position and accumulated opacity) every K samples in local memory, then
-// walks the segments from last to first: each segment is recomputed from its
-// checkpoint, its contributing samples are recorded, and they are visited in
-// reverse with the colour behind them S (S <- a c + (1 - a) S, starting from
-// the background).  Transmittance is never divided out, which would be
-// unstable as alpha approaches 1.
+// (position and accumulated opacity) every K samples in local memory, the
+// number of contributing samples of each K-sample segment, and the last 64
+// contributing samples.  It then walks the segments with contributions from
+// last to first: a segment whose samples are still among the remembered ones
+// uses them, any other is recomputed from its checkpoint; the samples are
+// visited in reverse with the colour behind them S (S <- a c + (1 - a) S,
+// starting from the background).  Transmittance is never divided out, which
+// would be unstable as alpha approaches 1.
 //
 // Gradients: voxel contributions are summed per trilinear cell in registers
 // while consecutive samples stay in one cell, then flushed with global
@@ -213,6 +215,8 @@ __device__ __forceinline__ void vox_add(float *gf, unsigned long long *gq, uint3
     atomicAdd(gf + i, x);
 }
 
+constexpr int kRing = 64;  // contributing samples remembered by the forward sweep
+
 template <int K, bool DET>
 __global__ void __launch_bounds__(128) k_diff_bwd(const DiffView *__restrict__ views,
                                                   const __grid_constant__ DiffGrid g,
@@ -250,15 +254,19 @@ __global__ void __launch_bounds__(128) k_diff_bwd(const DiffView *__restrict__ v
       const float kstep = pc.step_voxels * r.span;
       const float k = (pc.density * pc.step_voxels) * r.span;
       // forward sweep: checkpoints (t, accumulated opacity) before steps
-      // 1, K+1, 2K+1, ...
+      // 1, K+1, 2K+1, ..., the number of contributing samples of each
+      // segment, and the last kRing contributing samples themselves
       float ck_t[kMaxCk], ck_a[kMaxCk];
-      uint32_t nsteps = 0;
+      uint8_t ck_n[kMaxCk];
+      float ring_t[kRing], ring_a[kRing];
+      uint32_t nsteps = 0, ncontrib = 0;
       {
         float t = r.t0, acc_a = 0.0f;
         while (t < r.tf && nsteps < 4096u) {
           if (nsteps % K == 0u) {
             ck_t[nsteps / K] = t;
             ck_a[nsteps / K] = acc_a;
+            ck_n[nsteps / K] = 0;
           }
           nsteps++;
           DiffSample s;
@@ -267,6 +275,10 @@ __global__ void __launch_bounds__(128) k_diff_bwd(const DiffView *__restrict__ v
           if (!(s.v < pc.threshold)) {
             diff_tf(g, k, s);
             if (s.a > 0.003f) {
+              ring_t[ncontrib % kRing] = t;
+              ring_a[ncontrib % kRing] = acc_a;
+              ncontrib++;
+              ck_n[(nsteps - 1u) / K]++;
               acc_a = acc_a + (1.0f - acc_a) * s.a;
               stop = acc_a >= g.cutoff;
             }
@@ -275,32 +287,45 @@ __global__ void __launch_bounds__(128) k_diff_bwd(const DiffView *__restrict__ v
           t = fmaf(r.dt, r.span, t);
         }
       }
-      // reverse sweep over segments
+      // reverse sweep over segments with contributions
       float S_r = 0.02f, S_g = 0.02f, S_b = 0.03f;
       // current trilinear cell of the voxel-gradient aggregation
       uint32_t cell = 0xffffffffu, csx = 0, csy = 0, csz = 0;
       float cw[8] = {0, 0, 0, 0, 0, 0, 0, 0};
       float seg_t[K], seg_a[K];
       const int nck = (int)((nsteps + K - 1) / K);
+      uint32_t end = ncontrib;  // contributions of segments < j: [0, end)
       for (int j = nck - 1; j >= 0; j--) {
-        // recompute segment j, recording its contributing samples
+        const uint32_t nj = ck_n[j];
+        if (nj == 0u) continue;
+        const uint32_t start = end - nj;
+        const bool in_ring = ncontrib - start <= (uint32_t)kRing;
         int nseg = 0;
-        float t = ck_t[j], acc_a = ck_a[j];
-        const uint32_t s_end = min(nsteps, (uint32_t)(j + 1) * K);
-        for (uint32_t st = (uint32_t)j * K; st < s_end; st++) {
-          DiffSample s;
-          diff_sample(g, r, t, s);
-          if (!(s.v < pc.threshold)) {
-            diff_tf(g, k, s);
-            if (s.a > 0.003f) {
-              seg_t[nseg] = t;
-              seg_a[nseg] = acc_a;
-              nseg++;
-              acc_a = acc_a + (1.0f - acc_a) * s.a;
-            }
+        if (in_ring) {  // the segment's samples are still in the ring
+          for (uint32_t i = start; i < end; i++) {
+            seg_t[nseg] = ring_t[i % kRing];
+            seg_a[nseg] = ring_a[i % kRing];
+            nseg++;
           }
-          t = fmaf(r.dt, r.span, t);
+        } else {  // recompute segment j from its checkpoint
+          float t = ck_t[j], acc_a = ck_a[j];
+          const uint32_t s_end = min(nsteps, (uint32_t)(j + 1) * K);
+          for (uint32_t st = (uint32_t)j * K; st < s_end; st++) {
+            DiffSample s;
+            diff_sample(g, r, t, s);
+            if (!(s.v < pc.threshold)) {
+              diff_tf(g, k, s);
+              if (s.a > 0.003f) {
+                seg_t[nseg] = t;
+                seg_a[nseg] = acc_a;
+                nseg++;
+                acc_a = acc_a + (1.0f - acc_a) * s.a;
+              }
+            }
+            t = fmaf(r.dt, r.span, t);
+          }
         }
+        end = start;
         for (int i = nseg - 1; i >= 0; i--) {
           DiffSample s;
           diff_sample(g, r, seg_t[i], s);
