@@ -226,6 +226,97 @@ def fwd_bwd_bench(rb, ctx, torch, local: int, steps: int, adam_steps: int) -> di
                      "s_per_step": adam_s / adam_steps}}
 
 
+def batch_requests(rb, lut, rng, bm_scroll: int, bm_slab: int, slab_shape):
+    """The 64 seeded requests of the batched workload: 16 perspective views of
+    1920x1080 and 24 orthographic slice panes of 960x540 at arbitrary normals
+    over the 1024^3 cache, and 24 slab windows of 3072x3072x32 over the
+    3072x3072x96 slab cache."""
+    persp, panes, slabs = [], [], []
+    for i in range(16):
+        p = rb.orbit_view(float(rng.uniform()), 1920, 1080, lut, step_voxels=STEP_VOXELS,
+                          frame_index=i)
+        p.brick_mode = bm_scroll
+        persp.append(p)
+    for i in range(24):
+        n = rng.normal(size=3)
+        n /= np.linalg.norm(n)
+        up = np.cross(n, [1.0, 0.0, 0.0] if abs(n[0]) < 0.9 else [0.0, 1.0, 0.0])
+        up /= np.linalg.norm(up)
+        rt = np.cross(up, n)
+        p = rb.camera_view(0.0, 0.0, 1.0, 960, 540, lut, step_voxels=STEP_VOXELS, frame_index=i)
+        p.cam_origin[:] = (np.array([0.5, 0.5, 0.5]) - n * 1.0).tolist()
+        p.cam_forward[:] = n.tolist()
+        p.cam_right[:] = (rt * 0.6).tolist()
+        p.cam_up[:] = (up * 0.6 * 540 / 960).tolist()
+        p.view_flags = rb.VIEW_ORTHO | rb.VIEW_OBLIQUE
+        p.slab_z0, p.slab_depth = float(rng.uniform(900, 1100)), 32
+        p.brick_mode = bm_scroll
+        panes.append(p)
+    ext_y = slab_shape[1] / max(slab_shape)
+    for i in range(24):
+        p = rb.camera_view(0.0, 0.0, 1.0, 3072, 3072, lut, step_voxels=STEP_VOXELS, frame_index=i)
+        p.cam_origin[:] = [0.5, 0.5 * ext_y, -0.5]
+        p.cam_forward[:] = [0.0, 0.0, 1.0]
+        p.cam_right[:] = [0.5, 0.0, 0.0]
+        p.cam_up[:] = [0.0, 0.5 * ext_y, 0.0]
+        p.view_flags = rb.VIEW_ORTHO | rb.VIEW_AXIS(0)
+        p.slab_z0, p.slab_depth = float(rng.integers(0, slab_shape[2] - 32)), 32
+        p.brick_mode = bm_slab
+        slabs.append(p)
+    return persp + panes, slabs
+
+
+def batch_bench(rb, torch, local: int, ctx, reps: int) -> dict:
+    """Batched heterogeneous views (64 requests) over two brick caches, each
+    planned as one batch, autotuned, captured into a CUDA graph and timed by
+    graph replay."""
+    dev = f"cuda:{local}"
+    lut = rb.scroll_ramp_tf()
+    slab_shape = (3072, 3072, 96)
+    sctx = rb.Context(local)
+    sctx.set_transfer(lut)
+    sctx.set_alpha_cutoff(CUTOFF)
+    slab = rb.phantom(slab_shape, seed=SEED + 1)
+    sctx.bricks_build(slab, NLEV)
+    del slab
+    rng = np.random.default_rng(SEED)
+    scroll_views, slab_views = batch_requests(rb, lut, rng, ctx.brick_mode, sctx.brick_mode,
+                                              slab_shape)
+    out = {"requests": len(scroll_views) + len(slab_views), "batches": []}
+    total_ms, total_samples = 0.0, 0.0
+    for c, views, name in ((ctx, scroll_views, "1024^3 cache: 16 persp 1080p + 24 ortho panes"),
+                           (sctx, slab_views, "slab cache: 24 windows 3072x3072x32")):
+        imgs = [torch.zeros((v.viewport[1], v.viewport[0], 4), dtype=torch.uint8, device=dev)
+                for v in views]
+        b = rb.Batch(c, views, imgs)
+        sched, tune_ms = b.autotune(reps=2)
+        tot = torch.zeros(1, dtype=torch.int64, device=dev)
+        b.capture(total=tot, stream=c.stream)
+        torch.cuda.synchronize()
+        samples = float(tot.item())
+        st = torch.cuda.ExternalStream(c.stream, device=local)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            b.replay(stream=c.stream)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        rays = sum(v.viewport[0] * v.viewport[1] for v in views)
+        out["batches"].append({"views": name, "schedule": sched, "autotune_ms": tune_ms,
+                               "ms_per_launch": ms, "samples": samples, "rays": rays,
+                               "gsamples_per_s": samples / (ms * 1e-3) / 1e9})
+        total_ms += ms
+        total_samples += samples
+        b.close()
+        del imgs
+    sctx.close()
+    out["ms_per_batch"] = total_ms
+    out["value"] = total_samples / (total_ms * 1e-3) / 1e9
+    out["unit"] = "Gsamples/s"
+    return out
+
+
 def cpu_baseline(rb, orc, vol_pages, lut, frames: list[int], threads: int) -> dict:
     """The oracle (FP32 CPU restatement of the reference shader) on a bounded
     sample of the same workload: whole 1920x1080 frames of the orbit."""
@@ -378,6 +469,10 @@ def run_ours(args) -> None:
     e2e_value = samples_all / float(te.item()) / 1e9
     r.close()
 
+    bt = None
+    if not args.no_batch:
+        bt = batch_bench(rb, torch, local, ctx, reps=5)
+
     fb = None
     if not args.no_fwd_bwd:
         fb = fwd_bwd_bench(rb, ctx, torch, local, steps=20, adam_steps=100)
@@ -413,6 +508,7 @@ def run_ours(args) -> None:
                             "peak_kind": peak_kind,
                             "algorithmic_bytes_per_frame": alg / K},
                "fwd_bwd": fb,
+               "batch": bt,
                "gpu_launches": K,
                "clocks": clk.summary(),
                "cpu_baseline": cpu}
@@ -454,6 +550,7 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fwd-bwd", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--profile", type=int, default=0, metavar="N",
                     help="only build the workload and render N orbit frames (for ncu)")
     ap.add_argument("--profile-mode", type=int, default=0)

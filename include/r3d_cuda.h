@@ -169,6 +169,46 @@ int r3d_cuda_get_schedule(const r3d_cuda_ctx *ctx, r3d_cuda_schedule *sched);
  * (synchronizes the events). */
 int r3d_cuda_last_kernel_ns(r3d_cuda_ctx *ctx, uint64_t *ns);
 
+/* --- batched views ---------------------------------------------------------- */
+
+/* One view of a batch, with its own image: viewport[0] x viewport[1] RGBA8
+ * pixels in device memory, rows of viewport[0] pixels (view_org must be 0).
+ * No counterpart in the reference, which renders at most R3D_MAX_VIEWS panes
+ * into one offscreen image (src/vk/vkbackend.c:7121-7173). */
+typedef struct r3d_cuda_request {
+  r3d_frame_params view;
+  uint8_t *rgba;
+} r3d_cuda_request;
+
+typedef struct r3d_cuda_batch r3d_cuda_batch;
+
+/* Plans a batch of 1..64 requests over the context's scene (all views use
+ * it; requests may differ in size, projection and mode).  The plan keeps
+ * its view table and tile counters in device memory, so its launch reads no
+ * host data: it can be captured into a CUDA graph and replayed. */
+int r3d_cuda_batch_create(r3d_cuda_ctx *ctx, const r3d_cuda_request *reqs, uint32_t n,
+                          r3d_cuda_batch **out);
+void r3d_cuda_batch_destroy(r3d_cuda_batch *batch);
+/* Schedule of the batch's launches (default: persistent, 8x4 tiles). */
+int r3d_cuda_batch_set_schedule(r3d_cuda_batch *batch, const r3d_cuda_schedule *sched);
+int r3d_cuda_batch_get_schedule(const r3d_cuda_batch *batch, r3d_cuda_schedule *sched);
+/* Enqueues the batch on stream (NULL: the context's): one persistent
+ * launch per mode present (one in the common single-mode batch) draining
+ * the tiles of all its views, or one grid per view under a grid schedule.
+ * total_steps (nullable, device) += march iterations. */
+int r3d_cuda_batch_launch(r3d_cuda_batch *batch, unsigned long long *total_steps, void *stream);
+/* Captures r3d_cuda_batch_launch into a CUDA graph owned by the batch
+ * (replacing an earlier one), and launches that graph. */
+int r3d_cuda_batch_capture(r3d_cuda_batch *batch, unsigned long long *total_steps, void *stream);
+int r3d_cuda_batch_replay(r3d_cuda_batch *batch, void *stream);
+/* Autotuner: times every candidate schedule (one thread per ray; persistent
+ * with tile 8x4 / 16x2 / 32x1, refill threshold 8 / 16 / 24, 1 or 2 steps
+ * between refills) over `reps` launches each after a warm-up, keeps the
+ * fastest as the batch's schedule and returns it with its time per launch.
+ * Results are identical under every candidate. */
+int r3d_cuda_batch_autotune(r3d_cuda_batch *batch, uint32_t reps, r3d_cuda_schedule *best,
+                            float *best_ms);
+
 /* --- differentiable render and adjoint --------------------------------------- */
 
 /* No counterpart in the reference: render3d's emission-absorption

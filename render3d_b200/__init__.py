@@ -80,6 +80,10 @@ class Schedule(C.Structure):
                 ("blocks_per_sm", C.c_uint32)]
 
 
+class Request(C.Structure):
+    _fields_ = [("view", FrameParams), ("rgba", C.c_void_p)]
+
+
 class DiffScene(C.Structure):
     _fields_ = [("density", C.c_void_p), ("nx", C.c_uint32), ("ny", C.c_uint32),
                 ("nz", C.c_uint32), ("lut", C.c_void_p)]
@@ -142,6 +146,14 @@ def _load() -> C.CDLL:
         "r3d_cuda_set_schedule": (I, [P, C.POINTER(Schedule)]),
         "r3d_cuda_raycast_fwd_noalloc": (I, [P, P, U32, P, U32, U32, P]),
         "r3d_cuda_diff_forward": (I, [P, C.POINTER(DiffScene), P, U32, P, P, P]),
+        "r3d_cuda_batch_create": (I, [P, P, U32, C.POINTER(P)]),
+        "r3d_cuda_batch_destroy": (None, [P]),
+        "r3d_cuda_batch_set_schedule": (I, [P, C.POINTER(Schedule)]),
+        "r3d_cuda_batch_get_schedule": (I, [P, C.POINTER(Schedule)]),
+        "r3d_cuda_batch_launch": (I, [P, P, P]),
+        "r3d_cuda_batch_capture": (I, [P, P, P]),
+        "r3d_cuda_batch_replay": (I, [P, P]),
+        "r3d_cuda_batch_autotune": (I, [P, U32, C.POINTER(Schedule), C.POINTER(F)]),
         "r3d_cuda_raycast_bwd": (I, [P, C.POINTER(DiffScene), P, U32, P, C.POINTER(Grads), U32,
                                      I, P]),
         "r3d_cuda_get_schedule": (I, [P, C.POINTER(Schedule)]),
@@ -453,6 +465,52 @@ class Context:
         ns = C.c_uint64()
         self._check(lib.r3d_cuda_last_kernel_ns(self.h, C.byref(ns)))
         return ns.value
+
+
+class Batch:
+    """r3d_cuda_batch: many views with their own device images (tensors)."""
+
+    def __init__(self, ctx: Context, views, images):
+        arr = (Request * len(views))(*[Request(v, _ptr(im)) for v, im in zip(views, images)])
+        h = C.c_void_p()
+        ctx._check(lib.r3d_cuda_batch_create(ctx.h, arr, len(views), C.byref(h)))
+        self.ctx, self.h = ctx, h
+
+    def close(self) -> None:
+        if self.h:
+            lib.r3d_cuda_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_schedule(self, **kw) -> None:
+        sc = Schedule(kw.get("persistent", 1), kw.get("refill_min", 16), kw.get("tile_shape", 0),
+                      kw.get("unroll", 1), kw.get("blocks_per_sm", 0))
+        self.ctx._check(lib.r3d_cuda_batch_set_schedule(self.h, C.byref(sc)))
+
+    def schedule(self) -> dict:
+        sc = Schedule()
+        self.ctx._check(lib.r3d_cuda_batch_get_schedule(self.h, C.byref(sc)))
+        return {f: getattr(sc, f) for f, _ in Schedule._fields_}
+
+    def launch(self, total=None, stream: int = 0) -> None:
+        self.ctx._check(lib.r3d_cuda_batch_launch(self.h, _ptr(total) or None, stream or None))
+
+    def capture(self, total=None, stream: int = 0) -> None:
+        self.ctx._check(lib.r3d_cuda_batch_capture(self.h, _ptr(total) or None, stream or None))
+
+    def replay(self, stream: int = 0) -> None:
+        self.ctx._check(lib.r3d_cuda_batch_replay(self.h, stream or None))
+
+    def autotune(self, reps: int = 3) -> tuple[dict, float]:
+        sc = Schedule()
+        ms = C.c_float()
+        self.ctx._check(lib.r3d_cuda_batch_autotune(self.h, reps, C.byref(sc), C.byref(ms)))
+        return {f: getattr(sc, f) for f, _ in Schedule._fields_}, ms.value
 
 
 class Renderer:
