@@ -153,13 +153,18 @@ int r3d_cuda_raycast_fwd_noalloc(r3d_cuda_ctx *ctx, const r3d_frame_params *view
  * have ended whenever at least refill_min lanes are idle; tile_shape 0/1/2
  * = 8x4 / 16x2 / 32x1 rays; unroll = march steps between refill checks
  * (1 or 2); blocks_per_sm = resident 128-thread blocks per SM (0: the
- * occupancy limit).  Results are identical under every schedule. */
+ * occupancy limit).  shade_group (FULL mode, one-thread-per-ray launches):
+ * 0 shades each sample where its ray meets it; n > 0 lets lanes park a
+ * sample that needs gradient shading until n lanes of the warp (or all its
+ * live lanes) wait, and shades them together.  Results are identical under
+ * every schedule. */
 typedef struct r3d_cuda_schedule {
   uint32_t persistent;
   uint32_t refill_min;
   uint32_t tile_shape;
   uint32_t unroll;
   uint32_t blocks_per_sm;
+  uint32_t shade_group;
 } r3d_cuda_schedule;
 
 int r3d_cuda_set_schedule(r3d_cuda_ctx *ctx, const r3d_cuda_schedule *sched);

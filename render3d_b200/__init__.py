@@ -77,7 +77,7 @@ class Schedule(C.Structure):
     """r3d_cuda_schedule: forward launch scheduling (results never change)."""
     _fields_ = [("persistent", C.c_uint32), ("refill_min", C.c_uint32),
                 ("tile_shape", C.c_uint32), ("unroll", C.c_uint32),
-                ("blocks_per_sm", C.c_uint32)]
+                ("blocks_per_sm", C.c_uint32), ("shade_group", C.c_uint32)]
 
 
 class Request(C.Structure):
@@ -452,9 +452,10 @@ class Context:
         return out
 
     def set_schedule(self, persistent: int = 0, refill_min: int = 16, tile_shape: int = 0,
-                     unroll: int = 1, blocks_per_sm: int = 0) -> None:
+                     unroll: int = 1, blocks_per_sm: int = 0, shade_group: int = 0) -> None:
         self._check(lib.r3d_cuda_set_schedule(
-            self.h, C.byref(Schedule(persistent, refill_min, tile_shape, unroll, blocks_per_sm))))
+            self.h, C.byref(Schedule(persistent, refill_min, tile_shape, unroll, blocks_per_sm,
+                                     shade_group))))
 
     def schedule(self) -> dict:
         sc = Schedule()
@@ -489,7 +490,7 @@ class Batch:
 
     def set_schedule(self, **kw) -> None:
         sc = Schedule(kw.get("persistent", 1), kw.get("refill_min", 16), kw.get("tile_shape", 0),
-                      kw.get("unroll", 1), kw.get("blocks_per_sm", 0))
+                      kw.get("unroll", 1), kw.get("blocks_per_sm", 0), kw.get("shade_group", 0))
         self.ctx._check(lib.r3d_cuda_batch_set_schedule(self.h, C.byref(sc)))
 
     def schedule(self) -> dict:

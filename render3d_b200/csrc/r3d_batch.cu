@@ -15,7 +15,7 @@ struct r3d_cuda_batch {
   uint32_t n = 0;
   std::vector<r3d_frame_params> pcs;  // sanitized views
   std::vector<uint8_t *> imgs;
-  r3d_cuda_schedule sched = {1u, 16u, 0u, 1u, 0u};
+  r3d_cuda_schedule sched = {1u, 16u, 0u, 1u, 0u, 0u};
   // per schedule tile shape: device view tables (views grouped by mode)
   DevView *dviews[3] = {nullptr, nullptr, nullptr};
   uint32_t *queue = nullptr;  // one counter per group
@@ -117,7 +117,7 @@ extern "C" void r3d_cuda_batch_destroy(r3d_cuda_batch *b) {
 
 extern "C" int r3d_cuda_batch_set_schedule(r3d_cuda_batch *b, const r3d_cuda_schedule *sc) {
   if (!b || !sc || sc->persistent > 1u || sc->refill_min < 1u || sc->refill_min > 32u ||
-      sc->tile_shape > 2u || (sc->unroll != 1u && sc->unroll != 2u) || sc->blocks_per_sm > 32u)
+      sc->tile_shape > 2u || (sc->unroll != 1u && sc->unroll != 2u) || sc->shade_group > 32u || sc->blocks_per_sm > 32u)
     return batch_fail(b, R3D_E_INVALID, "batch_set_schedule: bad schedule");
   b->sched = *sc;
   return R3D_OK;
@@ -137,8 +137,11 @@ extern "C" int r3d_cuda_batch_launch(r3d_cuda_batch *b, unsigned long long *tota
   const r3d_cuda_schedule &sc = b->sched;
   if (!sc.persistent) {
     for (uint32_t i = 0; i < b->n; i++) {
+      const r3d_cuda_schedule keep = c->sched;
+      c->sched.shade_group = sc.shade_group;
       cudaError_t e = launch_view(c, b->pcs[i], b->imgs[i], b->pcs[i].viewport[0], nullptr,
                                   nullptr, total_steps, nullptr, st);
+      c->sched = keep;
       if (e != cudaSuccess) return cuda_fail(c, e, "batch_launch: grid");
     }
     return R3D_OK;
@@ -218,10 +221,10 @@ extern "C" int r3d_cuda_batch_autotune(r3d_cuda_batch *b, uint32_t reps, r3d_cud
   cudaSetDevice(c->device);
   cudaStream_t st = c->stream;
   std::vector<r3d_cuda_schedule> cands;
-  cands.push_back({0u, 16u, 0u, 1u, 0u});
+  for (uint32_t shade : {0u, 4u, 8u, 16u}) cands.push_back({0u, 16u, 0u, 1u, 0u, shade});
   for (uint32_t shape = 0; shape < 3; shape++)
     for (uint32_t refill : {8u, 16u, 24u})
-      for (uint32_t unroll : {1u, 2u}) cands.push_back({1u, refill, shape, unroll, 0u});
+      for (uint32_t unroll : {1u, 2u}) cands.push_back({1u, refill, shape, unroll, 0u, 0u});
   const r3d_cuda_schedule keep = b->sched;
   float bms = 1e30f;
   r3d_cuda_schedule bsc = keep;

@@ -826,7 +826,7 @@ extern "C" {
 
 int r3d_cuda_set_schedule(r3d_cuda_ctx *c, const r3d_cuda_schedule *sc) {
   if (!c || !sc || sc->persistent > 1u || sc->refill_min < 1u || sc->refill_min > 32u ||
-      sc->tile_shape > 2u || (sc->unroll != 1u && sc->unroll != 2u) ||
+      sc->tile_shape > 2u || (sc->unroll != 1u && sc->unroll != 2u) || sc->shade_group > 32u ||
       sc->blocks_per_sm > 32u)
     return fail(c, R3D_E_INVALID, "set_schedule: bad schedule");
   c->sched = *sc;

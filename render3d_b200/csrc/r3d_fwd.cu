@@ -28,15 +28,22 @@ constexpr uint32_t kBlockW = kFwdWarps >= 2 ? 16u : 8u;  // dispatch threads per
 constexpr uint32_t kBlockH = kFwdWarps == 4 ? 8u : 4u;   // and y
 static_assert(kFwdWarps == 1 || kFwdWarps == 2 || kFwdWarps == 4, "1, 2 or 4 warps");
 
-template <int PATH, int MODE, bool FAST, bool COUNT>
+// DEFER (FULL mode): gradient shading is the long branch of a step and
+// usually only one or two lanes of a warp need it at once.  A lane that
+// reaches a shaded sample parks it (ray_step returns kStepShade); the warp
+// shades the parked samples together once at least shade_min lanes are
+// waiting or every live lane is, so the branch runs with more lanes active.
+// Rays are independent, so each ray's arithmetic and result are unchanged.
+template <int PATH, int MODE, bool FAST, bool COUNT, bool DEFER>
 __global__ void R3D_FWD_BOUNDS k_raycast(const __grid_constant__ r3d_frame_params pc,
-                                                 const __grid_constant__ DevScene s,
-                                                 const uchar4 *__restrict__ lut,
-                                                 uchar4 *__restrict__ img, uint32_t out_w,
-                                                 uint32_t *__restrict__ steps_out,
-                                                 uint32_t *__restrict__ mip_out,
-                                                 unsigned long long *__restrict__ total,
-                                                 unsigned long long *__restrict__ counters) {
+                                         const __grid_constant__ DevScene s,
+                                         const uchar4 *__restrict__ lut,
+                                         uchar4 *__restrict__ img, uint32_t out_w,
+                                         uint32_t *__restrict__ steps_out,
+                                         uint32_t *__restrict__ mip_out,
+                                         unsigned long long *__restrict__ total,
+                                         unsigned long long *__restrict__ counters,
+                                         uint32_t shade_min) {
   __shared__ float4 tf[256];
   for (uint32_t i = threadIdx.x; i < 256u; i += blockDim.x) {
     uchar4 u = lut[i];
@@ -52,10 +59,40 @@ __global__ void R3D_FWD_BOUNDS k_raycast(const __grid_constant__ r3d_frame_param
   const uint32_t px = half ? tx * 2u : tx, py = half ? ty * 2u : ty;
   const uint32_t vw = pc.viewport[0], vh = pc.viewport[1];
   uint32_t my_steps = 0, my_tf = 0, my_grad = 0, my_walk = 0;
-  if (px < vw && py < vh) {
-    const ViewConst vc = view_const<PATH>(pc, s);
-    RayResult r;
+  const bool inside = px < vw && py < vh;
+  const ViewConst vc = view_const<PATH>(pc, s);
+  RayResult r;
+  if (DEFER) {
+    RayState st;
+    Pending pend;
+    bool active = inside && ray_begin<PATH, MODE>(pc, s, vc, px, py, st, r);
+    const bool marched = active;
+    bool parked = false;
+    while (true) {
+      if (__ballot_sync(0xffffffffu, active) == 0u) break;
+      if (active && !parked) {
+        const int rs = ray_step<PATH, MODE, FAST, COUNT, true>(s, vc, tf, st, pend);
+        if (rs == kStepDone)
+          active = false;
+        else if (rs == kStepShade)
+          parked = true;
+      }
+      const uint32_t need = __ballot_sync(0xffffffffu, parked);
+      if (need != 0u) {
+        const uint32_t live = __ballot_sync(0xffffffffu, active);
+        if ((uint32_t)__popc(need) >= shade_min || need == live) {
+          if (parked) {
+            parked = false;
+            if (!composite_sample<PATH, MODE, FAST, COUNT>(s, vc, st, pend)) active = false;
+          }
+        }
+      }
+    }
+    if (marched) ray_end<MODE>(vc, st, r);
+  } else if (inside) {
     march<PATH, MODE, FAST, COUNT>(pc, s, vc, tf, px, py, r);
+  }
+  if (inside) {
     my_tf = r.n_tf;
     my_grad = r.n_grad;
     my_walk = r.n_walk;
@@ -93,18 +130,27 @@ template <int PATH, int MODE, bool FAST>
 static cudaError_t launch_t(const r3d_frame_params &pc, const DevScene &s, const uchar4 *lut,
                             uint8_t *img, uint32_t out_w, uint32_t *steps, uint32_t *mip,
                             unsigned long long *total, unsigned long long *counters,
-                            cudaStream_t stream) {
+                            uint32_t shade, cudaStream_t stream) {
   const bool half = (pc.view_flags & R3D_VIEW_HALF) != 0u;
   uint32_t gw = half ? (pc.viewport[0] + 1u) / 2u : pc.viewport[0];
   uint32_t gh = half ? (pc.viewport[1] + 1u) / 2u : pc.viewport[1];
   dim3 grid((gw + kBlockW - 1u) / kBlockW, (gh + kBlockH - 1u) / kBlockH);
   const uint32_t threads = kFwdWarps * 32u;
-  if (counters)
-    k_raycast<PATH, MODE, FAST, true><<<grid, threads, 0, stream>>>(
-        pc, s, lut, (uchar4 *)img, out_w, steps, mip, total, counters);
-  else
-    k_raycast<PATH, MODE, FAST, false><<<grid, threads, 0, stream>>>(
-        pc, s, lut, (uchar4 *)img, out_w, steps, mip, total, nullptr);
+  constexpr bool kDeferable = MODE == R3D_MODE_FULL;
+  if (kDeferable && shade) {
+    if (counters)
+      k_raycast<PATH, MODE, FAST, true, kDeferable><<<grid, threads, 0, stream>>>(
+          pc, s, lut, (uchar4 *)img, out_w, steps, mip, total, counters, shade);
+    else
+      k_raycast<PATH, MODE, FAST, false, kDeferable><<<grid, threads, 0, stream>>>(
+          pc, s, lut, (uchar4 *)img, out_w, steps, mip, total, nullptr, shade);
+  } else if (counters) {
+    k_raycast<PATH, MODE, FAST, true, false><<<grid, threads, 0, stream>>>(
+        pc, s, lut, (uchar4 *)img, out_w, steps, mip, total, counters, 0u);
+  } else {
+    k_raycast<PATH, MODE, FAST, false, false><<<grid, threads, 0, stream>>>(
+        pc, s, lut, (uchar4 *)img, out_w, steps, mip, total, nullptr, 0u);
+  }
   return cudaGetLastError();
 }
 
@@ -112,25 +158,22 @@ template <int PATH>
 static cudaError_t launch_p(const r3d_frame_params &pc, const DevScene &s, bool fast,
                             const uchar4 *lut, uint8_t *img, uint32_t out_w, uint32_t *steps,
                             uint32_t *mip, unsigned long long *total,
-                            unsigned long long *cnt, cudaStream_t st) {
+                            unsigned long long *cnt, uint32_t shade, cudaStream_t st) {
   switch (pc.mode) {
     case R3D_MODE_FULL:
-      return fast ? launch_t<PATH, R3D_MODE_FULL, true>(pc, s, lut, img, out_w, steps, mip, total, cnt,
-                                                        st)
+      return fast ? launch_t<PATH, R3D_MODE_FULL, true>(pc, s, lut, img, out_w, steps, mip, total, cnt, shade, st)
                   : launch_t<PATH, R3D_MODE_FULL, false>(pc, s, lut, img, out_w, steps, mip,
-                                                         total, cnt, st);
+                                                         total, cnt, shade, st);
     case R3D_MODE_MIP:
-      return launch_t<PATH, R3D_MODE_MIP, false>(pc, s, lut, img, out_w, steps, mip, total, cnt, st);
+      return launch_t<PATH, R3D_MODE_MIP, false>(pc, s, lut, img, out_w, steps, mip, total, cnt, shade, st);
     case R3D_MODE_DEPTH:
-      return launch_t<PATH, R3D_MODE_DEPTH, false>(pc, s, lut, img, out_w, steps, mip, total, cnt, st);
+      return launch_t<PATH, R3D_MODE_DEPTH, false>(pc, s, lut, img, out_w, steps, mip, total, cnt, shade, st);
     case R3D_MODE_HEATMAP:
-      return launch_t<PATH, R3D_MODE_HEATMAP, false>(pc, s, lut, img, out_w, steps, mip, total, cnt,
-                                                     st);
+      return launch_t<PATH, R3D_MODE_HEATMAP, false>(pc, s, lut, img, out_w, steps, mip, total, cnt, shade, st);
     case R3D_MODE_RAYDIR:
-      return launch_t<PATH, R3D_MODE_RAYDIR, false>(pc, s, lut, img, out_w, steps, mip, total, cnt,
-                                                    st);
+      return launch_t<PATH, R3D_MODE_RAYDIR, false>(pc, s, lut, img, out_w, steps, mip, total, cnt, shade, st);
     default:
-      return launch_t<PATH, R3D_MODE_FLAT, false>(pc, s, lut, img, out_w, steps, mip, total, cnt, st);
+      return launch_t<PATH, R3D_MODE_FLAT, false>(pc, s, lut, img, out_w, steps, mip, total, cnt, shade, st);
   }
 }
 
@@ -140,11 +183,12 @@ cudaError_t launch_view(const r3d_cuda_ctx *c, const r3d_frame_params &pc, uint8
                         cudaStream_t stream) {
   DevScene s = c->scene();
   bool fast = c->quality == R3D_QUALITY_FAST;
+  const uint32_t shade = c->sched.shade_group;
   if (pc.brick_mode != 0u)
     return launch_p<PATH_LOD_BRICKS>(pc, s, fast, c->lut, img, out_w, steps, mip_index, total,
-                                     counters, stream);
+                                     counters, shade, stream);
   return launch_p<PATH_CUBE>(pc, s, fast, c->lut, img, out_w, steps, mip_index, total, counters,
-                             stream);
+                             shade, stream);
 }
 
 }  // namespace r3d

@@ -57,7 +57,7 @@ struct r3d_cuda_ctx {
   // forward scheduling and the view-table ring of persistent launches:
   // slot k holds one call's views (pinned host copy + device copy) and its
   // tile counters; ring_ev[k] completes once the slot's upload has run
-  r3d_cuda_schedule sched = {0u, 16u, 0u, 1u, 0u};
+  r3d_cuda_schedule sched = {0u, 16u, 0u, 1u, 0u, 0u};
   static constexpr int kRing = 4;
   r3d::DevView *ring_host = nullptr;
   r3d::DevView *ring_dev = nullptr;

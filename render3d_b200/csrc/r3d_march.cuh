@@ -381,6 +381,18 @@ __device__ __forceinline__ ViewConst view_const(const r3d_frame_params &pc, cons
   return v;
 }
 
+enum { kStepDone = 0, kStepCont = 1, kStepShade = 2 };
+
+// A contributing sample waiting for gradient shading and compositing.
+struct Pending {
+  float3 p;
+  float lod, lod_step, a;
+  float4 sm;  // TF sample
+  uint32_t slot;
+  float3 bl;
+  float grad_vox;
+};
+
 // State of one ray between march steps.
 struct RayState {
   float3 ro, dir;  // volume space
@@ -537,17 +549,103 @@ __device__ __forceinline__ float skip_block(const RayState &st, float3 p, float 
   return fmaxf(fminf(fminf(tex[0], tex[1]), tex[2]), st.t) + bsz * 0.01f;
 }
 
-// One iteration of the hot loop (raycast.slang:767-1021).  Returns false
-// when the ray is finished (loop condition failed, saturation or opacity
-// cutoff).
+// Gradient shading (FULL mode, raycast.slang:919-998) and front-to-back
+// compositing (:1015-1017) of a contributing sample, then the step advance
+// (:1020).  Returns false when the opacity cutoff ends the ray.
 template <int PATH, int MODE, bool FAST, bool COUNT>
-__device__ __forceinline__ bool ray_step(const DevScene &s, const ViewConst &vc,
-                                         const float4 *tf, RayState &st) {
+__device__ __forceinline__ bool composite_sample(const DevScene &s, const ViewConst &vc,
+                                                 RayState &st, const Pending &q) {
+  constexpr bool kLod = PATH == PATH_LOD_BRICKS;
+  constexpr bool kShaded = MODE == R3D_MODE_FULL;
+  const float3 dir = st.dir;
+  float col_r = q.sm.x, col_g = q.sm.y, col_b = q.sm.z;
+  if (kShaded) {
+    if (COUNT) st.n_grad++;
+    float g0, g1, g2;
+    if (FAST) {  // raycast.slang:919-955
+      const float ir3 = 0.57735026919f, renorm = 0.86602540378f;
+      float q0, q1, q2, q3;
+      if (kLod) {
+        float ev = q.grad_vox * ir3;
+        float3 u = q.bl;
+        q0 = brick_fetch(s, q.slot, make_float3(u.x + ev, u.y - ev, u.z - ev));
+        q1 = brick_fetch(s, q.slot, make_float3(u.x - ev, u.y - ev, u.z + ev));
+        q2 = brick_fetch(s, q.slot, make_float3(u.x - ev, u.y + ev, u.z - ev));
+        q3 = brick_fetch(s, q.slot, make_float3(u.x + ev, u.y + ev, u.z + ev));
+      } else {
+        float ee = (vc.voxel * q.lod_step) * ir3;
+        q0 = cube_sample(s.cube, make_float3(q.p.x + ee, q.p.y - ee, q.p.z - ee), q.lod);
+        q1 = cube_sample(s.cube, make_float3(q.p.x - ee, q.p.y - ee, q.p.z + ee), q.lod);
+        q2 = cube_sample(s.cube, make_float3(q.p.x - ee, q.p.y + ee, q.p.z - ee), q.lod);
+        q3 = cube_sample(s.cube, make_float3(q.p.x + ee, q.p.y + ee, q.p.z + ee), q.lod);
+      }
+      g0 = (((q0 - q1) - q2) + q3) * renorm;
+      g1 = (((-q0 - q1) + q2) + q3) * renorm;
+      g2 = (((-q0 + q1) - q2) + q3) * renorm;
+    } else {  // raycast.slang:957-986
+      if (kLod) {
+        float ev = q.grad_vox;
+        float3 u = q.bl;
+        g0 = brick_fetch(s, q.slot, make_float3(u.x + ev, u.y, u.z)) -
+             brick_fetch(s, q.slot, make_float3(u.x - ev, u.y, u.z));
+        g1 = brick_fetch(s, q.slot, make_float3(u.x, u.y + ev, u.z)) -
+             brick_fetch(s, q.slot, make_float3(u.x, u.y - ev, u.z));
+        g2 = brick_fetch(s, q.slot, make_float3(u.x, u.y, u.z + ev)) -
+             brick_fetch(s, q.slot, make_float3(u.x, u.y, u.z - ev));
+      } else {
+        float e = vc.voxel * q.lod_step;
+        g0 = cube_sample(s.cube, make_float3(q.p.x + e, q.p.y, q.p.z), q.lod) -
+             cube_sample(s.cube, make_float3(q.p.x - e, q.p.y, q.p.z), q.lod);
+        g1 = cube_sample(s.cube, make_float3(q.p.x, q.p.y + e, q.p.z), q.lod) -
+             cube_sample(s.cube, make_float3(q.p.x, q.p.y - e, q.p.z), q.lod);
+        g2 = cube_sample(s.cube, make_float3(q.p.x, q.p.y, q.p.z + e), q.lod) -
+             cube_sample(s.cube, make_float3(q.p.x, q.p.y, q.p.z - e), q.lod);
+      }
+    }
+    float3 gv = make_float3(g0, g1, g2);
+    float gm = sqrtf(dot3(gv, gv));
+    if (gm > 1e-4f) {  // raycast.slang:988-998
+      // key light, headlight l = -dir and its half vector normalize(l - dir)
+      const float3 key = norm3(make_float3(0.4f, 0.8f, -0.4f));
+      const float3 l = make_float3(-dir.x, -dir.y, -dir.z);
+      const float3 hv = norm3(make_float3(l.x - dir.x, l.y - dir.y, l.z - dir.z));
+      float inv = 1.0f / gm;
+      float3 n = make_float3(gv.x * inv, gv.y * inv, gv.z * inv);
+      float diff = fmaf(0.3f, fabsf(dot3(n, key)), 0.7f * fabsf(dot3(n, l)));
+      float spec = r3d_powi24f(fabsf(dot3(n, hv))) * 0.3f;
+      float lit = fmaf(0.75f, diff, 0.25f);
+      float w = sat_(gm * 6.0f);
+      float lm = fmaf(w, lit - 1.0f, 1.0f);
+      float sw = spec * w;
+      col_r = fmaf(col_r, lm, sw);
+      col_g = fmaf(col_g, lm, sw);
+      col_b = fmaf(col_b, lm, sw);
+    }
+  }
+  // front-to-back compositing (raycast.slang:1015-1017)
+  float wgt = (1.0f - st.acc_a) * q.a;
+  st.acc_r = fmaf(wgt, col_r, st.acc_r);
+  st.acc_g = fmaf(wgt, col_g, st.acc_g);
+  st.acc_b = fmaf(wgt, col_b, st.acc_b);
+  st.acc_a = st.acc_a + wgt;
+  if (st.acc_a >= s.alpha_cutoff) return false;
+  st.t = fmaf(vc.dt, q.lod_step, st.t);
+  return true;
+}
+
+// One iteration of the hot loop (raycast.slang:767-1021).  Returns
+// kStepDone when the ray is finished (loop condition failed, saturation or
+// opacity cutoff) and kStepCont otherwise.  With DEFER, a sample that needs
+// gradient shading stops before it: the sample is left in pend and
+// kStepShade returned; composite_sample(pend) completes the iteration.
+template <int PATH, int MODE, bool FAST, bool COUNT, bool DEFER = false>
+__device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, const float4 *tf,
+                                        RayState &st, Pending &pend) {
   constexpr bool kLod = PATH == PATH_LOD_BRICKS;
   constexpr bool kComposite = MODE == R3D_MODE_FULL || MODE == R3D_MODE_FLAT;
   constexpr bool kShaded = MODE == R3D_MODE_FULL;
   constexpr uint32_t ray_budget = kLod ? (kShaded ? 192u : 256u) : kMaxSteps;
-  if (!(st.t < st.tf_ && st.steps < ray_budget)) return false;
+  if (!(st.t < st.tf_ && st.steps < ray_budget)) return kStepDone;
   st.steps++;
   const float t = st.t;
   // LOD and step (raycast.slang:772-779)
@@ -594,7 +692,7 @@ __device__ __forceinline__ bool ray_step(const DevScene &s, const ViewConst &vc,
           st.t = skip_block(st, p, b.world_brick);
         else
           st.t = fmaf(vc.dt, lod_step, t);
-        return true;
+        return kStepCont;
       }
       v = tri_slot_at(s.br.pool + (size_t)b.slot * (128u * 128u * 128u), q);
     }
@@ -609,18 +707,18 @@ __device__ __forceinline__ bool ray_step(const DevScene &s, const ViewConst &vc,
     if ((MODE == R3D_MODE_MIP && b.ok && b.maxv <= st.mip_max) ||
         (v < vc.bgate && b.maxv < vc.bgate)) {
       st.t = skip_block(st, p, b.world_brick);
-      return true;
+      return kStepCont;
     }
   } else if (v < vc.occ_gate && occ_sample(s.cube, p) < vc.occ_gate) {
     st.t = skip_block(st, p, vc.bs);
-    return true;
+    return kStepCont;
   }
 
   if (v > st.mip_max) {
     st.mip_max = v;
     st.mip_index = st.steps;
   }
-  if (MODE == R3D_MODE_MIP && st.mip_max >= 0.999f) return false;
+  if (MODE == R3D_MODE_MIP && st.mip_max >= 0.999f) return kStepDone;
   if (MODE == R3D_MODE_DEPTH && st.first_hit < 0.0f && v > 0.05f) st.first_hit = t;
 
   if (kComposite && !cut) {
@@ -632,82 +730,17 @@ __device__ __forceinline__ bool ray_step(const DevScene &s, const ViewConst &vc,
       float4 sm = tf_sample(tf, tt);
       float a = 1.0f - r3d_powf(1.0f - sm.w, vc.opac_k * lod_step);
       if (a > 0.003f) {
-        float col_r = sm.x, col_g = sm.y, col_b = sm.z;
-        if (kShaded) {
-          if (COUNT) st.n_grad++;
-          float g0, g1, g2;
-          if (FAST) {  // raycast.slang:919-955
-            const float ir3 = 0.57735026919f, renorm = 0.86602540378f;
-            float q0, q1, q2, q3;
-            if (kLod) {
-              float ev = b.grad_vox * ir3;
-              float3 u = b.bl;
-              q0 = brick_fetch(s, b.slot, make_float3(u.x + ev, u.y - ev, u.z - ev));
-              q1 = brick_fetch(s, b.slot, make_float3(u.x - ev, u.y - ev, u.z + ev));
-              q2 = brick_fetch(s, b.slot, make_float3(u.x - ev, u.y + ev, u.z - ev));
-              q3 = brick_fetch(s, b.slot, make_float3(u.x + ev, u.y + ev, u.z + ev));
-            } else {
-              float ee = (vc.voxel * lod_step) * ir3;
-              q0 = cube_sample(s.cube, make_float3(p.x + ee, p.y - ee, p.z - ee), lod);
-              q1 = cube_sample(s.cube, make_float3(p.x - ee, p.y - ee, p.z + ee), lod);
-              q2 = cube_sample(s.cube, make_float3(p.x - ee, p.y + ee, p.z - ee), lod);
-              q3 = cube_sample(s.cube, make_float3(p.x + ee, p.y + ee, p.z + ee), lod);
-            }
-            g0 = (((q0 - q1) - q2) + q3) * renorm;
-            g1 = (((-q0 - q1) + q2) + q3) * renorm;
-            g2 = (((-q0 + q1) - q2) + q3) * renorm;
-          } else {  // raycast.slang:957-986
-            if (kLod) {
-              float ev = b.grad_vox;
-              float3 u = b.bl;
-              g0 = brick_fetch(s, b.slot, make_float3(u.x + ev, u.y, u.z)) -
-                   brick_fetch(s, b.slot, make_float3(u.x - ev, u.y, u.z));
-              g1 = brick_fetch(s, b.slot, make_float3(u.x, u.y + ev, u.z)) -
-                   brick_fetch(s, b.slot, make_float3(u.x, u.y - ev, u.z));
-              g2 = brick_fetch(s, b.slot, make_float3(u.x, u.y, u.z + ev)) -
-                   brick_fetch(s, b.slot, make_float3(u.x, u.y, u.z - ev));
-            } else {
-              float e = vc.voxel * lod_step;
-              g0 = cube_sample(s.cube, make_float3(p.x + e, p.y, p.z), lod) -
-                   cube_sample(s.cube, make_float3(p.x - e, p.y, p.z), lod);
-              g1 = cube_sample(s.cube, make_float3(p.x, p.y + e, p.z), lod) -
-                   cube_sample(s.cube, make_float3(p.x, p.y - e, p.z), lod);
-              g2 = cube_sample(s.cube, make_float3(p.x, p.y, p.z + e), lod) -
-                   cube_sample(s.cube, make_float3(p.x, p.y, p.z - e), lod);
-            }
-          }
-          float3 gv = make_float3(g0, g1, g2);
-          float gm = sqrtf(dot3(gv, gv));
-          if (gm > 1e-4f) {  // raycast.slang:988-998
-            // key light, headlight l = -dir and its half vector normalize(l - dir)
-            const float3 key = norm3(make_float3(0.4f, 0.8f, -0.4f));
-            const float3 l = make_float3(-dir.x, -dir.y, -dir.z);
-            const float3 hv = norm3(make_float3(l.x - dir.x, l.y - dir.y, l.z - dir.z));
-            float inv = 1.0f / gm;
-            float3 n = make_float3(gv.x * inv, gv.y * inv, gv.z * inv);
-            float diff = fmaf(0.3f, fabsf(dot3(n, key)), 0.7f * fabsf(dot3(n, l)));
-            float spec = r3d_powi24f(fabsf(dot3(n, hv))) * 0.3f;
-            float lit = fmaf(0.75f, diff, 0.25f);
-            float w = sat_(gm * 6.0f);
-            float lm = fmaf(w, lit - 1.0f, 1.0f);
-            float sw = spec * w;
-            col_r = fmaf(col_r, lm, sw);
-            col_g = fmaf(col_g, lm, sw);
-            col_b = fmaf(col_b, lm, sw);
-          }
+        const Pending q = {p, lod, lod_step, a, sm, b.slot, b.bl, b.grad_vox};
+        if (DEFER && kShaded) {  // shading runs later, grouped across the warp
+          pend = q;
+          return kStepShade;
         }
-        // front-to-back compositing (raycast.slang:1015-1017)
-        float wgt = (1.0f - st.acc_a) * a;
-        st.acc_r = fmaf(wgt, col_r, st.acc_r);
-        st.acc_g = fmaf(wgt, col_g, st.acc_g);
-        st.acc_b = fmaf(wgt, col_b, st.acc_b);
-        st.acc_a = st.acc_a + wgt;
-        if (st.acc_a >= s.alpha_cutoff) return false;
+        return composite_sample<PATH, MODE, FAST, COUNT>(s, vc, st, q) ? kStepCont : kStepDone;
       }
     }
   }
   st.t = fmaf(vc.dt, lod_step, t);  // raycast.slang:1020
-  return true;
+  return kStepCont;
 }
 
 // Final colour of a marched ray (raycast.slang:1023-1038).
@@ -744,8 +777,9 @@ __device__ __forceinline__ void march(const r3d_frame_params &pc, const DevScene
                                       const ViewConst &vc, const float4 *tf, uint32_t px,
                                       uint32_t py, RayResult &out) {
   RayState st;
+  Pending pend;
   if (!ray_begin<PATH, MODE>(pc, s, vc, px, py, st, out)) return;
-  while (ray_step<PATH, MODE, FAST, COUNT>(s, vc, tf, st)) {
+  while (ray_step<PATH, MODE, FAST, COUNT>(s, vc, tf, st, pend) != kStepDone) {
   }
   ray_end<MODE>(vc, st, out);
 }

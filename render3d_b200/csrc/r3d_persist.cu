@@ -163,7 +163,8 @@ __global__ void __launch_bounds__(128) k_raycast_persist(
       const ViewConst &vc = vcs[my_view];
 #pragma unroll
       for (int u = 0; u < UNROLL; u++) {
-        if (!ray_step<PATH, MODE, FAST, COUNT>(s, vc, tf, st)) {
+        Pending pend;
+        if (ray_step<PATH, MODE, FAST, COUNT>(s, vc, tf, st, pend) == kStepDone) {
           RayResult r;
           ray_end<MODE>(vc, st, r);
           store_ray<MODE>(views[my_view], my_px, my_py, r, steps_out, mip_out);

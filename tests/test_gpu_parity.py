@@ -54,7 +54,9 @@ def test_cube_builders_bit_exact(ctx, cube256):
     assert np.array_equal(ctx.cube_read(-1), cube256.occ)
 
 
-SCHEDULES = {"grid": dict(persistent=0), "persist": dict(persistent=1, refill_min=8),
+SCHEDULES = {"grid": dict(persistent=0), "grid_shade8": dict(persistent=0, shade_group=8),
+             "grid_shade32": dict(persistent=0, shade_group=32),
+             "persist": dict(persistent=1, refill_min=8),
              "persist_16x2_u2": dict(persistent=1, refill_min=4, tile_shape=1, unroll=2),
              "persist_32x1": dict(persistent=1, refill_min=24, tile_shape=2, unroll=1)}
 
