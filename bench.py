@@ -540,6 +540,98 @@ def run_profile(args) -> None:
     ctx.close()
 
 
+def run_sparse(args) -> None:
+    """The large-volume workload: a 2048^3 phantom (8 GiB, generated on the
+    device) with only the bricks whose maximum exceeds 40 resident, rendered
+    at 3840x2160 with LOD bias 0 and 1; and the adjoint at 512^3 FP32, 16
+    views of 512x512, step 0.25, checkpoints every 32 / 64 / 128 samples,
+    deterministic and atomic accumulation."""
+    import torch
+    import render3d_b200 as rb
+    lut = rb.scroll_ramp_tf()
+    ctx = rb.Context(0)
+    ctx.set_transfer(lut)
+    ctx.set_alpha_cutoff(CUTOFF)
+    t0 = time.perf_counter()
+    vol = ctx.phantom(2048, seed=SEED)
+    ctx.bricks_build(vol, NLEV, min_max=41)
+    del vol
+    torch.cuda.empty_cache()
+    build_s = time.perf_counter() - t0
+    info = ctx.bricks_info()
+    total_bricks = sum(((2048 >> l) // 128) ** 3 for l in range(NLEV))
+    img = torch.zeros((2160, 3840, 4), dtype=torch.uint8, device="cuda")
+    tot = torch.zeros(1, dtype=torch.int64, device="cuda")
+    st = torch.cuda.ExternalStream(ctx.stream)
+    out = {"workload": "sparse 2048^3 (bricks with max > 40 resident), 3840x2160, full shading",
+           "resident_bricks": info["nslots"], "total_bricks": total_bricks,
+           "resident_fraction": info["nslots"] / total_bricks, "build_s": build_s}
+    K = max(args.steps // 10, 20)
+    for bias in (0.0, 1.0):
+        def frame(i):
+            p = rb.orbit_view((i % ORBIT_FRAMES) / ORBIT_FRAMES, 3840, 2160, lut,
+                              step_voxels=STEP_VOXELS, lod_bias=bias, frame_index=i)
+            p.brick_mode = ctx.brick_mode
+            ctx.raycast(p, 3840, 2160, out=img, total=tot, stream=ctx.stream)
+        for i in range(10):
+            frame(i)
+        torch.cuda.synchronize()
+        tot.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for i in range(K):
+            frame(i)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / K
+        out[f"lod_bias_{int(bias)}"] = {"ms_per_frame": ms, "fps": 1000.0 / ms,
+                                        "gsamples_per_s": tot.item() / K / (ms * 1e-3) / 1e9}
+    ctx.close()
+    # adjoint at 512^3
+    ctx = rb.Context(0)
+    ctx.set_alpha_cutoff(0.98)
+    n, nv, w = 512, 16, 512
+    dens = ctx.phantom(n, seed=SEED).float().div_(255.0)
+    g = torch.Generator(device="cuda").manual_seed(SEED)
+    dens.add_(torch.randn(dens.shape, device="cuda", generator=g) * (10.0 / 255.0))
+    flut = torch.tensor(lut.astype(np.float32) / 255.0, device="cuda")
+    views = [rb.orbit_view(i / nv, w, w, lut, step_voxels=0.25, frame_index=i) for i in range(nv)]
+    for v in views:
+        v.max_mip = 0.0
+    nf = nv * w * w * 3
+    rgb = torch.empty(nf, device="cuda")
+    tot.zero_()
+    st = torch.cuda.ExternalStream(ctx.stream)
+    ctx.diff_forward(dens, flut, views, rgb, total=tot, stream=ctx.stream)
+    torch.cuda.synchronize()
+    samples = tot.item()
+    grad = torch.randn(nf, device="cuda", generator=g)
+    gd = torch.empty_like(dens)
+    gl = torch.empty_like(flut)
+    gs = torch.empty(1, device="cuda")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(3):
+        ctx.diff_forward(dens, flut, views, rgb, stream=ctx.stream)
+    e1.record(st)
+    torch.cuda.synchronize()
+    bwd = {"samples_per_pass": samples, "max_steps_per_ray": None,
+           "fwd_ms": e0.elapsed_time(e1) / 3}
+    for k in (32, 64, 128):
+        for det in (False, True):
+            ctx.raycast_bwd(dens, flut, views, grad, gd, gl, gs, k, det, stream=ctx.stream)
+            e0.record(st)
+            for _ in range(3):
+                ctx.raycast_bwd(dens, flut, views, grad, gd, gl, gs, k, det, stream=ctx.stream)
+            e1.record(st)
+            torch.cuda.synchronize()
+            bwd[f"bwd_k{k}_{'det' if det else 'atomic'}_ms"] = e0.elapsed_time(e1) / 3
+    out["adjoint_512"] = bwd
+    ctx.close()
+    print(json.dumps(out), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -551,6 +643,8 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fwd-bwd", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--workload", default="orbit1024", choices=["orbit1024", "sparse2048"],
+                    help="sparse2048: the large sparse volume and 512^3 adjoint (extra line)")
     ap.add_argument("--profile", type=int, default=0, metavar="N",
                     help="only build the workload and render N orbit frames (for ncu)")
     ap.add_argument("--profile-mode", type=int, default=0)
@@ -563,6 +657,8 @@ def main() -> None:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "sparse2048":
+        run_sparse(args)
     else:
         run_ours(args)
 

@@ -81,6 +81,14 @@ void r3d_host_phantom_default(uint32_t n, uint64_t seed, r3d_phantom_desc *d);
 int r3d_host_phantom(uint8_t *vox, uint32_t nx, uint32_t ny, uint32_t nz,
                      const r3d_phantom_desc *d, int threads);
 
+/* The same construction generated on the context's device into device
+ * memory vox (nx*ny*nz); synchronizes.  CUDA's double-precision log / sin /
+ * cos replace glibc's, so rare voxels on a rounding or sheet boundary may
+ * differ from r3d_host_phantom's. */
+struct r3d_cuda_ctx;
+int r3d_cuda_phantom(struct r3d_cuda_ctx *ctx, const r3d_phantom_desc *d, uint32_t nx,
+                     uint32_t ny, uint32_t nz, uint8_t *vox, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -190,6 +190,7 @@ def _load() -> C.CDLL:
                                        U32, F, P]),
         "r3d_host_phantom_default": (None, [U32, C.c_uint64, C.POINTER(PhantomDesc)]),
         "r3d_host_phantom": (I, [P, U32, U32, U32, C.POINTER(PhantomDesc), I]),
+        "r3d_cuda_phantom": (I, [P, C.POINTER(PhantomDesc), U32, U32, U32, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -442,6 +443,18 @@ class Context:
         self._check(lib.r3d_cuda_raycast_bwd(self.h, C.byref(sc), arr, len(views),
                                              _ptr(dl_drgb), C.byref(gr), ckpt_k,
                                              int(deterministic), stream or None))
+
+    def phantom(self, shape, seed: int = 1234, out=None):
+        """Seeded scroll phantom generated on the device: a (nz, ny, nx) uint8
+        CUDA tensor (allocated with torch when out is None)."""
+        import torch
+        nx, ny, nz = (shape, shape, shape) if isinstance(shape, int) else shape
+        d = PhantomDesc()
+        lib.r3d_host_phantom_default(max(nx, ny, nz), seed, C.byref(d))
+        if out is None:
+            out = torch.empty((nz, ny, nx), dtype=torch.uint8, device="cuda")
+        self._check(lib.r3d_cuda_phantom(self.h, C.byref(d), nx, ny, nz, _ptr(out), None))
+        return out
 
     def fmath_eval(self, x: np.ndarray, y: np.ndarray) -> np.ndarray:
         """Device log2, exp2, pow and x^24 of the inputs, (n, 4) float32."""
