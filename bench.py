@@ -42,6 +42,10 @@ CUTOFF = 0.99
 STEP_VOXELS = 0.5
 ORBIT_FRAMES = 120
 WORKLOAD = "scroll phantom 1024^3 u8, 128^3 bricks x 4 LOD levels, 1920x1080 full shading"
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_raycast
+# launch of this workload, mean of launches 3 and 4 of one ncu capture of
+# `python bench.py --profile 6` (orbit phases 2/120 and 3/120).
+FWD_DRAM_TRAFFIC_BYTES = 154.3e6
 METRIC = "raycast Gsamples/s & fps @1024^3 1080p; fwd+bwd Gsamples/s vs plain, same GPU"
 
 
@@ -141,6 +145,36 @@ def algorithmic_bytes(cnt: np.ndarray, pixels: int) -> float:
     per page-table walk and 4 per output pixel."""
     samples, tf, grad, walks = (float(x) for x in cnt)
     return 8.0 * samples + 48.0 * grad + 8.0 * tf + 4.0 * walks + 4.0 * pixels
+
+
+def mode_stats(rb, ctx, lut, torch, stream, total, img, frames: int) -> dict:
+    """Per-frame CUDA-event times (p50/p95/p99, like render3d's frame stats)
+    and Gsamples/s of the orbit in FULL, MIP and HEATMAP modes, each after
+    its own warm-up; each frame is bracketed by its own pair of events on the
+    launching stream."""
+    out = {}
+    for name, mode in (("full", 0), ("mip", 1), ("heatmap", 3)):
+        def frame(i):
+            ctx.raycast(orbit_params(rb, lut, i, ctx.brick_mode, mode), W, H, out=img,
+                        total=total, stream=ctx.stream)
+        for i in range(32):
+            frame(i)
+        torch.cuda.synchronize()
+        total.zero_()
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(frames)]
+        for i, (a, b) in enumerate(ev):
+            a.record(stream)
+            frame(i)
+            b.record(stream)
+        torch.cuda.synchronize()
+        t = np.array([a.elapsed_time(b) for a, b in ev])
+        out[name] = {"frames": frames, "p50_ms": float(np.percentile(t, 50)),
+                     "p95_ms": float(np.percentile(t, 95)),
+                     "p99_ms": float(np.percentile(t, 99)),
+                     "gsamples_per_s": float(total.item()) / (t.sum() * 1e-3) / 1e9}
+    return out
 
 
 def fwd_bwd_bench(rb, ctx, torch, local: int, steps: int, adam_steps: int) -> dict:
@@ -331,8 +365,8 @@ def cpu_baseline(rb, orc, vol_pages, lut, frames: list[int], threads: int) -> di
     dt = time.perf_counter() - t0
     return {"value": total / dt / 1e9, "unit": "Gsamples/s", "cores": threads, "kind": "port",
             "sample": f"{len(frames)} full 1920x1080 orbit frames (phases "
-                      f"{', '.join(str(i) for i in frames)} of 120), {total} samples, "
-                      f"{dt:.1f} s", "fps": len(frames) / dt}
+                      f"{frames[0]}..{frames[-1]} step {frames[1] - frames[0] if len(frames) > 1 else 0}"
+                      f" of 120), {total} samples, {dt:.1f} s", "fps": len(frames) / dt}
 
 
 def run_reference(args) -> None:
@@ -444,6 +478,8 @@ def run_ours(args) -> None:
     fps = K * world / (ms_max * 1e-3)
 
     # end to end through the render3d-facing API: r3d_frame + r3d_read_frame
+    modes = mode_stats(rb, ctx, lut, torch, stream, total, img, ORBIT_FRAMES * 2)
+
     r = rb.Renderer(W, H)
     r.set_transfer(lut)
     r.set_alpha_cutoff(CUTOFF)
@@ -487,7 +523,7 @@ def run_ours(args) -> None:
         if world == 1 and not args.no_cpu_baseline:
             import oracle as orc
             page, pool = ctx.bricks_read()
-            cpu = cpu_baseline(rb, orc, (page, pool, bm), lut, [0, 30],
+            cpu = cpu_baseline(rb, orc, (page, pool, bm), lut, list(range(0, ORBIT_FRAMES, 4)),
                                os.cpu_count() or 1)
             del pool
         out = {"metric": METRIC, "value": value,
@@ -504,9 +540,11 @@ def run_ours(args) -> None:
                "e2e": {"value": e2e_value, "unit": "Gsamples/s", "h2d_bytes_per_step": 248,
                        "d2h_bytes_per_step": W * H * 4, "fps": K * world / float(te.item())},
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
-                            "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                            "unit": "GB/s", "frac": achieved / peak,
+                            "traffic": FWD_DRAM_TRAFFIC_BYTES,
                             "peak_kind": peak_kind,
                             "algorithmic_bytes_per_frame": alg / K},
+               "modes": modes,
                "fwd_bwd": fb,
                "batch": bt,
                "gpu_launches": K,
@@ -648,10 +686,20 @@ def main() -> None:
     ap.add_argument("--profile", type=int, default=0, metavar="N",
                     help="only build the workload and render N orbit frames (for ncu)")
     ap.add_argument("--profile-mode", type=int, default=0)
+    ap.add_argument("--profile-diff", type=int, default=0, metavar="N",
+                    help="only run N forward+backward steps of the differentiable workload")
     ap.add_argument("--profile-size", type=int, default=N_EDGE)
     args = ap.parse_args()
     if args.profile:
         run_profile(args)
+        return
+    if args.profile_diff:
+        import torch
+        import render3d_b200 as rb
+        ctx = rb.Context(0)
+        fb = fwd_bwd_bench(rb, ctx, torch, 0, steps=args.profile_diff, adam_steps=1)
+        print("profile fwd+bwd steps done:", fb["steps"])
+        ctx.close()
         return
     if args.warmup < 3:
         args.warmup = 3
