@@ -537,6 +537,8 @@ def run_ours(args) -> None:
                           "parallelism": f"replicas x{world}"},
                "fps": fps, "mrays_per_s": W * H * K * world / (ms_max * 1e-3) / 1e6,
                "samples_per_frame": counts[0] / K,
+               "work_per_frame": {"samples": counts[0] / K, "tf_lookups": counts[1] / K,
+                                  "shaded": counts[2] / K, "page_walks": counts[3] / K},
                "e2e": {"value": e2e_value, "unit": "Gsamples/s", "h2d_bytes_per_step": 248,
                        "d2h_bytes_per_step": W * H * 4, "fps": K * world / float(te.item())},
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,

@@ -9,7 +9,7 @@
 // Minimum resident 128-thread blocks per SM the register allocator targets
 // (0: no target).
 #ifndef R3D_FWD_MIN_BLOCKS
-#define R3D_FWD_MIN_BLOCKS 0
+#define R3D_FWD_MIN_BLOCKS 7
 #endif
 // Warps per block: 1, 2 or 4 8x4 warp tiles.
 #ifndef R3D_FWD_WARPS

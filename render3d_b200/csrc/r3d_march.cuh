@@ -121,26 +121,6 @@ __device__ __forceinline__ float tri_u8(const uint8_t *__restrict__ g, uint32_t 
   return lerp_(e0, e1, fz) * kInv255;
 }
 
-// Trilinear inside one 128^3 slot at slot-local texel coordinates already
-// clamped to [0, 127].
-__device__ __forceinline__ float tri_slot(const uint8_t *__restrict__ g, float tx, float ty,
-                                          float tz) {
-  uint32_t x0 = (uint32_t)tx, y0 = (uint32_t)ty, z0 = (uint32_t)tz;
-  float fx = tx - (float)x0, fy = ty - (float)y0, fz = tz - (float)z0;
-  uint32_t dx1 = x0 < 127u ? 1u : 0u;
-  uint32_t dy1 = y0 < 127u ? 128u : 0u;
-  uint32_t dz1 = z0 < 127u ? 16384u : 0u;
-  const uint8_t *r00 = g + ((z0 << 14) | (y0 << 7) | x0);
-  float a0 = __ldg(r00), a1 = __ldg(r00 + dx1);
-  float b0 = __ldg(r00 + dy1), b1 = __ldg(r00 + dy1 + dx1);
-  float c0 = __ldg(r00 + dz1), c1 = __ldg(r00 + dz1 + dx1);
-  float d0 = __ldg(r00 + dz1 + dy1), d1 = __ldg(r00 + dz1 + dy1 + dx1);
-  float c00 = lerp_(a0, a1, fx), c10 = lerp_(b0, b1, fx);
-  float c01 = lerp_(c0, c1, fx), c11 = lerp_(d0, d1, fx);
-  float e0 = lerp_(c00, c10, fy), e1 = lerp_(c01, c11, fy);
-  return lerp_(e0, e1, fz) * kInv255;
-}
-
 // volumes[0].SampleLevel(p, lod): trilinear within a level, linear between
 // floor(lod) and floor(lod)+1 (raycast.slang:409-416, vkbackend.c:1058-1069)
 __device__ __forceinline__ float cube_sample(const DevCube &c, float3 p, float lod) {
@@ -300,12 +280,24 @@ __device__ __forceinline__ uint32_t floor_frac(float t, float &frac) {
   return __float_as_uint(r) & 0x7fffffu;
 }
 
+// One axis of bricks_fetch's coordinate: clamp to [0.5, 127.5] inside the
+// brick, texel-centre shift, floor and fraction.
+__device__ __forceinline__ uint32_t slot_axis(float b, float &frac) {
+  return floor_frac(clamp_(b, 0.5f, 127.5f) - 0.5f, frac);
+}
+
 __device__ __forceinline__ SlotCoord slot_coord(float3 bl) {
   SlotCoord q;
-  q.x0 = floor_frac(clamp_(bl.x, 0.5f, 127.5f) - 0.5f, q.fx);
-  q.y0 = floor_frac(clamp_(bl.y, 0.5f, 127.5f) - 0.5f, q.fy);
-  q.z0 = floor_frac(clamp_(bl.z, 0.5f, 127.5f) - 0.5f, q.fz);
+  q.x0 = slot_axis(bl.x, q.fx);
+  q.y0 = slot_axis(bl.y, q.fy);
+  q.z0 = slot_axis(bl.z, q.fz);
   return q;
+}
+
+// a byte as a float without the conversion unit: 2^23 + b has b in its
+// mantissa, and subtracting 2^23 is exact
+__device__ __forceinline__ float u8f(uint8_t b) {
+  return __uint_as_float(0x4B000000u | (uint32_t)b) - 8388608.0f;
 }
 
 __device__ __forceinline__ float tri_slot_at(const uint8_t *__restrict__ g, const SlotCoord &q) {
@@ -314,10 +306,10 @@ __device__ __forceinline__ float tri_slot_at(const uint8_t *__restrict__ g, cons
   uint32_t dy1 = q.y0 < 127u ? 128u : 0u;
   uint32_t dz1 = q.z0 < 127u ? 16384u : 0u;
   const uint8_t *r00 = g + ((q.z0 << 14) | (q.y0 << 7) | q.x0);
-  float a0 = __ldg(r00), a1 = __ldg(r00 + dx1);
-  float b0 = __ldg(r00 + dy1), b1 = __ldg(r00 + dy1 + dx1);
-  float c0 = __ldg(r00 + dz1), c1 = __ldg(r00 + dz1 + dx1);
-  float d0 = __ldg(r00 + dz1 + dy1), d1 = __ldg(r00 + dz1 + dy1 + dx1);
+  float a0 = u8f(__ldg(r00)), a1 = u8f(__ldg(r00 + dx1));
+  float b0 = u8f(__ldg(r00 + dy1)), b1 = u8f(__ldg(r00 + dy1 + dx1));
+  float c0 = u8f(__ldg(r00 + dz1)), c1 = u8f(__ldg(r00 + dz1 + dx1));
+  float d0 = u8f(__ldg(r00 + dz1 + dy1)), d1 = u8f(__ldg(r00 + dz1 + dy1 + dx1));
   float c00 = lerp_(a0, a1, fx), c10 = lerp_(b0, b1, fx);
   float c01 = lerp_(c0, c1, fx), c11 = lerp_(d0, d1, fx);
   float e0 = lerp_(c00, c10, fy), e1 = lerp_(c01, c11, fy);
@@ -327,17 +319,14 @@ __device__ __forceinline__ float tri_slot_at(const uint8_t *__restrict__ g, cons
 // bricks_fetch at atlas lod 0 (raycast.slang:284-288): clamp to
 // [0.5, 127.5] inside the brick, no cross-brick filtering
 __device__ __forceinline__ float brick_fetch(const DevScene &s, uint32_t slot, float3 bl) {
-  const uint8_t *g = s.br.pool + (size_t)slot * (128u * 128u * 128u);
-  float lx = clamp_(bl.x, 0.5f, 127.5f), ly = clamp_(bl.y, 0.5f, 127.5f),
-        lz = clamp_(bl.z, 0.5f, 127.5f);
-  return tri_slot(g, lx - 0.5f, ly - 0.5f, lz - 0.5f);
+  return tri_slot_at(s.br.pool + (size_t)slot * (128u * 128u * 128u), slot_coord(bl));
 }
 
 // TF lookup (raycast.slang:894) from raw 0..255 RGBA values in shared memory
 __device__ __forceinline__ float4 tf_sample(const float4 *tf, float t) {
-  uint32_t i0 = (uint32_t)t;
-  uint32_t i1 = min(i0 + 1u, 255u);
-  float f = t - (float)i0;
+  float f;
+  const uint32_t i0 = floor_frac(t, f);
+  const uint32_t i1 = min(i0 + 1u, 255u);
   float4 a = tf[i0], b = tf[i1];
   return make_float4(lerp_(a.x, b.x, f) * kInv255, lerp_(a.y, b.y, f) * kInv255,
                      lerp_(a.z, b.z, f) * kInv255, lerp_(a.w, b.w, f) * kInv255);
@@ -584,14 +573,26 @@ __device__ __forceinline__ bool composite_sample(const DevScene &s, const ViewCo
       g2 = (((-q0 + q1) - q2) + q3) * renorm;
     } else {  // raycast.slang:957-986
       if (kLod) {
-        float ev = q.grad_vox;
-        float3 u = q.bl;
-        g0 = brick_fetch(s, q.slot, make_float3(u.x + ev, u.y, u.z)) -
-             brick_fetch(s, q.slot, make_float3(u.x - ev, u.y, u.z));
-        g1 = brick_fetch(s, q.slot, make_float3(u.x, u.y + ev, u.z)) -
-             brick_fetch(s, q.slot, make_float3(u.x, u.y - ev, u.z));
-        g2 = brick_fetch(s, q.slot, make_float3(u.x, u.y, u.z + ev)) -
-             brick_fetch(s, q.slot, make_float3(u.x, u.y, u.z - ev));
+        // each tap moves one axis; the other two keep the sample's own
+        // clamped coordinates, so only the moved axis is recomputed
+        const float ev = q.grad_vox;
+        const float3 u = q.bl;
+        const uint8_t *g = s.br.pool + (size_t)q.slot * (128u * 128u * 128u);
+        const SlotCoord c = slot_coord(u);
+        SlotCoord a = c, b = c;
+        a.x0 = slot_axis(u.x + ev, a.fx);
+        b.x0 = slot_axis(u.x - ev, b.fx);
+        g0 = tri_slot_at(g, a) - tri_slot_at(g, b);
+        a = c;
+        b = c;
+        a.y0 = slot_axis(u.y + ev, a.fy);
+        b.y0 = slot_axis(u.y - ev, b.fy);
+        g1 = tri_slot_at(g, a) - tri_slot_at(g, b);
+        a = c;
+        b = c;
+        a.z0 = slot_axis(u.z + ev, a.fz);
+        b.z0 = slot_axis(u.z - ev, b.fz);
+        g2 = tri_slot_at(g, a) - tri_slot_at(g, b);
       } else {
         float e = vc.voxel * q.lod_step;
         g0 = cube_sample(s.cube, make_float3(q.p.x + e, q.p.y, q.p.z), q.lod) -
