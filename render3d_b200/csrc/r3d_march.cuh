@@ -238,11 +238,12 @@ __device__ __forceinline__ BrickCtx lod_locate_ex(const DevScene &s, float3 p, f
   return c;
 }
 
-// bricks_lod_locate_cached, raycast.slang:255-279
-__device__ __forceinline__ BrickCtx lod_locate_cached(const DevScene &s, float3 p, float lod,
-                                                      LodCache &lc, bool &walked) {
+// The hit test of bricks_lod_locate_cached (raycast.slang:255-279): true,
+// with the brick context in out, when the desired level and the brick under
+// p are the cached ones.
+__device__ __forceinline__ bool lod_cache_hit(const DevScene &s, float3 p, int desired,
+                                              const LodCache &lc, BrickCtx &out) {
   const DevBricks &b = s.br;
-  int desired = (int)clamp_(floorf(lod), 0.0f, (float)(b.nlev - 1u));
   if (lc.valid && lc.desired == desired) {
     float lv[3];
     bool same = true;
@@ -255,13 +256,12 @@ __device__ __forceinline__ BrickCtx lod_locate_cached(const DevScene &s, float3 
       same = same && lv[a] >= lc.lo[a] && lv[a] < lc.lo[a] + 128.0f;
     }
     if (same) {
-      BrickCtx c = lc.c;
-      c.bl = make_float3(lv[0] - lc.lo[0], lv[1] - lc.lo[1], lv[2] - lc.lo[2]);
-      return c;
+      out = lc.c;
+      out.bl = make_float3(lv[0] - lc.lo[0], lv[1] - lc.lo[1], lv[2] - lc.lo[2]);
+      return true;
     }
   }
-  walked = true;
-  return lod_locate_ex(s, p, lod, lc, desired);
+  return false;
 }
 
 // Slot-local texel coordinates of bricks_fetch (clamped, minus 0.5) and
@@ -387,6 +387,9 @@ struct RayState {
   float3 ro, dir;  // volume space
   float t, tf_, span_step;
   bool span_dom;  // span_step >= every exp2(lod): lod_step is span_step
+  // LOD bricks: for a footprint ratio y in [lod_ylo, lod_yhi) the desired
+  // level is lc.desired and lod_step is span_step (empty range: unknown)
+  float lod_ylo, lod_yhi;
   uint32_t steps, mip_index;
   float mip_max, first_hit;
   float acc_r, acc_g, acc_b, acc_a;
@@ -506,6 +509,8 @@ __device__ __forceinline__ bool ray_begin(const r3d_frame_params &pc, const DevS
   // two are exact and the margin covers the approximation), so beyond this
   // bound max(exp2(lod), span_step) is span_step without evaluating exp2
   st.span_dom = st.span_step >= r3d_exp2f(ceilf(vc.max_lod)) * 1.001f;
+  st.lod_ylo = R3D_FM_INF;
+  st.lod_yhi = 0.0f;
   st.steps = 0;
   st.mip_index = 0;
   st.mip_max = 0.0f;
@@ -634,6 +639,25 @@ __device__ __forceinline__ bool composite_sample(const DevScene &s, const ViewCo
   return true;
 }
 
+// The footprint ratios y for which the step's LOD decisions are known
+// without log2 / exp2, after the exact lod at some y gave desired level d:
+// lod = clamp(log2(y) + bias, 0, max_lod) has floor d for every y in
+// [2^(d - bias), 2^(d + 1 - bias)) (open at the ends for d = 0 and the top
+// level), narrowed by 2^-12 relative at each end -- 3.5e-4 in log2, far
+// above the error of r3d_log2f plus the rounding of the bias add -- and
+// when span_step >= 1.001 * 2^(d + 1) (2^max_lod at the top), lod_step is
+// span_step for every lod of the level.  Otherwise the range is empty.
+__device__ __forceinline__ void lod_range(RayState &st, const ViewConst &vc, int d, int top) {
+  const float hi_lod = d >= top ? vc.max_lod : (float)(d + 1);
+  if (!(st.span_step >= r3d_exp2f(hi_lod) * 1.001f)) {
+    st.lod_ylo = R3D_FM_INF;
+    st.lod_yhi = 0.0f;
+    return;
+  }
+  st.lod_ylo = d == 0 ? 0.0f : r3d_exp2f((float)d - vc.lod_bias) * (1.0f + 0x1p-12f);
+  st.lod_yhi = d >= top ? R3D_FM_INF : r3d_exp2f((float)(d + 1) - vc.lod_bias) * (1.0f - 0x1p-12f);
+}
+
 // One iteration of the hot loop (raycast.slang:767-1021).  Returns
 // kStepDone when the ray is finished (loop condition failed, saturation or
 // opacity cutoff) and kStepCont otherwise.  With DEFER, a sample that needs
@@ -650,13 +674,19 @@ __device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, 
   st.steps++;
   const float t = st.t;
   // LOD and step (raycast.slang:772-779)
-  float lod = 0.0f;
+  float lod = 0.0f, y = 1.0f;
+  bool lod_known = true;
   if (vc.lod_on) {
     float foot = vc.ortho ? vc.cone : t * vc.cone;
-    lod = clamp_(r3d_log2f(fmaxf(foot * vc.vox_inv, 1.0f)) + vc.lod_bias, 0.0f, vc.max_lod);
+    y = fmaxf(foot * vc.vox_inv, 1.0f);
+    if (kLod && y >= st.lod_ylo && y < st.lod_yhi)
+      lod_known = false;  // level and lod_step known (lod_range)
+    else
+      lod = clamp_(r3d_log2f(y) + vc.lod_bias, 0.0f, vc.max_lod);
   }
   const float lod_step =
-      st.span_dom ? st.span_step : fmaxf(lod == 0.0f ? 1.0f : r3d_exp2f(lod), st.span_step);
+      !lod_known || st.span_dom ? st.span_step
+                                : fmaxf(lod == 0.0f ? 1.0f : r3d_exp2f(lod), st.span_step);
   const float3 dir = st.dir;
   const float3 p =
       make_float3(fmaf(t, dir.x, st.ro.x), fmaf(t, dir.y, st.ro.y), fmaf(t, dir.z, st.ro.z));
@@ -664,9 +694,17 @@ __device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, 
   float v = 0.0f;
   BrickCtx b;
   if (kLod) {
-    bool walked = false;
-    b = lod_locate_cached(s, p, lod, st.lc, walked);
-    if (COUNT) st.n_walk += walked ? 1u : 0u;
+    const int top = (int)s.br.nlev - 1;
+    int desired = st.lc.desired;
+    if (lod_known) {
+      desired = (int)clamp_(floorf(lod), 0.0f, (float)top);
+      if (desired != st.lc.desired) lod_range(st, vc, desired, top);
+    }
+    if (!lod_cache_hit(s, p, desired, st.lc, b)) {  // walk the page table
+      if (!lod_known) lod = clamp_(r3d_log2f(y) + vc.lod_bias, 0.0f, vc.max_lod);
+      if (COUNT) st.n_walk++;
+      b = lod_locate_ex(s, p, lod, st.lc, desired);
+    }
     if (b.ok) {
       // Exact fetch elision: vub bounds the trilinear value from above
       // (every tap lies in the dilated block and rounding is monotone).
