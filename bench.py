@@ -147,6 +147,44 @@ def algorithmic_bytes(cnt: np.ndarray, pixels: int) -> float:
     return 8.0 * samples + 48.0 * grad + 8.0 * tf + 4.0 * walks + 4.0 * pixels
 
 
+def shard_bench(rb, torch, local: int, vol, lut, frames: int) -> dict:
+    """The same phantom as a single-level brick atlas (render3d's bricks mode
+    without LOD: a 1024^3 shard of 8^3 bricks, all resident in the identity
+    layout, atlas mips 0..3), 1920x1080 FULL along the orbit."""
+    c = rb.Context(local)
+    try:
+        c.set_transfer(lut)
+        c.set_alpha_cutoff(CUTOFF)
+        c.shard_build(vol)
+        img = torch.zeros((H, W, 4), dtype=torch.uint8, device=f"cuda:{local}")
+        tot = torch.zeros(1, dtype=torch.int64, device=f"cuda:{local}")
+        st = torch.cuda.ExternalStream(c.stream, device=local)
+
+        def frame(i):
+            p = rb.orbit_view((i % ORBIT_FRAMES) / ORBIT_FRAMES, W, H, lut, step_voxels=STEP_VOXELS,
+                              frame_index=i)
+            p.brick_mode = c.shard_mode
+            c.raycast(p, W, H, out=img, total=tot, stream=c.stream)
+        for i in range(20):
+            frame(i)
+        torch.cuda.synchronize()
+        tot.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for i in range(frames):
+            frame(i)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / frames
+        return {"workload": "scroll phantom 1024^3 as a single-level shard (8^3 bricks, identity "
+                            "layout, 4 atlas mips), 1920x1080 full shading",
+                "brick_mode": c.shard_mode, "ms_per_frame": ms, "fps": 1e3 / ms,
+                "gsamples_per_s": float(tot.item()) / frames / (ms * 1e-3) / 1e9}
+    finally:
+        c.close()
+
+
 def mode_stats(rb, ctx, lut, torch, stream, total, img, frames: int) -> dict:
     """Per-frame CUDA-event times (p50/p95/p99, like render3d's frame stats)
     and Gsamples/s of the orbit in FULL, MIP and HEATMAP modes, each after
@@ -505,6 +543,8 @@ def run_ours(args) -> None:
     e2e_value = samples_all / float(te.item()) / 1e9
     r.close()
 
+    shard = shard_bench(rb, torch, local, vol, lut, ORBIT_FRAMES * 2)
+
     bt = None
     if not args.no_batch:
         bt = batch_bench(rb, torch, local, ctx, reps=5)
@@ -547,6 +587,7 @@ def run_ours(args) -> None:
                             "peak_kind": peak_kind,
                             "algorithmic_bytes_per_frame": alg / K},
                "modes": modes,
+               "shard": shard,
                "fwd_bwd": fb,
                "batch": bt,
                "gpu_launches": K,

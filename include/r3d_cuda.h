@@ -102,6 +102,35 @@ int r3d_cuda_bricks_read(r3d_cuda_ctx *ctx, uint32_t *page, uint8_t *slots);
  * host buffer; dims receives its size. */
 int r3d_cuda_cube_read(r3d_cuda_ctx *ctx, int level, uint8_t *out, uint32_t dims[3]);
 
+/* Single-level brick atlas: render3d's bricks mode without the LOD flag, the
+ * decoded shard of a c5s volume (reference src/shaders/raycast.slang:163-180,
+ * 284-288,800-860; residency and atlas upkeep src/vk/vkbackend.c:3241-3330,
+ * 4060-4075,4236-4273).  The volume is a cube of edge = bpa * 128 voxels
+ * (x fastest, host or device pointer, 1 <= bpa <= 255).  The atlas holds
+ * abpa^3 slots of 128^3 (1 <= abpa <= bpa); slot s sits at texel
+ * (s % abpa, s / abpa % abpa, s / abpa^2) * 128 of one (abpa * 128)^3
+ * texture with 4 mips ((sum+4)/8 box), and a world-indexed 8^3 occupancy
+ * grid ((bpa * 16)^3, block maxima of resident bricks, 0 elsewhere, then
+ * 26-neighbour max dilation) serves the empty-space skip.  slot_of (host,
+ * bpa^3 entries in brick order) gives each brick's slot, or 0xFFFFFFFF for
+ * a brick that is not resident; NULL puts brick b in slot b and needs
+ * abpa == bpa.  Page entries are slot | brick max << 24.  When every brick
+ * sits in its own slot the atlas is laid out like the world and views
+ * sample it directly (the identity bit of brick_mode). */
+int r3d_cuda_shard_build(r3d_cuda_ctx *ctx, uint32_t edge, const uint8_t *voxels, uint32_t abpa,
+                         const uint32_t *slot_of);
+
+/* brick_mode word of the loaded atlas: bpa | abpa << 8 | 0x10000 when the
+ * layout is the identity (reference src/vk/vkbackend.c:4511-4517); 0 when
+ * none is loaded. */
+uint32_t r3d_cuda_shard_mode(const r3d_cuda_ctx *ctx);
+
+/* Copy of the atlas's page table (bpa^3 words, may be NULL) and of atlas
+ * mip `level` (0..3) or, for level == -1, the occupancy grid (out may be
+ * NULL); dims receives the copied grid's size. */
+int r3d_cuda_shard_read(r3d_cuda_ctx *ctx, int level, uint32_t *page, uint8_t *out,
+                        uint32_t dims[3]);
+
 /* --- forward raycast ------------------------------------------------------ */
 
 /* Optional per-pixel outputs of a forward raycast, in the same memory kind

@@ -48,6 +48,13 @@ void r3d_set_quality(r3d_renderer *r, uint32_t quality);
  * are left non-resident) from a raw u8 volume on the device. */
 int r3d_bricks_begin_volume(r3d_renderer *r, const r3d_volume_desc *d, const uint8_t *voxels,
                             uint32_t nlev, uint32_t min_max);
+/* Single-level bricks (a shard of edge = bpa * 128, the non-LOD bricks mode
+ * of r3d_bricks_begin, reference src/render/render.h:44-50): with
+ * pool_bpa == 0 or >= bpa the whole shard is resident in the identity
+ * layout, as in the reference when the volume fits the pool.  A smaller
+ * pool needs the streaming residency pump, which is not built: -1. */
+int r3d_bricks_begin_shard(r3d_renderer *r, const uint8_t *voxels, uint32_t edge,
+                           uint32_t pool_bpa);
 int r3d_bricks_end(r3d_renderer *r);
 void r3d_bricks_params(const r3d_renderer *r, r3d_frame_params *p);
 void r3d_bricks_extent(const r3d_renderer *r, float extent[3]);

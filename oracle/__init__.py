@@ -34,7 +34,7 @@ class Cube(C.Structure):
 
 class Bricks(C.Structure):
     _fields_ = [("page", C.c_void_p), ("page_words", C.c_uint32), ("pool", C.c_void_p),
-                ("nslots", C.c_uint32)]
+                ("nslots", C.c_uint32), ("atlas", C.c_void_p)]
 
 
 class Opts(C.Structure):
@@ -65,6 +65,10 @@ def _load():
     lib.orc_occupancy.argtypes = [P, U32, U32, U32, P]
     lib.orc_build_lod_bricks.restype = C.c_int64
     lib.orc_build_lod_bricks.argtypes = [P, U32, U32, U32, U32, U32, P, U32, P, C.c_uint64]
+    lib.orc_build_shard.restype = C.c_int
+    lib.orc_build_shard.argtypes = [P, U32, U32, P, P, P]
+    lib.orc_shard_occupancy.restype = None
+    lib.orc_shard_occupancy.argtypes = [P, U32, P, U32, P]
     lib.orc_lod_page_words.restype = U32
     lib.orc_lod_page_words.argtypes = [U32, U32, U32, U32]
     lib.orc_camera_basis.restype = None
@@ -146,6 +150,61 @@ class BrickScene:
         return cls(page, pool[: n * 128 ** 3] if n else pool[:0])
 
 
+class ShardScene:
+    """A single-level brick atlas: page table (bpa^3 entries) and atlas
+    level 0 ((abpa * 128)^3), with the oracle's own mips and world-indexed
+    occupancy grid."""
+
+    def __init__(self, page: np.ndarray, atlas0: np.ndarray, bpa: int, abpa: int):
+        self.page = np.ascontiguousarray(page, np.uint32)
+        assert self.page.size == bpa ** 3
+        a = abpa * 128
+        self.levels = [np.ascontiguousarray(atlas0, np.uint8).reshape(a, a, a)]
+        for m in range(1, 4):
+            s, d = a >> (m - 1), a >> m
+            dst = np.empty((d, d, d), np.uint8)
+            lib.orc_downsample(_p(self.levels[-1]), s, s, s, _p(dst), d, d, d)
+            self.levels.append(dst)
+        od = bpa * 16
+        self.occ = np.empty((od, od, od), np.uint8)
+        lib.orc_shard_occupancy(_p(self.levels[0]), abpa, _p(self.page), bpa, _p(self.occ))
+        self.atlas = Cube()
+        self.atlas.nlevels = 4
+        for m, lv in enumerate(self.levels):
+            self.atlas.dim[m][:] = (lv.shape[2], lv.shape[1], lv.shape[0])
+            self.atlas.level[m] = lv.ctypes.data
+        self.atlas.occ = self.occ.ctypes.data
+        self.atlas.odim[:] = (od, od, od)
+        self.bpa, self.abpa = bpa, abpa
+        self.identity = abpa == bpa and all(
+            (int(e) & 0xFFFFFF) == b and int(e) != 0xFFFFFFFF for b, e in enumerate(self.page))
+        self.b = Bricks(self.page.ctypes.data, self.page.size, None, abpa ** 3,
+                        C.addressof(self.atlas))
+
+    @property
+    def brick_mode(self) -> int:
+        return self.bpa | (self.abpa << 8) | (0x10000 if self.identity else 0)
+
+    @classmethod
+    def build(cls, vol: np.ndarray, abpa: int | None = None, slot_of=None) -> "ShardScene":
+        vol = np.ascontiguousarray(vol, np.uint8)
+        e = vol.shape[0]
+        bpa = e // 128
+        abpa = abpa or bpa
+        page = np.empty(bpa ** 3, np.uint32)
+        atlas0 = np.empty((abpa * 128,) * 3, np.uint8)
+        so = None if slot_of is None else np.ascontiguousarray(slot_of, np.uint32)
+        if lib.orc_build_shard(_p(vol), e, abpa, _p(so), _p(page), _p(atlas0)) < 0:
+            raise ValueError("orc_build_shard failed")
+        return cls(page, atlas0, bpa, abpa)
+
+
+def _scene_args(scene):
+    cube = C.byref(scene.c) if isinstance(scene, CubeScene) else None
+    br = C.byref(scene.b) if isinstance(scene, (BrickScene, ShardScene)) else None
+    return cube, br
+
+
 def render(params, scene, lut: np.ndarray, img_w: int, img_h: int, cutoff: float = 0.98,
            quality: int = 0, threads: int = 0, img: np.ndarray | None = None,
            want_aux: bool = True):
@@ -156,8 +215,7 @@ def render(params, scene, lut: np.ndarray, img_w: int, img_h: int, cutoff: float
     steps = np.zeros((img_h, img_w), np.uint32) if want_aux else None
     mipi = np.zeros((img_h, img_w), np.uint32) if want_aux else None
     aux = Aux(_p(steps), _p(mipi), 0, 0)
-    cube = C.byref(scene.c) if isinstance(scene, CubeScene) else None
-    br = C.byref(scene.b) if isinstance(scene, BrickScene) else None
+    cube, br = _scene_args(scene)
     rc = lib.orc_render_view(C.byref(params), cube, br, _p(lut), C.byref(Opts(cutoff, quality,
                              threads)), _p(img), img_w, img_h, C.byref(aux))
     if rc != 0:
@@ -175,8 +233,7 @@ def render_pixels(params, scene, lut: np.ndarray, xy: np.ndarray, cutoff: float 
     steps = np.zeros(n, np.uint32)
     mipi = np.zeros(n, np.uint32)
     lut = np.ascontiguousarray(lut, np.uint8)
-    cube = C.byref(scene.c) if isinstance(scene, CubeScene) else None
-    br = C.byref(scene.b) if isinstance(scene, BrickScene) else None
+    cube, br = _scene_args(scene)
     rc = lib.orc_render_pixels(C.byref(params), cube, br, _p(lut),
                                C.byref(Opts(cutoff, quality, threads)), _p(xy), n, _p(rgba),
                                _p(steps), _p(mipi))

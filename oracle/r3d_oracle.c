@@ -247,6 +247,18 @@ static float brick_fetch(const scene *s, uint32_t slot, v3f bl) {
   return tri_u8(g, 128u, 128u, 128u, lx - 0.5f, ly - 0.5f, lz - 0.5f);
 }
 
+/* bricks_fetch of the single-level atlas (:284-288): the brick-local
+ * position clamped to [inset, 128 - inset], inset = max(0.5 * 2^lod, 0.5),
+ * then the atlas sampled at lod like a cube texture at
+ * (slot origin + clamped position) / (abpa * 128) */
+static float shard_fetch(const orc_cube *atlas, float inv_adim, v3f org, v3f bl, float lod) {
+  float inset = fmaxf(0.5f * r3d_exp2f(lod), 0.5f), hi = 128.0f - inset;
+  v3f u = mk3((org.x + clampf_(bl.x, inset, hi)) * inv_adim,
+              (org.y + clampf_(bl.y, inset, hi)) * inv_adim,
+              (org.z + clampf_(bl.z, inset, hi)) * inv_adim);
+  return cube_sample(atlas, u, lod);
+}
+
 /* ------------------------------------------------------------ the march */
 
 typedef struct ray_out {
@@ -269,6 +281,10 @@ static void march(const r3d_frame_params *pc, const scene *s, const uint8_t lut[
   int ortho = (pc->view_flags & R3D_VIEW_ORTHO) != 0u;
   int bricks = pc->brick_mode != 0u;
   int lodb = bricks && (pc->brick_mode & R3D_BRICK_LOD_FLAG) != 0u;
+  int shard = bricks && !lodb;
+  uint32_t sh_bpa = pc->brick_mode & 0xffu, sh_abpa = (pc->brick_mode >> 8) & 0xffu;
+  int sh_ident = (pc->brick_mode & R3D_BRICK_IDENTITY_FLAG) != 0u;
+  const orc_cube *atlas = shard ? s->br->atlas : NULL;
 
   /* pix_ndc / ray_dir / ray_origin, :469-486 */
   float ux = ((float)px + 0.5f) / (float)pc->viewport[0];
@@ -308,6 +324,10 @@ static void march(const r3d_frame_params *pc, const scene *s, const uint8_t lut[
     vox_inv = md;
     max_lod = (float)(nlev - 1u);
     ext = mk3(bs[0] / md, bs[1] / md, bs[2] / md);
+  } else if (shard) { /* :659-661 */
+    voxel = 1.0f / (float)(sh_bpa * 128u);
+    vox_inv = (float)(sh_bpa * 128u);
+    max_lod = 3.0f;
   } else {
     const uint32_t *d = s->cube->dim[0];
     uint32_t cm = d[0] > d[1] ? d[0] : d[1];
@@ -401,6 +421,11 @@ static void march(const r3d_frame_params *pc, const scene *s, const uint8_t lut[
   brick_ctx b;
   memset(&b, 0, sizeof b);
   b.world_brick = 128.0f * voxel;
+  /* single-level page cache (:752-760) */
+  uint32_t b_last = 0xFFFFFFFFu;
+  float sh_n = (float)(sh_bpa * 128u);
+  float sh_inv = 1.0f / ((float)sh_abpa * 128.0f);
+  v3f sh_org = mk3(0.0f, 0.0f, 0.0f);
 
   while (t < tf_ && steps < ray_budget) {
     steps++;
@@ -414,6 +439,32 @@ static void march(const r3d_frame_params *pc, const scene *s, const uint8_t lut[
     if (lodb) {
       b = lod_locate_cached(s, p, lod, &lc);
       v = b.ok ? brick_fetch(s, b.slot, b.bl) : 0.0f;
+    } else if (shard && sh_ident) { /* :800-805 */
+      v = cube_sample(atlas, p, lod);
+    } else if (shard) { /* :806-822 */
+      float vp[3] = {satf(p.x) * sh_n, satf(p.y) * sh_n, satf(p.z) * sh_n};
+      uint32_t bc[3];
+      for (int a = 0; a < 3; a++) {
+        bc[a] = (uint32_t)vp[a] >> 7;
+        if (bc[a] > sh_bpa - 1u) bc[a] = sh_bpa - 1u;
+      }
+      uint32_t bi = (bc[2] * sh_bpa + bc[1]) * sh_bpa + bc[0];
+      if (bi != b_last) {
+        b_last = bi;
+        uint32_t e = page_rd(s, bi);
+        b.ok = e != 0xFFFFFFFFu;
+        b.slot = e & 0xFFFFFFu;
+        if (b.ok && b.slot >= sh_abpa * sh_abpa * sh_abpa) {
+          *s->status |= 1u;
+          b.ok = 0;
+        }
+        b.maxv = b.ok ? (float)(e >> 24) / 255.0f : 0.0f;
+        sh_org = mk3((float)(b.slot % sh_abpa) * 128.0f, (float)((b.slot / sh_abpa) % sh_abpa) * 128.0f,
+                     (float)(b.slot / (sh_abpa * sh_abpa)) * 128.0f);
+      }
+      b.bl = mk3(vp[0] - (float)(bc[0] << 7), vp[1] - (float)(bc[1] << 7),
+                 vp[2] - (float)(bc[2] << 7));
+      v = b.ok ? shard_fetch(atlas, sh_inv, sh_org, b.bl, lod) : 0.0f;
     } else {
       v = cube_sample(s->cube, p, lod);
     }
@@ -431,6 +482,18 @@ static void march(const r3d_frame_params *pc, const scene *s, const uint8_t lut[
       } else if (v < bgate && b.maxv < bgate) {
         void_blk = 1;
         bsz = b.world_brick;
+      }
+    } else if (shard) { /* :848-860 */
+      float bgate = fmaxf(occ_gate, 4.5f / 255.0f);
+      if (v < bgate) {
+        if (sh_ident) {
+          if (occ_sample(atlas->occ, atlas->odim, p) < bgate) void_blk = 1;
+        } else if (b.maxv < bgate) {
+          void_blk = 1;
+          bsz = 128.0f * voxel;
+        } else if (occ_sample(atlas->occ, atlas->odim, p) < bgate) {
+          void_blk = 1;
+        }
       }
     } else if (v < occ_gate && occ_sample(s->cube->occ, s->cube->odim, p) < occ_gate) {
       void_blk = 1;
@@ -471,12 +534,20 @@ static void march(const r3d_frame_params *pc, const scene *s, const uint8_t lut[
               q1 = brick_fetch(s, b.slot, mk3(b.bl.x - ev, b.bl.y - ev, b.bl.z + ev));
               q2 = brick_fetch(s, b.slot, mk3(b.bl.x - ev, b.bl.y + ev, b.bl.z - ev));
               q3 = brick_fetch(s, b.slot, mk3(b.bl.x + ev, b.bl.y + ev, b.bl.z + ev));
+            } else if (shard && !sh_ident) { /* :937-940 */
+              float ev = lod_step * ir3;
+              v3f u = b.bl;
+              q0 = shard_fetch(atlas, sh_inv, sh_org, mk3(u.x + ev, u.y - ev, u.z - ev), lod);
+              q1 = shard_fetch(atlas, sh_inv, sh_org, mk3(u.x - ev, u.y - ev, u.z + ev), lod);
+              q2 = shard_fetch(atlas, sh_inv, sh_org, mk3(u.x - ev, u.y + ev, u.z - ev), lod);
+              q3 = shard_fetch(atlas, sh_inv, sh_org, mk3(u.x + ev, u.y + ev, u.z + ev), lod);
             } else {
+              const orc_cube *tex = shard ? atlas : s->cube;
               float ee = (voxel * lod_step) * ir3;
-              q0 = cube_sample(s->cube, mk3(p.x + ee, p.y - ee, p.z - ee), lod);
-              q1 = cube_sample(s->cube, mk3(p.x - ee, p.y - ee, p.z + ee), lod);
-              q2 = cube_sample(s->cube, mk3(p.x - ee, p.y + ee, p.z - ee), lod);
-              q3 = cube_sample(s->cube, mk3(p.x + ee, p.y + ee, p.z + ee), lod);
+              q0 = cube_sample(tex, mk3(p.x + ee, p.y - ee, p.z - ee), lod);
+              q1 = cube_sample(tex, mk3(p.x - ee, p.y - ee, p.z + ee), lod);
+              q2 = cube_sample(tex, mk3(p.x - ee, p.y + ee, p.z - ee), lod);
+              q3 = cube_sample(tex, mk3(p.x + ee, p.y + ee, p.z + ee), lod);
             }
             g[0] = (((q0 - q1) - q2) + q3) * renorm;
             g[1] = (((-q0 - q1) + q2) + q3) * renorm;
@@ -491,14 +562,24 @@ static void march(const r3d_frame_params *pc, const scene *s, const uint8_t lut[
                      brick_fetch(s, b.slot, mk3(u.x, u.y - ev, u.z));
               g[2] = brick_fetch(s, b.slot, mk3(u.x, u.y, u.z + ev)) -
                      brick_fetch(s, b.slot, mk3(u.x, u.y, u.z - ev));
+            } else if (shard && !sh_ident) { /* :972-979 */
+              float ev = lod_step;
+              v3f u = b.bl;
+              g[0] = shard_fetch(atlas, sh_inv, sh_org, mk3(u.x + ev, u.y, u.z), lod) -
+                     shard_fetch(atlas, sh_inv, sh_org, mk3(u.x - ev, u.y, u.z), lod);
+              g[1] = shard_fetch(atlas, sh_inv, sh_org, mk3(u.x, u.y + ev, u.z), lod) -
+                     shard_fetch(atlas, sh_inv, sh_org, mk3(u.x, u.y - ev, u.z), lod);
+              g[2] = shard_fetch(atlas, sh_inv, sh_org, mk3(u.x, u.y, u.z + ev), lod) -
+                     shard_fetch(atlas, sh_inv, sh_org, mk3(u.x, u.y, u.z - ev), lod);
             } else {
+              const orc_cube *tex = shard ? atlas : s->cube;
               float e = voxel * lod_step;
-              g[0] = cube_sample(s->cube, mk3(p.x + e, p.y, p.z), lod) -
-                     cube_sample(s->cube, mk3(p.x - e, p.y, p.z), lod);
-              g[1] = cube_sample(s->cube, mk3(p.x, p.y + e, p.z), lod) -
-                     cube_sample(s->cube, mk3(p.x, p.y - e, p.z), lod);
-              g[2] = cube_sample(s->cube, mk3(p.x, p.y, p.z + e), lod) -
-                     cube_sample(s->cube, mk3(p.x, p.y, p.z - e), lod);
+              g[0] = cube_sample(tex, mk3(p.x + e, p.y, p.z), lod) -
+                     cube_sample(tex, mk3(p.x - e, p.y, p.z), lod);
+              g[1] = cube_sample(tex, mk3(p.x, p.y + e, p.z), lod) -
+                     cube_sample(tex, mk3(p.x, p.y - e, p.z), lod);
+              g[2] = cube_sample(tex, mk3(p.x, p.y, p.z + e), lod) -
+                     cube_sample(tex, mk3(p.x, p.y, p.z - e), lod);
             }
           }
           v3f gv = mk3(g[0], g[1], g[2]);
@@ -551,11 +632,18 @@ static int check_view(const r3d_frame_params *p, const orc_cube *cube, const orc
   if (p->slab_grid || p->clip_valid || p->overlay_flags ||
       (p->view_flags & (R3D_VIEW_SURF | R3D_VIEW_STRETCH)) || p->mode >= R3D_MODE_COUNT)
     return -1;
-  if (p->brick_mode) {
-    if (!(p->brick_mode & R3D_BRICK_LOD_FLAG) || !br || !br->page || br->page_words < 64u)
-      return -1;
+  if (p->brick_mode & R3D_BRICK_LOD_FLAG) {
+    if (!br || !br->page || br->page_words < 64u) return -1;
     uint32_t nlev = br->page[0];
     if (nlev < 1u || nlev > 15u) return -1;
+  } else if (p->brick_mode) { /* single-level atlas */
+    uint32_t bpa = p->brick_mode & 0xffu, abpa = (p->brick_mode >> 8) & 0xffu;
+    const orc_cube *a = br ? br->atlas : NULL;
+    if (!bpa || !abpa || abpa > bpa || !br || !br->page || br->page_words != bpa * bpa * bpa || !a ||
+        a->nlevels != 4u || !a->occ)
+      return -1;
+    for (int k = 0; k < 3; k++)
+      if (a->dim[0][k] != abpa * 128u || a->odim[k] != bpa * 16u) return -1;
   } else if (!cube || !cube->nlevels || !cube->occ) {
     return -1;
   }
@@ -706,6 +794,83 @@ void orc_occupancy(const uint8_t *vox, uint32_t nx, uint32_t ny, uint32_t nz, ui
 }
 
 static uint32_t ceil_div(uint32_t a, uint32_t b) { return (a + b - 1u) / b; }
+
+int orc_build_shard(const uint8_t *vox, uint32_t edge, uint32_t abpa, const uint32_t *slot_of,
+                    uint32_t *page, uint8_t *atlas0) {
+  if (!vox || !page || !edge || edge % 128u || edge / 128u > 255u) return -1;
+  uint32_t bpa = edge / 128u, nb = bpa * bpa * bpa;
+  if (!abpa || abpa > bpa || (!slot_of && abpa != bpa)) return -1;
+  uint32_t ns = abpa * abpa * abpa, a = abpa * 128u;
+  int identity = abpa == bpa;
+  if (atlas0) memset(atlas0, 0, (size_t)a * a * a);
+  for (uint32_t b = 0; b < nb; b++) {
+    uint32_t s = slot_of ? slot_of[b] : b;
+    identity = identity && s == b;
+    if (s == 0xFFFFFFFFu) {
+      page[b] = 0xFFFFFFFFu;
+      continue;
+    }
+    if (s >= ns) return -1;
+    uint32_t bx = b % bpa, by = (b / bpa) % bpa, bz = b / (bpa * bpa);
+    uint32_t sx = s % abpa, sy = (s / abpa) % abpa, sz = s / (abpa * abpa);
+    uint8_t m = 0;
+    for (uint32_t z = 0; z < 128u; z++)
+      for (uint32_t y = 0; y < 128u; y++) {
+        const uint8_t *src = vox + ((size_t)(bz * 128u + z) * edge + (by * 128u + y)) * edge +
+                             bx * 128u;
+        for (uint32_t x = 0; x < 128u; x++)
+          if (src[x] > m) m = src[x];
+        if (atlas0)
+          memcpy(atlas0 + ((size_t)(sz * 128u + z) * a + (sy * 128u + y)) * a + sx * 128u, src,
+                 128u);
+      }
+    page[b] = s | ((uint32_t)m << 24);
+  }
+  return identity ? 1 : 0;
+}
+
+void orc_shard_occupancy(const uint8_t *atlas0, uint32_t abpa, const uint32_t *page, uint32_t bpa,
+                         uint8_t *out) {
+  uint32_t od = bpa * 16u, a = abpa * 128u;
+  size_t n = (size_t)od * od * od;
+  uint8_t *raw = malloc(n);
+  if (!raw) return;
+  for (uint32_t wz = 0; wz < od; wz++)
+    for (uint32_t wy = 0; wy < od; wy++)
+      for (uint32_t wx = 0; wx < od; wx++) {
+        uint32_t e = page[((wz >> 4) * bpa + (wy >> 4)) * bpa + (wx >> 4)];
+        uint8_t m = 0;
+        if (e != 0xFFFFFFFFu) {
+          uint32_t s = e & 0xFFFFFFu;
+          uint32_t x0 = (s % abpa) * 128u + (wx & 15u) * 8u;
+          uint32_t y0 = ((s / abpa) % abpa) * 128u + (wy & 15u) * 8u;
+          uint32_t z0 = (s / (abpa * abpa)) * 128u + (wz & 15u) * 8u;
+          for (uint32_t z = z0; z < z0 + 8u; z++)
+            for (uint32_t y = y0; y < y0 + 8u; y++)
+              for (uint32_t x = x0; x < x0 + 8u; x++) {
+                uint8_t v = atlas0[((size_t)z * a + y) * a + x];
+                if (v > m) m = v;
+              }
+        }
+        raw[((size_t)wz * od + wy) * od + wx] = m;
+      }
+  for (uint32_t z = 0; z < od; z++)
+    for (uint32_t y = 0; y < od; y++)
+      for (uint32_t x = 0; x < od; x++) {
+        uint8_t m = 0;
+        for (int dz = -1; dz <= 1; dz++)
+          for (int dy = -1; dy <= 1; dy++)
+            for (int dx = -1; dx <= 1; dx++) {
+              int zz = (int)z + dz, yy = (int)y + dy, xx = (int)x + dx;
+              if (zz < 0 || yy < 0 || xx < 0 || zz >= (int)od || yy >= (int)od || xx >= (int)od)
+                continue;
+              uint8_t v = raw[((size_t)zz * od + (size_t)yy) * od + (size_t)xx];
+              if (v > m) m = v;
+            }
+        out[((size_t)z * od + y) * od + x] = m;
+      }
+  free(raw);
+}
 
 uint32_t orc_lod_page_words(uint32_t nx, uint32_t ny, uint32_t nz, uint32_t nlev) {
   uint32_t w = R3D_BRICK_PAGE_HEADER;

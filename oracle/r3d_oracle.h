@@ -37,13 +37,18 @@ typedef struct orc_cube {
   uint32_t odim[3];
 } orc_cube;
 
-/* Brick cache: the page table in render3d's word format and a pool of
- * 128^3 slots (slot s at pool + s * 128^3, x fastest). */
+/* Brick cache.  LOD mode (brick_mode with the LOD flag): the page table in
+ * render3d's word format and a pool of 128^3 slots (slot s at
+ * pool + s * 128^3, x fastest).  Single-level mode (no LOD flag,
+ * src/shaders/raycast.slang:163-180,800-822): page holds bpa^3 entries and
+ * atlas is the (abpa * 128)^3 atlas texture with its 4 mips, its occ field
+ * being the world-indexed (bpa * 16)^3 dilated occupancy grid. */
 typedef struct orc_bricks {
   const uint32_t *page;
   uint32_t page_words;
   const uint8_t *pool;
   uint32_t nslots;
+  const orc_cube *atlas;
 } orc_bricks;
 
 typedef struct orc_opts {
@@ -116,6 +121,24 @@ int64_t orc_build_lod_bricks(const uint8_t *vox, uint32_t nx, uint32_t ny, uint3
                              uint32_t nlev, uint32_t min_max, uint32_t *page,
                              uint32_t page_words, uint8_t *pool, uint64_t pool_slots);
 uint32_t orc_lod_page_words(uint32_t nx, uint32_t ny, uint32_t nz, uint32_t nlev);
+
+/* Single-level brick atlas from a cubic volume of edge bpa * 128: atlas
+ * level 0 ((abpa * 128)^3, slot s at (s % abpa, s / abpa % abpa,
+ * s / abpa^2) * 128, zeros where no brick sits) and the page table (bpa^3
+ * words, slot | brick max << 24, or 0xFFFFFFFF).  slot_of[b] is brick b's
+ * slot or 0xFFFFFFFF; NULL puts brick b in slot b (abpa == bpa).  Returns 1
+ * when every brick sits in its own slot (identity layout), 0 otherwise, -1
+ * on bad input.  Atlas mips come from orc_downsample
+ * (src/vk/vkbackend.c:4236-4273,3241-3330). */
+int orc_build_shard(const uint8_t *vox, uint32_t edge, uint32_t abpa, const uint32_t *slot_of,
+                    uint32_t *page, uint8_t *atlas0);
+
+/* World-indexed occupancy of a single-level atlas (src/shaders/occmax.comp,
+ * occdilate.comp): block w of the (bpa * 16)^3 grid is the maximum of the
+ * 8^3 atlas texels of its brick's slot (0 for absent bricks), followed by
+ * 26-neighbour max dilation. */
+void orc_shard_occupancy(const uint8_t *atlas0, uint32_t abpa, const uint32_t *page, uint32_t bpa,
+                         uint8_t *out);
 
 /* Host-side camera / TF helpers restated from src/core/camera.c:5-75,
  * src/core/transfer.c:5-50, src/core/lod.h:8-26 and src/core/mathx.h:34-43,

@@ -140,6 +140,9 @@ def _load() -> C.CDLL:
         "r3d_cuda_bricks_info": (I, [P, C.POINTER(U32), C.POINTER(U32), P, C.POINTER(U32)]),
         "r3d_cuda_bricks_read": (I, [P, P, P]),
         "r3d_cuda_cube_read": (I, [P, I, P, P]),
+        "r3d_cuda_shard_build": (I, [P, U32, P, U32, P]),
+        "r3d_cuda_shard_mode": (U32, [P]),
+        "r3d_cuda_shard_read": (I, [P, I, P, P, P]),
         "r3d_cuda_raycast_fwd": (I, [P, P, U32, P, U32, U32, C.POINTER(CudaAux), P]),
         "r3d_cuda_last_kernel_ns": (I, [P, C.POINTER(C.c_uint64)]),
         "r3d_cuda_fmath_eval": (I, [P, P, P, P, U32]),
@@ -165,6 +168,7 @@ def _load() -> C.CDLL:
         "r3d_set_alpha_cutoff": (I, [P, F]),
         "r3d_renderer_cuda": (P, [P]),
         "r3d_bricks_begin_volume": (I, [P, C.POINTER(VolumeDesc), P, U32, U32]),
+        "r3d_bricks_begin_shard": (I, [P, P, U32, U32]),
         "r3d_bricks_end": (I, [P]),
         "r3d_bricks_params": (None, [P, C.POINTER(FrameParams)]),
         "r3d_bricks_extent": (None, [P, P]),
@@ -395,6 +399,32 @@ class Context:
         self._check(lib.r3d_cuda_cube_read(self.h, level, _ptr(out), dims))
         return out
 
+    def shard_build(self, vol, abpa: int | None = None, slot_of=None) -> None:
+        """Single-level brick atlas from a cubic volume of edge bpa * 128
+        (z, y, x order); slot_of[b] is brick b's slot or 0xFFFFFFFF."""
+        e = vol.shape[0]
+        assert tuple(vol.shape) == (e, e, e)
+        bpa = e // 128
+        if slot_of is not None:
+            slot_of = np.ascontiguousarray(slot_of, np.uint32)
+            assert slot_of.size == bpa ** 3
+        self._check(lib.r3d_cuda_shard_build(self.h, e, _ptr(vol), abpa or bpa,
+                                             _ptr(slot_of)))
+
+    @property
+    def shard_mode(self) -> int:
+        return int(lib.r3d_cuda_shard_mode(self.h))
+
+    def shard_read(self, level: int = 0) -> tuple[np.ndarray, np.ndarray]:
+        """(page table, atlas mip `level` or, for -1, the occupancy grid)."""
+        dims = (C.c_uint32 * 3)()
+        self._check(lib.r3d_cuda_shard_read(self.h, level, None, None, dims))
+        bpa = self.shard_mode & 0xFF
+        page = np.empty(bpa ** 3, np.uint32)
+        out = np.empty((dims[2], dims[1], dims[0]), np.uint8)
+        self._check(lib.r3d_cuda_shard_read(self.h, level, _ptr(page), _ptr(out), dims))
+        return page, out
+
     def status(self, clear: bool = True) -> int:
         b = C.c_uint32()
         self._check(lib.r3d_cuda_status(self.h, C.byref(b), int(clear)))
@@ -562,6 +592,10 @@ class Renderer:
         nz, ny, nx = vol.shape
         self._ok(lib.r3d_bricks_begin_volume(self.r, C.byref(VolumeDesc(nx, ny, nz, 128, 1.0)),
                                              _ptr(vol), nlev, min_max), "r3d_bricks_begin")
+
+    def bricks_begin_shard(self, vol, pool_bpa: int = 0) -> None:
+        self._ok(lib.r3d_bricks_begin_shard(self.r, _ptr(vol), vol.shape[0], pool_bpa),
+                 "r3d_bricks_begin_shard")
 
     def bricks_params(self, p: FrameParams) -> None:
         lib.r3d_bricks_params(self.r, C.byref(p))

@@ -63,7 +63,7 @@ extern "C" int r3d_cuda_batch_create(r3d_cuda_ctx *c, const r3d_cuda_request *re
   // group by (path, mode), keep request order inside a group
   uint32_t order[kMaxBatchViews], gcount[kMaxBatchViews], group_of[kMaxBatchViews];
   for (uint32_t i = 0; i < n; i++) {
-    uint32_t key = (b->pcs[i].brick_mode ? 8u : 0u) | b->pcs[i].mode, g = 0;
+    uint32_t key = (uint32_t)path_of(b->pcs[i].brick_mode) * 8u | b->pcs[i].mode, g = 0;
     while (g < b->ngroups && b->gkey[g] != key) g++;
     if (g == b->ngroups) {
       b->gkey[b->ngroups] = key;
@@ -164,10 +164,10 @@ extern "C" int r3d_cuda_batch_launch(r3d_cuda_batch *b, unsigned long long *tota
     L.total = total_steps;
     L.mode = b->gkey[g] & 7u;
     L.fast = c->quality == R3D_QUALITY_FAST;
-    L.lod_bricks = (b->gkey[g] & 8u) != 0u;
+    L.path = (int)(b->gkey[g] >> 3);
     int per_sm = sc.blocks_per_sm
                      ? (int)sc.blocks_per_sm
-                     : persist_blocks_per_sm(L.lod_bricks, L.mode, L.fast, L.unroll);
+                     : persist_blocks_per_sm(L.path, L.mode, L.fast, L.unroll);
     uint32_t want = (uint32_t)per_sm * (uint32_t)sms;
     uint32_t cap = (L.ntiles + 3u) / 4u;
     L.blocks = want < cap ? want : (cap ? cap : 1u);

@@ -188,6 +188,7 @@ r3d::DevScene r3d_cuda_ctx::scene() const {
   memset(&s, 0, sizeof s);
   s.cube = cube;
   s.br = br;
+  s.sh = sh;
   s.status = status;
   s.alpha_cutoff = alpha_cutoff;
   s.tf_zero_t = tf_zero_t;
@@ -249,6 +250,8 @@ void r3d_cuda_destroy(r3d_cuda_ctx *c) {
   cudaFree(c->page);
   cudaFree(c->pool);
   cudaFree(c->bmax);
+  cudaFree(c->shard_buf);
+  cudaFree(c->shard_page);
   cudaFree(c->lut);
   cudaFree(c->status);
   cudaFree(c->img);
@@ -716,10 +719,13 @@ int prepare_view(r3d_cuda_ctx *c, const r3d_frame_params &in, uint32_t out_w,
     return fail(c, R3D_E_UNSUPPORTED, "view: overlay atlases are not implemented");
   if (!(in.max_mip >= 0.0f)) return fail(c, R3D_E_INVALID, "view: max_mip must be >= 0");
   if (!(in.step_voxels > 0.0f)) return fail(c, R3D_E_INVALID, "view: step_voxels must be > 0");
-  if (in.brick_mode) {
-    if (!(in.brick_mode & R3D_BRICK_LOD_FLAG))
-      return fail(c, R3D_E_UNSUPPORTED, "view: single-level brick atlases are not implemented");
+  if (in.brick_mode & R3D_BRICK_LOD_FLAG) {
     if (!c->have_bricks) return fail(c, R3D_E_STATE, "view: no brick cache loaded");
+  } else if (in.brick_mode) {
+    if (!c->have_shard) return fail(c, R3D_E_STATE, "view: no single-level brick atlas loaded");
+    if (in.brick_mode != r3d_cuda_shard_mode(c))
+      return fail(c, R3D_E_INVALID, "view: brick_mode 0x%x does not match the atlas (0x%x)",
+                  in.brick_mode, r3d_cuda_shard_mode(c));
   } else if (!c->have_cube) {
     return fail(c, R3D_E_STATE, "view: no volume uploaded");
   }
@@ -758,7 +764,7 @@ static int launch_views_persistent(r3d_cuda_ctx *c, const r3d_frame_params *pcs,
   uint32_t n = 0;
   for (uint32_t v = 0; v < nviews; v++) {
     if (!render[v]) continue;
-    uint32_t key = (pcs[v].brick_mode ? 8u : 0u) | pcs[v].mode;
+    uint32_t key = (uint32_t)path_of(pcs[v].brick_mode) * 8u | pcs[v].mode;
     uint32_t g = 0;
     while (g < ngroups && gkey[g] != key) g++;
     if (g == ngroups) {
@@ -808,10 +814,10 @@ static int launch_views_persistent(r3d_cuda_ctx *c, const r3d_frame_params *pcs,
     L.counters = counters;
     L.mode = gkey[g] & 7u;
     L.fast = c->quality == R3D_QUALITY_FAST;
-    L.lod_bricks = (gkey[g] & 8u) != 0u;
+    L.path = (int)(gkey[g] >> 3);
     int per_sm = sc.blocks_per_sm
                      ? (int)sc.blocks_per_sm
-                     : persist_blocks_per_sm(L.lod_bricks, L.mode, L.fast, L.unroll);
+                     : persist_blocks_per_sm(L.path, L.mode, L.fast, L.unroll);
     // no more blocks than there are tiles for their warps
     uint32_t want = (uint32_t)per_sm * (uint32_t)dev_sms;
     uint32_t cap = (L.ntiles + 3u) / 4u;

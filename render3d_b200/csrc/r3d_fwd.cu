@@ -184,11 +184,17 @@ cudaError_t launch_view(const r3d_cuda_ctx *c, const r3d_frame_params &pc, uint8
   DevScene s = c->scene();
   bool fast = c->quality == R3D_QUALITY_FAST;
   const uint32_t shade = c->sched.shade_group;
-  if (pc.brick_mode != 0u)
-    return launch_p<PATH_LOD_BRICKS>(pc, s, fast, c->lut, img, out_w, steps, mip_index, total,
-                                     counters, shade, stream);
-  return launch_p<PATH_CUBE>(pc, s, fast, c->lut, img, out_w, steps, mip_index, total, counters,
-                             shade, stream);
+  switch (path_of(pc.brick_mode)) {
+    case PATH_LOD_BRICKS:
+      return launch_p<PATH_LOD_BRICKS>(pc, s, fast, c->lut, img, out_w, steps, mip_index, total,
+                                       counters, shade, stream);
+    case PATH_SHARD:
+      return launch_p<PATH_SHARD>(pc, s, fast, c->lut, img, out_w, steps, mip_index, total,
+                                  counters, shade, stream);
+    default:
+      return launch_p<PATH_CUBE>(pc, s, fast, c->lut, img, out_w, steps, mip_index, total,
+                                 counters, shade, stream);
+  }
 }
 
 }  // namespace r3d

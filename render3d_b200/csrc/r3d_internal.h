@@ -31,6 +31,13 @@ struct r3d_cuda_ctx {
   bool have_bricks = false;
   r3d::DevBricks br{};
 
+  // single-level brick atlas: 4 mip levels, then the world-indexed
+  // occupancy grid, in one allocation; page table of bpa^3 entries
+  uint8_t *shard_buf = nullptr;
+  uint32_t *shard_page = nullptr;
+  bool have_shard = false;
+  r3d::DevShard sh{};
+
   // transfer function
   uchar4 *lut = nullptr;
   uint8_t lut_host[256][4];

@@ -23,7 +23,13 @@ constexpr int kMaxLevels = 16;
 constexpr uint32_t kMaxSteps = 4096u;  // raycast.slang:123
 constexpr float kInv255 = 1.0f / 255.0f;
 
-enum Path { PATH_CUBE = 0, PATH_LOD_BRICKS = 1 };
+enum Path { PATH_CUBE = 0, PATH_LOD_BRICKS = 1, PATH_SHARD = 2 };
+
+// Sampling path of a view from its brick_mode word (raycast.slang:157-160)
+__host__ __device__ inline int path_of(uint32_t brick_mode) {
+  return brick_mode == 0u ? PATH_CUBE
+                          : (brick_mode & R3D_BRICK_LOD_FLAG) ? PATH_LOD_BRICKS : PATH_SHARD;
+}
 
 struct DevCube {
   const uint8_t *lev[kMaxLevels];
@@ -55,9 +61,25 @@ struct DevBricks {
   float inv_scale[kMaxLevels];  // exact: scales are powers of two
 };
 
+// Single-level brick atlas: render3d's bricks mode without the LOD flag
+// (a shard of bpa^3 bricks of 128^3; src/shaders/raycast.slang:163-180,
+// 284-288,800-822,829-860).  The atlas is one texture of (abpa * 128)^3
+// texels with 4 box-filtered mips in which slot s occupies the 128^3 region
+// at (s % abpa, s / abpa % abpa, s / abpa^2) * 128; atlas.occ is the
+// world-indexed dilated 8^3 occupancy grid ((bpa * 16)^3, absent bricks 0).
+struct DevShard {
+  DevCube atlas;
+  const uint32_t *page;  // bpa^3 entries: slot | max << 24, or 0xFFFFFFFF
+  uint32_t bpa, abpa;
+  float n;         // bpa * 128: voxels per axis of the shard
+  float inv_adim;  // 1 / (abpa * 128)
+  uint32_t identity;  // every brick in its own slot: sample the atlas directly
+};
+
 struct DevScene {
   DevCube cube;
   DevBricks br;
+  DevShard sh;
   uint32_t *status;
   float alpha_cutoff;
   float tf_zero_t;  // TF coordinates below this have alpha exactly 0
@@ -322,6 +344,38 @@ __device__ __forceinline__ float brick_fetch(const DevScene &s, uint32_t slot, f
   return tri_slot_at(s.br.pool + (size_t)slot * (128u * 128u * 128u), slot_coord(bl));
 }
 
+// Texel origin of a single-level atlas slot (raycast.slang:176-177)
+__device__ __forceinline__ float3 shard_slot_org(const DevShard &h, uint32_t slot) {
+  const uint32_t sx = slot % h.abpa, sy = (slot / h.abpa) % h.abpa, sz = slot / (h.abpa * h.abpa);
+  return make_float3((float)sx * 128.0f, (float)sy * 128.0f, (float)sz * 128.0f);
+}
+
+// bricks_fetch of the single-level atlas (raycast.slang:284-288): the
+// brick-local position clamped to [inset, 128 - inset] with
+// inset = max(0.5 * 2^lod, 0.5), then the atlas sampled at lod like a cube
+// texture.  e2 = r3d_exp2f(lod).
+__device__ __forceinline__ float shard_fetch(const DevShard &h, float3 org, float3 bl, float lod,
+                                             float e2) {
+  const float inset = fmaxf(0.5f * e2, 0.5f), hi = 128.0f - inset;
+  const float3 u = make_float3((org.x + clamp_(bl.x, inset, hi)) * h.inv_adim,
+                               (org.y + clamp_(bl.y, inset, hi)) * h.inv_adim,
+                               (org.z + clamp_(bl.z, inset, hi)) * h.inv_adim);
+  return cube_sample(h.atlas, u, lod);
+}
+
+// Page entry of brick bi of the shard (raycast.slang:813-821); a slot
+// outside the atlas is treated as absent and flagged.
+__device__ __forceinline__ void shard_entry(const DevScene &s, uint32_t bi, BrickCtx &c) {
+  const uint32_t e = __ldg(s.sh.page + bi);
+  c.ok = e != 0xFFFFFFFFu;
+  c.slot = e & 0xFFFFFFu;
+  if (c.ok && c.slot >= s.sh.abpa * s.sh.abpa * s.sh.abpa) {
+    atomicOr(s.status, R3D_STATUS_PAGE_RANGE);
+    c.ok = false;
+  }
+  c.maxv = c.ok ? (float)(e >> 24) / 255.0f : 0.0f;
+}
+
 // TF lookup (raycast.slang:894) from raw 0..255 RGBA values in shared memory
 __device__ __forceinline__ float4 tf_sample(const float4 *tf, float t) {
   float f;
@@ -348,6 +402,11 @@ __device__ __forceinline__ ViewConst view_const(const r3d_frame_params &pc, cons
     v.vox_inv = s.br.md;
     v.max_lod = (float)(s.br.nlev - 1u);
     v.ext = make_float3(s.br.bs[0] / s.br.md, s.br.bs[1] / s.br.md, s.br.bs[2] / s.br.md);
+  } else if (PATH == PATH_SHARD) {  // raycast.slang:659-661: the atlas has 4 mips
+    v.voxel = 1.0f / s.sh.n;
+    v.vox_inv = s.sh.n;
+    v.max_lod = 3.0f;
+    v.ext = make_float3(1.0f, 1.0f, 1.0f);
   } else {
     v.voxel = 1.0f / (float)s.cube.maxdim;
     v.vox_inv = (float)s.cube.maxdim;
@@ -550,9 +609,15 @@ template <int PATH, int MODE, bool FAST, bool COUNT>
 __device__ __forceinline__ bool composite_sample(const DevScene &s, const ViewConst &vc,
                                                  RayState &st, const Pending &q) {
   constexpr bool kLod = PATH == PATH_LOD_BRICKS;
+  constexpr bool kShard = PATH == PATH_SHARD;
   constexpr bool kShaded = MODE == R3D_MODE_FULL;
   const float3 dir = st.dir;
   float col_r = q.sm.x, col_g = q.sm.y, col_b = q.sm.z;
+  // taps sampled like a cube texture: the cube, or the identity shard atlas
+  const DevCube &tex = kShard ? s.sh.atlas : s.cube;
+  // non-identity shard: taps at lod_step voxels through the slot
+  // (raycast.slang:937-940,972-979)
+  const bool slot_taps = kShard && !s.sh.identity;
   if (kShaded) {
     if (COUNT) st.n_grad++;
     float g0, g1, g2;
@@ -566,12 +631,20 @@ __device__ __forceinline__ bool composite_sample(const DevScene &s, const ViewCo
         q1 = brick_fetch(s, q.slot, make_float3(u.x - ev, u.y - ev, u.z + ev));
         q2 = brick_fetch(s, q.slot, make_float3(u.x - ev, u.y + ev, u.z - ev));
         q3 = brick_fetch(s, q.slot, make_float3(u.x + ev, u.y + ev, u.z + ev));
+      } else if (slot_taps) {
+        const float ev = q.lod_step * ir3;
+        const float3 u = q.bl, org = shard_slot_org(s.sh, q.slot);
+        const float e2 = r3d_exp2f(q.lod);
+        q0 = shard_fetch(s.sh, org, make_float3(u.x + ev, u.y - ev, u.z - ev), q.lod, e2);
+        q1 = shard_fetch(s.sh, org, make_float3(u.x - ev, u.y - ev, u.z + ev), q.lod, e2);
+        q2 = shard_fetch(s.sh, org, make_float3(u.x - ev, u.y + ev, u.z - ev), q.lod, e2);
+        q3 = shard_fetch(s.sh, org, make_float3(u.x + ev, u.y + ev, u.z + ev), q.lod, e2);
       } else {
         float ee = (vc.voxel * q.lod_step) * ir3;
-        q0 = cube_sample(s.cube, make_float3(q.p.x + ee, q.p.y - ee, q.p.z - ee), q.lod);
-        q1 = cube_sample(s.cube, make_float3(q.p.x - ee, q.p.y - ee, q.p.z + ee), q.lod);
-        q2 = cube_sample(s.cube, make_float3(q.p.x - ee, q.p.y + ee, q.p.z - ee), q.lod);
-        q3 = cube_sample(s.cube, make_float3(q.p.x + ee, q.p.y + ee, q.p.z + ee), q.lod);
+        q0 = cube_sample(tex, make_float3(q.p.x + ee, q.p.y - ee, q.p.z - ee), q.lod);
+        q1 = cube_sample(tex, make_float3(q.p.x - ee, q.p.y - ee, q.p.z + ee), q.lod);
+        q2 = cube_sample(tex, make_float3(q.p.x - ee, q.p.y + ee, q.p.z - ee), q.lod);
+        q3 = cube_sample(tex, make_float3(q.p.x + ee, q.p.y + ee, q.p.z + ee), q.lod);
       }
       g0 = (((q0 - q1) - q2) + q3) * renorm;
       g1 = (((-q0 - q1) + q2) + q3) * renorm;
@@ -598,14 +671,24 @@ __device__ __forceinline__ bool composite_sample(const DevScene &s, const ViewCo
         a.z0 = slot_axis(u.z + ev, a.fz);
         b.z0 = slot_axis(u.z - ev, b.fz);
         g2 = tri_slot_at(g, a) - tri_slot_at(g, b);
+      } else if (slot_taps) {
+        const float ev = q.lod_step;
+        const float3 u = q.bl, org = shard_slot_org(s.sh, q.slot);
+        const float e2 = r3d_exp2f(q.lod);
+        g0 = shard_fetch(s.sh, org, make_float3(u.x + ev, u.y, u.z), q.lod, e2) -
+             shard_fetch(s.sh, org, make_float3(u.x - ev, u.y, u.z), q.lod, e2);
+        g1 = shard_fetch(s.sh, org, make_float3(u.x, u.y + ev, u.z), q.lod, e2) -
+             shard_fetch(s.sh, org, make_float3(u.x, u.y - ev, u.z), q.lod, e2);
+        g2 = shard_fetch(s.sh, org, make_float3(u.x, u.y, u.z + ev), q.lod, e2) -
+             shard_fetch(s.sh, org, make_float3(u.x, u.y, u.z - ev), q.lod, e2);
       } else {
         float e = vc.voxel * q.lod_step;
-        g0 = cube_sample(s.cube, make_float3(q.p.x + e, q.p.y, q.p.z), q.lod) -
-             cube_sample(s.cube, make_float3(q.p.x - e, q.p.y, q.p.z), q.lod);
-        g1 = cube_sample(s.cube, make_float3(q.p.x, q.p.y + e, q.p.z), q.lod) -
-             cube_sample(s.cube, make_float3(q.p.x, q.p.y - e, q.p.z), q.lod);
-        g2 = cube_sample(s.cube, make_float3(q.p.x, q.p.y, q.p.z + e), q.lod) -
-             cube_sample(s.cube, make_float3(q.p.x, q.p.y, q.p.z - e), q.lod);
+        g0 = cube_sample(tex, make_float3(q.p.x + e, q.p.y, q.p.z), q.lod) -
+             cube_sample(tex, make_float3(q.p.x - e, q.p.y, q.p.z), q.lod);
+        g1 = cube_sample(tex, make_float3(q.p.x, q.p.y + e, q.p.z), q.lod) -
+             cube_sample(tex, make_float3(q.p.x, q.p.y - e, q.p.z), q.lod);
+        g2 = cube_sample(tex, make_float3(q.p.x, q.p.y, q.p.z + e), q.lod) -
+             cube_sample(tex, make_float3(q.p.x, q.p.y, q.p.z - e), q.lod);
       }
     }
     float3 gv = make_float3(g0, g1, g2);
@@ -667,6 +750,7 @@ template <int PATH, int MODE, bool FAST, bool COUNT, bool DEFER = false>
 __device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, const float4 *tf,
                                         RayState &st, Pending &pend) {
   constexpr bool kLod = PATH == PATH_LOD_BRICKS;
+  constexpr bool kShard = PATH == PATH_SHARD;
   constexpr bool kComposite = MODE == R3D_MODE_FULL || MODE == R3D_MODE_FLAT;
   constexpr bool kShaded = MODE == R3D_MODE_FULL;
   constexpr uint32_t ray_budget = kLod ? (kShaded ? 192u : 256u) : kMaxSteps;
@@ -735,6 +819,28 @@ __device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, 
       }
       v = tri_slot_at(s.br.pool + (size_t)b.slot * (128u * 128u * 128u), q);
     }
+  } else if (kShard) {
+    const DevShard &h = s.sh;
+    if (h.identity) {  // atlas layout == world layout (raycast.slang:800-805)
+      v = cube_sample(h.atlas, p, lod);
+    } else {
+      // page entry cached until the brick changes (raycast.slang:806-822)
+      const float3 vp = make_float3(sat_(p.x) * h.n, sat_(p.y) * h.n, sat_(p.z) * h.n);
+      const uint32_t bx = min((uint32_t)vp.x >> 7, h.bpa - 1u);
+      const uint32_t by = min((uint32_t)vp.y >> 7, h.bpa - 1u);
+      const uint32_t bz = min((uint32_t)vp.z >> 7, h.bpa - 1u);
+      const uint32_t bi = (bz * h.bpa + by) * h.bpa + bx;
+      if ((int)bi != st.lc.desired) {
+        st.lc.desired = (int)bi;
+        shard_entry(s, bi, st.lc.c);
+        if (COUNT) st.n_walk++;
+      }
+      b = st.lc.c;
+      b.bl = make_float3(vp.x - (float)(bx << 7), vp.y - (float)(by << 7), vp.z - (float)(bz << 7));
+      v = b.ok ? shard_fetch(h, shard_slot_org(h, b.slot), b.bl, lod,
+                             lod == 0.0f ? 1.0f : r3d_exp2f(lod))
+               : 0.0f;
+    }
   } else {
     v = cube_sample(s.cube, p, lod);
   }
@@ -747,6 +853,21 @@ __device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, 
         (v < vc.bgate && b.maxv < vc.bgate)) {
       st.t = skip_block(st, p, b.world_brick);
       return kStepCont;
+    }
+  } else if (kShard) {
+    if (v < vc.bgate) {
+      if (s.sh.identity) {  // 8^3 occupancy only
+        if (occ_sample(s.sh.atlas, p) < vc.bgate) {
+          st.t = skip_block(st, p, vc.bs);
+          return kStepCont;
+        }
+      } else if (b.maxv < vc.bgate) {  // whole brick (cached page entry)
+        st.t = skip_block(st, p, 128.0f * vc.voxel);
+        return kStepCont;
+      } else if (occ_sample(s.sh.atlas, p) < vc.bgate) {  // 8^3 block
+        st.t = skip_block(st, p, vc.bs);
+        return kStepCont;
+      }
     }
   } else if (v < vc.occ_gate && occ_sample(s.cube, p) < vc.occ_gate) {
     st.t = skip_block(st, p, vc.bs);

@@ -73,7 +73,7 @@ extern "C" int r3d_cuda_raycast_fwd_noalloc(r3d_cuda_ctx *c, const r3d_frame_par
   uint32_t gcount[kNoallocViews], gstart[kNoallocViews + 1], ngroups = 0, n = 0;
   for (uint32_t v = 0; v < nviews; v++) {
     if (!render[v]) continue;
-    uint32_t key = (pcs[v].brick_mode ? 8u : 0u) | pcs[v].mode, g = 0;
+    uint32_t key = (uint32_t)path_of(pcs[v].brick_mode) * 8u | pcs[v].mode, g = 0;
     while (g < ngroups && gkey[g] != key) g++;
     if (g == ngroups) {
       gkey[ngroups] = key;
@@ -118,9 +118,9 @@ extern "C" int r3d_cuda_raycast_fwd_noalloc(r3d_cuda_ctx *c, const r3d_frame_par
     L.unroll = 1u;
     L.mode = gkey[g] & 7u;
     L.fast = c->quality == R3D_QUALITY_FAST;
-    L.lod_bricks = (gkey[g] & 8u) != 0u;
+    L.path = (int)(gkey[g] >> 3);
     uint32_t want =
-        (uint32_t)persist_blocks_per_sm(L.lod_bricks, L.mode, L.fast, 1u) * (uint32_t)sms;
+        (uint32_t)persist_blocks_per_sm(L.path, L.mode, L.fast, 1u) * (uint32_t)sms;
     uint32_t cap = (L.ntiles + 3u) / 4u;
     L.blocks = want < cap ? want : (cap ? cap : 1u);
     cudaError_t e = launch_persist(L, s, st);

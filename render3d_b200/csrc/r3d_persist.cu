@@ -231,23 +231,29 @@ static cudaError_t launch_pm(const PersistLaunch &L, const DevScene &s, cudaStre
 }
 
 cudaError_t launch_persist(const PersistLaunch &L, const DevScene &s, cudaStream_t st) {
-  return L.lod_bricks ? launch_pm<PATH_LOD_BRICKS>(L, s, st) : launch_pm<PATH_CUBE>(L, s, st);
+  switch (L.path) {
+    case PATH_LOD_BRICKS: return launch_pm<PATH_LOD_BRICKS>(L, s, st);
+    case PATH_SHARD: return launch_pm<PATH_SHARD>(L, s, st);
+    default: return launch_pm<PATH_CUBE>(L, s, st);
+  }
 }
 
-int persist_blocks_per_sm(bool lod_bricks, uint32_t mode, bool fast, uint32_t unroll) {
+int persist_blocks_per_sm(int path, uint32_t mode, bool fast, uint32_t unroll) {
   // occupancy of the instantiation that launch_persist would pick
   int n = 0;
   cudaError_t e = cudaSuccess;
 #define R3D_OCC(P, M, F, U)                                                            \
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_raycast_persist<P, M, F, false, U>, \
                                                     128, 0)
-  if (lod_bricks) {
+  if (path == PATH_LOD_BRICKS) {
     if (mode == R3D_MODE_FULL && !fast) {
       if (unroll == 2) R3D_OCC(PATH_LOD_BRICKS, R3D_MODE_FULL, false, 2);
       else R3D_OCC(PATH_LOD_BRICKS, R3D_MODE_FULL, false, 1);
     } else {
       R3D_OCC(PATH_LOD_BRICKS, R3D_MODE_MIP, false, 1);
     }
+  } else if (path == PATH_SHARD) {
+    R3D_OCC(PATH_SHARD, R3D_MODE_FULL, false, 1);
   } else {
     R3D_OCC(PATH_CUBE, R3D_MODE_FULL, false, 1);
   }

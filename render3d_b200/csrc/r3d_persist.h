@@ -30,7 +30,7 @@ struct PersistLaunch {
   uint32_t blocks;
   uint32_t mode;
   bool fast;
-  bool lod_bricks;
+  int path;  // PATH_CUBE, PATH_LOD_BRICKS or PATH_SHARD
 };
 
 // Tile geometry for a tile shape (0: 8x4, 1: 16x2, 2: 32x1).
@@ -49,6 +49,6 @@ inline uint32_t view_tiles(DevView &v, uint32_t shape) {
 }
 
 cudaError_t launch_persist(const PersistLaunch &L, const DevScene &s, cudaStream_t st);
-int persist_blocks_per_sm(bool lod_bricks, uint32_t mode, bool fast, uint32_t unroll);
+int persist_blocks_per_sm(int path, uint32_t mode, bool fast, uint32_t unroll);
 
 }  // namespace r3d

@@ -122,6 +122,22 @@ int r3d_bricks_begin_volume(r3d_renderer *r, const r3d_volume_desc *d, const uin
   return 0;
 }
 
+int r3d_bricks_begin_shard(r3d_renderer *r, const uint8_t *voxels, uint32_t edge,
+                           uint32_t pool_bpa) {
+  if (!r) return -1;
+  if (pool_bpa && pool_bpa < edge / 128u) {
+    fprintf(stderr, "r3d: bricks_begin_shard: a pool smaller than the shard needs streaming "
+                    "residency, which is not available\n");
+    return -1;
+  }
+  int rc = r3d_cuda_shard_build(r->ctx, edge, voxels, edge / 128u, NULL);
+  if (rc != R3D_OK) return report(r, "bricks_begin_shard", rc);
+  r->bricks = 1;
+  r->brick_mode = r3d_cuda_shard_mode(r->ctx);
+  r->shape[0] = r->shape[1] = r->shape[2] = edge;
+  return 0;
+}
+
 int r3d_bricks_end(r3d_renderer *r) {
   if (!r) return -1;
   r->bricks = 0;
