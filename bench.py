@@ -248,23 +248,29 @@ def fwd_bwd_bench(rb, ctx, torch, local: int, steps: int, adam_steps: int) -> di
     gs = torch.empty(1, device=dev)
     grad = torch.empty(nf, device=dev)
 
-    def step():
-        ctx.diff_forward(dens, lut, views, rgb, stream=ctx.stream)
+    def step(tape=True):
+        # training forward (records the tape), loss gradient, adjoint
+        ctx.diff_forward(dens, lut, views, rgb, stream=ctx.stream, tape=tape)
         with torch.cuda.stream(st):
             torch.sub(rgb, target, out=grad)
             grad.mul_(2.0)
-        ctx.raycast_bwd(dens, lut, views, grad, gd, gl, gs, 64, True, stream=ctx.stream)
+        ctx.raycast_bwd(dens, lut, views, grad, gd, gl, gs, 64, True, stream=ctx.stream,
+                        tape=tape)
 
-    for _ in range(3):
-        step()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(st)
-    for _ in range(steps):
-        step()
-    e1.record(st)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / steps
+    def timed(tape):
+        for _ in range(3):
+            step(tape)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(steps):
+            step(tape)
+        e1.record(st)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    ms_ck = timed(False)  # backward re-marches every ray from its checkpoints
+    ms = timed(True)
     # 100 Adam steps on the voxels, LUT and density scale
     p_dens = dens.clone().requires_grad_(False)
     opt_state = [torch.zeros_like(p_dens), torch.zeros_like(p_dens)]
@@ -272,12 +278,13 @@ def fwd_bwd_bench(rb, ctx, torch, local: int, steps: int, adam_steps: int) -> di
     t0 = time.perf_counter()
     b1, b2, lr, eps = 0.9, 0.999, 2e-3, 1e-8
     for it in range(1, adam_steps + 1):
-        ctx.diff_forward(p_dens, lut, views, rgb, stream=ctx.stream)
+        ctx.diff_forward(p_dens, lut, views, rgb, stream=ctx.stream, tape=True)
         with torch.cuda.stream(st):
             torch.sub(rgb, target, out=grad)
             loss = float((grad * grad).sum().item()) if it in (1, adam_steps) else None
             grad.mul_(2.0)
-        ctx.raycast_bwd(p_dens, lut, views, grad, gd, gl, gs, 64, True, stream=ctx.stream)
+        ctx.raycast_bwd(p_dens, lut, views, grad, gd, gl, gs, 64, True, stream=ctx.stream,
+                        tape=True)
         with torch.cuda.stream(st):
             m, v2 = opt_state
             m.mul_(b1).add_(gd, alpha=1 - b1)
@@ -291,8 +298,10 @@ def fwd_bwd_bench(rb, ctx, torch, local: int, steps: int, adam_steps: int) -> di
     torch.cuda.synchronize()
     adam_s = time.perf_counter() - t0
     return {"workload": "256^3 FP32 density (phantom/255 + N(0,10/255)), 64 orbit views 256x256, "
-                        "step 0.5, L2 loss, checkpoints every 64 samples, deterministic",
+                        "step 0.5, L2 loss, tape of 64 contributions per ray (checkpoints "
+                        "every 64 samples beyond it), deterministic",
             "value": samples / (ms * 1e-3) / 1e9, "unit": "Gsamples/s", "ms_per_step": ms,
+            "ms_per_step_checkpoints_only": ms_ck,
             "samples_per_step": samples, "steps": steps,
             "adam": {"steps": adam_steps, "loss_first": loss0, "loss_last": lossN,
                      "s_per_step": adam_s / adam_steps}}
@@ -708,6 +717,14 @@ def run_sparse(args) -> None:
             e1.record(st)
             torch.cuda.synchronize()
             bwd[f"bwd_k{k}_{'det' if det else 'atomic'}_ms"] = e0.elapsed_time(e1) / 3
+            ctx.diff_forward(dens, flut, views, rgb, stream=ctx.stream, tape=True)
+            e0.record(st)
+            for _ in range(3):
+                ctx.raycast_bwd(dens, flut, views, grad, gd, gl, gs, k, det, stream=ctx.stream,
+                                tape=True)
+            e1.record(st)
+            torch.cuda.synchronize()
+            bwd[f"bwd_k{k}_{'det' if det else 'atomic'}_tape_ms"] = e0.elapsed_time(e1) / 3
     out["adjoint_512"] = bwd
     ctx.close()
     print(json.dumps(out), flush=True)

@@ -270,13 +270,32 @@ int r3d_cuda_diff_forward(r3d_cuda_ctx *ctx, const r3d_cuda_diff_scene *scene,
                           const r3d_frame_params *views, uint32_t nviews, float *rgb_out,
                           unsigned long long *total_steps, void *stream);
 
+/* The same render, recording a tape for the backward: per ray, the first 64
+ * contributing samples (march position and the opacity accumulated before
+ * them) and their count, in a context-owned buffer of 516 bytes per ray.
+ * A later r3d_cuda_raycast_bwd with R3D_BWD_TAPE over the same views and
+ * scene (same buffers, sizes and cutoff) reads it instead of marching the
+ * rays forward again; the grid and LUT contents must not change in
+ * between, and the backward must be ordered after this call.  Each call
+ * replaces the tape. */
+int r3d_cuda_diff_forward_tape(r3d_cuda_ctx *ctx, const r3d_cuda_diff_scene *scene,
+                               const r3d_frame_params *views, uint32_t nviews, float *rgb_out,
+                               unsigned long long *total_steps, void *stream);
+
+#define R3D_BWD_DETERMINISTIC 1u /* fixed-point accumulation */
+#define R3D_BWD_TAPE 2u          /* use the tape of r3d_cuda_diff_forward_tape */
+
 /* Adjoint of r3d_cuda_diff_forward: given dL/drgb in rgb_out's layout,
  * writes dL/dvoxel, dL/dLUT and dL/ddensity.  The march is recomputed in
  * reverse from checkpoints kept every ckpt_k (32, 64 or 128) samples.
- * deterministic = 0: FP32 atomic accumulation (last bits depend on the
- * execution order); 1: fixed-point accumulation (2^-32 resolution, int64),
- * bit-identical from run to run, using a context-owned buffer of
- * 8 * (nvox + 1025) bytes. */
+ * deterministic (flags): without R3D_BWD_DETERMINISTIC, FP32 atomic
+ * accumulation (last bits depend on the execution order); with it,
+ * fixed-point accumulation (2^-32 resolution, int64), bit-identical from
+ * run to run, using a context-owned buffer of 8 * (nvox + 1025) bytes.
+ * R3D_BWD_TAPE: rays whose contributions are all on the tape of the
+ * matching r3d_cuda_diff_forward_tape skip the forward sweep (same
+ * gradients, bit for bit in deterministic mode); R3D_E_STATE when no such
+ * tape exists. */
 int r3d_cuda_raycast_bwd(r3d_cuda_ctx *ctx, const r3d_cuda_diff_scene *scene,
                          const r3d_frame_params *views, uint32_t nviews, const float *dl_drgb,
                          const r3d_cuda_grads *out, uint32_t ckpt_k, int deterministic,

@@ -149,6 +149,7 @@ def _load() -> C.CDLL:
         "r3d_cuda_set_schedule": (I, [P, C.POINTER(Schedule)]),
         "r3d_cuda_raycast_fwd_noalloc": (I, [P, P, U32, P, U32, U32, P]),
         "r3d_cuda_diff_forward": (I, [P, C.POINTER(DiffScene), P, U32, P, P, P]),
+        "r3d_cuda_diff_forward_tape": (I, [P, C.POINTER(DiffScene), P, U32, P, P, P]),
         "r3d_cuda_batch_create": (I, [P, P, U32, C.POINTER(P)]),
         "r3d_cuda_batch_destroy": (None, [P]),
         "r3d_cuda_batch_set_schedule": (I, [P, C.POINTER(Schedule)]),
@@ -449,20 +450,23 @@ class Context:
                                              C.byref(aux) if aux else None, stream or None))
         return out
 
-    def diff_forward(self, density, lut, views, rgb_out, total=None, stream: int = 0):
+    def diff_forward(self, density, lut, views, rgb_out, total=None, stream: int = 0,
+                     tape: bool = False):
         """Differentiable render (device tensors): density (nz, ny, nx) f32,
-        lut (256, 4) f32, rgb_out f32 of sum(w*h*3) over the views."""
+        lut (256, 4) f32, rgb_out f32 of sum(w*h*3) over the views.  tape:
+        record the tape a raycast_bwd(tape=True) over the same views reads."""
         if isinstance(views, FrameParams):
             views = [views]
         arr = (FrameParams * len(views))(*views)
         nz, ny, nx = density.shape
         sc = DiffScene(_ptr(density), nx, ny, nz, _ptr(lut))
-        self._check(lib.r3d_cuda_diff_forward(self.h, C.byref(sc), arr, len(views),
-                                              _ptr(rgb_out), _ptr(total) or None,
-                                              stream or None))
+        fn = lib.r3d_cuda_diff_forward_tape if tape else lib.r3d_cuda_diff_forward
+        self._check(fn(self.h, C.byref(sc), arr, len(views), _ptr(rgb_out), _ptr(total) or None,
+                       stream or None))
 
     def raycast_bwd(self, density, lut, views, dl_drgb, g_density, g_lut, g_scale,
-                    ckpt_k: int = 32, deterministic: bool = False, stream: int = 0):
+                    ckpt_k: int = 32, deterministic: bool = False, stream: int = 0,
+                    tape: bool = False):
         """Adjoint of diff_forward into the given device gradient buffers."""
         if isinstance(views, FrameParams):
             views = [views]
@@ -472,7 +476,8 @@ class Context:
         gr = Grads(_ptr(g_density), _ptr(g_lut), _ptr(g_scale))
         self._check(lib.r3d_cuda_raycast_bwd(self.h, C.byref(sc), arr, len(views),
                                              _ptr(dl_drgb), C.byref(gr), ckpt_k,
-                                             int(deterministic), stream or None))
+                                             int(deterministic) | (2 if tape else 0),
+                                             stream or None))
 
     def phantom(self, shape, seed: int = 1234, out=None):
         """Seeded scroll phantom generated on the device: a (nz, ny, nx) uint8

@@ -258,6 +258,8 @@ void r3d_cuda_destroy(r3d_cuda_ctx *c) {
   cudaFree(c->aux_buf);
   cudaFree(c->total);
   cudaFree(c->diff_q);
+  cudaFree(c->tape);
+  cudaFree(c->tape_n);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   for (int k = 0; k < r3d_cuda_ctx::kRing; k++)

@@ -156,10 +156,19 @@ __device__ __forceinline__ void diff_tf(const DiffGrid &g, float k, DiffSample &
   o.a = 1.0f - r3d_powf(1.0f - o.alpha, k);
 }
 
+// Tape of a training forward: per ray, the first kTape contributing samples
+// (t, accumulated opacity before the sample) and their count.  A backward
+// over the same views and scene walks these in reverse instead of marching
+// the ray again; rays with more contributions take the checkpoint path.
+constexpr uint32_t kTape = 64;
+
+template <bool TAPE>
 __global__ void __launch_bounds__(128) k_diff_fwd(const DiffView *__restrict__ views,
                                                   const __grid_constant__ DiffGrid g,
                                                   float *__restrict__ rgb,
-                                                  unsigned long long *__restrict__ total) {
+                                                  unsigned long long *__restrict__ total,
+                                                  float2 *__restrict__ tape,
+                                                  uint32_t *__restrict__ tape_n) {
   const DiffView &vw = views[blockIdx.z];
   const r3d_frame_params &pc = vw.pc;
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
@@ -168,9 +177,11 @@ __global__ void __launch_bounds__(128) k_diff_fwd(const DiffView *__restrict__ v
   const uint32_t py = blockIdx.y * 8u + (warp >> 1) * 4u + (((lane >> 1) & 1u) | ((lane >> 2) & 2u));
   uint32_t steps = 0;
   if (px < pc.viewport[0] && py < pc.viewport[1]) {
+    const size_t ray = vw.out_off / 3u + (size_t)py * pc.viewport[0] + px;
     DiffRay r;
     diff_setup(pc, g, px, py, r);
     float acc_r = 0.0f, acc_g = 0.0f, acc_b = 0.0f, acc_a = 0.0f;
+    uint32_t nc = 0;
     if (r.hit) {
       const float k = (pc.density * pc.step_voxels) * r.span;
       float t = r.t0;
@@ -181,6 +192,8 @@ __global__ void __launch_bounds__(128) k_diff_fwd(const DiffView *__restrict__ v
         if (!(s.v < pc.threshold)) {
           diff_tf(g, k, s);
           if (s.a > 0.003f) {
+            if (TAPE && nc < kTape) tape[ray * kTape + nc] = make_float2(t, acc_a);
+            nc++;
             float w = (1.0f - acc_a) * s.a;
             acc_r = fmaf(w, s.s[0], acc_r);
             acc_g = fmaf(w, s.s[1], acc_g);
@@ -192,6 +205,7 @@ __global__ void __launch_bounds__(128) k_diff_fwd(const DiffView *__restrict__ v
         t = fmaf(r.dt, r.span, t);
       }
     }
+    if (TAPE) tape_n[ray] = nc;
     float tr = 1.0f - acc_a;
     float *o = rgb + vw.out_off + ((size_t)py * pc.viewport[0] + px) * 3u;
     o[0] = fmaf(tr, 0.02f, acc_r);
@@ -217,6 +231,88 @@ __device__ __forceinline__ void vox_add(float *gf, unsigned long long *gq, uint3
 
 constexpr int kRing = 64;  // contributing samples remembered by the forward sweep
 
+// State of one ray's reverse sweep: the colour behind the current sample,
+// the trilinear cell whose voxel gradients are being summed, and the
+// density-scale gradient.
+struct BwdRay {
+  float gr, gg, gb;  // dL/drgb of the pixel
+  float k, kstep;
+  float S_r, S_g, S_b;
+  uint32_t cell, csx, csy, csz;
+  float cw[8];
+  float g_density;
+};
+
+template <bool DET>
+__device__ __forceinline__ void bwd_flush(BwdRay &b, float *g_dens, unsigned long long *q_dens) {
+  if (b.cell == 0xffffffffu) return;
+#pragma unroll
+  for (int c = 0; c < 8; c++)
+    vox_add<DET>(g_dens, q_dens,
+                 b.cell + ((c & 1) ? b.csx : 0u) + ((c & 2) ? b.csy : 0u) + ((c & 4) ? b.csz : 0u),
+                 b.cw[c]);
+}
+
+// Adjoint of one contributing sample at t with accumulated opacity acc_a
+// before it, visited in reverse order (suffix colour S <- a c + (1 - a) S).
+template <bool DET>
+__device__ __forceinline__ void bwd_sample(const DiffGrid &g, const DiffRay &r, float t,
+                                           float acc_a, BwdRay &b, float *s_lut,
+                                           unsigned long long *s_qlut, float *g_dens,
+                                           unsigned long long *q_dens) {
+  DiffSample s;
+  diff_sample(g, r, t, s);
+  diff_tf(g, b.k, s);
+  const float tprev = 1.0f - acc_a;
+  const float dc_r = b.gr * tprev * s.a, dc_g = b.gg * tprev * s.a, dc_b = b.gb * tprev * s.a;
+  const float da = b.gr * tprev * (s.s[0] - b.S_r) + b.gg * tprev * (s.s[1] - b.S_g) +
+                   b.gb * tprev * (s.s[2] - b.S_b);
+  b.S_r = fmaf(s.a, s.s[0] - b.S_r, b.S_r);
+  b.S_g = fmaf(s.a, s.s[1] - b.S_g, b.S_g);
+  b.S_b = fmaf(s.a, s.s[2] - b.S_b, b.S_b);
+  float dalpha = 0.0f;
+  const bool alpha_free = s.s[3] > 0.0f && s.s[3] < 1.0f;
+  if (alpha_free) dalpha = da * b.k * r3d_powf(1.0f - s.alpha, b.k - 1.0f);
+  if (s.alpha < 1.0f)
+    b.g_density += da * (-(1.0f - s.a) * (r3d_log2f(1.0f - s.alpha) * 0.693147181f)) * b.kstep;
+  const float ds[4] = {dc_r, dc_g, dc_b, dalpha};
+  const float lf0 = 1.0f - s.f;
+  const float4 l0 = __ldg((const float4 *)g.lut + s.i0);
+  const float4 l1 = __ldg((const float4 *)g.lut + s.i1);
+  const float dl[4] = {l1.x - l0.x, l1.y - l0.y, l1.z - l0.z, l1.w - l0.w};
+  float dvv = 0.0f;
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    if (DET) {
+      atomicAdd(&s_qlut[s.i0 * 4u + c],
+                (unsigned long long)__double2ll_rn((double)(ds[c] * lf0) * kFix));
+      atomicAdd(&s_qlut[s.i1 * 4u + c],
+                (unsigned long long)__double2ll_rn((double)(ds[c] * s.f) * kFix));
+    } else {
+      atomicAdd(&s_lut[s.i0 * 4u + c], ds[c] * lf0);
+      atomicAdd(&s_lut[s.i1 * 4u + c], ds[c] * s.f);
+    }
+    dvv = fmaf(ds[c], dl[c], dvv);
+  }
+  const bool tt_free = s.tt > 0.0f && s.tt < 255.0f;
+  const float dv = tt_free ? dvv * 256.0f : 0.0f;
+  // trilinear scatter, aggregated per cell
+  if (s.base != b.cell || s.sx != b.csx || s.sy != b.csy || s.sz != b.csz) {
+    bwd_flush<DET>(b, g_dens, q_dens);
+    b.cell = s.base;
+    b.csx = s.sx;
+    b.csy = s.sy;
+    b.csz = s.sz;
+#pragma unroll
+    for (int c = 0; c < 8; c++) b.cw[c] = 0.0f;
+  }
+  const float wx[2] = {1.0f - s.fx, s.fx}, wy[2] = {1.0f - s.fy, s.fy},
+              wz[2] = {1.0f - s.fz, s.fz};
+#pragma unroll
+  for (int c = 0; c < 8; c++)
+    b.cw[c] = fmaf(dv, (wx[c & 1] * wy[(c >> 1) & 1]) * wz[c >> 2], b.cw[c]);
+}
+
 template <int K, bool DET>
 __global__ void __launch_bounds__(128) k_diff_bwd(const DiffView *__restrict__ views,
                                                   const __grid_constant__ DiffGrid g,
@@ -226,7 +322,9 @@ __global__ void __launch_bounds__(128) k_diff_bwd(const DiffView *__restrict__ v
                                                   float *__restrict__ g_lut,
                                                   unsigned long long *__restrict__ q_lut,
                                                   float *__restrict__ g_scale,
-                                                  unsigned long long *__restrict__ q_scale) {
+                                                  unsigned long long *__restrict__ q_scale,
+                                                  const float2 *__restrict__ tape,
+                                                  const uint32_t *__restrict__ tape_n) {
   constexpr int kMaxCk = (4096 + K - 1) / K;
   __shared__ float s_lut[DET ? 1 : 1024];
   __shared__ unsigned long long s_qlut[DET ? 1024 : 1];
@@ -244,161 +342,111 @@ __global__ void __launch_bounds__(128) k_diff_bwd(const DiffView *__restrict__ v
   const uint32_t px = blockIdx.x * 16u + (warp & 1u) * 8u +
                       ((lane & 1u) | ((lane >> 1) & 2u) | ((lane >> 2) & 4u));
   const uint32_t py = blockIdx.y * 8u + (warp >> 1) * 4u + (((lane >> 1) & 1u) | ((lane >> 2) & 2u));
-  float g_density = 0.0f;
+  BwdRay b;
+  b.g_density = 0.0f;
   if (px < pc.viewport[0] && py < pc.viewport[1]) {
+    const size_t ray = vw.out_off / 3u + (size_t)py * pc.viewport[0] + px;
     DiffRay r;
     diff_setup(pc, g, px, py, r);
     const float *gp = dl_drgb + vw.out_off + ((size_t)py * pc.viewport[0] + px) * 3u;
-    const float gr = gp[0], gg = gp[1], gb = gp[2];
-    if (r.hit && (gr != 0.0f || gg != 0.0f || gb != 0.0f)) {
-      const float kstep = pc.step_voxels * r.span;
-      const float k = (pc.density * pc.step_voxels) * r.span;
-      // forward sweep: checkpoints (t, accumulated opacity) before steps
-      // 1, K+1, 2K+1, ..., the number of contributing samples of each
-      // segment, and the last kRing contributing samples themselves
-      float ck_t[kMaxCk], ck_a[kMaxCk];
-      uint8_t ck_n[kMaxCk];
-      float ring_t[kRing], ring_a[kRing];
-      uint32_t nsteps = 0, ncontrib = 0;
-      {
-        float t = r.t0, acc_a = 0.0f;
-        while (t < r.tf && nsteps < 4096u) {
-          if (nsteps % K == 0u) {
-            ck_t[nsteps / K] = t;
-            ck_a[nsteps / K] = acc_a;
-            ck_n[nsteps / K] = 0;
-          }
-          nsteps++;
-          DiffSample s;
-          diff_sample(g, r, t, s);
-          bool stop = false;
-          if (!(s.v < pc.threshold)) {
-            diff_tf(g, k, s);
-            if (s.a > 0.003f) {
-              ring_t[ncontrib % kRing] = t;
-              ring_a[ncontrib % kRing] = acc_a;
-              ncontrib++;
-              ck_n[(nsteps - 1u) / K]++;
-              acc_a = acc_a + (1.0f - acc_a) * s.a;
-              stop = acc_a >= g.cutoff;
-            }
-          }
-          if (stop) break;
-          t = fmaf(r.dt, r.span, t);
+    b.gr = gp[0];
+    b.gg = gp[1];
+    b.gb = gp[2];
+    b.k = (pc.density * pc.step_voxels) * r.span;
+    b.kstep = pc.step_voxels * r.span;
+    b.S_r = 0.02f;
+    b.S_g = 0.02f;
+    b.S_b = 0.03f;
+    b.cell = 0xffffffffu;
+    b.csx = b.csy = b.csz = 0u;
+#pragma unroll
+    for (int c = 0; c < 8; c++) b.cw[c] = 0.0f;
+    const uint32_t ntape = tape ? tape_n[ray] : 0xffffffffu;
+    if (r.hit && (b.gr != 0.0f || b.gg != 0.0f || b.gb != 0.0f)) {
+      if (ntape <= kTape) {  // every contribution is on the tape
+        for (int i = (int)ntape - 1; i >= 0; i--) {
+          const float2 e = __ldg(tape + ray * kTape + i);
+          bwd_sample<DET>(g, r, e.x, e.y, b, s_lut, s_qlut, g_dens, q_dens);
         }
-      }
-      // reverse sweep over segments with contributions
-      float S_r = 0.02f, S_g = 0.02f, S_b = 0.03f;
-      // current trilinear cell of the voxel-gradient aggregation
-      uint32_t cell = 0xffffffffu, csx = 0, csy = 0, csz = 0;
-      float cw[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      float seg_t[K], seg_a[K];
-      const int nck = (int)((nsteps + K - 1) / K);
-      uint32_t end = ncontrib;  // contributions of segments < j: [0, end)
-      for (int j = nck - 1; j >= 0; j--) {
-        const uint32_t nj = ck_n[j];
-        if (nj == 0u) continue;
-        const uint32_t start = end - nj;
-        const bool in_ring = ncontrib - start <= (uint32_t)kRing;
-        int nseg = 0;
-        if (in_ring) {  // the segment's samples are still in the ring
-          for (uint32_t i = start; i < end; i++) {
-            seg_t[nseg] = ring_t[i % kRing];
-            seg_a[nseg] = ring_a[i % kRing];
-            nseg++;
-          }
-        } else {  // recompute segment j from its checkpoint
-          float t = ck_t[j], acc_a = ck_a[j];
-          const uint32_t s_end = min(nsteps, (uint32_t)(j + 1) * K);
-          for (uint32_t st = (uint32_t)j * K; st < s_end; st++) {
+      } else {
+        // forward sweep: checkpoints (t, accumulated opacity) before steps
+        // 1, K+1, 2K+1, ..., the number of contributing samples of each
+        // segment, and the last kRing contributing samples themselves
+        float ck_t[kMaxCk], ck_a[kMaxCk];
+        uint8_t ck_n[kMaxCk];
+        float ring_t[kRing], ring_a[kRing];
+        uint32_t nsteps = 0, ncontrib = 0;
+        {
+          float t = r.t0, acc_a = 0.0f;
+          while (t < r.tf && nsteps < 4096u) {
+            if (nsteps % K == 0u) {
+              ck_t[nsteps / K] = t;
+              ck_a[nsteps / K] = acc_a;
+              ck_n[nsteps / K] = 0;
+            }
+            nsteps++;
             DiffSample s;
             diff_sample(g, r, t, s);
+            bool stop = false;
             if (!(s.v < pc.threshold)) {
-              diff_tf(g, k, s);
+              diff_tf(g, b.k, s);
               if (s.a > 0.003f) {
-                seg_t[nseg] = t;
-                seg_a[nseg] = acc_a;
-                nseg++;
+                ring_t[ncontrib % kRing] = t;
+                ring_a[ncontrib % kRing] = acc_a;
+                ncontrib++;
+                ck_n[(nsteps - 1u) / K]++;
                 acc_a = acc_a + (1.0f - acc_a) * s.a;
+                stop = acc_a >= g.cutoff;
               }
             }
+            if (stop) break;
             t = fmaf(r.dt, r.span, t);
           }
         }
-        end = start;
-        for (int i = nseg - 1; i >= 0; i--) {
-          DiffSample s;
-          diff_sample(g, r, seg_t[i], s);
-          diff_tf(g, k, s);
-          const float tprev = 1.0f - seg_a[i];
-          const float dc_r = gr * tprev * s.a, dc_g = gg * tprev * s.a, dc_b = gb * tprev * s.a;
-          const float da = gr * tprev * (s.s[0] - S_r) + gg * tprev * (s.s[1] - S_g) +
-                           gb * tprev * (s.s[2] - S_b);
-          S_r = fmaf(s.a, s.s[0] - S_r, S_r);
-          S_g = fmaf(s.a, s.s[1] - S_g, S_g);
-          S_b = fmaf(s.a, s.s[2] - S_b, S_b);
-          float dalpha = 0.0f;
-          const bool alpha_free = s.s[3] > 0.0f && s.s[3] < 1.0f;
-          if (alpha_free) dalpha = da * k * r3d_powf(1.0f - s.alpha, k - 1.0f);
-          if (s.alpha < 1.0f)
-            g_density += da * (-(1.0f - s.a) * (r3d_log2f(1.0f - s.alpha) * 0.693147181f)) *
-                         kstep;
-          const float ds[4] = {dc_r, dc_g, dc_b, dalpha};
-          const float lf0 = 1.0f - s.f;
-          const float4 l0 = __ldg((const float4 *)g.lut + s.i0);
-          const float4 l1 = __ldg((const float4 *)g.lut + s.i1);
-          const float dl[4] = {l1.x - l0.x, l1.y - l0.y, l1.z - l0.z, l1.w - l0.w};
-          float dvv = 0.0f;
-#pragma unroll
-          for (int c = 0; c < 4; c++) {
-            if (DET) {
-              atomicAdd(&s_qlut[s.i0 * 4u + c],
-                        (unsigned long long)__double2ll_rn((double)(ds[c] * lf0) * kFix));
-              atomicAdd(&s_qlut[s.i1 * 4u + c],
-                        (unsigned long long)__double2ll_rn((double)(ds[c] * s.f) * kFix));
-            } else {
-              atomicAdd(&s_lut[s.i0 * 4u + c], ds[c] * lf0);
-              atomicAdd(&s_lut[s.i1 * 4u + c], ds[c] * s.f);
+        // reverse sweep over segments with contributions
+        float seg_t[K], seg_a[K];
+        const int nck = (int)((nsteps + K - 1) / K);
+        uint32_t end = ncontrib;  // contributions of segments < j: [0, end)
+        for (int j = nck - 1; j >= 0; j--) {
+          const uint32_t nj = ck_n[j];
+          if (nj == 0u) continue;
+          const uint32_t start = end - nj;
+          const bool in_ring = ncontrib - start <= (uint32_t)kRing;
+          int nseg = 0;
+          if (in_ring) {  // the segment's samples are still in the ring
+            for (uint32_t i = start; i < end; i++) {
+              seg_t[nseg] = ring_t[i % kRing];
+              seg_a[nseg] = ring_a[i % kRing];
+              nseg++;
             }
-            dvv = fmaf(ds[c], dl[c], dvv);
-          }
-          const bool tt_free = s.tt > 0.0f && s.tt < 255.0f;
-          const float dv = tt_free ? dvv * 256.0f : 0.0f;
-          // trilinear scatter, aggregated per cell
-          if (s.base != cell || s.sx != csx || s.sy != csy || s.sz != csz) {
-            if (cell != 0xffffffffu) {
-#pragma unroll
-              for (int c = 0; c < 8; c++)
-                vox_add<DET>(g_dens, q_dens,
-                             cell + ((c & 1) ? csx : 0u) + ((c & 2) ? csy : 0u) +
-                                 ((c & 4) ? csz : 0u),
-                             cw[c]);
+          } else {  // recompute segment j from its checkpoint
+            float t = ck_t[j], acc_a = ck_a[j];
+            const uint32_t s_end = min(nsteps, (uint32_t)(j + 1) * K);
+            for (uint32_t st = (uint32_t)j * K; st < s_end; st++) {
+              DiffSample s;
+              diff_sample(g, r, t, s);
+              if (!(s.v < pc.threshold)) {
+                diff_tf(g, b.k, s);
+                if (s.a > 0.003f) {
+                  seg_t[nseg] = t;
+                  seg_a[nseg] = acc_a;
+                  nseg++;
+                  acc_a = acc_a + (1.0f - acc_a) * s.a;
+                }
+              }
+              t = fmaf(r.dt, r.span, t);
             }
-            cell = s.base;
-            csx = s.sx;
-            csy = s.sy;
-            csz = s.sz;
-#pragma unroll
-            for (int c = 0; c < 8; c++) cw[c] = 0.0f;
           }
-          const float wx[2] = {1.0f - s.fx, s.fx}, wy[2] = {1.0f - s.fy, s.fy},
-                      wz[2] = {1.0f - s.fz, s.fz};
-#pragma unroll
-          for (int c = 0; c < 8; c++)
-            cw[c] = fmaf(dv, (wx[c & 1] * wy[(c >> 1) & 1]) * wz[c >> 2], cw[c]);
+          end = start;
+          for (int i = nseg - 1; i >= 0; i--)
+            bwd_sample<DET>(g, r, seg_t[i], seg_a[i], b, s_lut, s_qlut, g_dens, q_dens);
         }
       }
-      if (cell != 0xffffffffu) {
-#pragma unroll
-        for (int c = 0; c < 8; c++)
-          vox_add<DET>(g_dens, q_dens,
-                       cell + ((c & 1) ? csx : 0u) + ((c & 2) ? csy : 0u) + ((c & 4) ? csz : 0u),
-                       cw[c]);
-      }
+      bwd_flush<DET>(b, g_dens, q_dens);
     }
   }
   // density scale: warp reduction, one global add per warp
-  float gs = g_density;
+  float gs = b.g_density;
   if (DET) {
     long long q = __double2ll_rn((double)gs * kFix);
     for (int off = 16; off > 0; off >>= 1) q += __shfl_xor_sync(0xffffffffu, q, off);
@@ -483,10 +531,19 @@ static int diff_prepare(r3d_cuda_ctx *c, const r3d_cuda_diff_scene *sc,
   return R3D_OK;
 }
 
-extern "C" int r3d_cuda_diff_forward(r3d_cuda_ctx *c, const r3d_cuda_diff_scene *sc,
-                                     const r3d_frame_params *views, uint32_t nviews,
-                                     float *rgb_out, unsigned long long *total_steps,
-                                     void *stream) {
+// Identity of a tape: the views, the scene's buffers and sizes and the
+// cutoff of the forward that wrote it.
+static bool tape_matches(const r3d_cuda_ctx *c, const r3d_cuda_diff_scene *sc,
+                         const r3d_frame_params *views, uint32_t nviews) {
+  return c->tape_valid && c->tape_nviews == nviews && c->tape_density == sc->density &&
+         c->tape_lut == sc->lut && c->tape_dims[0] == sc->nx && c->tape_dims[1] == sc->ny &&
+         c->tape_dims[2] == sc->nz && c->tape_cutoff == c->alpha_cutoff &&
+         memcmp(c->tape_views, views, sizeof(r3d_frame_params) * nviews) == 0;
+}
+
+static int diff_forward(r3d_cuda_ctx *c, const r3d_cuda_diff_scene *sc,
+                        const r3d_frame_params *views, uint32_t nviews, float *rgb_out,
+                        unsigned long long *total_steps, void *stream, bool tape) {
   if (!c || !rgb_out) return fail(c, R3D_E_INVALID, "diff_forward: bad arguments");
   cudaSetDevice(c->device);
   cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
@@ -497,20 +554,68 @@ extern "C" int r3d_cuda_diff_forward(r3d_cuda_ctx *c, const r3d_cuda_diff_scene 
   size_t nf;
   int rc = diff_prepare(c, sc, views, nviews, g, dv, mw, mh, nf, st);
   if (rc != R3D_OK) return rc;
+  float2 *tp = nullptr;
+  uint32_t *tn = nullptr;
+  if (tape) {
+    const size_t rays = nf / 3u;
+    c->tape_valid = false;
+    if (c->tape_rays < rays) {  // grow; earlier work on the old buffers must finish first
+      R3D_CUDA_TRY(c, cudaDeviceSynchronize());
+      cudaFree(c->tape);
+      cudaFree(c->tape_n);
+      c->tape = nullptr;
+      c->tape_n = nullptr;
+      c->tape_rays = 0;
+      R3D_CUDA_TRY(c, cudaMalloc(&c->tape, rays * kTape * sizeof(float2)));
+      R3D_CUDA_TRY(c, cudaMalloc(&c->tape_n, rays * sizeof(uint32_t)));
+      c->tape_rays = rays;
+    }
+    tp = (float2 *)c->tape;
+    tn = c->tape_n;
+  }
   R3D_CUDA_TRY(c, cudaEventRecord(c->ev0, st));
   dim3 grid((mw + 15u) / 16u, (mh + 7u) / 8u, nviews);
-  k_diff_fwd<<<grid, 128, 0, st>>>(dv, g, rgb_out, total_steps);
+  if (tape)
+    k_diff_fwd<true><<<grid, 128, 0, st>>>(dv, g, rgb_out, total_steps, tp, tn);
+  else
+    k_diff_fwd<false><<<grid, 128, 0, st>>>(dv, g, rgb_out, total_steps, nullptr, nullptr);
   R3D_CUDA_TRY(c, cudaGetLastError());
   R3D_CUDA_TRY(c, cudaEventRecord(c->ev1, st));
   c->timed = true;
+  if (tape) {
+    memcpy(c->tape_views, views, sizeof(r3d_frame_params) * nviews);
+    c->tape_nviews = nviews;
+    c->tape_density = sc->density;
+    c->tape_lut = sc->lut;
+    c->tape_dims[0] = sc->nx;
+    c->tape_dims[1] = sc->ny;
+    c->tape_dims[2] = sc->nz;
+    c->tape_cutoff = c->alpha_cutoff;
+    c->tape_valid = true;
+  }
   return R3D_OK;
+}
+
+extern "C" int r3d_cuda_diff_forward(r3d_cuda_ctx *c, const r3d_cuda_diff_scene *sc,
+                                     const r3d_frame_params *views, uint32_t nviews,
+                                     float *rgb_out, unsigned long long *total_steps,
+                                     void *stream) {
+  return diff_forward(c, sc, views, nviews, rgb_out, total_steps, stream, false);
+}
+
+extern "C" int r3d_cuda_diff_forward_tape(r3d_cuda_ctx *c, const r3d_cuda_diff_scene *sc,
+                                          const r3d_frame_params *views, uint32_t nviews,
+                                          float *rgb_out, unsigned long long *total_steps,
+                                          void *stream) {
+  return diff_forward(c, sc, views, nviews, rgb_out, total_steps, stream, true);
 }
 
 template <int K, bool DET>
 static cudaError_t launch_bwd(dim3 grid, cudaStream_t st, const DiffView *dv, const DiffGrid &g,
                               const float *dl, float *gd, unsigned long long *qd, float *gl,
-                              unsigned long long *ql, float *gs, unsigned long long *qs) {
-  k_diff_bwd<K, DET><<<grid, 128, 0, st>>>(dv, g, dl, gd, qd, gl, ql, gs, qs);
+                              unsigned long long *ql, float *gs, unsigned long long *qs,
+                              const float2 *tp, const uint32_t *tn) {
+  k_diff_bwd<K, DET><<<grid, 128, 0, st>>>(dv, g, dl, gd, qd, gl, ql, gs, qs, tp, tn);
   return cudaGetLastError();
 }
 
@@ -523,6 +628,9 @@ extern "C" int r3d_cuda_raycast_bwd(r3d_cuda_ctx *c, const r3d_cuda_diff_scene *
   if (ckpt_k != 32u && ckpt_k != 64u && ckpt_k != 128u)
     return fail(c, R3D_E_INVALID, "raycast_bwd: checkpoint interval %u not 32, 64 or 128",
                 ckpt_k);
+  if (deterministic & ~(int)(R3D_BWD_DETERMINISTIC | R3D_BWD_TAPE))
+    return fail(c, R3D_E_INVALID, "raycast_bwd: unknown flags 0x%x", deterministic);
+  const bool det = (deterministic & (int)R3D_BWD_DETERMINISTIC) != 0;
   cudaSetDevice(c->device);
   cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
   DiffGrid g;
@@ -533,7 +641,7 @@ extern "C" int r3d_cuda_raycast_bwd(r3d_cuda_ctx *c, const r3d_cuda_diff_scene *
   if (rc != R3D_OK) return rc;
   const size_t nvox = (size_t)sc->nx * sc->ny * sc->nz;
   unsigned long long *qd = nullptr, *ql = nullptr, *qs = nullptr;
-  if (deterministic) {
+  if (det) {
     const size_t need = (nvox + 1024u + 1u) * sizeof(unsigned long long);
     if (c->diff_q_bytes < need) {
       cudaFree(c->diff_q);
@@ -551,21 +659,28 @@ extern "C" int r3d_cuda_raycast_bwd(r3d_cuda_ctx *c, const r3d_cuda_diff_scene *
     R3D_CUDA_TRY(c, cudaMemsetAsync(out->lut, 0, 1024 * sizeof(float), st));
     R3D_CUDA_TRY(c, cudaMemsetAsync(out->density_scale, 0, sizeof(float), st));
   }
+  // the tape of the matching training forward, when asked for
+  const bool use_tape = (deterministic & (int)R3D_BWD_TAPE) != 0;
+  if (use_tape && !tape_matches(c, sc, views, nviews))
+    return fail(c, R3D_E_STATE, "raycast_bwd: no tape of a training forward over these views "
+                                "and this scene");
+  const float2 *tp = use_tape ? (const float2 *)c->tape : nullptr;
+  const uint32_t *tn = use_tape ? c->tape_n : nullptr;
   R3D_CUDA_TRY(c, cudaEventRecord(c->ev0, st));
   dim3 grid((mw + 15u) / 16u, (mh + 7u) / 8u, nviews);
   cudaError_t e;
   float *gd = out->density, *gl = out->lut, *gs = out->density_scale;
-  if (deterministic) {
-    e = ckpt_k == 32u ? launch_bwd<32, true>(grid, st, dv, g, dl_drgb, gd, qd, gl, ql, gs, qs)
-        : ckpt_k == 64u ? launch_bwd<64, true>(grid, st, dv, g, dl_drgb, gd, qd, gl, ql, gs, qs)
-                        : launch_bwd<128, true>(grid, st, dv, g, dl_drgb, gd, qd, gl, ql, gs, qs);
+  if (det) {
+    e = ckpt_k == 32u ? launch_bwd<32, true>(grid, st, dv, g, dl_drgb, gd, qd, gl, ql, gs, qs, tp, tn)
+        : ckpt_k == 64u ? launch_bwd<64, true>(grid, st, dv, g, dl_drgb, gd, qd, gl, ql, gs, qs, tp, tn)
+                        : launch_bwd<128, true>(grid, st, dv, g, dl_drgb, gd, qd, gl, ql, gs, qs, tp, tn);
   } else {
-    e = ckpt_k == 32u ? launch_bwd<32, false>(grid, st, dv, g, dl_drgb, gd, qd, gl, ql, gs, qs)
-        : ckpt_k == 64u ? launch_bwd<64, false>(grid, st, dv, g, dl_drgb, gd, qd, gl, ql, gs, qs)
-                        : launch_bwd<128, false>(grid, st, dv, g, dl_drgb, gd, qd, gl, ql, gs, qs);
+    e = ckpt_k == 32u ? launch_bwd<32, false>(grid, st, dv, g, dl_drgb, gd, qd, gl, ql, gs, qs, tp, tn)
+        : ckpt_k == 64u ? launch_bwd<64, false>(grid, st, dv, g, dl_drgb, gd, qd, gl, ql, gs, qs, tp, tn)
+                        : launch_bwd<128, false>(grid, st, dv, g, dl_drgb, gd, qd, gl, ql, gs, qs, tp, tn);
   }
   if (e != cudaSuccess) return cuda_fail(c, e, "raycast_bwd: launch");
-  if (deterministic) {
+  if (det) {
     k_fix_to_float<<<grid_blocks(nvox), 256, 0, st>>>(qd, gd, nvox);
     k_fix_to_float<<<4, 256, 0, st>>>(ql, gl, 1024);
     k_fix_to_float<<<1, 32, 0, st>>>(qs, gs, 1);

@@ -61,6 +61,19 @@ struct r3d_cuda_ctx {
   unsigned long long *diff_q = nullptr;
   size_t diff_q_bytes = 0;
 
+  // tape of the last training forward (r3d_cuda_diff_forward_tape): per
+  // ray up to 64 contributing samples (float2) and their count, and the
+  // arguments it was recorded for
+  void *tape = nullptr;
+  uint32_t *tape_n = nullptr;
+  size_t tape_rays = 0;
+  bool tape_valid = false;
+  r3d_frame_params tape_views[64];
+  uint32_t tape_nviews = 0;
+  const float *tape_density = nullptr, *tape_lut = nullptr;
+  uint32_t tape_dims[3] = {0, 0, 0};
+  float tape_cutoff = 0.0f;
+
   // forward scheduling and the view-table ring of persistent launches:
   // slot k holds one call's views (pinned host copy + device copy) and its
   // tile counters; ring_ev[k] completes once the slot's upload has run

@@ -145,3 +145,67 @@ def test_adam_reduces_loss(rb, ctx, scene):
         opt.step()
         losses.append(loss.item())
     assert losses[-1] < 0.7 * losses[0]
+
+
+def _bwd(ctx, dvol, dlut, views, dg, k, det, tape):
+    import torch
+    gd = torch.zeros_like(dvol)
+    gl = torch.zeros_like(dlut)
+    gs = torch.zeros(1, device="cuda")
+    ctx.raycast_bwd(dvol, dlut, views, dg, gd, gl, gs, k, det, stream=ctx.stream, tape=tape)
+    torch.cuda.synchronize()
+    return gd, gl, gs
+
+
+@pytest.mark.parametrize("faint", [False, True])
+def test_tape_backward_equals_checkpoint_backward(rb, orc, ctx, scene, faint):
+    """The tape of a training forward replaces the backward's forward sweep
+    without changing a bit of the deterministic gradients.  faint: a LUT
+    whose alpha is 0.01 everywhere makes every sample contribute (hundreds
+    per ray), so most rays overflow the 64-entry tape and take the
+    checkpoint path inside the same launch."""
+    import torch
+    ctx.set_alpha_cutoff(0.98)
+    views = scene["views"]
+    lut = scene["lut"].copy()
+    if faint:
+        lut[:, 3] = 0.01
+    dlut = torch.tensor(lut, device="cuda")
+    n = sum(v.viewport[0] * v.viewport[1] * 3 for v in views)
+    rgb = torch.zeros(n, device="cuda")
+    ctx.diff_forward(scene["dvol"], dlut, views, rgb, stream=ctx.stream, tape=True)
+    dg = torch.randn(n, device="cuda", generator=torch.Generator("cuda").manual_seed(11))
+    for k in (32, 64):
+        a = _bwd(ctx, scene["dvol"], dlut, views, dg, k, True, tape=False)
+        b = _bwd(ctx, scene["dvol"], dlut, views, dg, k, True, tape=True)
+        for x, y in zip(a, b):
+            assert torch.equal(x, y), f"k={k}"
+    fa = _bwd(ctx, scene["dvol"], dlut, views, dg, 64, False, tape=True)
+    assert torch.allclose(fa[0], a[0], rtol=1e-4, atol=1e-6)
+    # and against the FP64 oracle
+    g = dg.cpu().numpy()
+    rd = np.zeros(scene["vol"].shape)
+    off = 0
+    for v in views:
+        sz = v.viewport[0] * v.viewport[1] * 3
+        gv = g[off:off + sz].reshape(v.viewport[1], v.viewport[0], 3)
+        rd += orc.diff_grad64(v, scene["vol"], lut, gv, 0.98, decisions32=True)[1]
+        off += sz
+    assert _rel(b[0].cpu().numpy(), rd) < 1e-4
+
+
+def test_tape_must_match(rb, ctx, scene):
+    import torch
+    views = scene["views"]
+    n = sum(v.viewport[0] * v.viewport[1] * 3 for v in views)
+    rgb = torch.zeros(n, device="cuda")
+    ctx.diff_forward(scene["dvol"], scene["dlut"], views, rgb, stream=ctx.stream, tape=True)
+    dg = torch.ones(n, device="cuda")
+    other = [v.copy() for v in views]
+    other[0].frame_index += 1
+    with pytest.raises(rb.R3DError):
+        _bwd(ctx, scene["dvol"], scene["dlut"], other, dg, 64, True, tape=True)
+    lut2 = scene["dlut"].clone()
+    with pytest.raises(rb.R3DError):
+        _bwd(ctx, scene["dvol"], lut2, views, dg, 64, True, tape=True)
+    _bwd(ctx, scene["dvol"], scene["dlut"], views, dg, 64, True, tape=True)
