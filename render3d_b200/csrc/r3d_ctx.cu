@@ -259,6 +259,7 @@ void r3d_cuda_destroy(r3d_cuda_ctx *c) {
   cudaFree(c->total);
   cudaFree(c->diff_q);
   cudaFree(c->tape);
+  cudaFree(c->diff_quad);
   cudaFree(c->tape_n);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);

@@ -45,6 +45,10 @@ struct DiffView {
 
 struct DiffGrid {
   const float *dens;
+  // per voxel (x, y, z): the densities at (x, y), (x1, y), (x, y1), (x1, y1)
+  // of its z plane, x1 = min(x + 1, nx - 1) and y1 likewise, so that a
+  // trilinear sample reads two float4 instead of eight floats
+  const float4 *quad;
   uint32_t n[3];
   uint32_t nmax;
   const float *lut;  // 256 x 4
@@ -133,11 +137,9 @@ __device__ __forceinline__ void diff_sample(const DiffGrid &g, const DiffRay &r,
   o.fx = fr[0];
   o.fy = fr[1];
   o.fz = fr[2];
-  const float *b = g.dens + o.base;
-  float c00 = lerp_(__ldg(b), __ldg(b + o.sx), fr[0]);
-  float c10 = lerp_(__ldg(b + o.sy), __ldg(b + o.sy + o.sx), fr[0]);
-  float c01 = lerp_(__ldg(b + o.sz), __ldg(b + o.sz + o.sx), fr[0]);
-  float c11 = lerp_(__ldg(b + o.sz + o.sy), __ldg(b + o.sz + o.sy + o.sx), fr[0]);
+  const float4 q0 = __ldg(g.quad + o.base), q1 = __ldg(g.quad + o.base + o.sz);
+  const float c00 = lerp_(q0.x, q0.y, fr[0]), c10 = lerp_(q0.z, q0.w, fr[0]);
+  const float c01 = lerp_(q1.x, q1.y, fr[0]), c11 = lerp_(q1.z, q1.w, fr[0]);
   o.v = lerp_(lerp_(c00, c10, fr[1]), lerp_(c01, c11, fr[1]), fr[2]);
 }
 
@@ -154,6 +156,18 @@ __device__ __forceinline__ void diff_tf(const DiffGrid &g, float k, DiffSample &
   o.s[3] = lerp_(l0.w, l1.w, o.f);
   o.alpha = clamp_(o.s[3], 0.0f, 1.0f);
   o.a = 1.0f - r3d_powf(1.0f - o.alpha, k);
+}
+
+// The quad grid of DiffGrid::quad from the density grid.
+__global__ void k_diff_quads(const float *__restrict__ d, uint32_t nx, uint32_t ny, uint32_t nz,
+                             float4 *__restrict__ q) {
+  const size_t n = (size_t)nx * ny * nz;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t x = (uint32_t)(i % nx), y = (uint32_t)((i / nx) % ny);
+    const size_t dx = x + 1u < nx ? 1u : 0u, dy = y + 1u < ny ? nx : 0u;
+    q[i] = make_float4(__ldg(d + i), __ldg(d + i + dx), __ldg(d + i + dy), __ldg(d + i + dy + dx));
+  }
 }
 
 // Tape of a training forward: per ray, the first kTape contributing samples
@@ -531,6 +545,30 @@ static int diff_prepare(r3d_cuda_ctx *c, const r3d_cuda_diff_scene *sc,
   return R3D_OK;
 }
 
+// Fills g.quad: the context's quad grid, rebuilt from the density unless
+// `reuse` and it was last built from this density buffer.
+static int diff_quads(r3d_cuda_ctx *c, const r3d_cuda_diff_scene *sc, DiffGrid &g, bool reuse,
+                      cudaStream_t st) {
+  const size_t nvox = (size_t)sc->nx * sc->ny * sc->nz;
+  const size_t need = nvox * sizeof(float4);
+  if (c->diff_quad_bytes < need) {  // grow; earlier work on the old buffer must finish first
+    R3D_CUDA_TRY(c, cudaDeviceSynchronize());
+    cudaFree(c->diff_quad);
+    c->diff_quad = nullptr;
+    c->diff_quad_bytes = 0;
+    c->quad_src = nullptr;
+    R3D_CUDA_TRY(c, cudaMalloc(&c->diff_quad, need));
+    c->diff_quad_bytes = need;
+  }
+  g.quad = (const float4 *)c->diff_quad;
+  if (reuse && c->quad_src == sc->density) return R3D_OK;
+  k_diff_quads<<<grid_blocks(nvox), 256, 0, st>>>(sc->density, sc->nx, sc->ny, sc->nz,
+                                                  (float4 *)c->diff_quad);
+  R3D_CUDA_TRY(c, cudaGetLastError());
+  c->quad_src = sc->density;
+  return R3D_OK;
+}
+
 // Identity of a tape: the views, the scene's buffers and sizes and the
 // cutoff of the forward that wrote it.
 static bool tape_matches(const r3d_cuda_ctx *c, const r3d_cuda_diff_scene *sc,
@@ -553,6 +591,8 @@ static int diff_forward(r3d_cuda_ctx *c, const r3d_cuda_diff_scene *sc,
   uint32_t mw, mh;
   size_t nf;
   int rc = diff_prepare(c, sc, views, nviews, g, dv, mw, mh, nf, st);
+  if (rc != R3D_OK) return rc;
+  rc = diff_quads(c, sc, g, false, st);
   if (rc != R3D_OK) return rc;
   float2 *tp = nullptr;
   uint32_t *tn = nullptr;
@@ -666,6 +706,9 @@ extern "C" int r3d_cuda_raycast_bwd(r3d_cuda_ctx *c, const r3d_cuda_diff_scene *
                                 "and this scene");
   const float2 *tp = use_tape ? (const float2 *)c->tape : nullptr;
   const uint32_t *tn = use_tape ? c->tape_n : nullptr;
+  // the tape's forward built the quads from this (unchanged) density
+  rc = diff_quads(c, sc, g, use_tape, st);
+  if (rc != R3D_OK) return rc;
   R3D_CUDA_TRY(c, cudaEventRecord(c->ev0, st));
   dim3 grid((mw + 15u) / 16u, (mh + 7u) / 8u, nviews);
   cudaError_t e;

@@ -60,6 +60,11 @@ struct r3d_cuda_ctx {
   // fixed-point gradient accumulators of the deterministic adjoint
   unsigned long long *diff_q = nullptr;
   size_t diff_q_bytes = 0;
+  // quad grid of the differentiable render (float4 per voxel) and the
+  // density buffer it was last built from
+  void *diff_quad = nullptr;
+  size_t diff_quad_bytes = 0;
+  const float *quad_src = nullptr;
 
   // tape of the last training forward (r3d_cuda_diff_forward_tape): per
   // ray up to 64 contributing samples (float2) and their count, and the
