@@ -174,6 +174,18 @@ __global__ void k_slot_blockmax(const uint8_t *__restrict__ pool, uint8_t *__res
   }
 }
 
+// Quad words of every slot (DevBricks::quad); one thread per texel.
+__global__ void k_slot_quads(const uint8_t *__restrict__ pool, uint32_t *__restrict__ quad,
+                             size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t x = (uint32_t)(i & 127u), y = (uint32_t)((i >> 7) & 127u);
+    const size_t dx = x < 127u ? 1u : 0u, dy = y < 127u ? 128u : 0u;
+    quad[i] = (uint32_t)pool[i] | ((uint32_t)pool[i + dx] << 8) | ((uint32_t)pool[i + dy] << 16) |
+              ((uint32_t)pool[i + dy + dx] << 24);
+  }
+}
+
 static unsigned grid_for(size_t n) {
   size_t b = (n + 255) / 256;
   return (unsigned)(b < 148u * 64u ? (b ? b : 1) : 148u * 64u);
@@ -250,6 +262,7 @@ void r3d_cuda_destroy(r3d_cuda_ctx *c) {
   cudaFree(c->page);
   cudaFree(c->pool);
   cudaFree(c->bmax);
+  cudaFree(c->quad);
   cudaFree(c->shard_buf);
   cudaFree(c->shard_page);
   cudaFree(c->lut);
@@ -421,12 +434,18 @@ static int build_blockmax(r3d_cuda_ctx *c) {
   size_t n = (size_t)(c->nslots ? c->nslots : 1u) * 4096u;
   R3D_CUDA_TRY(c, cudaMalloc(&c->bmax, n));
   R3D_CUDA_TRY(c, cudaMemsetAsync(c->bmax, 0, n, c->stream));
+  cudaFree(c->quad);
+  c->quad = nullptr;
+  const size_t nq = (size_t)(c->nslots ? c->nslots : 1u) * (128u * 128u * 128u);
+  R3D_CUDA_TRY(c, cudaMalloc(&c->quad, nq * sizeof(uint32_t)));
   if (c->nslots) {
     k_slot_blockmax<<<c->nslots, 256, 0, c->stream>>>(c->pool, c->bmax);
+    k_slot_quads<<<grid_for(nq), 256, 0, c->stream>>>(c->pool, c->quad, nq);
     R3D_CUDA_TRY(c, cudaGetLastError());
   }
   R3D_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   c->br.bmax = c->bmax;
+  c->br.quad = c->quad;
   return R3D_OK;
 }
 

@@ -50,6 +50,9 @@ struct DevBricks {
   // the slot), an upper bound of any trilinear sample whose base texel lies
   // in block b
   const uint8_t *bmax;
+  // per slot, 128^3 words: bytes (x, y), (x1, y), (x, y1), (x1, y1) of the
+  // texel's z plane, x1 = min(x + 1, 127) and y1 likewise
+  const uint32_t *quad;
   uint32_t nslots;
   uint32_t nlev;
   float bs[3];     // base shape
@@ -316,32 +319,37 @@ __device__ __forceinline__ SlotCoord slot_coord(float3 bl) {
   return q;
 }
 
-// a byte as a float without the conversion unit: 2^23 + b has b in its
-// mantissa, and subtracting 2^23 is exact
-__device__ __forceinline__ float u8f(uint8_t b) {
-  return __uint_as_float(0x4B000000u | (uint32_t)b) - 8388608.0f;
+// byte k of w as a float without the conversion unit: the byte permute
+// assembles the bits of 2^23 + byte, and subtracting 2^23 is exact
+__device__ __forceinline__ float qbyte(uint32_t w, uint32_t k) {
+  return __uint_as_float(__byte_perm(w, 0x4B000000u, k | 0x7540u)) - 8388608.0f;
 }
 
-__device__ __forceinline__ float tri_slot_at(const uint8_t *__restrict__ g, const SlotCoord &q) {
-  const float fx = q.fx, fy = q.fy, fz = q.fz;
-  uint32_t dx1 = q.x0 < 127u ? 1u : 0u;
-  uint32_t dy1 = q.y0 < 127u ? 128u : 0u;
-  uint32_t dz1 = q.z0 < 127u ? 16384u : 0u;
-  const uint8_t *r00 = g + ((q.z0 << 14) | (q.y0 << 7) | q.x0);
-  float a0 = u8f(__ldg(r00)), a1 = u8f(__ldg(r00 + dx1));
-  float b0 = u8f(__ldg(r00 + dy1)), b1 = u8f(__ldg(r00 + dy1 + dx1));
-  float c0 = u8f(__ldg(r00 + dz1)), c1 = u8f(__ldg(r00 + dz1 + dx1));
-  float d0 = u8f(__ldg(r00 + dz1 + dy1)), d1 = u8f(__ldg(r00 + dz1 + dy1 + dx1));
-  float c00 = lerp_(a0, a1, fx), c10 = lerp_(b0, b1, fx);
-  float c01 = lerp_(c0, c1, fx), c11 = lerp_(d0, d1, fx);
-  float e0 = lerp_(c00, c10, fy), e1 = lerp_(c01, c11, fy);
-  return lerp_(e0, e1, fz) * kInv255;
+// Trilinear inside one 128^3 slot at a clamped slot coordinate, on the quad
+// pool: the word of texel (x, y, z) holds the bytes at (x, y), (x1, y),
+// (x, y1), (x1, y1) of its z plane (x1, y1 clamped to the slot), so a
+// sample is two 4-byte loads; z1 is clamped the same way.  The lerps run
+// in 0..255 space, x then y then z, as on the byte grid.
+__device__ __forceinline__ float tri_slot_q(const uint32_t *__restrict__ g, const SlotCoord &q) {
+  const uint32_t dz1 = q.z0 < 127u ? 16384u : 0u;
+  const uint32_t *r = g + ((q.z0 << 14) | (q.y0 << 7) | q.x0);
+  const uint32_t w0 = __ldg(r), w1 = __ldg(r + dz1);
+  const float c00 = lerp_(qbyte(w0, 0), qbyte(w0, 1), q.fx);
+  const float c10 = lerp_(qbyte(w0, 2), qbyte(w0, 3), q.fx);
+  const float c01 = lerp_(qbyte(w1, 0), qbyte(w1, 1), q.fx);
+  const float c11 = lerp_(qbyte(w1, 2), qbyte(w1, 3), q.fx);
+  const float e0 = lerp_(c00, c10, q.fy), e1 = lerp_(c01, c11, q.fy);
+  return lerp_(e0, e1, q.fz) * kInv255;
+}
+
+__device__ __forceinline__ float slot_sample(const DevScene &s, uint32_t slot, const SlotCoord &q) {
+  return tri_slot_q(s.br.quad + (size_t)slot * (128u * 128u * 128u), q);
 }
 
 // bricks_fetch at atlas lod 0 (raycast.slang:284-288): clamp to
 // [0.5, 127.5] inside the brick, no cross-brick filtering
 __device__ __forceinline__ float brick_fetch(const DevScene &s, uint32_t slot, float3 bl) {
-  return tri_slot_at(s.br.pool + (size_t)slot * (128u * 128u * 128u), slot_coord(bl));
+  return slot_sample(s, slot, slot_coord(bl));
 }
 
 // Texel origin of a single-level atlas slot (raycast.slang:176-177)
@@ -655,22 +663,21 @@ __device__ __forceinline__ bool composite_sample(const DevScene &s, const ViewCo
         // clamped coordinates, so only the moved axis is recomputed
         const float ev = q.grad_vox;
         const float3 u = q.bl;
-        const uint8_t *g = s.br.pool + (size_t)q.slot * (128u * 128u * 128u);
         const SlotCoord c = slot_coord(u);
         SlotCoord a = c, b = c;
         a.x0 = slot_axis(u.x + ev, a.fx);
         b.x0 = slot_axis(u.x - ev, b.fx);
-        g0 = tri_slot_at(g, a) - tri_slot_at(g, b);
+        g0 = slot_sample(s, q.slot, a) - slot_sample(s, q.slot, b);
         a = c;
         b = c;
         a.y0 = slot_axis(u.y + ev, a.fy);
         b.y0 = slot_axis(u.y - ev, b.fy);
-        g1 = tri_slot_at(g, a) - tri_slot_at(g, b);
+        g1 = slot_sample(s, q.slot, a) - slot_sample(s, q.slot, b);
         a = c;
         b = c;
         a.z0 = slot_axis(u.z + ev, a.fz);
         b.z0 = slot_axis(u.z - ev, b.fz);
-        g2 = tri_slot_at(g, a) - tri_slot_at(g, b);
+        g2 = slot_sample(s, q.slot, a) - slot_sample(s, q.slot, b);
       } else if (slot_taps) {
         const float ev = q.lod_step;
         const float3 u = q.bl, org = shard_slot_org(s.sh, q.slot);
@@ -817,7 +824,7 @@ __device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, 
           st.t = fmaf(vc.dt, lod_step, t);
         return kStepCont;
       }
-      v = tri_slot_at(s.br.pool + (size_t)b.slot * (128u * 128u * 128u), q);
+      v = slot_sample(s, b.slot, q);
     }
   } else if (kShard) {
     const DevShard &h = s.sh;
