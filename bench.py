@@ -185,6 +185,40 @@ def shard_bench(rb, torch, local: int, vol, lut, frames: int) -> dict:
         c.close()
 
 
+def overlay_bench(rb, ctx, lut, torch, stream, total, img, frames: int) -> dict:
+    """The same orbit in FULL with two slot-parallel overlay atlases cut from
+    seeded device phantoms (ink at gain 1.5, a second scan fused at weight
+    128/255), per-frame event times."""
+    ink = ctx.phantom(N_EDGE, seed=SEED + 7)
+    ctx.overlay_build(0, ink)
+    reg = ctx.phantom(N_EDGE, seed=SEED + 8)
+    ctx.overlay_build(3, reg)
+    del ink, reg
+    torch.cuda.empty_cache()
+
+    def frame(i):
+        p = orbit_params(rb, lut, i, ctx.brick_mode)
+        p.overlay_flags = 1 | 16 | (128 << 16)
+        p.overlay_gain = 1.5
+        ctx.raycast(p, W, H, out=img, total=total, stream=ctx.stream)
+    for i in range(32):
+        frame(i)
+    torch.cuda.synchronize()
+    total.zero_()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(frames):
+        frame(i)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / frames
+    ctx.overlay_load(0, None)
+    ctx.overlay_load(3, None)
+    return {"workload": "1024^3 orbit, FULL, ink + registration overlays", "ms_per_frame": ms,
+            "fps": 1e3 / ms, "gsamples_per_s": float(total.item()) / frames / (ms * 1e-3) / 1e9}
+
+
 def mode_stats(rb, ctx, lut, torch, stream, total, img, frames: int) -> dict:
     """Per-frame CUDA-event times (p50/p95/p99, like render3d's frame stats)
     and Gsamples/s of the orbit in FULL, MIP and HEATMAP modes, each after
@@ -553,6 +587,7 @@ def run_ours(args) -> None:
     r.close()
 
     shard = shard_bench(rb, torch, local, vol, lut, ORBIT_FRAMES * 2)
+    overlays = overlay_bench(rb, ctx, lut, torch, stream, total, img, ORBIT_FRAMES * 2)
 
     bt = None
     if not args.no_batch:
@@ -597,6 +632,7 @@ def run_ours(args) -> None:
                             "algorithmic_bytes_per_frame": alg / K},
                "modes": modes,
                "shard": shard,
+               "overlays": overlays,
                "fwd_bwd": fb,
                "batch": bt,
                "gpu_launches": K,

@@ -98,6 +98,22 @@ int r3d_cuda_bricks_info(const r3d_cuda_ctx *ctx, uint32_t *page_words, uint32_t
                          uint32_t shape[3], uint32_t *nlev);
 int r3d_cuda_bricks_read(r3d_cuda_ctx *ctx, uint32_t *page, uint8_t *slots);
 
+/* Slot-parallel overlay atlases of the LOD brick cache (reference
+ * src/render/render.h:51-101; sampled by src/shaders/raycast.slang:45-115,
+ * 872-914,1000-1014,1032-1036): which = 0 ink (overlay_flags bit 0, tinted
+ * by the palette id in bits 8..15), 1 3D ink (bit 2), 2 paint labels,
+ * class ids 1..8 (bit 3), 3 registered second scan (bit 4, fuse weight in
+ * bits 16..23).  Each holds one 128^3 u8 brick per CT slot, in the CT
+ * pool's slot order (absent = 0).  _load takes the slot contents (host or
+ * device, nslots * 128^3 bytes; NULL removes the atlas); _build cuts them
+ * from a raw volume of the cache's shape: the CT's (sum+4)/8 box pyramid,
+ * or for labels the level-0 voxel at (x, y, z) << level
+ * (src/core/labelvol.c:172-196).  Rebuilding or reloading the brick cache
+ * removes every overlay. */
+int r3d_cuda_bricks_overlay_load(r3d_cuda_ctx *ctx, uint32_t which, const uint8_t *slots);
+int r3d_cuda_bricks_overlay_build(r3d_cuda_ctx *ctx, uint32_t which, const r3d_volume_desc *d,
+                                  const uint8_t *voxels);
+
 /* Copy of cube mip level `level` or (level == -1) the occupancy grid into a
  * host buffer; dims receives its size. */
 int r3d_cuda_cube_read(r3d_cuda_ctx *ctx, int level, uint8_t *out, uint32_t dims[3]);

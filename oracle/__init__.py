@@ -34,7 +34,7 @@ class Cube(C.Structure):
 
 class Bricks(C.Structure):
     _fields_ = [("page", C.c_void_p), ("page_words", C.c_uint32), ("pool", C.c_void_p),
-                ("nslots", C.c_uint32), ("atlas", C.c_void_p)]
+                ("nslots", C.c_uint32), ("atlas", C.c_void_p), ("ovl", C.c_void_p * 4)]
 
 
 class Opts(C.Structure):
@@ -65,6 +65,8 @@ def _load():
     lib.orc_occupancy.argtypes = [P, U32, U32, U32, P]
     lib.orc_build_lod_bricks.restype = C.c_int64
     lib.orc_build_lod_bricks.argtypes = [P, U32, U32, U32, U32, U32, P, U32, P, C.c_uint64]
+    lib.orc_build_lod_overlay.restype = C.c_int
+    lib.orc_build_lod_overlay.argtypes = [P, U32, U32, U32, P, U32, C.c_int, P, U32]
     lib.orc_build_shard.restype = C.c_int
     lib.orc_build_shard.argtypes = [P, U32, U32, P, P, P]
     lib.orc_shard_occupancy.restype = None
@@ -126,13 +128,30 @@ class CubeScene:
 
 
 class BrickScene:
-    """A LOD brick cache: page table + slot pool (x fastest)."""
+    """A LOD brick cache: page table + slot pool (x fastest), and optional
+    slot-parallel overlay atlases (ink, 3D ink, labels, registration)."""
 
     def __init__(self, page: np.ndarray, pool: np.ndarray):
         self.page = np.ascontiguousarray(page, np.uint32)
         self.pool = np.ascontiguousarray(pool, np.uint8)
         self.b = Bricks(self.page.ctypes.data, self.page.size, self.pool.ctypes.data,
                         self.pool.size // 128 ** 3)
+        self.ovl = [None] * 4
+
+    def set_overlay(self, which: int, slots: np.ndarray | None) -> None:
+        self.ovl[which] = None if slots is None else np.ascontiguousarray(slots, np.uint8)
+        self.b.ovl[which] = None if slots is None else self.ovl[which].ctypes.data
+
+    def build_overlay(self, which: int, vol: np.ndarray) -> np.ndarray:
+        """Overlay slot contents cut from a raw volume (labels: which == 2)."""
+        vol = np.ascontiguousarray(vol, np.uint8)
+        nz, ny, nx = vol.shape
+        pool = np.zeros(self.pool.size, np.uint8)
+        if lib.orc_build_lod_overlay(_p(vol), nx, ny, nz, _p(self.page), self.page.size,
+                                     int(which == 2), _p(pool), self.b.nslots) != 0:
+            raise ValueError("orc_build_lod_overlay failed")
+        self.set_overlay(which, pool)
+        return pool
 
     @classmethod
     def build(cls, vol: np.ndarray, nlev: int, min_max: int = 0) -> "BrickScene":

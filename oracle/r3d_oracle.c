@@ -259,6 +259,39 @@ static float shard_fetch(const orc_cube *atlas, float inv_adim, v3f org, v3f bl,
   return cube_sample(atlas, u, lod);
 }
 
+/* overlay atlas i at the sample's brick coordinate: ink / 3D ink /
+ * registration like bricks_fetch (:87-97,105-111), labels at the texel
+ * centre under bl (:99-104) */
+static float ovl_fetch(const scene *s, int i, uint32_t slot, v3f bl) {
+  const uint8_t *g = s->br->ovl[i] + (size_t)slot * (128u * 128u * 128u);
+  if (i == 2) {
+    float lx = clampf_(floorf(bl.x) + 0.5f, 0.5f, 127.5f),
+          ly = clampf_(floorf(bl.y) + 0.5f, 0.5f, 127.5f),
+          lz = clampf_(floorf(bl.z) + 0.5f, 0.5f, 127.5f);
+    return tri_u8(g, 128u, 128u, 128u, lx - 0.5f, ly - 0.5f, lz - 0.5f);
+  }
+  float lx = clampf_(bl.x, 0.5f, 127.5f), ly = clampf_(bl.y, 0.5f, 127.5f),
+        lz = clampf_(bl.z, 0.5f, 127.5f);
+  return tri_u8(g, 128u, 128u, 128u, lx - 0.5f, ly - 0.5f, lz - 0.5f);
+}
+
+/* label_color, :63-66 (palette :52-61) */
+static void label_color(float v, float c[3]) {
+  static const float pal[8][3] = {{0.82f, 0.66f, 0.43f}, {0.95f, 0.20f, 0.85f},
+                                  {0.20f, 0.80f, 0.80f}, {0.30f, 0.90f, 0.30f},
+                                  {1.00f, 0.55f, 0.15f}, {0.35f, 0.45f, 0.90f},
+                                  {0.95f, 0.90f, 0.20f}, {0.90f, 0.90f, 0.90f}};
+  uint32_t k = (uint32_t)floorf(fmaf(v, 255.0f, 0.5f));
+  k = k < 1u ? 1u : (k > 8u ? 8u : k);
+  for (int j = 0; j < 3; j++) c[j] = pal[k - 1u][j];
+}
+
+static void lerp3(float c[3], float r, float g, float b, float t) {
+  c[0] = lerpf_(c[0], r, t);
+  c[1] = lerpf_(c[1], g, t);
+  c[2] = lerpf_(c[2], b, t);
+}
+
 /* ------------------------------------------------------------ the march */
 
 typedef struct ray_out {
@@ -399,6 +432,12 @@ static void march(const r3d_frame_params *pc, const scene *s, const uint8_t lut[
   float acc[4] = {0, 0, 0, 0};
   uint32_t steps = 0, mip_index = 0;
   int composite = pc->mode == R3D_MODE_FULL || pc->mode == R3D_MODE_FLAT;
+  /* overlays (:45-49,67-73) */
+  uint32_t ovl = lodb ? pc->overlay_flags & 0x1Du : 0u;
+  float reg_alpha = (float)((pc->overlay_flags >> 16) & 0xffu) * (1.0f / 255.0f);
+  int pal1 = ((pc->overlay_flags >> 8) & 0xffu) == 1u;
+  float ovl_col[3] = {pal1 ? 0.3f : 0.25f, pal1 ? 0.72f : 1.0f, pal1 ? 1.0f : 0.55f};
+  float ink_max = 0.0f, ink2_max = 0.0f, lbl_max = 0.0f, reg_max = 0.0f;
   int shaded = pc->mode == R3D_MODE_FULL;
   uint32_t ray_budget = lodb ? (shaded ? 192u : 256u) : MAX_STEPS;
   float span_step = fmaxf((tf_ - tn) / ((float)ray_budget * dt), 1.0f);
@@ -476,7 +515,7 @@ static void march(const r3d_frame_params *pc, const scene *s, const uint8_t lut[
     float bsz = bs;
     if (lodb) {
       float bgate = fmaxf(occ_gate, 4.5f / 255.0f);
-      if (pc->mode == R3D_MODE_MIP && b.ok && b.maxv <= mip_max) {
+      if (pc->mode == R3D_MODE_MIP && !ovl && b.ok && b.maxv <= mip_max) {
         void_blk = 1;
         bsz = b.world_brick;
       } else if (v < bgate && b.maxv < bgate) {
@@ -513,16 +552,40 @@ static void march(const r3d_frame_params *pc, const scene *s, const uint8_t lut[
       mip_max = v;
       mip_index = steps;
     }
-    if (pc->mode == R3D_MODE_MIP && mip_max >= 0.999f) break; /* :888 */
+    if (ovl && pc->mode == R3D_MODE_MIP && b.ok) { /* :872-887 */
+      float k;
+      if ((ovl & 1u) && (k = ovl_fetch(s, 0, b.slot, b.bl)) > ink_max) ink_max = k;
+      if ((ovl & 4u) && (k = ovl_fetch(s, 1, b.slot, b.bl)) > ink2_max) ink2_max = k;
+      if ((ovl & 8u) && (k = ovl_fetch(s, 2, b.slot, b.bl)) > lbl_max) lbl_max = k;
+      if (ovl & 16u) {
+        k = ovl_fetch(s, 3, b.slot, b.bl);
+        if (k < pc->threshold) k = 0.0f;
+        if (k > reg_max) reg_max = k;
+      }
+    }
+    if (pc->mode == R3D_MODE_MIP && !ovl && mip_max >= 0.999f) break; /* :888 */
     if (first_hit < 0.0f && v > 0.05f) first_hit = t;         /* :891 */
 
     if (composite && !cut) {
-      float sm[4];
+      float sm[4], rs[4] = {0, 0, 0, 0};
       tf_sample(lut, v, sm);
+      int reg_live = (ovl & 16u) && b.ok;
+      if (reg_live) { /* the moving scan through the same TF (:895-905) */
+        float rv = ovl_fetch(s, 3, b.slot, b.bl);
+        if (rv < pc->threshold) rv = 0.0f;
+        tf_sample(lut, rv, rs);
+        sm[3] = fmaxf(sm[3], rs[3] * reg_alpha);
+      }
       /* opacity correction (:906) */
       float a = 1.0f - r3d_powf(1.0f - sm[3], opac_k * lod_step);
       if (a > 0.003f) {
         float col[3] = {sm[0], sm[1], sm[2]};
+        if (reg_live) { /* green/magenta fuse before shading (:910-914) */
+          v3f wl = mk3(0.333f, 0.334f, 0.333f);
+          float lm = dot3(mk3(rs[0], rs[1], rs[2]), wl);
+          float lf = dot3(mk3(col[0], col[1], col[2]), wl);
+          lerp3(col, lm, lf, lm, reg_alpha);
+        }
         if (shaded) {
           float g[3];
           if (o->quality == R3D_QUALITY_FAST) { /* :919-955 */
@@ -596,6 +659,19 @@ static void march(const r3d_frame_params *pc, const scene *s, const uint8_t lut[
             for (int k = 0; k < 3; k++) col[k] = fmaf(col[k], lm, sw);
           }
         }
+        if (ovl & 1u) /* tints after shading (:1000-1014) */
+          lerp3(col, ovl_col[0], ovl_col[1], ovl_col[2],
+                satf(ovl_fetch(s, 0, b.slot, b.bl) * pc->overlay_gain));
+        if (ovl & 4u)
+          lerp3(col, 1.0f, 0.30f, 0.22f, satf(ovl_fetch(s, 1, b.slot, b.bl) * pc->overlay_gain));
+        if (ovl & 8u) {
+          float k = ovl_fetch(s, 2, b.slot, b.bl);
+          if (k > 0.0f) {
+            float lc[3];
+            label_color(k, lc);
+            lerp3(col, lc[0], lc[1], lc[2], 0.65f);
+          }
+        }
         /* front-to-back compositing and early termination (:1015-1017) */
         float wgt = (1.0f - acc[3]) * a;
         for (int k = 0; k < 3; k++) acc[k] = fmaf(wgt, col[k], acc[k]);
@@ -624,12 +700,32 @@ static void march(const r3d_frame_params *pc, const scene *s, const uint8_t lut[
     out->rgb[2] = fmaf(tr, BG_B, acc[2]);
   } else {
     float m = mip_max * pc->density;
-    out->rgb[0] = out->rgb[1] = out->rgb[2] = m;
+    float c[3] = {m, m, m};
+    if (ovl & 16u) { /* reg_fuse, :113-116 */
+      float mr = reg_max * pc->density;
+      float lum = dot3(mk3(c[0], c[1], c[2]), mk3(0.333f, 0.334f, 0.333f));
+      lerp3(c, mr, lum, mr, reg_alpha);
+    }
+    if (ovl & 1u) lerp3(c, ovl_col[0], ovl_col[1], ovl_col[2], satf(ink_max * pc->overlay_gain));
+    if (ovl & 4u) lerp3(c, 1.0f, 0.30f, 0.22f, satf(ink2_max * pc->overlay_gain));
+    if ((ovl & 8u) && lbl_max > 0.0f) {
+      float lc[3];
+      label_color(lbl_max, lc);
+      lerp3(c, lc[0], lc[1], lc[2], 0.65f);
+    }
+    out->rgb[0] = c[0];
+    out->rgb[1] = c[1];
+    out->rgb[2] = c[2];
   }
 }
 
 static int check_view(const r3d_frame_params *p, const orc_cube *cube, const orc_bricks *br) {
-  if (p->slab_grid || p->clip_valid || p->overlay_flags ||
+  if ((p->overlay_flags & 0x1Du) &&
+      (!(p->brick_mode & R3D_BRICK_LOD_FLAG) || !br || ((p->overlay_flags & 1u) && !br->ovl[0]) ||
+       ((p->overlay_flags & 4u) && !br->ovl[1]) || ((p->overlay_flags & 8u) && !br->ovl[2]) ||
+       ((p->overlay_flags & 16u) && !br->ovl[3])))
+    return -1;
+  if (p->slab_grid || p->clip_valid ||
       (p->view_flags & (R3D_VIEW_SURF | R3D_VIEW_STRETCH)) || p->mode >= R3D_MODE_COUNT)
     return -1;
   if (p->brick_mode & R3D_BRICK_LOD_FLAG) {
@@ -794,6 +890,74 @@ void orc_occupancy(const uint8_t *vox, uint32_t nx, uint32_t ny, uint32_t nz, ui
 }
 
 static uint32_t ceil_div(uint32_t a, uint32_t b) { return (a + b - 1u) / b; }
+
+int orc_build_lod_overlay(const uint8_t *vox, uint32_t nx, uint32_t ny, uint32_t nz,
+                          const uint32_t *page, uint32_t page_words, int labels, uint8_t *pool,
+                          uint32_t nslots) {
+  if (page_words < R3D_BRICK_PAGE_HEADER || page[1] != nx || page[2] != ny || page[3] != nz)
+    return -1;
+  uint32_t nlev = page[0];
+  if (nlev < 1u || nlev > 15u || page_words != orc_lod_page_words(nx, ny, nz, nlev)) return -1;
+  uint32_t bd[16][3], E[16][3];
+  uint8_t *lev[16] = {0};
+  for (uint32_t l = 0; l < nlev; l++) {
+    uint32_t sc = 1u << l;
+    bd[l][0] = ceil_div(ceil_div(nx, sc), 128u);
+    bd[l][1] = ceil_div(ceil_div(ny, sc), 128u);
+    bd[l][2] = ceil_div(ceil_div(nz, sc), 128u);
+    for (int a = 0; a < 3; a++) E[l][a] = bd[l][a] * 128u;
+  }
+#define L0(X, Y, Z) \
+  ((X) < nx && (Y) < ny && (Z) < nz ? vox[((size_t)(Z) * ny + (Y)) * nx + (X)] : (uint8_t)0)
+  for (uint32_t l = 1; l < nlev; l++) {
+    lev[l] = malloc((size_t)E[l][0] * E[l][1] * E[l][2]);
+    if (!lev[l]) goto fail;
+    for (uint32_t z = 0; z < E[l][2]; z++)
+      for (uint32_t y = 0; y < E[l][1]; y++)
+        for (uint32_t x = 0; x < E[l][0]; x++) {
+          uint8_t v;
+          if (labels) {
+            uint64_t X = (uint64_t)x << l, Y = (uint64_t)y << l, Z = (uint64_t)z << l;
+            v = X < nx && Y < ny && Z < nz ? vox[(Z * ny + Y) * nx + X] : 0;
+          } else {
+            uint32_t sum = 4u;
+            for (uint32_t k = 0; k < 8u; k++) {
+              uint32_t xx = 2u * x + (k & 1u), yy = 2u * y + ((k >> 1) & 1u),
+                       zz = 2u * z + (k >> 2);
+              if (l == 1u)
+                sum += L0(xx, yy, zz);
+              else if (xx < E[l - 1][0] && yy < E[l - 1][1] && zz < E[l - 1][2])
+                sum += lev[l - 1][((size_t)zz * E[l - 1][1] + yy) * E[l - 1][0] + xx];
+            }
+            v = (uint8_t)(sum / 8u);
+          }
+          lev[l][((size_t)z * E[l][1] + y) * E[l][0] + x] = v;
+        }
+  }
+  for (uint32_t l = 0; l < nlev; l++) {
+    uint32_t off = page[4u + l * 4u];
+    for (uint32_t bz = 0; bz < bd[l][2]; bz++)
+      for (uint32_t by = 0; by < bd[l][1]; by++)
+        for (uint32_t bx = 0; bx < bd[l][0]; bx++) {
+          uint32_t e = page[off + (bz * bd[l][1] + by) * bd[l][0] + bx];
+          if (e == R3D_BRICK_ABSENT || (e & 0xFFFFFFu) >= nslots) continue;
+          uint8_t *dst = pool + (size_t)(e & 0xFFFFFFu) * (128u * 128u * 128u);
+          for (uint32_t z = 0; z < 128u; z++)
+            for (uint32_t y = 0; y < 128u; y++)
+              for (uint32_t x = 0; x < 128u; x++) {
+                uint32_t X = bx * 128u + x, Y = by * 128u + y, Z = bz * 128u + z;
+                dst[((size_t)z * 128u + y) * 128u + x] =
+                    l == 0u ? L0(X, Y, Z) : lev[l][((size_t)Z * E[l][1] + Y) * E[l][0] + X];
+              }
+        }
+  }
+#undef L0
+  for (uint32_t l = 1; l < nlev; l++) free(lev[l]);
+  return 0;
+fail:
+  for (uint32_t l = 1; l < nlev; l++) free(lev[l]);
+  return -1;
+}
 
 int orc_build_shard(const uint8_t *vox, uint32_t edge, uint32_t abpa, const uint32_t *slot_of,
                     uint32_t *page, uint8_t *atlas0) {

@@ -49,6 +49,10 @@ typedef struct orc_bricks {
   const uint8_t *pool;
   uint32_t nslots;
   const orc_cube *atlas;
+  /* LOD mode: slot-parallel overlay atlases in the pool's layout (ink,
+   * 3D ink, labels, registration; NULL when absent), sampled per
+   * src/shaders/raycast.slang:45-115,872-914,1000-1014,1032-1036 */
+  const uint8_t *ovl[4];
 } orc_bricks;
 
 typedef struct orc_opts {
@@ -121,6 +125,16 @@ int64_t orc_build_lod_bricks(const uint8_t *vox, uint32_t nx, uint32_t ny, uint3
                              uint32_t nlev, uint32_t min_max, uint32_t *page,
                              uint32_t page_words, uint8_t *pool, uint64_t pool_slots);
 uint32_t orc_lod_page_words(uint32_t nx, uint32_t ny, uint32_t nz, uint32_t nlev);
+
+/* Slot contents of an overlay atlas for an existing LOD page table: each
+ * resident brick (level l, slot s) receives the same brick of the overlay
+ * volume's level l -- the (sum+4)/8 box pyramid of orc_build_lod_bricks,
+ * or with labels != 0 the level-0 voxel at (x, y, z) << l
+ * (src/core/labelvol.c:172-196).  pool holds nslots * 128^3 bytes and is
+ * written only at resident slots.  Returns 0, or -1 on bad input. */
+int orc_build_lod_overlay(const uint8_t *vox, uint32_t nx, uint32_t ny, uint32_t nz,
+                          const uint32_t *page, uint32_t page_words, int labels, uint8_t *pool,
+                          uint32_t nslots);
 
 /* Single-level brick atlas from a cubic volume of edge bpa * 128: atlas
  * level 0 ((abpa * 128)^3, slot s at (s % abpa, s / abpa % abpa,

@@ -141,6 +141,8 @@ def _load() -> C.CDLL:
         "r3d_cuda_bricks_read": (I, [P, P, P]),
         "r3d_cuda_cube_read": (I, [P, I, P, P]),
         "r3d_cuda_shard_build": (I, [P, U32, P, U32, P]),
+        "r3d_cuda_bricks_overlay_load": (I, [P, U32, P]),
+        "r3d_cuda_bricks_overlay_build": (I, [P, U32, C.POINTER(VolumeDesc), P]),
         "r3d_cuda_shard_mode": (U32, [P]),
         "r3d_cuda_shard_read": (I, [P, I, P, P, P]),
         "r3d_cuda_raycast_fwd": (I, [P, P, U32, P, U32, U32, C.POINTER(CudaAux), P]),
@@ -399,6 +401,19 @@ class Context:
         out = np.empty((dims[2], dims[1], dims[0]), np.uint8)
         self._check(lib.r3d_cuda_cube_read(self.h, level, _ptr(out), dims))
         return out
+
+    def overlay_load(self, which: int, slots) -> None:
+        """Overlay atlas `which` (0 ink, 1 3D ink, 2 labels, 3 registration)
+        from slot contents in the CT pool's order, or None to remove it."""
+        if slots is not None and isinstance(slots, np.ndarray):
+            slots = np.ascontiguousarray(slots, np.uint8)
+        self._check(lib.r3d_cuda_bricks_overlay_load(self.h, which, _ptr(slots)))
+
+    def overlay_build(self, which: int, vol) -> None:
+        """Overlay atlas `which` cut from a raw volume of the cache's shape."""
+        nz, ny, nx = vol.shape
+        d = VolumeDesc(nx, ny, nz, 128, 1.0)
+        self._check(lib.r3d_cuda_bricks_overlay_build(self.h, which, C.byref(d), _ptr(vol)))
 
     def shard_build(self, vol, abpa: int | None = None, slot_of=None) -> None:
         """Single-level brick atlas from a cubic volume of edge bpa * 128

@@ -263,6 +263,7 @@ void r3d_cuda_destroy(r3d_cuda_ctx *c) {
   cudaFree(c->pool);
   cudaFree(c->bmax);
   cudaFree(c->quad);
+  for (int i = 0; i < 4; i++) cudaFree(c->ovl_quad[i]);
   cudaFree(c->shard_buf);
   cudaFree(c->shard_page);
   cudaFree(c->lut);
@@ -436,6 +437,11 @@ static int build_blockmax(r3d_cuda_ctx *c) {
   R3D_CUDA_TRY(c, cudaMemsetAsync(c->bmax, 0, n, c->stream));
   cudaFree(c->quad);
   c->quad = nullptr;
+  for (int i = 0; i < 4; i++) {  // overlays follow the old slot assignment
+    cudaFree(c->ovl_quad[i]);
+    c->ovl_quad[i] = nullptr;
+    c->br.ovl[i] = nullptr;
+  }
   const size_t nq = (size_t)(c->nslots ? c->nslots : 1u) * (128u * 128u * 128u);
   R3D_CUDA_TRY(c, cudaMalloc(&c->quad, nq * sizeof(uint32_t)));
   if (c->nslots) {
@@ -737,8 +743,15 @@ int prepare_view(r3d_cuda_ctx *c, const r3d_frame_params &in, uint32_t out_w,
     return fail(c, R3D_E_UNSUPPORTED, "view: slab / clipmap sampling is not implemented");
   if (in.view_flags & (R3D_VIEW_SURF | R3D_VIEW_STRETCH))
     return fail(c, R3D_E_UNSUPPORTED, "view: flattened-surface views are not implemented");
-  if (in.overlay_flags & 0x1Du)
-    return fail(c, R3D_E_UNSUPPORTED, "view: overlay atlases are not implemented");
+  if (in.overlay_flags & kOvlAtlases) {
+    if (!(in.brick_mode & R3D_BRICK_LOD_FLAG))
+      return fail(c, R3D_E_UNSUPPORTED, "view: overlay atlases need the LOD brick cache");
+    static const char *names[4] = {"ink", "3D ink", "labels", "registration"};
+    const uint32_t bit[4] = {kOvlInk, kOvlInk3d, kOvlLabels, kOvlReg};
+    for (int i = 0; i < 4; i++)
+      if ((in.overlay_flags & bit[i]) && !c->ovl_quad[i])
+        return fail(c, R3D_E_STATE, "view: overlay atlas '%s' is not loaded", names[i]);
+  }
   if (!(in.max_mip >= 0.0f)) return fail(c, R3D_E_INVALID, "view: max_mip must be >= 0");
   if (!(in.step_voxels > 0.0f)) return fail(c, R3D_E_INVALID, "view: step_voxels must be > 0");
   if (in.brick_mode & R3D_BRICK_LOD_FLAG) {
@@ -921,7 +934,11 @@ int r3d_cuda_raycast_fwd(r3d_cuda_ctx *c, const r3d_frame_params *views, uint32_
     }
   }
   R3D_CUDA_TRY(c, cudaEventRecord(c->ev0, st));
-  if (c->sched.persistent) {
+  // views with overlay atlases render through the grid kernel
+  bool any_ovl = false;
+  for (uint32_t v = 0; v < nviews; v++)
+    any_ovl = any_ovl || (render[v] && (pcs[v].overlay_flags & kOvlAtlases));
+  if (c->sched.persistent && !any_ovl) {
     int rc = launch_views_persistent(c, pcs, render, nviews, img, out_w, steps, mip, total,
                                      counters, st);
     if (rc != R3D_OK) return rc;

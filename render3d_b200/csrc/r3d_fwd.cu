@@ -34,7 +34,7 @@ static_assert(kFwdWarps == 1 || kFwdWarps == 2 || kFwdWarps == 4, "1, 2 or 4 war
 // shades the parked samples together once at least shade_min lanes are
 // waiting or every live lane is, so the branch runs with more lanes active.
 // Rays are independent, so each ray's arithmetic and result are unchanged.
-template <int PATH, int MODE, bool FAST, bool COUNT, bool DEFER>
+template <int PATH, int MODE, bool FAST, bool COUNT, bool DEFER, bool OVL = false>
 __global__ void R3D_FWD_BOUNDS k_raycast(const __grid_constant__ r3d_frame_params pc,
                                          const __grid_constant__ DevScene s,
                                          const uchar4 *__restrict__ lut,
@@ -90,7 +90,7 @@ __global__ void R3D_FWD_BOUNDS k_raycast(const __grid_constant__ r3d_frame_param
     }
     if (marched) ray_end<MODE>(vc, st, r);
   } else if (inside) {
-    march<PATH, MODE, FAST, COUNT>(pc, s, vc, tf, px, py, r);
+    march<PATH, MODE, FAST, COUNT, OVL>(pc, s, vc, tf, px, py, r);
   }
   if (inside) {
     my_tf = r.n_tf;
@@ -137,6 +137,20 @@ static cudaError_t launch_t(const r3d_frame_params &pc, const DevScene &s, const
   dim3 grid((gw + kBlockW - 1u) / kBlockW, (gh + kBlockH - 1u) / kBlockH);
   const uint32_t threads = kFwdWarps * 32u;
   constexpr bool kDeferable = MODE == R3D_MODE_FULL;
+  // overlay atlases: LOD bricks in the compositing and MIP modes
+  constexpr bool kOvl = PATH == PATH_LOD_BRICKS &&
+                        (MODE == R3D_MODE_FULL || MODE == R3D_MODE_FLAT || MODE == R3D_MODE_MIP);
+  if constexpr (kOvl) {
+    if (pc.overlay_flags & kOvlAtlases) {
+      if (counters)
+        k_raycast<PATH, MODE, FAST, true, false, true><<<grid, threads, 0, stream>>>(
+            pc, s, lut, (uchar4 *)img, out_w, steps, mip, total, counters, 0u);
+      else
+        k_raycast<PATH, MODE, FAST, false, false, true><<<grid, threads, 0, stream>>>(
+            pc, s, lut, (uchar4 *)img, out_w, steps, mip, total, nullptr, 0u);
+      return cudaGetLastError();
+    }
+  }
   if (kDeferable && shade) {
     if (counters)
       k_raycast<PATH, MODE, FAST, true, kDeferable><<<grid, threads, 0, stream>>>(

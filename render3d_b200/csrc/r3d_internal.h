@@ -25,6 +25,7 @@ struct r3d_cuda_ctx {
   uint8_t *pool = nullptr;
   uint8_t *bmax = nullptr;  // per-slot dilated 8^3 block maxima (4096 B/slot)
   uint32_t *quad = nullptr;  // per-slot quad words (DevBricks::quad)
+  uint32_t *ovl_quad[4] = {nullptr, nullptr, nullptr, nullptr};  // overlay atlases
   uint32_t page_words = 0;
   uint32_t nslots = 0;
   uint32_t abpa = 0;

@@ -53,6 +53,9 @@ struct DevBricks {
   // per slot, 128^3 words: bytes (x, y), (x1, y), (x, y1), (x1, y1) of the
   // texel's z plane, x1 = min(x + 1, 127) and y1 likewise
   const uint32_t *quad;
+  // slot-parallel overlay atlases in the same quad form: ink, 3D ink,
+  // labels, registration (nullptr: not loaded)
+  const uint32_t *ovl[4];
   uint32_t nslots;
   uint32_t nlev;
   float bs[3];     // base shape
@@ -346,6 +349,40 @@ __device__ __forceinline__ float slot_sample(const DevScene &s, uint32_t slot, c
   return tri_slot_q(s.br.quad + (size_t)slot * (128u * 128u * 128u), q);
 }
 
+// overlay_flags (raycast.slang:45-49): the four slot-parallel atlases
+constexpr uint32_t kOvlInk = 1u, kOvlInk3d = 4u, kOvlLabels = 8u, kOvlReg = 16u;
+constexpr uint32_t kOvlAtlases = kOvlInk | kOvlInk3d | kOvlLabels | kOvlReg;
+
+// paint-label palette, class id 1..8 (raycast.slang:52-61)
+static __constant__ float kLabelPal[8][3] = {
+    {0.82f, 0.66f, 0.43f}, {0.95f, 0.20f, 0.85f}, {0.20f, 0.80f, 0.80f}, {0.30f, 0.90f, 0.30f},
+    {1.00f, 0.55f, 0.15f}, {0.35f, 0.45f, 0.90f}, {0.95f, 0.90f, 0.20f}, {0.90f, 0.90f, 0.90f}};
+
+// bricks_fetch of overlay atlas i (ink, 3D ink, registration) at the
+// sample's clamped slot coordinate (raycast.slang:87-97,105-111)
+__device__ __forceinline__ float ovl_fetch(const DevScene &s, int i, uint32_t slot,
+                                           const SlotCoord &q) {
+  return tri_slot_q(s.br.ovl[i] + (size_t)slot * (128u * 128u * 128u), q);
+}
+
+// bricks_fetch_label (raycast.slang:99-104): the texel under bl, snapped
+// to its centre so that class ids never blend
+__device__ __forceinline__ float ovl_label(const DevScene &s, uint32_t slot, float3 bl) {
+  const uint32_t x = (uint32_t)(clamp_(floorf(bl.x) + 0.5f, 0.5f, 127.5f) - 0.5f);
+  const uint32_t y = (uint32_t)(clamp_(floorf(bl.y) + 0.5f, 0.5f, 127.5f) - 0.5f);
+  const uint32_t z = (uint32_t)(clamp_(floorf(bl.z) + 0.5f, 0.5f, 127.5f) - 0.5f);
+  const uint32_t w =
+      __ldg(s.br.ovl[2] + (size_t)slot * (128u * 128u * 128u) + ((z << 14) | (y << 7) | x));
+  return qbyte(w, 0) * kInv255;
+}
+
+// label_color (raycast.slang:63-66)
+__device__ __forceinline__ float3 label_color(float v) {
+  uint32_t c = (uint32_t)floorf(fmaf(v, 255.0f, 0.5f));
+  c = c < 1u ? 1u : (c > 8u ? 8u : c);
+  return make_float3(kLabelPal[c - 1u][0], kLabelPal[c - 1u][1], kLabelPal[c - 1u][2]);
+}
+
 // bricks_fetch at atlas lod 0 (raycast.slang:284-288): clamp to
 // [0.5, 127.5] inside the brick, no cross-brick filtering
 __device__ __forceinline__ float brick_fetch(const DevScene &s, uint32_t slot, float3 bl) {
@@ -400,6 +437,11 @@ struct ViewConst {
   float lod_bias, threshold, density;
   float3 ext;
   bool ortho, lod_on;
+  // overlays (raycast.slang:45-49,67-73): atlas bits, ink gain, the
+  // registration fuse weight and the ink tint
+  uint32_t ovl;
+  float ovl_gain, reg_alpha;
+  float3 ovl_col;
 };
 
 template <int PATH>
@@ -434,6 +476,11 @@ __device__ __forceinline__ ViewConst view_const(const r3d_frame_params &pc, cons
   v.ortho = (pc.view_flags & R3D_VIEW_ORTHO) != 0u;
   // with a zero LOD ceiling the clamp pins lod to 0 whatever log2 returns
   v.lod_on = v.max_lod != 0.0f;
+  v.ovl = pc.overlay_flags & kOvlAtlases;
+  v.ovl_gain = pc.overlay_gain;
+  v.reg_alpha = (float)((pc.overlay_flags >> 16) & 0xffu) * (1.0f / 255.0f);
+  v.ovl_col = ((pc.overlay_flags >> 8) & 0xffu) == 1u ? make_float3(0.3f, 0.72f, 1.0f)
+                                                      : make_float3(0.25f, 1.0f, 0.55f);
   return v;
 }
 
@@ -447,6 +494,8 @@ struct Pending {
   uint32_t slot;
   float3 bl;
   float grad_vox;
+  float4 rs;  // overlays: TF sample of the registration atlas
+  bool reg_live;
 };
 
 // State of one ray between march steps.
@@ -460,6 +509,7 @@ struct RayState {
   uint32_t steps, mip_index;
   float mip_max, first_hit;
   float acc_r, acc_g, acc_b, acc_a;
+  float ink_max, ink2_max, lbl_max, reg_max;  // overlay MIP maxima (raycast.slang:731-734)
   LodCache lc;
   uint32_t n_tf, n_grad, n_walk;
 };
@@ -583,6 +633,7 @@ __device__ __forceinline__ bool ray_begin(const r3d_frame_params &pc, const DevS
   st.mip_max = 0.0f;
   st.first_hit = -1.0f;
   st.acc_r = st.acc_g = st.acc_b = st.acc_a = 0.0f;
+  st.ink_max = st.ink2_max = st.lbl_max = st.reg_max = 0.0f;
   st.lc.valid = false;
   st.lc.desired = -1;
   st.lc.inv_scale = 1.0f;
@@ -613,7 +664,7 @@ __device__ __forceinline__ float skip_block(const RayState &st, float3 p, float 
 // Gradient shading (FULL mode, raycast.slang:919-998) and front-to-back
 // compositing (:1015-1017) of a contributing sample, then the step advance
 // (:1020).  Returns false when the opacity cutoff ends the ray.
-template <int PATH, int MODE, bool FAST, bool COUNT>
+template <int PATH, int MODE, bool FAST, bool COUNT, bool OVL = false>
 __device__ __forceinline__ bool composite_sample(const DevScene &s, const ViewConst &vc,
                                                  RayState &st, const Pending &q) {
   constexpr bool kLod = PATH == PATH_LOD_BRICKS;
@@ -621,6 +672,14 @@ __device__ __forceinline__ bool composite_sample(const DevScene &s, const ViewCo
   constexpr bool kShaded = MODE == R3D_MODE_FULL;
   const float3 dir = st.dir;
   float col_r = q.sm.x, col_g = q.sm.y, col_b = q.sm.z;
+  if (OVL && q.reg_live) {  // green/magenta fuse in TF space, before shading (:910-914)
+    const float3 wl = make_float3(0.333f, 0.334f, 0.333f);
+    const float lm = dot3(make_float3(q.rs.x, q.rs.y, q.rs.z), wl);
+    const float lf = dot3(make_float3(col_r, col_g, col_b), wl);
+    col_r = lerp_(col_r, lm, vc.reg_alpha);
+    col_g = lerp_(col_g, lf, vc.reg_alpha);
+    col_b = lerp_(col_b, lm, vc.reg_alpha);
+  }
   // taps sampled like a cube texture: the cube, or the identity shard atlas
   const DevCube &tex = kShard ? s.sh.atlas : s.cube;
   // non-identity shard: taps at lod_step voxels through the slot
@@ -718,6 +777,30 @@ __device__ __forceinline__ bool composite_sample(const DevScene &s, const ViewCo
       col_b = fmaf(col_b, lm, sw);
     }
   }
+  if (OVL) {  // overlay tints after shading (raycast.slang:1000-1014)
+    const SlotCoord c = slot_coord(q.bl);
+    if (vc.ovl & kOvlInk) {
+      const float k = sat_(ovl_fetch(s, 0, q.slot, c) * vc.ovl_gain);
+      col_r = lerp_(col_r, vc.ovl_col.x, k);
+      col_g = lerp_(col_g, vc.ovl_col.y, k);
+      col_b = lerp_(col_b, vc.ovl_col.z, k);
+    }
+    if (vc.ovl & kOvlInk3d) {
+      const float k = sat_(ovl_fetch(s, 1, q.slot, c) * vc.ovl_gain);
+      col_r = lerp_(col_r, 1.0f, k);
+      col_g = lerp_(col_g, 0.30f, k);
+      col_b = lerp_(col_b, 0.22f, k);
+    }
+    if (vc.ovl & kOvlLabels) {
+      const float k = ovl_label(s, q.slot, q.bl);
+      if (k > 0.0f) {
+        const float3 lc = label_color(k);
+        col_r = lerp_(col_r, lc.x, 0.65f);
+        col_g = lerp_(col_g, lc.y, 0.65f);
+        col_b = lerp_(col_b, lc.z, 0.65f);
+      }
+    }
+  }
   // front-to-back compositing (raycast.slang:1015-1017)
   float wgt = (1.0f - st.acc_a) * q.a;
   st.acc_r = fmaf(wgt, col_r, st.acc_r);
@@ -753,7 +836,7 @@ __device__ __forceinline__ void lod_range(RayState &st, const ViewConst &vc, int
 // opacity cutoff) and kStepCont otherwise.  With DEFER, a sample that needs
 // gradient shading stops before it: the sample is left in pend and
 // kStepShade returned; composite_sample(pend) completes the iteration.
-template <int PATH, int MODE, bool FAST, bool COUNT, bool DEFER = false>
+template <int PATH, int MODE, bool FAST, bool COUNT, bool DEFER = false, bool OVL = false>
 __device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, const float4 *tf,
                                         RayState &st, Pending &pend) {
   constexpr bool kLod = PATH == PATH_LOD_BRICKS;
@@ -817,7 +900,8 @@ __device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, 
       else
         elide = void_known &&
                 (cut_known || clamp_(fmaf(vub, 256.0f, -0.5f), 0.0f, 255.0f) < s.tf_zero_t);
-      if (elide) {  // the sample changes nothing but the march position
+      // overlays read every sample (MIP maxima, registration opacity)
+      if (!OVL && elide) {  // the sample changes nothing but the march position
         if ((MODE == R3D_MODE_MIP && b.maxv <= st.mip_max) || b.maxv < vc.bgate)
           st.t = skip_block(st, p, b.world_brick);
         else
@@ -856,7 +940,8 @@ __device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, 
 
   // empty-space skip (raycast.slang:829-869)
   if (kLod) {
-    if ((MODE == R3D_MODE_MIP && b.ok && b.maxv <= st.mip_max) ||
+    // MIP early-out only without overlays: ink can live where CT is dim
+    if ((MODE == R3D_MODE_MIP && !OVL && b.ok && b.maxv <= st.mip_max) ||
         (v < vc.bgate && b.maxv < vc.bgate)) {
       st.t = skip_block(st, p, b.world_brick);
       return kStepCont;
@@ -885,24 +970,54 @@ __device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, 
     st.mip_max = v;
     st.mip_index = st.steps;
   }
-  if (MODE == R3D_MODE_MIP && st.mip_max >= 0.999f) return kStepDone;
+  if (OVL && MODE == R3D_MODE_MIP && b.ok) {  // overlay maxima (raycast.slang:872-887)
+    const SlotCoord c = slot_coord(b.bl);
+    if (vc.ovl & kOvlInk) {
+      const float k = ovl_fetch(s, 0, b.slot, c);
+      if (k > st.ink_max) st.ink_max = k;
+    }
+    if (vc.ovl & kOvlInk3d) {
+      const float k = ovl_fetch(s, 1, b.slot, c);
+      if (k > st.ink2_max) st.ink2_max = k;
+    }
+    if (vc.ovl & kOvlLabels) {
+      const float k = ovl_label(s, b.slot, b.bl);
+      if (k > st.lbl_max) st.lbl_max = k;
+    }
+    if (vc.ovl & kOvlReg) {
+      float k = ovl_fetch(s, 3, b.slot, c);
+      if (k < vc.threshold) k = 0.0f;
+      if (k > st.reg_max) st.reg_max = k;
+    }
+  }
+  if (MODE == R3D_MODE_MIP && !OVL && st.mip_max >= 0.999f) return kStepDone;
   if (MODE == R3D_MODE_DEPTH && st.first_hit < 0.0f && v > 0.05f) st.first_hit = t;
 
   if (kComposite && !cut) {
     float tt = clamp_(fmaf(v, 256.0f, -0.5f), 0.0f, 255.0f);
+    const bool reg_live = OVL && (vc.ovl & kOvlReg) && b.ok;
     // below tf_zero_t both TF texels have alpha 0, so the opacity is
-    // exactly 0 and the sample cannot contribute
-    if (tt >= s.tf_zero_t) {
+    // exactly 0 and the sample cannot contribute (unless the registration
+    // scan lends it opacity)
+    if (tt >= s.tf_zero_t || reg_live) {
       if (COUNT) st.n_tf++;
       float4 sm = tf_sample(tf, tt);
+      float4 rs = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      if (reg_live) {  // the moving scan through the same TF (raycast.slang:895-905)
+        float rv = ovl_fetch(s, 3, b.slot, slot_coord(b.bl));
+        if (rv < vc.threshold) rv = 0.0f;
+        rs = tf_sample(tf, clamp_(fmaf(rv, 256.0f, -0.5f), 0.0f, 255.0f));
+        sm.w = fmaxf(sm.w, rs.w * vc.reg_alpha);
+      }
       float a = 1.0f - r3d_powf(1.0f - sm.w, vc.opac_k * lod_step);
       if (a > 0.003f) {
-        const Pending q = {p, lod, lod_step, a, sm, b.slot, b.bl, b.grad_vox};
+        const Pending q = {p, lod, lod_step, a, sm, b.slot, b.bl, b.grad_vox, rs, reg_live};
         if (DEFER && kShaded) {  // shading runs later, grouped across the warp
           pend = q;
           return kStepShade;
         }
-        return composite_sample<PATH, MODE, FAST, COUNT>(s, vc, st, q) ? kStepCont : kStepDone;
+        return composite_sample<PATH, MODE, FAST, COUNT, OVL>(s, vc, st, q) ? kStepCont
+                                                                           : kStepDone;
       }
     }
   }
@@ -911,7 +1026,7 @@ __device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, 
 }
 
 // Final colour of a marched ray (raycast.slang:1023-1038).
-template <int MODE>
+template <int MODE, bool OVL = false>
 __device__ __forceinline__ void ray_end(const ViewConst &vc, const RayState &st, RayResult &out) {
   constexpr bool kComposite = MODE == R3D_MODE_FULL || MODE == R3D_MODE_FLAT;
   out.steps = st.steps;
@@ -935,20 +1050,51 @@ __device__ __forceinline__ void ray_end(const ViewConst &vc, const RayState &st,
   } else {
     float m = st.mip_max * vc.density;
     out.rgb[0] = out.rgb[1] = out.rgb[2] = m;
+    if (OVL) {  // overlay MIP tints (raycast.slang:1032-1036)
+      float r = m, g = m, b = m;
+      if (vc.ovl & kOvlReg) {  // reg_fuse (raycast.slang:113-116)
+        const float mr = st.reg_max * vc.density;
+        const float lum = dot3(make_float3(r, g, b), make_float3(0.333f, 0.334f, 0.333f));
+        r = lerp_(r, mr, vc.reg_alpha);
+        g = lerp_(g, lum, vc.reg_alpha);
+        b = lerp_(b, mr, vc.reg_alpha);
+      }
+      if (vc.ovl & kOvlInk) {
+        const float k = sat_(st.ink_max * vc.ovl_gain);
+        r = lerp_(r, vc.ovl_col.x, k);
+        g = lerp_(g, vc.ovl_col.y, k);
+        b = lerp_(b, vc.ovl_col.z, k);
+      }
+      if (vc.ovl & kOvlInk3d) {
+        const float k = sat_(st.ink2_max * vc.ovl_gain);
+        r = lerp_(r, 1.0f, k);
+        g = lerp_(g, 0.30f, k);
+        b = lerp_(b, 0.22f, k);
+      }
+      if ((vc.ovl & kOvlLabels) && st.lbl_max > 0.0f) {
+        const float3 lc = label_color(st.lbl_max);
+        r = lerp_(r, lc.x, 0.65f);
+        g = lerp_(g, lc.y, 0.65f);
+        b = lerp_(b, lc.z, 0.65f);
+      }
+      out.rgb[0] = r;
+      out.rgb[1] = g;
+      out.rgb[2] = b;
+    }
   }
 }
 
 // One ray start to finish: raycast.slang main() for dispatch thread (px, py).
-template <int PATH, int MODE, bool FAST, bool COUNT = false>
+template <int PATH, int MODE, bool FAST, bool COUNT = false, bool OVL = false>
 __device__ __forceinline__ void march(const r3d_frame_params &pc, const DevScene &s,
                                       const ViewConst &vc, const float4 *tf, uint32_t px,
                                       uint32_t py, RayResult &out) {
   RayState st;
   Pending pend;
   if (!ray_begin<PATH, MODE>(pc, s, vc, px, py, st, out)) return;
-  while (ray_step<PATH, MODE, FAST, COUNT>(s, vc, tf, st, pend) != kStepDone) {
+  while (ray_step<PATH, MODE, FAST, COUNT, false, OVL>(s, vc, tf, st, pend) != kStepDone) {
   }
-  ray_end<MODE>(vc, st, out);
+  ray_end<MODE, OVL>(vc, st, out);
 }
 
 }  // namespace r3d

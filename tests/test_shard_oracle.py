@@ -93,3 +93,25 @@ def test_shard_view_validation(rb, orc, vol256, scroll_tf):
     p.brick_mode = 4 | (2 << 8)  # bpa does not match the atlas
     with pytest.raises(ValueError):
         orc.render(p, sh, scroll_tf, 32, 32)
+
+
+def test_overlay_builder(orc, vol256):
+    """Overlay slots cut from the CT volume itself are the CT slots; label
+    slots at a coarse level stride-sample the level-0 grid."""
+    sc = orc.BrickScene.build(vol256, 2, min_max=30)
+    assert np.array_equal(sc.build_overlay(0, vol256), sc.pool)
+    lab = (np.arange(256 ** 3, dtype=np.uint32).reshape(256, 256, 256) % 9).astype(np.uint8)
+    pool = sc.build_overlay(2, lab).reshape(-1, 128, 128, 128)
+    off1 = int(sc.page[4 + 4])  # level 1: a single 128^3 brick covering the volume
+    e = int(sc.page[off1])
+    if e != 0xFFFFFFFF:
+        assert np.array_equal(pool[e & 0xFFFFFF], lab[::2, ::2, ::2])
+    off0 = int(sc.page[4])
+    for b in range(8):
+        e = int(sc.page[off0 + b])
+        if e == 0xFFFFFFFF:
+            continue
+        bx, by, bz = b % 2, (b // 2) % 2, b // 4
+        assert np.array_equal(pool[e & 0xFFFFFF],
+                              lab[bz * 128:(bz + 1) * 128, by * 128:(by + 1) * 128,
+                                  bx * 128:(bx + 1) * 128])
