@@ -45,7 +45,7 @@ WORKLOAD = "scroll phantom 1024^3 u8, 128^3 bricks x 4 LOD levels, 1920x1080 ful
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_raycast
 # launch of this workload, mean of launches 3 and 4 of one ncu capture of
 # `python bench.py --profile 6` (orbit phases 2/120 and 3/120).
-FWD_DRAM_TRAFFIC_BYTES = 154.3e6
+FWD_DRAM_TRAFFIC_BYTES = 240.9e6
 METRIC = "raycast Gsamples/s & fps @1024^3 1080p; fwd+bwd Gsamples/s vs plain, same GPU"
 
 
