@@ -902,10 +902,11 @@ __device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, 
                 (cut_known || clamp_(fmaf(vub, 256.0f, -0.5f), 0.0f, 255.0f) < s.tf_zero_t);
       // overlays read every sample (MIP maxima, registration opacity)
       if (!OVL && elide) {  // the sample changes nothing but the march position
-        if ((MODE == R3D_MODE_MIP && b.maxv <= st.mip_max) || b.maxv < vc.bgate)
+        if ((MODE == R3D_MODE_MIP && b.maxv <= st.mip_max) || b.maxv < vc.bgate) {
           st.t = skip_block(st, p, b.world_brick);
-        else
-          st.t = fmaf(vc.dt, lod_step, t);
+          return kStepCont;
+        }
+        st.t = fmaf(vc.dt, lod_step, t);
         return kStepCont;
       }
       v = slot_sample(s, b.slot, q);
