@@ -98,6 +98,48 @@ int r3d_cuda_bricks_info(const r3d_cuda_ctx *ctx, uint32_t *page_words, uint32_t
                          uint32_t shape[3], uint32_t *nlev);
 int r3d_cuda_bricks_read(r3d_cuda_ctx *ctx, uint32_t *page, uint8_t *slots);
 
+/* Streaming LOD brick cache: the brick residency pump of render3d's
+ * streamed bricks mode (reference src/render/render.h:44-50 with a pool
+ * smaller than the volume; src/vk/vkbackend.c:3075-3106,5208-5340,
+ * 5416-5590).  _begin builds the whole LOD pyramid of a raw volume (as
+ * r3d_cuda_bricks_build with min_max 0) into pinned host memory and keeps
+ * only nslots device slots, of which the coarsest level takes its share for
+ * good.  Each _update requests the bricks of the view cone at their desired
+ * LOD (r3d_host_stream_desired), keeps the resident ones, and fills up to
+ * `budget` requests, nearest first, into free or least-recently-used slots
+ * not wanted this frame: one host-to-device copy per brick, then the slots'
+ * tables and the page table, all on the context's stream.  Bricks whose
+ * maximum is below 5 stay unpublished, like the reference's decoded air.
+ * Renders on the context's stream after an update see its bricks; views
+ * use r3d_cuda_brick_mode as for a resident cache. */
+typedef struct r3d_stream_view {
+  float eye[3], fwd[3]; /* volume-normalized camera position and direction */
+  float half_tan;       /* tan(fov / 2) */
+  float pixel_cone;     /* footprint of one pixel per unit distance */
+  uint32_t slice_z0, slice_depth; /* z window in voxels (depth 0: none) */
+  float gate;           /* bricks with max < gate * 255 are never requested */
+  uint32_t budget;      /* bricks copied in by this update, at most */
+} r3d_stream_view;
+typedef struct r3d_stream_stats {
+  uint32_t desired;   /* bricks of the request set (parents included) */
+  uint32_t requested; /* of those, not resident */
+  uint32_t uploaded;  /* copied in by this update */
+  uint32_t evicted;   /* slots taken from other bricks */
+  uint32_t resident;  /* occupied slots afterwards */
+} r3d_stream_stats;
+int r3d_cuda_stream_begin(r3d_cuda_ctx *ctx, const r3d_volume_desc *d, const uint8_t *voxels,
+                          uint32_t nlev, uint32_t nslots);
+/* The pump's inputs for a view, as render3d's main loop derives them
+ * (src/main.c:6886-6900): the camera moved into volume space by the view's
+ * model transform (ext = the volume's extent, r3d_bricks_extent), the
+ * diagonal half-angle tan(fov/2) * sqrt(1 + aspect^2), the pixel cone
+ * 2 tan(fov/2) / height * 2^lod_bias, the axis-slab z window and the
+ * skip gate. */
+void r3d_cuda_stream_view_of(const r3d_frame_params *p, const float ext[3], uint32_t budget,
+                             r3d_stream_view *view);
+int r3d_cuda_stream_update(r3d_cuda_ctx *ctx, const r3d_stream_view *view,
+                           r3d_stream_stats *stats);
+
 /* Slot-parallel overlay atlases of the LOD brick cache (reference
  * src/render/render.h:51-101; sampled by src/shaders/raycast.slang:45-115,
  * 872-914,1000-1014,1032-1036): which = 0 ink (overlay_flags bit 0, tinted

@@ -52,6 +52,28 @@ uint32_t r3d_host_lod_pick(float distance, float pixel_cone, float base_voxels,
                            uint32_t nlevels);
 uint32_t r3d_host_lod_fallback(uint32_t desired, uint32_t ordinal, uint32_t nlevels);
 
+/* View-cone LOD request of the brick streamer (src/vk/vkbackend.c:3082-3106,
+ * 5416-5500): for every level but the coarsest, the bricks inside the
+ * level's distance shell whose centre lies in the widened view cone
+ * (half_tan * 1.15 + 1e-3) or near the eye, and whose desired level
+ * (r3d_host_lod_pick of the centre distance) is that level.  Each one adds
+ * its parent (priority 0) and itself (priority 1), both with its squared
+ * distance; bricks whose maximum in page (the full pyramid's page table,
+ * every brick present) is below max(gate * 255 + 0.5, 5) are left out, and
+ * a brick is listed once (its first entry).  slice_depth > 0 limits z to
+ * [slice_z0, slice_z0 + slice_depth).  mark (page_words bytes, zeroed by
+ * the caller) records listed bricks.  Returns the number of candidates
+ * written (at most cap), sorted by priority, then distance. */
+typedef struct r3d_stream_cand {
+  float d2;
+  uint32_t brick;    /* page-table word index */
+  uint32_t priority; /* 0: parent kept ahead of its children, 1: desired */
+} r3d_stream_cand;
+uint32_t r3d_host_stream_desired(const uint32_t *page, uint32_t page_words, const float eye[3],
+                                 const float fwd[3], float half_tan, float pixel_cone,
+                                 uint32_t slice_z0, uint32_t slice_depth, float gate,
+                                 uint8_t *mark, r3d_stream_cand *out, uint32_t cap);
+
 /* A view of the scripted "orbit" benchmark at phase ph in [0,1): yaw = 2 pi ph,
  * pitch = 0.5 sin(4 pi ph), distance 2 around target (src/main.c:3932-3946),
  * identity volume transform, viewport w x h.  Other fields: step_voxels,

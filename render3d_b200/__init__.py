@@ -119,6 +119,21 @@ class FrameStats(C.Structure):
                 ("cpu_submit_ns", C.c_uint64)]
 
 
+class StreamView(C.Structure):
+    _fields_ = [("eye", C.c_float * 3), ("fwd", C.c_float * 3), ("half_tan", C.c_float),
+                ("pixel_cone", C.c_float), ("slice_z0", C.c_uint32), ("slice_depth", C.c_uint32),
+                ("gate", C.c_float), ("budget", C.c_uint32)]
+
+
+class StreamStats(C.Structure):
+    _fields_ = [("desired", C.c_uint32), ("requested", C.c_uint32), ("uploaded", C.c_uint32),
+                ("evicted", C.c_uint32), ("resident", C.c_uint32)]
+
+
+class StreamCand(C.Structure):
+    _fields_ = [("d2", C.c_float), ("brick", C.c_uint32), ("priority", C.c_uint32)]
+
+
 def _load() -> C.CDLL:
     if not os.path.exists(LIB_PATH):
         raise ImportError(f"{LIB_PATH} is not built; run python render3d_b200/build.py")
@@ -142,6 +157,10 @@ def _load() -> C.CDLL:
         "r3d_cuda_cube_read": (I, [P, I, P, P]),
         "r3d_cuda_shard_build": (I, [P, U32, P, U32, P]),
         "r3d_cuda_bricks_overlay_load": (I, [P, U32, P]),
+        "r3d_cuda_stream_begin": (I, [P, C.POINTER(VolumeDesc), P, U32, U32]),
+        "r3d_cuda_stream_update": (I, [P, C.POINTER(StreamView), C.POINTER(StreamStats)]),
+        "r3d_cuda_stream_view_of": (None, [P, P, U32, C.POINTER(StreamView)]),
+        "r3d_host_stream_desired": (U32, [P, U32, P, P, F, F, U32, U32, F, P, P, U32]),
         "r3d_cuda_bricks_overlay_build": (I, [P, U32, C.POINTER(VolumeDesc), P]),
         "r3d_cuda_shard_mode": (U32, [P]),
         "r3d_cuda_shard_read": (I, [P, I, P, P, P]),
@@ -226,6 +245,21 @@ def _ptr(a) -> int:
 
 
 # ------------------------------------------------------------------ host
+
+def stream_desired(page: np.ndarray, eye, fwd, half_tan: float, pixel_cone: float,
+                   gate: float = 0.0, slice_z0: int = 0, slice_depth: int = 0) -> np.ndarray:
+    """The streamer's request set (r3d_host_stream_desired) as a structured
+    array of (d2, brick, priority), sorted."""
+    page = np.ascontiguousarray(page, np.uint32)
+    mark = np.zeros(page.size, np.uint8)
+    out = (StreamCand * page.size)()
+    e3 = (C.c_float * 3)(*eye)
+    f3 = (C.c_float * 3)(*fwd)
+    n = lib.r3d_host_stream_desired(_ptr(page), page.size, e3, f3, half_tan, pixel_cone,
+                                    slice_z0, slice_depth, gate, _ptr(mark), out, page.size)
+    a = np.ctypeslib.as_array(out)[:n]
+    return a.copy()
+
 
 def tf_preset(idx: int) -> np.ndarray:
     lut = np.zeros((256, 4), np.uint8)
@@ -401,6 +435,22 @@ class Context:
         out = np.empty((dims[2], dims[1], dims[0]), np.uint8)
         self._check(lib.r3d_cuda_cube_read(self.h, level, _ptr(out), dims))
         return out
+
+    def stream_begin(self, vol, nlev: int, nslots: int) -> None:
+        """Streaming LOD cache: the whole pyramid in pinned host memory,
+        nslots device slots filled by stream_update."""
+        nz, ny, nx = vol.shape
+        d = VolumeDesc(nx, ny, nz, 128, 1.0)
+        self._check(lib.r3d_cuda_stream_begin(self.h, C.byref(d), _ptr(vol), nlev, nslots))
+
+    def stream_update(self, p: "FrameParams", budget: int, ext=(1.0, 1.0, 1.0)) -> dict:
+        """One pump update for view p; returns its statistics."""
+        v = StreamView()
+        e = (C.c_float * 3)(*ext)
+        lib.r3d_cuda_stream_view_of(C.byref(p), e, budget, C.byref(v))
+        st = StreamStats()
+        self._check(lib.r3d_cuda_stream_update(self.h, C.byref(v), C.byref(st)))
+        return {k: getattr(st, k) for k, _ in StreamStats._fields_}
 
     def overlay_load(self, which: int, slots) -> None:
         """Overlay atlas `which` (0 ink, 1 3D ink, 2 labels, 3 registration)

@@ -271,6 +271,8 @@ void r3d_cuda_destroy(r3d_cuda_ctx *c) {
   cudaFree(c->img);
   cudaFree(c->aux_buf);
   cudaFree(c->total);
+  stream_reset(c);
+  if (c->page_ev) cudaEventDestroy(c->page_ev);
   cudaFree(c->diff_q);
   cudaFree(c->tape);
   cudaFree(c->diff_quad);
@@ -429,7 +431,8 @@ static int decode_header(r3d_cuda_ctx *c, const uint32_t *page, uint32_t words, 
 }
 
 // (Re)builds the block-maximum table of the context's slot pool.
-static int build_blockmax(r3d_cuda_ctx *c) {
+int build_blockmax(r3d_cuda_ctx *c) {
+  if (c->defer_tables) return R3D_OK;
   cudaFree(c->bmax);
   c->bmax = nullptr;
   size_t n = (size_t)(c->nslots ? c->nslots : 1u) * 4096u;
@@ -455,7 +458,7 @@ static int build_blockmax(r3d_cuda_ctx *c) {
   return R3D_OK;
 }
 
-static uint32_t atlas_bpa(uint32_t nslots) {
+uint32_t atlas_bpa(uint32_t nslots) {
   uint32_t a = 1;
   while ((uint64_t)a * a * a < nslots) a++;
   return a;
@@ -470,6 +473,7 @@ int r3d_cuda_bricks_build(r3d_cuda_ctx *c, const r3d_volume_desc *d, const uint8
   uint32_t nx = d->nx, ny = d->ny, nz = d->nz;
   if (max(nx, max(ny, nz)) > 65535u) return fail(c, R3D_E_INVALID, "bricks_build: too large");
   cudaSetDevice(c->device);
+  stream_reset(c);
   cudaStream_t st = c->stream;
   R3D_CUDA_TRY(c, cudaStreamSynchronize(st));
   // level extents: level 0 is the volume itself, level l >= 1 the zero-
@@ -642,6 +646,7 @@ int r3d_cuda_bricks_load(r3d_cuda_ctx *c, const uint32_t *page, uint32_t page_wo
                          const uint8_t *slots, uint32_t nslots) {
   if (!c || !page || (!slots && nslots)) return fail(c, R3D_E_INVALID, "bricks_load: bad args");
   if (nslots >= (1u << 24)) return fail(c, R3D_E_INVALID, "bricks_load: too many slots");
+  stream_reset(c);
   DevBricks b;
   int rc = decode_header(c, page, page_words, nslots, b);
   if (rc != R3D_OK) return rc;

@@ -328,3 +328,92 @@ int r3d_host_phantom(uint8_t *vox, uint32_t nx, uint32_t ny, uint32_t nz,
   free(mask);
   return 0;
 }
+
+/* ------------------------------------------------- streamer request set */
+
+static void stream_axis_bounds(float eye, float radius, float edge, uint32_t n, uint32_t *lo,
+                               uint32_t *hi) {  // vkbackend.c:3096-3106
+  int a = (int)ceilf((eye - radius) / edge - 0.5f);
+  int b = (int)floorf((eye + radius) / edge - 0.5f) + 1;
+  if (a < 0) a = 0;
+  if (b < 0) b = 0;
+  if (a > (int)n) a = (int)n;
+  if (b > (int)n) b = (int)n;
+  *lo = (uint32_t)a;
+  *hi = (uint32_t)b;
+}
+
+static int stream_cand_cmp(const void *a, const void *b) {  // vkbackend.c:3075-3080
+  const r3d_stream_cand *ca = a, *cb = b;
+  if (ca->priority != cb->priority) return ca->priority < cb->priority ? -1 : 1;
+  float d = ca->d2 - cb->d2;
+  return d < 0.0f ? -1 : (d > 0.0f ? 1 : (ca->brick < cb->brick ? -1 : ca->brick > cb->brick));
+}
+
+uint32_t r3d_host_stream_desired(const uint32_t *page, uint32_t page_words, const float eye[3],
+                                 const float fwd[3], float half_tan, float pixel_cone,
+                                 uint32_t slice_z0, uint32_t slice_depth, float gate,
+                                 uint8_t *mark, r3d_stream_cand *out, uint32_t cap) {
+  if (!page || page_words < R3D_BRICK_PAGE_HEADER || !mark || !out) return 0;
+  const uint32_t nlev = page[0];
+  if (nlev < 1u || nlev > 15u) return 0;
+  const float maxdim = (float)(page[1] > page[2] ? (page[1] > page[3] ? page[1] : page[3])
+                                                 : (page[2] > page[3] ? page[2] : page[3]));
+  const float tanw = half_tan * 1.15f + 1e-3f;
+  int g8 = (int)(gate * 255.0f + 0.5f);
+  if (g8 < 5) g8 = 5;  // decoded-air noise floor (vkbackend.c:2348)
+  const float lod_factor = fmaxf(pixel_cone * maxdim, 1e-6f);
+  uint32_t n = 0;
+  for (uint32_t li = 0; li + 1u < nlev; li++) {
+    const uint32_t off = page[4u + 4u * li], packed = page[5u + 4u * li],
+                   scale = page[6u + 4u * li];
+    const uint32_t bd[3] = {packed & 1023u, (packed >> 10) & 1023u, packed >> 20};
+    const uint32_t poff = page[4u + 4u * (li + 1u)], ppacked = page[5u + 4u * (li + 1u)];
+    const uint32_t pbd[2] = {ppacked & 1023u, (ppacked >> 10) & 1023u};
+    const float edge = (float)(128u * scale) / maxdim;
+    const float brad = 0.8660254f * edge;
+    const float outer = exp2f((float)li + 1.0f) / lod_factor + brad;
+    uint32_t x0, x1, y0, y1, z0, z1;
+    stream_axis_bounds(eye[0], outer, edge, bd[0], &x0, &x1);
+    stream_axis_bounds(eye[1], outer, edge, bd[1], &y0, &y1);
+    stream_axis_bounds(eye[2], outer, edge, bd[2], &z0, &z1);
+    if (slice_depth) {
+      uint64_t zlast = (uint64_t)slice_z0 + slice_depth;
+      if (zlast > page[3]) zlast = page[3];
+      const uint32_t zbrick = 128u * scale;
+      const uint32_t sz0 = slice_z0 / zbrick, sz1 = (uint32_t)((zlast + zbrick - 1u) / zbrick);
+      if (z0 < sz0) z0 = sz0;
+      if (z1 > sz1) z1 = sz1;
+    }
+    for (uint32_t bz = z0; bz < z1; bz++)
+      for (uint32_t by = y0; by < y1; by++)
+        for (uint32_t bx = x0; bx < x1; bx++) {
+          const float cx = ((float)bx + 0.5f) * edge - eye[0];
+          const float cy = ((float)by + 0.5f) * edge - eye[1];
+          const float cz = ((float)bz + 0.5f) * edge - eye[2];
+          const float d2 = cx * cx + cy * cy + cz * cz;
+          const float along = cx * fwd[0] + cy * fwd[1] + cz * fwd[2];
+          bool vis = d2 < (edge + brad) * (edge + brad);
+          if (!vis && along > 0.0f) {
+            const float perp2 = d2 - along * along;
+            const float rad = along * tanw + brad;
+            vis = perp2 < rad * rad;
+          }
+          if (!vis) continue;
+          if (r3d_host_lod_pick(sqrtf(d2), pixel_cone, maxdim, nlev) != li) continue;
+          const uint32_t cand[2] = {
+              poff + ((bz >> 1) * pbd[1] + (by >> 1)) * pbd[0] + (bx >> 1),
+              off + (bz * bd[1] + by) * bd[0] + bx};
+          for (uint32_t k = 0; k < 2u; k++) {
+            const uint32_t b = cand[k];
+            if (b >= page_words || mark[b]) continue;
+            const uint32_t e = page[b];
+            if (e == R3D_BRICK_ABSENT || (int)(e >> 24) < g8) continue;
+            mark[b] = 1;
+            if (n < cap) out[n++] = (r3d_stream_cand){d2, b, k};
+          }
+        }
+  }
+  qsort(out, n, sizeof *out, stream_cand_cmp);
+  return n;
+}

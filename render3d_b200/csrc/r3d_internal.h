@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <vector>
 
 #include "r3d_cuda.h"
 #include "r3d_march.cuh"
@@ -32,6 +33,19 @@ struct r3d_cuda_ctx {
   uint32_t shape[3] = {0, 0, 0};
   bool have_bricks = false;
   r3d::DevBricks br{};
+
+  // streaming LOD cache: every brick of the pyramid in pinned host memory
+  // (store, indexed by its slot in the full build; store_page is that
+  // build's page table), a pool of nslots device slots, the host shadow of
+  // the device page table and the LRU state
+  bool streaming = false;
+  bool defer_tables = false;  // a brick build whose pool is about to be replaced
+  uint8_t *store = nullptr;
+  std::vector<uint32_t> store_page, slot_brick, slot_use, brick_slot;
+  uint32_t *page_shadow = nullptr;
+  uint32_t *stream_jobs = nullptr;  // device: slots filled by one update
+  uint32_t stream_frame = 0;
+  cudaEvent_t page_ev = nullptr;
 
   // single-level brick atlas: 4 mip levels, then the world-indexed
   // occupancy grid, in one allocation; page table of bpa^3 entries
@@ -109,6 +123,14 @@ cudaError_t launch_view(const r3d_cuda_ctx *c, const r3d_frame_params &pc, uint8
                         cudaStream_t stream);
 
 }  // namespace r3d
+
+// (Re)allocates and fills the per-slot block-maximum and quad tables of the
+// context's slot pool (dropping its overlays); atlas bricks per axis of a
+// pool of nslots slots.
+int build_blockmax(r3d_cuda_ctx *c);
+// Drops the streaming state (host store, shadows, LRU).
+void stream_reset(r3d_cuda_ctx *c);
+uint32_t atlas_bpa(uint32_t nslots);
 
 // Validates one view and clips its rect to the image (1: render, 0: empty
 // rect, < 0: error code).
