@@ -140,6 +140,28 @@ void r3d_cuda_stream_view_of(const r3d_frame_params *p, const float ext[3], uint
 int r3d_cuda_stream_update(r3d_cuda_ctx *ctx, const r3d_stream_view *view,
                            r3d_stream_stats *stats);
 
+/* Tiled slab: render3d's slab mode for wide, thin windows (reference
+ * src/core/slab.h, src/vk/vkbackend.c:2128-2335, sampled by
+ * src/shaders/raycast.slang:423-455).  The volume (nx x ny x nz, x fastest,
+ * host or device) is copied to the device; a window of wz slices (4 <= wz
+ * <= nz) from z0 lives in a z ring of tiles of at most 2048 texels per axis,
+ * each with a 1-texel apron copied from its neighbours (clamped at the
+ * edges).  An overview pyramid at scales 4, 8, ... up to the scale that fits
+ * the whole plane in 2046-texel tiles (4x box of the slice, then 2x chains,
+ * truncating averages) serves far footprints.  Views set slab_grid and
+ * the other slab fields with r3d_cuda_slab_params (slab_depth may be
+ * lowered).  _window moves the window to z0 (clamped to nz - wz),
+ * refilling only the ring layers of slices that enter it, after the frames
+ * already queued on the context's stream. */
+int r3d_cuda_slab_build(r3d_cuda_ctx *ctx, const r3d_volume_desc *d, const uint8_t *voxels,
+                        uint32_t wz, uint32_t z0);
+int r3d_cuda_slab_window(r3d_cuda_ctx *ctx, uint32_t z0);
+void r3d_cuda_slab_params(const r3d_cuda_ctx *ctx, r3d_frame_params *p);
+/* Copy of tile `tile` of level `level` (0 = base grid, 1.. overview, scale
+ * 4 << (level - 1)): (px + 2) x (py + 2) x wz bytes; dims receives them. */
+int r3d_cuda_slab_read(r3d_cuda_ctx *ctx, uint32_t level, uint32_t tile, uint8_t *out,
+                       uint32_t dims[3]);
+
 /* Slot-parallel overlay atlases of the LOD brick cache (reference
  * src/render/render.h:51-101; sampled by src/shaders/raycast.slang:45-115,
  * 872-914,1000-1014,1032-1036): which = 0 ink (overlay_flags bit 0, tinted

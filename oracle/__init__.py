@@ -32,9 +32,16 @@ class Cube(C.Structure):
                 ("level", C.c_void_p * 16), ("occ", C.c_void_p), ("odim", C.c_uint32 * 3)]
 
 
+class Slab(C.Structure):
+    _fields_ = [("wz", C.c_uint32), ("nlev", C.c_uint32), ("ovs", C.c_uint32), ("nx", C.c_uint32),
+                ("ny", C.c_uint32), ("z0", C.c_uint32), ("lev", (C.c_uint32 * 4) * 8),
+                ("tiles", C.c_void_p * 8)]
+
+
 class Bricks(C.Structure):
     _fields_ = [("page", C.c_void_p), ("page_words", C.c_uint32), ("pool", C.c_void_p),
-                ("nslots", C.c_uint32), ("atlas", C.c_void_p), ("ovl", C.c_void_p * 4)]
+                ("nslots", C.c_uint32), ("atlas", C.c_void_p), ("ovl", C.c_void_p * 4),
+                ("slab", C.c_void_p)]
 
 
 class Opts(C.Structure):
@@ -65,6 +72,10 @@ def _load():
     lib.orc_occupancy.argtypes = [P, U32, U32, U32, P]
     lib.orc_build_lod_bricks.restype = C.c_int64
     lib.orc_build_lod_bricks.argtypes = [P, U32, U32, U32, U32, U32, P, U32, P, C.c_uint64]
+    lib.orc_slab_layout.restype = U32
+    lib.orc_slab_layout.argtypes = [U32, U32, P, P]
+    lib.orc_slab_fill.restype = None
+    lib.orc_slab_fill.argtypes = [P, U32, U32, U32, U32, U32, C.c_void_p * 8]
     lib.orc_build_lod_overlay.restype = C.c_int
     lib.orc_build_lod_overlay.argtypes = [P, U32, U32, U32, P, U32, C.c_int, P, U32]
     lib.orc_build_shard.restype = C.c_int
@@ -218,9 +229,37 @@ class ShardScene:
         return cls(page, atlas0, bpa, abpa)
 
 
+class SlabScene:
+    """The tiled slab of a (nz, ny, nx) volume for the window [z0, z0 + wz),
+    assembled the reference's way."""
+
+    def __init__(self, vol: np.ndarray, wz: int, z0: int):
+        vol = np.ascontiguousarray(vol, np.uint8)
+        nz, ny, nx = vol.shape
+        lev = ((C.c_uint32 * 4) * 8)()
+        ovs = C.c_uint32()
+        nl = lib.orc_slab_layout(nx, ny, lev, C.byref(ovs))
+        if not nl:
+            raise ValueError("slab layout")
+        self.s = Slab()
+        self.s.wz, self.s.nlev, self.s.ovs, self.s.nx, self.s.ny, self.s.z0 = wz, nl, ovs.value, nx, ny, z0
+        self.tiles = []
+        ptrs = (C.c_void_p * 8)()
+        for l in range(nl):
+            gx, gy, px, py = lev[l]
+            self.s.lev[l][:] = (gx, gy, px, py)
+            t = np.zeros((gx * gy, wz, py + 2, px + 2), np.uint8)
+            self.tiles.append(t)
+            ptrs[l] = t.ctypes.data
+            self.s.tiles[l] = t.ctypes.data
+        lib.orc_slab_fill(_p(vol), nx, ny, nz, wz, z0, ptrs)
+        self.b = Bricks()
+        self.b.slab = C.addressof(self.s)
+
+
 def _scene_args(scene):
     cube = C.byref(scene.c) if isinstance(scene, CubeScene) else None
-    br = C.byref(scene.b) if isinstance(scene, (BrickScene, ShardScene)) else None
+    br = C.byref(scene.b) if isinstance(scene, (BrickScene, ShardScene, SlabScene)) else None
     return cube, br
 
 

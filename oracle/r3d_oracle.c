@@ -292,6 +292,68 @@ static void lerp3(float c[3], float r, float g, float b, float t) {
   c[2] = lerpf_(c[2], b, t);
 }
 
+/* slab tile k of level L at normalized (u, v, w): linear, clamp to edge in
+ * x and y, REPEAT in w (vkbackend.c:2203-2211) */
+static float slab_tile(const orc_slab *sl, int L, uint32_t k, float u, float v, float w) {
+  uint32_t tw = sl->lev[L][2] + 2u, th = sl->lev[L][3] + 2u, wz = sl->wz;
+  const uint8_t *g = sl->tiles[L] + (size_t)k * tw * th * wz;
+  float tx = clampf_(fmaf(u, (float)tw, -0.5f), 0.0f, (float)(tw - 1u));
+  float ty = clampf_(fmaf(v, (float)th, -0.5f), 0.0f, (float)(th - 1u));
+  float tz = fmaf(w, (float)wz, -0.5f);
+  uint32_t x0 = (uint32_t)tx, y0 = (uint32_t)ty;
+  float fx = tx - (float)x0, fy = ty - (float)y0;
+  float zf = floorf(tz), fz = tz - zf;
+  int zi = (int)zf % (int)wz;
+  if (zi < 0) zi += (int)wz;
+  uint32_t z0 = (uint32_t)zi, z1 = z0 + 1u < wz ? z0 + 1u : 0u;
+  uint32_t x1 = x0 + 1u < tw ? x0 + 1u : tw - 1u, y1 = y0 + 1u < th ? y0 + 1u : th - 1u;
+  size_t sy = tw, sz = (size_t)tw * th;
+#define T(X, Y, Z) ((float)g[(size_t)(X) + (size_t)(Y) * sy + (size_t)(Z) * sz])
+  float c00 = lerpf_(T(x0, y0, z0), T(x1, y0, z0), fx);
+  float c10 = lerpf_(T(x0, y1, z0), T(x1, y1, z0), fx);
+  float c01 = lerpf_(T(x0, y0, z1), T(x1, y0, z1), fx);
+  float c11 = lerpf_(T(x0, y1, z1), T(x1, y1, z1), fx);
+#undef T
+  return lerpf_(lerpf_(c00, c10, fy), lerpf_(c01, c11, fy), fz) * INV255;
+}
+
+/* vol_sample of the tiled slab (raycast.slang:423-455) */
+static float slab_sample(const orc_slab *sl, v3f p, float lod) {
+  float nx = (float)sl->nx, ny = (float)sl->ny, px = (float)sl->lev[0][2],
+        py = (float)sl->lev[0][3];
+  float wx = p.x * nx, wy = p.y * nx;
+  float zc = ((float)sl->z0 + 0.5f) + p.z * nx;
+  float zq = zc / (float)sl->wz;
+  float w = zq - floorf(zq);
+  int lev = (int)floorf(lod) - 2;
+  if (lev >= 0) {
+    int nl = (int)(r3d_log2f((float)sl->ovs) + 0.5f) - 1;
+    if (lev > nl - 1) lev = nl - 1;
+    float sc = (float)(4 << lev);
+    float vnx = ceilf(nx / sc), vny = ceilf(ny / sc);
+    float gxl = ceilf(vnx / 2046.0f), gyl = ceilf(vny / 2046.0f);
+    float pxl = ceilf(vnx / gxl), pyl = ceilf(vny / gyl);
+    float wxl = wx / sc, wyl = wy / sc;
+    float oix = fminf(floorf(fmaxf(wxl, 0.0f) / pxl), gxl - 1.0f);
+    float oiy = fminf(floorf(fmaxf(wyl, 0.0f) / pyl), gyl - 1.0f);
+    float ou = ((wxl - oix * pxl) + 1.0f) / (pxl + 2.0f);
+    float ov = ((wyl - oiy * pyl) + 1.0f) / (pyl + 2.0f);
+    return slab_tile(sl, lev + 1, (uint32_t)(oiy * gxl + oix), ou, ov, w);
+  }
+  uint32_t gx = sl->lev[0][0], gy = sl->lev[0][1];
+  uint32_t ix = (uint32_t)(fmaxf(wx, 0.0f) / px), iy = (uint32_t)(fmaxf(wy, 0.0f) / py);
+  if (ix > gx - 1u) ix = gx - 1u;
+  if (iy > gy - 1u) iy = gy - 1u;
+  float u = ((wx - (float)ix * px) + 1.0f) / (px + 2.0f);
+  float v = ((wy - (float)iy * py) + 1.0f) / (py + 2.0f);
+  return slab_tile(sl, 0, iy * gx + ix, u, v, w);
+}
+
+/* a gradient tap: the slab's vol_sample or a cube-like texture */
+static float tap_sample(const scene *s, int slab, const orc_cube *tex, v3f p, float lod) {
+  return slab ? slab_sample(s->br->slab, p, lod) : cube_sample(tex, p, lod);
+}
+
 /* ------------------------------------------------------------ the march */
 
 typedef struct ray_out {
@@ -314,7 +376,8 @@ static void march(const r3d_frame_params *pc, const scene *s, const uint8_t lut[
   int ortho = (pc->view_flags & R3D_VIEW_ORTHO) != 0u;
   int bricks = pc->brick_mode != 0u;
   int lodb = bricks && (pc->brick_mode & R3D_BRICK_LOD_FLAG) != 0u;
-  int shard = bricks && !lodb;
+  int slab = pc->slab_grid != 0u;
+  int shard = bricks && !lodb && !slab;
   uint32_t sh_bpa = pc->brick_mode & 0xffu, sh_abpa = (pc->brick_mode >> 8) & 0xffu;
   int sh_ident = (pc->brick_mode & R3D_BRICK_IDENTITY_FLAG) != 0u;
   const orc_cube *atlas = shard ? s->br->atlas : NULL;
@@ -357,6 +420,13 @@ static void march(const r3d_frame_params *pc, const scene *s, const uint8_t lut[
     vox_inv = md;
     max_lod = (float)(nlev - 1u);
     ext = mk3(bs[0] / md, bs[1] / md, bs[2] / md);
+  } else if (slab) { /* :672-677, :305-314 */
+    const orc_slab *sl = s->br->slab;
+    voxel = 1.0f / pc->slab_nx;
+    vox_inv = pc->slab_nx;
+    max_lod = r3d_log2f((float)((pc->slab_grid >> 16) & 0xffu)) + 2.0f;
+    ext = mk3(1.0f, pc->slab_ny / pc->slab_nx, (float)pc->slab_depth / pc->slab_nx);
+    (void)sl;
   } else if (shard) { /* :659-661 */
     voxel = 1.0f / (float)(sh_bpa * 128u);
     vox_inv = (float)(sh_bpa * 128u);
@@ -441,6 +511,7 @@ static void march(const r3d_frame_params *pc, const scene *s, const uint8_t lut[
   int shaded = pc->mode == R3D_MODE_FULL;
   uint32_t ray_budget = lodb ? (shaded ? 192u : 256u) : MAX_STEPS;
   float span_step = fmaxf((tf_ - tn) / ((float)ray_budget * dt), 1.0f);
+  float slab_cap = fmaxf(1.0f, (tf_ - tn) / (4.0f * dt)); /* :778-779 */
   float bs = OCC_BLOCK * voxel;
   float occ_gate = fmaxf(pc->skip_gate, 0.5f / 255.0f);
   float opac_k = pc->density * pc->step_voxels;
@@ -472,12 +543,15 @@ static void march(const r3d_frame_params *pc, const scene *s, const uint8_t lut[
     float foot = ortho ? cone : t * cone;
     float lod = clampf_(r3d_log2f(fmaxf(foot * vox_inv, 1.0f)) + pc->lod_bias, 0.0f, max_lod);
     float lod_step = fmaxf(r3d_exp2f(lod), span_step);
+    if (slab) lod_step = fminf(lod_step, slab_cap);
     v3f p = mk3(fmaf(t, dir.x, ro.x), fmaf(t, dir.y, ro.y), fmaf(t, dir.z, ro.z));
 
     float v;
     if (lodb) {
       b = lod_locate_cached(s, p, lod, &lc);
       v = b.ok ? brick_fetch(s, b.slot, b.bl) : 0.0f;
+    } else if (slab) {
+      v = slab_sample(s->br->slab, p, lod);
     } else if (shard && sh_ident) { /* :800-805 */
       v = cube_sample(atlas, p, lod);
     } else if (shard) { /* :806-822 */
@@ -534,7 +608,7 @@ static void march(const r3d_frame_params *pc, const scene *s, const uint8_t lut[
           void_blk = 1;
         }
       }
-    } else if (v < occ_gate && occ_sample(s->cube->occ, s->cube->odim, p) < occ_gate) {
+    } else if (!slab && v < occ_gate && occ_sample(s->cube->occ, s->cube->odim, p) < occ_gate) {
       void_blk = 1;
     }
     if (void_blk) {
@@ -607,10 +681,10 @@ static void march(const r3d_frame_params *pc, const scene *s, const uint8_t lut[
             } else {
               const orc_cube *tex = shard ? atlas : s->cube;
               float ee = (voxel * lod_step) * ir3;
-              q0 = cube_sample(tex, mk3(p.x + ee, p.y - ee, p.z - ee), lod);
-              q1 = cube_sample(tex, mk3(p.x - ee, p.y - ee, p.z + ee), lod);
-              q2 = cube_sample(tex, mk3(p.x - ee, p.y + ee, p.z - ee), lod);
-              q3 = cube_sample(tex, mk3(p.x + ee, p.y + ee, p.z + ee), lod);
+              q0 = tap_sample(s, slab, tex, mk3(p.x + ee, p.y - ee, p.z - ee), lod);
+              q1 = tap_sample(s, slab, tex, mk3(p.x - ee, p.y - ee, p.z + ee), lod);
+              q2 = tap_sample(s, slab, tex, mk3(p.x - ee, p.y + ee, p.z - ee), lod);
+              q3 = tap_sample(s, slab, tex, mk3(p.x + ee, p.y + ee, p.z + ee), lod);
             }
             g[0] = (((q0 - q1) - q2) + q3) * renorm;
             g[1] = (((-q0 - q1) + q2) + q3) * renorm;
@@ -637,12 +711,12 @@ static void march(const r3d_frame_params *pc, const scene *s, const uint8_t lut[
             } else {
               const orc_cube *tex = shard ? atlas : s->cube;
               float e = voxel * lod_step;
-              g[0] = cube_sample(tex, mk3(p.x + e, p.y, p.z), lod) -
-                     cube_sample(tex, mk3(p.x - e, p.y, p.z), lod);
-              g[1] = cube_sample(tex, mk3(p.x, p.y + e, p.z), lod) -
-                     cube_sample(tex, mk3(p.x, p.y - e, p.z), lod);
-              g[2] = cube_sample(tex, mk3(p.x, p.y, p.z + e), lod) -
-                     cube_sample(tex, mk3(p.x, p.y, p.z - e), lod);
+              g[0] = tap_sample(s, slab, tex, mk3(p.x + e, p.y, p.z), lod) -
+                     tap_sample(s, slab, tex, mk3(p.x - e, p.y, p.z), lod);
+              g[1] = tap_sample(s, slab, tex, mk3(p.x, p.y + e, p.z), lod) -
+                     tap_sample(s, slab, tex, mk3(p.x, p.y - e, p.z), lod);
+              g[2] = tap_sample(s, slab, tex, mk3(p.x, p.y, p.z + e), lod) -
+                     tap_sample(s, slab, tex, mk3(p.x, p.y, p.z - e), lod);
             }
           }
           v3f gv = mk3(g[0], g[1], g[2]);
@@ -725,7 +799,16 @@ static int check_view(const r3d_frame_params *p, const orc_cube *cube, const orc
        ((p->overlay_flags & 4u) && !br->ovl[1]) || ((p->overlay_flags & 8u) && !br->ovl[2]) ||
        ((p->overlay_flags & 16u) && !br->ovl[3])))
     return -1;
-  if (p->slab_grid || p->clip_valid ||
+  if (p->slab_grid) { /* slab views need the slab and must describe its window */
+    const orc_slab *sl = br ? br->slab : NULL;
+    if (!sl || p->brick_mode || p->slab_wz != sl->wz || p->slab_z0 != (float)sl->z0 ||
+        p->slab_nx != (float)sl->nx || p->slab_ny != (float)sl->ny ||
+        p->slab_px != (float)sl->lev[0][2] || p->slab_py != (float)sl->lev[0][3] ||
+        p->slab_grid != (sl->lev[0][0] | (sl->lev[0][1] << 8) | (sl->ovs << 16)) ||
+        p->slab_depth < 1u || p->slab_depth > sl->wz - 1u)
+      return -1;
+  }
+  if (p->clip_valid ||
       (p->view_flags & (R3D_VIEW_SURF | R3D_VIEW_STRETCH)) || p->mode >= R3D_MODE_COUNT)
     return -1;
   if (p->brick_mode & R3D_BRICK_LOD_FLAG) {
@@ -740,7 +823,7 @@ static int check_view(const r3d_frame_params *p, const orc_cube *cube, const orc
       return -1;
     for (int k = 0; k < 3; k++)
       if (a->dim[0][k] != abpa * 128u || a->odim[k] != bpa * 16u) return -1;
-  } else if (!cube || !cube->nlevels || !cube->occ) {
+  } else if (!p->slab_grid && (!cube || !cube->nlevels || !cube->occ)) {
     return -1;
   }
   return 0;
@@ -890,6 +973,90 @@ void orc_occupancy(const uint8_t *vox, uint32_t nx, uint32_t ny, uint32_t nz, ui
 }
 
 static uint32_t ceil_div(uint32_t a, uint32_t b) { return (a + b - 1u) / b; }
+
+static int slab_layout1(uint32_t nx, uint32_t ny, uint32_t out[4]) { /* slab.h:42-62 */
+  uint32_t maxp = 2046u;
+  out[0] = (nx + maxp - 1u) / maxp;
+  out[1] = (ny + maxp - 1u) / maxp;
+  if (out[0] > 22u || out[1] > 22u) return -1;
+  out[2] = (nx + out[0] - 1u) / out[0];
+  out[3] = (ny + out[1] - 1u) / out[1];
+  return 0;
+}
+
+uint32_t orc_slab_layout(uint32_t nx, uint32_t ny, uint32_t lev[8][4], uint32_t *ovs) {
+  if (slab_layout1(nx, ny, lev[0]) != 0) return 0;
+  uint32_t o = 4u;
+  while ((nx + o - 1u) / o > 2046u || (ny + o - 1u) / o > 2046u) o <<= 1;
+  uint32_t nov = 1u;
+  for (uint32_t s = 4u; s < o; s <<= 1) nov++;
+  if (nov + 1u > 8u) return 0;
+  for (uint32_t l = 1; l <= nov; l++) {
+    uint32_t s = 4u << (l - 1u);
+    slab_layout1((nx + s - 1u) / s, (ny + s - 1u) / s, lev[l]);
+  }
+  if (ovs) *ovs = o;
+  return nov + 1u;
+}
+
+/* vkbackend.c:2128-2144: truncating n x n box average, clipped at the edges */
+static void slab_down(const uint8_t *src, uint32_t nx, uint32_t ny, uint32_t n, uint8_t *dst) {
+  uint32_t ox = (nx + n - 1u) / n, oy = (ny + n - 1u) / n;
+  for (uint32_t y = 0; y < oy; y++)
+    for (uint32_t x = 0; x < ox; x++) {
+      uint32_t x0 = x * n, x1 = x0 + n > nx ? nx : x0 + n;
+      uint32_t y0 = y * n, y1 = y0 + n > ny ? ny : y0 + n;
+      uint32_t sum = 0;
+      for (uint32_t yy = y0; yy < y1; yy++)
+        for (uint32_t xx = x0; xx < x1; xx++) sum += src[(size_t)yy * nx + xx];
+      dst[(size_t)y * ox + x] = (uint8_t)(sum / ((y1 - y0) * (x1 - x0)));
+    }
+}
+
+/* tile slices of one level from a plane into ring `layer` (vkbackend.c:2148-2164) */
+static void slab_tiles(const uint8_t *plane, uint32_t nx, uint32_t ny, const uint32_t L[4],
+                       uint32_t wz, uint32_t layer, uint8_t *tiles) {
+  uint32_t tw = L[2] + 2u, th = L[3] + 2u;
+  size_t tb = (size_t)tw * th * wz;
+  for (uint32_t j = 0; j < L[1]; j++)
+    for (uint32_t i = 0; i < L[0]; i++)
+      for (uint32_t ty = 0; ty < th; ty++)
+        for (uint32_t tx = 0; tx < tw; tx++) {
+          int64_t cx = (int64_t)i * L[2] - 1 + tx, cy = (int64_t)j * L[3] - 1 + ty;
+          cx = cx < 0 ? 0 : (cx >= (int64_t)nx ? (int64_t)nx - 1 : cx);
+          cy = cy < 0 ? 0 : (cy >= (int64_t)ny ? (int64_t)ny - 1 : cy);
+          tiles[(size_t)(j * L[0] + i) * tb + (size_t)layer * tw * th + (size_t)ty * tw + tx] =
+              plane[(size_t)cy * nx + (size_t)cx];
+        }
+}
+
+void orc_slab_fill(const uint8_t *vox, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t wz,
+                   uint32_t z0, uint8_t *const tiles[8]) {
+  uint32_t lev[8][4], ovs = 0;
+  uint32_t nl = orc_slab_layout(nx, ny, lev, &ovs);
+  if (!nl || z0 + wz > nz) return;
+  uint8_t *a = malloc((size_t)nx * ny), *b = malloc((size_t)nx * ny);
+  if (!a || !b) goto out;
+  for (uint32_t s = z0; s < z0 + wz; s++) {
+    const uint8_t *slice = vox + (size_t)s * nx * ny;
+    uint32_t layer = s % wz;
+    slab_tiles(slice, nx, ny, lev[0], wz, layer, tiles[0]);
+    const uint8_t *prev = slice;
+    uint32_t pnx = nx, pny = ny;
+    for (uint32_t l = 1; l < nl; l++) {
+      uint8_t *dst = (l & 1u) ? a : b;
+      uint32_t f = l == 1u ? 4u : 2u;
+      slab_down(prev, pnx, pny, f, dst);
+      pnx = (pnx + f - 1u) / f;
+      pny = (pny + f - 1u) / f;
+      slab_tiles(dst, pnx, pny, lev[l], wz, layer, tiles[l]);
+      prev = dst;
+    }
+  }
+out:
+  free(a);
+  free(b);
+}
 
 int orc_build_lod_overlay(const uint8_t *vox, uint32_t nx, uint32_t ny, uint32_t nz,
                           const uint32_t *page, uint32_t page_words, int labels, uint8_t *pool,

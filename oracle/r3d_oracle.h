@@ -37,6 +37,16 @@ typedef struct orc_cube {
   uint32_t odim[3];
 } orc_cube;
 
+/* Tiled slab (src/core/slab.h, raycast.slang:423-455): per level (0 base,
+ * 1.. overview at scale 4 << (level - 1)) gx * gy tiles of (px + 2) x
+ * (py + 2) x wz texels, tile k at tiles[level] + k * tile bytes; ring
+ * layer s % wz holds world slice s.  z0 is the window start. */
+typedef struct orc_slab {
+  uint32_t wz, nlev, ovs, nx, ny, z0;
+  uint32_t lev[8][4]; /* gx, gy, px, py */
+  const uint8_t *tiles[8];
+} orc_slab;
+
 /* Brick cache.  LOD mode (brick_mode with the LOD flag): the page table in
  * render3d's word format and a pool of 128^3 slots (slot s at
  * pool + s * 128^3, x fastest).  Single-level mode (no LOD flag,
@@ -53,6 +63,8 @@ typedef struct orc_bricks {
    * 3D ink, labels, registration; NULL when absent), sampled per
    * src/shaders/raycast.slang:45-115,872-914,1000-1014,1032-1036 */
   const uint8_t *ovl[4];
+  /* slab views (slab_grid != 0) sample this instead */
+  const orc_slab *slab;
 } orc_bricks;
 
 typedef struct orc_opts {
@@ -135,6 +147,17 @@ uint32_t orc_lod_page_words(uint32_t nx, uint32_t ny, uint32_t nz, uint32_t nlev
 int orc_build_lod_overlay(const uint8_t *vox, uint32_t nx, uint32_t ny, uint32_t nz,
                           const uint32_t *page, uint32_t page_words, int labels, uint8_t *pool,
                           uint32_t nslots);
+
+/* Slab layout of an nx x ny plane with ring depth wz (slab.h:42-62,
+ * 122-135): per level gx, gy, px, py; returns the level count (base +
+ * overview) and the overview scale, or 0 when the plane needs more than
+ * 22 tiles per axis. */
+uint32_t orc_slab_layout(uint32_t nx, uint32_t ny, uint32_t lev[8][4], uint32_t *ovs);
+/* Tiles of every level for the window [z0, z0 + wz) of a volume, as the
+ * reference assembles them (vkbackend.c:2128-2164,2280-2325); tiles[l]
+ * must hold gx * gy * (px + 2) * (py + 2) * wz bytes of level l. */
+void orc_slab_fill(const uint8_t *vox, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t wz,
+                   uint32_t z0, uint8_t *const tiles[8]);
 
 /* Single-level brick atlas from a cubic volume of edge bpa * 128: atlas
  * level 0 ((abpa * 128)^3, slot s at (s % abpa, s / abpa % abpa,

@@ -157,6 +157,10 @@ def _load() -> C.CDLL:
         "r3d_cuda_cube_read": (I, [P, I, P, P]),
         "r3d_cuda_shard_build": (I, [P, U32, P, U32, P]),
         "r3d_cuda_bricks_overlay_load": (I, [P, U32, P]),
+        "r3d_cuda_slab_build": (I, [P, C.POINTER(VolumeDesc), P, U32, U32]),
+        "r3d_cuda_slab_window": (I, [P, U32]),
+        "r3d_cuda_slab_params": (None, [P, P]),
+        "r3d_cuda_slab_read": (I, [P, U32, U32, P, P]),
         "r3d_cuda_stream_begin": (I, [P, C.POINTER(VolumeDesc), P, U32, U32]),
         "r3d_cuda_stream_update": (I, [P, C.POINTER(StreamView), C.POINTER(StreamStats)]),
         "r3d_cuda_stream_view_of": (None, [P, P, U32, C.POINTER(StreamView)]),
@@ -451,6 +455,25 @@ class Context:
         st = StreamStats()
         self._check(lib.r3d_cuda_stream_update(self.h, C.byref(v), C.byref(st)))
         return {k: getattr(st, k) for k, _ in StreamStats._fields_}
+
+    def slab_build(self, vol, wz: int, z0: int = 0) -> None:
+        """Tiled slab over a (nz, ny, nx) volume: a ring of wz slices from z0."""
+        nz, ny, nx = vol.shape
+        d = VolumeDesc(nx, ny, nz, 128, 1.0)
+        self._check(lib.r3d_cuda_slab_build(self.h, C.byref(d), _ptr(vol), wz, z0))
+
+    def slab_window(self, z0: int) -> None:
+        self._check(lib.r3d_cuda_slab_window(self.h, z0))
+
+    def slab_params(self, p: "FrameParams") -> None:
+        lib.r3d_cuda_slab_params(self.h, C.byref(p))
+
+    def slab_read(self, level: int, tile: int) -> np.ndarray:
+        dims = (C.c_uint32 * 3)()
+        self._check(lib.r3d_cuda_slab_read(self.h, level, tile, None, dims))
+        out = np.empty((dims[2], dims[1], dims[0]), np.uint8)
+        self._check(lib.r3d_cuda_slab_read(self.h, level, tile, _ptr(out), dims))
+        return out
 
     def overlay_load(self, which: int, slots) -> None:
         """Overlay atlas `which` (0 ink, 1 3D ink, 2 labels, 3 registration)

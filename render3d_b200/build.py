@@ -42,7 +42,7 @@ C_FLAGS = ["-O2", "-std=c2x", "-D_GNU_SOURCE", "-fPIC", "-ffp-contract=off", "-W
            "-Wextra", "-I" + INC, "-I" + os.path.join(CUDA_HOME, "include")]
 
 CU_SOURCES = ["r3d_ctx.cu", "r3d_fwd.cu", "r3d_persist.cu", "r3d_noalloc.cu", "r3d_diff.cu", "r3d_batch.cu",
-              "r3d_phantom.cu", "r3d_diag.cu", "r3d_shard.cu", "r3d_overlay.cu", "r3d_stream.cu"]
+              "r3d_phantom.cu", "r3d_diag.cu", "r3d_shard.cu", "r3d_overlay.cu", "r3d_stream.cu", "r3d_slab.cu"]
 C_SOURCES = ["r3d_render.c", "r3d_host.c"]
 CLI_SOURCES = ["r3d_headless.c"]
 

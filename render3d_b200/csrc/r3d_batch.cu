@@ -66,7 +66,7 @@ extern "C" int r3d_cuda_batch_create(r3d_cuda_ctx *c, const r3d_cuda_request *re
   // group by (path, mode), keep request order inside a group
   uint32_t order[kMaxBatchViews], gcount[kMaxBatchViews], group_of[kMaxBatchViews];
   for (uint32_t i = 0; i < n; i++) {
-    uint32_t key = (uint32_t)path_of(b->pcs[i].brick_mode) * 8u | b->pcs[i].mode, g = 0;
+    uint32_t key = (uint32_t)path_of_view(b->pcs[i]) * 8u | b->pcs[i].mode, g = 0;
     while (g < b->ngroups && b->gkey[g] != key) g++;
     if (g == b->ngroups) {
       b->gkey[b->ngroups] = key;

@@ -201,6 +201,7 @@ r3d::DevScene r3d_cuda_ctx::scene() const {
   s.cube = cube;
   s.br = br;
   s.sh = sh;
+  s.sl = sl;
   s.status = status;
   s.alpha_cutoff = alpha_cutoff;
   s.tf_zero_t = tf_zero_t;
@@ -272,6 +273,7 @@ void r3d_cuda_destroy(r3d_cuda_ctx *c) {
   cudaFree(c->aux_buf);
   cudaFree(c->total);
   stream_reset(c);
+  slab_reset(c);
   if (c->page_ev) cudaEventDestroy(c->page_ev);
   cudaFree(c->diff_q);
   cudaFree(c->tape);
@@ -744,8 +746,24 @@ int prepare_view(r3d_cuda_ctx *c, const r3d_frame_params &in, uint32_t out_w,
                         uint32_t out_h, r3d_frame_params &pc) {
   pc = in;
   if (in.mode >= R3D_MODE_COUNT) return fail(c, R3D_E_INVALID, "view: mode %u", in.mode);
-  if (in.slab_grid || in.clip_valid)
-    return fail(c, R3D_E_UNSUPPORTED, "view: slab / clipmap sampling is not implemented");
+  if (in.clip_valid)
+    return fail(c, R3D_E_UNSUPPORTED, "view: clipmap sampling is not implemented");
+  if (in.slab_grid) {  // tiled slab: the view must describe the loaded window
+    if (!c->have_slab) return fail(c, R3D_E_STATE, "view: no slab loaded");
+    r3d_frame_params ref;
+    memset(&ref, 0, sizeof ref);
+    r3d_cuda_slab_params(c, &ref);
+    if (in.slab_grid != ref.slab_grid || in.slab_wz != ref.slab_wz ||
+        in.slab_z0 != ref.slab_z0 || in.slab_nx != ref.slab_nx || in.slab_ny != ref.slab_ny ||
+        in.slab_px != ref.slab_px || in.slab_py != ref.slab_py || in.brick_mode)
+      return fail(c, R3D_E_INVALID, "view: slab parameters do not match the loaded window "
+                                    "(r3d_cuda_slab_params)");
+    if (in.slab_depth < 1u || in.slab_depth > in.slab_wz - 1u)
+      return fail(c, R3D_E_INVALID, "view: slab_depth %u not in [1, %u]", in.slab_depth,
+                  in.slab_wz - 1u);
+    if (in.overlay_flags & kOvlAtlases)
+      return fail(c, R3D_E_UNSUPPORTED, "view: overlay atlases need the LOD brick cache");
+  }
   if (in.view_flags & (R3D_VIEW_SURF | R3D_VIEW_STRETCH))
     return fail(c, R3D_E_UNSUPPORTED, "view: flattened-surface views are not implemented");
   if (in.overlay_flags & kOvlAtlases) {
@@ -766,7 +784,7 @@ int prepare_view(r3d_cuda_ctx *c, const r3d_frame_params &in, uint32_t out_w,
     if (in.brick_mode != r3d_cuda_shard_mode(c))
       return fail(c, R3D_E_INVALID, "view: brick_mode 0x%x does not match the atlas (0x%x)",
                   in.brick_mode, r3d_cuda_shard_mode(c));
-  } else if (!c->have_cube) {
+  } else if (!in.slab_grid && !c->have_cube) {
     return fail(c, R3D_E_STATE, "view: no volume uploaded");
   }
   uint32_t ox = in.view_org & 0xffffu, oy = (in.view_org >> 16) & 0xffffu;
@@ -804,7 +822,7 @@ static int launch_views_persistent(r3d_cuda_ctx *c, const r3d_frame_params *pcs,
   uint32_t n = 0;
   for (uint32_t v = 0; v < nviews; v++) {
     if (!render[v]) continue;
-    uint32_t key = (uint32_t)path_of(pcs[v].brick_mode) * 8u | pcs[v].mode;
+    uint32_t key = (uint32_t)path_of_view(pcs[v]) * 8u | pcs[v].mode;
     uint32_t g = 0;
     while (g < ngroups && gkey[g] != key) g++;
     if (g == ngroups) {

@@ -198,7 +198,10 @@ cudaError_t launch_view(const r3d_cuda_ctx *c, const r3d_frame_params &pc, uint8
   DevScene s = c->scene();
   bool fast = c->quality == R3D_QUALITY_FAST;
   const uint32_t shade = c->sched.shade_group;
-  switch (path_of(pc.brick_mode)) {
+  switch (path_of_view(pc)) {
+    case PATH_SLAB:
+      return launch_p<PATH_SLAB>(pc, s, fast, c->lut, img, out_w, steps, mip_index, total,
+                                 counters, shade, stream);
     case PATH_LOD_BRICKS:
       return launch_p<PATH_LOD_BRICKS>(pc, s, fast, c->lut, img, out_w, steps, mip_index, total,
                                        counters, shade, stream);

@@ -47,6 +47,16 @@ struct r3d_cuda_ctx {
   uint32_t stream_frame = 0;
   cudaEvent_t page_ev = nullptr;
 
+  // tiled slab: tiles of every level in one buffer, the source volume and
+  // per-level overview planes for 16 slices (fill scratch)
+  uint8_t *slab_buf = nullptr, *slab_src = nullptr, *slab_planes = nullptr;
+  uint32_t slab_dims[3] = {0, 0, 0};
+  uint32_t slab_ovn[r3d::kSlabLevels][2] = {};
+  size_t slab_plane_off[r3d::kSlabLevels] = {};
+  uint32_t slab_win = 0;
+  bool have_slab = false;
+  r3d::DevSlab sl{};
+
   // single-level brick atlas: 4 mip levels, then the world-indexed
   // occupancy grid, in one allocation; page table of bpa^3 entries
   uint8_t *shard_buf = nullptr;
@@ -130,6 +140,8 @@ cudaError_t launch_view(const r3d_cuda_ctx *c, const r3d_frame_params &pc, uint8
 int build_blockmax(r3d_cuda_ctx *c);
 // Drops the streaming state (host store, shadows, LRU).
 void stream_reset(r3d_cuda_ctx *c);
+// Frees the tiled slab.
+void slab_reset(r3d_cuda_ctx *c);
 uint32_t atlas_bpa(uint32_t nslots);
 
 // Validates one view and clips its rect to the image (1: render, 0: empty

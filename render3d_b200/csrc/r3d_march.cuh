@@ -23,12 +23,16 @@ constexpr int kMaxLevels = 16;
 constexpr uint32_t kMaxSteps = 4096u;  // raycast.slang:123
 constexpr float kInv255 = 1.0f / 255.0f;
 
-enum Path { PATH_CUBE = 0, PATH_LOD_BRICKS = 1, PATH_SHARD = 2 };
+enum Path { PATH_CUBE = 0, PATH_LOD_BRICKS = 1, PATH_SHARD = 2, PATH_SLAB = 3 };
 
-// Sampling path of a view from its brick_mode word (raycast.slang:157-160)
+// Sampling path of a view: the tiled slab when slab_grid is set, else by
+// its brick_mode word (raycast.slang:134-140,157-160)
 __host__ __device__ inline int path_of(uint32_t brick_mode) {
   return brick_mode == 0u ? PATH_CUBE
                           : (brick_mode & R3D_BRICK_LOD_FLAG) ? PATH_LOD_BRICKS : PATH_SHARD;
+}
+__host__ __device__ inline int path_of_view(const r3d_frame_params &pc) {
+  return pc.slab_grid ? PATH_SLAB : path_of(pc.brick_mode);
 }
 
 struct DevCube {
@@ -82,10 +86,31 @@ struct DevShard {
   uint32_t identity;  // every brick in its own slot: sample the atlas directly
 };
 
+// Tiled slab (raycast.slang:423-455, src/core/slab.h): a wide, thin window
+// of a volume as a grid of tiles of (px + 2) x (py + 2) x wz texels -- the
+// payload plus a 1-texel apron copied from the neighbours (clamped at the
+// volume's edges) -- whose z is a ring: world slice s in layer s % wz.
+// Level 0 is the base grid, levels 1.. the overview pyramid at scales
+// 4 << (level - 1); tile (i, j) of a level starts at off + (j * gx + i) *
+// (px + 2) * (py + 2) * wz bytes of the pool.
+struct DevSlabLevel {
+  uint32_t gx, gy, px, py;
+  size_t off;
+};
+constexpr int kSlabLevels = 8;
+struct DevSlab {
+  const uint8_t *pool;
+  uint32_t wz, nlev;  // ring depth; levels (base + overview)
+  uint32_t ovs;       // overview downscale of the coarsest level
+  float nx, ny, px, py, z0;  // the frame parameters slab_nx/ny/px/py/z0 of the window
+  DevSlabLevel lev[kSlabLevels];
+};
+
 struct DevScene {
   DevCube cube;
   DevBricks br;
   DevShard sh;
+  DevSlab sl;
   uint32_t *status;
   float alpha_cutoff;
   float tf_zero_t;  // TF coordinates below this have alpha exactly 0
@@ -408,6 +433,65 @@ __device__ __forceinline__ float shard_fetch(const DevShard &h, float3 org, floa
   return cube_sample(h.atlas, u, lod);
 }
 
+// A slab tile sampled at normalized (u, v, w) like the slab sampler
+// (src/vk/vkbackend.c:2203-2211): linear, clamp to edge in x and y (the
+// apron makes tiles seamless), REPEAT in w so the z ring wraps.
+__device__ __forceinline__ float slab_tile(const DevSlab &sl, int L, uint32_t k, float u, float v,
+                                           float w) {
+  const DevSlabLevel &lv = sl.lev[L];
+  const uint32_t tw = lv.px + 2u, th = lv.py + 2u, wz = sl.wz;
+  const uint8_t *g = sl.pool + lv.off + (size_t)k * tw * th * wz;
+  const float tx = clamp_(fmaf(u, (float)tw, -0.5f), 0.0f, (float)(tw - 1u));
+  const float ty = clamp_(fmaf(v, (float)th, -0.5f), 0.0f, (float)(th - 1u));
+  const float tz = fmaf(w, (float)wz, -0.5f);
+  const uint32_t x0 = (uint32_t)tx, y0 = (uint32_t)ty;
+  const float fx = tx - (float)x0, fy = ty - (float)y0;
+  const float zf = floorf(tz), fz = tz - zf;
+  int zi = (int)zf % (int)wz;
+  if (zi < 0) zi += (int)wz;
+  const uint32_t z0 = (uint32_t)zi, z1 = z0 + 1u < wz ? z0 + 1u : 0u;
+  const uint32_t x1 = min(x0 + 1u, tw - 1u), y1 = min(y0 + 1u, th - 1u);
+  const size_t sy = tw, sz = (size_t)tw * th;
+  const uint8_t *r00 = g + y0 * sy + z0 * sz, *r10 = g + y1 * sy + z0 * sz;
+  const uint8_t *r01 = g + y0 * sy + z1 * sz, *r11 = g + y1 * sy + z1 * sz;
+  const float c00 = lerp_((float)__ldg(r00 + x0), (float)__ldg(r00 + x1), fx);
+  const float c10 = lerp_((float)__ldg(r10 + x0), (float)__ldg(r10 + x1), fx);
+  const float c01 = lerp_((float)__ldg(r01 + x0), (float)__ldg(r01 + x1), fx);
+  const float c11 = lerp_((float)__ldg(r11 + x0), (float)__ldg(r11 + x1), fx);
+  return lerp_(lerp_(c00, c10, fy), lerp_(c01, c11, fy), fz) * kInv255;
+}
+
+// vol_sample of the tiled slab (raycast.slang:423-455): voxel coordinates
+// of p, the ring coordinate, then the overview level whose prefilter
+// (4 << level) matches the footprint, or the base tile under p.
+__device__ __forceinline__ float slab_sample(const DevSlab &sl, float3 p, float lod) {
+  const float wx = p.x * sl.nx, wy = p.y * sl.nx;
+  const float zc = (sl.z0 + 0.5f) + p.z * sl.nx;
+  const float zq = zc / (float)sl.wz;
+  const float w = zq - floorf(zq);  // frac: the ring wraps
+  int lev = (int)floorf(lod) - 2;
+  if (lev >= 0) {
+    const int nl = (int)(r3d_log2f((float)sl.ovs) + 0.5f) - 1;
+    lev = min(lev, nl - 1);
+    const float sc = (float)(4 << lev);
+    const float vnx = ceilf(sl.nx / sc), vny = ceilf(sl.ny / sc);
+    const float gxl = ceilf(vnx / 2046.0f), gyl = ceilf(vny / 2046.0f);
+    const float pxl = ceilf(vnx / gxl), pyl = ceilf(vny / gyl);
+    const float wxl = wx / sc, wyl = wy / sc;
+    const float oix = fminf(floorf(fmaxf(wxl, 0.0f) / pxl), gxl - 1.0f);
+    const float oiy = fminf(floorf(fmaxf(wyl, 0.0f) / pyl), gyl - 1.0f);
+    const float ou = ((wxl - oix * pxl) + 1.0f) / (pxl + 2.0f);
+    const float ov = ((wyl - oiy * pyl) + 1.0f) / (pyl + 2.0f);
+    return slab_tile(sl, lev + 1, (uint32_t)(oiy * gxl + oix), ou, ov, w);
+  }
+  const uint32_t gx = sl.lev[0].gx, gy = sl.lev[0].gy;
+  const uint32_t ix = min((uint32_t)(fmaxf(wx, 0.0f) / sl.px), gx - 1u);
+  const uint32_t iy = min((uint32_t)(fmaxf(wy, 0.0f) / sl.py), gy - 1u);
+  const float u = ((wx - (float)ix * sl.px) + 1.0f) / (sl.px + 2.0f);
+  const float v = ((wy - (float)iy * sl.py) + 1.0f) / (sl.py + 2.0f);
+  return slab_tile(sl, 0, iy * gx + ix, u, v, w);
+}
+
 // Page entry of brick bi of the shard (raycast.slang:813-821); a slot
 // outside the atlas is treated as absent and flagged.
 __device__ __forceinline__ void shard_entry(const DevScene &s, uint32_t bi, BrickCtx &c) {
@@ -457,6 +541,11 @@ __device__ __forceinline__ ViewConst view_const(const r3d_frame_params &pc, cons
     v.vox_inv = s.sh.n;
     v.max_lod = 3.0f;
     v.ext = make_float3(1.0f, 1.0f, 1.0f);
+  } else if (PATH == PATH_SLAB) {  // raycast.slang:672-677,305-314
+    v.voxel = 1.0f / pc.slab_nx;
+    v.vox_inv = pc.slab_nx;
+    v.max_lod = r3d_log2f((float)((pc.slab_grid >> 16) & 0xffu)) + 2.0f;
+    v.ext = make_float3(1.0f, pc.slab_ny / pc.slab_nx, (float)pc.slab_depth / pc.slab_nx);
   } else {
     v.voxel = 1.0f / (float)s.cube.maxdim;
     v.vox_inv = (float)s.cube.maxdim;
@@ -506,6 +595,7 @@ struct RayState {
   // LOD bricks: for a footprint ratio y in [lod_ylo, lod_yhi) the desired
   // level is lc.desired and lod_step is span_step (empty range: unknown)
   float lod_ylo, lod_yhi;
+  float slab_cap;  // tiled slab: at least 4 samples across the box (raycast.slang:778-779)
   uint32_t steps, mip_index;
   float mip_max, first_hit;
   float acc_r, acc_g, acc_b, acc_a;
@@ -622,6 +712,7 @@ __device__ __forceinline__ bool ray_begin(const r3d_frame_params &pc, const DevS
   st.t = fmaf(hash12(px, py, pc.frame_index), vc.dt, tn);
   st.tf_ = tf_;
   st.span_step = fmaxf((tf_ - tn) / ((float)ray_budget * vc.dt), 1.0f);
+  st.slab_cap = fmaxf(1.0f, (tf_ - tn) / (4.0f * vc.dt));
   // exp2(lod) <= 2^ceil(max_lod) for every lod the clamp admits (powers of
   // two are exact and the margin covers the approximation), so beyond this
   // bound max(exp2(lod), span_step) is span_step without evaluating exp2
@@ -661,6 +752,13 @@ __device__ __forceinline__ float skip_block(const RayState &st, float3 p, float 
   return fmaxf(fminf(fminf(tex[0], tex[1]), tex[2]), st.t) + bsz * 0.01f;
 }
 
+// A gradient tap: the tiled slab's vol_sample, or a cube-like texture.
+template <bool SLAB>
+__device__ __forceinline__ float tap_sample(const DevScene &s, const DevCube &tex, float3 p,
+                                            float lod) {
+  return SLAB ? slab_sample(s.sl, p, lod) : cube_sample(tex, p, lod);
+}
+
 // Gradient shading (FULL mode, raycast.slang:919-998) and front-to-back
 // compositing (:1015-1017) of a contributing sample, then the step advance
 // (:1020).  Returns false when the opacity cutoff ends the ray.
@@ -682,6 +780,7 @@ __device__ __forceinline__ bool composite_sample(const DevScene &s, const ViewCo
   }
   // taps sampled like a cube texture: the cube, or the identity shard atlas
   const DevCube &tex = kShard ? s.sh.atlas : s.cube;
+  constexpr bool kSlab = PATH == PATH_SLAB;
   // non-identity shard: taps at lod_step voxels through the slot
   // (raycast.slang:937-940,972-979)
   const bool slot_taps = kShard && !s.sh.identity;
@@ -708,10 +807,10 @@ __device__ __forceinline__ bool composite_sample(const DevScene &s, const ViewCo
         q3 = shard_fetch(s.sh, org, make_float3(u.x + ev, u.y + ev, u.z + ev), q.lod, e2);
       } else {
         float ee = (vc.voxel * q.lod_step) * ir3;
-        q0 = cube_sample(tex, make_float3(q.p.x + ee, q.p.y - ee, q.p.z - ee), q.lod);
-        q1 = cube_sample(tex, make_float3(q.p.x - ee, q.p.y - ee, q.p.z + ee), q.lod);
-        q2 = cube_sample(tex, make_float3(q.p.x - ee, q.p.y + ee, q.p.z - ee), q.lod);
-        q3 = cube_sample(tex, make_float3(q.p.x + ee, q.p.y + ee, q.p.z + ee), q.lod);
+        q0 = tap_sample<kSlab>(s, tex, make_float3(q.p.x + ee, q.p.y - ee, q.p.z - ee), q.lod);
+        q1 = tap_sample<kSlab>(s, tex, make_float3(q.p.x - ee, q.p.y - ee, q.p.z + ee), q.lod);
+        q2 = tap_sample<kSlab>(s, tex, make_float3(q.p.x - ee, q.p.y + ee, q.p.z - ee), q.lod);
+        q3 = tap_sample<kSlab>(s, tex, make_float3(q.p.x + ee, q.p.y + ee, q.p.z + ee), q.lod);
       }
       g0 = (((q0 - q1) - q2) + q3) * renorm;
       g1 = (((-q0 - q1) + q2) + q3) * renorm;
@@ -749,12 +848,12 @@ __device__ __forceinline__ bool composite_sample(const DevScene &s, const ViewCo
              shard_fetch(s.sh, org, make_float3(u.x, u.y, u.z - ev), q.lod, e2);
       } else {
         float e = vc.voxel * q.lod_step;
-        g0 = cube_sample(tex, make_float3(q.p.x + e, q.p.y, q.p.z), q.lod) -
-             cube_sample(tex, make_float3(q.p.x - e, q.p.y, q.p.z), q.lod);
-        g1 = cube_sample(tex, make_float3(q.p.x, q.p.y + e, q.p.z), q.lod) -
-             cube_sample(tex, make_float3(q.p.x, q.p.y - e, q.p.z), q.lod);
-        g2 = cube_sample(tex, make_float3(q.p.x, q.p.y, q.p.z + e), q.lod) -
-             cube_sample(tex, make_float3(q.p.x, q.p.y, q.p.z - e), q.lod);
+        g0 = tap_sample<kSlab>(s, tex, make_float3(q.p.x + e, q.p.y, q.p.z), q.lod) -
+             tap_sample<kSlab>(s, tex, make_float3(q.p.x - e, q.p.y, q.p.z), q.lod);
+        g1 = tap_sample<kSlab>(s, tex, make_float3(q.p.x, q.p.y + e, q.p.z), q.lod) -
+             tap_sample<kSlab>(s, tex, make_float3(q.p.x, q.p.y - e, q.p.z), q.lod);
+        g2 = tap_sample<kSlab>(s, tex, make_float3(q.p.x, q.p.y, q.p.z + e), q.lod) -
+             tap_sample<kSlab>(s, tex, make_float3(q.p.x, q.p.y, q.p.z - e), q.lod);
       }
     }
     float3 gv = make_float3(g0, g1, g2);
@@ -841,6 +940,7 @@ __device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, 
                                         RayState &st, Pending &pend) {
   constexpr bool kLod = PATH == PATH_LOD_BRICKS;
   constexpr bool kShard = PATH == PATH_SHARD;
+  constexpr bool kSlab = PATH == PATH_SLAB;
   constexpr bool kComposite = MODE == R3D_MODE_FULL || MODE == R3D_MODE_FLAT;
   constexpr bool kShaded = MODE == R3D_MODE_FULL;
   constexpr uint32_t ray_budget = kLod ? (kShaded ? 192u : 256u) : kMaxSteps;
@@ -858,9 +958,10 @@ __device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, 
     else
       lod = clamp_(r3d_log2f(y) + vc.lod_bias, 0.0f, vc.max_lod);
   }
-  const float lod_step =
+  float lod_step =
       !lod_known || st.span_dom ? st.span_step
                                 : fmaxf(lod == 0.0f ? 1.0f : r3d_exp2f(lod), st.span_step);
+  if (kSlab) lod_step = fminf(lod_step, st.slab_cap);
   const float3 dir = st.dir;
   const float3 p =
       make_float3(fmaf(t, dir.x, st.ro.x), fmaf(t, dir.y, st.ro.y), fmaf(t, dir.z, st.ro.z));
@@ -933,6 +1034,8 @@ __device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, 
                              lod == 0.0f ? 1.0f : r3d_exp2f(lod))
                : 0.0f;
     }
+  } else if (kSlab) {
+    v = slab_sample(s.sl, p, lod);
   } else {
     v = cube_sample(s.cube, p, lod);
   }
@@ -962,8 +1065,8 @@ __device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, 
         return kStepCont;
       }
     }
-  } else if (v < vc.occ_gate && occ_sample(s.cube, p) < vc.occ_gate) {
-    st.t = skip_block(st, p, vc.bs);
+  } else if (!kSlab && v < vc.occ_gate && occ_sample(s.cube, p) < vc.occ_gate) {
+    st.t = skip_block(st, p, vc.bs);  // (no empty-space skip in slab mode: raycast.slang:861)
     return kStepCont;
   }
 

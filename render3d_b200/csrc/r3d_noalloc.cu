@@ -75,7 +75,7 @@ extern "C" int r3d_cuda_raycast_fwd_noalloc(r3d_cuda_ctx *c, const r3d_frame_par
   uint32_t gcount[kNoallocViews], gstart[kNoallocViews + 1], ngroups = 0, n = 0;
   for (uint32_t v = 0; v < nviews; v++) {
     if (!render[v]) continue;
-    uint32_t key = (uint32_t)path_of(pcs[v].brick_mode) * 8u | pcs[v].mode, g = 0;
+    uint32_t key = (uint32_t)path_of_view(pcs[v]) * 8u | pcs[v].mode, g = 0;
     while (g < ngroups && gkey[g] != key) g++;
     if (g == ngroups) {
       gkey[ngroups] = key;

@@ -234,6 +234,7 @@ cudaError_t launch_persist(const PersistLaunch &L, const DevScene &s, cudaStream
   switch (L.path) {
     case PATH_LOD_BRICKS: return launch_pm<PATH_LOD_BRICKS>(L, s, st);
     case PATH_SHARD: return launch_pm<PATH_SHARD>(L, s, st);
+    case PATH_SLAB: return launch_pm<PATH_SLAB>(L, s, st);
     default: return launch_pm<PATH_CUBE>(L, s, st);
   }
 }
@@ -254,6 +255,8 @@ int persist_blocks_per_sm(int path, uint32_t mode, bool fast, uint32_t unroll) {
     }
   } else if (path == PATH_SHARD) {
     R3D_OCC(PATH_SHARD, R3D_MODE_FULL, false, 1);
+  } else if (path == PATH_SLAB) {
+    R3D_OCC(PATH_SLAB, R3D_MODE_FULL, false, 1);
   } else {
     R3D_OCC(PATH_CUBE, R3D_MODE_FULL, false, 1);
   }
