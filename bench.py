@@ -22,6 +22,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -814,6 +815,83 @@ def stream_bench(rb, torch, lut, nslots: int = 1024, budget: int = 16,
         ctx.close()
 
 
+def sections_bench(rb, torch, lut, frames: int) -> dict:
+    """Whole cross-sections of an 8192 x 8192 x 64 phantom (4 GiB, generated
+    on the device) in the two modes built for them: the tiled slab (ring of
+    32 slices) and the XY clipmap (window depth 32).  A 1920x1080 camera
+    faces the section and pans across it; each mode is timed rendering a
+    fixed window, and with a per-frame update (slab: the window scrolls one
+    slice; clip: the focus follows the pan and the window scrolls one slice,
+    so levels recentre and ring layers refill).  Device time of the frames
+    with CUDA events on the context stream."""
+    nx, ny, nz, wz = 8192, 8192, 64, 32
+    out = {"workload": f"cross-sections of {nx}x{ny}x{nz}, 1920x1080 face-on pan, full shading"}
+    ctx = rb.Context(0)
+    try:
+        ctx.set_transfer(lut)
+        ctx.set_alpha_cutoff(CUTOFF)
+        vol = ctx.phantom((nx, ny, nz), seed=SEED)
+        t0 = time.perf_counter()
+        ctx.slab_build(vol, wz, 0)
+        torch.cuda.synchronize()
+        slab_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        ctx.clip_build(vol, wz)
+        ctx.clip_frame(0.3 * nx, 0.5 * ny, 0)
+        torch.cuda.synchronize()
+        clip_s = time.perf_counter() - t0
+        del vol
+        torch.cuda.empty_cache()
+        img = torch.zeros((H, W, 4), dtype=torch.uint8, device="cuda")
+        tot = torch.zeros(1, dtype=torch.int64, device="cuda")
+        st = torch.cuda.ExternalStream(ctx.stream)
+        ext = (1.0, ny / nx, (wz - 2) / nx)
+
+        def view(i):
+            u = 0.3 + 0.4 * (i % 240) / 240.0
+            p = rb.camera_view(0.05 * math.sin(i * 0.05), 0.02, 0.12, W, H, lut,
+                               target=(u, 0.5 * ext[1], 0.5 * ext[2]), step_voxels=STEP_VOXELS,
+                               frame_index=i)
+            return p, u
+
+        def run(kind, update):
+            def frame(i):
+                p, u = view(i)
+                if kind == "slab":
+                    if update:
+                        ctx.slab_window((i // 4) % (nz - wz))
+                    ctx.slab_params(p)
+                    p.slab_depth = wz - 2
+                else:
+                    if update:
+                        ctx.clip_frame(u * nx, 0.5 * ny, (i // 4) % (nz - wz))
+                    ctx.clip_params(p)
+                p.density = 6.0
+                ctx.raycast(p, W, H, out=img, total=tot, stream=ctx.stream)
+            for i in range(10):
+                frame(i)
+            torch.cuda.synchronize()
+            tot.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0 = time.perf_counter()
+            e0.record(st)
+            for i in range(10, 10 + frames):
+                frame(i)
+            e1.record(st)
+            torch.cuda.synchronize()
+            wall = time.perf_counter() - t0
+            ms = e0.elapsed_time(e1) / frames
+            return {"ms_per_frame": ms, "fps": 1000.0 / ms, "wall_fps": frames / wall,
+                    "gsamples_per_s": tot.item() / frames / (ms * 1e-3) / 1e9}
+        out["slab"] = {"build_s": slab_s, "fixed_window": run("slab", False),
+                       "window_scroll_every_4_frames": run("slab", True)}
+        out["clip"] = {"build_s": clip_s, "fixed_window": run("clip", False),
+                       "focus_pan_and_scroll": run("clip", True)}
+    finally:
+        ctx.close()
+    return out
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -825,7 +903,8 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fwd-bwd", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
-    ap.add_argument("--workload", default="orbit1024", choices=["orbit1024", "sparse2048"],
+    ap.add_argument("--workload", default="orbit1024",
+                    choices=["orbit1024", "sparse2048", "sections8192"],
                     help="sparse2048: the large sparse volume and 512^3 adjoint (extra line)")
     ap.add_argument("--profile", type=int, default=0, metavar="N",
                     help="only build the workload and render N orbit frames (for ncu)")
@@ -851,6 +930,11 @@ def main() -> None:
         run_reference(args)
     elif args.workload == "sparse2048":
         run_sparse(args)
+    elif args.workload == "sections8192":
+        import torch
+        import render3d_b200 as rb
+        print(json.dumps(sections_bench(rb, torch, rb.scroll_ramp_tf(),
+                                        max(args.steps // 5, 60))), flush=True)
     else:
         run_ours(args)
 

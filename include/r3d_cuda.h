@@ -19,6 +19,7 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include "r3d_host.h"
 #include "r3d_types.h"
 
 #ifdef __cplusplus
@@ -161,6 +162,62 @@ void r3d_cuda_slab_params(const r3d_cuda_ctx *ctx, r3d_frame_params *p);
  * 4 << (level - 1)): (px + 2) x (py + 2) x wz bytes; dims receives them. */
 int r3d_cuda_slab_read(r3d_cuda_ctx *ctx, uint32_t level, uint32_t tile, uint8_t *out,
                        uint32_t dims[3]);
+
+/* XY clipmap: render3d's clip mode for whole cross-sections (reference
+ * src/core/clip.h, src/vk/vkclip.c, sampled by
+ * src/shaders/raycast.slang:357-408).  Six nested levels of spacing 2^l
+ * around a focus, each a 2048^2 texture (2046 payload texels and a 1-texel
+ * apron) with a ring of depth_max / 2^l + 3 (at least 4) level slices.
+ * Level 0 is the volume (nx x ny x nz, x fastest, host or device; copied to
+ * the device), level 1 its 2^3 box with coordinates clamped at full
+ * resolution, levels 2..5 the tight 2^3 box pyramid of tools/mkpyramid; all
+ * boxes truncate.  _frame recentres the levels whose coverage the focus
+ * (fx, fy in voxels) has drifted from by more than a quarter (origins
+ * snapped to 16 level voxels), fills the ring layers of the window from z0
+ * that are missing, on the context's stream, and writes the view fields
+ * (slab_nx/ny/z0/wz/depth, clip_orig, clip_valid) into p when p is not
+ * NULL. */
+int r3d_cuda_clip_build(r3d_cuda_ctx *ctx, const r3d_volume_desc *d, const uint8_t *voxels,
+                        uint32_t depth_max);
+int r3d_cuda_clip_frame(r3d_cuda_ctx *ctx, double fx, double fy, uint64_t z0,
+                        r3d_frame_params *p);
+void r3d_cuda_clip_params(const r3d_cuda_ctx *ctx, r3d_frame_params *p);
+/* Copy of ring layer `layer` of level `level` (2048^2 bytes). */
+int r3d_cuda_clip_read(r3d_cuda_ctx *ctx, uint32_t level, uint32_t layer, uint8_t *out);
+
+/* Virtual slab: render3d's vslab mode (reference src/render/render.h:161-191,
+ * src/core/vslab.h, src/vk/vkbackend.c:5675-6660, sampled by
+ * src/shaders/raycast.slang:321-367).  A W x H x D window anywhere in the
+ * volume (nx x ny x nz, x fastest, host or device; copied to the device),
+ * rendered from world-anchored toroidal tile grids laid out by
+ * r3d_host_vslab_init with z_margin resident slices on each side.  The
+ * reference streams cells from a shard store on a worker thread; here
+ * _frame plans the frame's fills (r3d_host_vslab_plan, at most budget cell
+ * fills), runs them on the context's stream, records them in the ledger,
+ * publishes the validity table and writes the view fields (slab_grid with
+ * bit 24 set, brick_mode = packed pyramid grids, slab_wz/z0/nx/ny/px/py/
+ * depth/x0/y0) into p when p is not NULL.  Frames queued later on the
+ * context's stream see the fills.  R3D_E_INVALID for a window
+ * r3d_host_vslab_init rejects or whose grids do not fit the view fields
+ * (base 63, pyramid 15 tiles per axis). */
+typedef struct r3d_vslab_stats {
+  uint32_t jobs;    /* cell fills this frame */
+  uint32_t slices;  /* base slices written this frame */
+  uint32_t pending; /* window cells whose visible span is still missing */
+  uint32_t pad;
+  int64_t origin[3]; /* window origin x0, y0, z0 (r3d_vslab_get) */
+} r3d_vslab_stats;
+int r3d_cuda_vslab_begin(r3d_cuda_ctx *ctx, const r3d_volume_desc *d, const uint8_t *voxels,
+                         uint32_t W, uint32_t H, uint32_t D, uint32_t z_margin);
+int r3d_cuda_vslab_frame(r3d_cuda_ctx *ctx, double fx, double fy, int64_t z0, uint32_t budget,
+                         r3d_frame_params *p, r3d_vslab_stats *st);
+void r3d_cuda_vslab_params(const r3d_cuda_ctx *ctx, r3d_frame_params *p);
+/* The layout (origin included) of the loaded window. */
+int r3d_cuda_vslab_layout(const r3d_cuda_ctx *ctx, r3d_vslab_layout *out);
+/* Copy of tile `tile` ((px + 2)^2 * wz bytes, layer-major) and of the
+ * validity table (4 words per base tile: key, za, zb, 0). */
+int r3d_cuda_vslab_read(r3d_cuda_ctx *ctx, uint32_t tile, uint8_t *out);
+int r3d_cuda_vslab_table(r3d_cuda_ctx *ctx, uint32_t *out);
 
 /* Slot-parallel overlay atlases of the LOD brick cache (reference
  * src/render/render.h:51-101; sampled by src/shaders/raycast.slang:45-115,

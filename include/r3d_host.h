@@ -74,6 +74,72 @@ uint32_t r3d_host_stream_desired(const uint32_t *page, uint32_t page_words, cons
                                  uint32_t slice_z0, uint32_t slice_depth, float gate,
                                  uint8_t *mark, r3d_stream_cand *out, uint32_t cap);
 
+/* Virtual slab: a W x H x D window anywhere in a volume, rendered from
+ * world-anchored toroidal tile grids (src/core/vslab.h).  Level l has
+ * spacing s = {1, 4, 8, 16, 32}[l] and cells of px * s voxels; cell (cx, cy)
+ * lives in tile base + (cy mod gy) * gx + (cx mod gx), each tile
+ * (px + 2)^2 texels (one-texel apron) by a ring of wz = D + 2 + 2 z_margin
+ * slices, world slice z in layer z mod wz.  gx = 0 marks an absent level. */
+#define R3D_VS_LEVELS 5u
+typedef struct r3d_vslab_layout {
+  uint64_t nx, ny, nz;      /* volume */
+  uint32_t W, H, D;         /* visible window */
+  uint32_t px, wz, z_margin;
+  int64_t x0, y0, z0;       /* window origin; -1 before the first frame */
+  uint32_t s[R3D_VS_LEVELS], gx[R3D_VS_LEVELS], gy[R3D_VS_LEVELS], base[R3D_VS_LEVELS];
+  uint32_t ntiles;
+} r3d_vslab_layout;
+/* Layout of a window (vslab.h:55-105): payload px = max(W, H) / 8 rounded
+ * up to 32 in [64, 2016], shrunk while one tile ring exceeds 3 GiB; per
+ * level ceil(W / cell) (+2 where the axis can move) tiles per axis, pyramid
+ * levels only while max(W, H) / s >= 1024.  -1 for a window that does not
+ * fit (W or H < 64 or beyond the volume, D < 2 or > 2044, ring > 2046 or
+ * deeper than the volume). */
+int r3d_host_vslab_init(r3d_vslab_layout *v, uint64_t nx, uint64_t ny, uint64_t nz, uint32_t W,
+                        uint32_t H, uint32_t D, uint32_t z_margin);
+/* Resident z range [a, b) for a visible window at z0: the margin around it,
+ * shifted inside the volume (vslab.h:113-125). */
+void r3d_host_vslab_zrange(const r3d_vslab_layout *v, int64_t z0, int64_t *a, int64_t *b);
+/* Cells [c0, c1] of level l covering [o, o + span) on an axis of n voxels,
+ * clamped to the volume (vslab.h:129-139). */
+void r3d_host_vslab_range(const r3d_vslab_layout *v, uint32_t l, int64_t o, uint64_t n,
+                          uint32_t span, int64_t *c0, int64_t *c1);
+
+/* Ledger entry of one base tile: the cell it holds (INT64_MIN: none) and
+ * the slices [za, zb) of that cell its ring holds. */
+typedef struct r3d_vslab_cell {
+  int64_t cx, cy, za, zb;
+} r3d_vslab_cell;
+/* One fill: slices [zs0, zs0 + nz) of base cell (cx, cy), and the pyramid
+ * texels derived from them. */
+typedef struct r3d_vslab_job {
+  int64_t cx, cy, zs0;
+  uint32_t nz, prio;
+} r3d_vslab_job;
+/* One frame of the virtual slab (src/vk/vkbackend.c:6390-6620): the window
+ * follows the focus (origin fx - W/2, fy - H/2 snapped down to 16 and kept
+ * in the volume; z0 kept in [0, nz - D]), then the base cells under it are
+ * listed with the slices they miss: the visible span [z0, z0 + D + 2) first
+ * (priority 0, completing a partial span without rewriting what is held),
+ * then the z margin in 16-slice steps, the direction of travel first;
+ * sorted by priority, then squared cell distance from the window centre.
+ * When the window moved in x or y, the cells one column / row beyond it in
+ * the direction of motion follow (whole resident range), where the
+ * straddle tile can host them.  At most budget jobs are written (and at
+ * most cap); the layout's origin becomes the frame's.  Returns the number
+ * of jobs. */
+uint32_t r3d_host_vslab_plan(r3d_vslab_layout *v, const r3d_vslab_cell *cells, double fx,
+                             double fy, int64_t z0, uint32_t budget, r3d_vslab_job *jobs,
+                             uint32_t cap);
+/* Records a finished job in the ledger (vkbackend.c:6408-6430): a new cell
+ * takes the job's slices, a held one grows by them, and the range is
+ * clamped to the resident range of the window at z0.  Returns the base
+ * slot. */
+uint32_t r3d_host_vslab_apply(const r3d_vslab_layout *v, r3d_vslab_cell *cells,
+                              const r3d_vslab_job *j, int64_t z0);
+/* Validity key of cell (cx, cy) (vslab.h:146-150). */
+uint32_t r3d_host_vslab_key(int64_t cx, int64_t cy);
+
 /* A view of the scripted "orbit" benchmark at phase ph in [0,1): yaw = 2 pi ph,
  * pitch = 0.5 sin(4 pi ph), distance 2 around target (src/main.c:3932-3946),
  * identity volume transform, viewport w x h.  Other fields: step_voxels,

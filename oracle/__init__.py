@@ -38,10 +38,22 @@ class Slab(C.Structure):
                 ("tiles", C.c_void_p * 8)]
 
 
+class Clip(C.Structure):
+    _fields_ = [("wzl", C.c_uint32 * 6), ("lev", C.c_void_p * 6), ("ox", C.c_float * 6),
+                ("oy", C.c_float * 6), ("valid", C.c_uint32), ("nx", C.c_uint32),
+                ("z0", C.c_uint32)]
+
+
+class VSlab(C.Structure):
+    _fields_ = [("px", C.c_uint32), ("wz", C.c_uint32), ("ntiles", C.c_uint32),
+                ("gx", C.c_uint32 * 5), ("gy", C.c_uint32 * 5), ("base", C.c_uint32 * 5),
+                ("tiles", C.c_void_p), ("table", C.c_void_p)]
+
+
 class Bricks(C.Structure):
     _fields_ = [("page", C.c_void_p), ("page_words", C.c_uint32), ("pool", C.c_void_p),
                 ("nslots", C.c_uint32), ("atlas", C.c_void_p), ("ovl", C.c_void_p * 4),
-                ("slab", C.c_void_p)]
+                ("slab", C.c_void_p), ("clip", C.c_void_p), ("vslab", C.c_void_p)]
 
 
 class Opts(C.Structure):
@@ -76,6 +88,10 @@ def _load():
     lib.orc_slab_layout.argtypes = [U32, U32, P, P]
     lib.orc_slab_fill.restype = None
     lib.orc_slab_fill.argtypes = [P, U32, U32, U32, U32, U32, C.c_void_p * 8]
+    lib.orc_vslab_fill.restype = None
+    lib.orc_vslab_fill.argtypes = [P, P, U32, U32, C.c_int64, C.c_int64, C.c_int64, U32]
+    lib.orc_clip_fill.restype = None
+    lib.orc_clip_fill.argtypes = [P, U32, U32, U32, U32, U32, P, C.c_void_p * 6]
     lib.orc_build_lod_overlay.restype = C.c_int
     lib.orc_build_lod_overlay.argtypes = [P, U32, U32, U32, P, U32, C.c_int, P, U32]
     lib.orc_build_shard.restype = C.c_int
@@ -257,9 +273,287 @@ class SlabScene:
         self.b.slab = C.addressof(self.s)
 
 
+CLIP_LEVELS, CLIP_TEX, CLIP_PAYLOAD, CLIP_SNAP = 6, 2048, 2046, 16
+
+
+def _clip_snap(v: int, q: int) -> int:
+    """src/core/clip.h:38-42: round toward minus infinity to a multiple of q."""
+    return v // q * q if v >= 0 else -((-v + q - 1) // q) * q
+
+
+def clip_origins(nx: int, ny: int, fx: float, fy: float, prev=None):
+    """Level origins after a frame focused on (fx, fy) voxels: each level
+    recentres (src/core/clip.h:48-66) on the first frame and whenever the
+    focus drifted more than a quarter of its coverage from its centre, unless
+    the coverage spans the whole volume (clip.h:98-108; vkclip.c:320-346
+    passes the truncated focus)."""
+    fx, fy = int(fx), int(fy)
+    out = []
+    for l in range(CLIP_LEVELS):
+        s = 1 << l
+        cov = CLIP_PAYLOAD * s
+        if prev is not None:
+            ox, oy = prev[l]
+            cx, cy = ox + cov // 2, oy + cov // 2
+            if (cov >= nx and cov >= ny) or not (abs(fx - cx) > cov // 4 or abs(fy - cy) > cov // 4):
+                out.append((ox, oy))
+                continue
+        snap = CLIP_SNAP * s
+        ox, oy = _clip_snap(fx - cov // 2, snap), _clip_snap(fy - cov // 2, snap)
+        ox, oy = max(ox, 0), max(oy, 0)
+        if ox + cov > nx:
+            ox = _clip_snap(nx - cov, snap)
+        if oy + cov > ny:
+            oy = _clip_snap(ny - cov, snap)
+        out.append((max(ox, 0), max(oy, 0)))
+    return out
+
+
+class ClipScene:
+    """The XY clipmap of a (nz, ny, nx) volume for the window from z0 with
+    the given level origins (clip_origins), every level valid."""
+
+    def __init__(self, vol: np.ndarray, depth_max: int, origins, z0: int):
+        vol = np.ascontiguousarray(vol, np.uint8)
+        nz, ny, nx = vol.shape
+        self.c = Clip()
+        self.tex = []
+        ptrs = (C.c_void_p * 6)()
+        orig = (C.c_float * 12)()
+        for l in range(CLIP_LEVELS):
+            wzl = max(depth_max // (1 << l) + 3, 4)
+            t = np.zeros((wzl, CLIP_TEX, CLIP_TEX), np.uint8)
+            self.tex.append(t)
+            ptrs[l] = t.ctypes.data
+            self.c.wzl[l] = wzl
+            self.c.lev[l] = t.ctypes.data
+            self.c.ox[l], self.c.oy[l] = float(origins[l][0]), float(origins[l][1])
+            orig[2 * l], orig[2 * l + 1] = float(origins[l][0]), float(origins[l][1])
+        self.c.valid, self.c.nx, self.c.z0 = (1 << CLIP_LEVELS) - 1, nx, z0
+        self.ny, self.depth = ny, depth_max
+        lib.orc_clip_fill(_p(vol), nx, ny, nz, depth_max, z0, C.addressof(orig), ptrs)
+        self.b = Bricks()
+        self.b.clip = C.addressof(self.c)
+
+    def params(self, p) -> None:
+        """The view fields of a clip frame (vkclip.c:428-455), slab_depth the
+        whole window."""
+        p.slab_nx, p.slab_ny, p.slab_z0 = float(self.c.nx), float(self.ny), float(self.c.z0)
+        p.slab_wz = p.slab_depth = self.depth
+        for l in range(CLIP_LEVELS):
+            p.clip_orig[l][0], p.clip_orig[l][1] = self.c.ox[l], self.c.oy[l]
+        p.clip_valid, p.slab_grid, p.brick_mode = self.c.valid, 0, 0
+
+
+VS_SCALE = (1, 4, 8, 16, 32)
+
+
+def vslab_layout(nx, ny, nz, W, H, D, z_margin=0):
+    """Window layout (src/core/vslab.h:55-105) as a dict, or None for a
+    window that does not fit."""
+    ring = D + 2 + 2 * z_margin
+    if W < 64 or H < 64 or W > nx or H > ny or D < 2 or D > 2044 or D > nz or ring > 2046 \
+            or ring > nz:
+        return None
+    m = max(W, H)
+    px = min(max((m // 8 + 31) & ~31, 64), 2016)
+    while px > 64 and (px + 2) ** 2 * ring > 3 << 30:
+        px -= 32
+    ex, ey = (2 if W < nx else 0), (2 if H < ny else 0)
+    gx, gy, base, nt = [], [], [], 0
+    for l, s in enumerate(VS_SCALE):
+        cs = px * s
+        base.append(nt)
+        if l and m // s < 1024:
+            gx.append(0)
+            gy.append(0)
+            continue
+        gx.append(-(-W // cs) + ex)
+        gy.append(-(-H // cs) + ey)
+        nt += gx[-1] * gy[-1]
+    return dict(nx=nx, ny=ny, nz=nz, W=W, H=H, D=D, px=px, wz=ring, z_margin=z_margin,
+                gx=gx, gy=gy, base=base, ntiles=nt, x0=-1, y0=-1, z0=-1)
+
+
+def _vs_zrange(v, z0):
+    za = max(z0 - v["z_margin"], 0)
+    zb = za + v["wz"]
+    if zb > v["nz"]:
+        zb = v["nz"]
+        za = max(zb - v["wz"], 0)
+    return za, zb
+
+
+def _vs_range(v, o, n, span):
+    cs = v["px"]
+    return max(o // cs, 0), min((o + span - 1) // cs, (n - 1) // cs)
+
+
+def _cdiv(a, b):
+    """C integer division (truncating toward zero)."""
+    q = abs(a) // abs(b)
+    return q if (a >= 0) == (b > 0) else -q
+
+
+def vslab_plan(v, cells, fx, fy, z0, budget):
+    """One frame of the virtual slab's fill scheduler (vkbackend.c:6390-6620)
+    with every queued fill finishing within the frame: returns the jobs
+    (cx, cy, zs0, nz) in order and moves the window.  cells: slot ->
+    [cx, cy, za, zb] (cx None: empty)."""
+    px0, py0, pz0 = v["x0"], v["y0"], v["z0"]
+    W, H, D, px = v["W"], v["H"], v["D"], v["px"]
+    x0, y0 = int(fx) - W // 2, int(fy) - H // 2
+    x0 = 0 if x0 < 0 else x0 & ~15
+    y0 = 0 if y0 < 0 else y0 & ~15
+    mx, my = max(v["nx"] - W, 0), max(v["ny"] - H, 0)
+    x0 = mx & ~15 if x0 > mx else x0
+    y0 = my & ~15 if y0 > my else y0
+    z0 = min(max(z0, 0), max(v["nz"] - D, 0))
+    za_w, zb_w = _vs_zrange(v, z0)
+    vis_end = min(z0 + D + 2, v["nz"])
+    up = pz0 < 0 or z0 >= pz0
+    v["x0"], v["y0"], v["z0"] = x0, y0, z0
+    cx0, cx1 = _vs_range(v, x0, v["nx"], W)
+    cy0, cy1 = _vs_range(v, y0, v["ny"], H)
+    gx, gy = v["gx"][0], v["gy"][0]
+    ccx, ccy = (x0 + W // 2) // px, (y0 + H // 2) // px
+    mchunks = (v["z_margin"] + 15) // 16
+    jobs = []
+    for cy in range(cy0, cy1 + 1):
+        for cx in range(cx0, cx1 + 1):
+            if len(jobs) >= 64:
+                break
+            c = cells[(cy % gy) * gx + cx % gx]
+            held = c[0] == cx and c[1] == cy
+            s0, s1, prio = z0, vis_end, 0
+            if held:
+                za, zb = c[2], c[3]
+                if za <= za_w and zb >= zb_w:
+                    continue
+                visible = za <= z0 and zb >= vis_end
+                if not visible and za < vis_end and zb > z0:
+                    if za > z0:
+                        s1 = min(za, vis_end)
+                    else:
+                        s0 = max(zb, z0)
+                elif visible:
+                    if up and zb < zb_w:
+                        grow, extra = True, 0
+                    elif not up and za > za_w:
+                        grow, extra = False, 0
+                    elif za > za_w:
+                        grow, extra = False, mchunks
+                    else:
+                        grow, extra = True, mchunks
+                    if grow:
+                        s0, s1, filled = zb, min(zb + 16, zb_w), zb - vis_end
+                    else:
+                        s1, s0, filled = za, max(za - 16, za_w), z0 - za
+                    prio = 1 + extra + (filled // 16 if filled > 0 else 0)
+            jobs.append([prio, (cx - ccx) ** 2 + (cy - ccy) ** 2, cx, cy, s0, s1 - s0])
+        if len(jobs) >= 64:
+            break
+    n = len(jobs)
+    for a in range(n - 1):  # the reference's exchange sort
+        for b in range(a + 1, n):
+            if jobs[b][0] < jobs[a][0] or (jobs[b][0] == jobs[a][0] and jobs[b][1] < jobs[a][1]):
+                jobs[a], jobs[b] = jobs[b], jobs[a]
+    out = [tuple(j[2:]) for j in jobs[:budget]]
+    if px0 >= 0 and (x0 != px0 or y0 != py0):
+        pf = []
+        mxc, myc = (v["nx"] - 1) // px, (v["ny"] - 1) // px
+        if x0 != px0:
+            cxc = cx1 + 1 if x0 > px0 else cx0 - 1
+            if 0 <= cxc <= mxc and cx1 - cx0 + 2 <= gx:
+                pf += [(cxc, cy) for cy in range(cy0, cy1 + 1)][:48]
+        if y0 != py0:
+            cyc = cy1 + 1 if y0 > py0 else cy0 - 1
+            if 0 <= cyc <= myc and cy1 - cy0 + 2 <= gy:
+                pf += [(cx, cyc) for cx in range(cx0, cx1 + 1)][:48 - len(pf)]
+        for cx, cy in pf:
+            if len(out) >= budget:
+                break
+            c = cells[(cy % gy) * gx + cx % gx]
+            if c[0] == cx and c[1] == cy and c[2] <= za_w and c[3] >= zb_w:
+                continue
+            if any(j[0] == cx and j[1] == cy for j in out):
+                continue
+            out.append((cx, cy, za_w, zb_w - za_w))
+    return out
+
+
+def vslab_apply(v, cells, job):
+    """A finished fill in the ledger (vkbackend.c:6408-6430); returns the slot."""
+    cx, cy, zs0, nz = job
+    za_w, zb_w = _vs_zrange(v, v["z0"])
+    slot = (cy % v["gy"][0]) * v["gx"][0] + cx % v["gx"][0]
+    c = cells[slot]
+    if c[0] != cx or c[1] != cy:
+        c[2], c[3] = zs0, zs0 + nz
+    else:
+        c[2], c[3] = min(c[2], zs0), max(c[3], zs0 + nz)
+    c[0], c[1] = cx, cy
+    c[2] = max(c[2], za_w)
+    c[3] = max(min(c[3], zb_w), c[2])
+    return slot
+
+
+class VSlabScene:
+    """The virtual slab of a (nz, ny, nx) volume, driven frame by frame with
+    the scheduler restated above; the tiles are filled by the oracle's
+    restatement of the reference's fill."""
+
+    def __init__(self, vol: np.ndarray, W: int, H: int, D: int, z_margin: int = 0):
+        self.vol = np.ascontiguousarray(vol, np.uint8)
+        nz, ny, nx = self.vol.shape
+        self.v = vslab_layout(nx, ny, nz, W, H, D, z_margin)
+        if self.v is None:
+            raise ValueError("vslab layout")
+        v = self.v
+        T = v["px"] + 2
+        self.tiles = np.zeros((v["ntiles"], v["wz"], T, T), np.uint8)
+        nslot = v["gx"][0] * v["gy"][0]
+        self.table = np.zeros((nslot, 4), np.uint32)
+        self.cells = [[None, None, 0, 0] for _ in range(nslot)]
+        self.s = VSlab()
+        self.s.px, self.s.wz, self.s.ntiles = v["px"], v["wz"], v["ntiles"]
+        for l in range(5):
+            self.s.gx[l], self.s.gy[l], self.s.base[l] = v["gx"][l], v["gy"][l], v["base"][l]
+        self.s.tiles, self.s.table = self.tiles.ctypes.data, self.table.ctypes.data
+        self.b = Bricks()
+        self.b.vslab = C.addressof(self.s)
+
+    def frame(self, fx, fy, z0, budget):
+        """Plans and runs one frame's fills; returns the jobs."""
+        nz, ny, nx = self.vol.shape
+        jobs = vslab_plan(self.v, self.cells, fx, fy, z0, budget)
+        for j in jobs:
+            cx, cy, zs0, n = j
+            if n:
+                lib.orc_vslab_fill(C.byref(self.s), _p(self.vol), nx, ny, cx, cy, zs0, n)
+            slot = vslab_apply(self.v, self.cells, j)
+            c = self.cells[slot]
+            self.table[slot] = ((c[0] & 1023) | ((c[1] & 1023) << 10) | 0x80000000, c[2], c[3], 0)
+        return jobs
+
+    def params(self, p) -> None:
+        """The view fields of the frame (vkbackend.c:6628-6645)."""
+        v = self.v
+        p.slab_grid = v["gx"][0] | (v["gy"][0] << 6) | (1 << 24)
+        p.brick_mode = sum((v["gx"][l] | (v["gy"][l] << 4)) << ((l - 1) * 8) for l in range(1, 5))
+        p.slab_wz, p.slab_z0 = v["wz"], float(max(v["z0"], 0))
+        p.slab_nx, p.slab_ny = float(v["W"]), float(v["H"])
+        p.slab_px = p.slab_py = float(v["px"])
+        p.slab_depth = v["D"]
+        p.slab_x0, p.slab_y0 = float(max(v["x0"], 0)), float(max(v["y0"], 0))
+        p.clip_valid = 0
+
+
 def _scene_args(scene):
     cube = C.byref(scene.c) if isinstance(scene, CubeScene) else None
-    br = C.byref(scene.b) if isinstance(scene, (BrickScene, ShardScene, SlabScene)) else None
+    br = (C.byref(scene.b)
+          if isinstance(scene, (BrickScene, ShardScene, SlabScene, ClipScene, VSlabScene))
+          else None)
     return cube, br
 
 

@@ -137,6 +137,7 @@ typedef struct scene {
   const orc_cube *cube;
   const orc_bricks *br;
   uint32_t *status;
+  const r3d_frame_params *pc; /* the view */
 } scene;
 
 static inline uint32_t page_rd(const scene *s, uint32_t i) {
@@ -292,11 +293,10 @@ static void lerp3(float c[3], float r, float g, float b, float t) {
   c[2] = lerpf_(c[2], b, t);
 }
 
-/* slab tile k of level L at normalized (u, v, w): linear, clamp to edge in
- * x and y, REPEAT in w (vkbackend.c:2203-2211) */
-static float slab_tile(const orc_slab *sl, int L, uint32_t k, float u, float v, float w) {
-  uint32_t tw = sl->lev[L][2] + 2u, th = sl->lev[L][3] + 2u, wz = sl->wz;
-  const uint8_t *g = sl->tiles[L] + (size_t)k * tw * th * wz;
+/* a tw x th x wz texture at normalized (u, v, w): linear, clamp to edge in
+ * x and y, REPEAT in w (the slab sampler, vkbackend.c:2203-2211) */
+static float tex_wrapz(const uint8_t *g, uint32_t tw, uint32_t th, uint32_t wz, float u, float v,
+                       float w) {
   float tx = clampf_(fmaf(u, (float)tw, -0.5f), 0.0f, (float)(tw - 1u));
   float ty = clampf_(fmaf(v, (float)th, -0.5f), 0.0f, (float)(th - 1u));
   float tz = fmaf(w, (float)wz, -0.5f);
@@ -315,6 +315,12 @@ static float slab_tile(const orc_slab *sl, int L, uint32_t k, float u, float v, 
   float c11 = lerpf_(T(x0, y1, z1), T(x1, y1, z1), fx);
 #undef T
   return lerpf_(lerpf_(c00, c10, fy), lerpf_(c01, c11, fy), fz) * INV255;
+}
+
+/* slab tile k of level L */
+static float slab_tile(const orc_slab *sl, int L, uint32_t k, float u, float v, float w) {
+  uint32_t tw = sl->lev[L][2] + 2u, th = sl->lev[L][3] + 2u, wz = sl->wz;
+  return tex_wrapz(sl->tiles[L] + (size_t)k * tw * th * wz, tw, th, wz, u, v, w);
 }
 
 /* vol_sample of the tiled slab (raycast.slang:423-455) */
@@ -349,9 +355,92 @@ static float slab_sample(const orc_slab *sl, v3f p, float lod) {
   return slab_tile(sl, 0, iy * gx + ix, u, v, w);
 }
 
-/* a gradient tap: the slab's vol_sample or a cube-like texture */
-static float tap_sample(const scene *s, int slab, const orc_cube *tex, v3f p, float lod) {
-  return slab ? slab_sample(s->br->slab, p, lod) : cube_sample(tex, p, lod);
+/* vs_sample, :331-367: the base cell under p must be the one its tile
+ * holds, with the sample's slice span; then the pyramid level matching the
+ * footprint (stepping down past absent levels) or the base tile.  Cells
+ * convert through int for the key. */
+static float vs_sample(const orc_vslab *v, const r3d_frame_params *pc, v3f p, float lod) {
+  float P = pc->slab_px, T = P + 2.0f;
+  uint32_t Tu = v->px + 2u;
+  size_t tb = (size_t)Tu * Tu * v->wz;
+  float wx = pc->slab_x0 + p.x * pc->slab_nx;
+  float wy = pc->slab_y0 + p.y * pc->slab_nx;
+  float zc = (pc->slab_z0 + 0.5f) + p.z * pc->slab_nx;
+  float zq = zc / (float)pc->slab_wz, w = zq - floorf(zq);
+  float gx0 = (float)(pc->slab_grid & 63u), gy0 = (float)((pc->slab_grid >> 6) & 63u);
+  float cbx = floorf(wx / P), cby = floorf(wy / P);
+  float pbx = cbx - floorf(cbx / gx0) * gx0, pby = cby - floorf(cby / gy0) * gy0;
+  uint32_t want = ((uint32_t)(int32_t)cbx & 1023u) | (((uint32_t)(int32_t)cby & 1023u) << 10) |
+                  0x80000000u;
+  uint32_t s4 = (uint32_t)(pby * gx0 + pbx) * 4u;
+  if (v->table[s4] != want) return 0.0f;
+  if (zc - 0.5f < (float)v->table[s4 + 1] || zc + 0.5f > (float)v->table[s4 + 2]) return 0.0f;
+  int lev = (int)floorf(lod) - 2;
+  if (lev > 3) lev = 3;
+  while (lev >= 0 && ((pc->brick_mode >> (8u * (uint32_t)lev)) & 0xffu) == 0u) lev--;
+  if (lev < 0) {
+    float lx = (wx - cbx * P) + 1.0f, ly = (wy - cby * P) + 1.0f;
+    return tex_wrapz(v->tiles + (size_t)(s4 / 4u) * tb, Tu, Tu, v->wz, lx / T, ly / T, w);
+  }
+  float sc = (float)(4 << lev);
+  uint32_t gp = pc->brick_mode >> (8u * (uint32_t)lev);
+  float gxl = (float)(gp & 15u), gyl = (float)((gp >> 4) & 15u);
+  uint32_t bse = (pc->slab_grid & 63u) * ((pc->slab_grid >> 6) & 63u);
+  for (int k = 0; k < lev; k++) {
+    uint32_t gk = pc->brick_mode >> (8u * (uint32_t)k);
+    bse += (gk & 15u) * ((gk >> 4) & 15u);
+  }
+  float tx = wx / sc, ty = wy / sc;
+  float cx = floorf(tx / P), cy = floorf(ty / P);
+  float qx = cx - floorf(cx / gxl) * gxl, qy = cy - floorf(cy / gyl) * gyl;
+  float lx = (tx - cx * P) + 1.0f, ly = (ty - cy * P) + 1.0f;
+  uint32_t k = bse + (uint32_t)(qy * gxl + qx);
+  return tex_wrapz(v->tiles + (size_t)k * tb, Tu, Tu, v->wz, lx / T, ly / T, w);
+}
+
+/* sample_clip_level, :360-376 */
+static float clip_level(const orc_clip *cl, int l, v3f p) {
+  float s = (float)(1u << l), nx = (float)cl->nx;
+  float wx = p.x * nx, wy = p.y * nx;
+  float zw = ((float)cl->z0 + 0.5f) + p.z * nx;
+  float u = ((wx - cl->ox[l]) / s + 1.0f) / 2048.0f;
+  float v = ((wy - cl->oy[l]) / s + 1.0f) / 2048.0f;
+  float zq = (zw / s) / (float)cl->wzl[l];
+  return tex_wrapz(cl->lev[l], 2048u, 2048u, cl->wzl[l], u, v, zq - floorf(zq));
+}
+
+/* pick_clip_level, :380-395 */
+static int clip_pick(const orc_clip *cl, v3f p, float lod) {
+  float nx = (float)cl->nx, wx = p.x * nx, wy = p.y * nx;
+  int desired = (int)clampf_(lod, 0.0f, 5.0f);
+  for (int step = 0; step < 6; step++) {
+    int li = desired + step;
+    if (li > 5) li = 5 - step;
+    if (li < 0) continue;
+    if (!(cl->valid & (1u << li))) continue;
+    float s = (float)(1u << li);
+    float tx = (wx - cl->ox[li]) / s + 1.0f, ty = (wy - cl->oy[li]) / s + 1.0f;
+    if (tx < 1.0f || tx >= 2047.0f || ty < 1.0f || ty >= 2047.0f) continue;
+    return li;
+  }
+  return -1;
+}
+
+/* a gradient tap by sampling path: the slab's vol_sample; clip mode's
+ * picked level (or vol_sample without one, :942-946,967-974); the virtual
+ * slab's vol_sample; else a cube-like texture */
+enum { TAP_TEX, TAP_SLAB, TAP_CLIP, TAP_VSLAB };
+static float tap_sample(const scene *s, int kind, const orc_cube *tex, v3f p, float lod,
+                        int cl_l) {
+  switch (kind) {
+    case TAP_SLAB: return slab_sample(s->br->slab, p, lod);
+    case TAP_VSLAB: return vs_sample(s->br->vslab, s->pc, p, lod);
+    case TAP_CLIP:
+      if (cl_l >= 0) return clip_level(s->br->clip, cl_l, p);
+      cl_l = clip_pick(s->br->clip, p, lod);
+      return cl_l < 0 ? 0.0f : clip_level(s->br->clip, cl_l, p);
+    default: return cube_sample(tex, p, lod);
+  }
 }
 
 /* ------------------------------------------------------------ the march */
@@ -374,10 +463,13 @@ static void march(const r3d_frame_params *pc, const scene *s, const uint8_t lut[
   if (px >= pc->viewport[0] || py >= pc->viewport[1]) return;
   out->store = 1;
   int ortho = (pc->view_flags & R3D_VIEW_ORTHO) != 0u;
-  int bricks = pc->brick_mode != 0u;
+  int vslab = pc->clip_valid == 0u && (pc->slab_grid & (1u << 24)) != 0u;
+  int bricks = !vslab && pc->brick_mode != 0u; /* a virtual slab's brick_mode packs its grids */
   int lodb = bricks && (pc->brick_mode & R3D_BRICK_LOD_FLAG) != 0u;
-  int slab = pc->slab_grid != 0u;
-  int shard = bricks && !lodb && !slab;
+  int clip = pc->clip_valid != 0u;
+  int slab = !clip && !vslab && pc->slab_grid != 0u;
+  int tk = clip ? TAP_CLIP : vslab ? TAP_VSLAB : slab ? TAP_SLAB : TAP_TEX;
+  int shard = bricks && !lodb && !slab && !clip;
   uint32_t sh_bpa = pc->brick_mode & 0xffu, sh_abpa = (pc->brick_mode >> 8) & 0xffu;
   int sh_ident = (pc->brick_mode & R3D_BRICK_IDENTITY_FLAG) != 0u;
   const orc_cube *atlas = shard ? s->br->atlas : NULL;
@@ -420,6 +512,21 @@ static void march(const r3d_frame_params *pc, const scene *s, const uint8_t lut[
     vox_inv = md;
     max_lod = (float)(nlev - 1u);
     ext = mk3(bs[0] / md, bs[1] / md, bs[2] / md);
+  } else if (vslab) { /* :661-671, :305-314 */
+    voxel = 1.0f / pc->slab_nx;
+    vox_inv = pc->slab_nx;
+    max_lod = 3.0f; /* +2 past the coarsest present pyramid level */
+    for (int l = 3; l >= 0; l--)
+      if (((pc->brick_mode >> (8u * (uint32_t)l)) & 0xffu) != 0u) {
+        max_lod = (float)l + 4.0f;
+        break;
+      }
+    ext = mk3(1.0f, pc->slab_ny / pc->slab_nx, (float)pc->slab_depth / pc->slab_nx);
+  } else if (clip) { /* :651-654, :305-314 */
+    voxel = 1.0f / pc->slab_nx;
+    vox_inv = pc->slab_nx;
+    max_lod = 7.0f;
+    ext = mk3(1.0f, pc->slab_ny / pc->slab_nx, (float)pc->slab_depth / pc->slab_nx);
   } else if (slab) { /* :672-677, :305-314 */
     const orc_slab *sl = s->br->slab;
     voxel = 1.0f / pc->slab_nx;
@@ -543,15 +650,21 @@ static void march(const r3d_frame_params *pc, const scene *s, const uint8_t lut[
     float foot = ortho ? cone : t * cone;
     float lod = clampf_(r3d_log2f(fmaxf(foot * vox_inv, 1.0f)) + pc->lod_bias, 0.0f, max_lod);
     float lod_step = fmaxf(r3d_exp2f(lod), span_step);
-    if (slab) lod_step = fminf(lod_step, slab_cap);
+    if (slab || clip || vslab) lod_step = fminf(lod_step, slab_cap);
     v3f p = mk3(fmaf(t, dir.x, ro.x), fmaf(t, dir.y, ro.y), fmaf(t, dir.z, ro.z));
 
     float v;
+    int cl_lvl = -1; /* clip: the level picked once per sample (:782) */
     if (lodb) {
       b = lod_locate_cached(s, p, lod, &lc);
       v = b.ok ? brick_fetch(s, b.slot, b.bl) : 0.0f;
+    } else if (clip) { /* :785-787 */
+      cl_lvl = clip_pick(s->br->clip, p, lod);
+      v = cl_lvl < 0 ? 0.0f : clip_level(s->br->clip, cl_lvl, p);
     } else if (slab) {
       v = slab_sample(s->br->slab, p, lod);
+    } else if (vslab) {
+      v = vs_sample(s->br->vslab, pc, p, lod);
     } else if (shard && sh_ident) { /* :800-805 */
       v = cube_sample(atlas, p, lod);
     } else if (shard) { /* :806-822 */
@@ -608,7 +721,8 @@ static void march(const r3d_frame_params *pc, const scene *s, const uint8_t lut[
           void_blk = 1;
         }
       }
-    } else if (!slab && v < occ_gate && occ_sample(s->cube->occ, s->cube->odim, p) < occ_gate) {
+    } else if (!slab && !clip && !vslab && v < occ_gate &&
+               occ_sample(s->cube->occ, s->cube->odim, p) < occ_gate) {
       void_blk = 1;
     }
     if (void_blk) {
@@ -681,10 +795,10 @@ static void march(const r3d_frame_params *pc, const scene *s, const uint8_t lut[
             } else {
               const orc_cube *tex = shard ? atlas : s->cube;
               float ee = (voxel * lod_step) * ir3;
-              q0 = tap_sample(s, slab, tex, mk3(p.x + ee, p.y - ee, p.z - ee), lod);
-              q1 = tap_sample(s, slab, tex, mk3(p.x - ee, p.y - ee, p.z + ee), lod);
-              q2 = tap_sample(s, slab, tex, mk3(p.x - ee, p.y + ee, p.z - ee), lod);
-              q3 = tap_sample(s, slab, tex, mk3(p.x + ee, p.y + ee, p.z + ee), lod);
+              q0 = tap_sample(s, tk, tex, mk3(p.x + ee, p.y - ee, p.z - ee), lod, cl_lvl);
+              q1 = tap_sample(s, tk, tex, mk3(p.x - ee, p.y - ee, p.z + ee), lod, cl_lvl);
+              q2 = tap_sample(s, tk, tex, mk3(p.x - ee, p.y + ee, p.z - ee), lod, cl_lvl);
+              q3 = tap_sample(s, tk, tex, mk3(p.x + ee, p.y + ee, p.z + ee), lod, cl_lvl);
             }
             g[0] = (((q0 - q1) - q2) + q3) * renorm;
             g[1] = (((-q0 - q1) + q2) + q3) * renorm;
@@ -711,12 +825,12 @@ static void march(const r3d_frame_params *pc, const scene *s, const uint8_t lut[
             } else {
               const orc_cube *tex = shard ? atlas : s->cube;
               float e = voxel * lod_step;
-              g[0] = tap_sample(s, slab, tex, mk3(p.x + e, p.y, p.z), lod) -
-                     tap_sample(s, slab, tex, mk3(p.x - e, p.y, p.z), lod);
-              g[1] = tap_sample(s, slab, tex, mk3(p.x, p.y + e, p.z), lod) -
-                     tap_sample(s, slab, tex, mk3(p.x, p.y - e, p.z), lod);
-              g[2] = tap_sample(s, slab, tex, mk3(p.x, p.y, p.z + e), lod) -
-                     tap_sample(s, slab, tex, mk3(p.x, p.y, p.z - e), lod);
+              g[0] = tap_sample(s, tk, tex, mk3(p.x + e, p.y, p.z), lod, cl_lvl) -
+                     tap_sample(s, tk, tex, mk3(p.x - e, p.y, p.z), lod, cl_lvl);
+              g[1] = tap_sample(s, tk, tex, mk3(p.x, p.y + e, p.z), lod, cl_lvl) -
+                     tap_sample(s, tk, tex, mk3(p.x, p.y - e, p.z), lod, cl_lvl);
+              g[2] = tap_sample(s, tk, tex, mk3(p.x, p.y, p.z + e), lod, cl_lvl) -
+                     tap_sample(s, tk, tex, mk3(p.x, p.y, p.z - e), lod, cl_lvl);
             }
           }
           v3f gv = mk3(g[0], g[1], g[2]);
@@ -799,7 +913,18 @@ static int check_view(const r3d_frame_params *p, const orc_cube *cube, const orc
        ((p->overlay_flags & 4u) && !br->ovl[1]) || ((p->overlay_flags & 8u) && !br->ovl[2]) ||
        ((p->overlay_flags & 16u) && !br->ovl[3])))
     return -1;
-  if (p->slab_grid) { /* slab views need the slab and must describe its window */
+  int vslab = !p->clip_valid && (p->slab_grid & (1u << 24)) != 0u;
+  if (vslab) { /* virtual-slab views must describe the loaded grids */
+    const orc_vslab *v = br ? br->vslab : NULL;
+    uint32_t bm = 0;
+    if (v)
+      for (int l = 1; l < 5; l++) bm |= (v->gx[l] | (v->gy[l] << 4)) << (8 * (l - 1));
+    if (!v || p->slab_grid != (v->gx[0] | (v->gy[0] << 6) | (1u << 24)) || p->brick_mode != bm ||
+        p->slab_wz != v->wz || p->slab_px != (float)v->px || p->slab_nx < 1.0f ||
+        p->slab_depth < 1u || (p->overlay_flags & 0x1Du))
+      return -1;
+  }
+  if (p->slab_grid && !vslab && !p->clip_valid) { /* slab views: the slab's window */
     const orc_slab *sl = br ? br->slab : NULL;
     if (!sl || p->brick_mode || p->slab_wz != sl->wz || p->slab_z0 != (float)sl->z0 ||
         p->slab_nx != (float)sl->nx || p->slab_ny != (float)sl->ny ||
@@ -808,10 +933,21 @@ static int check_view(const r3d_frame_params *p, const orc_cube *cube, const orc
         p->slab_depth < 1u || p->slab_depth > sl->wz - 1u)
       return -1;
   }
-  if (p->clip_valid ||
-      (p->view_flags & (R3D_VIEW_SURF | R3D_VIEW_STRETCH)) || p->mode >= R3D_MODE_COUNT)
+  if (p->clip_valid) { /* clip views must describe the loaded levels */
+    const orc_clip *cl = br ? br->clip : NULL;
+    if (!cl || p->clip_valid != cl->valid || p->brick_mode || p->slab_grid ||
+        p->slab_nx != (float)cl->nx || p->slab_z0 != (float)cl->z0 ||
+        p->slab_wz != cl->wzl[0] - 3u || p->slab_depth < 1u || p->slab_depth > p->slab_wz ||
+        (p->overlay_flags & 0x1Du))
+      return -1;
+    for (int l = 0; l < 6; l++)
+      if (p->clip_orig[l][0] != cl->ox[l] || p->clip_orig[l][1] != cl->oy[l]) return -1;
+  }
+  if ((p->view_flags & (R3D_VIEW_SURF | R3D_VIEW_STRETCH)) || p->mode >= R3D_MODE_COUNT)
     return -1;
-  if (p->brick_mode & R3D_BRICK_LOD_FLAG) {
+  if (vslab) {
+    /* brick_mode packs the pyramid grids (checked above) */
+  } else if (p->brick_mode & R3D_BRICK_LOD_FLAG) {
     if (!br || !br->page || br->page_words < 64u) return -1;
     uint32_t nlev = br->page[0];
     if (nlev < 1u || nlev > 15u) return -1;
@@ -823,7 +959,8 @@ static int check_view(const r3d_frame_params *p, const orc_cube *cube, const orc
       return -1;
     for (int k = 0; k < 3; k++)
       if (a->dim[0][k] != abpa * 128u || a->odim[k] != bpa * 16u) return -1;
-  } else if (!p->slab_grid && (!cube || !cube->nlevels || !cube->occ)) {
+  } else if (!vslab && !p->slab_grid && !p->clip_valid &&
+             (!cube || !cube->nlevels || !cube->occ)) {
     return -1;
   }
   return 0;
@@ -844,7 +981,7 @@ int orc_render_view(const r3d_frame_params *p, const orc_cube *cube, const orc_b
     num_threads(o->threads > 0 ? o->threads : omp_get_max_threads())
   for (uint32_t ty = 0; ty < gh; ty++) {
     uint32_t st = 0;
-    scene s = {cube, bricks, &st};
+    scene s = {cube, bricks, &st, p};
     for (uint32_t tx = 0; tx < gw; tx++) {
       ray_out r;
       march(p, &s, lut, o, tx, ty, &r);
@@ -878,7 +1015,7 @@ int orc_render_pixels(const r3d_frame_params *p, const orc_cube *cube, const orc
     num_threads(o->threads > 0 ? o->threads : omp_get_max_threads())
   for (uint32_t i = 0; i < n; i++) {
     uint32_t st = 0;
-    scene s = {cube, bricks, &st};
+    scene s = {cube, bricks, &st, p};
     ray_out r;
     march(p, &s, lut, o, xy[2 * i], xy[2 * i + 1], &r);
     uint8_t px[4] = {0, 0, 0, 0};
@@ -1028,6 +1165,146 @@ static void slab_tiles(const uint8_t *plane, uint32_t nx, uint32_t ny, const uin
           tiles[(size_t)(j * L[0] + i) * tb + (size_t)layer * tw * th + (size_t)ty * tw + tx] =
               plane[(size_t)cy * nx + (size_t)cx];
         }
+}
+
+/* truncating N x N box of a w x h plane (row pitch stride), vkbackend.c:5682-5696 */
+static void vs_box(const uint8_t *src, uint32_t stride, uint32_t w, uint32_t h, uint32_t N,
+                   uint8_t *dst) {
+  for (uint32_t y = 0; y < h / N; y++)
+    for (uint32_t x = 0; x < w / N; x++) {
+      uint32_t sum = 0;
+      for (uint32_t yy = 0; yy < N; yy++)
+        for (uint32_t xx = 0; xx < N; xx++) sum += src[(size_t)(y * N + yy) * stride + x * N + xx];
+      dst[(size_t)y * (w / N) + x] = (uint8_t)(sum / (N * N));
+    }
+}
+
+void orc_vslab_fill(orc_vslab *v, const uint8_t *vox, uint32_t nx, uint32_t ny, int64_t cx,
+                    int64_t cy, int64_t zs0, uint32_t nz) {
+  const uint32_t P = v->px, T = P + 2u;
+  const size_t plane = (size_t)T * T, tb = plane * v->wz;
+  const uint32_t slot = (uint32_t)(cy % v->gy[0]) * v->gx[0] + (uint32_t)(cx % v->gx[0]);
+  uint8_t *box = malloc(plane), *ds[5] = {0};
+  for (uint32_t l = 1; l < 5; l++) ds[l] = malloc((size_t)(P / 4u) * (P / 4u));
+  if (!box || !ds[4]) goto out;
+  static const uint32_t scale[5] = {1u, 4u, 8u, 16u, 32u};
+  for (uint32_t k = 0; k < nz; k++) {
+    const int64_t z = zs0 + k;
+    const size_t layer = (size_t)(z % v->wz) * plane;
+    /* the decoded cell box: near edges duplicated, far edges zero */
+    for (uint32_t ty = 0; ty < T; ty++)
+      for (uint32_t tx = 0; tx < T; tx++) {
+        int64_t wx = cx * (int64_t)P - 1 + tx, wy = cy * (int64_t)P - 1 + ty;
+        uint8_t val = 0;
+        if (wx < (int64_t)nx && wy < (int64_t)ny)
+          val = vox[((size_t)z * ny + (size_t)(wy < 0 ? 0 : wy)) * nx + (size_t)(wx < 0 ? 0 : wx)];
+        box[(size_t)ty * T + tx] = val;
+      }
+    memcpy(v->tiles + (size_t)(v->base[0] + slot) * tb + layer, box, plane);
+    if (!v->gx[1]) continue;
+    /* pyramid strips: 4x from the payload, then 2x chains */
+    vs_box(box + T + 1u, T, P, P, 4u, ds[1]);
+    for (uint32_t l = 2; l < 5 && v->gx[l]; l++)
+      vs_box(ds[l - 1], P / scale[l - 1], P / scale[l - 1], P / scale[l - 1], 2u, ds[l]);
+    for (uint32_t l = 1; l < 5 && v->gx[l]; l++) {
+      const int64_t n = P / scale[l], t0x = cx * n, t0y = cy * n, Pi = P;
+      int64_t p0x = (t0x - 1) / Pi, p1x = (t0x + n) / Pi;
+      int64_t p0y = (t0y - 1) / Pi, p1y = (t0y + n) / Pi;
+      if (p0x < 0) p0x = 0;
+      if (p0y < 0) p0y = 0;
+      for (int64_t qy = p0y; qy <= p1y; qy++)
+        for (int64_t qx = p0x; qx <= p1x; qx++) {
+          int64_t ax = t0x > qx * Pi - 1 ? t0x : qx * Pi - 1;
+          int64_t bx = t0x + n < qx * Pi + Pi + 1 ? t0x + n : qx * Pi + Pi + 1;
+          int64_t ay = t0y > qy * Pi - 1 ? t0y : qy * Pi - 1;
+          int64_t by = t0y + n < qy * Pi + Pi + 1 ? t0y + n : qy * Pi + Pi + 1;
+          if (ax >= bx || ay >= by) continue;
+          uint32_t ti = v->base[l] + (uint32_t)(qy % v->gy[l]) * v->gx[l] + (uint32_t)(qx % v->gx[l]);
+          uint8_t *dst = v->tiles + (size_t)ti * tb + layer;
+          for (int64_t y = ay; y < by; y++)
+            for (int64_t x = ax; x < bx; x++)
+              dst[(size_t)(y - qy * Pi + 1) * T + (size_t)(x - qx * Pi + 1)] =
+                  ds[l][(size_t)(y - t0y) * n + (size_t)(x - t0x)];
+        }
+    }
+  }
+out:
+  free(box);
+  for (uint32_t l = 1; l < 5; l++) free(ds[l]);
+}
+
+/* tight 2^3 box, truncating (tools/mkpyramid/main.c:53-69): dst is
+ * (sx/2, sy/2, sz/2) */
+static void clip_down2(const uint8_t *src, uint32_t sx, uint32_t sy, uint32_t sz, uint8_t *dst) {
+  uint32_t hx = sx / 2u, hy = sy / 2u, hz = sz / 2u;
+  for (uint32_t z = 0; z < hz; z++)
+    for (uint32_t y = 0; y < hy; y++)
+      for (uint32_t x = 0; x < hx; x++) {
+        uint32_t v = 0;
+        for (uint32_t k = 0; k < 8u; k++)
+          v += src[((size_t)(2u * z + (k >> 2)) * sy + 2u * y + ((k >> 1) & 1u)) * sx + 2u * x +
+                   (k & 1u)];
+        dst[((size_t)z * hy + y) * hx + x] = (uint8_t)(v / 8u);
+      }
+}
+
+static int64_t clampi64(int64_t v, int64_t lo, int64_t hi) { return v < lo ? lo : v > hi ? hi : v; }
+
+void orc_clip_fill(const uint8_t *vox, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t depth_max,
+                   uint32_t z0, const float orig[6][2], uint8_t *const tex[6]) {
+  const uint32_t T = 2048u;
+  uint8_t *pyr[6] = {0};
+  uint32_t pd[6][3];
+  pd[0][0] = nx, pd[0][1] = ny, pd[0][2] = nz;
+  for (int l = 1; l < 6; l++)
+    for (int a = 0; a < 3; a++) pd[l][a] = pd[l - 1][a] / 2u;
+  /* the pyramid: half = down2(volume), level l = down2(level l-1) */
+  const uint8_t *prev = vox;
+  for (int l = 1; l < 6; l++) {
+    size_t n = (size_t)pd[l][0] * pd[l][1] * pd[l][2];
+    pyr[l] = malloc(n ? n : 1u);
+    if (!pyr[l]) goto out;
+    if (n) clip_down2(prev, pd[l - 1][0], pd[l - 1][1], pd[l - 1][2], pyr[l]);
+    prev = pyr[l];
+  }
+  for (int l = 0; l < 6; l++) {
+    uint32_t wzl = depth_max / (1u << l) + 3u;
+    if (wzl < 4u) wzl = 4u;
+    int64_t s = (int64_t)1 << l;
+    int64_t ox = (int64_t)orig[l][0], oy = (int64_t)orig[l][1];
+    int64_t vx0 = ox / s - 1, vy0 = oy / s - 1; /* texel 0 in level voxels */
+    for (uint32_t k = 0; k < wzl; k++) {
+      int64_t ls = (int64_t)(z0 >> l) + k;
+      uint8_t *dst = tex[l] + (size_t)(ls % wzl) * T * T;
+      for (uint32_t ty = 0; ty < T; ty++)
+        for (uint32_t tx = 0; tx < T; tx++) {
+          uint32_t v = 0;
+          if (l == 0) { /* produce_slice level 0: decode_region_clamped (vkclip.c:138-176) */
+            if (ls < (int64_t)nz)
+              v = vox[((size_t)ls * ny + (size_t)clampi64(vy0 + ty, 0, ny - 1)) * nx +
+                      (size_t)clampi64(vx0 + tx, 0, nx - 1)];
+          } else if (l == 1) { /* full-resolution 2^3 box (vkclip.c:181-199) */
+            for (uint32_t q = 0; q < 8u; q++) {
+              int64_t z = 2 * ls + (q >> 2);
+              if (z >= (int64_t)nz) continue;
+              int64_t x = clampi64(2 * (vx0 + tx) + (q & 1u), 0, nx - 1);
+              int64_t y = clampi64(2 * (vy0 + ty) + ((q >> 1) & 1u), 0, ny - 1);
+              v += vox[((size_t)z * ny + (size_t)y) * nx + (size_t)x];
+            }
+            v /= 8u;
+          } else if (ls < (int64_t)pd[l][2] && pd[l][0] && pd[l][1]) {
+            /* produce_from_pyramid (vkclip.c:101-132): rows and columns
+             * clamped at the level's extent */
+            int64_t x = clampi64(vx0 + tx, 0, pd[l][0] - 1);
+            int64_t y = clampi64(vy0 + ty, 0, pd[l][1] - 1);
+            v = pyr[l][((size_t)ls * pd[l][1] + (size_t)y) * pd[l][0] + (size_t)x];
+          }
+          dst[(size_t)ty * T + tx] = (uint8_t)v;
+        }
+    }
+  }
+out:
+  for (int l = 1; l < 6; l++) free(pyr[l]);
 }
 
 void orc_slab_fill(const uint8_t *vox, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t wz,

@@ -47,6 +47,29 @@ typedef struct orc_slab {
   const uint8_t *tiles[8];
 } orc_slab;
 
+/* XY clipmap (src/core/clip.h, raycast.slang:357-408): level l is a
+ * 2048 x 2048 x wzl[l] texture, ring layer ls % wzl[l] holding level
+ * slice ls; ox, oy are the level origins (clip_orig), valid the level mask,
+ * nx the volume width and z0 the window start. */
+typedef struct orc_clip {
+  uint32_t wzl[6];
+  const uint8_t *lev[6];
+  float ox[6], oy[6];
+  uint32_t valid, nx, z0;
+} orc_clip;
+
+/* Virtual slab (src/core/vslab.h, raycast.slang:321-367): level l
+ * (spacing 1, 4, 8, 16, 32; gx = 0 absent) has gx x gy tiles from tile
+ * base[l] of the pool, each (px + 2)^2 texels by wz ring slices; table holds
+ * four words per base tile (key, za, zb, 0).  Views carry the window origin
+ * and grids in their frame parameters. */
+typedef struct orc_vslab {
+  uint32_t px, wz, ntiles;
+  uint32_t gx[5], gy[5], base[5];
+  uint8_t *tiles;
+  uint32_t *table;
+} orc_vslab;
+
 /* Brick cache.  LOD mode (brick_mode with the LOD flag): the page table in
  * render3d's word format and a pool of 128^3 slots (slot s at
  * pool + s * 128^3, x fastest).  Single-level mode (no LOD flag,
@@ -63,8 +86,10 @@ typedef struct orc_bricks {
    * 3D ink, labels, registration; NULL when absent), sampled per
    * src/shaders/raycast.slang:45-115,872-914,1000-1014,1032-1036 */
   const uint8_t *ovl[4];
-  /* slab views (slab_grid != 0) sample this instead */
+  /* slab views (slab_grid != 0) and clip views (clip_valid != 0) sample these */
   const orc_slab *slab;
+  const orc_clip *clip;
+  const orc_vslab *vslab; /* virtual-slab views (slab_grid bit 24) */
 } orc_bricks;
 
 typedef struct orc_opts {
@@ -158,6 +183,25 @@ uint32_t orc_slab_layout(uint32_t nx, uint32_t ny, uint32_t lev[8][4], uint32_t 
  * must hold gx * gy * (px + 2) * (py + 2) * wz bytes of level l. */
 void orc_slab_fill(const uint8_t *vox, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t wz,
                    uint32_t z0, uint8_t *const tiles[8]);
+
+/* Clipmap level textures for the window from z0 with the given level
+ * origins (vkclip.c:101-185, tools/mkpyramid): level 0 the volume, level 1
+ * its truncating 2^3 box with coordinates clamped at full resolution,
+ * levels 2..5 the tight truncating 2^3 box pyramid clamped at its own
+ * extent; texel (tx, ty) is level voxel (ox / 2^l - 1 + tx, oy / 2^l - 1 +
+ * ty); slices outside the volume are zero.  wzl[l] = max(depth_max / 2^l
+ * + 3, 4); tex[l] holds 2048 * 2048 * wzl[l] bytes. */
+void orc_clip_fill(const uint8_t *vox, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t depth_max,
+                   uint32_t z0, const float orig[6][2], uint8_t *const tex[6]);
+
+/* One virtual-slab fill (vkbackend.c:5985-6125): slices [zs0, zs0 + nz) of
+ * base cell (cx, cy) into its base tile (texel (tx, ty) holds world voxel
+ * (cx px - 1 + tx, cy px - 1 + ty) clamped up to 0, zero past the volume's
+ * far edges), then each present pyramid level's strip (truncating 4x4 box
+ * of the payload, then 2x2 boxes) into the tiles it overlaps, aprons
+ * included (vkbackend.c:6032-6057).  Ring layer of slice z: z % wz. */
+void orc_vslab_fill(orc_vslab *v, const uint8_t *vox, uint32_t nx, uint32_t ny, int64_t cx,
+                    int64_t cy, int64_t zs0, uint32_t nz);
 
 /* Single-level brick atlas from a cubic volume of edge bpa * 128: atlas
  * level 0 ((abpa * 128)^3, slot s at (s % abpa, s / abpa % abpa,

@@ -134,6 +134,29 @@ class StreamCand(C.Structure):
     _fields_ = [("d2", C.c_float), ("brick", C.c_uint32), ("priority", C.c_uint32)]
 
 
+class VslabLayout(C.Structure):
+    _fields_ = [("nx", C.c_uint64), ("ny", C.c_uint64), ("nz", C.c_uint64),
+                ("W", C.c_uint32), ("H", C.c_uint32), ("D", C.c_uint32),
+                ("px", C.c_uint32), ("wz", C.c_uint32), ("z_margin", C.c_uint32),
+                ("x0", C.c_int64), ("y0", C.c_int64), ("z0", C.c_int64),
+                ("s", C.c_uint32 * 5), ("gx", C.c_uint32 * 5), ("gy", C.c_uint32 * 5),
+                ("base", C.c_uint32 * 5), ("ntiles", C.c_uint32)]
+
+
+class VslabCell(C.Structure):
+    _fields_ = [("cx", C.c_int64), ("cy", C.c_int64), ("za", C.c_int64), ("zb", C.c_int64)]
+
+
+class VslabJob(C.Structure):
+    _fields_ = [("cx", C.c_int64), ("cy", C.c_int64), ("zs0", C.c_int64), ("nz", C.c_uint32),
+                ("prio", C.c_uint32)]
+
+
+class VslabStats(C.Structure):
+    _fields_ = [("jobs", C.c_uint32), ("slices", C.c_uint32), ("pending", C.c_uint32),
+                ("pad", C.c_uint32), ("origin", C.c_int64 * 3)]
+
+
 def _load() -> C.CDLL:
     if not os.path.exists(LIB_PATH):
         raise ImportError(f"{LIB_PATH} is not built; run python render3d_b200/build.py")
@@ -158,6 +181,22 @@ def _load() -> C.CDLL:
         "r3d_cuda_shard_build": (I, [P, U32, P, U32, P]),
         "r3d_cuda_bricks_overlay_load": (I, [P, U32, P]),
         "r3d_cuda_slab_build": (I, [P, C.POINTER(VolumeDesc), P, U32, U32]),
+        "r3d_cuda_clip_build": (I, [P, C.POINTER(VolumeDesc), P, U32]),
+        "r3d_cuda_clip_frame": (I, [P, C.c_double, C.c_double, C.c_uint64, P]),
+        "r3d_cuda_clip_params": (None, [P, P]),
+        "r3d_cuda_clip_read": (I, [P, U32, U32, P]),
+        "r3d_cuda_vslab_begin": (I, [P, C.POINTER(VolumeDesc), P, U32, U32, U32, U32]),
+        "r3d_cuda_vslab_frame": (I, [P, C.c_double, C.c_double, C.c_int64, U32, P, P]),
+        "r3d_cuda_vslab_params": (None, [P, P]),
+        "r3d_cuda_vslab_layout": (I, [P, P]),
+        "r3d_cuda_vslab_read": (I, [P, U32, P]),
+        "r3d_cuda_vslab_table": (I, [P, P]),
+        "r3d_host_vslab_init": (I, [P, C.c_uint64, C.c_uint64, C.c_uint64, U32, U32, U32, U32]),
+        "r3d_host_vslab_zrange": (None, [P, C.c_int64, P, P]),
+        "r3d_host_vslab_range": (None, [P, U32, C.c_int64, C.c_uint64, U32, P, P]),
+        "r3d_host_vslab_plan": (U32, [P, P, C.c_double, C.c_double, C.c_int64, U32, P, U32]),
+        "r3d_host_vslab_apply": (U32, [P, P, P, C.c_int64]),
+        "r3d_host_vslab_key": (U32, [C.c_int64, C.c_int64]),
         "r3d_cuda_slab_window": (I, [P, U32]),
         "r3d_cuda_slab_params": (None, [P, P]),
         "r3d_cuda_slab_read": (I, [P, U32, U32, P, P]),
@@ -263,6 +302,32 @@ def stream_desired(page: np.ndarray, eye, fwd, half_tan: float, pixel_cone: floa
                                     slice_z0, slice_depth, gate, _ptr(mark), out, page.size)
     a = np.ctypeslib.as_array(out)[:n]
     return a.copy()
+
+
+class VslabHost:
+    """The virtual slab's host layout and fill scheduler (r3d_host_vslab_*):
+    a layout, its ledger of base tiles and one frame's plan + ledger update,
+    without a device."""
+
+    def __init__(self, nx, ny, nz, W, H, D, z_margin=0):
+        self.v = VslabLayout()
+        if lib.r3d_host_vslab_init(C.byref(self.v), nx, ny, nz, W, H, D, z_margin) != 0:
+            raise ValueError("vslab layout")
+        n = self.v.gx[0] * self.v.gy[0]
+        self.cells = (VslabCell * n)()
+        for c in self.cells:
+            c.cx = c.cy = -(1 << 63)
+
+    def frame(self, fx, fy, z0, budget):
+        """Plans one frame, records its jobs as finished; returns them as
+        (cx, cy, zs0, nz) tuples."""
+        jobs = (VslabJob * 112)()
+        n = lib.r3d_host_vslab_plan(C.byref(self.v), self.cells, fx, fy, z0, budget, jobs, 112)
+        out = []
+        for j in jobs[:n]:
+            lib.r3d_host_vslab_apply(C.byref(self.v), self.cells, C.byref(j), self.v.z0)
+            out.append((j.cx, j.cy, j.zs0, j.nz))
+        return out
 
 
 def tf_preset(idx: int) -> np.ndarray:
@@ -455,6 +520,57 @@ class Context:
         st = StreamStats()
         self._check(lib.r3d_cuda_stream_update(self.h, C.byref(v), C.byref(st)))
         return {k: getattr(st, k) for k, _ in StreamStats._fields_}
+
+    def clip_build(self, vol, depth_max: int) -> None:
+        nz, ny, nx = vol.shape
+        d = VolumeDesc(nx, ny, nz, 128, 1.0)
+        self._check(lib.r3d_cuda_clip_build(self.h, C.byref(d), _ptr(vol), depth_max))
+
+    def clip_frame(self, fx: float, fy: float, z0: int, p: "FrameParams | None" = None) -> None:
+        self._check(lib.r3d_cuda_clip_frame(self.h, fx, fy, z0,
+                                            C.byref(p) if p is not None else None))
+
+    def clip_params(self, p: "FrameParams") -> None:
+        lib.r3d_cuda_clip_params(self.h, C.byref(p))
+
+    def vslab_begin(self, vol, W: int, H: int, D: int, z_margin: int = 0) -> None:
+        nz, ny, nx = vol.shape
+        d = VolumeDesc(nx, ny, nz, 128, 1.0)
+        self._check(lib.r3d_cuda_vslab_begin(self.h, C.byref(d), _ptr(vol), W, H, D, z_margin))
+
+    def vslab_frame(self, fx: float, fy: float, z0: int, budget: int,
+                    p: "FrameParams | None" = None) -> dict:
+        st = VslabStats()
+        self._check(lib.r3d_cuda_vslab_frame(self.h, fx, fy, z0, budget,
+                                             C.byref(p) if p is not None else None,
+                                             C.byref(st)))
+        return {"jobs": st.jobs, "slices": st.slices, "pending": st.pending,
+                "origin": tuple(st.origin)}
+
+    def vslab_params(self, p: "FrameParams") -> None:
+        lib.r3d_cuda_vslab_params(self.h, C.byref(p))
+
+    def vslab_layout(self) -> VslabLayout:
+        v = VslabLayout()
+        self._check(lib.r3d_cuda_vslab_layout(self.h, C.byref(v)))
+        return v
+
+    def vslab_read(self, tile: int) -> np.ndarray:
+        v = self.vslab_layout()
+        out = np.empty((v.wz, v.px + 2, v.px + 2), np.uint8)
+        self._check(lib.r3d_cuda_vslab_read(self.h, tile, _ptr(out)))
+        return out
+
+    def vslab_table(self) -> np.ndarray:
+        v = self.vslab_layout()
+        out = np.empty((v.gx[0] * v.gy[0], 4), np.uint32)
+        self._check(lib.r3d_cuda_vslab_table(self.h, _ptr(out)))
+        return out
+
+    def clip_read(self, level: int, layer: int) -> np.ndarray:
+        out = np.empty((2048, 2048), np.uint8)
+        self._check(lib.r3d_cuda_clip_read(self.h, level, layer, _ptr(out)))
+        return out
 
     def slab_build(self, vol, wz: int, z0: int = 0) -> None:
         """Tiled slab over a (nz, ny, nx) volume: a ring of wz slices from z0."""

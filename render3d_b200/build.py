@@ -41,8 +41,13 @@ CC = shutil.which("gcc", path="/usr/bin:/bin") or "gcc"
 C_FLAGS = ["-O2", "-std=c2x", "-D_GNU_SOURCE", "-fPIC", "-ffp-contract=off", "-Wall",
            "-Wextra", "-I" + INC, "-I" + os.path.join(CUDA_HOME, "include")]
 
-CU_SOURCES = ["r3d_ctx.cu", "r3d_fwd.cu", "r3d_persist.cu", "r3d_noalloc.cu", "r3d_diff.cu", "r3d_batch.cu",
-              "r3d_phantom.cu", "r3d_diag.cu", "r3d_shard.cu", "r3d_overlay.cu", "r3d_stream.cu", "r3d_slab.cu"]
+CU_SOURCES = ["r3d_ctx.cu", "r3d_fwd.cu", "r3d_persist.cu", "r3d_noalloc.cu", "r3d_diff.cu",
+              "r3d_batch.cu", "r3d_phantom.cu", "r3d_diag.cu", "r3d_shard.cu", "r3d_overlay.cu",
+              "r3d_stream.cu", "r3d_slab.cu", "r3d_clip.cu", "r3d_vslab.cu"]
+# sources compiled once more per sampling path (-DR3D_FWD_PATH=p), so the
+# paths' raycast kernels compile in parallel
+PER_PATH = {"r3d_fwd.cu", "r3d_persist.cu"}
+N_PATHS = 6
 C_SOURCES = ["r3d_render.c", "r3d_host.c"]
 CLI_SOURCES = ["r3d_headless.c"]
 
@@ -72,24 +77,41 @@ def _run(cmd: list[str], log=None, verbose=False) -> None:
         raise RuntimeError("build step failed: " + " ".join(cmd[:3]))
 
 
+def _compile_jobs() -> list[tuple[list[str], str, str]]:
+    """(compiler command without -c/-o, source, object) of every object."""
+    jobs = []
+    for src in CU_SOURCES:
+        s = os.path.join(CSRC, src)
+        jobs.append(([NVCC] + NVCC_FLAGS, s, os.path.join(BUILD, src + ".o")))
+        if src in PER_PATH:
+            for p in range(N_PATHS):
+                jobs.append(([NVCC] + NVCC_FLAGS + [f"-DR3D_FWD_PATH={p}"], s,
+                             os.path.join(BUILD, f"{src}.p{p}.o")))
+    for src in C_SOURCES:
+        jobs.append(([CC] + C_FLAGS, os.path.join(CSRC, src), os.path.join(BUILD, src + ".o")))
+    return jobs
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
-    """Compiles whatever is out of date; returns the library path."""
+    """Compiles whatever is out of date, in parallel; returns the library path."""
+    import concurrent.futures as cf
+    import io
     os.makedirs(BUILD, exist_ok=True)
     hdrs = _headers()
-    objs = []
+    jobs = _compile_jobs()
+    objs = [o for _, _, o in jobs]
+    todo = [(cmd, s, o) for cmd, s, o in jobs if force or _newer(o, [s] + hdrs)]
     with open(os.path.join(BUILD, "ptxas.log"), "a") as log:
-        for src in CU_SOURCES:
-            s = os.path.join(CSRC, src)
-            o = os.path.join(BUILD, src + ".o")
-            if force or _newer(o, [s] + hdrs):
-                _run([NVCC] + NVCC_FLAGS + ["-c", s, "-o", o], log, verbose)
-            objs.append(o)
-        for src in C_SOURCES:
-            s = os.path.join(CSRC, src)
-            o = os.path.join(BUILD, src + ".o")
-            if force or _newer(o, [s] + hdrs):
-                _run([CC] + C_FLAGS + ["-c", s, "-o", o], log, verbose)
-            objs.append(o)
+        def one(job):
+            cmd, s, o = job
+            buf = io.StringIO()
+            try:
+                _run(cmd + ["-c", s, "-o", o], buf, verbose)
+            finally:
+                log.write(buf.getvalue())
+        with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
+            for f in [ex.submit(one, j) for j in todo]:
+                f.result()
         if force or _newer(LIB, objs):
             _run([NVCC] + GENCODE + ["-shared", "-o", LIB] + objs +
                  ["-lcudart", "-lpthread", "-lm"], log, verbose)

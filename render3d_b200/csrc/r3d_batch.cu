@@ -98,7 +98,7 @@ extern "C" int r3d_cuda_batch_create(r3d_cuda_ctx *c, const r3d_cuda_request *re
       }
       b->ntiles[shape][g] = tiles;
     }
-    e = cudaMemcpy(b->dviews[shape], hv.data(), sizeof(DevView) * n, cudaMemcpyHostToDevice);
+    e = copy_sync(c->stream, b->dviews[shape], hv.data(), sizeof(DevView) * n);
   }
   if (e != cudaSuccess) {
     r3d_cuda_batch_destroy(b);

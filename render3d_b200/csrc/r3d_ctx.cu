@@ -202,6 +202,8 @@ r3d::DevScene r3d_cuda_ctx::scene() const {
   s.br = br;
   s.sh = sh;
   s.sl = sl;
+  s.cl = cl;
+  s.vs = vs;
   s.status = status;
   s.alpha_cutoff = alpha_cutoff;
   s.tf_zero_t = tf_zero_t;
@@ -237,7 +239,12 @@ int r3d_cuda_create(int device, r3d_cuda_ctx **out) {
     r3d_cuda_destroy(c);
     return R3D_E_CUDA;
   }
-  cudaMemset(c->status, 0, sizeof(uint32_t));
+  if (cudaMemsetAsync(c->status, 0, sizeof(uint32_t), c->stream) != cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess) {
+    cudaGetLastError();
+    r3d_cuda_destroy(c);
+    return R3D_E_CUDA;
+  }
   for (int k = 0; k < r3d_cuda_ctx::kRing; k++)
     if (cudaEventCreateWithFlags(&c->ring_ev[k], cudaEventDisableTiming) != cudaSuccess) {
       r3d_cuda_destroy(c);
@@ -274,6 +281,8 @@ void r3d_cuda_destroy(r3d_cuda_ctx *c) {
   cudaFree(c->total);
   stream_reset(c);
   slab_reset(c);
+  clip_reset(c);
+  vslab_reset(c);
   if (c->page_ev) cudaEventDestroy(c->page_ev);
   cudaFree(c->diff_q);
   cudaFree(c->tape);
@@ -300,7 +309,7 @@ int r3d_cuda_status(r3d_cuda_ctx *c, uint32_t *bits, int clear) {
   uint32_t v = 0;
   R3D_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   R3D_CUDA_TRY(c, cudaMemcpy(&v, c->status, 4, cudaMemcpyDeviceToHost));
-  if (clear) R3D_CUDA_TRY(c, cudaMemset(c->status, 0, 4));
+  if (clear) R3D_CUDA_TRY(c, cudaMemsetAsync(c->status, 0, 4, c->stream));
   if (bits) *bits = v;
   return R3D_OK;
 }
@@ -659,9 +668,9 @@ int r3d_cuda_bricks_load(r3d_cuda_ctx *c, const uint32_t *page, uint32_t page_wo
   size_t pool_bytes = (size_t)(nslots ? nslots : 1u) * (128u * 128u * 128u);
   cudaError_t e = cudaMalloc(&dpage, (size_t)page_words * 4);
   if (e == cudaSuccess) e = cudaMalloc(&dpool, pool_bytes);
-  if (e == cudaSuccess) e = cudaMemcpy(dpage, page, (size_t)page_words * 4, cudaMemcpyDefault);
+  if (e == cudaSuccess) e = copy_sync(c->stream, dpage, page, (size_t)page_words * 4);
   if (e == cudaSuccess && nslots)
-    e = cudaMemcpy(dpool, slots, (size_t)nslots * (128u * 128u * 128u), cudaMemcpyDefault);
+    e = copy_sync(c->stream, dpool, slots, (size_t)nslots * (128u * 128u * 128u));
   if (e != cudaSuccess) {
     cudaFree(dpage);
     cudaFree(dpool);
@@ -746,9 +755,39 @@ int prepare_view(r3d_cuda_ctx *c, const r3d_frame_params &in, uint32_t out_w,
                         uint32_t out_h, r3d_frame_params &pc) {
   pc = in;
   if (in.mode >= R3D_MODE_COUNT) return fail(c, R3D_E_INVALID, "view: mode %u", in.mode);
-  if (in.clip_valid)
-    return fail(c, R3D_E_UNSUPPORTED, "view: clipmap sampling is not implemented");
-  if (in.slab_grid) {  // tiled slab: the view must describe the loaded window
+  if (in.clip_valid) {  // clipmap: the view must describe the loaded levels
+    if (!c->have_clip) return fail(c, R3D_E_STATE, "view: no clipmap loaded");
+    r3d_frame_params ref;
+    memset(&ref, 0, sizeof ref);
+    r3d_cuda_clip_params(c, &ref);
+    if (in.clip_valid != ref.clip_valid || in.slab_z0 != ref.slab_z0 ||
+        in.slab_nx != ref.slab_nx || in.slab_ny != ref.slab_ny || in.slab_wz != ref.slab_wz ||
+        memcmp(in.clip_orig, ref.clip_orig, sizeof ref.clip_orig) || in.brick_mode ||
+        in.slab_grid)
+      return fail(c, R3D_E_INVALID, "view: clipmap parameters do not match the loaded levels "
+                                    "(r3d_cuda_clip_params)");
+    if (in.slab_depth < 1u || in.slab_depth > in.slab_wz)
+      return fail(c, R3D_E_INVALID, "view: slab_depth %u not in [1, %u]", in.slab_depth,
+                  in.slab_wz);
+    if (in.overlay_flags & kOvlAtlases)
+      return fail(c, R3D_E_UNSUPPORTED, "view: overlay atlases need the LOD brick cache");
+  } else if (in.slab_grid & kVslabGrid) {  // virtual slab: the view must describe the window
+    if (!c->have_vslab) return fail(c, R3D_E_STATE, "view: no virtual slab loaded");
+    r3d_frame_params ref;
+    memset(&ref, 0, sizeof ref);
+    r3d_cuda_vslab_params(c, &ref);
+    if (in.slab_grid != ref.slab_grid || in.brick_mode != ref.brick_mode ||
+        in.slab_wz != ref.slab_wz || in.slab_z0 != ref.slab_z0 || in.slab_nx != ref.slab_nx ||
+        in.slab_ny != ref.slab_ny || in.slab_px != ref.slab_px || in.slab_py != ref.slab_py ||
+        in.slab_x0 != ref.slab_x0 || in.slab_y0 != ref.slab_y0)
+      return fail(c, R3D_E_INVALID, "view: virtual-slab parameters do not match the loaded "
+                                    "window (r3d_cuda_vslab_params)");
+    if (in.slab_depth < 1u || in.slab_depth > c->vsl.D)
+      return fail(c, R3D_E_INVALID, "view: slab_depth %u not in [1, %u]", in.slab_depth,
+                  c->vsl.D);
+    if (in.overlay_flags & kOvlAtlases)
+      return fail(c, R3D_E_UNSUPPORTED, "view: overlay atlases need the LOD brick cache");
+  } else if (in.slab_grid) {  // tiled slab: the view must describe the loaded window
     if (!c->have_slab) return fail(c, R3D_E_STATE, "view: no slab loaded");
     r3d_frame_params ref;
     memset(&ref, 0, sizeof ref);
@@ -777,14 +816,16 @@ int prepare_view(r3d_cuda_ctx *c, const r3d_frame_params &in, uint32_t out_w,
   }
   if (!(in.max_mip >= 0.0f)) return fail(c, R3D_E_INVALID, "view: max_mip must be >= 0");
   if (!(in.step_voxels > 0.0f)) return fail(c, R3D_E_INVALID, "view: step_voxels must be > 0");
-  if (in.brick_mode & R3D_BRICK_LOD_FLAG) {
+  if (in.slab_grid & kVslabGrid) {
+    // brick_mode holds the pyramid grids (checked above)
+  } else if (in.brick_mode & R3D_BRICK_LOD_FLAG) {
     if (!c->have_bricks) return fail(c, R3D_E_STATE, "view: no brick cache loaded");
   } else if (in.brick_mode) {
     if (!c->have_shard) return fail(c, R3D_E_STATE, "view: no single-level brick atlas loaded");
     if (in.brick_mode != r3d_cuda_shard_mode(c))
       return fail(c, R3D_E_INVALID, "view: brick_mode 0x%x does not match the atlas (0x%x)",
                   in.brick_mode, r3d_cuda_shard_mode(c));
-  } else if (!in.slab_grid && !c->have_cube) {
+  } else if (!in.slab_grid && !in.clip_valid && !c->have_cube) {
     return fail(c, R3D_E_STATE, "view: no volume uploaded");
   }
   uint32_t ox = in.view_org & 0xffffu, oy = (in.view_org >> 16) & 0xffffu;

@@ -191,27 +191,41 @@ static cudaError_t launch_p(const r3d_frame_params &pc, const DevScene &s, bool 
   }
 }
 
+#ifdef R3D_FWD_PATH
+// The build compiles this file once per sampling path (R3D_FWD_PATH = 0..5)
+// so that the paths' kernels compile in parallel; each object defines its
+// path's entry.
+template <>
+cudaError_t launch_path<R3D_FWD_PATH>(const r3d_frame_params &pc, const DevScene &s, bool fast,
+                                      const uchar4 *lut, uint8_t *img, uint32_t out_w,
+                                      uint32_t *steps, uint32_t *mip, unsigned long long *total,
+                                      unsigned long long *cnt, uint32_t shade, cudaStream_t st) {
+  return launch_p<R3D_FWD_PATH>(pc, s, fast, lut, img, out_w, steps, mip, total, cnt, shade, st);
+}
+#else
 cudaError_t launch_view(const r3d_cuda_ctx *c, const r3d_frame_params &pc, uint8_t *img,
                         uint32_t out_w, uint32_t *steps, uint32_t *mip_index,
                         unsigned long long *total, unsigned long long *counters,
                         cudaStream_t stream) {
-  DevScene s = c->scene();
-  bool fast = c->quality == R3D_QUALITY_FAST;
+  const DevScene s = c->scene();
+  const bool fast = c->quality == R3D_QUALITY_FAST;
   const uint32_t shade = c->sched.shade_group;
+#define R3D_PATH_CASE(P)                                                                   \
+  case P:                                                                                  \
+    return launch_path<P>(pc, s, fast, c->lut, img, out_w, steps, mip_index, total, counters, \
+                          shade, stream)
   switch (path_of_view(pc)) {
-    case PATH_SLAB:
-      return launch_p<PATH_SLAB>(pc, s, fast, c->lut, img, out_w, steps, mip_index, total,
-                                 counters, shade, stream);
-    case PATH_LOD_BRICKS:
-      return launch_p<PATH_LOD_BRICKS>(pc, s, fast, c->lut, img, out_w, steps, mip_index, total,
-                                       counters, shade, stream);
-    case PATH_SHARD:
-      return launch_p<PATH_SHARD>(pc, s, fast, c->lut, img, out_w, steps, mip_index, total,
-                                  counters, shade, stream);
+    R3D_PATH_CASE(PATH_VSLAB);
+    R3D_PATH_CASE(PATH_CLIP);
+    R3D_PATH_CASE(PATH_SLAB);
+    R3D_PATH_CASE(PATH_LOD_BRICKS);
+    R3D_PATH_CASE(PATH_SHARD);
     default:
-      return launch_p<PATH_CUBE>(pc, s, fast, c->lut, img, out_w, steps, mip_index, total,
-                                 counters, shade, stream);
+      return launch_path<PATH_CUBE>(pc, s, fast, c->lut, img, out_w, steps, mip_index, total,
+                                    counters, shade, stream);
   }
+#undef R3D_PATH_CASE
 }
+#endif
 
 }  // namespace r3d

@@ -417,3 +417,209 @@ uint32_t r3d_host_stream_desired(const uint32_t *page, uint32_t page_words, cons
   qsort(out, n, sizeof *out, stream_cand_cmp);
   return n;
 }
+
+/* ---- virtual slab layout and fill planner ---- */
+
+static const uint32_t vs_scale[R3D_VS_LEVELS] = {1u, 4u, 8u, 16u, 32u};
+
+int r3d_host_vslab_init(r3d_vslab_layout *v, uint64_t nx, uint64_t ny, uint64_t nz, uint32_t W,
+                        uint32_t H, uint32_t D, uint32_t z_margin) {
+  const uint64_t ring = (uint64_t)D + 2u + 2u * (uint64_t)z_margin;
+  if (!v || W < 64u || H < 64u || W > nx || H > ny || D < 2u || D > 2044u || D > nz ||
+      ring > 2046u || ring > nz)
+    return -1;
+  memset(v, 0, sizeof *v);
+  v->nx = nx, v->ny = ny, v->nz = nz;
+  v->W = W, v->H = H, v->D = D;
+  v->wz = (uint32_t)ring;
+  v->z_margin = z_margin;
+  const uint32_t m = W > H ? W : H;
+  uint32_t px = (m / 8u + 31u) & ~31u;
+  px = px < 64u ? 64u : (px > 2016u ? 2016u : px);
+  while (px > 64u && (uint64_t)(px + 2u) * (px + 2u) * v->wz > (3ull << 30)) px -= 32u;
+  v->px = px;
+  /* a movable axis adds a straddle tile and a prefetch tile */
+  const uint32_t ex = W < nx ? 2u : 0u, ey = H < ny ? 2u : 0u;
+  uint32_t nt = 0;
+  for (uint32_t l = 0; l < R3D_VS_LEVELS; l++) {
+    const uint64_t cs = (uint64_t)px * vs_scale[l];
+    v->s[l] = vs_scale[l];
+    v->base[l] = nt;
+    if (l && m / vs_scale[l] < 1024u) continue; /* pyramid level not needed */
+    v->gx[l] = (uint32_t)((W + cs - 1u) / cs) + ex;
+    v->gy[l] = (uint32_t)((H + cs - 1u) / cs) + ey;
+    nt += v->gx[l] * v->gy[l];
+  }
+  v->ntiles = nt;
+  v->x0 = v->y0 = v->z0 = -1;
+  return 0;
+}
+
+void r3d_host_vslab_zrange(const r3d_vslab_layout *v, int64_t z0, int64_t *a, int64_t *b) {
+  int64_t za = z0 - (int64_t)v->z_margin;
+  if (za < 0) za = 0;
+  int64_t zb = za + (int64_t)v->wz;
+  if (zb > (int64_t)v->nz) {
+    zb = (int64_t)v->nz;
+    za = zb - (int64_t)v->wz;
+    if (za < 0) za = 0;
+  }
+  *a = za, *b = zb;
+}
+
+void r3d_host_vslab_range(const r3d_vslab_layout *v, uint32_t l, int64_t o, uint64_t n,
+                          uint32_t span, int64_t *c0, int64_t *c1) {
+  const int64_t cs = (int64_t)v->px * (int64_t)v->s[l];
+  int64_t a = o / cs, b = (o + (int64_t)span - 1) / cs;
+  const int64_t last = ((int64_t)n - 1) / cs;
+  *c0 = a < 0 ? 0 : a;
+  *c1 = b > last ? last : b;
+}
+
+uint32_t r3d_host_vslab_key(int64_t cx, int64_t cy) {
+  return ((uint32_t)cx & 1023u) | (((uint32_t)cy & 1023u) << 10) | 0x80000000u;
+}
+
+static uint32_t vs_slot(const r3d_vslab_layout *v, int64_t cx, int64_t cy) {
+  return (uint32_t)(cy % v->gy[0]) * v->gx[0] + (uint32_t)(cx % v->gx[0]);
+}
+
+static int64_t vs_max0(uint64_t n, uint32_t span) {
+  const int64_t m = (int64_t)n - (int64_t)span;
+  return m < 0 ? 0 : m;
+}
+
+uint32_t r3d_host_vslab_plan(r3d_vslab_layout *v, const r3d_vslab_cell *cells, double fx,
+                             double fy, int64_t z0, uint32_t budget, r3d_vslab_job *out,
+                             uint32_t cap) {
+  if (!v || !cells || (!out && cap)) return 0;
+  const int64_t px0 = v->x0, py0 = v->y0, pz0 = v->z0;
+  int64_t x0 = (int64_t)fx - v->W / 2, y0 = (int64_t)fy - v->H / 2;
+  x0 = x0 < 0 ? 0 : (x0 & ~(int64_t)15);
+  y0 = y0 < 0 ? 0 : (y0 & ~(int64_t)15);
+  if (x0 > vs_max0(v->nx, v->W)) x0 = vs_max0(v->nx, v->W) & ~(int64_t)15;
+  if (y0 > vs_max0(v->ny, v->H)) y0 = vs_max0(v->ny, v->H) & ~(int64_t)15;
+  if (z0 < 0) z0 = 0;
+  if (z0 > vs_max0(v->nz, v->D)) z0 = vs_max0(v->nz, v->D);
+  int64_t za_want, zb_want;
+  r3d_host_vslab_zrange(v, z0, &za_want, &zb_want);
+  int64_t vis_end = z0 + (int64_t)v->D + 2;
+  if (vis_end > (int64_t)v->nz) vis_end = (int64_t)v->nz;
+  const int up = pz0 < 0 || z0 >= pz0; /* direction of z travel */
+  v->x0 = x0, v->y0 = y0, v->z0 = z0;
+
+  int64_t cx0, cx1, cy0, cy1;
+  r3d_host_vslab_range(v, 0, x0, v->nx, v->W, &cx0, &cx1);
+  r3d_host_vslab_range(v, 0, y0, v->ny, v->H, &cy0, &cy1);
+  r3d_vslab_job jobs[64];
+  uint64_t dist[64];
+  uint32_t nj = 0;
+  const int64_t ccx = (x0 + v->W / 2) / (int64_t)v->px, ccy = (y0 + v->H / 2) / (int64_t)v->px;
+  const uint32_t mchunks = (v->z_margin + 15u) / 16u;
+  for (int64_t cy = cy0; cy <= cy1 && nj < 64u; cy++)
+    for (int64_t cx = cx0; cx <= cx1 && nj < 64u; cx++) {
+      const r3d_vslab_cell *c = &cells[vs_slot(v, cx, cy)];
+      r3d_vslab_job j = {cx, cy, z0, (uint32_t)(vis_end - z0), 0u};
+      const int held = c->cx == cx && c->cy == cy;
+      const int visible = held && c->za <= z0 && c->zb >= vis_end;
+      if (held) {
+        if (c->za <= za_want && c->zb >= zb_want) continue; /* whole range resident */
+        int64_t s0 = z0, s1 = vis_end;
+        if (!visible && c->za < vis_end && c->zb > z0) {
+          /* finish the visible span around what is held */
+          if (c->za > z0) {
+            s1 = c->za < vis_end ? c->za : vis_end;
+          } else {
+            s0 = c->zb > z0 ? c->zb : z0;
+          }
+        } else if (visible) {
+          /* grow the margin, 16 slices at a time, travel direction first */
+          int grow_up;
+          uint32_t extra;
+          if (up && c->zb < zb_want) {
+            grow_up = 1, extra = 0u;
+          } else if (!up && c->za > za_want) {
+            grow_up = 0, extra = 0u;
+          } else if (c->za > za_want) {
+            grow_up = 0, extra = mchunks;
+          } else {
+            grow_up = 1, extra = mchunks;
+          }
+          int64_t filled;
+          if (grow_up) {
+            s0 = c->zb;
+            s1 = s0 + 16 < zb_want ? s0 + 16 : zb_want;
+            filled = c->zb - vis_end;
+          } else {
+            s1 = c->za;
+            s0 = s1 - 16 > za_want ? s1 - 16 : za_want;
+            filled = z0 - c->za;
+          }
+          j.prio = 1u + extra + (uint32_t)(filled > 0 ? filled / 16 : 0);
+        }
+        j.zs0 = s0;
+        j.nz = (uint32_t)(s1 - s0);
+      }
+      const int64_t dx = cx - ccx, dy = cy - ccy;
+      dist[nj] = (uint64_t)(dx * dx + dy * dy);
+      jobs[nj++] = j;
+    }
+  /* exchange sort by (priority, distance), the reference's order */
+  for (uint32_t a = 0; a + 1u < nj; a++)
+    for (uint32_t b = a + 1u; b < nj; b++)
+      if (jobs[b].prio < jobs[a].prio || (jobs[b].prio == jobs[a].prio && dist[b] < dist[a])) {
+        r3d_vslab_job t = jobs[a];
+        jobs[a] = jobs[b], jobs[b] = t;
+        uint64_t td = dist[a];
+        dist[a] = dist[b], dist[b] = td;
+      }
+  uint32_t n = 0;
+  for (uint32_t k = 0; k < nj && n < budget && n < cap; k++) out[n++] = jobs[k];
+  /* prefetch the column / row past the window in the direction of motion */
+  if (px0 >= 0 && (x0 != px0 || y0 != py0)) {
+    int64_t pf[48][2];
+    uint32_t npf = 0;
+    const int64_t mxc = ((int64_t)v->nx - 1) / v->px, myc = ((int64_t)v->ny - 1) / v->px;
+    if (x0 != px0) {
+      const int64_t cxc = x0 > px0 ? cx1 + 1 : cx0 - 1;
+      if (cxc >= 0 && cxc <= mxc && cx1 - cx0 + 2 <= (int64_t)v->gx[0])
+        for (int64_t cy = cy0; cy <= cy1 && npf < 48u; cy++) pf[npf][0] = cxc, pf[npf++][1] = cy;
+    }
+    if (y0 != py0) {
+      const int64_t cyc = y0 > py0 ? cy1 + 1 : cy0 - 1;
+      if (cyc >= 0 && cyc <= myc && cy1 - cy0 + 2 <= (int64_t)v->gy[0])
+        for (int64_t cx = cx0; cx <= cx1 && npf < 48u; cx++) pf[npf][0] = cx, pf[npf++][1] = cyc;
+    }
+    for (uint32_t k = 0; k < npf && n < budget && n < cap; k++) {
+      const r3d_vslab_cell *c = &cells[vs_slot(v, pf[k][0], pf[k][1])];
+      if (c->cx == pf[k][0] && c->cy == pf[k][1] && c->za <= za_want && c->zb >= zb_want)
+        continue;
+      int dup = 0; /* a cell listed twice (both axes moved) fills once */
+      for (uint32_t m = 0; m < n; m++) dup |= out[m].cx == pf[k][0] && out[m].cy == pf[k][1];
+      if (dup) continue;
+      r3d_vslab_job j = {pf[k][0], pf[k][1], za_want, (uint32_t)(zb_want - za_want), 0u};
+      out[n++] = j;
+    }
+  }
+  return n;
+}
+
+uint32_t r3d_host_vslab_apply(const r3d_vslab_layout *v, r3d_vslab_cell *cells,
+                              const r3d_vslab_job *j, int64_t z0) {
+  int64_t za_want, zb_want;
+  r3d_host_vslab_zrange(v, z0, &za_want, &zb_want);
+  const uint32_t slot = vs_slot(v, j->cx, j->cy);
+  r3d_vslab_cell *c = &cells[slot];
+  const int64_t a = j->zs0, b = j->zs0 + (int64_t)j->nz;
+  if (c->cx != j->cx || c->cy != j->cy) {
+    c->za = a, c->zb = b;
+  } else {
+    if (a < c->za) c->za = a;
+    if (b > c->zb) c->zb = b;
+  }
+  c->cx = j->cx, c->cy = j->cy;
+  if (c->za < za_want) c->za = za_want;
+  if (c->zb > zb_want) c->zb = zb_want;
+  if (c->zb < c->za) c->zb = c->za;
+  return slot;
+}

@@ -57,6 +57,32 @@ struct r3d_cuda_ctx {
   bool have_slab = false;
   r3d::DevSlab sl{};
 
+  // XY clipmap: the source volume, its tight 2^3 box pyramid (levels 2..5),
+  // the level textures, their origins and the level slice each ring layer
+  // holds (-1: none)
+  uint8_t *clip_src = nullptr, *clip_pyr = nullptr, *clip_tex = nullptr;
+  size_t clip_pyr_off[r3d::kClipLevels] = {};
+  uint32_t clip_pyr_dim[r3d::kClipLevels][3] = {};
+  uint32_t clip_dims[3] = {0, 0, 0};
+  uint32_t clip_depth = 0;
+  int64_t clip_org[r3d::kClipLevels][2] = {};
+  std::vector<int64_t> clip_layer[r3d::kClipLevels];
+  bool have_clip = false;
+  r3d::DevClip cl{};
+
+  // virtual slab: the source volume, the tile pool, the validity table
+  // (device and its host copy), the ledger of the base tiles and scratch for
+  // one fill's pyramid strips
+  uint8_t *vs_src = nullptr, *vs_tiles = nullptr, *vs_strip = nullptr;
+  uint32_t *vs_table = nullptr;
+  std::vector<uint32_t> vs_table_host;
+  std::vector<r3d_vslab_cell> vs_cells;
+  std::vector<r3d_vslab_job> vs_jobs;
+  r3d_vslab_layout vsl{};
+  size_t vs_strip_off[r3d::kVsLevels] = {};
+  bool have_vslab = false;
+  r3d::DevVslab vs{};
+
   // single-level brick atlas: 4 mip levels, then the world-indexed
   // occupancy grid, in one allocation; page table of bpa^3 entries
   uint8_t *shard_buf = nullptr;
@@ -126,6 +152,22 @@ int fail(r3d_cuda_ctx *c, int code, const char *fmt, ...);
 int cuda_fail(r3d_cuda_ctx *c, cudaError_t e, const char *what);
 bool is_device_ptr(const void *p);
 
+// A copy in either direction (host or device source) ordered on stream s and
+// complete on return.  Uploads go through here rather than cudaMemcpy on the
+// legacy stream: the context's stream is non-blocking, so a device-to-device
+// or staged pageable cudaMemcpy is not ordered before its kernels.
+inline cudaError_t copy_sync(cudaStream_t s, void *dst, const void *src, size_t n) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, n, cudaMemcpyDefault, s);
+  return e == cudaSuccess ? cudaStreamSynchronize(s) : e;
+}
+
+// The forward launch of one sampling path (each defined in its own object).
+template <int PATH>
+cudaError_t launch_path(const r3d_frame_params &pc, const DevScene &s, bool fast,
+                        const uchar4 *lut, uint8_t *img, uint32_t out_w, uint32_t *steps,
+                        uint32_t *mip, unsigned long long *total, unsigned long long *cnt,
+                        uint32_t shade, cudaStream_t st);
+
 // Forward launch of one sanitized view into a device image.
 cudaError_t launch_view(const r3d_cuda_ctx *c, const r3d_frame_params &pc, uint8_t *img,
                         uint32_t out_w, uint32_t *steps, uint32_t *mip_index,
@@ -140,8 +182,10 @@ cudaError_t launch_view(const r3d_cuda_ctx *c, const r3d_frame_params &pc, uint8
 int build_blockmax(r3d_cuda_ctx *c);
 // Drops the streaming state (host store, shadows, LRU).
 void stream_reset(r3d_cuda_ctx *c);
-// Frees the tiled slab.
+// Frees the tiled slab / the clipmap.
 void slab_reset(r3d_cuda_ctx *c);
+void clip_reset(r3d_cuda_ctx *c);
+void vslab_reset(r3d_cuda_ctx *c);
 uint32_t atlas_bpa(uint32_t nslots);
 
 // Validates one view and clips its rect to the image (1: render, 0: empty

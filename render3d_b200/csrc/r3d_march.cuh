@@ -23,16 +23,31 @@ constexpr int kMaxLevels = 16;
 constexpr uint32_t kMaxSteps = 4096u;  // raycast.slang:123
 constexpr float kInv255 = 1.0f / 255.0f;
 
-enum Path { PATH_CUBE = 0, PATH_LOD_BRICKS = 1, PATH_SHARD = 2, PATH_SLAB = 3 };
+enum Path {
+  PATH_CUBE = 0,
+  PATH_LOD_BRICKS = 1,
+  PATH_SHARD = 2,
+  PATH_SLAB = 3,
+  PATH_CLIP = 4,
+  PATH_VSLAB = 5
+};
+constexpr int kNumPaths = 6;
+// slab_grid bit of a virtual-slab view (vkbackend.c:6629); a tiled slab's
+// slab_grid stops at bit 23 (its overview scale, at most 32, in bits 16..23)
+constexpr uint32_t kVslabGrid = 1u << 24;
 
-// Sampling path of a view: the tiled slab when slab_grid is set, else by
-// its brick_mode word (raycast.slang:134-140,157-160)
+// Sampling path of a view: the clipmap when clip_valid is set, the virtual
+// slab or the tiled slab by slab_grid, else by its brick_mode word
+// (raycast.slang:134-140,157-160)
 __host__ __device__ inline int path_of(uint32_t brick_mode) {
   return brick_mode == 0u ? PATH_CUBE
                           : (brick_mode & R3D_BRICK_LOD_FLAG) ? PATH_LOD_BRICKS : PATH_SHARD;
 }
 __host__ __device__ inline int path_of_view(const r3d_frame_params &pc) {
-  return pc.slab_grid ? PATH_SLAB : path_of(pc.brick_mode);
+  return pc.clip_valid                 ? PATH_CLIP
+         : (pc.slab_grid & kVslabGrid) ? PATH_VSLAB
+         : pc.slab_grid                ? PATH_SLAB
+                                       : path_of(pc.brick_mode);
 }
 
 struct DevCube {
@@ -106,11 +121,43 @@ struct DevSlab {
   DevSlabLevel lev[kSlabLevels];
 };
 
+// XY clipmap (raycast.slang:357-408, src/core/clip.h): 6 nested levels of
+// spacing 2^l, each a 2048 x 2048 x wzl texture (2046 payload texels and a
+// 1-texel apron) whose texel (tx, ty) holds level voxel (ox / 2^l - 1 + tx,
+// oy / 2^l - 1 + ty) and whose z is a ring of level slices.
+constexpr int kClipLevels = 6;
+struct DevClip {
+  const uint8_t *lev[kClipLevels];
+  uint32_t wzl[kClipLevels];
+  float ox[kClipLevels], oy[kClipLevels];  // clip_orig of the frame parameters
+  uint32_t valid;                          // clip_valid
+  float nx, z0;                            // slab_nx, slab_z0
+};
+
+// Virtual slab (raycast.slang:321-367, src/core/vslab.h): world-anchored
+// toroidal tile grids.  Level l (spacing 1, 4, 8, 16, 32) has gx x gy tiles
+// of (px + 2)^2 texels by a ring of wz slices; level cell (cx, cy) lives in
+// tile base + (cy mod gy) * gx + (cx mod gx), texel t of the tile holding
+// level texel cx * px - 1 + t.  gx = 0: level absent.  table holds four
+// words per base tile: the key of the cell it holds (0: none) and the world
+// slices [za, zb) it holds.
+constexpr int kVsLevels = 5;
+struct DevVslab {
+  const uint8_t *tiles;
+  const uint32_t *table;
+  size_t tile_bytes;
+  uint32_t px, wz;
+  uint32_t gx[kVsLevels], gy[kVsLevels], base[kVsLevels];
+  float x0, y0, z0, nx;  // the frame parameters slab_x0/y0/z0 and slab_nx (= W)
+};
+
 struct DevScene {
   DevCube cube;
   DevBricks br;
   DevShard sh;
   DevSlab sl;
+  DevClip cl;
+  DevVslab vs;
   uint32_t *status;
   float alpha_cutoff;
   float tf_zero_t;  // TF coordinates below this have alpha exactly 0
@@ -436,11 +483,8 @@ __device__ __forceinline__ float shard_fetch(const DevShard &h, float3 org, floa
 // A slab tile sampled at normalized (u, v, w) like the slab sampler
 // (src/vk/vkbackend.c:2203-2211): linear, clamp to edge in x and y (the
 // apron makes tiles seamless), REPEAT in w so the z ring wraps.
-__device__ __forceinline__ float slab_tile(const DevSlab &sl, int L, uint32_t k, float u, float v,
-                                           float w) {
-  const DevSlabLevel &lv = sl.lev[L];
-  const uint32_t tw = lv.px + 2u, th = lv.py + 2u, wz = sl.wz;
-  const uint8_t *g = sl.pool + lv.off + (size_t)k * tw * th * wz;
+__device__ __forceinline__ float tex_wrapz(const uint8_t *__restrict__ g, uint32_t tw, uint32_t th,
+                                           uint32_t wz, float u, float v, float w) {
   const float tx = clamp_(fmaf(u, (float)tw, -0.5f), 0.0f, (float)(tw - 1u));
   const float ty = clamp_(fmaf(v, (float)th, -0.5f), 0.0f, (float)(th - 1u));
   const float tz = fmaf(w, (float)wz, -0.5f);
@@ -459,6 +503,85 @@ __device__ __forceinline__ float slab_tile(const DevSlab &sl, int L, uint32_t k,
   const float c01 = lerp_((float)__ldg(r01 + x0), (float)__ldg(r01 + x1), fx);
   const float c11 = lerp_((float)__ldg(r11 + x0), (float)__ldg(r11 + x1), fx);
   return lerp_(lerp_(c00, c10, fy), lerp_(c01, c11, fy), fz) * kInv255;
+}
+
+__device__ __forceinline__ float slab_tile(const DevSlab &sl, int L, uint32_t k, float u, float v,
+                                           float w) {
+  const DevSlabLevel &lv = sl.lev[L];
+  const uint32_t tw = lv.px + 2u, th = lv.py + 2u, wz = sl.wz;
+  return tex_wrapz(sl.pool + lv.off + (size_t)k * tw * th * wz, tw, th, wz, u, v, w);
+}
+
+// sample_clip_level (raycast.slang:360-376): level l's texture at p, its z
+// ring wrapping in level slices
+__device__ __forceinline__ float clip_level(const DevClip &cl, int l, float3 p) {
+  const float s = (float)(1u << l);
+  const float wx = p.x * cl.nx, wy = p.y * cl.nx;
+  const float zw = (cl.z0 + 0.5f) + p.z * cl.nx;
+  const float u = ((wx - cl.ox[l]) / s + 1.0f) / 2048.0f;
+  const float v = ((wy - cl.oy[l]) / s + 1.0f) / 2048.0f;
+  const float zq = (zw / s) / (float)cl.wzl[l];
+  return tex_wrapz(cl.lev[l], 2048u, 2048u, cl.wzl[l], u, v, zq - floorf(zq));
+}
+
+// pick_clip_level (raycast.slang:380-395): the finest valid level holding
+// p from the desired one (coarser first once past the top), or -1
+__device__ __forceinline__ int clip_pick(const DevClip &cl, float3 p, float lod) {
+  const float wx = p.x * cl.nx, wy = p.y * cl.nx;
+  const int desired = (int)clamp_(lod, 0.0f, 5.0f);
+  for (int step = 0; step < 6; step++) {
+    int li = desired + step;
+    if (li > 5) li = 5 - step;
+    if (li < 0) continue;
+    if (!(cl.valid & (1u << li))) continue;
+    const float s = (float)(1u << li);
+    const float tx = (wx - cl.ox[li]) / s + 1.0f, ty = (wy - cl.oy[li]) / s + 1.0f;
+    if (tx < 1.0f || tx >= 2047.0f || ty < 1.0f || ty >= 2047.0f) continue;
+    return li;
+  }
+  return -1;
+}
+
+// vs_sample (raycast.slang:331-367): the base cell under p must be the one
+// its tile holds and hold the sample's slice span; then the pyramid level
+// whose prefilter (4 << level) matches the footprint, stepping down past
+// absent levels, or the base tile.  Cells convert through int so that the
+// key of a cell left of the volume is defined.
+__device__ __forceinline__ float vs_sample(const DevVslab &v, float3 p, float lod) {
+  const float P = (float)v.px, T = P + 2.0f;
+  const uint32_t Tu = v.px + 2u;
+  const float wx = v.x0 + p.x * v.nx, wy = v.y0 + p.y * v.nx;
+  const float zc = (v.z0 + 0.5f) + p.z * v.nx;
+  const float zq = zc / (float)v.wz, w = zq - floorf(zq);
+  const float gx0 = (float)v.gx[0], gy0 = (float)v.gy[0];
+  const float cbx = floorf(wx / P), cby = floorf(wy / P);
+  const float pbx = cbx - floorf(cbx / gx0) * gx0, pby = cby - floorf(cby / gy0) * gy0;
+  const uint32_t want = ((uint32_t)(int32_t)cbx & 1023u) |
+                        (((uint32_t)(int32_t)cby & 1023u) << 10) | 0x80000000u;
+  const uint32_t slot = (uint32_t)(pby * gx0 + pbx);
+  const uint4 e = __ldg(reinterpret_cast<const uint4 *>(v.table) + slot);
+  if (e.x != want) return 0.0f;  // not resident
+  if (zc - 0.5f < (float)e.y || zc + 0.5f > (float)e.z) return 0.0f;
+  int lev = min((int)floorf(lod) - 2, 3);
+  while (lev >= 0 && v.gx[lev + 1] == 0u) lev--;
+  if (lev < 0) {
+    const float lx = (wx - cbx * P) + 1.0f, ly = (wy - cby * P) + 1.0f;
+    return tex_wrapz(v.tiles + (size_t)slot * v.tile_bytes, Tu, Tu, v.wz, lx / T, ly / T, w);
+  }
+  const int L = lev + 1;
+  const float sc = (float)(4 << lev), gxl = (float)v.gx[L], gyl = (float)v.gy[L];
+  const float tx = wx / sc, ty = wy / sc;
+  const float cx = floorf(tx / P), cy = floorf(ty / P);
+  const float qx = cx - floorf(cx / gxl) * gxl, qy = cy - floorf(cy / gyl) * gyl;
+  const float lx = (tx - cx * P) + 1.0f, ly = (ty - cy * P) + 1.0f;
+  const uint32_t k = v.base[L] + (uint32_t)(qy * gxl + qx);
+  return tex_wrapz(v.tiles + (size_t)k * v.tile_bytes, Tu, Tu, v.wz, lx / T, ly / T, w);
+}
+
+// vol_sample in clip mode (raycast.slang:400-403)
+__device__ __forceinline__ float clip_sample(const DevClip &cl, float3 p, float lod) {
+  const int l = clip_pick(cl, p, lod);
+  return l < 0 ? 0.0f : clip_level(cl, l, p);
 }
 
 // vol_sample of the tiled slab (raycast.slang:423-455): voxel coordinates
@@ -541,6 +664,21 @@ __device__ __forceinline__ ViewConst view_const(const r3d_frame_params &pc, cons
     v.vox_inv = s.sh.n;
     v.max_lod = 3.0f;
     v.ext = make_float3(1.0f, 1.0f, 1.0f);
+  } else if (PATH == PATH_CLIP) {  // raycast.slang:651-654,305-314
+    v.voxel = 1.0f / pc.slab_nx;
+    v.vox_inv = pc.slab_nx;
+    v.max_lod = 7.0f;
+    v.ext = make_float3(1.0f, pc.slab_ny / pc.slab_nx, (float)pc.slab_depth / pc.slab_nx);
+  } else if (PATH == PATH_VSLAB) {  // raycast.slang:661-671,305-314
+    v.voxel = 1.0f / pc.slab_nx;
+    v.vox_inv = pc.slab_nx;
+    v.max_lod = 3.0f;  // +2 past the coarsest present pyramid level
+    for (int l = 3; l >= 0; l--)
+      if (((pc.brick_mode >> (8 * l)) & 0xffu) != 0u) {
+        v.max_lod = (float)l + 4.0f;
+        break;
+      }
+    v.ext = make_float3(1.0f, pc.slab_ny / pc.slab_nx, (float)pc.slab_depth / pc.slab_nx);
   } else if (PATH == PATH_SLAB) {  // raycast.slang:672-677,305-314
     v.voxel = 1.0f / pc.slab_nx;
     v.vox_inv = pc.slab_nx;
@@ -752,11 +890,16 @@ __device__ __forceinline__ float skip_block(const RayState &st, float3 p, float 
   return fmaxf(fminf(fminf(tex[0], tex[1]), tex[2]), st.t) + bsz * 0.01f;
 }
 
-// A gradient tap: the tiled slab's vol_sample, or a cube-like texture.
-template <bool SLAB>
+// A gradient tap: the tiled slab's vol_sample; in clip mode the level the
+// sample picked (or, without one, vol_sample; raycast.slang:942-946,
+// 967-974); else a cube-like texture.
+template <int PATH>
 __device__ __forceinline__ float tap_sample(const DevScene &s, const DevCube &tex, float3 p,
-                                            float lod) {
-  return SLAB ? slab_sample(s.sl, p, lod) : cube_sample(tex, p, lod);
+                                            float lod, int clip_l) {
+  if (PATH == PATH_SLAB) return slab_sample(s.sl, p, lod);
+  if (PATH == PATH_VSLAB) return vs_sample(s.vs, p, lod);
+  if (PATH == PATH_CLIP) return clip_l >= 0 ? clip_level(s.cl, clip_l, p) : clip_sample(s.cl, p, lod);
+  return cube_sample(tex, p, lod);
 }
 
 // Gradient shading (FULL mode, raycast.slang:919-998) and front-to-back
@@ -807,10 +950,10 @@ __device__ __forceinline__ bool composite_sample(const DevScene &s, const ViewCo
         q3 = shard_fetch(s.sh, org, make_float3(u.x + ev, u.y + ev, u.z + ev), q.lod, e2);
       } else {
         float ee = (vc.voxel * q.lod_step) * ir3;
-        q0 = tap_sample<kSlab>(s, tex, make_float3(q.p.x + ee, q.p.y - ee, q.p.z - ee), q.lod);
-        q1 = tap_sample<kSlab>(s, tex, make_float3(q.p.x - ee, q.p.y - ee, q.p.z + ee), q.lod);
-        q2 = tap_sample<kSlab>(s, tex, make_float3(q.p.x - ee, q.p.y + ee, q.p.z - ee), q.lod);
-        q3 = tap_sample<kSlab>(s, tex, make_float3(q.p.x + ee, q.p.y + ee, q.p.z + ee), q.lod);
+        q0 = tap_sample<PATH>(s, tex, make_float3(q.p.x + ee, q.p.y - ee, q.p.z - ee), q.lod, (int)q.slot);
+        q1 = tap_sample<PATH>(s, tex, make_float3(q.p.x - ee, q.p.y - ee, q.p.z + ee), q.lod, (int)q.slot);
+        q2 = tap_sample<PATH>(s, tex, make_float3(q.p.x - ee, q.p.y + ee, q.p.z - ee), q.lod, (int)q.slot);
+        q3 = tap_sample<PATH>(s, tex, make_float3(q.p.x + ee, q.p.y + ee, q.p.z + ee), q.lod, (int)q.slot);
       }
       g0 = (((q0 - q1) - q2) + q3) * renorm;
       g1 = (((-q0 - q1) + q2) + q3) * renorm;
@@ -848,12 +991,12 @@ __device__ __forceinline__ bool composite_sample(const DevScene &s, const ViewCo
              shard_fetch(s.sh, org, make_float3(u.x, u.y, u.z - ev), q.lod, e2);
       } else {
         float e = vc.voxel * q.lod_step;
-        g0 = tap_sample<kSlab>(s, tex, make_float3(q.p.x + e, q.p.y, q.p.z), q.lod) -
-             tap_sample<kSlab>(s, tex, make_float3(q.p.x - e, q.p.y, q.p.z), q.lod);
-        g1 = tap_sample<kSlab>(s, tex, make_float3(q.p.x, q.p.y + e, q.p.z), q.lod) -
-             tap_sample<kSlab>(s, tex, make_float3(q.p.x, q.p.y - e, q.p.z), q.lod);
-        g2 = tap_sample<kSlab>(s, tex, make_float3(q.p.x, q.p.y, q.p.z + e), q.lod) -
-             tap_sample<kSlab>(s, tex, make_float3(q.p.x, q.p.y, q.p.z - e), q.lod);
+        g0 = tap_sample<PATH>(s, tex, make_float3(q.p.x + e, q.p.y, q.p.z), q.lod, (int)q.slot) -
+             tap_sample<PATH>(s, tex, make_float3(q.p.x - e, q.p.y, q.p.z), q.lod, (int)q.slot);
+        g1 = tap_sample<PATH>(s, tex, make_float3(q.p.x, q.p.y + e, q.p.z), q.lod, (int)q.slot) -
+             tap_sample<PATH>(s, tex, make_float3(q.p.x, q.p.y - e, q.p.z), q.lod, (int)q.slot);
+        g2 = tap_sample<PATH>(s, tex, make_float3(q.p.x, q.p.y, q.p.z + e), q.lod, (int)q.slot) -
+             tap_sample<PATH>(s, tex, make_float3(q.p.x, q.p.y, q.p.z - e), q.lod, (int)q.slot);
       }
     }
     float3 gv = make_float3(g0, g1, g2);
@@ -941,6 +1084,8 @@ __device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, 
   constexpr bool kLod = PATH == PATH_LOD_BRICKS;
   constexpr bool kShard = PATH == PATH_SHARD;
   constexpr bool kSlab = PATH == PATH_SLAB;
+  constexpr bool kClip = PATH == PATH_CLIP;
+  constexpr bool kVslab = PATH == PATH_VSLAB;
   constexpr bool kComposite = MODE == R3D_MODE_FULL || MODE == R3D_MODE_FLAT;
   constexpr bool kShaded = MODE == R3D_MODE_FULL;
   constexpr uint32_t ray_budget = kLod ? (kShaded ? 192u : 256u) : kMaxSteps;
@@ -961,7 +1106,7 @@ __device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, 
   float lod_step =
       !lod_known || st.span_dom ? st.span_step
                                 : fmaxf(lod == 0.0f ? 1.0f : r3d_exp2f(lod), st.span_step);
-  if (kSlab) lod_step = fminf(lod_step, st.slab_cap);
+  if (kSlab || kClip || kVslab) lod_step = fminf(lod_step, st.slab_cap);
   const float3 dir = st.dir;
   const float3 p =
       make_float3(fmaf(t, dir.x, st.ro.x), fmaf(t, dir.y, st.ro.y), fmaf(t, dir.z, st.ro.z));
@@ -1036,6 +1181,12 @@ __device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, 
     }
   } else if (kSlab) {
     v = slab_sample(s.sl, p, lod);
+  } else if (kVslab) {
+    v = vs_sample(s.vs, p, lod);
+  } else if (kClip) {  // the level is picked once; taps reuse it (raycast.slang:785-787)
+    const int cl = clip_pick(s.cl, p, lod);
+    b.slot = (uint32_t)cl;
+    v = cl < 0 ? 0.0f : clip_level(s.cl, cl, p);
   } else {
     v = cube_sample(s.cube, p, lod);
   }
@@ -1065,7 +1216,8 @@ __device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, 
         return kStepCont;
       }
     }
-  } else if (!kSlab && v < vc.occ_gate && occ_sample(s.cube, p) < vc.occ_gate) {
+  } else if (!kSlab && !kClip && !kVslab && v < vc.occ_gate &&
+             occ_sample(s.cube, p) < vc.occ_gate) {
     st.t = skip_block(st, p, vc.bs);  // (no empty-space skip in slab mode: raycast.slang:861)
     return kStepCont;
   }

@@ -86,7 +86,7 @@ int r3d_cuda_bricks_overlay_load(r3d_cuda_ctx *c, uint32_t which, const uint8_t 
   if (is_device_ptr(slots)) return set_overlay(c, which, slots);
   uint8_t *tmp = nullptr;
   R3D_CUDA_TRY(c, cudaMalloc(&tmp, bytes ? bytes : 1u));
-  cudaError_t e = cudaMemcpy(tmp, slots, bytes, cudaMemcpyHostToDevice);
+  cudaError_t e = copy_sync(c->stream, tmp, slots, bytes);
   int rc = e == cudaSuccess ? set_overlay(c, which, tmp) : cuda_fail(c, e, "bricks_overlay_load");
   cudaFree(tmp);
   return rc;

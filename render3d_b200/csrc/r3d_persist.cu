@@ -230,42 +230,58 @@ static cudaError_t launch_pm(const PersistLaunch &L, const DevScene &s, cudaStre
   }
 }
 
-cudaError_t launch_persist(const PersistLaunch &L, const DevScene &s, cudaStream_t st) {
-  switch (L.path) {
-    case PATH_LOD_BRICKS: return launch_pm<PATH_LOD_BRICKS>(L, s, st);
-    case PATH_SHARD: return launch_pm<PATH_SHARD>(L, s, st);
-    case PATH_SLAB: return launch_pm<PATH_SLAB>(L, s, st);
-    default: return launch_pm<PATH_CUBE>(L, s, st);
-  }
+#ifdef R3D_FWD_PATH
+// Compiled once per sampling path (R3D_FWD_PATH = 0..5), as the forward
+// kernels are.
+template <>
+cudaError_t persist_path<R3D_FWD_PATH>(const PersistLaunch &L, const DevScene &s,
+                                       cudaStream_t st) {
+  return launch_pm<R3D_FWD_PATH>(L, s, st);
 }
 
-int persist_blocks_per_sm(int path, uint32_t mode, bool fast, uint32_t unroll) {
-  // occupancy of the instantiation that launch_persist would pick
+template <>
+int persist_occupancy<R3D_FWD_PATH>(uint32_t mode, bool fast, uint32_t unroll) {
+  // occupancy of the instantiation that persist_path picks
+  constexpr int P = R3D_FWD_PATH;
   int n = 0;
-  cudaError_t e = cudaSuccess;
-#define R3D_OCC(P, M, F, U)                                                            \
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_raycast_persist<P, M, F, false, U>, \
-                                                    128, 0)
-  if (path == PATH_LOD_BRICKS) {
-    if (mode == R3D_MODE_FULL && !fast) {
-      if (unroll == 2) R3D_OCC(PATH_LOD_BRICKS, R3D_MODE_FULL, false, 2);
-      else R3D_OCC(PATH_LOD_BRICKS, R3D_MODE_FULL, false, 1);
-    } else {
-      R3D_OCC(PATH_LOD_BRICKS, R3D_MODE_MIP, false, 1);
-    }
-  } else if (path == PATH_SHARD) {
-    R3D_OCC(PATH_SHARD, R3D_MODE_FULL, false, 1);
-  } else if (path == PATH_SLAB) {
-    R3D_OCC(PATH_SLAB, R3D_MODE_FULL, false, 1);
-  } else {
-    R3D_OCC(PATH_CUBE, R3D_MODE_FULL, false, 1);
-  }
-#undef R3D_OCC
+  cudaError_t e;
+  if (P == PATH_LOD_BRICKS && (mode != R3D_MODE_FULL || fast))
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &n, k_raycast_persist<P, R3D_MODE_MIP, false, false, 1>, 128, 0);
+  else if (P == PATH_LOD_BRICKS && unroll == 2)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &n, k_raycast_persist<P, R3D_MODE_FULL, false, false, 2>, 128, 0);
+  else
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &n, k_raycast_persist<P, R3D_MODE_FULL, false, false, 1>, 128, 0);
   if (e != cudaSuccess) {
     cudaGetLastError();
     return 4;
   }
   return n > 0 ? n : 1;
 }
+#else
+cudaError_t launch_persist(const PersistLaunch &L, const DevScene &s, cudaStream_t st) {
+  switch (L.path) {
+    case PATH_VSLAB: return persist_path<PATH_VSLAB>(L, s, st);
+    case PATH_CLIP: return persist_path<PATH_CLIP>(L, s, st);
+    case PATH_SLAB: return persist_path<PATH_SLAB>(L, s, st);
+    case PATH_LOD_BRICKS: return persist_path<PATH_LOD_BRICKS>(L, s, st);
+    case PATH_SHARD: return persist_path<PATH_SHARD>(L, s, st);
+    default: return persist_path<PATH_CUBE>(L, s, st);
+  }
+}
+
+int persist_blocks_per_sm(int path, uint32_t mode, bool fast, uint32_t unroll) {
+  switch (path) {
+    case PATH_VSLAB: return persist_occupancy<PATH_VSLAB>(mode, fast, unroll);
+    case PATH_CLIP: return persist_occupancy<PATH_CLIP>(mode, fast, unroll);
+    case PATH_SLAB: return persist_occupancy<PATH_SLAB>(mode, fast, unroll);
+    case PATH_LOD_BRICKS: return persist_occupancy<PATH_LOD_BRICKS>(mode, fast, unroll);
+    case PATH_SHARD: return persist_occupancy<PATH_SHARD>(mode, fast, unroll);
+    default: return persist_occupancy<PATH_CUBE>(mode, fast, unroll);
+  }
+}
+#endif
 
 }  // namespace r3d

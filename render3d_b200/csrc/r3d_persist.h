@@ -30,7 +30,7 @@ struct PersistLaunch {
   uint32_t blocks;
   uint32_t mode;
   bool fast;
-  int path;  // PATH_CUBE, PATH_LOD_BRICKS or PATH_SHARD
+  int path;  // a Path
 };
 
 // Tile geometry for a tile shape (0: 8x4, 1: 16x2, 2: 32x1).
@@ -50,5 +50,10 @@ inline uint32_t view_tiles(DevView &v, uint32_t shape) {
 
 cudaError_t launch_persist(const PersistLaunch &L, const DevScene &s, cudaStream_t st);
 int persist_blocks_per_sm(int path, uint32_t mode, bool fast, uint32_t unroll);
+// Per-path halves of the two above (each defined in its own object).
+template <int PATH>
+cudaError_t persist_path(const PersistLaunch &L, const DevScene &s, cudaStream_t st);
+template <int PATH>
+int persist_occupancy(uint32_t mode, bool fast, uint32_t unroll);
 
 }  // namespace r3d

@@ -171,7 +171,7 @@ int r3d_cuda_shard_build(r3d_cuda_ctx *c, uint32_t edge, const uint8_t *voxels, 
   for (uint32_t b = 0; b < nb; b++)
     page[b] = slot[b] == R3D_BRICK_ABSENT ? R3D_BRICK_ABSENT : slot[b] | (maxv[b] << 24);
   if (e == cudaSuccess)
-    e = cudaMemcpy(dpage, page.data(), sizeof(uint32_t) * nb, cudaMemcpyHostToDevice);
+    e = copy_sync(c->stream, dpage, page.data(), sizeof(uint32_t) * nb);
   cudaFree(vtmp);
   cudaFree(dslot);
   cudaFree(dbrick);

@@ -178,7 +178,7 @@ int r3d_cuda_slab_build(r3d_cuda_ctx *c, const r3d_volume_desc *d, const uint8_t
   cudaError_t e = cudaMalloc(&c->slab_buf, off);
   if (e == cudaSuccess) e = cudaMalloc(&c->slab_src, vbytes);
   if (e == cudaSuccess) e = cudaMalloc(&c->slab_planes, planes ? planes : 1u);
-  if (e == cudaSuccess) e = cudaMemcpy(c->slab_src, voxels, vbytes, cudaMemcpyDefault);
+  if (e == cudaSuccess) e = copy_sync(c->stream, c->slab_src, voxels, vbytes);
   if (e != cudaSuccess) {
     slab_reset(c);
     return cuda_fail(c, e, "slab_build");

@@ -115,13 +115,11 @@ int r3d_cuda_stream_begin(r3d_cuda_ctx *c, const r3d_volume_desc *d, const uint8
   }
   if (!c->page_ev) R3D_CUDA_TRY(c, cudaEventCreateWithFlags(&c->page_ev, cudaEventDisableTiming));
   c->store_page.resize(words);
-  R3D_CUDA_TRY(c, cudaMemcpy(c->store_page.data(), c->page, (size_t)words * 4u,
-                             cudaMemcpyDeviceToHost));
+  R3D_CUDA_TRY(c, copy_sync(c->stream, c->store_page.data(), c->page, (size_t)words * 4u));
   cudaError_t e = cudaMallocHost(&c->store, (size_t)nall * kSlotBytes);
   if (e == cudaSuccess) e = cudaMallocHost(&c->page_shadow, (size_t)words * 4u);
   if (e == cudaSuccess) e = cudaMalloc(&c->stream_jobs, (size_t)std::min(nslots, 65535u) * 4u);
-  if (e == cudaSuccess)
-    e = cudaMemcpy(c->store, c->pool, (size_t)nall * kSlotBytes, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = copy_sync(c->stream, c->store, c->pool, (size_t)nall * kSlotBytes);
   if (e != cudaSuccess) {
     stream_reset(c);
     c->have_bricks = false;
@@ -131,7 +129,7 @@ int r3d_cuda_stream_begin(r3d_cuda_ctx *c, const r3d_volume_desc *d, const uint8
   cudaFree(c->pool);
   c->pool = nullptr;
   e = cudaMalloc(&c->pool, (size_t)nslots * kSlotBytes);
-  if (e == cudaSuccess) e = cudaMemset(c->pool, 0, (size_t)nslots * kSlotBytes);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->pool, 0, (size_t)nslots * kSlotBytes, c->stream);
   if (e != cudaSuccess) {
     stream_reset(c);
     c->have_bricks = false;

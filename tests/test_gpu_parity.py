@@ -138,12 +138,15 @@ def test_multiview_rects(rb, orc, ctx, cube256, scroll_tf, sched):
 
 def test_unsupported_views_error(rb, ctx, cube256, scroll_tf):
     p = elev35(rb, scroll_tf, w=64, h=64)
-    for field, val in [("slab_grid", 1), ("clip_valid", 1), ("overlay_flags", 1)]:
+    # slab, virtual-slab and clip views on a context holding none of them:
+    # R3D_E_STATE; overlay atlases on a cube view: R3D_E_UNSUPPORTED
+    for field, val, code in [("slab_grid", 1, -5), ("slab_grid", 1 << 24, -5),
+                             ("clip_valid", 1, -5), ("overlay_flags", 1, -4)]:
         q = p.copy()
         setattr(q, field, val)
         with pytest.raises(rb.R3DError) as e:
             ctx.raycast(q, 64, 64)
-        assert e.value.code == -4
+        assert e.value.code == code, field
     q = p.copy()
     q.view_flags = rb.VIEW_SURF
     with pytest.raises(rb.R3DError):
