@@ -219,6 +219,40 @@ int r3d_cuda_vslab_layout(const r3d_cuda_ctx *ctx, r3d_vslab_layout *out);
 int r3d_cuda_vslab_read(r3d_cuda_ctx *ctx, uint32_t tile, uint8_t *out);
 int r3d_cuda_vslab_table(r3d_cuda_ctx *ctx, uint32_t *out);
 
+/* Flattened-segment (surf) views: render3d's segment pane (reference
+ * src/render/render.h:193-202 and 58-107, src/vk/vkbackend.c:1674-2066,
+ * src/shaders/surfvol.comp, raycast.slang:515-638).
+ * _surf_begin: the segment as two w x h RGBA32F grids (host or device),
+ * surface points (xyz voxels + valid flag in w) and unit normals; w, h >= 3.
+ * Replaces earlier grids (r3d_surf_begin and r3d_surf_swap).
+ * _surfvol_begin: a w x h x layers flattened volume (two bytes a texel: CT
+ * and overlay), nback layers behind the surface, grid scale (sx, sy) cells
+ * per flattened voxel.  _surfvol_window: texel (x, y, l) samples the LOD
+ * brick cache at surface(u, v) + normal(u, v) * (zoff0 + l - nback), u =
+ * u0 + (x + 0.5) * step (v likewise), at the level of the xy pitch, and the
+ * whole window is baked on the context's stream (the reference bakes row
+ * bands over frames).  _surfvol_overlay selects the overlay atlas baked into
+ * the second byte (0 ink, 1 3D ink, 3 registration, -1 none) and _mark
+ * re-bakes after the brick cache or an overlay changed.  _surfvol_params
+ * writes the view fields (slab_x0/y0 = u0/v0, slab_px = step, slab_nx/ny/wz
+ * = window, slab_grid = nback, max_mip = zoff0, vol_tx/ty = grid scale) and
+ * sets R3D_VIEW_SURF; the caller sets the view centre (cam_origin x, y),
+ * half extents (cam_right x, cam_up y), slab_z0 (normal offset) and
+ * slab_depth (marched layers).  _surfmask: a grid-space class image
+ * (0 unlabeled, 1 background, 2 ink) tinted by overlay_flags bit 5; NULL
+ * clears it. */
+int r3d_cuda_surf_begin(r3d_cuda_ctx *ctx, uint32_t w, uint32_t h, const float *coords_rgba,
+                        const float *normals_rgba);
+int r3d_cuda_surfvol_begin(r3d_cuda_ctx *ctx, uint32_t w, uint32_t h, uint32_t layers,
+                           uint32_t nback, float sx, float sy);
+int r3d_cuda_surfvol_window(r3d_cuda_ctx *ctx, double u0, double v0, float step, float zoff0);
+int r3d_cuda_surfvol_overlay(r3d_cuda_ctx *ctx, int atlas);
+int r3d_cuda_surfvol_mark(r3d_cuda_ctx *ctx);
+void r3d_cuda_surfvol_params(const r3d_cuda_ctx *ctx, r3d_frame_params *p);
+/* Copy of the flattened volume (w * h * layers * 2 bytes, x fastest). */
+int r3d_cuda_surfvol_read(r3d_cuda_ctx *ctx, uint8_t *out);
+int r3d_cuda_surfmask(r3d_cuda_ctx *ctx, const uint8_t *m, uint32_t w, uint32_t h);
+
 /* Slot-parallel overlay atlases of the LOD brick cache (reference
  * src/render/render.h:51-101; sampled by src/shaders/raycast.slang:45-115,
  * 872-914,1000-1014,1032-1036): which = 0 ink (overlay_flags bit 0, tinted

@@ -54,14 +54,17 @@ typedef struct r3d_frame_params {
   uint32_t mode;
   uint32_t frame_index; /* jitter seed */
   float threshold;      /* low-cut: samples below it are void */
-  /* tiled-slab sampling (not implemented by this library; 0 selects cube) */
+  /* window fields of the tiled slab (slab_grid: gx | gy << 8 | ovs << 16),
+   * the virtual slab (slab_grid: gx | gy << 6 | 1 << 24; brick_mode packs
+   * its pyramid grids), the clipmap and flattened-segment views (slab_grid:
+   * layers behind the surface); r3d_cuda_*_params fill them */
   uint32_t slab_grid;
   uint32_t slab_wz;
   float slab_z0; /* bricks: slab near face / crop-box z origin, voxels */
   float slab_nx, slab_ny;
   float slab_px, slab_py; /* bricks: crop-box x/y extents, voxels */
   uint32_t slab_depth;    /* bricks: slab thickness in voxels (0 = off) */
-  /* clipmap sampling (not implemented by this library; must be 0) */
+  /* clipmap: valid level mask (non-zero selects the clipmap) and origins */
   uint32_t clip_valid;
   float clip_orig[6][2];
   /* model transform: p_volume = R^T (p_world - t - c) + c, c = extent / 2;
@@ -79,7 +82,7 @@ typedef struct r3d_frame_params {
   float slab_x0, slab_y0; /* bricks: crop-box origin x/y, voxels */
   uint32_t view_org;      /* output pixel origin, x | y << 16 */
   uint32_t view_flags;    /* R3D_VIEW_* bits */
-  float overlay_gain;     /* overlays: not implemented, must be 0 flags */
+  float overlay_gain;     /* overlay tint strength */
   uint32_t overlay_flags;
 } r3d_frame_params;
 
@@ -91,9 +94,9 @@ _Static_assert(sizeof(r3d_frame_params) == 248, "r3d_frame_params is 248 bytes")
 
 /* view_flags bits (reference src/render/render_types.h:96-105). */
 #define R3D_VIEW_ORTHO 1u    /* parallel rays; cam_right/up = half extents */
-#define R3D_VIEW_SURF 2u     /* flattened-surface view (not implemented) */
+#define R3D_VIEW_SURF 2u     /* flattened-segment view (r3d_cuda_surfvol_*) */
 #define R3D_VIEW_OBLIQUE 4u  /* bricks slab clipped along the ray */
-#define R3D_VIEW_STRETCH 8u  /* surf view heatmap (not implemented) */
+#define R3D_VIEW_STRETCH 8u  /* surf view: flattening-distortion heatmap */
 #define R3D_VIEW_CROP 16u    /* bricks: clip to the crop box */
 #define R3D_VIEW_HALF 32u    /* one ray per 2x2 pixel block */
 #define R3D_VIEW_AXIS(a) ((uint32_t)(a) << 8) /* bricks slab axis 0=z 1=x 2=y */

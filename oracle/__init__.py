@@ -50,10 +50,17 @@ class VSlab(C.Structure):
                 ("tiles", C.c_void_p), ("table", C.c_void_p)]
 
 
+class Surf(C.Structure):
+    _fields_ = [("coords", C.c_void_p), ("normals", C.c_void_p), ("gw", C.c_uint32),
+                ("gh", C.c_uint32), ("vol", C.c_void_p), ("W", C.c_uint32), ("H", C.c_uint32),
+                ("L", C.c_uint32), ("mask", C.c_void_p), ("mw", C.c_uint32), ("mh", C.c_uint32)]
+
+
 class Bricks(C.Structure):
     _fields_ = [("page", C.c_void_p), ("page_words", C.c_uint32), ("pool", C.c_void_p),
                 ("nslots", C.c_uint32), ("atlas", C.c_void_p), ("ovl", C.c_void_p * 4),
-                ("slab", C.c_void_p), ("clip", C.c_void_p), ("vslab", C.c_void_p)]
+                ("slab", C.c_void_p), ("clip", C.c_void_p), ("vslab", C.c_void_p),
+                ("surf", C.c_void_p)]
 
 
 class Opts(C.Structure):
@@ -88,6 +95,8 @@ def _load():
     lib.orc_slab_layout.argtypes = [U32, U32, P, P]
     lib.orc_slab_fill.restype = None
     lib.orc_slab_fill.argtypes = [P, U32, U32, U32, U32, U32, C.c_void_p * 8]
+    lib.orc_surf_bake.restype = None
+    lib.orc_surf_bake.argtypes = [P, P, F, F, F, F, F, F, U32, C.c_int]
     lib.orc_vslab_fill.restype = None
     lib.orc_vslab_fill.argtypes = [P, P, U32, U32, C.c_int64, C.c_int64, C.c_int64, U32]
     lib.orc_clip_fill.restype = None
@@ -549,10 +558,52 @@ class VSlabScene:
         p.clip_valid = 0
 
 
+class SurfScene:
+    """A flattened segment over a LOD brick cache (BrickScene): the grids
+    (gh, gw, 4) float32 of surface points (xyz, valid) and normals, a
+    W x H x L flattened volume baked by the oracle's restatement of the
+    reference's bake, and an optional supervision mask (mh, mw) u8."""
+
+    def __init__(self, bricks: "BrickScene", coords, normals, W: int, H: int, L: int,
+                 nback: int, sx: float, sy: float, mask=None):
+        self.bricks = bricks
+        self.coords = np.ascontiguousarray(coords, np.float32)
+        self.normals = np.ascontiguousarray(normals, np.float32)
+        gh, gw = self.coords.shape[:2]
+        self.vol = np.zeros((L, H, W, 2), np.uint8)
+        self.nback = nback if nback < L else L // 2
+        self.sx, self.sy = sx, sy
+        self.mask = None if mask is None else np.ascontiguousarray(mask, np.uint8)
+        self.s = Surf(self.coords.ctypes.data, self.normals.ctypes.data, gw, gh,
+                      self.vol.ctypes.data, W, H, L,
+                      None if self.mask is None else self.mask.ctypes.data,
+                      0 if self.mask is None else self.mask.shape[1],
+                      0 if self.mask is None else self.mask.shape[0])
+        self.b = Bricks()
+        C.memmove(C.addressof(self.b), C.addressof(bricks.b), C.sizeof(Bricks))
+        self.b.surf = C.addressof(self.s)
+        self.window = None
+
+    def bake(self, u0: float, v0: float, step: float, zoff0: float, ovl: int = -1) -> None:
+        lib.orc_surf_bake(C.byref(self.s), C.byref(self.bricks.b), u0, v0, step, zoff0,
+                          self.sx, self.sy, self.nback, ovl)
+        self.window = (np.float32(u0), np.float32(v0), np.float32(step), np.float32(zoff0))
+
+    def params(self, p) -> None:
+        """View fields of the baked window (vkbackend.c:2054-2066)."""
+        u0, v0, step, zoff0 = self.window
+        p.slab_x0, p.slab_y0, p.slab_px = float(u0), float(v0), float(step)
+        p.slab_nx, p.slab_ny, p.slab_wz = float(self.s.W), float(self.s.H), self.s.L
+        p.slab_grid, p.max_mip = self.nback, float(zoff0)
+        p.vol_tx, p.vol_ty = float(np.float32(self.sx)), float(np.float32(self.sy))
+        p.view_flags |= 2
+
+
 def _scene_args(scene):
     cube = C.byref(scene.c) if isinstance(scene, CubeScene) else None
     br = (C.byref(scene.b)
-          if isinstance(scene, (BrickScene, ShardScene, SlabScene, ClipScene, VSlabScene))
+          if isinstance(scene, (BrickScene, ShardScene, SlabScene, ClipScene, VSlabScene,
+                                SurfScene))
           else None)
     return cube, br
 

@@ -452,6 +452,257 @@ typedef struct ray_out {
   int store; /* 0: pixel outside the viewport */
 } ray_out;
 
+/* ------------------------------------------------- flattened segment */
+
+/* GLSL mix(x, y, a) = x (1 - a) + y a */
+static inline float mixf_(float x, float y, float a) { return fmaf(y, a, x * (1.0f - a)); }
+
+/* bricks_sample_c, surfvol.comp:54-96, with its per-column brick cache */
+typedef struct surf_cache {
+  int valid;
+  uint32_t scale, bc[3], slot;
+} surf_cache;
+
+static void surf_brick_sample(const scene *s, uint32_t lod, int ovl, v3f wp, v3f shape,
+                              surf_cache *c, float out[2]) {
+  float bv[3] = {clampf_(wp.x, 0.0f, fmaxf(shape.x - 0.001f, 0.0f)),
+                 clampf_(wp.y, 0.0f, fmaxf(shape.y - 0.001f, 0.0f)),
+                 clampf_(wp.z, 0.0f, fmaxf(shape.z - 0.001f, 0.0f))};
+  uint32_t nlev = page_rd(s, 0);
+  if (c->valid) {
+    float lv[3];
+    uint32_t bc[3];
+    for (int a = 0; a < 3; a++) lv[a] = bv[a] / (float)c->scale, bc[a] = (uint32_t)lv[a] >> 7;
+    if (bc[0] == c->bc[0] && bc[1] == c->bc[1] && bc[2] == c->bc[2]) {
+      v3f bl = mk3(lv[0] - (float)(bc[0] << 7), lv[1] - (float)(bc[1] << 7), lv[2] - (float)(bc[2] << 7));
+      out[0] = brick_fetch(s, c->slot, bl);
+      out[1] = ovl >= 0 ? ovl_fetch(s, ovl, c->slot, bl) : 0.0f;
+      return;
+    }
+  }
+  int desired = (int)(lod < nlev - 1u ? lod : nlev - 1u), last = (int)nlev - 1;
+  for (int stp = 0; stp < 4; stp++) {
+    int li = stp < 3 ? desired + stp : last;
+    if (li > last || (stp == 3 && li <= desired + 2)) continue;
+    uint32_t h = 4u + (uint32_t)li * 4u;
+    uint32_t off = page_rd(s, h), packed = page_rd(s, h + 1u), scale = page_rd(s, h + 2u);
+    uint32_t bd[3] = {packed & 1023u, (packed >> 10) & 1023u, packed >> 20};
+    float lv[3];
+    uint32_t bc[3];
+    for (int a = 0; a < 3; a++) {
+      lv[a] = bv[a] / (float)scale;
+      bc[a] = (uint32_t)lv[a] >> 7;
+      if (bc[a] > bd[a] - 1u) bc[a] = bd[a] - 1u;
+    }
+    uint32_t e = page_rd(s, off + (bc[2] * bd[1] + bc[1]) * bd[0] + bc[0]);
+    if (e == 0xFFFFFFFFu) continue;
+    c->valid = 1;
+    c->scale = scale;
+    memcpy(c->bc, bc, sizeof bc);
+    c->slot = e & 0xFFFFFFu;
+    v3f bl = mk3(lv[0] - (float)(bc[0] << 7), lv[1] - (float)(bc[1] << 7), lv[2] - (float)(bc[2] << 7));
+    out[0] = brick_fetch(s, c->slot, bl);
+    out[1] = ovl >= 0 ? ovl_fetch(s, ovl, c->slot, bl) : 0.0f;
+    return;
+  }
+  c->valid = 0;
+  out[0] = out[1] = 0.0f;
+}
+
+void orc_surf_bake(orc_surf *sf, const orc_bricks *br, float u0, float v0, float step,
+                   float zoff0, float sx, float sy, uint32_t nback, int ovl) {
+  uint32_t st = 0;
+  scene s = {NULL, br, &st, NULL};
+  uint32_t nlev = br->page[0], lod = 0;
+  for (float sc = step; sc >= 2.0f && lod + 1u < nlev; sc *= 0.5f) lod++; /* vkbackend.c:7013 */
+  v3f shape = mk3((float)br->page[1], (float)br->page[2], (float)br->page[3]);
+  const uint32_t gw = sf->gw, gh = sf->gh;
+#pragma omp parallel for schedule(dynamic, 4)
+  for (uint32_t y = 0; y < sf->H; y++)
+    for (uint32_t x = 0; x < sf->W; x++) {
+      float fu = fmaf((float)x + 0.5f, step, u0), fv = fmaf((float)y + 0.5f, step, v0);
+      float gx = fu * sx, gy = fv * sy;
+      int ok = 0;
+      v3f wp0 = mk3(0, 0, 0), nrm = mk3(0, 0, 0);
+      if (gx >= 0.0f && gy >= 0.0f && gx <= (float)(gw - 1u) && gy <= (float)(gh - 1u)) {
+        uint32_t ix = (uint32_t)gx, iy = (uint32_t)gy;
+        if (ix > gw - 2u) ix = gw - 2u;
+        if (iy > gh - 2u) iy = gh - 2u;
+        float fx = gx - (float)ix, fy = gy - (float)iy;
+        const float *c00 = sf->coords + 4u * ((size_t)iy * gw + ix), *c10 = c00 + 4,
+                    *c01 = c00 + 4u * gw, *c11 = c01 + 4;
+        if (fminf(fminf(c00[3], c10[3]), fminf(c01[3], c11[3])) >= 0.5f) {
+          const float *n00 = sf->normals + 4u * ((size_t)iy * gw + ix), *n10 = n00 + 4,
+                      *n01 = n00 + 4u * gw, *n11 = n01 + 4;
+          float w[3], n[3];
+          for (int a = 0; a < 3; a++) {
+            w[a] = mixf_(mixf_(c00[a], c10[a], fx), mixf_(c01[a], c11[a], fx), fy);
+            n[a] = mixf_(mixf_(n00[a], n10[a], fx), mixf_(n01[a], n11[a], fx), fy);
+          }
+          wp0 = mk3(w[0], w[1], w[2]);
+          nrm = mk3(n[0], n[1], n[2]);
+          float nl = sqrtf(dot3(nrm, nrm));
+          if (nl > 1e-4f) {
+            nrm = mk3(nrm.x / nl, nrm.y / nl, nrm.z / nl);
+            ok = 1;
+          }
+        }
+      }
+      surf_cache c = {0, 1u, {0, 0, 0}, 0};
+      for (uint32_t z = 0; z < sf->L; z++) {
+        float v[2] = {0.0f, 0.0f};
+        if (ok) {
+          float k = fmaf((float)z - (float)nback, 1.0f, zoff0);
+          v3f wp = mk3(fmaf(nrm.x, k, wp0.x), fmaf(nrm.y, k, wp0.y), fmaf(nrm.z, k, wp0.z));
+          if (wp.x >= 0.0f && wp.y >= 0.0f && wp.z >= 0.0f && wp.x < shape.x && wp.y < shape.y &&
+              wp.z < shape.z)
+            surf_brick_sample(&s, lod, ovl, wp, shape, &c, v);
+        }
+        uint8_t *o = sf->vol + (((size_t)z * sf->H + y) * sf->W + x) * 2u;
+        o[0] = unorm8(v[0]);
+        o[1] = unorm8(v[1]);
+      }
+    }
+}
+
+/* the flattened volume, clamp-to-edge trilinear at normalized uvw */
+static void surf_tex(const orc_surf *sf, float u, float v, float t, float out[2]) {
+  float tx = clampf_(fmaf(u, (float)sf->W, -0.5f), 0.0f, (float)(sf->W - 1u));
+  float ty = clampf_(fmaf(v, (float)sf->H, -0.5f), 0.0f, (float)(sf->H - 1u));
+  float tz = clampf_(fmaf(t, (float)sf->L, -0.5f), 0.0f, (float)(sf->L - 1u));
+  uint32_t x0 = (uint32_t)tx, y0 = (uint32_t)ty, z0 = (uint32_t)tz;
+  float fx = tx - (float)x0, fy = ty - (float)y0, fz = tz - (float)z0;
+  uint32_t x1 = x0 + 1u < sf->W ? x0 + 1u : sf->W - 1u, y1 = y0 + 1u < sf->H ? y0 + 1u : sf->H - 1u,
+           z1 = z0 + 1u < sf->L ? z0 + 1u : sf->L - 1u;
+  for (int ch = 0; ch < 2; ch++) {
+#define T(X, Y, Z) ((float)sf->vol[(((size_t)(Z) * sf->H + (Y)) * sf->W + (X)) * 2u + ch])
+    float a = lerpf_(lerpf_(T(x0, y0, z0), T(x1, y0, z0), fx), lerpf_(T(x0, y1, z0), T(x1, y1, z0), fx), fy);
+    float b = lerpf_(lerpf_(T(x0, y0, z1), T(x1, y0, z1), fx), lerpf_(T(x0, y1, z1), T(x1, y1, z1), fx), fy);
+#undef T
+    out[ch] = lerpf_(a, b, fz) * INV255;
+  }
+}
+
+/* flat_overlay_color, :76-81 */
+static void flat_overlay_color(uint32_t f, float c[3]) {
+  float r = 0.25f, g = 1.0f, b = 0.55f;
+  if (f & 16u) r = 1.0f, g = 0.25f, b = 1.0f;
+  else if (f & 2u) r = 0.25f, g = 1.0f, b = 0.55f;
+  else if (f & 4u) r = 1.0f, g = 0.30f, b = 0.22f;
+  else if (((f >> 8) & 0xffu) == 1u) r = 0.3f, g = 0.72f, b = 1.0f;
+  c[0] = r, c[1] = g, c[2] = b;
+}
+
+/* the surf branch of main(), :515-638, for pixel (px, py) */
+static void surf_pixel(const r3d_frame_params *pc, const orc_surf *sf, const uint8_t lut[256][4],
+                       const orc_opts *o, uint32_t px, uint32_t py, float rgb[3]) {
+  const float bg[3] = {0.02f, 0.02f, 0.03f};
+  memcpy(rgb, bg, sizeof bg);
+  float ux = ((float)px + 0.5f) / (float)pc->viewport[0];
+  float uy = ((float)py + 0.5f) / (float)pc->viewport[1];
+  float nx = ux * 2.0f - 1.0f, ny = 1.0f - uy * 2.0f;
+  float fu = fmaf(ny, pc->cam_up[0], fmaf(nx, pc->cam_right[0], pc->cam_origin[0]));
+  float fv = fmaf(ny, pc->cam_up[1], fmaf(nx, pc->cam_right[1], pc->cam_origin[1]));
+  float tx = (fu - pc->slab_x0) / pc->slab_px, ty = (fv - pc->slab_y0) / pc->slab_px;
+  if (tx < 0.0f || ty < 0.0f || tx >= pc->slab_nx || ty >= pc->slab_ny) return;
+  float L = (float)pc->slab_wz;
+  float center = (pc->slab_z0 - pc->max_mip) + (float)(pc->slab_grid & 0xffffu);
+  float halfd = 0.5f * fmaxf((float)pc->slab_depth, 1.0f);
+  float lo = clampf_(center - halfd, 0.0f, L), hi = clampf_(center + halfd, 0.0f, L);
+  if (lo >= hi) return;
+  float ix = 1.0f / pc->slab_nx, iy = 1.0f / pc->slab_ny, iz = 1.0f / L;
+  float vk[2];
+  if (pc->view_flags & R3D_VIEW_STRETCH) { /* distortion heatmap, :540-570 */
+    float gx = fu * pc->vol_tx, gy = fv * pc->vol_ty;
+    int gix = (int)clampf_(gx, 1.0f, (float)sf->gw - 2.0f);
+    int giy = (int)clampf_(gy, 1.0f, (float)sf->gh - 2.0f);
+    const float *cu0 = sf->coords + 4u * ((size_t)giy * sf->gw + gix - 1);
+    const float *cu1 = sf->coords + 4u * ((size_t)giy * sf->gw + gix + 1);
+    const float *cv0 = sf->coords + 4u * ((size_t)(giy - 1) * sf->gw + gix);
+    const float *cv1 = sf->coords + 4u * ((size_t)(giy + 1) * sf->gw + gix);
+    if (fminf(fminf(cu0[3], cu1[3]), fminf(cv0[3], cv1[3])) < 0.5f) return;
+    v3f du = mk3(cu1[0] - cu0[0], cu1[1] - cu0[1], cu1[2] - cu0[2]);
+    v3f dv = mk3(cv1[0] - cv0[0], cv1[1] - cv0[1], cv1[2] - cv0[2]);
+    float su = sqrtf(dot3(du, du)) * 0.5f * pc->vol_tx;
+    float sv = sqrtf(dot3(dv, dv)) * 0.5f * pc->vol_ty;
+    float x = clampf_(r3d_log2f(fmaxf(0.5f * (su + sv), 1e-4f)) / 0.35f, -1.0f, 1.0f);
+    float m = r3d_powf(fabsf(x), 0.6f);
+    float tint[3] = {1.0f, 0.15f, 0.0f};
+    if (x < 0.0f) tint[0] = 0.0f, tint[1] = 0.35f, tint[2] = 1.0f;
+    surf_tex(sf, tx * ix, ty * iy, clampf_(center, lo, hi) * iz, vk);
+    float k = fmaf(0.5f, vk[0], 0.5f);
+    for (int c = 0; c < 3; c++) rgb[c] = lerpf_(0.95f, tint[c], m) * k;
+    return;
+  }
+  float dt = fmaxf(pc->step_voxels, 0.25f);
+  float t = fmaf(hash12(px, py, pc->frame_index), dt, lo);
+  float mip_max = 0.0f, ink_max = 0.0f, acc[4] = {0, 0, 0, 0};
+  int composite = pc->mode != R3D_MODE_MIP, ovl = (pc->overlay_flags & 1u) != 0u;
+  float oc[3];
+  flat_overlay_color(pc->overlay_flags, oc);
+  float opac_k = pc->density * pc->step_voxels;
+  for (uint32_t k = 0; k < 512u && t < hi; k++, t += dt) {
+    float u = tx * ix, w = ty * iy, z = t * iz;
+    surf_tex(sf, u, w, z, vk);
+    float v = vk[0];
+    if (ovl && vk[1] > ink_max) ink_max = vk[1];
+    if (v < pc->threshold) continue;
+    if (v > mip_max) mip_max = v;
+    if (!composite) continue;
+    float sm[4];
+    tf_sample(lut, v, sm);
+    float a = 1.0f - r3d_powf(1.0f - sm[3], opac_k);
+    if (a <= 0.003f) continue;
+    float col[3] = {sm[0], sm[1], sm[2]};
+    if (pc->mode == R3D_MODE_FULL) { /* gradients in flattened space */
+      float p1[2], m1[2];
+      surf_tex(sf, u + ix, w, z, p1), surf_tex(sf, u - ix, w, z, m1);
+      float g0 = p1[0] - m1[0];
+      surf_tex(sf, u, w + iy, z, p1), surf_tex(sf, u, w - iy, z, m1);
+      float g1 = p1[0] - m1[0];
+      surf_tex(sf, u, w, z + iz, p1), surf_tex(sf, u, w, z - iz, m1);
+      float g2 = p1[0] - m1[0];
+      float gm = sqrtf(fmaf(g2, g2, fmaf(g1, g1, g0 * g0)));
+      if (gm > 1e-4f) {
+        float diff = fmaf(0.7f, fabsf(g2 / gm), 0.3f);
+        float lit = fmaf(0.75f, diff, 0.25f);
+        float lm = lerpf_(1.0f, lit, satf(gm * 6.0f));
+        for (int c = 0; c < 3; c++) col[c] *= lm;
+      }
+    }
+    if (ovl) {
+      float kk = satf(vk[1] * pc->overlay_gain);
+      for (int c = 0; c < 3; c++) col[c] = lerpf_(col[c], oc[c], kk);
+    }
+    float wgt = (1.0f - acc[3]) * a;
+    for (int c = 0; c < 3; c++) acc[c] = fmaf(wgt, col[c], acc[c]);
+    acc[3] = acc[3] + wgt;
+    if (acc[3] >= o->alpha_cutoff) break;
+  }
+  if (composite) {
+    float tr = 1.0f - acc[3];
+    for (int c = 0; c < 3; c++) rgb[c] = fmaf(tr, bg[c], acc[c]);
+  } else {
+    float m = mip_max * pc->density;
+    float kk = satf(ink_max * pc->overlay_gain);
+    for (int c = 0; c < 3; c++) rgb[c] = ovl ? lerpf_(m, oc[c], kk) : m;
+  }
+  if ((pc->overlay_flags & 32u) && sf->mask) { /* supervision mask, :619-635 */
+    float gx = fu * pc->vol_tx, gy = fv * pc->vol_ty;
+    float upx = (float)sf->mw / fmaxf((float)sf->gw - 1.0f, 1.0f);
+    float upy = (float)sf->mh / fmaxf((float)sf->gh - 1.0f, 1.0f);
+    float mxf = gx * upx, myf = gy * upy;
+    if (mxf > -1.0f && myf > -1.0f && mxf < (float)sf->mw && myf < (float)sf->mh) {
+      uint32_t mc = sf->mask[(size_t)(int)myf * sf->mw + (size_t)(int)mxf];
+      const float blue[3] = {0.25f, 0.45f, 1.0f}, orange[3] = {1.0f, 0.55f, 0.10f};
+      for (int c = 0; c < 3; c++) {
+        if (mc == 1u) rgb[c] = lerpf_(rgb[c], blue[c], 0.45f);
+        else if (mc >= 2u) rgb[c] = lerpf_(rgb[c], orange[c], 0.55f);
+      }
+    }
+  }
+}
+
 /* main(), :505-1038, for one dispatch thread (tx, ty) of the view */
 static void march(const r3d_frame_params *pc, const scene *s, const uint8_t lut[256][4],
                   const orc_opts *o, uint32_t tx, uint32_t ty, ray_out *out) {
@@ -462,6 +713,10 @@ static void march(const r3d_frame_params *pc, const scene *s, const uint8_t lut[
   out->store = 0;
   if (px >= pc->viewport[0] || py >= pc->viewport[1]) return;
   out->store = 1;
+  if (pc->view_flags & R3D_VIEW_SURF) {
+    surf_pixel(pc, s->br->surf, lut, o, px, py, out->rgb);
+    return;
+  }
   int ortho = (pc->view_flags & R3D_VIEW_ORTHO) != 0u;
   int vslab = pc->clip_valid == 0u && (pc->slab_grid & (1u << 24)) != 0u;
   int bricks = !vslab && pc->brick_mode != 0u; /* a virtual slab's brick_mode packs its grids */
@@ -908,6 +1163,14 @@ static void march(const r3d_frame_params *pc, const scene *s, const uint8_t lut[
 }
 
 static int check_view(const r3d_frame_params *p, const orc_cube *cube, const orc_bricks *br) {
+  if (p->view_flags & R3D_VIEW_SURF) { /* flattened segment: the baked window */
+    const orc_surf *sf = br ? br->surf : NULL;
+    if (!sf || !sf->vol || sf->gw < 3u || sf->gh < 3u || p->slab_nx != (float)sf->W ||
+        p->slab_ny != (float)sf->H || p->slab_wz != sf->L || !(p->slab_px > 0.0f) ||
+        p->mode >= R3D_MODE_COUNT)
+      return -1;
+    return 0;
+  }
   if ((p->overlay_flags & 0x1Du) &&
       (!(p->brick_mode & R3D_BRICK_LOD_FLAG) || !br || ((p->overlay_flags & 1u) && !br->ovl[0]) ||
        ((p->overlay_flags & 4u) && !br->ovl[1]) || ((p->overlay_flags & 8u) && !br->ovl[2]) ||
@@ -943,8 +1206,7 @@ static int check_view(const r3d_frame_params *p, const orc_cube *cube, const orc
     for (int l = 0; l < 6; l++)
       if (p->clip_orig[l][0] != cl->ox[l] || p->clip_orig[l][1] != cl->oy[l]) return -1;
   }
-  if ((p->view_flags & (R3D_VIEW_SURF | R3D_VIEW_STRETCH)) || p->mode >= R3D_MODE_COUNT)
-    return -1;
+  if (p->mode >= R3D_MODE_COUNT) return -1;
   if (vslab) {
     /* brick_mode packs the pyramid grids (checked above) */
   } else if (p->brick_mode & R3D_BRICK_LOD_FLAG) {

@@ -70,6 +70,19 @@ typedef struct orc_vslab {
   uint32_t *table;
 } orc_vslab;
 
+/* Flattened segment (src/shaders/surfvol.comp, raycast.slang:515-638):
+ * gw x gh grids of surface points (x, y, z, valid) and normals (x, y, z, -),
+ * the baked W x H x L flattened volume (CT and overlay bytes per texel, x
+ * fastest) and an optional mw x mh supervision mask. */
+typedef struct orc_surf {
+  const float *coords, *normals;
+  uint32_t gw, gh;
+  uint8_t *vol;
+  uint32_t W, H, L;
+  const uint8_t *mask;
+  uint32_t mw, mh;
+} orc_surf;
+
 /* Brick cache.  LOD mode (brick_mode with the LOD flag): the page table in
  * render3d's word format and a pool of 128^3 slots (slot s at
  * pool + s * 128^3, x fastest).  Single-level mode (no LOD flag,
@@ -90,6 +103,7 @@ typedef struct orc_bricks {
   const orc_slab *slab;
   const orc_clip *clip;
   const orc_vslab *vslab; /* virtual-slab views (slab_grid bit 24) */
+  const orc_surf *surf;   /* flattened-segment views (R3D_VIEW_SURF) */
 } orc_bricks;
 
 typedef struct orc_opts {
@@ -202,6 +216,13 @@ void orc_clip_fill(const uint8_t *vox, uint32_t nx, uint32_t ny, uint32_t nz, ui
  * included (vkbackend.c:6032-6057).  Ring layer of slice z: z % wz. */
 void orc_vslab_fill(orc_vslab *v, const uint8_t *vox, uint32_t nx, uint32_t ny, int64_t cx,
                     int64_t cy, int64_t zs0, uint32_t nz);
+
+/* The bake of surfvol.comp:98-153 over the whole window: texel (x, y, l)
+ * samples the LOD brick cache br (page, pool; ovl[ovl] into the second byte
+ * when ovl >= 0) at surface(u, v) + normal(u, v) * (zoff0 + l - nback),
+ * u = u0 + (x + 0.5) step, at the level of the xy pitch. */
+void orc_surf_bake(orc_surf *sf, const orc_bricks *br, float u0, float v0, float step,
+                   float zoff0, float sx, float sy, uint32_t nback, int ovl);
 
 /* Single-level brick atlas from a cubic volume of edge bpa * 128: atlas
  * level 0 ((abpa * 128)^3, slot s at (s % abpa, s / abpa % abpa,

@@ -185,6 +185,14 @@ def _load() -> C.CDLL:
         "r3d_cuda_clip_frame": (I, [P, C.c_double, C.c_double, C.c_uint64, P]),
         "r3d_cuda_clip_params": (None, [P, P]),
         "r3d_cuda_clip_read": (I, [P, U32, U32, P]),
+        "r3d_cuda_surf_begin": (I, [P, U32, U32, P, P]),
+        "r3d_cuda_surfvol_begin": (I, [P, U32, U32, U32, U32, F, F]),
+        "r3d_cuda_surfvol_window": (I, [P, C.c_double, C.c_double, F, F]),
+        "r3d_cuda_surfvol_overlay": (I, [P, I]),
+        "r3d_cuda_surfvol_mark": (I, [P]),
+        "r3d_cuda_surfvol_params": (None, [P, P]),
+        "r3d_cuda_surfvol_read": (I, [P, P]),
+        "r3d_cuda_surfmask": (I, [P, P, U32, U32]),
         "r3d_cuda_vslab_begin": (I, [P, C.POINTER(VolumeDesc), P, U32, U32, U32, U32]),
         "r3d_cuda_vslab_frame": (I, [P, C.c_double, C.c_double, C.c_int64, U32, P, P]),
         "r3d_cuda_vslab_params": (None, [P, P]),
@@ -532,6 +540,41 @@ class Context:
 
     def clip_params(self, p: "FrameParams") -> None:
         lib.r3d_cuda_clip_params(self.h, C.byref(p))
+
+    def surf_begin(self, coords, normals) -> None:
+        """Segment grids: (gh, gw, 4) float32 surface points (xyz, valid) and
+        normals, host arrays or device tensors."""
+        gh, gw = coords.shape[:2]
+        self._check(lib.r3d_cuda_surf_begin(self.h, gw, gh, _ptr(coords), _ptr(normals)))
+
+    def surfvol_begin(self, W: int, H: int, L: int, nback: int, sx: float, sy: float) -> None:
+        self._check(lib.r3d_cuda_surfvol_begin(self.h, W, H, L, nback, sx, sy))
+
+    def surfvol_window(self, u0: float, v0: float, step: float, zoff0: float) -> None:
+        self._check(lib.r3d_cuda_surfvol_window(self.h, u0, v0, step, zoff0))
+
+    def surfvol_overlay(self, atlas: int) -> None:
+        self._check(lib.r3d_cuda_surfvol_overlay(self.h, atlas))
+
+    def surfvol_mark(self) -> None:
+        self._check(lib.r3d_cuda_surfvol_mark(self.h))
+
+    def surfvol_params(self, p: "FrameParams") -> None:
+        lib.r3d_cuda_surfvol_params(self.h, C.byref(p))
+
+    def surfvol_read(self) -> np.ndarray:
+        p = FrameParams()
+        lib.r3d_cuda_surfvol_params(self.h, C.byref(p))
+        out = np.empty((p.slab_wz, int(p.slab_ny), int(p.slab_nx), 2), np.uint8)
+        self._check(lib.r3d_cuda_surfvol_read(self.h, _ptr(out)))
+        return out
+
+    def surfmask(self, m) -> None:
+        if m is None:
+            self._check(lib.r3d_cuda_surfmask(self.h, None, 0, 0))
+        else:
+            m = np.ascontiguousarray(m, np.uint8)
+            self._check(lib.r3d_cuda_surfmask(self.h, _ptr(m), m.shape[1], m.shape[0]))
 
     def vslab_begin(self, vol, W: int, H: int, D: int, z_margin: int = 0) -> None:
         nz, ny, nx = vol.shape

@@ -53,9 +53,9 @@ extern "C" int r3d_cuda_batch_create(r3d_cuda_ctx *c, const r3d_cuda_request *re
     }
     r3d_frame_params pc;
     int rc = prepare_view(c, v, v.viewport[0], v.viewport[1], pc);
-    if (rc >= 0 && (v.overlay_flags & kOvlAtlases))
-      rc = fail(c, R3D_E_UNSUPPORTED, "batch: request %u: overlay views render through "
-                                      "r3d_cuda_raycast_fwd", i);
+    if (rc >= 0 && ((v.overlay_flags & kOvlAtlases) || (v.view_flags & R3D_VIEW_SURF)))
+      rc = fail(c, R3D_E_UNSUPPORTED, "batch: request %u: overlay and surface views render "
+                                      "through r3d_cuda_raycast_fwd", i);
     if (rc < 0) {
       delete b;
       return rc;

@@ -283,6 +283,7 @@ void r3d_cuda_destroy(r3d_cuda_ctx *c) {
   slab_reset(c);
   clip_reset(c);
   vslab_reset(c);
+  surf_reset(c);
   if (c->page_ev) cudaEventDestroy(c->page_ev);
   cudaFree(c->diff_q);
   cudaFree(c->tape);
@@ -749,12 +750,45 @@ int r3d_cuda_cube_read(r3d_cuda_ctx *c, int level, uint8_t *out, uint32_t dims[3
 
 }  // extern "C"
 
-// Validates and sanitizes one view against the image (the rectangle rule of
-// src/vk/vkbackend.c:6871-6900).  Returns 1 to render, 0 to skip, < 0 error.
+// The view's rectangle clipped to the image (src/vk/vkbackend.c:6871-6900):
+// 1 to render, 0 when nothing of it is inside.
+static int view_rect(const r3d_frame_params &in, uint32_t out_w, uint32_t out_h,
+                     r3d_frame_params &pc) {
+  uint32_t ox = in.view_org & 0xffffu, oy = (in.view_org >> 16) & 0xffffu;
+  uint32_t vw = in.viewport[0] ? in.viewport[0] : out_w;
+  uint32_t vh = in.viewport[1] ? in.viewport[1] : out_h;
+  bool ok = ox < out_w && oy < out_h;
+  if (ok) {
+    vw = min(vw, out_w - ox);
+    vh = min(vh, out_h - oy);
+    ok = vw && vh;
+  }
+  pc.view_org = ox | (oy << 16);
+  pc.viewport[0] = ok ? vw : 0u;
+  pc.viewport[1] = ok ? vh : 0u;
+  return ok ? 1 : 0;
+}
+
+// Validates and sanitizes one view against the image.  Returns 1 to render,
+// 0 to skip, < 0 error.
 int prepare_view(r3d_cuda_ctx *c, const r3d_frame_params &in, uint32_t out_w,
                         uint32_t out_h, r3d_frame_params &pc) {
   pc = in;
   if (in.mode >= R3D_MODE_COUNT) return fail(c, R3D_E_INVALID, "view: mode %u", in.mode);
+  if (in.view_flags & R3D_VIEW_SURF) {  // flattened segment: the view must describe the window
+    if (!c->sv_vol || !c->sv_baked)
+      return fail(c, R3D_E_STATE, "view: no baked surface volume (r3d_cuda_surfvol_window)");
+    r3d_frame_params ref = in;
+    r3d_cuda_surfvol_params(c, &ref);
+    if (in.slab_x0 != ref.slab_x0 || in.slab_y0 != ref.slab_y0 || in.slab_px != ref.slab_px ||
+        in.slab_nx != ref.slab_nx || in.slab_ny != ref.slab_ny || in.slab_wz != ref.slab_wz ||
+        in.slab_grid != ref.slab_grid || in.max_mip != ref.max_mip ||
+        in.vol_tx != ref.vol_tx || in.vol_ty != ref.vol_ty)
+      return fail(c, R3D_E_INVALID, "view: surface parameters do not match the baked window "
+                                    "(r3d_cuda_surfvol_params)");
+    if (!(in.step_voxels > 0.0f)) return fail(c, R3D_E_INVALID, "view: step_voxels must be > 0");
+    return view_rect(in, out_w, out_h, pc);
+  }
   if (in.clip_valid) {  // clipmap: the view must describe the loaded levels
     if (!c->have_clip) return fail(c, R3D_E_STATE, "view: no clipmap loaded");
     r3d_frame_params ref;
@@ -803,8 +837,6 @@ int prepare_view(r3d_cuda_ctx *c, const r3d_frame_params &in, uint32_t out_w,
     if (in.overlay_flags & kOvlAtlases)
       return fail(c, R3D_E_UNSUPPORTED, "view: overlay atlases need the LOD brick cache");
   }
-  if (in.view_flags & (R3D_VIEW_SURF | R3D_VIEW_STRETCH))
-    return fail(c, R3D_E_UNSUPPORTED, "view: flattened-surface views are not implemented");
   if (in.overlay_flags & kOvlAtlases) {
     if (!(in.brick_mode & R3D_BRICK_LOD_FLAG))
       return fail(c, R3D_E_UNSUPPORTED, "view: overlay atlases need the LOD brick cache");
@@ -828,19 +860,7 @@ int prepare_view(r3d_cuda_ctx *c, const r3d_frame_params &in, uint32_t out_w,
   } else if (!in.slab_grid && !in.clip_valid && !c->have_cube) {
     return fail(c, R3D_E_STATE, "view: no volume uploaded");
   }
-  uint32_t ox = in.view_org & 0xffffu, oy = (in.view_org >> 16) & 0xffffu;
-  uint32_t vw = in.viewport[0] ? in.viewport[0] : out_w;
-  uint32_t vh = in.viewport[1] ? in.viewport[1] : out_h;
-  bool ok = ox < out_w && oy < out_h;
-  if (ok) {
-    vw = min(vw, out_w - ox);
-    vh = min(vh, out_h - oy);
-    ok = vw && vh;
-  }
-  pc.view_org = ox | (oy << 16);
-  pc.viewport[0] = ok ? vw : 0u;
-  pc.viewport[1] = ok ? vh : 0u;
-  return ok ? 1 : 0;
+  return view_rect(in, out_w, out_h, pc);
 }
 
 // Persistent launches for the renderable views of one call: views sharing a
@@ -998,10 +1018,12 @@ int r3d_cuda_raycast_fwd(r3d_cuda_ctx *c, const r3d_frame_params *views, uint32_
     }
   }
   R3D_CUDA_TRY(c, cudaEventRecord(c->ev0, st));
-  // views with overlay atlases render through the grid kernel
+  // views with overlay atlases and flattened-segment views render through
+  // their own grid kernels
   bool any_ovl = false;
   for (uint32_t v = 0; v < nviews; v++)
-    any_ovl = any_ovl || (render[v] && (pcs[v].overlay_flags & kOvlAtlases));
+    any_ovl = any_ovl || (render[v] && ((pcs[v].overlay_flags & kOvlAtlases) ||
+                                        (pcs[v].view_flags & R3D_VIEW_SURF)));
   if (c->sched.persistent && !any_ovl) {
     int rc = launch_views_persistent(c, pcs, render, nviews, img, out_w, steps, mip, total,
                                      counters, st);

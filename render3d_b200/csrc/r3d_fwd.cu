@@ -207,6 +207,8 @@ cudaError_t launch_view(const r3d_cuda_ctx *c, const r3d_frame_params &pc, uint8
                         uint32_t out_w, uint32_t *steps, uint32_t *mip_index,
                         unsigned long long *total, unsigned long long *counters,
                         cudaStream_t stream) {
+  if (pc.view_flags & R3D_VIEW_SURF)
+    return launch_surf(c, pc, img, out_w, steps, mip_index, stream);
   const DevScene s = c->scene();
   const bool fast = c->quality == R3D_QUALITY_FAST;
   const uint32_t shade = c->sched.shade_group;

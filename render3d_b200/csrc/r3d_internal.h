@@ -83,6 +83,18 @@ struct r3d_cuda_ctx {
   bool have_vslab = false;
   r3d::DevVslab vs{};
 
+  // flattened-segment views: the segment grids (xyz + valid, normals), the
+  // baked flattened volume (W x H x L texels of CT, overlay) and its window,
+  // the supervision mask
+  float4 *surf_coords = nullptr, *surf_normals = nullptr;
+  uint32_t surf_gw = 0, surf_gh = 0;
+  uint8_t *sv_vol = nullptr, *surf_mask = nullptr;
+  uint32_t surf_mw = 0, surf_mh = 0;
+  uint32_t sv_W = 0, sv_H = 0, sv_L = 0, sv_nback = 0;
+  float sv_sx = 0.0f, sv_sy = 0.0f, sv_u0 = 0.0f, sv_v0 = 0.0f, sv_step = 0.0f, sv_zoff0 = 0.0f;
+  int sv_ovl = -1;  // overlay atlas baked into G (-1: none)
+  bool sv_baked = false;
+
   // single-level brick atlas: 4 mip levels, then the world-indexed
   // occupancy grid, in one allocation; page table of bpa^3 entries
   uint8_t *shard_buf = nullptr;
@@ -168,6 +180,10 @@ cudaError_t launch_path(const r3d_frame_params &pc, const DevScene &s, bool fast
                         uint32_t *mip, unsigned long long *total, unsigned long long *cnt,
                         uint32_t shade, cudaStream_t st);
 
+// Flattened-segment view (view_flags R3D_VIEW_SURF) into a device image.
+cudaError_t launch_surf(const r3d_cuda_ctx *c, const r3d_frame_params &pc, uint8_t *img,
+                        uint32_t out_w, uint32_t *steps, uint32_t *mip, cudaStream_t st);
+
 // Forward launch of one sanitized view into a device image.
 cudaError_t launch_view(const r3d_cuda_ctx *c, const r3d_frame_params &pc, uint8_t *img,
                         uint32_t out_w, uint32_t *steps, uint32_t *mip_index,
@@ -186,6 +202,7 @@ void stream_reset(r3d_cuda_ctx *c);
 void slab_reset(r3d_cuda_ctx *c);
 void clip_reset(r3d_cuda_ctx *c);
 void vslab_reset(r3d_cuda_ctx *c);
+void surf_reset(r3d_cuda_ctx *c);
 uint32_t atlas_bpa(uint32_t nslots);
 
 // Validates one view and clips its rect to the image (1: render, 0: empty

@@ -66,8 +66,9 @@ extern "C" int r3d_cuda_raycast_fwd_noalloc(r3d_cuda_ctx *c, const r3d_frame_par
   for (uint32_t v = 0; v < nviews; v++) {
     render[v] = prepare_view(c, views[v], out_w, out_h, pcs[v]);
     if (render[v] < 0) return render[v];
-    if (views[v].overlay_flags & kOvlAtlases)
-      return fail(c, R3D_E_UNSUPPORTED, "raycast_fwd_noalloc: overlay views are not supported");
+    if ((views[v].overlay_flags & kOvlAtlases) || (views[v].view_flags & R3D_VIEW_SURF))
+      return fail(c, R3D_E_UNSUPPORTED,
+                  "raycast_fwd_noalloc: overlay and surface views are not supported");
   }
   // views sharing a sampling path and mode form one launch
   DevView hv[kNoallocViews];
