@@ -817,8 +817,9 @@ def stream_bench(rb, torch, lut, nslots: int = 1024, budget: int = 16,
 
 def sections_bench(rb, torch, lut, frames: int) -> dict:
     """Whole cross-sections of an 8192 x 8192 x 64 phantom (4 GiB, generated
-    on the device) in the two modes built for them: the tiled slab (ring of
-    32 slices) and the XY clipmap (window depth 32).  A 1920x1080 camera
+    on the device) in the three modes built for them: the tiled slab (ring
+    of 32 slices), the XY clipmap (window depth 32) and the virtual slab
+    (vslab_bench).  A 1920x1080 camera
     faces the section and pans across it; each mode is timed rendering a
     fixed window, and with a per-frame update (slab: the window scrolls one
     slice; clip: the focus follows the pan and the window scrolls one slice,
@@ -831,6 +832,7 @@ def sections_bench(rb, torch, lut, frames: int) -> dict:
         ctx.set_transfer(lut)
         ctx.set_alpha_cutoff(CUTOFF)
         vol = ctx.phantom((nx, ny, nz), seed=SEED)
+        out["vslab"] = vslab_bench(rb, torch, lut, vol, frames)
         t0 = time.perf_counter()
         ctx.slab_build(vol, wz, 0)
         torch.cuda.synchronize()
@@ -892,6 +894,137 @@ def sections_bench(rb, torch, lut, frames: int) -> dict:
     return out
 
 
+def vslab_bench(rb, torch, lut, vol, frames: int) -> dict:
+    """The virtual slab over the same volume: the whole 8192^2 x 30 section
+    (fixed, then scrolling one slice every 4 frames with 64 cell fills a
+    frame), and a 4096^2 x 30 window with a 16-slice z margin panning across
+    the volume (16 fills a frame).  Device time of fills and frames with
+    CUDA events on the context stream; fills are counted per frame."""
+    nz, ny, nx = vol.shape
+    out = {}
+    for name, (Wn, Hn, zm, budget, pan) in {
+            "whole_section": (nx, ny, 0, 64, False),
+            "window_4096_pan": (4096, 4096, 16, 16, True)}.items():
+        ctx = rb.Context(0)
+        try:
+            ctx.set_transfer(lut)
+            ctx.set_alpha_cutoff(CUTOFF)
+            D = 30
+            ctx.vslab_begin(vol, Wn, Hn, D, zm)
+            img = torch.zeros((H, W, 4), dtype=torch.uint8, device="cuda")
+            tot = torch.zeros(1, dtype=torch.int64, device="cuda")
+            st = torch.cuda.ExternalStream(ctx.stream)
+            ext = (1.0, Hn / Wn, D / Wn)
+
+            def frame(i, update):
+                fx = (0.3 + 0.4 * (i % 240) / 240.0) * nx if pan else nx / 2
+                z0 = (i // 4) % (nz - D - 2) if update else 8
+                s = ctx.vslab_frame(fx, ny / 2, z0, budget)
+                p = rb.camera_view(0.05 * math.sin(i * 0.05), 0.02, 0.12 * Wn / nx, W, H, lut,
+                                   target=(0.5, 0.5 * ext[1], 0.5 * ext[2]),
+                                   step_voxels=STEP_VOXELS, frame_index=i)
+                ctx.vslab_params(p)
+                p.density = 6.0
+                ctx.raycast(p, W, H, out=img, total=tot, stream=ctx.stream)
+                return s["jobs"]
+            for i in range(12):  # fill the window
+                frame(i, False)
+            res = {}
+            for mode, update in (("fixed", False), ("moving", True)):
+                torch.cuda.synchronize()
+                tot.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                jobs = 0
+                e0.record(st)
+                for i in range(12, 12 + frames):
+                    jobs += frame(i, update)
+                e1.record(st)
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1) / frames
+                res[mode] = {"ms_per_frame": ms, "fps": 1000.0 / ms,
+                             "fills_per_frame": jobs / frames,
+                             "gsamples_per_s": tot.item() / frames / (ms * 1e-3) / 1e9}
+            lay = ctx.vslab_layout()
+            res["tiles"] = lay.ntiles
+            res["tile_gb"] = lay.ntiles * (lay.px + 2) ** 2 * lay.wz / 1e9
+            out[name] = res
+        finally:
+            ctx.close()
+    return out
+
+
+def surf_bench(rb, torch, lut, frames: int) -> dict:
+    """Flattened-segment views over the 1024^3 LOD brick cache: a wavy sheet
+    (513 x 513 grid of 2-voxel cells) baked into a 2048 x 2048 x 96
+    flattened volume at pitch 0.5 and 2 voxels, then 1920x1080 surf views in
+    FULL at two zooms.  Bake and frame times with CUDA events."""
+    n = N_EDGE
+    ctx = rb.Context(0)
+    try:
+        ctx.set_transfer(lut)
+        ctx.set_alpha_cutoff(CUTOFF)
+        vol = ctx.phantom(n, seed=SEED)
+        ctx.bricks_build(vol, NLEV)
+        del vol
+        g = 513
+        j, i = np.mgrid[0:g, 0:g].astype(np.float64)
+        x, y = 0.5 * n - 512.0 + 2.0 * i, 0.5 * n - 512.0 + 2.0 * j
+        z = 0.5 * n + 60.0 * np.sin(x / 90.0) + 40.0 * np.cos(y / 130.0)
+        nrm = np.stack([-60.0 / 90.0 * np.cos(x / 90.0), 40.0 / 130.0 * np.sin(y / 130.0),
+                        np.ones_like(x)], -1)
+        nrm /= np.linalg.norm(nrm, axis=-1, keepdims=True)
+        coords = np.zeros((g, g, 4), np.float32)
+        coords[..., 0], coords[..., 1], coords[..., 2], coords[..., 3] = x, y, z, 1.0
+        normals = np.zeros((g, g, 4), np.float32)
+        normals[..., :3] = nrm
+        ctx.surf_begin(coords, normals)
+        Wv, Hv, Lv = 2048, 2048, 96
+        ctx.surfvol_begin(Wv, Hv, Lv, Lv // 2, 0.5, 0.5)
+        st = torch.cuda.ExternalStream(ctx.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        out = {"workload": "1024^3 LOD bricks, 513^2 segment grid, 2048x2048x96 flattened "
+                           "volume, 1920x1080 surf views"}
+        img = torch.zeros((H, W, 4), dtype=torch.uint8, device="cuda")
+        for step in (0.5, 2.0):
+            ctx.surfvol_window(0.0, 0.0, step, 0.0)  # warm
+            torch.cuda.synchronize()
+            e0.record(st)
+            for k in range(5):
+                ctx.surfvol_window(float(k), 0.0, step, 0.0)
+            e1.record(st)
+            torch.cuda.synchronize()
+            bake_ms = e0.elapsed_time(e1) / 5
+            span = Wv * step
+            res = {"bake_ms": bake_ms,
+                   "bake_gtexels_per_s": Wv * Hv * Lv / (bake_ms * 1e-3) / 1e9}
+            for zoom, half_w in (("whole_window", 0.5 * span), ("quarter", 0.125 * span)):
+                def frame(i):
+                    p = rb.FrameParams()
+                    p.viewport[0], p.viewport[1] = W, H
+                    p.mode = 0
+                    p.cam_origin[:] = (0.5 * span + 4.0 * math.sin(i * 0.1), 0.5 * span, 0.0)
+                    p.cam_right[:] = (half_w, 0.0, 0.0)
+                    p.cam_up[:] = (0.0, half_w * H / W, 0.0)
+                    p.step_voxels, p.density, p.threshold = 0.5, 1.5, 0.02
+                    p.slab_z0, p.slab_depth, p.frame_index = 0.0, 64, i
+                    ctx.surfvol_params(p)
+                    ctx.raycast(p, W, H, out=img, stream=ctx.stream)
+                for i in range(5):
+                    frame(i)
+                torch.cuda.synchronize()
+                e0.record(st)
+                for i in range(frames):
+                    frame(i)
+                e1.record(st)
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1) / frames
+                res[zoom] = {"ms_per_frame": ms, "fps": 1000.0 / ms}
+            out[f"pitch_{step}"] = res
+        return out
+    finally:
+        ctx.close()
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -904,7 +1037,7 @@ def main() -> None:
     ap.add_argument("--no-fwd-bwd", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--workload", default="orbit1024",
-                    choices=["orbit1024", "sparse2048", "sections8192"],
+                    choices=["orbit1024", "sparse2048", "sections8192", "surf1024"],
                     help="sparse2048: the large sparse volume and 512^3 adjoint (extra line)")
     ap.add_argument("--profile", type=int, default=0, metavar="N",
                     help="only build the workload and render N orbit frames (for ncu)")
@@ -930,6 +1063,11 @@ def main() -> None:
         run_reference(args)
     elif args.workload == "sparse2048":
         run_sparse(args)
+    elif args.workload == "surf1024":
+        import torch
+        import render3d_b200 as rb
+        print(json.dumps(surf_bench(rb, torch, rb.scroll_ramp_tf(), max(args.steps // 5, 60))),
+              flush=True)
     elif args.workload == "sections8192":
         import torch
         import render3d_b200 as rb

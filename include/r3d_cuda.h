@@ -328,6 +328,17 @@ int r3d_cuda_raycast_fwd(r3d_cuda_ctx *ctx, const r3d_frame_params *views, uint3
                          uint8_t *rgba_out, uint32_t out_w, uint32_t out_h,
                          const r3d_cuda_aux *aux, void *stream);
 
+/* Dispatch rows [row0, row1) of one view into the device image (rows of
+ * the halved grid for half-resolution views; row0 is rounded down to a
+ * multiple of 8).  No counterpart in the reference: the headless render
+ * layer draws a frame as row bands on two streams so that each band's
+ * device-to-host copy overlaps the bands still rendering (r3d_read_frame).
+ * Every pixel equals the one r3d_cuda_raycast_fwd renders.  Surface views
+ * are rejected (R3D_E_UNSUPPORTED). */
+int r3d_cuda_raycast_rows(r3d_cuda_ctx *ctx, const r3d_frame_params *view, uint8_t *rgba_out,
+                          uint32_t out_w, uint32_t out_h, uint32_t row0, uint32_t row1,
+                          void *stream);
+
 /* Forward raycast that allocates no device memory.  No counterpart in the
  * reference: it exists for callers that must not let the library allocate
  * while they render -- applications that give the renderer a fixed device-

@@ -216,6 +216,7 @@ def _load() -> C.CDLL:
         "r3d_cuda_shard_mode": (U32, [P]),
         "r3d_cuda_shard_read": (I, [P, I, P, P, P]),
         "r3d_cuda_raycast_fwd": (I, [P, P, U32, P, U32, U32, C.POINTER(CudaAux), P]),
+        "r3d_cuda_raycast_rows": (I, [P, P, P, U32, U32, U32, U32, P]),
         "r3d_cuda_last_kernel_ns": (I, [P, C.POINTER(C.c_uint64)]),
         "r3d_cuda_fmath_eval": (I, [P, P, P, P, U32]),
         "r3d_cuda_set_schedule": (I, [P, C.POINTER(Schedule)]),
@@ -575,6 +576,12 @@ class Context:
         else:
             m = np.ascontiguousarray(m, np.uint8)
             self._check(lib.r3d_cuda_surfmask(self.h, _ptr(m), m.shape[1], m.shape[0]))
+
+    def raycast_rows(self, p: "FrameParams", out, out_w: int, out_h: int, row0: int, row1: int,
+                     stream: int = 0) -> None:
+        """Dispatch rows [row0, row1) of one view into a device image."""
+        self._check(lib.r3d_cuda_raycast_rows(self.h, C.byref(p), _ptr(out), out_w, out_h, row0,
+                                              row1, stream or None))
 
     def vslab_begin(self, vol, W: int, H: int, D: int, z_margin: int = 0) -> None:
         nz, ny, nx = vol.shape

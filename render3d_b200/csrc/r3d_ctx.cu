@@ -964,6 +964,27 @@ int r3d_cuda_get_schedule(const r3d_cuda_ctx *c, r3d_cuda_schedule *sc) {
   return R3D_OK;
 }
 
+int r3d_cuda_raycast_rows(r3d_cuda_ctx *c, const r3d_frame_params *view, uint8_t *rgba_out,
+                          uint32_t out_w, uint32_t out_h, uint32_t row0, uint32_t row1,
+                          void *stream) {
+  if (!c || !view || !rgba_out || !out_w || !out_h || out_w > 65535u || out_h > 65535u)
+    return fail(c, R3D_E_INVALID, "raycast_rows: bad arguments");
+  if (!is_device_ptr(rgba_out))
+    return fail(c, R3D_E_INVALID, "raycast_rows: the image must be device memory");
+  if (view->view_flags & R3D_VIEW_SURF)
+    return fail(c, R3D_E_UNSUPPORTED, "raycast_rows: surface views render whole");
+  cudaSetDevice(c->device);
+  r3d_frame_params pc;
+  const int rc = prepare_view(c, *view, out_w, out_h, pc);
+  if (rc <= 0) return rc;
+  Rows rows;
+  rows.row0 = row0;
+  rows.row1 = row1;
+  R3D_CUDA_TRY(c, launch_view(c, pc, rgba_out, out_w, nullptr, nullptr, nullptr, nullptr,
+                              stream ? (cudaStream_t)stream : c->stream, rows));
+  return R3D_OK;
+}
+
 int r3d_cuda_raycast_fwd(r3d_cuda_ctx *c, const r3d_frame_params *views, uint32_t nviews,
                          uint8_t *rgba_out, uint32_t out_w, uint32_t out_h,
                          const r3d_cuda_aux *aux, void *stream) {

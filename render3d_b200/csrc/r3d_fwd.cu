@@ -43,7 +43,7 @@ __global__ void R3D_FWD_BOUNDS k_raycast(const __grid_constant__ r3d_frame_param
                                          uint32_t *__restrict__ mip_out,
                                          unsigned long long *__restrict__ total,
                                          unsigned long long *__restrict__ counters,
-                                         uint32_t shade_min) {
+                                         uint32_t shade_min, uint32_t row0) {
   __shared__ float4 tf[256];
   for (uint32_t i = threadIdx.x; i < 256u; i += blockDim.x) {
     uchar4 u = lut[i];
@@ -54,7 +54,7 @@ __global__ void R3D_FWD_BOUNDS k_raycast(const __grid_constant__ r3d_frame_param
   const uint32_t lx = (lane & 1u) | ((lane >> 1) & 2u) | ((lane >> 2) & 4u);
   const uint32_t ly = ((lane >> 1) & 1u) | ((lane >> 2) & 2u);
   const uint32_t tx = blockIdx.x * kBlockW + (warp & 1u) * 8u + lx;
-  const uint32_t ty = blockIdx.y * kBlockH + (warp >> 1) * 4u + ly;
+  const uint32_t ty = row0 + blockIdx.y * kBlockH + (warp >> 1) * 4u + ly;
   const bool half = (pc.view_flags & R3D_VIEW_HALF) != 0u;
   const uint32_t px = half ? tx * 2u : tx, py = half ? ty * 2u : ty;
   const uint32_t vw = pc.viewport[0], vh = pc.viewport[1];
@@ -130,11 +130,14 @@ template <int PATH, int MODE, bool FAST>
 static cudaError_t launch_t(const r3d_frame_params &pc, const DevScene &s, const uchar4 *lut,
                             uint8_t *img, uint32_t out_w, uint32_t *steps, uint32_t *mip,
                             unsigned long long *total, unsigned long long *counters,
-                            uint32_t shade, cudaStream_t stream) {
+                            uint32_t shade, const Rows &rows, cudaStream_t stream) {
   const bool half = (pc.view_flags & R3D_VIEW_HALF) != 0u;
   uint32_t gw = half ? (pc.viewport[0] + 1u) / 2u : pc.viewport[0];
   uint32_t gh = half ? (pc.viewport[1] + 1u) / 2u : pc.viewport[1];
-  dim3 grid((gw + kBlockW - 1u) / kBlockW, (gh + kBlockH - 1u) / kBlockH);
+  // dispatch rows [row0, row1) of the view; row0 starts a block row
+  const uint32_t row0 = rows.row0 / kBlockH * kBlockH, row1 = min(rows.row1, gh);
+  if (row0 >= row1) return cudaSuccess;
+  dim3 grid((gw + kBlockW - 1u) / kBlockW, (row1 - row0 + kBlockH - 1u) / kBlockH);
   const uint32_t threads = kFwdWarps * 32u;
   constexpr bool kDeferable = MODE == R3D_MODE_FULL;
   // overlay atlases: LOD bricks in the compositing and MIP modes
@@ -144,26 +147,26 @@ static cudaError_t launch_t(const r3d_frame_params &pc, const DevScene &s, const
     if (pc.overlay_flags & kOvlAtlases) {
       if (counters)
         k_raycast<PATH, MODE, FAST, true, false, true><<<grid, threads, 0, stream>>>(
-            pc, s, lut, (uchar4 *)img, out_w, steps, mip, total, counters, 0u);
+            pc, s, lut, (uchar4 *)img, out_w, steps, mip, total, counters, 0u, row0);
       else
         k_raycast<PATH, MODE, FAST, false, false, true><<<grid, threads, 0, stream>>>(
-            pc, s, lut, (uchar4 *)img, out_w, steps, mip, total, nullptr, 0u);
+            pc, s, lut, (uchar4 *)img, out_w, steps, mip, total, nullptr, 0u, row0);
       return cudaGetLastError();
     }
   }
   if (kDeferable && shade) {
     if (counters)
       k_raycast<PATH, MODE, FAST, true, kDeferable><<<grid, threads, 0, stream>>>(
-          pc, s, lut, (uchar4 *)img, out_w, steps, mip, total, counters, shade);
+          pc, s, lut, (uchar4 *)img, out_w, steps, mip, total, counters, shade, row0);
     else
       k_raycast<PATH, MODE, FAST, false, kDeferable><<<grid, threads, 0, stream>>>(
-          pc, s, lut, (uchar4 *)img, out_w, steps, mip, total, nullptr, shade);
+          pc, s, lut, (uchar4 *)img, out_w, steps, mip, total, nullptr, shade, row0);
   } else if (counters) {
     k_raycast<PATH, MODE, FAST, true, false><<<grid, threads, 0, stream>>>(
-        pc, s, lut, (uchar4 *)img, out_w, steps, mip, total, counters, 0u);
+        pc, s, lut, (uchar4 *)img, out_w, steps, mip, total, counters, 0u, row0);
   } else {
     k_raycast<PATH, MODE, FAST, false, false><<<grid, threads, 0, stream>>>(
-        pc, s, lut, (uchar4 *)img, out_w, steps, mip, total, nullptr, 0u);
+        pc, s, lut, (uchar4 *)img, out_w, steps, mip, total, nullptr, 0u, row0);
   }
   return cudaGetLastError();
 }
@@ -172,22 +175,23 @@ template <int PATH>
 static cudaError_t launch_p(const r3d_frame_params &pc, const DevScene &s, bool fast,
                             const uchar4 *lut, uint8_t *img, uint32_t out_w, uint32_t *steps,
                             uint32_t *mip, unsigned long long *total,
-                            unsigned long long *cnt, uint32_t shade, cudaStream_t st) {
+                            unsigned long long *cnt, uint32_t shade, const Rows &rows,
+                            cudaStream_t st) {
   switch (pc.mode) {
     case R3D_MODE_FULL:
-      return fast ? launch_t<PATH, R3D_MODE_FULL, true>(pc, s, lut, img, out_w, steps, mip, total, cnt, shade, st)
+      return fast ? launch_t<PATH, R3D_MODE_FULL, true>(pc, s, lut, img, out_w, steps, mip, total, cnt, shade, rows, st)
                   : launch_t<PATH, R3D_MODE_FULL, false>(pc, s, lut, img, out_w, steps, mip,
-                                                         total, cnt, shade, st);
+                                                         total, cnt, shade, rows, st);
     case R3D_MODE_MIP:
-      return launch_t<PATH, R3D_MODE_MIP, false>(pc, s, lut, img, out_w, steps, mip, total, cnt, shade, st);
+      return launch_t<PATH, R3D_MODE_MIP, false>(pc, s, lut, img, out_w, steps, mip, total, cnt, shade, rows, st);
     case R3D_MODE_DEPTH:
-      return launch_t<PATH, R3D_MODE_DEPTH, false>(pc, s, lut, img, out_w, steps, mip, total, cnt, shade, st);
+      return launch_t<PATH, R3D_MODE_DEPTH, false>(pc, s, lut, img, out_w, steps, mip, total, cnt, shade, rows, st);
     case R3D_MODE_HEATMAP:
-      return launch_t<PATH, R3D_MODE_HEATMAP, false>(pc, s, lut, img, out_w, steps, mip, total, cnt, shade, st);
+      return launch_t<PATH, R3D_MODE_HEATMAP, false>(pc, s, lut, img, out_w, steps, mip, total, cnt, shade, rows, st);
     case R3D_MODE_RAYDIR:
-      return launch_t<PATH, R3D_MODE_RAYDIR, false>(pc, s, lut, img, out_w, steps, mip, total, cnt, shade, st);
+      return launch_t<PATH, R3D_MODE_RAYDIR, false>(pc, s, lut, img, out_w, steps, mip, total, cnt, shade, rows, st);
     default:
-      return launch_t<PATH, R3D_MODE_FLAT, false>(pc, s, lut, img, out_w, steps, mip, total, cnt, shade, st);
+      return launch_t<PATH, R3D_MODE_FLAT, false>(pc, s, lut, img, out_w, steps, mip, total, cnt, shade, rows, st);
   }
 }
 
@@ -199,14 +203,16 @@ template <>
 cudaError_t launch_path<R3D_FWD_PATH>(const r3d_frame_params &pc, const DevScene &s, bool fast,
                                       const uchar4 *lut, uint8_t *img, uint32_t out_w,
                                       uint32_t *steps, uint32_t *mip, unsigned long long *total,
-                                      unsigned long long *cnt, uint32_t shade, cudaStream_t st) {
-  return launch_p<R3D_FWD_PATH>(pc, s, fast, lut, img, out_w, steps, mip, total, cnt, shade, st);
+                                      unsigned long long *cnt, uint32_t shade, const Rows &rows,
+                                      cudaStream_t st) {
+  return launch_p<R3D_FWD_PATH>(pc, s, fast, lut, img, out_w, steps, mip, total, cnt, shade, rows,
+                                st);
 }
 #else
 cudaError_t launch_view(const r3d_cuda_ctx *c, const r3d_frame_params &pc, uint8_t *img,
                         uint32_t out_w, uint32_t *steps, uint32_t *mip_index,
                         unsigned long long *total, unsigned long long *counters,
-                        cudaStream_t stream) {
+                        cudaStream_t stream, const Rows &rows) {
   if (pc.view_flags & R3D_VIEW_SURF)
     return launch_surf(c, pc, img, out_w, steps, mip_index, stream);
   const DevScene s = c->scene();
@@ -215,7 +221,7 @@ cudaError_t launch_view(const r3d_cuda_ctx *c, const r3d_frame_params &pc, uint8
 #define R3D_PATH_CASE(P)                                                                   \
   case P:                                                                                  \
     return launch_path<P>(pc, s, fast, c->lut, img, out_w, steps, mip_index, total, counters, \
-                          shade, stream)
+                          shade, rows, stream)
   switch (path_of_view(pc)) {
     R3D_PATH_CASE(PATH_VSLAB);
     R3D_PATH_CASE(PATH_CLIP);
@@ -224,7 +230,7 @@ cudaError_t launch_view(const r3d_cuda_ctx *c, const r3d_frame_params &pc, uint8
     R3D_PATH_CASE(PATH_SHARD);
     default:
       return launch_path<PATH_CUBE>(pc, s, fast, c->lut, img, out_w, steps, mip_index, total,
-                                    counters, shade, stream);
+                                    counters, shade, rows, stream);
   }
 #undef R3D_PATH_CASE
 }

@@ -173,12 +173,18 @@ inline cudaError_t copy_sync(cudaStream_t s, void *dst, const void *src, size_t 
   return e == cudaSuccess ? cudaStreamSynchronize(s) : e;
 }
 
+// Dispatch rows [row0, row1) of a view (half-resolution views: rows of the
+// halved grid); row0 is rounded down to a block row.
+struct Rows {
+  uint32_t row0 = 0u, row1 = 0xffffffffu;
+};
+
 // The forward launch of one sampling path (each defined in its own object).
 template <int PATH>
 cudaError_t launch_path(const r3d_frame_params &pc, const DevScene &s, bool fast,
                         const uchar4 *lut, uint8_t *img, uint32_t out_w, uint32_t *steps,
                         uint32_t *mip, unsigned long long *total, unsigned long long *cnt,
-                        uint32_t shade, cudaStream_t st);
+                        uint32_t shade, const Rows &rows, cudaStream_t st);
 
 // Flattened-segment view (view_flags R3D_VIEW_SURF) into a device image.
 cudaError_t launch_surf(const r3d_cuda_ctx *c, const r3d_frame_params &pc, uint8_t *img,
@@ -188,7 +194,7 @@ cudaError_t launch_surf(const r3d_cuda_ctx *c, const r3d_frame_params &pc, uint8
 cudaError_t launch_view(const r3d_cuda_ctx *c, const r3d_frame_params &pc, uint8_t *img,
                         uint32_t out_w, uint32_t *steps, uint32_t *mip_index,
                         unsigned long long *total, unsigned long long *counters,
-                        cudaStream_t stream);
+                        cudaStream_t stream, const Rows &rows = Rows());
 
 }  // namespace r3d
 

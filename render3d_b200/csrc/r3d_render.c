@@ -5,7 +5,11 @@
  * the offscreen RGBA8 image lives in device memory, each view is one
  * raycast launch into its rect, frames are paced two in flight, and the GPU
  * raycast time of a frame is reported two frames later, as the reference's
- * timestamp queries are. */
+ * timestamp queries are.  A frame of one view covering the whole image is
+ * drawn as row bands, each on its own stream so that they run
+ * concurrently (a band waiting for the previous one would pay its slowest
+ * block); r3d_read_frame then copies each band to the host as soon as it is
+ * done, so the copy of a frame overlaps its rendering. */
 #include "r3d_render.h"
 
 #include <cuda_runtime_api.h>
@@ -17,6 +21,7 @@
 #include "r3d_cuda.h"
 
 #define FRAMES_IN_FLIGHT 2
+#define BANDS 3
 
 struct r3d_renderer {
   r3d_cuda_ctx *ctx;
@@ -28,6 +33,13 @@ struct r3d_renderer {
   uint32_t slot;
   cudaEvent_t ev_begin[FRAMES_IN_FLIGHT], ev_end[FRAMES_IN_FLIGHT];
   int ev_used[FRAMES_IN_FLIGHT];
+  /* banded frames: the render streams of bands 1.. (band 0 runs on the
+   * context's stream), the copy stream, one event per band and the image
+   * rows of band k, [band_row[k], band_row[k + 1]) */
+  cudaStream_t band_stream[BANDS - 1], copy_stream;
+  cudaEvent_t band_ev[BANDS];
+  uint32_t nbands; /* bands of the last frame; 0: drawn whole */
+  uint32_t band_row[BANDS + 1];
 };
 
 static uint64_t now_ns(void) {
@@ -74,6 +86,20 @@ int r3d_create(SDL_Window *win, const r3d_config *cfg, r3d_renderer **out) {
       r3d_destroy(r);
       return -1;
     }
+  if (cudaStreamCreateWithFlags(&r->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    r3d_destroy(r);
+    return -1;
+  }
+  for (int i = 0; i < BANDS - 1; i++)
+    if (cudaStreamCreateWithFlags(&r->band_stream[i], cudaStreamNonBlocking) != cudaSuccess) {
+      r3d_destroy(r);
+      return -1;
+    }
+  for (int i = 0; i < BANDS; i++)
+    if (cudaEventCreateWithFlags(&r->band_ev[i], cudaEventDisableTiming) != cudaSuccess) {
+      r3d_destroy(r);
+      return -1;
+    }
   *out = r;
   return 0;
 }
@@ -81,10 +107,18 @@ int r3d_create(SDL_Window *win, const r3d_config *cfg, r3d_renderer **out) {
 void r3d_destroy(r3d_renderer *r) {
   if (!r) return;
   if (r->ctx) cudaStreamSynchronize((cudaStream_t)r3d_cuda_stream(r->ctx));
+  for (int i = 0; i < BANDS - 1; i++)
+    if (r->band_stream[i]) cudaStreamSynchronize(r->band_stream[i]);
+  if (r->copy_stream) cudaStreamSynchronize(r->copy_stream);
   for (int i = 0; i < FRAMES_IN_FLIGHT; i++) {
     if (r->ev_begin[i]) cudaEventDestroy(r->ev_begin[i]);
     if (r->ev_end[i]) cudaEventDestroy(r->ev_end[i]);
   }
+  for (int i = 0; i < BANDS; i++)
+    if (r->band_ev[i]) cudaEventDestroy(r->band_ev[i]);
+  for (int i = 0; i < BANDS - 1; i++)
+    if (r->band_stream[i]) cudaStreamDestroy(r->band_stream[i]);
+  if (r->copy_stream) cudaStreamDestroy(r->copy_stream);
   cudaFree(r->offscreen);
   r3d_cuda_destroy(r->ctx);
   free(r);
@@ -190,8 +224,36 @@ int r3d_frame_views(r3d_renderer *r, const r3d_frame_params *views, uint32_t nvi
   if (st) st->cpu_wait_ns = now_ns() - t0;
   t0 = now_ns();
   if (cudaEventRecord(r->ev_begin[slot], stream) != cudaSuccess) return -1;
-  int rc = r3d_cuda_raycast_fwd(r->ctx, views, nviews, r->offscreen, r->w, r->h, NULL, stream);
-  if (rc != R3D_OK) return report(r, "frame", rc);
+  const r3d_frame_params *v = views;
+  const int whole = nviews == 1u && !(v->view_flags & R3D_VIEW_SURF) && v->view_org == 0u &&
+                    (v->viewport[0] == 0u || v->viewport[0] == r->w) &&
+                    (v->viewport[1] == 0u || v->viewport[1] == r->h) && r->h >= 256u;
+  r->nbands = 0;
+  if (whole) {
+    /* row bands (multiples of 8 dispatch rows), band k > 0 on band stream
+     * k - 1, which starts after this frame's begin event; the context's
+     * stream then waits for every band */
+    const int half = (v->view_flags & R3D_VIEW_HALF) != 0u;
+    const uint32_t gh = half ? (r->h + 1u) / 2u : r->h;
+    const uint32_t rb = ((gh + BANDS - 1u) / BANDS + 7u) / 8u * 8u;
+    uint32_t k = 0;
+    for (uint32_t r0 = 0; r0 < gh && k < BANDS; r0 += rb, k++) {
+      const uint32_t r1 = r0 + rb < gh ? r0 + rb : gh;
+      cudaStream_t s = k ? r->band_stream[k - 1] : stream;
+      if (k && cudaStreamWaitEvent(s, r->ev_begin[slot], 0) != cudaSuccess) return -1;
+      int rc = r3d_cuda_raycast_rows(r->ctx, v, r->offscreen, r->w, r->h, r0, r1, s);
+      if (rc != R3D_OK) return report(r, "frame", rc);
+      if (cudaEventRecord(r->band_ev[k], s) != cudaSuccess) return -1;
+      r->band_row[k] = half ? 2u * r0 : r0;
+      r->band_row[k + 1] = half ? (2u * r1 < r->h ? 2u * r1 : r->h) : r1;
+    }
+    for (uint32_t j = 1; j < k; j++)
+      if (cudaStreamWaitEvent(stream, r->band_ev[j], 0) != cudaSuccess) return -1;
+    r->nbands = k;
+  } else {
+    int rc = r3d_cuda_raycast_fwd(r->ctx, views, nviews, r->offscreen, r->w, r->h, NULL, stream);
+    if (rc != R3D_OK) return report(r, "frame", rc);
+  }
   if (cudaEventRecord(r->ev_end[slot], stream) != cudaSuccess) return -1;
   r->ev_used[slot] = 1;
   if (st) {
@@ -208,6 +270,24 @@ int r3d_read_frame(r3d_renderer *r, uint8_t *rgba, uint32_t *w, uint32_t *h) {
   *h = r->h;
   if (!rgba) return 0;
   cudaStream_t stream = (cudaStream_t)r3d_cuda_stream(r->ctx);
+  if (r->nbands) {
+    /* each band as soon as it is drawn, on the copy stream */
+    const size_t row = (size_t)r->w * 4u;
+    for (uint32_t k = 0; k < r->nbands; k++) {
+      const size_t off = r->band_row[k] * row, n = (r->band_row[k + 1] - r->band_row[k]) * row;
+      if (cudaStreamWaitEvent(r->copy_stream, r->band_ev[k], 0) != cudaSuccess ||
+          (n && cudaMemcpyAsync(rgba + off, r->offscreen + off, n, cudaMemcpyDeviceToHost,
+                                r->copy_stream) != cudaSuccess)) {
+        fprintf(stderr, "r3d: read_frame copy failed\n");
+        return -1;
+      }
+    }
+    if (cudaStreamSynchronize(r->copy_stream) != cudaSuccess) {
+      fprintf(stderr, "r3d: read_frame copy failed\n");
+      return -1;
+    }
+    return 0;
+  }
   if (cudaMemcpyAsync(rgba, r->offscreen, (size_t)r->w * r->h * 4, cudaMemcpyDeviceToHost,
                       stream) != cudaSuccess ||
       cudaStreamSynchronize(stream) != cudaSuccess) {
