@@ -119,6 +119,11 @@ struct DevSlab {
   uint32_t ovs;       // overview downscale of the coarsest level
   float nx, ny, px, py, z0;  // the frame parameters slab_nx/ny/px/py/z0 of the window
   DevSlabLevel lev[kSlabLevels];
+  // per-view constants of vs_sample's overview branch (raycast.slang:430-446),
+  // evaluated once with the shader's own float expressions: the number of
+  // overview levels, and per level k the grid and payload gxl, gyl, pxl, pyl
+  int nov;
+  float ov[kSlabLevels][4];
 };
 
 // XY clipmap (raycast.slang:357-408, src/core/clip.h): 6 nested levels of
@@ -491,9 +496,11 @@ __device__ __forceinline__ float tex_wrapz(const uint8_t *__restrict__ g, uint32
   const uint32_t x0 = (uint32_t)tx, y0 = (uint32_t)ty;
   const float fx = tx - (float)x0, fy = ty - (float)y0;
   const float zf = floorf(tz), fz = tz - zf;
-  int zi = (int)zf % (int)wz;
-  if (zi < 0) zi += (int)wz;
-  const uint32_t z0 = (uint32_t)zi, z1 = z0 + 1u < wz ? z0 + 1u : 0u;
+  // w is a fraction in [0, 1), so floor(tz) lies in [-1, wz - 1] and its
+  // ring layer is one conditional away (the modulo of the restatement)
+  const int zi = (int)zf;
+  const uint32_t z0 = zi < 0 ? wz - 1u : min((uint32_t)zi, wz - 1u);
+  const uint32_t z1 = z0 + 1u < wz ? z0 + 1u : 0u;
   const uint32_t x1 = min(x0 + 1u, tw - 1u), y1 = min(y0 + 1u, th - 1u);
   const size_t sy = tw, sz = (size_t)tw * th;
   const uint8_t *r00 = g + y0 * sy + z0 * sz, *r10 = g + y1 * sy + z0 * sz;
@@ -514,13 +521,14 @@ __device__ __forceinline__ float slab_tile(const DevSlab &sl, int L, uint32_t k,
 
 // sample_clip_level (raycast.slang:360-376): level l's texture at p, its z
 // ring wrapping in level slices
+// (divisions by the powers of two 2^l and 2048 are exact as products)
 __device__ __forceinline__ float clip_level(const DevClip &cl, int l, float3 p) {
-  const float s = (float)(1u << l);
+  const float is = 1.0f / (float)(1u << l);
   const float wx = p.x * cl.nx, wy = p.y * cl.nx;
   const float zw = (cl.z0 + 0.5f) + p.z * cl.nx;
-  const float u = ((wx - cl.ox[l]) / s + 1.0f) / 2048.0f;
-  const float v = ((wy - cl.oy[l]) / s + 1.0f) / 2048.0f;
-  const float zq = (zw / s) / (float)cl.wzl[l];
+  const float u = fmaf(wx - cl.ox[l], is, 1.0f) * (1.0f / 2048.0f);
+  const float v = fmaf(wy - cl.oy[l], is, 1.0f) * (1.0f / 2048.0f);
+  const float zq = (zw * is) / (float)cl.wzl[l];
   return tex_wrapz(cl.lev[l], 2048u, 2048u, cl.wzl[l], u, v, zq - floorf(zq));
 }
 
@@ -534,8 +542,8 @@ __device__ __forceinline__ int clip_pick(const DevClip &cl, float3 p, float lod)
     if (li > 5) li = 5 - step;
     if (li < 0) continue;
     if (!(cl.valid & (1u << li))) continue;
-    const float s = (float)(1u << li);
-    const float tx = (wx - cl.ox[li]) / s + 1.0f, ty = (wy - cl.oy[li]) / s + 1.0f;
+    const float is = 1.0f / (float)(1u << li);  // exact: a power of two
+    const float tx = fmaf(wx - cl.ox[li], is, 1.0f), ty = fmaf(wy - cl.oy[li], is, 1.0f);
     if (tx < 1.0f || tx >= 2047.0f || ty < 1.0f || ty >= 2047.0f) continue;
     return li;
   }
@@ -569,8 +577,9 @@ __device__ __forceinline__ float vs_sample(const DevVslab &v, float3 p, float lo
     return tex_wrapz(v.tiles + (size_t)slot * v.tile_bytes, Tu, Tu, v.wz, lx / T, ly / T, w);
   }
   const int L = lev + 1;
-  const float sc = (float)(4 << lev), gxl = (float)v.gx[L], gyl = (float)v.gy[L];
-  const float tx = wx / sc, ty = wy / sc;
+  const float isc = 1.0f / (float)(4 << lev);  // exact: a power of two
+  const float gxl = (float)v.gx[L], gyl = (float)v.gy[L];
+  const float tx = wx * isc, ty = wy * isc;
   const float cx = floorf(tx / P), cy = floorf(ty / P);
   const float qx = cx - floorf(cx / gxl) * gxl, qy = cy - floorf(cy / gyl) * gyl;
   const float lx = (tx - cx * P) + 1.0f, ly = (ty - cy * P) + 1.0f;
@@ -594,13 +603,11 @@ __device__ __forceinline__ float slab_sample(const DevSlab &sl, float3 p, float 
   const float w = zq - floorf(zq);  // frac: the ring wraps
   int lev = (int)floorf(lod) - 2;
   if (lev >= 0) {
-    const int nl = (int)(r3d_log2f((float)sl.ovs) + 0.5f) - 1;
-    lev = min(lev, nl - 1);
-    const float sc = (float)(4 << lev);
-    const float vnx = ceilf(sl.nx / sc), vny = ceilf(sl.ny / sc);
-    const float gxl = ceilf(vnx / 2046.0f), gyl = ceilf(vny / 2046.0f);
-    const float pxl = ceilf(vnx / gxl), pyl = ceilf(vny / gyl);
-    const float wxl = wx / sc, wyl = wy / sc;
+    lev = min(lev, sl.nov - 1);
+    const float gxl = sl.ov[lev][0], gyl = sl.ov[lev][1], pxl = sl.ov[lev][2], pyl = sl.ov[lev][3];
+    // division by the power of two 4 << lev is exact as a product
+    const float isc = 1.0f / (float)(4 << lev);
+    const float wxl = wx * isc, wyl = wy * isc;
     const float oix = fminf(floorf(fmaxf(wxl, 0.0f) / pxl), gxl - 1.0f);
     const float oiy = fminf(floorf(fmaxf(wyl, 0.0f) / pyl), gyl - 1.0f);
     const float ou = ((wxl - oix * pxl) + 1.0f) / (pxl + 2.0f);

@@ -160,6 +160,18 @@ int r3d_cuda_slab_build(r3d_cuda_ctx *c, const r3d_volume_desc *d, const uint8_t
   sl.ny = (float)ny;
   sl.px = (float)base.px;
   sl.py = (float)base.py;
+  // the overview branch's per-level constants, in the shader's float
+  // expressions (raycast.slang:430-446)
+  sl.nov = (int)(r3d_log2f((float)ovs) + 0.5f) - 1;
+  for (int k = 0; k < sl.nov && k < kSlabLevels; k++) {
+    const float sc = (float)(4 << k);
+    const float vnx = ceilf(sl.nx / sc), vny = ceilf(sl.ny / sc);
+    const float gxl = ceilf(vnx / 2046.0f), gyl = ceilf(vny / 2046.0f);
+    sl.ov[k][0] = gxl;
+    sl.ov[k][1] = gyl;
+    sl.ov[k][2] = ceilf(vnx / gxl);
+    sl.ov[k][3] = ceilf(vny / gyl);
+  }
   size_t off = 0, planes = 0;
   for (uint32_t lev = 0; lev < sl.nlev; lev++) {
     SlabLayout l = base;
