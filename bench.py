@@ -647,6 +647,52 @@ def run_ours(args) -> None:
     return out
 
 
+def run_profile_sections(args) -> None:
+    """Renders args.profile_sections frames (1920x1080, FULL) of each section
+    mode over a 4096 x 4096 x 40 phantom -- tiled slab, clipmap, virtual
+    slab -- and of a flattened segment over 512^3 bricks (a 1024 x 1024 x 64
+    window, its bakes included); the command line that ncu captures."""
+    import torch
+    import render3d_b200 as rb
+    lut = rb.scroll_ramp_tf()
+    n = args.profile_sections
+    img = torch.zeros((H, W, 4), dtype=torch.uint8, device="cuda")
+    nx, ny, nz, d = 4096, 4096, 40, 16
+    ctx = rb.Context(0)
+    ctx.set_transfer(lut)
+    ctx.set_alpha_cutoff(CUTOFF)
+    vol = ctx.phantom((nx, ny, nz), seed=SEED)
+    ext = (1.0, 1.0, d / nx)
+
+    def view(i, setup):
+        p = rb.camera_view(0.05 * math.sin(i * 0.05), 0.02, 0.25, W, H, lut,
+                           target=(0.5, 0.5 * ext[1], 0.5 * ext[2]), step_voxels=STEP_VOXELS,
+                           frame_index=i)
+        setup(p)
+        p.density = 6.0
+        ctx.raycast(p, W, H, out=img, stream=ctx.stream)
+
+    ctx.slab_build(vol, d + 2, 4)
+
+    def slab_setup(p):
+        ctx.slab_params(p)
+        p.slab_depth = d
+    ctx.clip_build(vol, d)
+    ctx.clip_frame(nx / 2, ny / 2, 4)
+    ctx.vslab_begin(vol, nx, ny, d)
+    for _ in range(2):
+        ctx.vslab_frame(nx / 2, ny / 2, 4, 64)
+    for setup in (slab_setup, ctx.clip_params, ctx.vslab_params):
+        for i in range(n):
+            view(i, setup)
+    torch.cuda.synchronize()
+    ctx.close()
+    del vol
+    torch.cuda.empty_cache()
+    s = surf_bench(rb, torch, lut, n, n=512, window=(1024, 1024, 64))
+    print("profile section frames done:", n, "surf pitch 0.5 bake ms", s["pitch_0.5"]["bake_ms"])
+
+
 def run_profile(args) -> None:
     """Renders args.profile frames of the workload with no timing: the
     command line that ncu captures."""
@@ -953,12 +999,12 @@ def vslab_bench(rb, torch, lut, vol, frames: int) -> dict:
     return out
 
 
-def surf_bench(rb, torch, lut, frames: int) -> dict:
-    """Flattened-segment views over the 1024^3 LOD brick cache: a wavy sheet
-    (513 x 513 grid of 2-voxel cells) baked into a 2048 x 2048 x 96
-    flattened volume at pitch 0.5 and 2 voxels, then 1920x1080 surf views in
-    FULL at two zooms.  Bake and frame times with CUDA events."""
-    n = N_EDGE
+def surf_bench(rb, torch, lut, frames: int, n: int = N_EDGE, window=(2048, 2048, 96)) -> dict:
+    """Flattened-segment views over the n^3 (default 1024^3) LOD brick
+    cache: a wavy sheet (513 x 513 grid of 2-voxel cells around the centre)
+    baked into a 2048 x 2048 x 96 flattened volume at pitch 0.5 and 2
+    voxels, then 1920x1080 surf views in FULL at two zooms.  Bake and frame
+    times with CUDA events."""
     ctx = rb.Context(0)
     try:
         ctx.set_transfer(lut)
@@ -969,7 +1015,7 @@ def surf_bench(rb, torch, lut, frames: int) -> dict:
         g = 513
         j, i = np.mgrid[0:g, 0:g].astype(np.float64)
         x, y = 0.5 * n - 512.0 + 2.0 * i, 0.5 * n - 512.0 + 2.0 * j
-        z = 0.5 * n + 60.0 * np.sin(x / 90.0) + 40.0 * np.cos(y / 130.0)
+        z = 0.5 * n + 60.0 * n / 1024.0 * np.sin(x / 90.0) + 40.0 * n / 1024.0 * np.cos(y / 130.0)
         nrm = np.stack([-60.0 / 90.0 * np.cos(x / 90.0), 40.0 / 130.0 * np.sin(y / 130.0),
                         np.ones_like(x)], -1)
         nrm /= np.linalg.norm(nrm, axis=-1, keepdims=True)
@@ -978,11 +1024,11 @@ def surf_bench(rb, torch, lut, frames: int) -> dict:
         normals = np.zeros((g, g, 4), np.float32)
         normals[..., :3] = nrm
         ctx.surf_begin(coords, normals)
-        Wv, Hv, Lv = 2048, 2048, 96
+        Wv, Hv, Lv = window
         ctx.surfvol_begin(Wv, Hv, Lv, Lv // 2, 0.5, 0.5)
         st = torch.cuda.ExternalStream(ctx.stream)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        out = {"workload": "1024^3 LOD bricks, 513^2 segment grid, 2048x2048x96 flattened "
+        out = {"workload": f"{n}^3 LOD bricks, 513^2 segment grid, {Wv}x{Hv}x{Lv} flattened "
                            "volume, 1920x1080 surf views"}
         img = torch.zeros((H, W, 4), dtype=torch.uint8, device="cuda")
         for step in (0.5, 2.0):
@@ -1042,12 +1088,17 @@ def main() -> None:
     ap.add_argument("--profile", type=int, default=0, metavar="N",
                     help="only build the workload and render N orbit frames (for ncu)")
     ap.add_argument("--profile-mode", type=int, default=0)
+    ap.add_argument("--profile-sections", type=int, default=0, metavar="N",
+                    help="only render N frames of each section mode and of flattened views")
     ap.add_argument("--profile-diff", type=int, default=0, metavar="N",
                     help="only run N forward+backward steps of the differentiable workload")
     ap.add_argument("--profile-size", type=int, default=N_EDGE)
     args = ap.parse_args()
     if args.profile:
         run_profile(args)
+        return
+    if args.profile_sections:
+        run_profile_sections(args)
         return
     if args.profile_diff:
         import torch

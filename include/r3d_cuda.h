@@ -365,10 +365,12 @@ int r3d_cuda_raycast_fwd_noalloc(r3d_cuda_ctx *ctx, const r3d_frame_params *view
  * = 8x4 / 16x2 / 32x1 rays; unroll = march steps between refill checks
  * (1 or 2); blocks_per_sm = resident 128-thread blocks per SM (0: the
  * occupancy limit).  shade_group (FULL mode, one-thread-per-ray launches):
- * 0 shades each sample where its ray meets it; n > 0 lets lanes park a
- * sample that needs gradient shading until n lanes of the warp (or all its
- * live lanes) wait, and shades them together.  Results are identical under
- * every schedule. */
+ * n > 0 lets lanes park a sample that needs gradient shading until n lanes
+ * of the warp (or all its live lanes) wait, and shades them together (1:
+ * each sample where its ray meets it); 0 picks the sampling path's default,
+ * 16 for the tiled slab, clipmap and virtual slab, whose gradient taps are
+ * whole section lookups, and ungrouped shading for the cube and brick
+ * paths.  Results are identical under every schedule. */
 typedef struct r3d_cuda_schedule {
   uint32_t persistent;
   uint32_t refill_min;

@@ -217,12 +217,19 @@ cudaError_t launch_view(const r3d_cuda_ctx *c, const r3d_frame_params &pc, uint8
     return launch_surf(c, pc, img, out_w, steps, mip_index, stream);
   const DevScene s = c->scene();
   const bool fast = c->quality == R3D_QUALITY_FAST;
-  const uint32_t shade = c->sched.shade_group;
+  // shade_group 0 picks the path's default: grouped shading pays where a
+  // gradient tap is a whole section lookup (tiled slab, clipmap, virtual
+  // slab: 13-31 % faster frames at 16) and costs where it is a fetch inside
+  // the cached brick (LOD bricks, cube: 1.7x slower frames)
+  const int path = path_of_view(pc);
+  const uint32_t shade = c->sched.shade_group ? c->sched.shade_group
+                         : (path == PATH_SLAB || path == PATH_CLIP || path == PATH_VSLAB) ? 16u
+                                                                                          : 0u;
 #define R3D_PATH_CASE(P)                                                                   \
   case P:                                                                                  \
     return launch_path<P>(pc, s, fast, c->lut, img, out_w, steps, mip_index, total, counters, \
                           shade, rows, stream)
-  switch (path_of_view(pc)) {
+  switch (path) {
     R3D_PATH_CASE(PATH_VSLAB);
     R3D_PATH_CASE(PATH_CLIP);
     R3D_PATH_CASE(PATH_SLAB);
