@@ -934,6 +934,7 @@ __device__ __forceinline__ bool composite_sample(const DevScene &s, const ViewCo
   // non-identity shard: taps at lod_step voxels through the slot
   // (raycast.slang:937-940,972-979)
   const bool slot_taps = kShard && !s.sh.identity;
+  constexpr bool kSection = PATH == PATH_SLAB || PATH == PATH_CLIP || PATH == PATH_VSLAB;
   if (kShaded) {
     if (COUNT) st.n_grad++;
     float g0, g1, g2;
@@ -955,6 +956,22 @@ __device__ __forceinline__ bool composite_sample(const DevScene &s, const ViewCo
         q1 = shard_fetch(s.sh, org, make_float3(u.x - ev, u.y - ev, u.z + ev), q.lod, e2);
         q2 = shard_fetch(s.sh, org, make_float3(u.x - ev, u.y + ev, u.z - ev), q.lod, e2);
         q3 = shard_fetch(s.sh, org, make_float3(u.x + ev, u.y + ev, u.z + ev), q.lod, e2);
+      } else if (kSection) {
+        // one inlined copy of the section lookup, looped over the taps, so
+        // that the kernel stays in the instruction cache
+        const float ee = (vc.voxel * q.lod_step) * ir3;
+        q0 = q1 = q2 = q3 = 0.0f;
+#pragma unroll 1
+        for (int k = 0; k < 4; k++) {  // signs (+--), (--+), (-+-), (+++)
+          const float dx = (k == 0 || k == 3) ? ee : -ee, dy = k >= 2 ? ee : -ee;
+          const float dz = (k & 1) ? ee : -ee;
+          const float t = tap_sample<PATH>(s, tex, make_float3(q.p.x + dx, q.p.y + dy, q.p.z + dz),
+                                           q.lod, (int)q.slot);
+          if (k == 0) q0 = t;
+          else if (k == 1) q1 = t;
+          else if (k == 2) q2 = t;
+          else q3 = t;
+        }
       } else {
         float ee = (vc.voxel * q.lod_step) * ir3;
         q0 = tap_sample<PATH>(s, tex, make_float3(q.p.x + ee, q.p.y - ee, q.p.z - ee), q.lod, (int)q.slot);
@@ -996,6 +1013,28 @@ __device__ __forceinline__ bool composite_sample(const DevScene &s, const ViewCo
              shard_fetch(s.sh, org, make_float3(u.x, u.y - ev, u.z), q.lod, e2);
         g2 = shard_fetch(s.sh, org, make_float3(u.x, u.y, u.z + ev), q.lod, e2) -
              shard_fetch(s.sh, org, make_float3(u.x, u.y, u.z - ev), q.lod, e2);
+      } else if (kSection) {  // looped taps, as above
+        const float e = vc.voxel * q.lod_step;
+        float plus = 0.0f;
+        g0 = g1 = g2 = 0.0f;
+#pragma unroll 1
+        for (int k = 0; k < 6; k++) {  // +x, -x, +y, -y, +z, -z
+          const int ax = k >> 1;
+          const float d = (k & 1) ? -e : e;
+          const float t = tap_sample<PATH>(
+              s, tex,
+              make_float3(ax == 0 ? q.p.x + d : q.p.x, ax == 1 ? q.p.y + d : q.p.y,
+                          ax == 2 ? q.p.z + d : q.p.z),
+              q.lod, (int)q.slot);
+          if (!(k & 1)) {
+            plus = t;
+          } else {
+            const float g = plus - t;
+            if (ax == 0) g0 = g;
+            else if (ax == 1) g1 = g;
+            else g2 = g;
+          }
+        }
       } else {
         float e = vc.voxel * q.lod_step;
         g0 = tap_sample<PATH>(s, tex, make_float3(q.p.x + e, q.p.y, q.p.z), q.lod, (int)q.slot) -
