@@ -247,6 +247,31 @@ def _load() -> C.CDLL:
         "r3d_bricks_params": (None, [P, C.POINTER(FrameParams)]),
         "r3d_bricks_extent": (None, [P, P]),
         "r3d_bricks_shape": (None, [P, P]),
+        "r3d_slab_init": (I, [P, P]),
+        "r3d_slab_window": (I, [P, P, U32]),
+        "r3d_slab_params": (None, [P, P]),
+        "r3d_clip_begin_volume": (I, [P, P, U32]),
+        "r3d_clip_frame": (I, [P, C.c_double, C.c_double, C.c_uint64, P]),
+        "r3d_bricks_begin_stream": (I, [P, C.POINTER(VolumeDesc), P, U32, U32]),
+        "r3d_bricks_stream": (None, [P, P, P, F, F, U32, U32, F, U32]),
+        "r3d_bricks_get_stats": (None, [P, P]),
+        "r3d_bricks_flush": (None, [P]),
+        "r3d_bricks_overlay_volume": (I, [P, U32, C.POINTER(VolumeDesc), P]),
+        "r3d_vslab_begin_volume": (I, [P, P, P]),
+        "r3d_vslab_frame": (None, [P, C.c_double, C.c_double, C.c_int64, U32, P]),
+        "r3d_vslab_get": (None, [P, P, P]),
+        "r3d_vslab_resident_pending": (U32, [P]),
+        "r3d_surf_begin": (I, [P, U32, U32, P, P]),
+        "r3d_surf_swap": (I, [P, U32, U32, P, P, F, F]),
+        "r3d_surfvol_begin": (I, [P, U32, U32, U32, U32, F, F]),
+        "r3d_surfvol_window": (None, [P, C.c_double, C.c_double, F, F]),
+        "r3d_surfvol_visible": (None, [P, U32, U32, U32, U32, U32, U32]),
+        "r3d_surfvol_mark": (None, [P]),
+        "r3d_surfvol_overlay_enable": (None, [P, C.c_bool]),
+        "r3d_surfvol_params": (None, [P, P]),
+        "r3d_surfmask": (I, [P, P, U32, U32]),
+        "r3d_surfmask_clear": (None, [P]),
+        "r3d_max_dim3d": (U32, [P]),
         "r3d_frame": (I, [P, C.POINTER(FrameParams), C.POINTER(FrameStats)]),
         "r3d_frame_views": (I, [P, P, U32, C.POINTER(FrameStats)]),
         "r3d_read_frame": (I, [P, P, C.POINTER(U32), C.POINTER(U32)]),
@@ -816,6 +841,38 @@ class Batch:
         return {f: getattr(sc, f) for f, _ in Schedule._fields_}, ms.value
 
 
+class Volume(C.Structure):
+    """r3d_volume: a raw u8 volume held by the caller."""
+    _fields_ = [("voxels", C.c_void_p), ("nx", C.c_uint32), ("ny", C.c_uint32),
+                ("nz", C.c_uint32), ("nbytes", C.c_size_t), ("voxel_um", C.c_float)]
+
+
+class SlabDesc(C.Structure):
+    _fields_ = [("nx", C.c_uint32), ("ny", C.c_uint32), ("nz", C.c_uint32), ("wz", C.c_uint32)]
+
+
+class VslabDesc(C.Structure):
+    _fields_ = [("nx", C.c_uint32), ("ny", C.c_uint32), ("nz", C.c_uint32), ("W", C.c_uint32),
+                ("H", C.c_uint32), ("D", C.c_uint32), ("cache_dir", C.c_char_p),
+                ("shard_url", C.c_char_p), ("z_prefetch", C.c_uint32),
+                ("prefetch_slots", C.c_uint32), ("prefetch_threads", C.c_uint32)]
+
+
+class BricksStats(C.Structure):
+    _fields_ = [("nb", C.c_uint32), ("hot", C.c_uint32), ("hot_cap", C.c_uint32),
+                ("warm_bricks", C.c_uint32), ("warm_bytes", C.c_uint64), ("warm_cap", C.c_uint64),
+                ("inflight", C.c_uint32), ("decoded", C.c_uint64), ("jobs", C.c_uint64),
+                ("stream_ns", C.c_uint64), ("failures", C.c_uint32), ("nlevels", C.c_uint32),
+                ("lod_wanted", C.c_uint32 * 8), ("lod_requests", C.c_uint64 * 8),
+                ("net_pending", C.c_uint32), ("net_fetched", C.c_uint64),
+                ("net_encoded", C.c_uint64)]
+
+
+def _volume(vol) -> Volume:
+    nz, ny, nx = vol.shape
+    return Volume(_ptr(vol), nx, ny, nz, nx * ny * nz, 0.0)
+
+
 class Renderer:
     """The headless render3d interface (r3d_render.h)."""
 
@@ -858,6 +915,81 @@ class Renderer:
 
     def bricks_params(self, p: FrameParams) -> None:
         lib.r3d_bricks_params(self.r, C.byref(p))
+
+    # section modes and flattened views, with render.h's names
+    def slab_init(self, shape, wz: int) -> None:
+        nz, ny, nx = shape
+        self._ok(lib.r3d_slab_init(self.r, C.byref(SlabDesc(nx, ny, nz, wz))), "r3d_slab_init")
+
+    def slab_window(self, vol, z0: int) -> None:
+        self._ok(lib.r3d_slab_window(self.r, C.byref(_volume(vol)), z0), "r3d_slab_window")
+
+    def slab_params(self, p: FrameParams) -> None:
+        lib.r3d_slab_params(self.r, C.byref(p))
+
+    def clip_begin_volume(self, vol, depth_max: int) -> None:
+        self._ok(lib.r3d_clip_begin_volume(self.r, C.byref(_volume(vol)), depth_max),
+                 "r3d_clip_begin_volume")
+
+    def clip_frame(self, fx: float, fy: float, z0: int, p: FrameParams) -> None:
+        self._ok(lib.r3d_clip_frame(self.r, fx, fy, z0, C.byref(p)), "r3d_clip_frame")
+
+    def bricks_begin_stream(self, vol, nlev: int, nslots: int) -> None:
+        nz, ny, nx = vol.shape
+        self._ok(lib.r3d_bricks_begin_stream(self.r, C.byref(VolumeDesc(nx, ny, nz, 128, 1.0)),
+                                             _ptr(vol), nlev, nslots), "r3d_bricks_begin_stream")
+
+    def bricks_stream(self, view: "StreamView") -> None:
+        lib.r3d_bricks_stream(self.r, view.eye, view.fwd, view.half_tan, view.pixel_cone,
+                              view.slice_z0, view.slice_depth, view.gate, view.budget)
+
+    def bricks_stats(self) -> BricksStats:
+        st = BricksStats()
+        lib.r3d_bricks_get_stats(self.r, C.byref(st))
+        return st
+
+    def bricks_overlay_volume(self, which: int, vol) -> None:
+        nz, ny, nx = vol.shape
+        self._ok(lib.r3d_bricks_overlay_volume(self.r, which,
+                                               C.byref(VolumeDesc(nx, ny, nz, 128, 1.0)),
+                                               _ptr(vol)), "r3d_bricks_overlay_volume")
+
+    def vslab_begin_volume(self, vol, W: int, H: int, D: int, z_prefetch: int = 0) -> None:
+        nz, ny, nx = vol.shape
+        d = VslabDesc(nx, ny, nz, W, H, D, None, None, z_prefetch, 0, 0)
+        self._ok(lib.r3d_vslab_begin_volume(self.r, C.byref(d), _ptr(vol)),
+                 "r3d_vslab_begin_volume")
+
+    def vslab_frame(self, fx: float, fy: float, z0: int, budget: int, p: FrameParams) -> None:
+        lib.r3d_vslab_frame(self.r, fx, fy, z0, budget, C.byref(p))
+
+    def vslab_get(self) -> tuple[tuple[int, int, int], int]:
+        o = (C.c_int64 * 3)()
+        pending = C.c_uint32()
+        lib.r3d_vslab_get(self.r, o, C.byref(pending))
+        return tuple(o), pending.value
+
+    def surf_begin(self, coords, normals) -> None:
+        gh, gw = coords.shape[:2]
+        self._ok(lib.r3d_surf_begin(self.r, gw, gh, _ptr(coords), _ptr(normals)),
+                 "r3d_surf_begin")
+
+    def surf_swap(self, coords, normals, sx: float, sy: float) -> None:
+        gh, gw = coords.shape[:2]
+        self._ok(lib.r3d_surf_swap(self.r, gw, gh, _ptr(coords), _ptr(normals), sx, sy),
+                 "r3d_surf_swap")
+
+    def surfvol_begin(self, W: int, H: int, L: int, nback: int, sx: float, sy: float) -> None:
+        self._ok(lib.r3d_surfvol_begin(self.r, W, H, L, nback, sx, sy), "r3d_surfvol_begin")
+
+    def surfvol_window(self, u0: float, v0: float, step: float, zoff0: float) -> None:
+        lib.r3d_surfvol_window(self.r, u0, v0, step, zoff0)
+
+    def surfvol_overlay_enable(self, on: bool) -> None:
+        lib.r3d_surfvol_overlay_enable(self.r, on)
+
+    def surfvol_params(self, p: FrameParams) -> None:
+        lib.r3d_surfvol_params(self.r, C.byref(p))
 
     def set_transfer(self, lut: np.ndarray) -> None:
         self._ok(lib.r3d_set_transfer(self.r, _ptr(np.ascontiguousarray(lut, np.uint8))),

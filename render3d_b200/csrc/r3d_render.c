@@ -40,6 +40,15 @@ struct r3d_renderer {
   cudaEvent_t band_ev[BANDS];
   uint32_t nbands; /* bands of the last frame; 0: drawn whole */
   uint32_t band_row[BANDS + 1];
+  /* section modes and flattened views driven through this interface */
+  r3d_slab_desc slab;        /* from r3d_slab_init (wz 0: none) */
+  const uint8_t *slab_src;   /* the volume the tiles were built from */
+  int streaming;
+  r3d_stream_stats stream_last;
+  uint64_t stream_uploaded;
+  uint32_t surf_w, surf_h, surf_l, surf_nback; /* surfvol window */
+  int surf_baked;
+  float surf_win[4]; /* u0, v0, step, zoff0 of the last bake */
 };
 
 static uint64_t now_ns(void) {
@@ -160,8 +169,8 @@ int r3d_bricks_begin_shard(r3d_renderer *r, const uint8_t *voxels, uint32_t edge
                            uint32_t pool_bpa) {
   if (!r) return -1;
   if (pool_bpa && pool_bpa < edge / 128u) {
-    fprintf(stderr, "r3d: bricks_begin_shard: a pool smaller than the shard needs streaming "
-                    "residency, which is not available\n");
+    fprintf(stderr, "r3d: bricks_begin_shard: a single-level shard is resident whole; a pool "
+                    "smaller than the volume streams as an LOD cache (r3d_bricks_begin_stream)\n");
     return -1;
   }
   int rc = r3d_cuda_shard_build(r->ctx, edge, voxels, edge / 128u, NULL);
@@ -296,3 +305,220 @@ int r3d_read_frame(r3d_renderer *r, uint8_t *rgba, uint32_t *w, uint32_t *h) {
   }
   return 0;
 }
+
+/* ---- tiled slab (render.h:22-33) ---- */
+
+int r3d_slab_init(r3d_renderer *r, const r3d_slab_desc *d) {
+  if (!r || !d || !d->nx || !d->ny || !d->nz || d->wz < 4u || d->wz > d->nz) return -1;
+  r->slab = *d;
+  r->slab_src = NULL;
+  return 0;
+}
+
+int r3d_slab_window(r3d_renderer *r, const r3d_volume *src, uint32_t z0) {
+  if (!r || !r->slab.wz || !src || !src->voxels || src->nx != r->slab.nx ||
+      src->ny != r->slab.ny || src->nz != r->slab.nz)
+    return -1;
+  const uint32_t zmax = r->slab.nz - r->slab.wz;
+  if (z0 > zmax) z0 = zmax;
+  if (src->voxels != r->slab_src) {
+    r3d_volume_desc d = {src->nx, src->ny, src->nz, 128u, 1.0f};
+    int rc = r3d_cuda_slab_build(r->ctx, &d, src->voxels, r->slab.wz, z0);
+    if (rc != R3D_OK) return report(r, "slab_window", rc);
+    r->slab_src = src->voxels;
+    return 0;
+  }
+  return report(r, "slab_window", r3d_cuda_slab_window(r->ctx, z0));
+}
+
+void r3d_slab_params(const r3d_renderer *r, r3d_frame_params *p) {
+  if (r && p) r3d_cuda_slab_params(r->ctx, p);
+}
+
+/* ---- clipmap (render.h:35-41) ---- */
+
+int r3d_clip_begin_volume(r3d_renderer *r, const r3d_volume *src, uint32_t depth_max) {
+  if (!r || !src || !src->voxels) return -1;
+  r3d_volume_desc d = {src->nx, src->ny, src->nz, 128u, 1.0f};
+  return report(r, "clip_begin", r3d_cuda_clip_build(r->ctx, &d, src->voxels, depth_max));
+}
+
+int r3d_clip_frame(r3d_renderer *r, double fx, double fy, uint64_t z0, r3d_frame_params *p) {
+  if (!r) return -1;
+  return report(r, "clip_frame", r3d_cuda_clip_frame(r->ctx, fx, fy, z0, p));
+}
+
+/* ---- streamed LOD cache (render.h:116-160) ---- */
+
+int r3d_bricks_begin_stream(r3d_renderer *r, const r3d_volume_desc *d, const uint8_t *voxels,
+                            uint32_t nlev, uint32_t nslots) {
+  if (!r) return -1;
+  int rc = r3d_cuda_stream_begin(r->ctx, d, voxels, nlev, nslots);
+  if (rc != R3D_OK) return report(r, "bricks_begin_stream", rc);
+  r->bricks = 1;
+  r->streaming = 1;
+  r->stream_uploaded = 0;
+  memset(&r->stream_last, 0, sizeof r->stream_last);
+  r->brick_mode = r3d_cuda_brick_mode(r->ctx);
+  r3d_cuda_bricks_info(r->ctx, NULL, NULL, r->shape, NULL);
+  return 0;
+}
+
+void r3d_bricks_stream(r3d_renderer *r, const float eye[3], const float fwd[3], float half_tan,
+                       float pixel_cone, uint32_t slice_z0, uint32_t slice_depth, float gate,
+                       uint32_t budget) {
+  if (!r || !r->streaming || !eye || !fwd) return;
+  r3d_stream_view v;
+  memcpy(v.eye, eye, sizeof v.eye);
+  memcpy(v.fwd, fwd, sizeof v.fwd);
+  v.half_tan = half_tan;
+  v.pixel_cone = pixel_cone;
+  v.slice_z0 = slice_z0;
+  v.slice_depth = slice_depth;
+  v.gate = gate;
+  v.budget = budget;
+  r3d_stream_stats st;
+  if (report(r, "bricks_stream", r3d_cuda_stream_update(r->ctx, &v, &st)) == 0) {
+    r->stream_last = st;
+    r->stream_uploaded += st.uploaded;
+  }
+}
+
+void r3d_bricks_get_stats(r3d_renderer *r, r3d_bricks_stats *st) {
+  if (!r || !st) return;
+  memset(st, 0, sizeof *st);
+  if (!r->bricks) return;
+  uint32_t nslots = 0, nlev = 0, shape[3] = {0, 0, 0};
+  r3d_cuda_bricks_info(r->ctx, NULL, &nslots, shape, &nlev);
+  st->nlevels = nlev;
+  st->hot_cap = nslots;
+  st->hot = r->streaming ? r->stream_last.resident : nslots;
+  st->inflight = r->streaming ? r->stream_last.uploaded : 0u;
+  st->decoded = r->stream_uploaded;
+  uint32_t nb = 0;
+  for (uint32_t l = 0; l < nlev && l < 16u; l++) {
+    uint32_t s = 128u << l, b = 1u;
+    for (int a = 0; a < 3; a++) b *= (shape[a] + s - 1u) / s;
+    nb += b;
+  }
+  st->nb = nb;
+}
+
+void r3d_bricks_flush(r3d_renderer *r) {
+  if (r) cudaStreamSynchronize((cudaStream_t)r3d_cuda_stream(r->ctx));
+}
+
+int r3d_bricks_overlay_volume(r3d_renderer *r, uint32_t which, const r3d_volume_desc *d,
+                              const uint8_t *voxels) {
+  if (!r) return -1;
+  return report(r, "bricks_overlay", r3d_cuda_bricks_overlay_build(r->ctx, which, d, voxels));
+}
+
+/* ---- virtual slab (render.h:161-184) ---- */
+
+int r3d_vslab_begin_volume(r3d_renderer *r, const r3d_vslab_desc *d, const uint8_t *voxels) {
+  if (!r || !d || !voxels) return -1;
+  r3d_volume_desc vd = {d->nx, d->ny, d->nz, 128u, 1.0f};
+  return report(r, "vslab_begin",
+                r3d_cuda_vslab_begin(r->ctx, &vd, voxels, d->W, d->H, d->D, d->z_prefetch));
+}
+
+void r3d_vslab_frame(r3d_renderer *r, double fx, double fy, int64_t z0, uint32_t budget,
+                     r3d_frame_params *p) {
+  if (r) report(r, "vslab_frame", r3d_cuda_vslab_frame(r->ctx, fx, fy, z0, budget, p, NULL));
+}
+
+/* origin and the window cells still missing their visible slices */
+static uint32_t vslab_pending(const r3d_renderer *r, int64_t o[3]) {
+  r3d_vslab_layout v;
+  if (r3d_cuda_vslab_layout(r->ctx, &v) != R3D_OK) return 0;
+  if (o) o[0] = v.x0, o[1] = v.y0, o[2] = v.z0;
+  r3d_vslab_stats st;
+  /* a zero-budget frame at the current origin moves nothing and fills
+   * nothing; it only reports */
+  if (v.x0 < 0 ||
+      r3d_cuda_vslab_frame(r->ctx, (double)v.x0 + v.W / 2, (double)v.y0 + v.H / 2, v.z0, 0u, NULL,
+                           &st) != R3D_OK)
+    return 0;
+  return st.pending;
+}
+
+void r3d_vslab_get(const r3d_renderer *r, int64_t o[3], uint32_t *pending) {
+  if (!r) return;
+  const uint32_t n = vslab_pending(r, o);
+  if (pending) *pending = n;
+}
+
+uint32_t r3d_vslab_resident_pending(const r3d_renderer *r) {
+  return r ? vslab_pending(r, NULL) : 0u;
+}
+
+/* ---- flattened-segment views (render.h:193-238) ---- */
+
+int r3d_surf_begin(r3d_renderer *r, uint32_t w, uint32_t h, const float *coords_rgba,
+                   const float *normals_rgba) {
+  if (!r) return -1;
+  return report(r, "surf_begin", r3d_cuda_surf_begin(r->ctx, w, h, coords_rgba, normals_rgba));
+}
+
+int r3d_surf_swap(r3d_renderer *r, uint32_t w, uint32_t h, const float *coords_rgba,
+                  const float *normals_rgba, float sx, float sy) {
+  if (!r || !r->surf_w) return -1;
+  /* new grids, the window re-made with the new scale: the next _window
+   * call bakes everything, as in the reference */
+  int rc = r3d_cuda_surf_begin(r->ctx, w, h, coords_rgba, normals_rgba);
+  if (rc == R3D_OK)
+    rc = r3d_cuda_surfvol_begin(r->ctx, r->surf_w, r->surf_h, r->surf_l, r->surf_nback, sx, sy);
+  r->surf_baked = 0;
+  return report(r, "surf_swap", rc);
+}
+
+int r3d_surfvol_begin(r3d_renderer *r, uint32_t w, uint32_t h, uint32_t layers,
+                      uint32_t nback, float sx, float sy) {
+  if (!r) return -1;
+  int rc = r3d_cuda_surfvol_begin(r->ctx, w, h, layers, nback, sx, sy);
+  if (rc != R3D_OK) return report(r, "surfvol_begin", rc);
+  r->surf_w = w, r->surf_h = h, r->surf_l = layers, r->surf_nback = nback;
+  r->surf_baked = 0;
+  return 0;
+}
+
+void r3d_surfvol_window(r3d_renderer *r, double u0, double v0, float step, float zoff0) {
+  if (!r || !r->surf_w) return;
+  const float w[4] = {(float)u0, (float)v0, step, zoff0};
+  if (r->surf_baked && !memcmp(w, r->surf_win, sizeof w)) return; /* unchanged */
+  if (report(r, "surfvol_window", r3d_cuda_surfvol_window(r->ctx, u0, v0, step, zoff0)) == 0) {
+    memcpy(r->surf_win, w, sizeof w);
+    r->surf_baked = 1;
+  }
+}
+
+void r3d_surfvol_visible(r3d_renderer *r, uint32_t x0, uint32_t y0, uint32_t z0, uint32_t x1,
+                         uint32_t y1, uint32_t z1) {
+  (void)r, (void)x0, (void)y0, (void)z0, (void)x1, (void)y1, (void)z1;
+}
+
+void r3d_surfvol_mark(r3d_renderer *r) {
+  if (r) report(r, "surfvol_mark", r3d_cuda_surfvol_mark(r->ctx));
+}
+
+void r3d_surfvol_overlay_enable(r3d_renderer *r, bool enable) {
+  if (r) report(r, "surfvol_overlay", r3d_cuda_surfvol_overlay(r->ctx, enable ? 0 : -1));
+}
+
+void r3d_surfvol_params(const r3d_renderer *r, r3d_frame_params *p) {
+  if (r && p) r3d_cuda_surfvol_params(r->ctx, p);
+}
+
+int r3d_surfmask(r3d_renderer *r, const uint8_t *m, uint32_t w, uint32_t h) {
+  if (!r || !m || !w || !h) return -1;
+  return report(r, "surfmask", r3d_cuda_surfmask(r->ctx, m, w, h));
+}
+
+void r3d_surfmask_clear(r3d_renderer *r) {
+  if (r) report(r, "surfmask_clear", r3d_cuda_surfmask(r->ctx, NULL, 0, 0));
+}
+
+/* the largest surf window side to request: r3d_cuda_surfvol_begin takes up
+ * to 2048 layers (and 16384 texels a side) */
+uint32_t r3d_max_dim3d(const r3d_renderer *r) { return r ? 2048u : 0u; }
