@@ -140,6 +140,23 @@ void r3d_cuda_stream_view_of(const r3d_frame_params *p, const float ext[3], uint
                              r3d_stream_view *view);
 int r3d_cuda_stream_update(r3d_cuda_ctx *ctx, const r3d_stream_view *view,
                            r3d_stream_stats *stats);
+/* The multi-view pump (reference r3d_bricks_stream_begin / _box / _point /
+ * _submit, src/render/render.h:128-139, src/vk/vkbackend.c:5244-5414,
+ * 5519-5590): _collect_begin opens a frame's request set and pins the
+ * coarsest level; _collect_view adds a view's cone (budget unused),
+ * _collect_box a volume-normalized box at the level matching pixel_cone
+ * (r3d_host_stream_box), _collect_point one brick of a level and its parent
+ * (r3d_host_stream_point), each listing a brick at most once per frame;
+ * _submit sorts them all (priority, then distance), touches the resident
+ * ones and fills up to budget of the rest as _update does, which is begin +
+ * view + submit.  Collects and submit without an open frame fail with
+ * R3D_E_STATE. */
+int r3d_cuda_stream_collect_begin(r3d_cuda_ctx *ctx);
+int r3d_cuda_stream_collect_view(r3d_cuda_ctx *ctx, const r3d_stream_view *view);
+int r3d_cuda_stream_collect_box(r3d_cuda_ctx *ctx, const float lo[3], const float hi[3],
+                                float pixel_cone, float gate);
+int r3d_cuda_stream_collect_point(r3d_cuda_ctx *ctx, const float p[3], uint32_t level, float gate);
+int r3d_cuda_stream_submit(r3d_cuda_ctx *ctx, uint32_t budget, r3d_stream_stats *stats);
 
 /* Tiled slab: render3d's slab mode for wide, thin windows (reference
  * src/core/slab.h, src/vk/vkbackend.c:2128-2335, sampled by
@@ -247,6 +264,15 @@ int r3d_cuda_surfvol_begin(r3d_cuda_ctx *ctx, uint32_t w, uint32_t h, uint32_t l
                            uint32_t nback, float sx, float sy);
 int r3d_cuda_surfvol_window(r3d_cuda_ctx *ctx, double u0, double v0, float step, float zoff0);
 int r3d_cuda_surfvol_overlay(r3d_cuda_ctx *ctx, int atlas);
+/* Live 2.5D ink prediction (reference r3d_surfvol_inkpred / _clear,
+ * src/render/render.h:222-230, src/shaders/surfvol.comp:127-150): w x h
+ * float probabilities, texel (0, 0) at grid coordinates (g0u, g0v),
+ * px_per_grid texels per grid unit.  Each bake samples it (clamp-to-edge
+ * bilinear) once per (u, v) column and writes it into G over every layer
+ * where the column falls inside it, replacing the overlay atlas there.
+ * Uploading re-bakes the window; pred NULL drops it and re-bakes. */
+int r3d_cuda_surfvol_inkpred(r3d_cuda_ctx *ctx, const float *pred, uint32_t w, uint32_t h,
+                             float g0u, float g0v, float px_per_grid);
 int r3d_cuda_surfvol_mark(r3d_cuda_ctx *ctx);
 void r3d_cuda_surfvol_params(const r3d_cuda_ctx *ctx, r3d_frame_params *p);
 /* Copy of the flattened volume (w * h * layers * 2 bytes, x fastest). */

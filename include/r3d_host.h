@@ -73,6 +73,24 @@ uint32_t r3d_host_stream_desired(const uint32_t *page, uint32_t page_words, cons
                                  const float fwd[3], float half_tan, float pixel_cone,
                                  uint32_t slice_z0, uint32_t slice_depth, float gate,
                                  uint8_t *mark, r3d_stream_cand *out, uint32_t cap);
+/* The multi-view collects (src/vk/vkbackend.c:5330-5414), appending to the
+ * n candidates already in out with the same mark, gate and listing rules,
+ * unsorted; each returns the new count.  _box: a volume-normalized box;
+ * the level whose voxel pitch matches pixel_cone (floor(log2(max(pixel_cone
+ * * max(shape), 1)))), coarsened one level at a time until the box holds at
+ * most 2048 of its bricks; each brick of the box adds its parent
+ * (priority 0, absent at the coarsest level) and itself (priority 1), with
+ * the squared distance of its centre from the box's centre.  _point: the
+ * brick of `level` (clamped to the coarsest) containing p, clamped to the
+ * level's grid, after its parent; both at distance 0. */
+uint32_t r3d_host_stream_box(const uint32_t *page, uint32_t page_words, const float lo[3],
+                             const float hi[3], float pixel_cone, float gate, uint8_t *mark,
+                             r3d_stream_cand *out, uint32_t cap, uint32_t n);
+uint32_t r3d_host_stream_point(const uint32_t *page, uint32_t page_words, const float p[3],
+                               uint32_t level, float gate, uint8_t *mark, r3d_stream_cand *out,
+                               uint32_t cap, uint32_t n);
+/* Sorts candidates by priority, then distance, then brick. */
+void r3d_host_stream_sort(r3d_stream_cand *c, uint32_t n);
 
 /* Virtual slab: a W x H x D window anywhere in a volume, rendered from
  * world-anchored toroidal tile grids (src/core/vslab.h).  Level l has

@@ -102,6 +102,13 @@ int r3d_bricks_begin_stream(r3d_renderer *r, const r3d_volume_desc *d, const uin
 void r3d_bricks_stream(r3d_renderer *r, const float eye[3], const float fwd[3], float half_tan,
                        float pixel_cone, uint32_t slice_z0, uint32_t slice_depth, float gate,
                        uint32_t budget);
+/* Multi-view pump (render.h:128-139): begin (false: not streaming), any
+ * number of box / point collects, then submit. */
+bool r3d_bricks_stream_begin(r3d_renderer *r);
+void r3d_bricks_stream_box(r3d_renderer *r, const float lo[3], const float hi[3],
+                           float pixel_cone, float gate);
+void r3d_bricks_stream_point(r3d_renderer *r, const float p[3], uint32_t level, float gate);
+void r3d_bricks_stream_submit(r3d_renderer *r, uint32_t budget);
 /* Same fields as the reference's r3d_bricks_stats; the warm-tier, decode
  * and network fields stay 0 (the warm tier holds decoded bricks). */
 typedef struct r3d_bricks_stats {
@@ -157,7 +164,16 @@ void r3d_surfvol_window(r3d_renderer *r, double u0, double v0, float step, float
 void r3d_surfvol_visible(r3d_renderer *r, uint32_t x0, uint32_t y0, uint32_t z0, uint32_t x1,
                          uint32_t y1, uint32_t z1);
 void r3d_surfvol_mark(r3d_renderer *r);
+/* Live 2.5D ink prediction: w x h probabilities, texel (0, 0) at grid
+ * coordinates (g0u, g0v), px_per_grid texels per grid unit; re-bakes. */
+int r3d_surfvol_inkpred(r3d_renderer *r, const float *pred, uint32_t w, uint32_t h, float g0u,
+                        float g0v, float px_per_grid);
+void r3d_surfvol_inkpred_clear(r3d_renderer *r);
+/* The bake's overlay byte: none unless the ink atlas is loaded and
+ * _overlay_enable is on; then the registration atlas while _regtap is on,
+ * else the 3D ink atlas when loaded, else the ink atlas. */
 void r3d_surfvol_overlay_enable(r3d_renderer *r, bool enable);
+void r3d_surfvol_regtap(r3d_renderer *r, bool on);
 void r3d_surfvol_params(const r3d_renderer *r, r3d_frame_params *p);
 int r3d_surfmask(r3d_renderer *r, const uint8_t *m, uint32_t w, uint32_t h);
 void r3d_surfmask_clear(r3d_renderer *r);

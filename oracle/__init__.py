@@ -53,7 +53,9 @@ class VSlab(C.Structure):
 class Surf(C.Structure):
     _fields_ = [("coords", C.c_void_p), ("normals", C.c_void_p), ("gw", C.c_uint32),
                 ("gh", C.c_uint32), ("vol", C.c_void_p), ("W", C.c_uint32), ("H", C.c_uint32),
-                ("L", C.c_uint32), ("mask", C.c_void_p), ("mw", C.c_uint32), ("mh", C.c_uint32)]
+                ("L", C.c_uint32), ("mask", C.c_void_p), ("mw", C.c_uint32), ("mh", C.c_uint32),
+                ("pred", C.c_void_p), ("pw", C.c_uint32), ("ph", C.c_uint32), ("pg0u", C.c_float),
+                ("pg0v", C.c_float), ("pppg", C.c_float)]
 
 
 class Bricks(C.Structure):
@@ -583,6 +585,19 @@ class SurfScene:
         C.memmove(C.addressof(self.b), C.addressof(bricks.b), C.sizeof(Bricks))
         self.b.surf = C.addressof(self.s)
         self.window = None
+
+    def inkpred(self, pred, g0u: float, g0v: float, px_per_grid: float) -> None:
+        """Live 2.5D ink prediction for later bakes: (ph, pw) float32
+        probabilities, texel (0, 0) at grid coordinates (g0u, g0v);
+        pred None drops it (vkbackend.c:1900-1968)."""
+        if pred is None:
+            self.pred = None
+            self.s.pred, self.s.pw, self.s.ph = None, 0, 0
+            return
+        self.pred = np.ascontiguousarray(pred, np.float32)
+        self.s.pred = self.pred.ctypes.data
+        self.s.ph, self.s.pw = self.pred.shape
+        self.s.pg0u, self.s.pg0v, self.s.pppg = g0u, g0v, px_per_grid
 
     def bake(self, u0: float, v0: float, step: float, zoff0: float, ovl: int = -1) -> None:
         lib.orc_surf_bake(C.byref(self.s), C.byref(self.bricks.b), u0, v0, step, zoff0,

@@ -509,6 +509,19 @@ static void surf_brick_sample(const scene *s, uint32_t lod, int ovl, v3f wp, v3f
   out[0] = out[1] = 0.0f;
 }
 
+/* the prediction texture, clamp-to-edge bilinear at texel-space position
+ * (px, py) sampled as textureLod(inkpred, (pp + 0.5) / size) */
+static float pred_sample(const orc_surf *sf, float px, float py) {
+  float u = (px + 0.5f) / (float)sf->pw, v = (py + 0.5f) / (float)sf->ph;
+  float tx = clampf_(fmaf(u, (float)sf->pw, -0.5f), 0.0f, (float)(sf->pw - 1u));
+  float ty = clampf_(fmaf(v, (float)sf->ph, -0.5f), 0.0f, (float)(sf->ph - 1u));
+  uint32_t x0 = (uint32_t)tx, y0 = (uint32_t)ty;
+  uint32_t x1 = x0 + 1u < sf->pw ? x0 + 1u : sf->pw - 1u, y1 = y0 + 1u < sf->ph ? y0 + 1u : sf->ph - 1u;
+  float fx = tx - (float)x0, fy = ty - (float)y0;
+  const float *r0 = sf->pred + (size_t)y0 * sf->pw, *r1 = sf->pred + (size_t)y1 * sf->pw;
+  return lerpf_(lerpf_(r0[x0], r0[x1], fx), lerpf_(r1[x0], r1[x1], fx), fy);
+}
+
 void orc_surf_bake(orc_surf *sf, const orc_bricks *br, float u0, float v0, float step,
                    float zoff0, float sx, float sy, uint32_t nback, int ovl) {
   uint32_t st = 0;
@@ -548,6 +561,13 @@ void orc_surf_bake(orc_surf *sf, const orc_bricks *br, float u0, float v0, float
           }
         }
       }
+      /* one prediction per column, over every layer (surfvol.comp:127-150) */
+      float pred = -1.0f;
+      if (sf->pred) {
+        float px = (gx - sf->pg0u) * sf->pppg, py = (gy - sf->pg0v) * sf->pppg;
+        if (px >= 0.0f && py >= 0.0f && px < (float)sf->pw && py < (float)sf->ph)
+          pred = pred_sample(sf, px, py);
+      }
       surf_cache c = {0, 1u, {0, 0, 0}, 0};
       for (uint32_t z = 0; z < sf->L; z++) {
         float v[2] = {0.0f, 0.0f};
@@ -558,6 +578,7 @@ void orc_surf_bake(orc_surf *sf, const orc_bricks *br, float u0, float v0, float
               wp.z < shape.z)
             surf_brick_sample(&s, lod, ovl, wp, shape, &c, v);
         }
+        if (pred >= 0.0f) v[1] = pred;
         uint8_t *o = sf->vol + (((size_t)z * sf->H + y) * sf->W + x) * 2u;
         o[0] = unorm8(v[0]);
         o[1] = unorm8(v[1]);

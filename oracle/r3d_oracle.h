@@ -81,6 +81,11 @@ typedef struct orc_surf {
   uint32_t W, H, L;
   const uint8_t *mask;
   uint32_t mw, mh;
+  /* live 2.5D ink prediction (NULL: none): pw x ph floats, texel (0, 0) at
+   * grid coordinates (pg0u, pg0v), pppg texels per grid unit */
+  const float *pred;
+  uint32_t pw, ph;
+  float pg0u, pg0v, pppg;
 } orc_surf;
 
 /* Brick cache.  LOD mode (brick_mode with the LOD flag): the page table in

@@ -190,6 +190,7 @@ def _load() -> C.CDLL:
         "r3d_cuda_surfvol_window": (I, [P, C.c_double, C.c_double, F, F]),
         "r3d_cuda_surfvol_overlay": (I, [P, I]),
         "r3d_cuda_surfvol_mark": (I, [P]),
+        "r3d_cuda_surfvol_inkpred": (I, [P, P, U32, U32, F, F, F]),
         "r3d_cuda_surfvol_params": (None, [P, P]),
         "r3d_cuda_surfvol_read": (I, [P, P]),
         "r3d_cuda_surfmask": (I, [P, P, U32, U32]),
@@ -212,6 +213,14 @@ def _load() -> C.CDLL:
         "r3d_cuda_stream_update": (I, [P, C.POINTER(StreamView), C.POINTER(StreamStats)]),
         "r3d_cuda_stream_view_of": (None, [P, P, U32, C.POINTER(StreamView)]),
         "r3d_host_stream_desired": (U32, [P, U32, P, P, F, F, U32, U32, F, P, P, U32]),
+        "r3d_host_stream_box": (U32, [P, U32, P, P, F, F, P, P, U32, U32]),
+        "r3d_host_stream_point": (U32, [P, U32, P, U32, F, P, P, U32, U32]),
+        "r3d_host_stream_sort": (None, [P, U32]),
+        "r3d_cuda_stream_collect_begin": (I, [P]),
+        "r3d_cuda_stream_collect_view": (I, [P, C.POINTER(StreamView)]),
+        "r3d_cuda_stream_collect_box": (I, [P, P, P, F, F]),
+        "r3d_cuda_stream_collect_point": (I, [P, P, U32, F]),
+        "r3d_cuda_stream_submit": (I, [P, U32, C.POINTER(StreamStats)]),
         "r3d_cuda_bricks_overlay_build": (I, [P, U32, C.POINTER(VolumeDesc), P]),
         "r3d_cuda_shard_mode": (U32, [P]),
         "r3d_cuda_shard_read": (I, [P, I, P, P, P]),
@@ -254,6 +263,10 @@ def _load() -> C.CDLL:
         "r3d_clip_frame": (I, [P, C.c_double, C.c_double, C.c_uint64, P]),
         "r3d_bricks_begin_stream": (I, [P, C.POINTER(VolumeDesc), P, U32, U32]),
         "r3d_bricks_stream": (None, [P, P, P, F, F, U32, U32, F, U32]),
+        "r3d_bricks_stream_begin": (C.c_bool, [P]),
+        "r3d_bricks_stream_box": (None, [P, P, P, F, F]),
+        "r3d_bricks_stream_point": (None, [P, P, U32, F]),
+        "r3d_bricks_stream_submit": (None, [P, U32]),
         "r3d_bricks_get_stats": (None, [P, P]),
         "r3d_bricks_flush": (None, [P]),
         "r3d_bricks_overlay_volume": (I, [P, U32, C.POINTER(VolumeDesc), P]),
@@ -268,6 +281,9 @@ def _load() -> C.CDLL:
         "r3d_surfvol_visible": (None, [P, U32, U32, U32, U32, U32, U32]),
         "r3d_surfvol_mark": (None, [P]),
         "r3d_surfvol_overlay_enable": (None, [P, C.c_bool]),
+        "r3d_surfvol_regtap": (None, [P, C.c_bool]),
+        "r3d_surfvol_inkpred": (I, [P, P, U32, U32, F, F, F]),
+        "r3d_surfvol_inkpred_clear": (None, [P]),
         "r3d_surfvol_params": (None, [P, P]),
         "r3d_surfmask": (I, [P, P, U32, U32]),
         "r3d_surfmask_clear": (None, [P]),
@@ -336,6 +352,40 @@ def stream_desired(page: np.ndarray, eye, fwd, half_tan: float, pixel_cone: floa
                                     slice_z0, slice_depth, gate, _ptr(mark), out, page.size)
     a = np.ctypeslib.as_array(out)[:n]
     return a.copy()
+
+
+class StreamCollect:
+    """One frame's request set built on the host from any number of cone,
+    box and point collects (r3d_host_stream_desired / _box / _point), as
+    the context's collect calls build it."""
+
+    def __init__(self, page: np.ndarray):
+        self.page = np.ascontiguousarray(page, np.uint32)
+        self.mark = np.zeros(self.page.size, np.uint8)
+        self.out = (StreamCand * self.page.size)()
+        self.n = 0
+
+    def box(self, lo, hi, pixel_cone: float, gate: float = 0.0) -> None:
+        self.n = lib.r3d_host_stream_box(_ptr(self.page), self.page.size, (C.c_float * 3)(*lo),
+                                         (C.c_float * 3)(*hi), pixel_cone, gate, _ptr(self.mark),
+                                         self.out, self.page.size, self.n)
+
+    def point(self, p, level: int, gate: float = 0.0) -> None:
+        self.n = lib.r3d_host_stream_point(_ptr(self.page), self.page.size, (C.c_float * 3)(*p),
+                                           level, gate, _ptr(self.mark), self.out,
+                                           self.page.size, self.n)
+
+    def cone(self, eye, fwd, half_tan: float, pixel_cone: float, gate: float = 0.0,
+             slice_z0: int = 0, slice_depth: int = 0) -> None:
+        tail = C.cast(C.addressof(self.out) + self.n * C.sizeof(StreamCand), C.c_void_p)
+        self.n += lib.r3d_host_stream_desired(_ptr(self.page), self.page.size,
+                                              (C.c_float * 3)(*eye), (C.c_float * 3)(*fwd),
+                                              half_tan, pixel_cone, slice_z0, slice_depth, gate,
+                                              _ptr(self.mark), tail, self.page.size - self.n)
+
+    def sorted(self) -> np.ndarray:
+        lib.r3d_host_stream_sort(self.out, self.n)
+        return np.ctypeslib.as_array(self.out)[:self.n].copy()
 
 
 class VslabHost:
@@ -555,6 +605,26 @@ class Context:
         self._check(lib.r3d_cuda_stream_update(self.h, C.byref(v), C.byref(st)))
         return {k: getattr(st, k) for k, _ in StreamStats._fields_}
 
+    def stream_collect_begin(self) -> None:
+        self._check(lib.r3d_cuda_stream_collect_begin(self.h))
+
+    def stream_collect_view(self, p: "FrameParams", ext=(1.0, 1.0, 1.0)) -> None:
+        v = StreamView()
+        lib.r3d_cuda_stream_view_of(C.byref(p), (C.c_float * 3)(*ext), 0, C.byref(v))
+        self._check(lib.r3d_cuda_stream_collect_view(self.h, C.byref(v)))
+
+    def stream_collect_box(self, lo, hi, pixel_cone: float, gate: float = 0.0) -> None:
+        self._check(lib.r3d_cuda_stream_collect_box(self.h, (C.c_float * 3)(*lo),
+                                                    (C.c_float * 3)(*hi), pixel_cone, gate))
+
+    def stream_collect_point(self, p, level: int, gate: float = 0.0) -> None:
+        self._check(lib.r3d_cuda_stream_collect_point(self.h, (C.c_float * 3)(*p), level, gate))
+
+    def stream_submit(self, budget: int) -> dict:
+        st = StreamStats()
+        self._check(lib.r3d_cuda_stream_submit(self.h, budget, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in StreamStats._fields_}
+
     def clip_build(self, vol, depth_max: int) -> None:
         nz, ny, nx = vol.shape
         d = VolumeDesc(nx, ny, nz, 128, 1.0)
@@ -594,6 +664,16 @@ class Context:
         out = np.empty((p.slab_wz, int(p.slab_ny), int(p.slab_nx), 2), np.uint8)
         self._check(lib.r3d_cuda_surfvol_read(self.h, _ptr(out)))
         return out
+
+    def surfvol_inkpred(self, pred, g0u: float = 0.0, g0v: float = 0.0,
+                        px_per_grid: float = 1.0) -> None:
+        """Live 2.5D ink prediction, (h, w) float32; None drops it."""
+        if pred is None:
+            self._check(lib.r3d_cuda_surfvol_inkpred(self.h, None, 0, 0, 0.0, 0.0, 0.0))
+            return
+        pred = np.ascontiguousarray(pred, np.float32)
+        self._check(lib.r3d_cuda_surfvol_inkpred(self.h, _ptr(pred), pred.shape[1], pred.shape[0],
+                                                 g0u, g0v, px_per_grid))
 
     def surfmask(self, m) -> None:
         if m is None:
@@ -943,6 +1023,19 @@ class Renderer:
         lib.r3d_bricks_stream(self.r, view.eye, view.fwd, view.half_tan, view.pixel_cone,
                               view.slice_z0, view.slice_depth, view.gate, view.budget)
 
+    def bricks_stream_begin(self) -> bool:
+        return bool(lib.r3d_bricks_stream_begin(self.r))
+
+    def bricks_stream_box(self, lo, hi, pixel_cone: float, gate: float = 0.0) -> None:
+        lib.r3d_bricks_stream_box(self.r, (C.c_float * 3)(*lo), (C.c_float * 3)(*hi), pixel_cone,
+                                  gate)
+
+    def bricks_stream_point(self, p, level: int, gate: float = 0.0) -> None:
+        lib.r3d_bricks_stream_point(self.r, (C.c_float * 3)(*p), level, gate)
+
+    def bricks_stream_submit(self, budget: int) -> None:
+        lib.r3d_bricks_stream_submit(self.r, budget)
+
     def bricks_stats(self) -> BricksStats:
         st = BricksStats()
         lib.r3d_bricks_get_stats(self.r, C.byref(st))
@@ -987,6 +1080,17 @@ class Renderer:
 
     def surfvol_overlay_enable(self, on: bool) -> None:
         lib.r3d_surfvol_overlay_enable(self.r, on)
+
+    def surfvol_regtap(self, on: bool) -> None:
+        lib.r3d_surfvol_regtap(self.r, on)
+
+    def surfvol_inkpred(self, pred, g0u: float, g0v: float, px_per_grid: float) -> None:
+        pred = np.ascontiguousarray(pred, np.float32)
+        self._ok(lib.r3d_surfvol_inkpred(self.r, _ptr(pred), pred.shape[1], pred.shape[0], g0u,
+                                         g0v, px_per_grid), "r3d_surfvol_inkpred")
+
+    def surfvol_inkpred_clear(self) -> None:
+        lib.r3d_surfvol_inkpred_clear(self.r)
 
     def surfvol_params(self, p: FrameParams) -> None:
         lib.r3d_surfvol_params(self.r, C.byref(p))

@@ -418,6 +418,121 @@ uint32_t r3d_host_stream_desired(const uint32_t *page, uint32_t page_words, cons
   return n;
 }
 
+void r3d_host_stream_sort(r3d_stream_cand *c, uint32_t n) {
+  if (c && n > 1u) qsort(c, n, sizeof *c, stream_cand_cmp);
+}
+
+/* the brick of level li under voxel-normalized position coordinate v */
+static uint32_t stream_level(const uint32_t *page, uint32_t li, uint32_t *off, uint32_t bd[3],
+                             float *edge, float maxdim) {
+  const uint32_t packed = page[5u + 4u * li];
+  *off = page[4u + 4u * li];
+  bd[0] = packed & 1023u, bd[1] = (packed >> 10) & 1023u, bd[2] = packed >> 20;
+  *edge = (float)(128u * page[6u + 4u * li]) / maxdim;
+  return page[6u + 4u * li];
+}
+
+/* appends brick b unless listed already, absent, or darker than g8 */
+static uint32_t stream_add(const uint32_t *page, uint32_t page_words, uint32_t b, float d2,
+                           uint32_t priority, int g8, uint8_t *mark, r3d_stream_cand *out,
+                           uint32_t cap, uint32_t n) {
+  if (b >= page_words || mark[b]) return n;
+  const uint32_t e = page[b];
+  if (e == R3D_BRICK_ABSENT || (int)(e >> 24) < g8) return n;
+  mark[b] = 1;
+  if (n < cap) out[n++] = (r3d_stream_cand){d2, b, priority};
+  return n;
+}
+
+static int stream_gate8(float gate) {
+  int g8 = (int)(gate * 255.0f + 0.5f);
+  return g8 < 5 ? 5 : g8;  // decoded-air noise floor (vkbackend.c:2348)
+}
+
+static float stream_maxdim(const uint32_t *page) {
+  return (float)(page[1] > page[2] ? (page[1] > page[3] ? page[1] : page[3])
+                                   : (page[2] > page[3] ? page[2] : page[3]));
+}
+
+uint32_t r3d_host_stream_box(const uint32_t *page, uint32_t page_words, const float lo[3],
+                             const float hi[3], float pixel_cone, float gate, uint8_t *mark,
+                             r3d_stream_cand *out, uint32_t cap, uint32_t n) {
+  if (!page || page_words < R3D_BRICK_PAGE_HEADER || !lo || !hi || !mark || !out) return n;
+  const uint32_t nlev = page[0];
+  if (nlev < 1u || nlev > 15u) return n;
+  const int g8 = stream_gate8(gate);
+  const float maxdim = stream_maxdim(page);
+  const float vpp = fmaxf(pixel_cone * maxdim, 1.0f);  // base voxels per pixel
+  uint32_t desired = (uint32_t)floorf(log2f(vpp));
+  if (desired >= nlev) desired = nlev - 1u;
+  uint32_t off, bd[3], rng[3][2];
+  float edge;
+  for (;;) {  // coarsen until the box holds at most 2048 bricks
+    stream_level(page, desired, &off, bd, &edge, maxdim);
+    uint64_t count = 1;
+    for (int a = 0; a < 3; a++) {
+      int64_t a0 = (int64_t)floorf(lo[a] / edge), a1 = (int64_t)floorf(hi[a] / edge) + 1;
+      if (a0 < 0) a0 = 0;
+      if (a1 > (int64_t)bd[a]) a1 = (int64_t)bd[a];
+      if (a1 < a0) a1 = a0;
+      rng[a][0] = (uint32_t)a0, rng[a][1] = (uint32_t)a1;
+      count *= (uint64_t)(a1 - a0);
+    }
+    if (count <= 2048u || desired + 1u >= nlev) break;
+    desired++;
+  }
+  const float cx0 = (lo[0] + hi[0]) * 0.5f, cy0 = (lo[1] + hi[1]) * 0.5f,
+              cz0 = (lo[2] + hi[2]) * 0.5f;
+  uint32_t poff = 0, pbd[3] = {0, 0, 0};
+  float pedge;
+  const int parent = desired + 1u < nlev;
+  if (parent) stream_level(page, desired + 1u, &poff, pbd, &pedge, maxdim);
+  for (uint32_t bz = rng[2][0]; bz < rng[2][1]; bz++)
+    for (uint32_t by = rng[1][0]; by < rng[1][1]; by++)
+      for (uint32_t bx = rng[0][0]; bx < rng[0][1]; bx++) {
+        const float dx = ((float)bx + 0.5f) * edge - cx0;
+        const float dy = ((float)by + 0.5f) * edge - cy0;
+        const float dz = ((float)bz + 0.5f) * edge - cz0;
+        const float d2 = dx * dx + dy * dy + dz * dz;
+        if (parent)
+          n = stream_add(page, page_words, poff + ((bz >> 1) * pbd[1] + (by >> 1)) * pbd[0] + (bx >> 1),
+                         d2, 0u, g8, mark, out, cap, n);
+        n = stream_add(page, page_words, off + (bz * bd[1] + by) * bd[0] + bx, d2, 1u, g8, mark, out,
+                       cap, n);
+      }
+  return n;
+}
+
+uint32_t r3d_host_stream_point(const uint32_t *page, uint32_t page_words, const float p[3],
+                               uint32_t level, float gate, uint8_t *mark, r3d_stream_cand *out,
+                               uint32_t cap, uint32_t n) {
+  if (!page || page_words < R3D_BRICK_PAGE_HEADER || !p || !mark || !out) return n;
+  const uint32_t nlev = page[0];
+  if (nlev < 1u || nlev > 15u) return n;
+  const int g8 = stream_gate8(gate);
+  const float maxdim = stream_maxdim(page);
+  if (level >= nlev) level = nlev - 1u;
+  uint32_t off, bd[3], bc[3];
+  float edge;
+  stream_level(page, level, &off, bd, &edge, maxdim);
+  for (int a = 0; a < 3; a++) {
+    int64_t i = (int64_t)(p[a] / edge);
+    if (i < 0) i = 0;
+    if (i >= (int64_t)bd[a]) i = (int64_t)bd[a] - 1;
+    bc[a] = (uint32_t)i;
+  }
+  if (level + 1u < nlev) {
+    uint32_t poff, pbd[3];
+    float pedge;
+    stream_level(page, level + 1u, &poff, pbd, &pedge, maxdim);
+    n = stream_add(page, page_words,
+                   poff + ((bc[2] >> 1) * pbd[1] + (bc[1] >> 1)) * pbd[0] + (bc[0] >> 1), 0.0f, 0u,
+                   g8, mark, out, cap, n);
+  }
+  return stream_add(page, page_words, off + (bc[2] * bd[1] + bc[1]) * bd[0] + bc[0], 0.0f, 1u, g8,
+                    mark, out, cap, n);
+}
+
 /* ---- virtual slab layout and fill planner ---- */
 
 static const uint32_t vs_scale[R3D_VS_LEVELS] = {1u, 4u, 8u, 16u, 32u};

@@ -46,6 +46,11 @@ struct r3d_cuda_ctx {
   uint32_t *stream_jobs = nullptr;  // device: slots filled by one update
   uint32_t stream_frame = 0;
   cudaEvent_t page_ev = nullptr;
+  // the request set of an open collect (one frame's views), and the
+  // bricks it lists (page_words bytes)
+  bool stream_open = false;
+  std::vector<r3d_stream_cand> stream_cand;
+  std::vector<uint8_t> stream_mark;
 
   // tiled slab: tiles of every level in one buffer, the source volume and
   // per-level overview planes for 16 slices (fill scratch)
@@ -93,6 +98,10 @@ struct r3d_cuda_ctx {
   uint32_t sv_W = 0, sv_H = 0, sv_L = 0, sv_nback = 0;
   float sv_sx = 0.0f, sv_sy = 0.0f, sv_u0 = 0.0f, sv_v0 = 0.0f, sv_step = 0.0f, sv_zoff0 = 0.0f;
   int sv_ovl = -1;  // overlay atlas baked into G (-1: none)
+  // live 2.5D ink prediction baked into G over every layer (null: none)
+  float *sv_pred = nullptr;
+  uint32_t sv_pw = 0, sv_ph = 0;
+  float sv_pg0u = 0.0f, sv_pg0v = 0.0f, sv_pppg = 0.0f;
   bool sv_baked = false;
 
   // single-level brick atlas: 4 mip levels, then the world-indexed

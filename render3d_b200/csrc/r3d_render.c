@@ -49,6 +49,9 @@ struct r3d_renderer {
   uint32_t surf_w, surf_h, surf_l, surf_nback; /* surfvol window */
   int surf_baked;
   float surf_win[4]; /* u0, v0, step, zoff0 of the last bake */
+  /* overlay atlases loaded (bit k: atlas k) and the flattened bake's pick */
+  uint32_t ovl_loaded;
+  int sv_use_overlay, sv_regtap, sv_pick;
 };
 
 static uint64_t now_ns(void) {
@@ -62,6 +65,19 @@ static int report(r3d_renderer *r, const char *what, int rc) {
     fprintf(stderr, "r3d: %s failed (%d): %s\n", what, rc,
             r && r->ctx ? r3d_cuda_last_error(r->ctx) : "");
   return rc;
+}
+
+/* The atlas the flattened bake writes into G (vkbackend.c:1815-1822,7033):
+ * none unless the ink atlas is loaded and r3d_surfvol_overlay_enable is
+ * on; then the registration atlas while its tap is on, else the 3D ink
+ * atlas when loaded, else the ink atlas.  Re-bakes when the pick changes. */
+static void surf_pick(r3d_renderer *r) {
+  if (!r->surf_w) return;
+  int which = -1;
+  if ((r->ovl_loaded & 1u) && r->sv_use_overlay)
+    which = r->sv_regtap && (r->ovl_loaded & 8u) ? 3 : (r->ovl_loaded & 2u) ? 1 : 0;
+  if (which == r->sv_pick) return;
+  if (report(r, "surfvol_overlay", r3d_cuda_surfvol_overlay(r->ctx, which)) == 0) r->sv_pick = which;
 }
 
 int r3d_create(SDL_Window *win, const r3d_config *cfg, r3d_renderer **out) {
@@ -160,6 +176,7 @@ int r3d_bricks_begin_volume(r3d_renderer *r, const r3d_volume_desc *d, const uin
   int rc = r3d_cuda_bricks_build(r->ctx, d, voxels, nlev, min_max);
   if (rc != R3D_OK) return report(r, "bricks_begin_volume", rc);
   r->bricks = 1;
+  r->ovl_loaded = 0;
   r->brick_mode = r3d_cuda_brick_mode(r->ctx);
   r3d_cuda_bricks_info(r->ctx, NULL, NULL, r->shape, NULL);
   return 0;
@@ -176,6 +193,7 @@ int r3d_bricks_begin_shard(r3d_renderer *r, const uint8_t *voxels, uint32_t edge
   int rc = r3d_cuda_shard_build(r->ctx, edge, voxels, edge / 128u, NULL);
   if (rc != R3D_OK) return report(r, "bricks_begin_shard", rc);
   r->bricks = 1;
+  r->ovl_loaded = 0;
   r->brick_mode = r3d_cuda_shard_mode(r->ctx);
   r->shape[0] = r->shape[1] = r->shape[2] = edge;
   return 0;
@@ -185,6 +203,7 @@ int r3d_bricks_end(r3d_renderer *r) {
   if (!r) return -1;
   r->bricks = 0;
   r->brick_mode = 0;
+  r->ovl_loaded = 0;
   return 0;
 }
 
@@ -356,6 +375,7 @@ int r3d_bricks_begin_stream(r3d_renderer *r, const r3d_volume_desc *d, const uin
   int rc = r3d_cuda_stream_begin(r->ctx, d, voxels, nlev, nslots);
   if (rc != R3D_OK) return report(r, "bricks_begin_stream", rc);
   r->bricks = 1;
+  r->ovl_loaded = 0;
   r->streaming = 1;
   r->stream_uploaded = 0;
   memset(&r->stream_last, 0, sizeof r->stream_last);
@@ -379,6 +399,34 @@ void r3d_bricks_stream(r3d_renderer *r, const float eye[3], const float fwd[3], 
   v.budget = budget;
   r3d_stream_stats st;
   if (report(r, "bricks_stream", r3d_cuda_stream_update(r->ctx, &v, &st)) == 0) {
+    r->stream_last = st;
+    r->stream_uploaded += st.uploaded;
+  }
+}
+
+/* The multi-view pump: the reference's begin returns false while a decode
+ * batch is in flight; uploads here finish within _submit, so a frame can
+ * always be opened while streaming. */
+bool r3d_bricks_stream_begin(r3d_renderer *r) {
+  if (!r || !r->streaming) return false;
+  return report(r, "bricks_stream_begin", r3d_cuda_stream_collect_begin(r->ctx)) == 0;
+}
+
+void r3d_bricks_stream_box(r3d_renderer *r, const float lo[3], const float hi[3],
+                           float pixel_cone, float gate) {
+  if (r && r->streaming)
+    report(r, "bricks_stream_box", r3d_cuda_stream_collect_box(r->ctx, lo, hi, pixel_cone, gate));
+}
+
+void r3d_bricks_stream_point(r3d_renderer *r, const float p[3], uint32_t level, float gate) {
+  if (r && r->streaming)
+    report(r, "bricks_stream_point", r3d_cuda_stream_collect_point(r->ctx, p, level, gate));
+}
+
+void r3d_bricks_stream_submit(r3d_renderer *r, uint32_t budget) {
+  if (!r || !r->streaming) return;
+  r3d_stream_stats st;
+  if (report(r, "bricks_stream_submit", r3d_cuda_stream_submit(r->ctx, budget, &st)) == 0) {
     r->stream_last = st;
     r->stream_uploaded += st.uploaded;
   }
@@ -411,7 +459,11 @@ void r3d_bricks_flush(r3d_renderer *r) {
 int r3d_bricks_overlay_volume(r3d_renderer *r, uint32_t which, const r3d_volume_desc *d,
                               const uint8_t *voxels) {
   if (!r) return -1;
-  return report(r, "bricks_overlay", r3d_cuda_bricks_overlay_build(r->ctx, which, d, voxels));
+  int rc = r3d_cuda_bricks_overlay_build(r->ctx, which, d, voxels);
+  if (rc != R3D_OK) return report(r, "bricks_overlay", rc);
+  r->ovl_loaded |= 1u << which;
+  surf_pick(r);
+  return 0;
 }
 
 /* ---- virtual slab (render.h:161-184) ---- */
@@ -480,6 +532,8 @@ int r3d_surfvol_begin(r3d_renderer *r, uint32_t w, uint32_t h, uint32_t layers,
   if (rc != R3D_OK) return report(r, "surfvol_begin", rc);
   r->surf_w = w, r->surf_h = h, r->surf_l = layers, r->surf_nback = nback;
   r->surf_baked = 0;
+  r->sv_pick = -2; /* the context's pick is unknown: set it again */
+  surf_pick(r);
   return 0;
 }
 
@@ -503,7 +557,29 @@ void r3d_surfvol_mark(r3d_renderer *r) {
 }
 
 void r3d_surfvol_overlay_enable(r3d_renderer *r, bool enable) {
-  if (r) report(r, "surfvol_overlay", r3d_cuda_surfvol_overlay(r->ctx, enable ? 0 : -1));
+  if (!r) return;
+  r->sv_use_overlay = enable;
+  surf_pick(r);
+}
+
+void r3d_surfvol_regtap(r3d_renderer *r, bool on) {
+  /* vkbackend.c:5154-5169: a no-op without a surface volume, or to turn
+   * the tap on without a registration atlas */
+  if (!r || !r->surf_w || (on && !(r->ovl_loaded & 8u))) return;
+  r->sv_regtap = on;
+  surf_pick(r);
+}
+
+int r3d_surfvol_inkpred(r3d_renderer *r, const float *pred, uint32_t w, uint32_t h, float g0u,
+                        float g0v, float px_per_grid) {
+  if (!r || !r->surf_w || !pred || !w || !h) return -1;
+  return report(r, "surfvol_inkpred",
+                r3d_cuda_surfvol_inkpred(r->ctx, pred, w, h, g0u, g0v, px_per_grid));
+}
+
+void r3d_surfvol_inkpred_clear(r3d_renderer *r) {
+  if (r && r->surf_w)
+    report(r, "surfvol_inkpred_clear", r3d_cuda_surfvol_inkpred(r->ctx, NULL, 0, 0, 0, 0, 0));
 }
 
 void r3d_surfvol_params(const r3d_renderer *r, r3d_frame_params *p) {

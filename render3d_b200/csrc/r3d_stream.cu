@@ -90,6 +90,9 @@ void stream_reset(r3d_cuda_ctx *c) {
   c->slot_brick.clear();
   c->slot_use.clear();
   c->brick_slot.clear();
+  c->stream_cand.clear();
+  c->stream_mark.clear();
+  c->stream_open = false;
   c->streaming = false;
 }
 
@@ -197,15 +200,14 @@ void r3d_cuda_stream_view_of(const r3d_frame_params *p, const float ext[3], uint
   v->budget = budget;
 }
 
-int r3d_cuda_stream_update(r3d_cuda_ctx *c, const r3d_stream_view *v, r3d_stream_stats *out) {
-  if (!c || !v) return fail(c, R3D_E_INVALID, "stream_update: bad arguments");
+int r3d_cuda_stream_collect_begin(r3d_cuda_ctx *c) {
+  if (!c) return R3D_E_INVALID;
   if (!c->streaming || !c->have_bricks)
-    return fail(c, R3D_E_STATE, "stream_update: no streaming cache");
+    return fail(c, R3D_E_STATE, "stream_collect_begin: no streaming cache");
   cudaSetDevice(c->device);
   // the previous update's page upload reads the shadow: let it finish
   R3D_CUDA_TRY(c, cudaEventSynchronize(c->page_ev));
-  const uint32_t words = c->page_words, nlev = c->br.nlev;
-  const uint32_t frame = ++c->stream_frame;
+  const uint32_t nlev = c->br.nlev, frame = ++c->stream_frame;
   // pin the coarsest level's stamps
   const uint32_t coarse_off = c->br.off[nlev - 1u];
   const uint32_t ncoarse = c->br.bd[nlev - 1u][0] * c->br.bd[nlev - 1u][1] * c->br.bd[nlev - 1u][2];
@@ -213,12 +215,75 @@ int r3d_cuda_stream_update(r3d_cuda_ctx *c, const r3d_stream_view *v, r3d_stream
     const uint32_t s = c->brick_slot[coarse_off + i];
     if (s != R3D_BRICK_ABSENT) c->slot_use[s] = frame;
   }
-  std::vector<uint8_t> mark(words, 0);
-  std::vector<r3d_stream_cand> cand(words);
-  const uint32_t n =
-      r3d_host_stream_desired(c->store_page.data(), words, v->eye, v->fwd, v->half_tan,
-                              v->pixel_cone, v->slice_z0, v->slice_depth, v->gate, mark.data(),
-                              cand.data(), words);
+  c->stream_mark.assign(c->page_words, 0);
+  c->stream_cand.clear();
+  c->stream_cand.reserve(c->page_words);  // a brick is listed once
+  c->stream_open = true;
+  return R3D_OK;
+}
+
+static int collect_check(r3d_cuda_ctx *c, const char *what) {
+  if (!c) return R3D_E_INVALID;
+  if (!c->stream_open) return fail(c, R3D_E_STATE, "%s: no open collect (stream_collect_begin)", what);
+  return R3D_OK;
+}
+
+}  // extern "C"
+
+// grows the candidate list by what a collect appended into its tail
+template <class F>
+static void collect_into(r3d_cuda_ctx *c, F f) {
+  const uint32_t n0 = (uint32_t)c->stream_cand.size(), cap = c->page_words;
+  c->stream_cand.resize(cap);
+  const uint32_t n = f(c->stream_cand.data(), cap, n0);
+  c->stream_cand.resize(n);
+}
+
+extern "C" {
+
+int r3d_cuda_stream_collect_view(r3d_cuda_ctx *c, const r3d_stream_view *v) {
+  int rc = collect_check(c, "stream_collect_view");
+  if (rc != R3D_OK) return rc;
+  if (!v) return fail(c, R3D_E_INVALID, "stream_collect_view: no view");
+  collect_into(c, [&](r3d_stream_cand *out, uint32_t cap, uint32_t n0) {
+    return n0 + r3d_host_stream_desired(c->store_page.data(), c->page_words, v->eye, v->fwd,
+                                        v->half_tan, v->pixel_cone, v->slice_z0, v->slice_depth,
+                                        v->gate, c->stream_mark.data(), out + n0, cap - n0);
+  });
+  return R3D_OK;
+}
+
+int r3d_cuda_stream_collect_box(r3d_cuda_ctx *c, const float lo[3], const float hi[3],
+                                float pixel_cone, float gate) {
+  int rc = collect_check(c, "stream_collect_box");
+  if (rc != R3D_OK) return rc;
+  if (!lo || !hi) return fail(c, R3D_E_INVALID, "stream_collect_box: no box");
+  collect_into(c, [&](r3d_stream_cand *out, uint32_t cap, uint32_t n0) {
+    return r3d_host_stream_box(c->store_page.data(), c->page_words, lo, hi, pixel_cone, gate,
+                               c->stream_mark.data(), out, cap, n0);
+  });
+  return R3D_OK;
+}
+
+int r3d_cuda_stream_collect_point(r3d_cuda_ctx *c, const float p[3], uint32_t level, float gate) {
+  int rc = collect_check(c, "stream_collect_point");
+  if (rc != R3D_OK) return rc;
+  if (!p) return fail(c, R3D_E_INVALID, "stream_collect_point: no point");
+  collect_into(c, [&](r3d_stream_cand *out, uint32_t cap, uint32_t n0) {
+    return r3d_host_stream_point(c->store_page.data(), c->page_words, p, level, gate,
+                                 c->stream_mark.data(), out, cap, n0);
+  });
+  return R3D_OK;
+}
+
+int r3d_cuda_stream_submit(r3d_cuda_ctx *c, uint32_t budget, r3d_stream_stats *out) {
+  int rc = collect_check(c, "stream_submit");
+  if (rc != R3D_OK) return rc;
+  c->stream_open = false;
+  cudaSetDevice(c->device);
+  const uint32_t frame = c->stream_frame, n = (uint32_t)c->stream_cand.size();
+  r3d_stream_cand *cand = c->stream_cand.data();
+  r3d_host_stream_sort(cand, n);  // every collect's candidates, nearest first
   r3d_stream_stats stats;
   memset(&stats, 0, sizeof stats);
   stats.desired = n;
@@ -232,7 +297,7 @@ int r3d_cuda_stream_update(r3d_cuda_ctx *c, const r3d_stream_view *v, r3d_stream
   }
   stats.requested = (uint32_t)req.size();
   std::vector<uint32_t> slots, src;
-  for (size_t k = 0; k < req.size() && slots.size() < v->budget; k++) {
+  for (size_t k = 0; k < req.size() && slots.size() < budget; k++) {
     // free slot first, else the least recently used one not wanted this
     // frame (vkbackend.c:5320-5332); none left: stop rather than thrash
     uint32_t best = R3D_BRICK_ABSENT, bu = UINT32_MAX;
@@ -262,9 +327,20 @@ int r3d_cuda_stream_update(r3d_cuda_ctx *c, const r3d_stream_view *v, r3d_stream
   }
   stats.uploaded = (uint32_t)slots.size();
   for (uint32_t s = 0; s < c->nslots; s++) stats.resident += c->slot_brick[s] != R3D_BRICK_ABSENT;
-  int rc = R3D_OK;
+  c->stream_cand.clear();
   if (!slots.empty()) rc = stream_upload(c, slots, src);
   if (out) *out = stats;
+  return rc;
+}
+
+int r3d_cuda_stream_update(r3d_cuda_ctx *c, const r3d_stream_view *v, r3d_stream_stats *out) {
+  if (!c || !v) return fail(c, R3D_E_INVALID, "stream_update: bad arguments");
+  if (!c->streaming || !c->have_bricks)
+    return fail(c, R3D_E_STATE, "stream_update: no streaming cache");
+  int rc = r3d_cuda_stream_collect_begin(c);
+  if (rc == R3D_OK) rc = r3d_cuda_stream_collect_view(c, v);
+  if (rc == R3D_OK) rc = r3d_cuda_stream_submit(c, v->budget, out);
+  c->stream_open = false;
   return rc;
 }
 

@@ -27,7 +27,24 @@ struct SurfBake {
   uint32_t W, H, L, nback, lod;
   int ovl;       // overlay atlas baked into G, or -1
   uint8_t *vol;  // W x H x L texels of (R, G), x fastest
+  const float *pred;  // live ink prediction, pw x ph, or null
+  uint32_t pw, ph;
+  float pg0u, pg0v, pppg;  // texel (0, 0) in grid coordinates; texels per grid unit
 };
+
+// The prediction texture, clamp-to-edge bilinear at texel-space position
+// (px, py), sampled as textureLod(inkpred, (pp + 0.5) / size)
+// (surfvol.comp:131-136).
+__device__ __forceinline__ float pred_sample(const SurfBake &b, float px, float py) {
+  const float u = (px + 0.5f) / (float)b.pw, v = (py + 0.5f) / (float)b.ph;
+  const float tx = clamp_(fmaf(u, (float)b.pw, -0.5f), 0.0f, (float)(b.pw - 1u));
+  const float ty = clamp_(fmaf(v, (float)b.ph, -0.5f), 0.0f, (float)(b.ph - 1u));
+  const uint32_t x0 = (uint32_t)tx, y0 = (uint32_t)ty;
+  const uint32_t x1 = min(x0 + 1u, b.pw - 1u), y1 = min(y0 + 1u, b.ph - 1u);
+  const float fx = tx - (float)x0, fy = ty - (float)y0;
+  const float *r0 = b.pred + (size_t)y0 * b.pw, *r1 = b.pred + (size_t)y1 * b.pw;
+  return lerp_(lerp_(__ldg(r0 + x0), __ldg(r0 + x1), fx), lerp_(__ldg(r1 + x0), __ldg(r1 + x1), fx), fy);
+}
 
 // Per-column brick cache of the bake (surfvol.comp:40-52)
 struct ColCache {
@@ -113,6 +130,12 @@ __global__ void k_surf_bake(const __grid_constant__ DevScene s, const __grid_con
   }
   const float3 shape = make_float3((float)__ldg(s.br.page + 1), (float)__ldg(s.br.page + 2),
                                    (float)__ldg(s.br.page + 3));
+  // one prediction per column, painted over every layer (surfvol.comp:127-150)
+  float pred = -1.0f;
+  if (b.pred) {
+    const float px = (gx - b.pg0u) * b.pppg, py = (gy - b.pg0v) * b.pppg;
+    if (px >= 0.0f && py >= 0.0f && px < (float)b.pw && py < (float)b.ph) pred = pred_sample(b, px, py);
+  }
   ColCache c = {false, 1u, 0u, 0u, 0u, 0u};
   for (uint32_t z = z0; z < z1; z++) {
     float2 v = make_float2(0.0f, 0.0f);
@@ -123,6 +146,7 @@ __global__ void k_surf_bake(const __grid_constant__ DevScene s, const __grid_con
           wp.z < shape.z)
         v = surf_brick_sample(s, b, wp, shape, c);
     }
+    if (pred >= 0.0f) v.y = pred;
     uint8_t *o = b.vol + (((size_t)z * b.H + y) * b.W + x) * 2u;
     o[0] = unorm8(v.x);
     o[1] = unorm8(v.y);
@@ -335,6 +359,9 @@ void surf_reset(r3d_cuda_ctx *c) {
   cudaFree(c->surf_normals);
   cudaFree(c->sv_vol);
   cudaFree(c->surf_mask);
+  cudaFree(c->sv_pred);
+  c->sv_pred = nullptr;
+  c->sv_pw = c->sv_ph = 0;
   c->surf_coords = c->surf_normals = nullptr;
   c->sv_vol = nullptr;
   c->surf_mask = nullptr;
@@ -363,6 +390,9 @@ static int surf_bake(r3d_cuda_ctx *c) {
   b.lod = lodq;
   b.ovl = c->sv_ovl;
   b.vol = c->sv_vol;
+  b.pred = c->sv_pred;
+  b.pw = c->sv_pw, b.ph = c->sv_ph;
+  b.pg0u = c->sv_pg0u, b.pg0v = c->sv_pg0v, b.pppg = c->sv_pppg;
   const dim3 threads(8, 8), grid((b.W + 7u) / 8u, (b.H + 7u) / 8u);
   k_surf_bake<<<grid, threads, 0, c->stream>>>(c->scene(), b, 0u, b.L);
   R3D_CUDA_TRY(c, cudaGetLastError());
@@ -435,6 +465,36 @@ int r3d_cuda_surfvol_overlay(r3d_cuda_ctx *c, int atlas) {
   cudaSetDevice(c->device);
   c->sv_ovl = atlas;
   return surf_bake(c);
+}
+
+int r3d_cuda_surfvol_inkpred(r3d_cuda_ctx *c, const float *pred, uint32_t w, uint32_t h, float g0u,
+                             float g0v, float px_per_grid) {
+  if (!c) return R3D_E_INVALID;
+  if (!c->sv_vol) return fail(c, R3D_E_STATE, "surfvol_inkpred: no surface volume");
+  cudaSetDevice(c->device);
+  if (!pred) {  // clear (vkbackend.c:1963-1968): re-bake without it
+    if (!c->sv_pred) return R3D_OK;
+    R3D_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    cudaFree(c->sv_pred);
+    c->sv_pred = nullptr;
+    c->sv_pw = c->sv_ph = 0;
+    return surf_bake(c);
+  }
+  if (!w || !h || !(px_per_grid > 0.0f))
+    return fail(c, R3D_E_INVALID, "surfvol_inkpred: a %ux%u prediction at %g texels per grid unit",
+                w, h, (double)px_per_grid);
+  R3D_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  const size_t bytes = (size_t)w * h * sizeof(float);
+  if (c->sv_pw != w || c->sv_ph != h) {  // size change: a new buffer
+    cudaFree(c->sv_pred);
+    c->sv_pred = nullptr;
+    c->sv_pw = c->sv_ph = 0;
+    R3D_CUDA_TRY(c, cudaMalloc(&c->sv_pred, bytes));
+  }
+  R3D_CUDA_TRY(c, copy_sync(c->stream, c->sv_pred, pred, bytes));
+  c->sv_pw = w, c->sv_ph = h;
+  c->sv_pg0u = g0u, c->sv_pg0v = g0v, c->sv_pppg = px_per_grid;
+  return surf_bake(c);  // repaint the window with the new probabilities
 }
 
 int r3d_cuda_surfvol_mark(r3d_cuda_ctx *c) {

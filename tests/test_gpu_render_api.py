@@ -105,9 +105,23 @@ def test_stream_and_overlay_calls(rb, phantom256, scroll_tf):
             st = r.bricks_stats()
             assert st.hot_cap == 5 and st.nlevels == 2 and st.nb == 9 and st.hot <= 5
             assert np.array_equal(_frame(r, p), c.raycast(p, W, H)), i
+        # the multi-view pump: a box and a point into one frame
+        assert r.bricks_stream_begin()
+        r.bricks_stream_box((0.1, 0.2, 0.3), (0.6, 0.5, 0.6), 0.6 / 256)
+        r.bricks_stream_point((0.8, 0.8, 0.2), 0)
+        r.bricks_stream_submit(3)
+        c.stream_collect_begin()
+        c.stream_collect_box((0.1, 0.2, 0.3), (0.6, 0.5, 0.6), 0.6 / 256)
+        c.stream_collect_point((0.8, 0.8, 0.2), 0)
+        st = c.stream_submit(3)
+        assert r.bricks_stats().inflight == st["uploaded"]
+        p = elev35(rb, scroll_tf, W, H, step_voxels=0.5)
+        r.bricks_params(p)
+        assert np.array_equal(_frame(r, p), c.raycast(p, W, H))
         r.close()
         c.close()
         r, c = _pair(rb, scroll_tf)
+        assert not r.bricks_stream_begin()  # not streaming
         ink = np.roll(phantom256, 5, axis=2)
         r.bricks_begin_volume(phantom256, 2)
         r.bricks_overlay_volume(0, ink)
@@ -153,6 +167,38 @@ def test_surf_calls(rb, phantom256, scroll_tf):
             q = p.copy()
             c.surfvol_params(q)
             assert np.array_equal(_frame(r, p), c.raycast(q, W, H)), win
+        # the bake's overlay pick: 3D ink, once loaded, wins over ink; the
+        # registration tap over both; a live prediction over the pick
+        ink3, reg = np.roll(phantom256, -9, axis=0), np.roll(phantom256, 4, axis=2)
+        pred = np.random.default_rng(3).random((40, 50), np.float32)
+        for which, arr in ((1, ink3), (3, reg)):
+            r.bricks_overlay_volume(which, arr)
+            c.overlay_build(which, arr)
+        for regtap, want, use_pred in ((False, 1, False), (True, 3, False), (True, 3, True),
+                                       (False, 1, True), (False, 1, False)):
+            r.surfvol_regtap(regtap)
+            c.surfvol_overlay(want)
+            if use_pred:
+                r.surfvol_inkpred(pred, 20.0, 18.0, 1.5)
+                c.surfvol_inkpred(pred, 20.0, 18.0, 1.5)
+            else:
+                r.surfvol_inkpred_clear()
+                c.surfvol_inkpred(None)
+            p = rb.FrameParams()
+            p.viewport[0], p.viewport[1] = W, H
+            p.cam_origin[:] = (70.0, 60.0, 0.0)
+            p.cam_right[:] = (80.0, 0.0, 0.0)
+            p.cam_up[:] = (0.0, 64.0, 0.0)
+            p.step_voxels, p.density, p.threshold = 0.5, 1.5, 0.02
+            p.slab_depth, p.overlay_flags, p.overlay_gain = 16, 1, 1.5
+            r.surfvol_params(p)
+            q = p.copy()
+            c.surfvol_params(q)
+            assert np.array_equal(_frame(r, p), c.raycast(q, W, H)), (regtap, use_pred)
+            want_vol = c.surfvol_read()
+            got_vol = np.empty_like(want_vol)
+            assert rb.lib.r3d_cuda_surfvol_read(r.cuda, got_vol.ctypes.data) == 0
+            assert np.array_equal(got_vol, want_vol), (regtap, use_pred)
         r.surf_swap(coords, normals, 0.5, 0.5)  # the next window bakes everything
         r.surfvol_window(2.0, 3.0, 1.0, 0.0)
         p = rb.FrameParams()

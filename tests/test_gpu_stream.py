@@ -80,3 +80,68 @@ def test_stream_errors(rb, vol512, scroll_tf):
             c.stream_update(p, budget=4)
     finally:
         c.close()
+
+
+def test_stream_collects(rb, orc, vol512, scroll_tf):
+    """The multi-view pump: a box, points and a cone collected into one
+    frame upload the host request set's bricks nearest first; a cone alone
+    through begin / collect_view / submit equals stream_update; collects
+    outside an open frame fail."""
+    full = orc.BrickScene.build(vol512, 3).page  # every brick of the pyramid
+    box = ((0.2, 0.25, 0.3), (0.7, 0.6, 0.45), 0.6 / 512)
+    pts = [((0.5, 0.5, 0.35), 0), ((0.05, 0.9, 0.9), 1)]
+    c, d = rb.Context(0), rb.Context(0)
+    try:
+        for x in (c, d):
+            x.set_transfer(scroll_tf)
+            x.set_alpha_cutoff(0.98)
+            x.stream_begin(vol512, 3, 30)
+        with pytest.raises(rb.R3DError):
+            c.stream_collect_box(*box)  # no open frame
+        with pytest.raises(rb.R3DError):
+            c.stream_submit(4)
+        c.stream_collect_begin()
+        c.stream_collect_box(*box)
+        for p, lvl in pts:
+            c.stream_collect_point(p, lvl)
+        st = c.stream_submit(budget=12)
+        col = rb.StreamCollect(full)
+        col.box(*box)
+        for p, lvl in pts:
+            col.point(p, lvl)
+        want = col.sorted()
+        assert st["desired"] == col.n and st["uploaded"] == min(12, st["requested"])
+        page, pool = c.bricks_read()
+        coarse = int(page[4 + 8])
+        req = [int(b) for b in want["brick"] if b != coarse]
+        assert st["requested"] == len(req)
+        assert all(page[b] != 0xFFFFFFFF for b in req[:12])  # nearest first
+        assert all(page[b] == 0xFFFFFFFF for b in req[12:])
+        p = _view(rb, scroll_tf, 0.8, -0.3, 1.4)
+        p.brick_mode = c.brick_mode
+        ref = orc.render(p, orc.BrickScene(page, pool), scroll_tf, 320, 240)[0]
+        _cmp(c.raycast(p, 320, 240), ref, "after collects")
+        # a cone alone, two ways: d through stream_update, e through the collects
+        for i in range(3):
+            p = _view(rb, scroll_tf, 0.3 + 0.4 * i, -0.35, 1.2)
+            p.brick_mode = d.brick_mode
+            s1 = d.stream_update(p, budget=5)
+            assert s1["uploaded"] <= 5
+        e = rb.Context(0)
+        try:
+            e.set_transfer(scroll_tf)
+            e.set_alpha_cutoff(0.98)
+            e.stream_begin(vol512, 3, 30)
+            for i in range(3):
+                p = _view(rb, scroll_tf, 0.3 + 0.4 * i, -0.35, 1.2)
+                p.brick_mode = e.brick_mode
+                e.stream_collect_begin()
+                e.stream_collect_view(p)
+                s2 = e.stream_submit(budget=5)
+            assert np.array_equal(e.bricks_read(slots=False)[0], d.bricks_read(slots=False)[0])
+            assert s2 == s1
+        finally:
+            e.close()
+    finally:
+        c.close()
+        d.close()

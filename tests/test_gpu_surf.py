@@ -153,3 +153,30 @@ def test_surf_validation(rb, surf, scroll_tf):
             fresh.raycast(p, 64, 64)
     finally:
         fresh.close()
+
+
+def test_surf_inkpred_bit_exact(rb, orc, surf):
+    """A live prediction at a fractional origin and pitch, bilinear and
+    clamped at its edge, replaces G over every layer inside it; dropping it
+    restores the plain bake."""
+    c, sc = surf
+    rng = np.random.default_rng(31)
+    pred = rng.random((57, 83), np.float32)
+    pred[:5] = -0.25  # negative probabilities leave the overlay byte
+    c.surfvol_overlay(0)
+    try:
+        for g0u, g0v, ppg in ((10.3, 5.6, 1.7), (-3.0, 20.25, 0.8)):
+            c.surfvol_inkpred(pred, g0u, g0v, ppg)
+            c.surfvol_window(2.0, 3.0, 1.0, 0.0)
+            sc.inkpred(pred, g0u, g0v, ppg)
+            sc.bake(2.0, 3.0, 1.0, 0.0, 0)
+            got = c.surfvol_read()
+            assert np.array_equal(got, sc.vol), f"{np.argwhere(got != sc.vol)[:5]}"
+            col = (got[..., 1] == got[:1, ..., 1]).all(axis=0)  # one value per column
+            assert col.mean() > 0.3
+    finally:
+        c.surfvol_inkpred(None)
+        sc.inkpred(None, 0, 0, 0)
+    c.surfvol_window(2.0, 3.0, 1.0, 0.0)
+    sc.bake(2.0, 3.0, 1.0, 0.0, 0)
+    assert np.array_equal(c.surfvol_read(), sc.vol)
