@@ -279,6 +279,24 @@ void r3d_cuda_surfvol_params(const r3d_cuda_ctx *ctx, r3d_frame_params *p);
 int r3d_cuda_surfvol_read(r3d_cuda_ctx *ctx, uint8_t *out);
 int r3d_cuda_surfmask(r3d_cuda_ctx *ctx, const uint8_t *m, uint32_t w, uint32_t h);
 
+/* Post-decode 3D display filter (reference r3d_bricks_postfilter /
+ * r3d_bricks_refilter, src/render/render.h:62-73, src/shaders/postfilt.comp):
+ * each brick that lands in a slot after the call is filtered once, with
+ * its neighbourhoods clamped to the slot.  mode: low byte 1 median of 3^3,
+ * 2 median of 5^3, 3 max of 3^3, 4 max of 5^3 (other values: none); bit 8
+ * adds an unsharp pass after it, centre + amount * (centre - mean of 3^3)
+ * clamped to [0, 1].  targets: bit 0 the CT bricks, bit 1 the ink overlay
+ * atlas, bit 2 the 3D ink atlas (0: the CT bricks).  Applies to resident
+ * builds, streamed uploads and overlay builds and loads; the settings
+ * survive new builds.  Per-slot tables (block maxima, quads) derive from
+ * the filtered bricks; page-table maxima stay those of the bricks as
+ * built, as the reference keeps the decoder's.  _refilter (streaming
+ * caches only; R3D_E_STATE for a resident cache) copies every resident
+ * brick but the coarsest level's in again from the host store through the
+ * current filter, and re-bakes a flattened window. */
+int r3d_cuda_bricks_postfilter(r3d_cuda_ctx *ctx, uint32_t mode, float amount, uint32_t targets);
+int r3d_cuda_bricks_refilter(r3d_cuda_ctx *ctx);
+
 /* Slot-parallel overlay atlases of the LOD brick cache (reference
  * src/render/render.h:51-101; sampled by src/shaders/raycast.slang:45-115,
  * 872-914,1000-1014,1032-1036): which = 0 ink (overlay_flags bit 0, tinted
@@ -292,6 +310,8 @@ int r3d_cuda_surfmask(r3d_cuda_ctx *ctx, const uint8_t *m, uint32_t w, uint32_t 
  * (src/core/labelvol.c:172-196).  Rebuilding or reloading the brick cache
  * removes every overlay. */
 int r3d_cuda_bricks_overlay_load(r3d_cuda_ctx *ctx, uint32_t which, const uint8_t *slots);
+/* Reads atlas `which` back as nslots 128^3 slots (the layout _load takes). */
+int r3d_cuda_bricks_overlay_read(r3d_cuda_ctx *ctx, uint32_t which, uint8_t *slots);
 int r3d_cuda_bricks_overlay_build(r3d_cuda_ctx *ctx, uint32_t which, const r3d_volume_desc *d,
                                   const uint8_t *voxels);
 

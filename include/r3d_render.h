@@ -129,6 +129,12 @@ void r3d_bricks_flush(r3d_renderer *r);
 /* Overlay atlas `which` (0 ink, 1 3D ink, 2 labels, 3 registration) of the
  * LOD cache from a raw volume of the cache's shape (render.h:51-101 read
  * c5d trees and label sources instead). */
+/* Post-decode display filter (render.h:62-73): the mode, amount and target
+ * bits of r3d_cuda_bricks_postfilter, for bricks built, streamed in or
+ * loaded as overlays from now on; _refilter re-streams the resident bricks
+ * of a streamed cache through it (a resident cache is filtered when built). */
+void r3d_bricks_postfilter(r3d_renderer *r, uint32_t mode, float amount, uint32_t targets);
+void r3d_bricks_refilter(r3d_renderer *r);
 int r3d_bricks_overlay_volume(r3d_renderer *r, uint32_t which, const r3d_volume_desc *d,
                               const uint8_t *voxels);
 

@@ -97,6 +97,8 @@ def _load():
     lib.orc_slab_layout.argtypes = [U32, U32, P, P]
     lib.orc_slab_fill.restype = None
     lib.orc_slab_fill.argtypes = [P, U32, U32, U32, U32, U32, C.c_void_p * 8]
+    lib.orc_postfilter.restype = None
+    lib.orc_postfilter.argtypes = [P, U32, U32, F]
     lib.orc_surf_bake.restype = None
     lib.orc_surf_bake.argtypes = [P, P, F, F, F, F, F, F, U32, C.c_int]
     lib.orc_vslab_fill.restype = None
@@ -719,3 +721,11 @@ def ref_lib():
         return None
     r = C.CDLL(REF_LIB_PATH)
     return r
+
+
+def postfilter(slots, mode: int, amount: float = 0.0) -> np.ndarray:
+    """The display filter (orc_postfilter) of (n, 128, 128, 128) u8 slots,
+    returned as a filtered copy."""
+    out = np.array(slots, np.uint8, order="C", copy=True).reshape(-1, 128, 128, 128)
+    lib.orc_postfilter(out.ctypes.data, out.shape[0], mode, amount)
+    return out

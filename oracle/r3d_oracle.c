@@ -1943,3 +1943,104 @@ void orc_m3_ypr(float yaw, float pitch, float roll, float rows[3][3]) {
   rows[2][1] = sy * sr + cy * sp * cr;
   rows[2][2] = cy * cp;
 }
+
+/* ---- post-decode display filter (src/shaders/postfilt.comp) ---- */
+
+/* texelFetch of the slot at l + d, clamped to the slot (postfilt.comp:27-29) */
+static float pf_fetch(const uint8_t *slot, int x, int y, int z, int dx, int dy, int dz) {
+  int cx = x + dx, cy = y + dy, cz = z + dz;
+  cx = cx < 0 ? 0 : cx > 127 ? 127 : cx;
+  cy = cy < 0 ? 0 : cy > 127 ? 127 : cy;
+  cz = cz < 0 ? 0 : cz > 127 ? 127 : cz;
+  return (float)slot[((size_t)cz * 128 + cy) * 128 + cx] / 255.0f;
+}
+
+/* one voxel of shader mode m (1 median 27, 2 unsharp, 3 median 125, 4 max
+ * 27, 5 max 125), postfilt.comp:31-104 */
+static float pf_voxel(const uint8_t *s, int x, int y, int z, int m, float amount) {
+  if (m == 1) { /* partial selection up to rank 13 */
+    float v[27];
+    int n = 0;
+    for (int dz = -1; dz <= 1; dz++)
+      for (int dy = -1; dy <= 1; dy++)
+        for (int dx = -1; dx <= 1; dx++) v[n++] = pf_fetch(s, x, y, z, dx, dy, dz);
+    for (int i = 0; i <= 13; i++) {
+      int mi = i;
+      for (int j = i + 1; j < 27; j++)
+        if (v[j] < v[mi]) mi = j;
+      float t = v[i];
+      v[i] = v[mi];
+      v[mi] = t;
+    }
+    return v[13];
+  }
+  if (m == 2) { /* centre pushed off the box mean */
+    float sum = 0.0f;
+    for (int dz = -1; dz <= 1; dz++)
+      for (int dy = -1; dy <= 1; dy++)
+        for (int dx = -1; dx <= 1; dx++) sum += pf_fetch(s, x, y, z, dx, dy, dz);
+    float center = pf_fetch(s, x, y, z, 0, 0, 0);
+    return clampf_(center + amount * (center - sum / 27.0f), 0.0f, 1.0f);
+  }
+  if (m == 3) { /* u8 histogram, 4 high bits then 4 low bits */
+    int cnt[16] = {0}, rank = 62, coarse = 15, acc = 0;
+    for (int dz = -2; dz <= 2; dz++)
+      for (int dy = -2; dy <= 2; dy++)
+        for (int dx = -2; dx <= 2; dx++) {
+          int q = (int)rintf(pf_fetch(s, x, y, z, dx, dy, dz) * 255.0f);
+          cnt[q >> 4]++;
+        }
+    for (int i = 0; i < 16; i++) {
+      if (acc + cnt[i] > rank) {
+        coarse = i;
+        break;
+      }
+      acc += cnt[i];
+    }
+    int rank2 = rank - acc, fine = 15;
+    memset(cnt, 0, sizeof cnt);
+    for (int dz = -2; dz <= 2; dz++)
+      for (int dy = -2; dy <= 2; dy++)
+        for (int dx = -2; dx <= 2; dx++) {
+          int q = (int)rintf(pf_fetch(s, x, y, z, dx, dy, dz) * 255.0f);
+          if ((q >> 4) == coarse) cnt[q & 15]++;
+        }
+    acc = 0;
+    for (int i = 0; i < 16; i++) {
+      if (acc + cnt[i] > rank2) {
+        fine = i;
+        break;
+      }
+      acc += cnt[i];
+    }
+    return (float)(coarse * 16 + fine) / 255.0f;
+  }
+  int rr = m == 4 ? 1 : 2; /* max pool */
+  float o = 0.0f;
+  for (int dz = -rr; dz <= rr; dz++)
+    for (int dy = -rr; dy <= rr; dy++)
+      for (int dx = -rr; dx <= rr; dx++) o = fmaxf(o, pf_fetch(s, x, y, z, dx, dy, dz));
+  return o;
+}
+
+void orc_postfilter(uint8_t *slots, uint32_t n, uint32_t mode, float amount) {
+  static const int prim2shader[5] = {0, 1, 3, 4, 5}; /* vkbackend.c:3411-3417 */
+  const uint32_t prim = mode & 0xFFu;
+  const size_t sb = (size_t)128 * 128 * 128;
+  uint8_t *tmp = malloc(sb);
+  if (!tmp) return;
+  for (uint32_t k = 0; k < n; k++) {
+    uint8_t *s = slots + k * sb;
+    for (int pass = 0; pass < 2; pass++) {
+      int m = pass == 0 ? (prim < 5u ? prim2shader[prim] : 0) : (mode & 0x100u ? 2 : 0);
+      if (!m) continue;
+#pragma omp parallel for schedule(static)
+      for (int z = 0; z < 128; z++)
+        for (int y = 0; y < 128; y++)
+          for (int x = 0; x < 128; x++)
+            tmp[((size_t)z * 128 + y) * 128 + x] = unorm8(pf_voxel(s, x, y, z, m, amount));
+      memcpy(s, tmp, sb);
+    }
+  }
+  free(tmp);
+}

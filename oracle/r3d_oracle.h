@@ -259,6 +259,12 @@ uint32_t orc_lod_pick(float distance, float pixel_cone, float base_voxels, uint3
 uint32_t orc_lod_fallback(uint32_t desired, uint32_t ordinal, uint32_t nlevels);
 void orc_m3_ypr(float yaw, float pitch, float roll, float rows[3][3]);
 
+/* Post-decode display filter of n 128^3 slots in place (src/shaders/
+ * postfilt.comp run by src/vk/vkbackend.c:3398-3466): mode low byte 1
+ * median of 3^3, 2 median of 5^3, 3 max of 3^3, 4 max of 5^3, then the
+ * unsharp pass when bit 8 is set; neighbourhoods clamp to the slot. */
+void orc_postfilter(uint8_t *slots, uint32_t n, uint32_t mode, float amount);
+
 #ifdef __cplusplus
 }
 #endif

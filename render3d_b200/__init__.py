@@ -191,6 +191,9 @@ def _load() -> C.CDLL:
         "r3d_cuda_surfvol_overlay": (I, [P, I]),
         "r3d_cuda_surfvol_mark": (I, [P]),
         "r3d_cuda_surfvol_inkpred": (I, [P, P, U32, U32, F, F, F]),
+        "r3d_cuda_bricks_postfilter": (I, [P, U32, F, U32]),
+        "r3d_cuda_bricks_refilter": (I, [P]),
+        "r3d_cuda_bricks_overlay_read": (I, [P, U32, P]),
         "r3d_cuda_surfvol_params": (None, [P, P]),
         "r3d_cuda_surfvol_read": (I, [P, P]),
         "r3d_cuda_surfmask": (I, [P, P, U32, U32]),
@@ -282,6 +285,8 @@ def _load() -> C.CDLL:
         "r3d_surfvol_mark": (None, [P]),
         "r3d_surfvol_overlay_enable": (None, [P, C.c_bool]),
         "r3d_surfvol_regtap": (None, [P, C.c_bool]),
+        "r3d_bricks_postfilter": (None, [P, U32, F, U32]),
+        "r3d_bricks_refilter": (None, [P]),
         "r3d_surfvol_inkpred": (I, [P, P, U32, U32, F, F, F]),
         "r3d_surfvol_inkpred_clear": (None, [P]),
         "r3d_surfvol_params": (None, [P, P]),
@@ -665,6 +670,20 @@ class Context:
         self._check(lib.r3d_cuda_surfvol_read(self.h, _ptr(out)))
         return out
 
+    def bricks_postfilter(self, mode: int, amount: float = 0.0, targets: int = 1) -> None:
+        """The display filter for bricks landing in slots from now on."""
+        self._check(lib.r3d_cuda_bricks_postfilter(self.h, mode, amount, targets))
+
+    def bricks_refilter(self) -> None:
+        self._check(lib.r3d_cuda_bricks_refilter(self.h))
+
+    def overlay_read(self, which: int) -> np.ndarray:
+        """Overlay atlas `which` as (nslots, 128, 128, 128) u8."""
+        n = self.bricks_info()["nslots"]
+        out = np.empty((n, 128, 128, 128), np.uint8)
+        self._check(lib.r3d_cuda_bricks_overlay_read(self.h, which, _ptr(out)))
+        return out
+
     def surfvol_inkpred(self, pred, g0u: float = 0.0, g0v: float = 0.0,
                         px_per_grid: float = 1.0) -> None:
         """Live 2.5D ink prediction, (h, w) float32; None drops it."""
@@ -1022,6 +1041,12 @@ class Renderer:
     def bricks_stream(self, view: "StreamView") -> None:
         lib.r3d_bricks_stream(self.r, view.eye, view.fwd, view.half_tan, view.pixel_cone,
                               view.slice_z0, view.slice_depth, view.gate, view.budget)
+
+    def bricks_postfilter(self, mode: int, amount: float = 0.0, targets: int = 1) -> None:
+        lib.r3d_bricks_postfilter(self.r, mode, amount, targets)
+
+    def bricks_refilter(self) -> None:
+        lib.r3d_bricks_refilter(self.r)
 
     def bricks_stream_begin(self) -> bool:
         return bool(lib.r3d_bricks_stream_begin(self.r))

@@ -284,6 +284,7 @@ void r3d_cuda_destroy(r3d_cuda_ctx *c) {
   clip_reset(c);
   vslab_reset(c);
   surf_reset(c);
+  postfilter_reset(c);
   if (c->page_ev) cudaEventDestroy(c->page_ev);
   cudaFree(c->diff_q);
   cudaFree(c->tape);
@@ -641,6 +642,15 @@ int r3d_cuda_bricks_build(r3d_cuda_ctx *c, const r3d_volume_desc *d, const uint8
     c->shape[2] = nz;
     c->br = b;
     c->have_bricks = false;
+    // the display filter, before the tables that derive from the slots (a
+    // build whose pool becomes a streaming store stays unfiltered: its
+    // bricks are filtered when uploaded)
+    if (!c->defer_tables && postfilter_on(c, 0u)) {
+      std::vector<uint32_t> all(nslots);
+      for (uint32_t s = 0; s < nslots; s++) all[s] = s;
+      rc = postfilter_slots(c, 0u, c->pool, all.data(), nslots);
+      if (rc != R3D_OK) goto out;
+    }
     rc = build_blockmax(c);
     if (rc != R3D_OK) goto out;
     c->have_bricks = true;

@@ -49,6 +49,11 @@ struct r3d_cuda_ctx {
   // the request set of an open collect (one frame's views), and the
   // bricks it lists (page_words bytes)
   bool stream_open = false;
+  // post-decode display filter (mode word, sharpen amount, target bits:
+  // 0 CT, 1 ink atlas, 2 3D ink atlas) and its scratch slots
+  uint32_t pf_mode = 0, pf_targets = 1;
+  float pf_amount = 0.0f;
+  uint8_t *pf_scratch = nullptr;
   std::vector<r3d_stream_cand> stream_cand;
   std::vector<uint8_t> stream_mark;
 
@@ -213,6 +218,13 @@ cudaError_t launch_view(const r3d_cuda_ctx *c, const r3d_frame_params &pc, uint8
 int build_blockmax(r3d_cuda_ctx *c);
 // Drops the streaming state (host store, shadows, LRU).
 void stream_reset(r3d_cuda_ctx *c);
+// The display filter: whether it changes target t (0 CT, 1 ink atlas, 2 3D
+// ink atlas), and filtering n slots of a 128^3-slot pool in place, on the
+// context's stream.
+bool postfilter_on(const r3d_cuda_ctx *c, uint32_t target);
+int postfilter_slots(r3d_cuda_ctx *c, uint32_t target, uint8_t *pool, const uint32_t *slots,
+                     uint32_t n);
+void postfilter_reset(r3d_cuda_ctx *c);
 // Frees the tiled slab / the clipmap.
 void slab_reset(r3d_cuda_ctx *c);
 void clip_reset(r3d_cuda_ctx *c);

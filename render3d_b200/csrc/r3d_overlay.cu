@@ -42,13 +42,20 @@ __global__ void k_label_stride(const uint8_t *__restrict__ vol, uint32_t nx, uin
   }
 }
 
+// Byte 0 of every quad word: the atlas's own texels.
+__global__ void k_quad_texels(const uint32_t *__restrict__ quad, uint8_t *__restrict__ out, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    out[i] = (uint8_t)(quad[i] & 0xFFu);
+}
+
 static unsigned ovl_grid(size_t n) {
   size_t b = (n + 255) / 256;
   return (unsigned)(b < 148u * 64u ? (b ? b : 1) : 148u * 64u);
 }
 
 // Converts a byte pool (device) into overlay atlas `which`.
-static int set_overlay(r3d_cuda_ctx *c, uint32_t which, const uint8_t *pool) {
+static int overlay_quads(r3d_cuda_ctx *c, uint32_t which, const uint8_t *pool) {
   const size_t n = (size_t)(c->nslots ? c->nslots : 1u) * (128u * 128u * 128u);
   uint32_t *q = nullptr;
   R3D_CUDA_TRY(c, cudaMalloc(&q, n * sizeof(uint32_t)));
@@ -63,6 +70,32 @@ static int set_overlay(r3d_cuda_ctx *c, uint32_t which, const uint8_t *pool) {
   c->ovl_quad[which] = q;
   c->br.ovl[which] = q;
   return R3D_OK;
+}
+
+// overlay_quads through the display filter when it targets the atlas (ink:
+// target 1, 3D ink: 2); a pool the context does not own is filtered in a
+// copy.
+static int set_overlay(r3d_cuda_ctx *c, uint32_t which, const uint8_t *pool, bool owned) {
+  if (which >= 2u || !c->nslots || !postfilter_on(c, which + 1u)) return overlay_quads(c, which, pool);
+  const size_t n = (size_t)c->nslots * (128u * 128u * 128u);
+  uint8_t *f = owned ? const_cast<uint8_t *>(pool) : nullptr;
+  if (!owned) {
+    R3D_CUDA_TRY(c, cudaMalloc(&f, n));
+    cudaError_t e = cudaMemcpyAsync(f, pool, n, cudaMemcpyDeviceToDevice, c->stream);
+    if (e != cudaSuccess) {
+      cudaFree(f);
+      return cuda_fail(c, e, "bricks_overlay: filter copy");
+    }
+  }
+  std::vector<uint32_t> all(c->nslots);
+  for (uint32_t s = 0; s < c->nslots; s++) all[s] = s;
+  int rc = postfilter_slots(c, which + 1u, f, all.data(), c->nslots);
+  if (rc == R3D_OK) rc = overlay_quads(c, which, f);  // synchronizes the stream
+  if (!owned) {
+    cudaStreamSynchronize(c->stream);
+    cudaFree(f);
+  }
+  return rc;
 }
 
 }  // namespace r3d
@@ -83,13 +116,29 @@ int r3d_cuda_bricks_overlay_load(r3d_cuda_ctx *c, uint32_t which, const uint8_t 
     return R3D_OK;
   }
   const size_t bytes = (size_t)c->nslots * (128u * 128u * 128u);
-  if (is_device_ptr(slots)) return set_overlay(c, which, slots);
+  if (is_device_ptr(slots)) return set_overlay(c, which, slots, false);
   uint8_t *tmp = nullptr;
   R3D_CUDA_TRY(c, cudaMalloc(&tmp, bytes ? bytes : 1u));
   cudaError_t e = copy_sync(c->stream, tmp, slots, bytes);
-  int rc = e == cudaSuccess ? set_overlay(c, which, tmp) : cuda_fail(c, e, "bricks_overlay_load");
+  int rc = e == cudaSuccess ? set_overlay(c, which, tmp, true) : cuda_fail(c, e, "bricks_overlay_load");
   cudaFree(tmp);
   return rc;
+}
+
+int r3d_cuda_bricks_overlay_read(r3d_cuda_ctx *c, uint32_t which, uint8_t *slots) {
+  if (!c || which > 3u || !slots) return fail(c, R3D_E_INVALID, "bricks_overlay_read: bad arguments");
+  if (!c->ovl_quad[which]) return fail(c, R3D_E_STATE, "bricks_overlay_read: atlas %u is not loaded", which);
+  cudaSetDevice(c->device);
+  const size_t n = (size_t)c->nslots * (128u * 128u * 128u);
+  if (!n) return R3D_OK;
+  uint8_t *tmp = nullptr;
+  R3D_CUDA_TRY(c, cudaMalloc(&tmp, n));
+  k_quad_texels<<<ovl_grid(n), 256, 0, c->stream>>>(c->ovl_quad[which], tmp, n);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(slots, tmp, n, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(tmp);
+  return e == cudaSuccess ? R3D_OK : cuda_fail(c, e, "bricks_overlay_read");
 }
 
 int r3d_cuda_bricks_overlay_build(r3d_cuda_ctx *c, uint32_t which, const r3d_volume_desc *d,
@@ -166,7 +215,7 @@ int r3d_cuda_bricks_overlay_build(r3d_cuda_ctx *c, uint32_t which, const r3d_vol
     joff += lvl_count[l];
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  int rc = e == cudaSuccess ? set_overlay(c, which, pool) : cuda_fail(c, e, "bricks_overlay_build");
+  int rc = e == cudaSuccess ? set_overlay(c, which, pool, true) : cuda_fail(c, e, "bricks_overlay_build");
   cudaFree(lev);
   cudaFree(pool);
   cudaFree(jobs);

@@ -456,6 +456,15 @@ void r3d_bricks_flush(r3d_renderer *r) {
   if (r) cudaStreamSynchronize((cudaStream_t)r3d_cuda_stream(r->ctx));
 }
 
+void r3d_bricks_postfilter(r3d_renderer *r, uint32_t mode, float amount, uint32_t targets) {
+  if (r) report(r, "bricks_postfilter", r3d_cuda_bricks_postfilter(r->ctx, mode, amount, targets));
+}
+
+void r3d_bricks_refilter(r3d_renderer *r) {
+  /* a no-op without a streamed LOD cache, as the reference's without one */
+  if (r && r->streaming) report(r, "bricks_refilter", r3d_cuda_bricks_refilter(r->ctx));
+}
+
 int r3d_bricks_overlay_volume(r3d_renderer *r, uint32_t which, const r3d_volume_desc *d,
                               const uint8_t *voxels) {
   if (!r) return -1;

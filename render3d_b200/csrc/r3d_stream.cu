@@ -60,6 +60,9 @@ static int stream_upload(r3d_cuda_ctx *c, const std::vector<uint32_t> &slots,
     R3D_CUDA_TRY(c, cudaMemcpyAsync(c->pool + (size_t)slots[i] * kSlotBytes,
                                     c->store + (size_t)src[i] * kSlotBytes, kSlotBytes,
                                     cudaMemcpyHostToDevice, st));
+  // the display filter, before the slot tables
+  const int frc = postfilter_slots(c, 0u, c->pool, slots.data(), (uint32_t)slots.size());
+  if (frc != R3D_OK) return frc;
   for (size_t j0 = 0; j0 < slots.size(); j0 += 65535u) {
     const uint32_t nj = (uint32_t)std::min<size_t>(slots.size() - j0, 65535u);
     R3D_CUDA_TRY(c, cudaMemcpyAsync(c->stream_jobs + j0, slots.data() + j0, nj * 4u,
@@ -330,6 +333,31 @@ int r3d_cuda_stream_submit(r3d_cuda_ctx *c, uint32_t budget, r3d_stream_stats *o
   c->stream_cand.clear();
   if (!slots.empty()) rc = stream_upload(c, slots, src);
   if (out) *out = stats;
+  return rc;
+}
+
+int r3d_cuda_bricks_refilter(r3d_cuda_ctx *c) {
+  if (!c) return R3D_E_INVALID;
+  if (!c->have_bricks) return fail(c, R3D_E_STATE, "bricks_refilter: no brick cache");
+  if (!c->streaming)
+    return fail(c, R3D_E_STATE, "bricks_refilter: a resident cache is filtered when it is built; "
+                                "build it again to apply another filter");
+  cudaSetDevice(c->device);
+  R3D_CUDA_TRY(c, cudaEventSynchronize(c->page_ev));
+  // every resident brick but the pinned coarsest level's, again from the
+  // store through the current filter (vkbackend.c:4875-4906 invalidates
+  // them to re-stream; here they are refilled within the call)
+  const uint32_t nlev = c->br.nlev, c0 = c->br.off[nlev - 1u];
+  const uint32_t c1 = c0 + c->br.bd[nlev - 1u][0] * c->br.bd[nlev - 1u][1] * c->br.bd[nlev - 1u][2];
+  std::vector<uint32_t> slots, src;
+  for (uint32_t s = 0; s < c->nslots; s++) {
+    const uint32_t b = c->slot_brick[s];
+    if (b == R3D_BRICK_ABSENT || (b >= c0 && b < c1)) continue;
+    slots.push_back(s);
+    src.push_back(c->store_page[b] & 0xFFFFFFu);
+  }
+  int rc = slots.empty() ? R3D_OK : stream_upload(c, slots, src);
+  if (rc == R3D_OK) rc = r3d_cuda_surfvol_mark(c);  // a baked flattened window re-bakes
   return rc;
 }
 
