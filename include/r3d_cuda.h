@@ -310,6 +310,20 @@ int r3d_cuda_bricks_refilter(r3d_cuda_ctx *ctx);
  * (src/core/labelvol.c:172-196).  Rebuilding or reloading the brick cache
  * removes every overlay. */
 int r3d_cuda_bricks_overlay_load(r3d_cuda_ctx *ctx, uint32_t which, const uint8_t *slots);
+/* CPU-sourced atlases (reference r3d_bricks_labels / _labels_sync,
+ * r3d_bricks_regatlas / _sync / _detach, src/render/render.h:74-97,
+ * src/vk/vkbackend.c:4908-5150): _attach gives atlas `which` a source of
+ * per-brick content (r3d_brick_src); a missing atlas starts cleared, and
+ * re-attaching (or attaching to one built or loaded) zeroes every slot
+ * before refilling it.  Each _sync round picks up to budget slots (0 or
+ * over 16: 16) by r3d_host_atlas_pick: stale slots zeroed first, else
+ * slots whose brick's generation changed, fetched on the calling thread;
+ * it uploads them on the context's stream and reports how many in
+ * *synced.  _detach drops the source and keeps the atlas; a sync without a
+ * source does nothing.  A new brick cache detaches every source. */
+int r3d_cuda_bricks_atlas_attach(r3d_cuda_ctx *ctx, uint32_t which, const r3d_brick_src *src);
+int r3d_cuda_bricks_atlas_sync(r3d_cuda_ctx *ctx, uint32_t which, uint32_t budget, uint32_t *synced);
+int r3d_cuda_bricks_atlas_detach(r3d_cuda_ctx *ctx, uint32_t which);
 /* Reads atlas `which` back as nslots 128^3 slots (the layout _load takes). */
 int r3d_cuda_bricks_overlay_read(r3d_cuda_ctx *ctx, uint32_t which, uint8_t *slots);
 int r3d_cuda_bricks_overlay_build(r3d_cuda_ctx *ctx, uint32_t which, const r3d_volume_desc *d,

@@ -92,6 +92,33 @@ uint32_t r3d_host_stream_point(const uint32_t *page, uint32_t page_words, const 
 /* Sorts candidates by priority, then distance, then brick. */
 void r3d_host_stream_sort(r3d_stream_cand *c, uint32_t n);
 
+/* A CPU-sourced slot-parallel atlas (labels, registration; reference
+ * r3d_label_src, src/render/render.h:80-101): gen(level, bx, by, bz) is a
+ * cheap content generation of a brick (0: no content), fetch(...) fills
+ * the brick's 128^3 bytes, x fastest. */
+typedef struct r3d_brick_src {
+  uint32_t (*gen)(void *user, uint32_t level, uint32_t bx, uint32_t by, uint32_t bz);
+  void (*fetch)(void *user, uint32_t level, uint32_t bx, uint32_t by, uint32_t bz, uint8_t *out);
+  void *user;
+} r3d_brick_src;
+
+/* Level and brick coordinates of page-table word b (b in a level's range). */
+int r3d_host_brick_locate(const uint32_t *page, uint32_t b, uint32_t *level, uint32_t *bx,
+                          uint32_t *by, uint32_t *bz);
+
+/* One sync round of such an atlas (src/vk/vkbackend.c:4990-5060): slot s
+ * holds brick slot_brick[s] (R3D_BRICK_ABSENT: free) and its atlas content
+ * carries key keys[s] (0: zeros, else (brick + 1) << 32 | generation).
+ * First the stale slots, whose key names another brick, are picked to be
+ * zeroed (new key 0); only when there are none, the slots whose wanted key
+ * (from src->gen of their brick; 0 when it returns 0) differs from theirs.
+ * At most budget slots (0 or over 16: 16), in slot order.  Writes each
+ * pick's slot, brick and new key; the caller fetches the bricks with a
+ * nonzero key and zeroes the rest.  Returns the number picked. */
+uint32_t r3d_host_atlas_pick(const uint32_t *page, const uint32_t *slot_brick, uint32_t nslots,
+                             const uint64_t *keys, const r3d_brick_src *src, uint32_t budget,
+                             uint32_t *sel_slot, uint32_t *sel_brick, uint64_t *sel_key);
+
 /* Virtual slab: a W x H x D window anywhere in a volume, rendered from
  * world-anchored toroidal tile grids (src/core/vslab.h).  Level l has
  * spacing s = {1, 4, 8, 16, 32}[l] and cells of px * s voxels; cell (cx, cy)

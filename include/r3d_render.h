@@ -129,6 +129,22 @@ void r3d_bricks_flush(r3d_renderer *r);
 /* Overlay atlas `which` (0 ink, 1 3D ink, 2 labels, 3 registration) of the
  * LOD cache from a raw volume of the cache's shape (render.h:51-101 read
  * c5d trees and label sources instead). */
+/* CPU-sourced atlases (render.h:74-97): labels (overlay_flags bit 3) and
+ * registration (bit 4).  gen() is polled per resident slot on each sync;
+ * fetch() fills a 128^3 brick only when gen changed.  _regatlas_sync runs
+ * its round within the call; _regatlas_detach drops the source before the
+ * caller destroys it and keeps the atlas for a later re-attach. */
+typedef struct r3d_label_src {
+  uint32_t (*gen)(void *user, uint32_t level, uint32_t bx, uint32_t by, uint32_t bz);
+  void (*fetch)(void *user, uint32_t level, uint32_t bx, uint32_t by, uint32_t bz,
+                uint8_t *out);
+  void *user;
+} r3d_label_src;
+int r3d_bricks_labels(r3d_renderer *r, const r3d_label_src *src);
+void r3d_bricks_labels_sync(r3d_renderer *r, uint32_t budget);
+int r3d_bricks_regatlas(r3d_renderer *r, const r3d_label_src *src);
+void r3d_bricks_regatlas_sync(r3d_renderer *r, uint32_t budget);
+void r3d_bricks_regatlas_detach(r3d_renderer *r);
 /* Post-decode display filter (render.h:62-73): the mode, amount and target
  * bits of r3d_cuda_bricks_postfilter, for bricks built, streamed in or
  * loaded as overlays from now on; _refilter re-streams the resident bricks

@@ -134,6 +134,32 @@ class StreamCand(C.Structure):
     _fields_ = [("d2", C.c_float), ("brick", C.c_uint32), ("priority", C.c_uint32)]
 
 
+GEN_FN = C.CFUNCTYPE(C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32)
+FETCH_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                       C.POINTER(C.c_uint8))
+
+
+class BrickSrc(C.Structure):
+    """r3d_brick_src / r3d_label_src: per-brick content generation and fetch."""
+    _fields_ = [("gen", GEN_FN), ("fetch", FETCH_FN), ("user", C.c_void_p)]
+
+
+def brick_src(gen, fetch) -> BrickSrc:
+    """A source from Python callables gen(level, bx, by, bz) -> int and
+    fetch(level, bx, by, bz) -> (128, 128, 128) u8 array.  Keep the
+    returned object alive while it is attached."""
+    def g(_u, l, x, y, z):
+        return int(gen(l, x, y, z)) & 0xFFFFFFFF
+
+    def f(_u, l, x, y, z, out):
+        a = np.ascontiguousarray(fetch(l, x, y, z), np.uint8).reshape(-1)
+        assert a.size == 128 ** 3
+        C.memmove(out, a.ctypes.data, a.size)
+    s = BrickSrc(GEN_FN(g), FETCH_FN(f), None)
+    s._keep = (g, f)
+    return s
+
+
 class VslabLayout(C.Structure):
     _fields_ = [("nx", C.c_uint64), ("ny", C.c_uint64), ("nz", C.c_uint64),
                 ("W", C.c_uint32), ("H", C.c_uint32), ("D", C.c_uint32),
@@ -194,6 +220,12 @@ def _load() -> C.CDLL:
         "r3d_cuda_bricks_postfilter": (I, [P, U32, F, U32]),
         "r3d_cuda_bricks_refilter": (I, [P]),
         "r3d_cuda_bricks_overlay_read": (I, [P, U32, P]),
+        "r3d_cuda_bricks_atlas_attach": (I, [P, U32, C.POINTER(BrickSrc)]),
+        "r3d_cuda_bricks_atlas_sync": (I, [P, U32, U32, C.POINTER(C.c_uint32)]),
+        "r3d_cuda_bricks_atlas_detach": (I, [P, U32]),
+        "r3d_host_brick_locate": (I, [P, U32, C.POINTER(U32), C.POINTER(U32), C.POINTER(U32),
+                                      C.POINTER(U32)]),
+        "r3d_host_atlas_pick": (U32, [P, P, U32, P, C.POINTER(BrickSrc), U32, P, P, P]),
         "r3d_cuda_surfvol_params": (None, [P, P]),
         "r3d_cuda_surfvol_read": (I, [P, P]),
         "r3d_cuda_surfmask": (I, [P, P, U32, U32]),
@@ -286,6 +318,11 @@ def _load() -> C.CDLL:
         "r3d_surfvol_overlay_enable": (None, [P, C.c_bool]),
         "r3d_surfvol_regtap": (None, [P, C.c_bool]),
         "r3d_bricks_postfilter": (None, [P, U32, F, U32]),
+        "r3d_bricks_labels": (I, [P, C.POINTER(BrickSrc)]),
+        "r3d_bricks_labels_sync": (None, [P, U32]),
+        "r3d_bricks_regatlas": (I, [P, C.POINTER(BrickSrc)]),
+        "r3d_bricks_regatlas_sync": (None, [P, U32]),
+        "r3d_bricks_regatlas_detach": (None, [P]),
         "r3d_bricks_refilter": (None, [P]),
         "r3d_surfvol_inkpred": (I, [P, P, U32, U32, F, F, F]),
         "r3d_surfvol_inkpred_clear": (None, [P]),
@@ -677,6 +714,19 @@ class Context:
     def bricks_refilter(self) -> None:
         self._check(lib.r3d_cuda_bricks_refilter(self.h))
 
+    def atlas_attach(self, which: int, src: BrickSrc) -> None:
+        self._check(lib.r3d_cuda_bricks_atlas_attach(self.h, which, C.byref(src)))
+        self._srcs = getattr(self, "_srcs", {})
+        self._srcs[which] = src
+
+    def atlas_sync(self, which: int, budget: int = 0) -> int:
+        n = C.c_uint32()
+        self._check(lib.r3d_cuda_bricks_atlas_sync(self.h, which, budget, C.byref(n)))
+        return n.value
+
+    def atlas_detach(self, which: int) -> None:
+        self._check(lib.r3d_cuda_bricks_atlas_detach(self.h, which))
+
     def overlay_read(self, which: int) -> np.ndarray:
         """Overlay atlas `which` as (nslots, 128, 128, 128) u8."""
         n = self.bricks_info()["nslots"]
@@ -1044,6 +1094,25 @@ class Renderer:
 
     def bricks_postfilter(self, mode: int, amount: float = 0.0, targets: int = 1) -> None:
         lib.r3d_bricks_postfilter(self.r, mode, amount, targets)
+
+    def bricks_labels(self, src: BrickSrc) -> None:
+        self._srcs = getattr(self, "_srcs", {})
+        self._srcs[2] = src
+        self._ok(lib.r3d_bricks_labels(self.r, C.byref(src)), "r3d_bricks_labels")
+
+    def bricks_labels_sync(self, budget: int = 0) -> None:
+        lib.r3d_bricks_labels_sync(self.r, budget)
+
+    def bricks_regatlas(self, src: BrickSrc) -> None:
+        self._srcs = getattr(self, "_srcs", {})
+        self._srcs[3] = src
+        self._ok(lib.r3d_bricks_regatlas(self.r, C.byref(src)), "r3d_bricks_regatlas")
+
+    def bricks_regatlas_sync(self, budget: int = 0) -> None:
+        lib.r3d_bricks_regatlas_sync(self.r, budget)
+
+    def bricks_regatlas_detach(self) -> None:
+        lib.r3d_bricks_regatlas_detach(self.r)
 
     def bricks_refilter(self) -> None:
         lib.r3d_bricks_refilter(self.r)

@@ -272,6 +272,8 @@ void r3d_cuda_destroy(r3d_cuda_ctx *c) {
   cudaFree(c->bmax);
   cudaFree(c->quad);
   for (int i = 0; i < 4; i++) cudaFree(c->ovl_quad[i]);
+  cudaFreeHost(c->ovl_stage);
+  cudaFree(c->ovl_stage_dev);
   cudaFree(c->shard_buf);
   cudaFree(c->shard_page);
   cudaFree(c->lut);
@@ -457,6 +459,8 @@ int build_blockmax(r3d_cuda_ctx *c) {
     cudaFree(c->ovl_quad[i]);
     c->ovl_quad[i] = nullptr;
     c->br.ovl[i] = nullptr;
+    c->ovl_src_on[i] = false;  // a new cache detaches CPU-sourced atlases
+    c->ovl_key[i].clear();
   }
   const size_t nq = (size_t)(c->nslots ? c->nslots : 1u) * (128u * 128u * 128u);
   R3D_CUDA_TRY(c, cudaMalloc(&c->quad, nq * sizeof(uint32_t)));

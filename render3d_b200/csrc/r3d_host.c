@@ -533,6 +533,58 @@ uint32_t r3d_host_stream_point(const uint32_t *page, uint32_t page_words, const 
                     mark, out, cap, n);
 }
 
+/* ---- CPU-sourced slot-parallel atlases ---- */
+
+int r3d_host_brick_locate(const uint32_t *page, uint32_t b, uint32_t *level, uint32_t *bx,
+                          uint32_t *by, uint32_t *bz) {
+  if (!page) return -1;
+  const uint32_t nlev = page[0];
+  for (uint32_t l = 0; l < nlev && l < 15u; l++) {
+    const uint32_t off = page[4u + 4u * l], packed = page[5u + 4u * l];
+    const uint32_t dx = packed & 1023u, dy = (packed >> 10) & 1023u, dz = packed >> 20;
+    if (b < off || b - off >= dx * dy * dz) continue;
+    const uint32_t local = b - off;
+    *level = l;
+    *bx = local % dx;
+    *by = (local / dx) % dy;
+    *bz = local / (dx * dy);
+    return 0;
+  }
+  return -1;
+}
+
+uint32_t r3d_host_atlas_pick(const uint32_t *page, const uint32_t *slot_brick, uint32_t nslots,
+                             const uint64_t *keys, const r3d_brick_src *src, uint32_t budget,
+                             uint32_t *sel_slot, uint32_t *sel_brick, uint64_t *sel_key) {
+  if (!page || !slot_brick || !keys || !src || !src->gen) return 0;
+  if (!budget || budget > 16u) budget = 16u;
+  uint32_t n = 0;
+  /* stale slots first: a slot given to another brick still shows the old
+   * brick's content (vkbackend.c:4998-5020) */
+  for (uint32_t s = 0; s < nslots && n < budget; s++) {
+    const uint32_t b = slot_brick[s];
+    if (b == R3D_BRICK_ABSENT) continue;
+    const uint64_t key = keys[s];
+    if (key == 0 || (uint32_t)(key >> 32) == b + 1u) continue;
+    sel_slot[n] = s, sel_brick[n] = b, sel_key[n] = 0;
+    n++;
+  }
+  if (n) return n;
+  /* fill: content generations that changed (vkbackend.c:5022-5046) */
+  for (uint32_t s = 0; s < nslots && n < budget; s++) {
+    const uint32_t b = slot_brick[s];
+    if (b == R3D_BRICK_ABSENT) continue;
+    uint32_t l, bx, by, bz;
+    if (r3d_host_brick_locate(page, b, &l, &bx, &by, &bz) != 0) continue;
+    const uint32_t g = src->gen(src->user, l, bx, by, bz);
+    const uint64_t want = g ? (((uint64_t)b + 1u) << 32) | g : 0u;
+    if (keys[s] == want) continue;
+    sel_slot[n] = s, sel_brick[n] = b, sel_key[n] = want;
+    n++;
+  }
+  return n;
+}
+
 /* ---- virtual slab layout and fill planner ---- */
 
 static const uint32_t vs_scale[R3D_VS_LEVELS] = {1u, 4u, 8u, 16u, 32u};

@@ -27,6 +27,12 @@ struct r3d_cuda_ctx {
   uint8_t *bmax = nullptr;  // per-slot dilated 8^3 block maxima (4096 B/slot)
   uint32_t *quad = nullptr;  // per-slot quad words (DevBricks::quad)
   uint32_t *ovl_quad[4] = {nullptr, nullptr, nullptr, nullptr};  // overlay atlases
+  // CPU-sourced atlases: the attached source, each slot's content key and
+  // the staging slots (pinned host and device) of one sync round
+  r3d_brick_src ovl_src[4] = {};
+  bool ovl_src_on[4] = {false, false, false, false};
+  std::vector<uint64_t> ovl_key[4];
+  uint8_t *ovl_stage = nullptr, *ovl_stage_dev = nullptr;
   uint32_t page_words = 0;
   uint32_t nslots = 0;
   uint32_t abpa = 0;

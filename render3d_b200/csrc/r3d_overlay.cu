@@ -69,6 +69,7 @@ static int overlay_quads(r3d_cuda_ctx *c, uint32_t which, const uint8_t *pool) {
   cudaFree(c->ovl_quad[which]);
   c->ovl_quad[which] = q;
   c->br.ovl[which] = q;
+  if (c->ovl_src_on[which]) c->ovl_key[which].assign(c->nslots, UINT64_MAX);  // replaced content
   return R3D_OK;
 }
 
@@ -123,6 +124,95 @@ int r3d_cuda_bricks_overlay_load(r3d_cuda_ctx *c, uint32_t which, const uint8_t 
   int rc = e == cudaSuccess ? set_overlay(c, which, tmp, true) : cuda_fail(c, e, "bricks_overlay_load");
   cudaFree(tmp);
   return rc;
+}
+
+// ---- CPU-sourced atlases (vkbackend.c:4908-5150) ----
+
+static constexpr uint32_t kAtlasBatch = 16u, kSlotTexels = 128u * 128u * 128u;
+
+int r3d_cuda_bricks_atlas_attach(r3d_cuda_ctx *c, uint32_t which, const r3d_brick_src *src) {
+  if (!c || which > 3u || !src || !src->gen || !src->fetch)
+    return fail(c, R3D_E_INVALID, "bricks_atlas_attach: atlas 0..3 and a gen and fetch callback");
+  if (!c->have_bricks) return fail(c, R3D_E_STATE, "bricks_atlas_attach: no brick cache");
+  cudaSetDevice(c->device);
+  R3D_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  if (!c->ovl_stage) {
+    R3D_CUDA_TRY(c, cudaMallocHost(&c->ovl_stage, (size_t)kAtlasBatch * kSlotTexels));
+    R3D_CUDA_TRY(c, cudaMalloc(&c->ovl_stage_dev, (size_t)kAtlasBatch * kSlotTexels));
+  }
+  uint64_t key0 = UINT64_MAX;  // content of unknown bricks: zeroed first
+  if (!c->ovl_quad[which]) {   // a cleared atlas
+    const size_t n = (size_t)(c->nslots ? c->nslots : 1u) * kSlotTexels;
+    uint32_t *q = nullptr;
+    R3D_CUDA_TRY(c, cudaMalloc(&q, n * sizeof(uint32_t)));
+    cudaError_t e = cudaMemsetAsync(q, 0, n * sizeof(uint32_t), c->stream);
+    if (e != cudaSuccess) {
+      cudaFree(q);
+      return cuda_fail(c, e, "bricks_atlas_attach");
+    }
+    c->ovl_quad[which] = q;
+    c->br.ovl[which] = q;
+    key0 = 0;
+  }
+  c->ovl_key[which].assign(c->nslots, key0);
+  c->ovl_src[which] = *src;
+  c->ovl_src_on[which] = true;
+  return R3D_OK;
+}
+
+int r3d_cuda_bricks_atlas_detach(r3d_cuda_ctx *c, uint32_t which) {
+  if (!c || which > 3u) return fail(c, R3D_E_INVALID, "bricks_atlas_detach: atlas 0..3");
+  c->ovl_src_on[which] = false;  // the atlas and its keys stay for a re-attach
+  c->ovl_src[which] = r3d_brick_src{};
+  return R3D_OK;
+}
+
+int r3d_cuda_bricks_atlas_sync(r3d_cuda_ctx *c, uint32_t which, uint32_t budget, uint32_t *synced) {
+  if (synced) *synced = 0;
+  if (!c || which > 3u) return fail(c, R3D_E_INVALID, "bricks_atlas_sync: atlas 0..3");
+  if (!c->ovl_src_on[which] || !c->have_bricks) return R3D_OK;
+  cudaSetDevice(c->device);
+  // which brick each slot holds: the pump's table, or the page table of a
+  // resident cache
+  std::vector<uint32_t> page, sb;
+  const uint32_t *hpage, *slot_brick;
+  if (c->streaming) {
+    hpage = c->store_page.data();
+    slot_brick = c->slot_brick.data();
+  } else {
+    page.resize(c->page_words);
+    R3D_CUDA_TRY(c, copy_sync(c->stream, page.data(), c->page, page.size() * 4u));
+    sb.assign(c->nslots, R3D_BRICK_ABSENT);
+    for (uint32_t b = R3D_BRICK_PAGE_HEADER; b < c->page_words; b++)
+      if (page[b] != R3D_BRICK_ABSENT && (page[b] & 0xFFFFFFu) < c->nslots) sb[page[b] & 0xFFFFFFu] = b;
+    hpage = page.data();
+    slot_brick = sb.data();
+  }
+  uint32_t sel[kAtlasBatch], selb[kAtlasBatch];
+  uint64_t key[kAtlasBatch];
+  const uint32_t n = r3d_host_atlas_pick(hpage, slot_brick, c->nslots, c->ovl_key[which].data(),
+                                         &c->ovl_src[which], budget, sel, selb, key);
+  if (!n) return R3D_OK;
+  // the staging slots of the previous round are free once the stream is
+  R3D_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  for (uint32_t i = 0; i < n; i++) {
+    uint8_t *dst = c->ovl_stage + (size_t)i * kSlotTexels;
+    uint32_t l, bx, by, bz;
+    if (key[i] && r3d_host_brick_locate(hpage, selb[i], &l, &bx, &by, &bz) == 0)
+      c->ovl_src[which].fetch(c->ovl_src[which].user, l, bx, by, bz, dst);
+    else
+      memset(dst, 0, kSlotTexels);
+  }
+  R3D_CUDA_TRY(c, cudaMemcpyAsync(c->ovl_stage_dev, c->ovl_stage, (size_t)n * kSlotTexels,
+                                  cudaMemcpyHostToDevice, c->stream));
+  for (uint32_t i = 0; i < n; i++)  // that slot's overlay words
+    k_slot_quads<<<ovl_grid(kSlotTexels), 256, 0, c->stream>>>(
+        c->ovl_stage_dev + (size_t)i * kSlotTexels, c->ovl_quad[which] + (size_t)sel[i] * kSlotTexels,
+        kSlotTexels);
+  R3D_CUDA_TRY(c, cudaGetLastError());
+  for (uint32_t i = 0; i < n; i++) c->ovl_key[which][sel[i]] = key[i];
+  if (synced) *synced = n;
+  return R3D_OK;
 }
 
 int r3d_cuda_bricks_overlay_read(r3d_cuda_ctx *c, uint32_t which, uint8_t *slots) {

@@ -456,6 +456,44 @@ void r3d_bricks_flush(r3d_renderer *r) {
   if (r) cudaStreamSynchronize((cudaStream_t)r3d_cuda_stream(r->ctx));
 }
 
+/* ---- CPU-sourced atlases: labels (2), registration (3) ---- */
+
+static int atlas_attach(r3d_renderer *r, uint32_t which, const r3d_label_src *src,
+                        const char *what) {
+  if (!r || !r->bricks || !src || !src->gen || !src->fetch) return -1;
+  const r3d_brick_src s = {src->gen, src->fetch, src->user};
+  int rc = report(r, what, r3d_cuda_bricks_atlas_attach(r->ctx, which, &s));
+  if (rc == 0) r->ovl_loaded |= 1u << which;
+  return rc;
+}
+
+int r3d_bricks_labels(r3d_renderer *r, const r3d_label_src *src) {
+  return atlas_attach(r, 2u, src, "bricks_labels");
+}
+
+void r3d_bricks_labels_sync(r3d_renderer *r, uint32_t budget) {
+  if (r) report(r, "bricks_labels_sync", r3d_cuda_bricks_atlas_sync(r->ctx, 2u, budget, NULL));
+}
+
+int r3d_bricks_regatlas(r3d_renderer *r, const r3d_label_src *src) {
+  return atlas_attach(r, 3u, src, "bricks_regatlas");
+}
+
+/* the reference syncs the registration atlas on a worker thread and this
+ * call only observes it; here the round runs within the call (the
+ * reference's own fallback when the worker is missing) */
+void r3d_bricks_regatlas_sync(r3d_renderer *r, uint32_t budget) {
+  if (!r) return;
+  uint32_t n = 0;
+  if (report(r, "bricks_regatlas_sync", r3d_cuda_bricks_atlas_sync(r->ctx, 3u, budget, &n)) == 0 &&
+      n && r->sv_pick == 3)
+    r3d_surfvol_mark(r); /* the flattened bake taps this atlas */
+}
+
+void r3d_bricks_regatlas_detach(r3d_renderer *r) {
+  if (r) r3d_cuda_bricks_atlas_detach(r->ctx, 3u);
+}
+
 void r3d_bricks_postfilter(r3d_renderer *r, uint32_t mode, float amount, uint32_t targets) {
   if (r) report(r, "bricks_postfilter", r3d_cuda_bricks_postfilter(r->ctx, mode, amount, targets));
 }
