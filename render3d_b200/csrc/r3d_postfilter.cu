@@ -17,9 +17,9 @@
 // gathered from shared memory as packed bytes (two aligned words and a
 // funnel shift per row), so the medians are exact rank selections done
 // four bytes at a time: eight rounds of a bit-serial search, each counting
-// the bytes below a candidate with __vsetltu4.  Max pools fold the same
-// words with __vmaxu4.  Results are bit-identical to the shader's sort /
-// histogram formulation for bytes, which the oracle restates directly.
+// the bytes below a candidate with __vsetltu4.  Max pools are separable
+// (k_maxpool).  Results are bit-identical to the shader's sort / histogram
+// formulation for bytes, which the oracle restates directly.
 #include <string.h>
 
 #include "r3d_internal.h"
@@ -29,13 +29,49 @@ namespace r3d {
 constexpr uint32_t kSlot = 128u, kSlotBytes = kSlot * kSlot * kSlot;
 constexpr uint32_t kPfWave = 64u;            // slots per launch (scratch of 128 MiB)
 constexpr int kTX = 32, kTY = 8, kTZ = 8;    // output tile
-constexpr int kRowBytes = 36;                // 32 + 2 * 2 halo, a multiple of 4
+constexpr int kRowWords = 10;                // a halo row: slot x0 - 4 .. x0 + 35
+constexpr int kRowBytes = 4 * kRowWords;
 
-enum PfOp { kMedian = 0, kMax = 1, kSharpen = 2 };
+enum PfOp { kMedian = 0, kSharpen = 1 };
 
 struct PfJobs {
   uint32_t src[kPfWave], dst[kPfWave];  // slot index of each job (in src / dst buffers)
 };
+
+// Stages the tile's halo rows (z0 - R .. z0 + 8 + R, y likewise) as aligned
+// words of slot x x0 - 4 .. x0 + 35, the slot clamp applied: clamped y and
+// z rows, and at the x edges the edge byte repeated through the word
+// outside the slot.  Output x of the tile sits at row byte x + 4.
+template <int R>
+__device__ __forceinline__ void load_tile(uint8_t (*t)[kTY + 2 * R][kRowBytes], const uint8_t *s,
+                                          uint32_t x0, uint32_t y0, uint32_t z0) {
+  constexpr int TY = kTY + 2 * R, TZ = kTZ + 2 * R, kWords = TZ * TY * kRowWords;
+  constexpr int kIters = (kWords + 255) / 256;  // blocks of 256 threads
+  uint32_t w[kIters];
+  // every load in flight before the first shared store
+#pragma unroll
+  for (int it = 0; it < kIters; it++) {
+    const uint32_t i = threadIdx.x + 256u * it;
+    if (i >= (uint32_t)kWords) break;
+    const uint32_t row = i / kRowWords, wi = i % kRowWords;
+    const int ly = (int)(row % TY), lz = (int)(row / TY);
+    const int gy = min(max((int)y0 + ly - R, 0), 127), gz = min(max((int)z0 + lz - R, 0), 127);
+    const int gw = (int)(x0 >> 2) - 1 + (int)wi;  // -1 .. 32
+    const uint32_t *g = reinterpret_cast<const uint32_t *>(s + ((size_t)gz * kSlot + gy) * kSlot);
+    w[it] = __ldg(g + min(max(gw, 0), 31));
+  }
+#pragma unroll
+  for (int it = 0; it < kIters; it++) {
+    const uint32_t i = threadIdx.x + 256u * it;
+    if (i >= (uint32_t)kWords) break;
+    const uint32_t row = i / kRowWords, wi = i % kRowWords;
+    const int gw = (int)(x0 >> 2) - 1 + (int)wi;
+    uint32_t v = w[it];
+    if (gw < 0) v = (v & 0xFFu) * 0x01010101u;
+    if (gw > 31) v = (v >> 24) * 0x01010101u;
+    reinterpret_cast<uint32_t *>(&t[row / TY][row % TY][0])[wi] = v;
+  }
+}
 
 // the rank-th smallest byte (0-based) of the bytes packed in w (pad bytes
 // 0xFF are never counted below a candidate)
@@ -53,16 +89,6 @@ __device__ __forceinline__ uint32_t rank_select(const uint32_t (&w)[NW], uint32_
   return res;
 }
 
-template <int NW>
-__device__ __forceinline__ uint32_t max_bytes(const uint32_t (&w)[NW]) {
-  uint32_t m = w[0];
-#pragma unroll
-  for (int i = 1; i < NW; i++) m = __vmaxu4(m, w[i]);
-  m = __vmaxu4(m, m >> 16);
-  m = __vmaxu4(m, m >> 8);
-  return m & 0xFFu;
-}
-
 template <int R, int OP>
 __global__ void __launch_bounds__(256) k_postfilter(const uint8_t *__restrict__ src,
                                                     uint8_t *__restrict__ dst,
@@ -74,20 +100,13 @@ __global__ void __launch_bounds__(256) k_postfilter(const uint8_t *__restrict__ 
   const uint32_t tid = threadIdx.x, j = blockIdx.y;
   const uint32_t x0 = (blockIdx.x & 3u) * kTX, y0 = ((blockIdx.x >> 2) & 15u) * kTY,
                  z0 = (blockIdx.x >> 6) * kTZ;
-  const uint8_t *s = src + (size_t)jobs.src[j] * kSlotBytes;
-  // halo rows, the slot clamp applied here (columns past the 32 + 2R used
-  // ones are clamped copies too, so every byte read below is initialized)
-  for (uint32_t i = tid; i < (uint32_t)(TZ * TY * kRowBytes); i += 256u) {
-    const int lx = (int)(i % kRowBytes), ly = (int)((i / kRowBytes) % TY), lz = (int)(i / (kRowBytes * TY));
-    const int gx = min(max((int)x0 + lx - R, 0), 127), gy = min(max((int)y0 + ly - R, 0), 127),
-              gz = min(max((int)z0 + lz - R, 0), 127);
-    t[lz][ly][lx] = __ldg(s + ((size_t)gz * kSlot + gy) * kSlot + gx);
-  }
+  load_tile<R>(t, src + (size_t)jobs.src[j] * kSlotBytes, x0, y0, z0);
   if (OP == kSharpen) lut[tid] = (float)tid / 255.0f;  // texelFetch of an R8 texel
   __syncthreads();
   const uint32_t x = tid & 31u, y = tid >> 5;
   uint8_t *d = dst + (size_t)jobs.dst[j] * kSlotBytes + ((size_t)z0 * kSlot + y0 + y) * kSlot + x0 + x;
-  const uint32_t xa = x & ~3u, sh = 8u * (x & 3u);
+  // the window of output x starts at row byte x + 4 - R
+  const uint32_t xb = x + 4u - (uint32_t)R, xa = xb & ~3u, sh = 8u * (xb & 3u);
 #pragma unroll 1
   for (int z = 0; z < kTZ; z++) {
     uint32_t out;
@@ -95,8 +114,8 @@ __global__ void __launch_bounds__(256) k_postfilter(const uint8_t *__restrict__ 
       float sum = 0.0f;
       for (int dz = 0; dz < 3; dz++)
         for (int dy = 0; dy < 3; dy++)
-          for (int dx = 0; dx < 3; dx++) sum += lut[t[z + dz][y + dy][x + dx]];
-      const float center = lut[t[z + 1][y + 1][x + 1]];
+          for (int dx = 0; dx < 3; dx++) sum += lut[t[z + dz][y + dy][xb + dx]];
+      const float center = lut[t[z + 1][y + 1][xb + 1]];
       const float v = fminf(fmaxf(center + amount * (center - sum / 27.0f), 0.0f), 1.0f);
       out = (uint32_t)(int)fmaf(v, 255.0f, 0.5f);
     } else if (R == 1) {
@@ -106,9 +125,9 @@ __global__ void __launch_bounds__(256) k_postfilter(const uint8_t *__restrict__ 
       for (int r = 0; r < 9; r++) {
         const uint32_t *row = reinterpret_cast<const uint32_t *>(&t[z + r / 3][y + r % 3][xa]);
         const uint32_t a = __funnelshift_r(row[0], row[1], sh);
-        w[r] = OP == kMedian ? (a | 0xFF000000u) : (a & 0x00FFFFFFu);
+        w[r] = a | 0xFF000000u;
       }
-      out = OP == kMedian ? rank_select<9>(w, 13u) : max_bytes<9>(w);
+      out = rank_select<9>(w, 13u);
     } else {
       // 25 rows of 5 bytes: the first four of each row in one word, the
       // fifth bytes packed four to a word (7 words, 3 pad bytes)
@@ -120,17 +139,66 @@ __global__ void __launch_bounds__(256) k_postfilter(const uint8_t *__restrict__ 
         w[r] = __funnelshift_r(r0, r1, sh);
         const uint32_t fifth = (r1 >> sh) & 0xFFu;
         if (r % 4 == 0)
-          w[25 + r / 4] = fifth | (OP == kMedian ? 0xFFFFFF00u : 0u);
+          w[25 + r / 4] = fifth | 0xFFFFFF00u;
         else
           w[25 + r / 4] = (w[25 + r / 4] & ~(0xFFu << (8 * (r % 4)))) | (fifth << (8 * (r % 4)));
       }
-      out = OP == kMedian ? rank_select<32>(w, 62u) : max_bytes<32>(w);
+      out = rank_select<32>(w, 62u);
     }
     d[(size_t)z * kSlot * kSlot] = (uint8_t)out;
   }
 }
 
+// Max pools, separable: the window is a box and the slot clamp acts per
+// axis, so the max of the box is the max over z of the max over y of the
+// max over x.  Three passes through shared memory, four bytes a word: x
+// (halo rows -> 32-wide rows), y, then z straight to the slot.
+template <int R>
+__global__ void __launch_bounds__(256) k_maxpool(const uint8_t *__restrict__ src,
+                                                 uint8_t *__restrict__ dst,
+                                                 const __grid_constant__ PfJobs jobs, float) {
+  constexpr int TY = kTY + 2 * R, TZ = kTZ + 2 * R;
+  __shared__ __align__(16) uint8_t t[TZ][TY][kRowBytes];
+  __shared__ __align__(16) uint32_t mx[TZ][TY][kTX / 4];  // max over x
+  __shared__ __align__(16) uint32_t my[TZ][kTY][kTX / 4];  // then over y
+  const uint32_t tid = threadIdx.x, j = blockIdx.y;
+  const uint32_t x0 = (blockIdx.x & 3u) * kTX, y0 = ((blockIdx.x >> 2) & 15u) * kTY,
+                 z0 = (blockIdx.x >> 6) * kTZ;
+  load_tile<R>(t, src + (size_t)jobs.src[j] * kSlotBytes, x0, y0, z0);
+  __syncthreads();
+  // x: the 4 outputs of word g sit in row word g + 1; their windows reach R
+  // bytes into words g and g + 2
+  for (uint32_t i = tid; i < (uint32_t)(TZ * TY * (kTX / 4)); i += 256u) {
+    const uint32_t g = i % (kTX / 4), ly = (i / (kTX / 4)) % TY, lz = i / ((kTX / 4) * TY);
+    const uint32_t *row = reinterpret_cast<const uint32_t *>(&t[lz][ly][0]);
+    const uint32_t w0 = row[g], w1 = row[g + 1], w2 = row[g + 2];
+    uint32_t m = w1;
+#pragma unroll
+    for (int k = 1; k <= R; k++)
+      m = __vmaxu4(m, __vmaxu4(__funnelshift_r(w0, w1, 32 - 8 * k), __funnelshift_r(w1, w2, 8 * k)));
+    mx[lz][ly][g] = m;
+  }
+  __syncthreads();
+  for (uint32_t i = tid; i < (uint32_t)(TZ * kTY * (kTX / 4)); i += 256u) {
+    const uint32_t g = i % (kTX / 4), y = (i / (kTX / 4)) % kTY, lz = i / ((kTX / 4) * kTY);
+    uint32_t m = mx[lz][y][g];
+#pragma unroll
+    for (int k = 1; k <= 2 * R; k++) m = __vmaxu4(m, mx[lz][y + k][g]);
+    my[lz][y][g] = m;
+  }
+  __syncthreads();
+  uint8_t *d = dst + (size_t)jobs.dst[j] * kSlotBytes;
+  for (uint32_t i = tid; i < (uint32_t)(kTZ * kTY * (kTX / 4)); i += 256u) {
+    const uint32_t g = i % (kTX / 4), y = (i / (kTX / 4)) % kTY, z = i / ((kTX / 4) * kTY);
+    uint32_t m = my[z][y][g];
+#pragma unroll
+    for (int k = 1; k <= 2 * R; k++) m = __vmaxu4(m, my[z + k][y][g]);
+    *reinterpret_cast<uint32_t *>(d + ((size_t)(z0 + z) * kSlot + y0 + y) * kSlot + x0 + 4u * g) = m;
+  }
+}
+
 using PfKernel = void (*)(const uint8_t *, uint8_t *, const PfJobs, float);
+
 
 // the kernel of a primary filter id (1 median 3^3, 2 median 5^3, 3 max 3^3,
 // 4 max 5^3), or null
@@ -138,8 +206,8 @@ static PfKernel primary_kernel(uint32_t prim) {
   switch (prim) {
     case 1: return k_postfilter<1, kMedian>;
     case 2: return k_postfilter<2, kMedian>;
-    case 3: return k_postfilter<1, kMax>;
-    case 4: return k_postfilter<2, kMax>;
+    case 3: return k_maxpool<1>;
+    case 4: return k_maxpool<2>;
     default: return nullptr;
   }
 }
