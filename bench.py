@@ -693,6 +693,44 @@ def run_profile_sections(args) -> None:
     print("profile section frames done:", n, "surf pitch 0.5 bake ms", s["pitch_0.5"]["bake_ms"])
 
 
+def run_profile_filter(args) -> None:
+    """The post-decode display filter: a streamed 512^3 cache with every
+    brick resident (73 slots, 3 levels), re-filtered args.profile_filter
+    times in each mode (the 72 non-coarsest slots copied in again from the
+    host store, then filtered).  Prints CUDA-event times on the context's
+    stream per refilter and the filter's share per slot (beyond the
+    unfiltered re-upload); the command line that ncu captures."""
+    import torch
+    import render3d_b200 as rb
+    lut = rb.scroll_ramp_tf()
+    vol = rb.phantom(512, seed=SEED)
+    ctx = rb.Context(0)
+    ctx.stream_begin(vol, 3, 73)
+    p = rb.camera_view(0.5, -0.4, 0.9, W, H, lut, step_voxels=STEP_VOXELS)
+    for _ in range(30):
+        st = ctx.stream_update(p, 64)
+    assert st["resident"] == 73
+    ev = torch.cuda.ExternalStream(ctx.stream)
+    out = {}
+    for mode in (0, 1, 2, 3, 4, 0x100, 0x101):
+        ctx.bricks_postfilter(mode, 1.0)
+        ctx.bricks_refilter()  # warm
+        times = []
+        for _ in range(args.profile_filter):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(ev)
+            ctx.bricks_refilter()
+            b.record(ev)
+            b.synchronize()
+            times.append(a.elapsed_time(b))
+        out[mode] = min(times)
+    base = out[0]
+    res = {f"{m:#x}": {"ms_per_refilter": round(t, 4),
+                       "filter_us_per_slot": round((t - base) * 1e3 / 72, 2)} for m, t in out.items()}
+    print(json.dumps({"profile_filter": res, "slots": 72, "reps": args.profile_filter}))
+    ctx.close()
+
+
 def run_profile(args) -> None:
     """Renders args.profile frames of the workload with no timing: the
     command line that ncu captures."""
@@ -1092,6 +1130,8 @@ def main() -> None:
                     help="only render N frames of each section mode and of flattened views")
     ap.add_argument("--profile-diff", type=int, default=0, metavar="N",
                     help="only run N forward+backward steps of the differentiable workload")
+    ap.add_argument("--profile-filter", type=int, default=0, metavar="N",
+                    help="only re-filter a streamed 512^3 cache N times in each display filter")
     ap.add_argument("--profile-size", type=int, default=N_EDGE)
     args = ap.parse_args()
     if args.profile:
@@ -1099,6 +1139,9 @@ def main() -> None:
         return
     if args.profile_sections:
         run_profile_sections(args)
+        return
+    if args.profile_filter:
+        run_profile_filter(args)
         return
     if args.profile_diff:
         import torch
