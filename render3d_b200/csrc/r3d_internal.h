@@ -225,11 +225,12 @@ int build_blockmax(r3d_cuda_ctx *c);
 // Drops the streaming state (host store, shadows, LRU).
 void stream_reset(r3d_cuda_ctx *c);
 // The display filter: whether it changes target t (0 CT, 1 ink atlas, 2 3D
-// ink atlas), and filtering n slots of a 128^3-slot pool in place, on the
-// context's stream.
+// ink atlas), and filtering n slots in place on the context's stream, of a
+// linear pool of 128^3 slots (atlas_bpa 0) or of a single-level atlas of
+// atlas_bpa^3 slots.
 bool postfilter_on(const r3d_cuda_ctx *c, uint32_t target);
 int postfilter_slots(r3d_cuda_ctx *c, uint32_t target, uint8_t *pool, const uint32_t *slots,
-                     uint32_t n);
+                     uint32_t n, uint32_t atlas_bpa = 0u);
 void postfilter_reset(r3d_cuda_ctx *c);
 // Frees the tiled slab / the clipmap.
 void slab_reset(r3d_cuda_ctx *c);

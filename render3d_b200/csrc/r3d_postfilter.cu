@@ -34,17 +34,35 @@ constexpr int kRowBytes = 4 * kRowWords;
 
 enum PfOp { kMedian = 0, kSharpen = 1 };
 
+struct PfLayout {
+  uint32_t abpa;  // 0: a linear pool; else an atlas of abpa^3 slots
+};
+
 struct PfJobs {
   uint32_t src[kPfWave], dst[kPfWave];  // slot index of each job (in src / dst buffers)
+  PfLayout src_l, dst_l;
 };
+
+// Texel (x, y, z) of slot s: a linear pool (abpa 0: slot s at s * 128^3, x
+// fastest) or a single-level atlas of abpa^3 slots ((abpa * 128)^3 texels,
+// slot s at (s mod abpa, s / abpa mod abpa, s / abpa^2) * 128).
+__device__ __forceinline__ size_t slot_texel(const PfLayout &l, uint32_t s, uint32_t x, uint32_t y,
+                                             uint32_t z) {
+  if (!l.abpa) return (size_t)s * kSlotBytes + ((size_t)z * kSlot + y) * kSlot + x;
+  const size_t a = (size_t)l.abpa * kSlot;
+  const size_t sx = (s % l.abpa) * kSlot, sy = ((s / l.abpa) % l.abpa) * kSlot,
+               sz = (s / (l.abpa * l.abpa)) * kSlot;
+  return ((sz + z) * a + sy + y) * a + sx + x;
+}
 
 // Stages the tile's halo rows (z0 - R .. z0 + 8 + R, y likewise) as aligned
 // words of slot x x0 - 4 .. x0 + 35, the slot clamp applied: clamped y and
 // z rows, and at the x edges the edge byte repeated through the word
 // outside the slot.  Output x of the tile sits at row byte x + 4.
 template <int R>
-__device__ __forceinline__ void load_tile(uint8_t (*t)[kTY + 2 * R][kRowBytes], const uint8_t *s,
-                                          uint32_t x0, uint32_t y0, uint32_t z0) {
+__device__ __forceinline__ void load_tile(uint8_t (*t)[kTY + 2 * R][kRowBytes], const uint8_t *src,
+                                          const PfLayout &l, uint32_t slot, uint32_t x0, uint32_t y0,
+                                          uint32_t z0) {
   constexpr int TY = kTY + 2 * R, TZ = kTZ + 2 * R, kWords = TZ * TY * kRowWords;
   constexpr int kIters = (kWords + 255) / 256;  // blocks of 256 threads
   uint32_t w[kIters];
@@ -57,7 +75,7 @@ __device__ __forceinline__ void load_tile(uint8_t (*t)[kTY + 2 * R][kRowBytes], 
     const int ly = (int)(row % TY), lz = (int)(row / TY);
     const int gy = min(max((int)y0 + ly - R, 0), 127), gz = min(max((int)z0 + lz - R, 0), 127);
     const int gw = (int)(x0 >> 2) - 1 + (int)wi;  // -1 .. 32
-    const uint32_t *g = reinterpret_cast<const uint32_t *>(s + ((size_t)gz * kSlot + gy) * kSlot);
+    const uint32_t *g = reinterpret_cast<const uint32_t *>(src + slot_texel(l, slot, 0, gy, gz));
     w[it] = __ldg(g + min(max(gw, 0), 31));
   }
 #pragma unroll
@@ -100,11 +118,13 @@ __global__ void __launch_bounds__(256) k_postfilter(const uint8_t *__restrict__ 
   const uint32_t tid = threadIdx.x, j = blockIdx.y;
   const uint32_t x0 = (blockIdx.x & 3u) * kTX, y0 = ((blockIdx.x >> 2) & 15u) * kTY,
                  z0 = (blockIdx.x >> 6) * kTZ;
-  load_tile<R>(t, src + (size_t)jobs.src[j] * kSlotBytes, x0, y0, z0);
+  load_tile<R>(t, src, jobs.src_l, jobs.src[j], x0, y0, z0);
   if (OP == kSharpen) lut[tid] = (float)tid / 255.0f;  // texelFetch of an R8 texel
   __syncthreads();
   const uint32_t x = tid & 31u, y = tid >> 5;
-  uint8_t *d = dst + (size_t)jobs.dst[j] * kSlotBytes + ((size_t)z0 * kSlot + y0 + y) * kSlot + x0 + x;
+  uint8_t *d = dst + slot_texel(jobs.dst_l, jobs.dst[j], x0 + x, y0 + y, z0);
+  const size_t zstride = jobs.dst_l.abpa ? (size_t)jobs.dst_l.abpa * kSlot * jobs.dst_l.abpa * kSlot
+                                         : (size_t)kSlot * kSlot;
   // the window of output x starts at row byte x + 4 - R
   const uint32_t xb = x + 4u - (uint32_t)R, xa = xb & ~3u, sh = 8u * (xb & 3u);
 #pragma unroll 1
@@ -145,7 +165,7 @@ __global__ void __launch_bounds__(256) k_postfilter(const uint8_t *__restrict__ 
       }
       out = rank_select<32>(w, 62u);
     }
-    d[(size_t)z * kSlot * kSlot] = (uint8_t)out;
+    d[(size_t)z * zstride] = (uint8_t)out;
   }
 }
 
@@ -164,7 +184,7 @@ __global__ void __launch_bounds__(256) k_maxpool(const uint8_t *__restrict__ src
   const uint32_t tid = threadIdx.x, j = blockIdx.y;
   const uint32_t x0 = (blockIdx.x & 3u) * kTX, y0 = ((blockIdx.x >> 2) & 15u) * kTY,
                  z0 = (blockIdx.x >> 6) * kTZ;
-  load_tile<R>(t, src + (size_t)jobs.src[j] * kSlotBytes, x0, y0, z0);
+  load_tile<R>(t, src, jobs.src_l, jobs.src[j], x0, y0, z0);
   __syncthreads();
   // x: the 4 outputs of word g sit in row word g + 1; their windows reach R
   // bytes into words g and g + 2
@@ -187,17 +207,32 @@ __global__ void __launch_bounds__(256) k_maxpool(const uint8_t *__restrict__ src
     my[lz][y][g] = m;
   }
   __syncthreads();
-  uint8_t *d = dst + (size_t)jobs.dst[j] * kSlotBytes;
   for (uint32_t i = tid; i < (uint32_t)(kTZ * kTY * (kTX / 4)); i += 256u) {
     const uint32_t g = i % (kTX / 4), y = (i / (kTX / 4)) % kTY, z = i / ((kTX / 4) * kTY);
     uint32_t m = my[z][y][g];
 #pragma unroll
     for (int k = 1; k <= 2 * R; k++) m = __vmaxu4(m, my[z + k][y][g]);
-    *reinterpret_cast<uint32_t *>(d + ((size_t)(z0 + z) * kSlot + y0 + y) * kSlot + x0 + 4u * g) = m;
+    *reinterpret_cast<uint32_t *>(dst + slot_texel(jobs.dst_l, jobs.dst[j], x0 + 4u * g, y0 + y, z0 + z)) = m;
   }
 }
 
 using PfKernel = void (*)(const uint8_t *, uint8_t *, const PfJobs, float);
+
+// Slot copies between layouts, 16 bytes a thread (one CTA per 128 x 8 x 8
+// block of a slot).
+__global__ void __launch_bounds__(256) k_slot_copy(const uint8_t *__restrict__ src,
+                                                   uint8_t *__restrict__ dst,
+                                                   const __grid_constant__ PfJobs jobs) {
+  const uint32_t j = blockIdx.y, tid = threadIdx.x;
+  const uint32_t y0 = (blockIdx.x & 15u) * 8u, z0 = (blockIdx.x >> 4) * 8u;
+#pragma unroll
+  for (int it = 0; it < 2; it++) {
+    const uint32_t i = tid + 256u * it;  // 512 chunks of 16 bytes: 8 per row, 8 x 8 rows
+    const uint32_t x = (i & 7u) * 16u, y = y0 + ((i >> 3) & 7u), z = z0 + (i >> 6);
+    *reinterpret_cast<uint4 *>(dst + slot_texel(jobs.dst_l, jobs.dst[j], x, y, z)) =
+        *reinterpret_cast<const uint4 *>(src + slot_texel(jobs.src_l, jobs.src[j], x, y, z));
+  }
+}
 
 
 // the kernel of a primary filter id (1 median 3^3, 2 median 5^3, 3 max 3^3,
@@ -227,7 +262,7 @@ bool postfilter_on(const r3d_cuda_ctx *c, uint32_t target) {
 }
 
 int postfilter_slots(r3d_cuda_ctx *c, uint32_t target, uint8_t *pool, const uint32_t *slots,
-                     uint32_t n) {
+                     uint32_t n, uint32_t atlas_bpa) {
   if (!n || !postfilter_on(c, target)) return R3D_OK;
   const PfKernel prim = primary_kernel(c->pf_mode & 0xFFu);
   const bool sharpen = (c->pf_mode & 0x100u) != 0;
@@ -237,6 +272,8 @@ int postfilter_slots(r3d_cuda_ctx *c, uint32_t target, uint8_t *pool, const uint
   for (uint32_t w0 = 0; w0 < n; w0 += kPfWave) {
     const uint32_t wn = min(n - w0, kPfWave);
     PfJobs to_scratch, back;
+    to_scratch.src_l = back.dst_l = PfLayout{atlas_bpa};
+    to_scratch.dst_l = back.src_l = PfLayout{0u};
     for (uint32_t i = 0; i < wn; i++) {
       to_scratch.src[i] = back.dst[i] = slots[w0 + i];
       to_scratch.dst[i] = back.src[i] = i;
@@ -251,11 +288,8 @@ int postfilter_slots(r3d_cuda_ctx *c, uint32_t target, uint8_t *pool, const uint
                                                    prim ? pool : c->pf_scratch,
                                                    prim ? back : to_scratch, c->pf_amount);
     R3D_CUDA_TRY(c, cudaGetLastError());
-    if (!(prim && sharpen))
-      for (uint32_t i = 0; i < wn; i++)
-        R3D_CUDA_TRY(c, cudaMemcpyAsync(pool + (size_t)slots[w0 + i] * kSlotBytes,
-                                        c->pf_scratch + (size_t)i * kSlotBytes, kSlotBytes,
-                                        cudaMemcpyDeviceToDevice, st));
+    if (!(prim && sharpen)) k_slot_copy<<<dim3(16u * 16u, wn), 256, 0, st>>>(c->pf_scratch, pool, back);
+    R3D_CUDA_TRY(c, cudaGetLastError());
   }
   return R3D_OK;
 }

@@ -153,6 +153,24 @@ int r3d_cuda_shard_build(r3d_cuda_ctx *c, uint32_t edge, const uint8_t *voxels, 
   if (e == cudaSuccess) {
     k_shard_place<<<shard_grid((size_t)a * a * a / 16u), 256, 0, c->stream>>>(vol, edge, bpa,
                                                                              dbrick, abpa, buf);
+    // the display filter on the placed slots, before the mips and the
+    // occupancy derived from them (page maxima stay the source bricks')
+    if (postfilter_on(c, 0u)) {
+      std::vector<uint32_t> used;
+      for (uint32_t s = 0; s < ns; s++)
+        if (brick[s] != R3D_BRICK_ABSENT) used.push_back(s);
+      const int frc = postfilter_slots(c, 0u, buf, used.data(), (uint32_t)used.size(), abpa);
+      if (frc != R3D_OK) {
+        cudaStreamSynchronize(c->stream);
+        cudaFree(vtmp);
+        cudaFree(dslot);
+        cudaFree(dbrick);
+        cudaFree(dmax);
+        cudaFree(dpage);
+        cudaFree(buf);
+        return frc;
+      }
+    }
     k_brick_max<<<nb, 256, 0, c->stream>>>(vol, edge, edge, edge, bpa, bpa, dmax);
     for (uint32_t m = 1; m < 4u; m++) {
       const uint32_t s = a >> (m - 1), d = a >> m;

@@ -159,3 +159,37 @@ def test_render_level_calls(rb, noisy, scroll_tf):
     finally:
         c.close()
         r.close()
+
+
+@pytest.mark.parametrize("mode", [4, 0x101])
+@pytest.mark.parametrize("slot_of", [None, [3, ABSENT, 5, 1, 0, 7, 2, 6]])
+def test_shard_atlas(rb, orc, noisy, scroll_tf, mode, slot_of):
+    """A single-level shard atlas filters its placed slots before the mips
+    and the occupancy derived from them; page maxima stay the bricks'."""
+    c = rb.Context(0)
+    try:
+        c.set_transfer(scroll_tf)
+        c.set_alpha_cutoff(0.98)
+        c.shard_build(noisy, 2, slot_of)
+        page0, a0 = c.shard_read(0)
+        c.bricks_postfilter(mode, 1.0)
+        c.shard_build(noisy, 2, slot_of)
+        want0 = a0.copy()
+        used = range(8) if slot_of is None else [s for s in slot_of if s != ABSENT]
+        for s in used:
+            sx, sy, sz = (s % 2) * 128, ((s // 2) % 2) * 128, (s // 4) * 128
+            box = (slice(sz, sz + 128), slice(sy, sy + 128), slice(sx, sx + 128))
+            want0[box] = orc.postfilter(a0[box], mode, 1.0)[0]
+        assert not np.array_equal(want0, a0)
+        sc = orc.ShardScene(page0, want0, 2, 2)
+        for m in range(4):
+            page, lv = c.shard_read(m)
+            assert np.array_equal(page, page0)
+            assert np.array_equal(lv, sc.levels[m]), f"mip {m}"
+        assert np.array_equal(c.shard_read(-1)[1], sc.occ)
+        p = elev35(rb, scroll_tf, 256, 192, step_voxels=0.5)
+        p.brick_mode = c.shard_mode
+        ref = orc.render(p, sc, scroll_tf, 256, 192)[0]
+        _cmp(c.raycast(p, 256, 192), ref, f"shard mode {mode:#x}")
+    finally:
+        c.close()
