@@ -193,3 +193,23 @@ def test_shard_atlas(rb, orc, noisy, scroll_tf, mode, slot_of):
         _cmp(c.raycast(p, 256, 192), ref, f"shard mode {mode:#x}")
     finally:
         c.close()
+
+
+def test_targets_together(rb, orc, noisy, plain):
+    """Targets 1 | 2: the CT bricks and the ink atlas both filtered; the
+    3D ink atlas not."""
+    ink = np.roll(noisy, 5, axis=0)
+    c = rb.Context(0)
+    try:
+        c.bricks_build(noisy, 2)
+        c.overlay_build(0, ink)
+        o0 = c.overlay_read(0)
+        c.bricks_postfilter(3, 0.0, targets=3)
+        c.bricks_build(noisy, 2)
+        c.overlay_build(0, ink)
+        c.overlay_build(1, ink)
+        assert np.array_equal(c.bricks_read()[1].reshape(plain[1].shape), orc.postfilter(plain[1], 3))
+        assert np.array_equal(c.overlay_read(0), orc.postfilter(o0, 3))
+        assert np.array_equal(c.overlay_read(1), o0)
+    finally:
+        c.close()

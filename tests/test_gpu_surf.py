@@ -180,3 +180,27 @@ def test_surf_inkpred_bit_exact(rb, orc, surf):
     c.surfvol_window(2.0, 3.0, 1.0, 0.0)
     sc.bake(2.0, 3.0, 1.0, 0.0, 0)
     assert np.array_equal(c.surfvol_read(), sc.vol)
+
+
+def test_surf_inkpred_edges(rb, orc, surf):
+    """A 1 x 1 prediction (bilinear and clamp both degenerate), one that
+    lies outside the window, and NaN probabilities (never >= 0: the overlay
+    byte stays); bad arguments are rejected."""
+    c, sc = surf
+    c.surfvol_overlay(0)
+    cases = [(np.full((1, 1), 0.7, np.float32), 20.0, 20.0, 10.0),
+             (np.full((4, 4), 0.9, np.float32), 500.0, 500.0, 1.0),
+             (np.where(np.arange(64).reshape(8, 8) % 3 == 0, np.nan, 0.3).astype(np.float32),
+              8.0, 9.0, 0.5)]
+    try:
+        for pred, g0u, g0v, ppg in cases:
+            c.surfvol_inkpred(pred, g0u, g0v, ppg)
+            c.surfvol_window(2.0, 3.0, 1.0, 0.0)
+            sc.inkpred(pred, g0u, g0v, ppg)
+            sc.bake(2.0, 3.0, 1.0, 0.0, 0)
+            assert np.array_equal(c.surfvol_read(), sc.vol), (pred.shape, g0u)
+        with pytest.raises(rb.R3DError):
+            c.surfvol_inkpred(np.ones((2, 2), np.float32), 0.0, 0.0, 0.0)  # no texel pitch
+    finally:
+        c.surfvol_inkpred(None)
+        sc.inkpred(None, 0, 0, 0)
