@@ -8,10 +8,10 @@
 
 // Minimum resident 128-thread blocks per SM the register allocator targets
 // (0: no target).  The plain LOD-brick kernels (no overlay atlases, counters
-// or parked shading, not the step heatmap) get one block more, with no
-// spills: at 64 registers they run 1-2 % faster
-// (1080p FULL and MIP), while the overlay and shard kernels lose 14 % and
-// 4 % and the heatmap 3 % at that bound.
+// or parked shading, not the step heatmap) get one block more, MIP two, all
+// without spills: 1080p FULL runs 2 % faster at 64 registers and MIP 5 %
+// at 56, while the overlay and shard kernels lose 14 % and 4 % and the
+// heatmap 3 % at 8 blocks, and FULL spills at 9.
 #ifndef R3D_FWD_MIN_BLOCKS
 #define R3D_FWD_MIN_BLOCKS 7
 #endif
@@ -23,7 +23,9 @@
 #define R3D_FWD_BOUNDS                                                                     \
   __launch_bounds__(R3D_FWD_WARPS * 32,                                                    \
                     R3D_FWD_MIN_BLOCKS + (PATH == PATH_LOD_BRICKS && !OVL && !COUNT &&     \
-                                          !DEFER && MODE != R3D_MODE_HEATMAP ? 1 : 0))
+                                                  !DEFER && MODE != R3D_MODE_HEATMAP             \
+                                              ? (MODE == R3D_MODE_MIP ? 2 : 1)                   \
+                                              : 0))
 #else
 #define R3D_FWD_BOUNDS __launch_bounds__(R3D_FWD_WARPS * 32)
 #endif
