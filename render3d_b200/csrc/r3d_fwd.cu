@@ -22,10 +22,10 @@
 #if R3D_FWD_MIN_BLOCKS > 0
 #define R3D_FWD_BOUNDS                                                                     \
   __launch_bounds__(R3D_FWD_WARPS * 32,                                                    \
-                    R3D_FWD_MIN_BLOCKS + (PATH == PATH_LOD_BRICKS && !OVL && !COUNT &&     \
-                                                  !DEFER && MODE != R3D_MODE_HEATMAP             \
-                                              ? (MODE == R3D_MODE_MIP ? 2 : 1)                   \
-                                              : 0))
+                    (R3D_FWD_MIN_BLOCKS + (PATH == PATH_LOD_BRICKS && !OVL && !COUNT &&    \
+                                                   !DEFER && MODE != R3D_MODE_HEATMAP            \
+                                               ? (MODE == R3D_MODE_MIP ? 2 : 1)                  \
+                                               : 0)) * 4 / R3D_FWD_WARPS)
 #else
 #define R3D_FWD_BOUNDS __launch_bounds__(R3D_FWD_WARPS * 32)
 #endif
