@@ -433,53 +433,92 @@ def batch_bench(rb, torch, local: int, ctx, reps: int) -> dict:
     return out
 
 
-def cpu_baseline(rb, orc, vol_pages, lut, frames: list[int], threads: int) -> dict:
+def cpu_baseline(rb, orc, ctx, vol_pages, lut, frames: list[int], threads: int) -> dict:
     """The oracle (FP32 CPU restatement of the reference shader) on a bounded
-    sample of the same workload: whole 1920x1080 frames of the orbit."""
+    sample of the same workload: whole 1920x1080 frames of the orbit, timed.
+    Each oracle frame is also compared with the GPU's frame of the same view
+    (pixels, per-ray step counts), and a few more frames are compared in MIP
+    (with MIP indices) and HEATMAP mode, untimed: the parity record of the
+    benchmark configuration."""
     page, pool, brick_mode = vol_pages
     sc = orc.BrickScene(page, pool)
-    total, t0 = 0, time.perf_counter()
+    total, dt = 0, 0.0
+    par = {"frames": {}, "max_lsb": 0, "steps_equal": True, "mip_equal": True}
+    gsteps = np.zeros((H, W), np.uint32)
+    gmip = np.zeros((H, W), np.uint32)
+
+    def compare(p, ref, rsteps, rmip):
+        img = ctx.raycast(p, W, H, steps=gsteps, mip_index=gmip)
+        par["max_lsb"] = max(par["max_lsb"], int(np.abs(img.astype(np.int16) -
+                                                        ref.astype(np.int16)).max()))
+        par["steps_equal"] &= bool(np.array_equal(gsteps, rsteps))
+        if p.mode == 1:
+            par["mip_equal"] &= bool(np.array_equal(gmip, rmip))
+
     for i in frames:
         p = orbit_params(rb, lut, i, brick_mode)
-        _, _, _, tot, _ = orc.render(p, sc, lut, W, H, cutoff=CUTOFF, threads=threads,
-                                     want_aux=False)
+        t0 = time.perf_counter()
+        ref, rsteps, rmip, tot, _ = orc.render(p, sc, lut, W, H, cutoff=CUTOFF, threads=threads)
+        dt += time.perf_counter() - t0
         total += tot
-    dt = time.perf_counter() - t0
+        compare(p, ref, rsteps, rmip)
+    par["frames"]["full"] = len(frames)
+    for name, mode in (("mip", 1), ("heatmap", 3)):
+        picked = frames[::max(1, len(frames) // 4)][:4]
+        for i in picked:
+            p = orbit_params(rb, lut, i, brick_mode, mode)
+            ref, rsteps, rmip, _, _ = orc.render(p, sc, lut, W, H, cutoff=CUTOFF,
+                                                 threads=threads)
+            compare(p, ref, rsteps, rmip)
+        par["frames"][name] = len(picked)
     return {"value": total / dt / 1e9, "unit": "Gsamples/s", "cores": threads, "kind": "port",
             "sample": f"{len(frames)} full 1920x1080 orbit frames (phases "
                       f"{frames[0]}..{frames[-1]} step {frames[1] - frames[0] if len(frames) > 1 else 0}"
-                      f" of 120), {total} samples, {dt:.1f} s", "fps": len(frames) / dt}
+                      f" of 120), {total} samples, {dt:.1f} s", "fps": len(frames) / dt,
+            "parity": par}
 
 
 def run_reference(args) -> None:
-    """CPU arm: the oracle on all host threads; each step traces a bounded,
-    evenly strided 1/16 of the rays of one orbit frame (every 4th pixel of
-    every 4th row), so the whole run takes minutes."""
+    """CPU arm: the oracle (the CPU restatement of the reference shader) on all
+    host threads, over the same workload built by the oracle itself (phantom,
+    brick cache, TF and orbit views bit-equal to the library's), so nothing
+    of the library under test is loaded.  Each step renders one whole
+    1920x1080 orbit frame when the run has at most 400 frames (about 0.3 s of
+    CPU each on 16 threads); longer runs trace an evenly strided 1/16 of each
+    frame's rays (every 4th pixel of every 4th row) to stay within minutes."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import render3d_b200 as rb
     import oracle as orc
     threads = os.cpu_count() or 1
-    vol = rb.phantom(N_EDGE, seed=SEED)
+    vol = orc.phantom(N_EDGE, seed=SEED, threads=threads)
     sc = orc.BrickScene.build(vol, NLEV)  # the oracle's own brick builder
     del vol
-    lut = rb.scroll_ramp_tf()
-    brick_mode = 9 | (NLEV << 8) | rb.BRICK_LOD_FLAG
-    ys, xs = np.mgrid[0:H:4, 0:W:4]
-    xy = np.stack([xs.ravel(), ys.ravel()], axis=1).astype(np.uint32)
+    lut = orc.scroll_ramp_tf()
+    brick_mode = 9 | (NLEV << 8) | orc.BRICK_LOD_FLAG
+    whole = args.warmup + args.steps <= 400
+    if not whole:
+        ys, xs = np.mgrid[0:H:4, 0:W:4]
+        xy = np.stack([xs.ravel(), ys.ravel()], axis=1).astype(np.uint32)
     times, samples = [], []
     for s in range(args.warmup + args.steps):
-        p = orbit_params(rb, lut, s, brick_mode)
+        p = orc.orbit_view((s % ORBIT_FRAMES) / ORBIT_FRAMES, W, H, lut, step_voxels=STEP_VOXELS,
+                           frame_index=s)
+        p.brick_mode = brick_mode
         t0 = time.perf_counter()
-        _, st, _ = orc.render_pixels(p, sc, lut, xy, cutoff=CUTOFF, threads=threads)
+        if whole:
+            tot = orc.render(p, sc, lut, W, H, cutoff=CUTOFF, threads=threads,
+                             want_aux=False)[3]
+        else:
+            tot = float(orc.render_pixels(p, sc, lut, xy, cutoff=CUTOFF, threads=threads)[1].sum())
         dt = time.perf_counter() - t0
         if s >= args.warmup:
             times.append(dt)
-            samples.append(float(st.sum()))
+            samples.append(float(tot))
     t = sum(times)
     v = sum(samples) / t / 1e9
-    sample = (f"per step: {xy.shape[0]} rays (every 4th pixel of every 4th row) of one "
+    sample = ("per step: one whole 1920x1080 orbit frame" if whole else
+              f"per step: {xy.shape[0]} rays (every 4th pixel of every 4th row) of one "
               "1920x1080 orbit frame")
     out = {"impl": "reference", "metric": METRIC,
            "value": v, "unit": "Gsamples/s", "n_gpus": args.gpus, "steps": args.steps,
@@ -604,13 +643,15 @@ def run_ours(args) -> None:
     achieved = alg / (ms * 1e-3) / 1e9
     out = None
     if rank == 0:
-        cpu = None
+        cpu = parity = None
         if world == 1 and not args.no_cpu_baseline:
             import oracle as orc
             page, pool = ctx.bricks_read()
-            cpu = cpu_baseline(rb, orc, (page, pool, bm), lut, list(range(0, ORBIT_FRAMES, 4)),
-                               os.cpu_count() or 1)
+            ctx.set_alpha_cutoff(CUTOFF)  # the adjoint workload left it at 0.98
+            cpu = cpu_baseline(rb, orc, ctx, (page, pool, bm), lut,
+                               list(range(0, ORBIT_FRAMES, 4)), os.cpu_count() or 1)
             del pool
+            parity = cpu.pop("parity")
         out = {"metric": METRIC, "value": value,
                "unit": "Gsamples/s", "n_gpus": world, "steps": K, "warmup": Wm,
                "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
@@ -638,7 +679,8 @@ def run_ours(args) -> None:
                "batch": bt,
                "gpu_launches": K,
                "clocks": clk.summary(),
-               "cpu_baseline": cpu}
+               "cpu_baseline": cpu,
+               "parity": parity}
         print(json.dumps(out), flush=True)
     ctx.close()
     if dist:

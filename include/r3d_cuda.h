@@ -405,15 +405,21 @@ int r3d_cuda_raycast_rows(r3d_cuda_ctx *ctx, const r3d_frame_params *view, uint8
  * memory budget at start-up, or real-time render threads for which an
  * allocation (which can synchronize the device) is a frame hitch.  Same
  * views, image rules and results as r3d_cuda_raycast_fwd with a device
- * rgba_out (required here), without the auxiliary outputs; it always runs
- * the persistent queue-draining kernel.  Its per-call scratch (the view
- * table and tile counters) lives in a 32 KiB array of device memory inside
- * the library, which every GPU that loads the library holds until the
- * process exits; at most 64 views fit, larger calls fail with
- * R3D_E_INVALID.  The first call on a device looks up that array's device
- * address, so make it before any stream capture.  All calls share the
- * array: calls that overlap on the GPU (different streams, or different
- * contexts on one device) race and must be serialized by the caller. */
+ * rgba_out (required here), without the auxiliary outputs.  It runs the
+ * persistent queue-draining kernel with the context's schedule (tile shape,
+ * refill threshold, unroll, blocks per SM; r3d_cuda_set_schedule) whatever
+ * its persistent flag.  Its per-call scratch (the view table and tile
+ * counters) lives in a 32 KiB array of device memory inside the library,
+ * which every GPU that loads the library holds until the process exits; at
+ * most 64 views fit, larger calls fail with R3D_E_INVALID.  The views reach
+ * that array through kernel launch parameters, so no host buffer is read
+ * after the call returns.  The first call on a device looks up that array's
+ * device address, so make it before any stream capture; the lookup is not
+ * repeated, so the entry point must not be used across a cudaDeviceReset.
+ * All calls share the array and each overwrites it: calls queued on one
+ * stream run one after the other, but calls that overlap on the GPU
+ * (different streams, or different contexts on one device) race and must be
+ * serialized by the caller. */
 int r3d_cuda_raycast_fwd_noalloc(r3d_cuda_ctx *ctx, const r3d_frame_params *views,
                                  uint32_t nviews, uint8_t *rgba_out, uint32_t out_w,
                                  uint32_t out_h, void *stream);

@@ -131,10 +131,42 @@ def _load():
     lib.orc_fmath_eval.argtypes = [P, P, P, U32]
     lib.orc_m3_ypr.restype = None
     lib.orc_m3_ypr.argtypes = [F, F, F, P]
+    lib.orc_orbit_view.restype = None
+    lib.orc_orbit_view.argtypes = [P, F, P, U32, U32, F, F, F, U32, U32, F, P]
+    lib.orc_phantom.restype = C.c_int
+    lib.orc_phantom.argtypes = [P, U32, U32, U32, C.c_uint64, C.c_int]
     return lib
 
 
 lib = _load()
+
+
+# r3d_frame_params (include/r3d_types.h; the reference's 248-byte layout,
+# src/render/render_types.h:47-94), declared here too so that the CPU
+# baseline builds its views without loading the library under test
+class FrameParams(C.Structure):
+    _fields_ = [
+        ("cam_origin", C.c_float * 3), ("step_voxels", C.c_float),
+        ("cam_right", C.c_float * 3), ("density", C.c_float),
+        ("cam_up", C.c_float * 3), ("lod_bias", C.c_float),
+        ("cam_forward", C.c_float * 3), ("max_mip", C.c_float),
+        ("viewport", C.c_uint32 * 2), ("mode", C.c_uint32), ("frame_index", C.c_uint32),
+        ("threshold", C.c_float), ("slab_grid", C.c_uint32), ("slab_wz", C.c_uint32),
+        ("slab_z0", C.c_float), ("slab_nx", C.c_float), ("slab_ny", C.c_float),
+        ("slab_px", C.c_float), ("slab_py", C.c_float), ("slab_depth", C.c_uint32),
+        ("clip_valid", C.c_uint32), ("clip_orig", (C.c_float * 2) * 6),
+        ("vol_r0", C.c_float * 3), ("vol_tx", C.c_float),
+        ("vol_r1", C.c_float * 3), ("vol_ty", C.c_float),
+        ("vol_r2", C.c_float * 3), ("vol_tz", C.c_float),
+        ("brick_mode", C.c_uint32), ("skip_gate", C.c_float),
+        ("slab_x0", C.c_float), ("slab_y0", C.c_float),
+        ("view_org", C.c_uint32), ("view_flags", C.c_uint32),
+        ("overlay_gain", C.c_float), ("overlay_flags", C.c_uint32),
+    ]
+
+
+assert C.sizeof(FrameParams) == 248
+BRICK_LOD_FLAG = 0x20000  # brick_mode's LOD flag (src/vk/vkbackend.c:4511-4517)
 
 
 def _p(a):
@@ -729,3 +761,39 @@ def postfilter(slots, mode: int, amount: float = 0.0) -> np.ndarray:
     out = np.array(slots, np.uint8, order="C", copy=True).reshape(-1, 128, 128, 128)
     lib.orc_postfilter(out.ctypes.data, out.shape[0], mode, amount)
     return out
+
+
+def tf_build(points) -> np.ndarray:
+    """r3d_tf_build (src/core/transfer.c:5-23) of [(value, (r, g, b, a)), ...]."""
+    vals = np.array([q[0] for q in points], np.uint8)
+    cols = np.array([q[1] for q in points], np.uint8).reshape(-1, 4)
+    lut = np.zeros((256, 4), np.uint8)
+    lib.orc_tf_build(_p(vals), _p(cols), len(points), _p(lut))
+    return lut
+
+
+def scroll_ramp_tf() -> np.ndarray:
+    """The benchmark TF: alpha 0 below 40, rising to 230 at 200 and flat to
+    255, grey RGB ramp."""
+    return tf_build([(0, (0, 0, 0, 0)), (40, (40, 40, 40, 0)), (200, (200, 200, 200, 230)),
+                     (255, (255, 255, 255, 230))])
+
+
+def orbit_view(ph: float, w: int, h: int, lut: np.ndarray, target=(0.5, 0.5, 0.5),
+               step_voxels: float = 1.0, density: float = 1.0, lod_bias: float = 0.0,
+               mode: int = 0, frame_index: int = 0, low_cut: float = 0.0) -> FrameParams:
+    """The benchmark's scripted orbit view at phase ph (orc_orbit_view)."""
+    p = FrameParams()
+    lib.orc_orbit_view(C.byref(p), ph, _p(np.array(target, np.float32)), w, h, step_voxels,
+                       density, lod_bias, mode, frame_index, low_cut,
+                       _p(np.ascontiguousarray(lut, np.uint8)))
+    return p
+
+
+def phantom(n, seed: int = 1234, threads: int = 0) -> np.ndarray:
+    """The seeded scroll phantom (orc_phantom) as a (nz, ny, nx) u8 array."""
+    nx, ny, nz = (n, n, n) if isinstance(n, int) else n
+    vol = np.empty((nz, ny, nx), np.uint8)
+    if lib.orc_phantom(_p(vol), nx, ny, nz, seed, threads) != 0:
+        raise ValueError("orc_phantom: bad arguments")
+    return vol

@@ -1944,6 +1944,100 @@ void orc_m3_ypr(float yaw, float pitch, float roll, float rows[3][3]) {
   rows[2][2] = cy * cp;
 }
 
+/* ------------------------------------------------- benchmark inputs */
+
+/* The benchmark's scripted orbit view at phase ph (src/main.c:3932-3946 and
+ * the frame set-up of src/main.c:6788-6824): turntable camera from the
+ * reference's default position, yaw = ph * tau, pitch = 0.5 sin(2 ph tau),
+ * orbiting `target` at distance 2, 60 degree field of view; camera basis of
+ * src/core/camera.c:65-75, skip gate of src/main.c:1238-1242, identity
+ * volume rotation (src/core/mathx.h:34-43 at zero angles). */
+void orc_orbit_view(r3d_frame_params *p, float ph, const float target[3], uint32_t w, uint32_t h,
+                    float step_voxels, float density, float lod_bias, uint32_t mode,
+                    uint32_t frame_index, float low_cut, const uint8_t lut[256][4]) {
+  const float tau = 6.2831853f;
+  const float yaw = ph * tau, pitch = 0.5f * sinf(ph * tau * 2.0f);
+  memset(p, 0, sizeof *p);
+  orc_orbit_pos(yaw, pitch, target, 2.0f, p->cam_origin);
+  orc_camera_basis(yaw, pitch, 1.04719755f, (float)w / (float)h, p->cam_right, p->cam_up,
+                   p->cam_forward);
+  p->step_voxels = step_voxels;
+  p->density = density;
+  p->lod_bias = lod_bias;
+  p->max_mip = 10.0f;
+  p->viewport[0] = w;
+  p->viewport[1] = h;
+  p->mode = mode;
+  p->frame_index = frame_index;
+  p->threshold = low_cut / 255.0f;
+  float vis = 255.0f;
+  for (uint32_t i = 0; i < 256u; i++)
+    if (lut[i][3] != 0) {
+      vis = (float)i;
+      break;
+    }
+  p->skip_gate = fmaxf(low_cut, vis - 0.5f) / 255.0f;
+  float m[3][3];
+  orc_m3_ypr(0.0f, 0.0f, 0.0f, m);
+  memcpy(p->vol_r0, m[0], 12);
+  memcpy(p->vol_r1, m[1], 12);
+  memcpy(p->vol_r2, m[2], 12);
+}
+
+static uint64_t orc_splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+/* The seeded scroll phantom (the benchmark's synthetic volume): an
+ * Archimedean spiral of papyrus sheets about the z axis through the volume
+ * centre, r = r0 + pitch * theta / 2pi with r0 = 8, a voxel papyrus when its
+ * radial distance to the nearest wrap is below 3 (6-voxel sheets) and
+ * r0 <= r < radius; pitch 14 up to an edge of 256, else 18; radius 110/256 of
+ * the largest edge.  Papyrus ~N(130, 15), air ~N(12, 4), plus N(0, 6) noise,
+ * rounded and clamped to 0..255.  Voxel i draws its two normals by
+ * Box-Muller from splitmix64(seed ^ 2i) and splitmix64(seed ^ (2i + 1)).
+ * vox is (nz, ny, nx), x fastest. */
+int orc_phantom(uint8_t *vox, uint32_t nx, uint32_t ny, uint32_t nz, uint64_t seed, int threads) {
+  if (!vox || !nx || !ny || !nz) return -1;
+  uint32_t n = nx > ny ? nx : ny;
+  n = n > nz ? n : nz;
+  const double pitch = n <= 256u ? 14.0 : 18.0, radius = (double)(110.0f * (float)n / 256.0f);
+  const double r0 = 8.0, half = 3.0, two_pi = 6.283185307179586;
+  uint8_t *mask = malloc((size_t)nx * ny);
+  if (!mask) return -1;
+  const double cx = 0.5 * nx, cy = 0.5 * ny;
+  for (uint32_t y = 0; y < ny; y++)
+    for (uint32_t x = 0; x < nx; x++) {
+      double dx = x + 0.5 - cx, dy = y + 0.5 - cy;
+      double r = sqrt(dx * dx + dy * dy), th = atan2(dy, dx);
+      if (th < 0.0) th += two_pi;
+      double m = fmod(r - r0 - pitch * th / two_pi, pitch);
+      if (m < 0.0) m += pitch;
+      double dist = m < pitch - m ? m : pitch - m;
+      mask[(size_t)y * nx + x] = dist < half && r >= r0 && r < radius;
+    }
+  const int nt = threads > 0 ? threads : omp_get_max_threads();
+#pragma omp parallel for schedule(static) num_threads(nt)
+  for (int64_t z = 0; z < (int64_t)nz; z++)
+    for (uint32_t y = 0; y < ny; y++)
+      for (uint32_t x = 0; x < nx; x++) {
+        const uint64_t i = ((uint64_t)z * ny + y) * nx + x;
+        const uint64_t h1 = orc_splitmix64(seed ^ (i * 2u)), h2 = orc_splitmix64(seed ^ (i * 2u + 1u));
+        const double u1 = ((double)(h1 >> 11) + 1.0) * 0x1.0p-53, u2 = (double)(h2 >> 11) * 0x1.0p-53;
+        const double rad = sqrt(-2.0 * log(u1));
+        const int pap = mask[(size_t)y * nx + x];
+        double v = (pap ? 130.0 : 12.0) + (pap ? 15.0 : 4.0) * (rad * cos(two_pi * u2)) +
+                   6.0 * (rad * sin(two_pi * u2));
+        v = floor(v + 0.5);
+        vox[i] = (uint8_t)(v < 0.0 ? 0.0 : (v > 255.0 ? 255.0 : v));
+      }
+  free(mask);
+  return 0;
+}
+
 /* ---- post-decode display filter (src/shaders/postfilt.comp) ---- */
 
 /* texelFetch of the slot at l + d, clamped to the slot (postfilt.comp:27-29) */

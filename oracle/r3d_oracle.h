@@ -259,6 +259,15 @@ uint32_t orc_lod_pick(float distance, float pixel_cone, float base_voxels, uint3
 uint32_t orc_lod_fallback(uint32_t desired, uint32_t ordinal, uint32_t nlevels);
 void orc_m3_ypr(float yaw, float pitch, float roll, float rows[3][3]);
 
+/* The benchmark's inputs, restated here so that the CPU baseline needs
+ * nothing from the library under test: the scripted orbit view
+ * (src/main.c:3932-3946 with src/core/camera.c's basis) and the seeded
+ * scroll phantom. */
+void orc_orbit_view(r3d_frame_params *p, float ph, const float target[3], uint32_t w, uint32_t h,
+                    float step_voxels, float density, float lod_bias, uint32_t mode,
+                    uint32_t frame_index, float low_cut, const uint8_t lut[256][4]);
+int orc_phantom(uint8_t *vox, uint32_t nx, uint32_t ny, uint32_t nz, uint64_t seed, int threads);
+
 /* Post-decode display filter of n 128^3 slots in place (src/shaders/
  * postfilt.comp run by src/vk/vkbackend.c:3398-3466): mode low byte 1
  * median of 3^3, 2 median of 5^3, 3 max of 3^3, 4 max of 5^3, then the

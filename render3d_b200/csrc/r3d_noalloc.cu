@@ -12,6 +12,9 @@
 // already loaded into the context.
 #include <string.h>
 
+#include <algorithm>
+#include <atomic>
+
 #include "r3d_internal.h"
 
 namespace {
@@ -24,13 +27,37 @@ constexpr size_t kTableBytes = sizeof(r3d::DevView) * kNoallocViews;
 constexpr size_t kScratchBytes = 32768;  // 32 KiB
 static_assert(kTableBytes + kNoallocViews * sizeof(uint32_t) <= kScratchBytes,
               "scratch too small for the view table");
+static_assert(sizeof(r3d::DevView) % 4u == 0u, "view records are copied as words");
 
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
 // Device address of g_scratch for each device (the host-side symbol is not a
-// device address).  Filled on the first call on a device.
+// device address).  Looked up by the first call on a device, with that
+// device current; concurrent first calls store the same value.  A
+// cudaDeviceReset reloads the module, so this cache (and the entry point)
+// must not be used across one.
 constexpr int kMaxDevices = 64;
-static void *g_scratch_dev[kMaxDevices];
+static std::atomic<void *> g_scratch_dev[kMaxDevices];
+
+// The view records of one call, passed by value as the table writer's launch
+// parameters (at most 8 views, 2.3 KiB, per launch): the kernel reads no
+// host buffer after the call returns.
+constexpr uint32_t kChunkViews = 8;
+struct TableChunk {
+  r3d::DevView v[kChunkViews];
+};
+
+// Writes n (<= 8) view records at dst and, when nq > 0, zeroes the first nq
+// tile counters of the call.
+__global__ void k_noalloc_table(r3d::DevView *__restrict__ dst, uint32_t n,
+                                uint32_t *__restrict__ queue, uint32_t nq,
+                                const __grid_constant__ TableChunk t) {
+  const uint32_t *src = reinterpret_cast<const uint32_t *>(t.v);
+  uint32_t *d = reinterpret_cast<uint32_t *>(dst);
+  const uint32_t words = n * (uint32_t)(sizeof(r3d::DevView) / 4u);
+  for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) d[i] = src[i];
+  for (uint32_t i = threadIdx.x; i < nq; i += blockDim.x) queue[i] = 0u;
+}
 
 }  // namespace
 
@@ -51,15 +78,16 @@ extern "C" int r3d_cuda_raycast_fwd_noalloc(r3d_cuda_ctx *c, const r3d_frame_par
   R3D_CUDA_TRY(c, cudaSetDevice(c->device));
   if (!is_device_ptr(rgba_out))
     return fail(c, R3D_E_INVALID, "raycast_fwd_noalloc: the image must be device memory");
-  if (!g_scratch_dev[c->device]) {  // once per device, with that device current
-    void *p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
-    if (e != cudaSuccess || !p) return cuda_fail(c, e, "raycast_fwd_noalloc: scratch address");
-    g_scratch_dev[c->device] = p;
+  void *base = g_scratch_dev[c->device].load(std::memory_order_acquire);
+  if (!base) {  // once per device, with that device current
+    cudaError_t e = cudaGetSymbolAddress(&base, g_scratch);
+    if (e != cudaSuccess || !base) return cuda_fail(c, e, "raycast_fwd_noalloc: scratch address");
+    g_scratch_dev[c->device].store(base, std::memory_order_release);
   }
-  DevView *table = (DevView *)g_scratch_dev[c->device];
-  uint32_t *queue = (uint32_t *)((unsigned char *)g_scratch_dev[c->device] + kTableBytes);
+  DevView *table = (DevView *)base;
+  uint32_t *queue = (uint32_t *)((unsigned char *)base + kTableBytes);
   cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  const r3d_cuda_schedule &sc = c->sched;
 
   r3d_frame_params pcs[kNoallocViews];
   int render[kNoallocViews];
@@ -71,7 +99,8 @@ extern "C" int r3d_cuda_raycast_fwd_noalloc(r3d_cuda_ctx *c, const r3d_frame_par
                   "raycast_fwd_noalloc: overlay and surface views are not supported");
   }
   // views sharing a sampling path and mode form one launch
-  DevView hv[kNoallocViews];
+  TableChunk chunk[kNoallocViews / kChunkViews];
+  DevView *hv = &chunk[0].v[0];
   uint32_t order[kNoallocViews], group_of[kNoallocViews], gkey[kNoallocViews];
   uint32_t gcount[kNoallocViews], gstart[kNoallocViews + 1], ngroups = 0, n = 0;
   for (uint32_t v = 0; v < nviews; v++) {
@@ -89,7 +118,6 @@ extern "C" int r3d_cuda_raycast_fwd_noalloc(r3d_cuda_ctx *c, const r3d_frame_par
   if (!n) return R3D_OK;
   gstart[0] = 0;
   for (uint32_t g = 0; g < ngroups; g++) gstart[g + 1] = gstart[g] + gcount[g];
-  const uint32_t shape = 0u;  // 8x4 tiles
   uint32_t fill[kNoallocViews] = {0}, ntiles[kNoallocViews] = {0};
   for (uint32_t i = 0; i < n; i++) {
     uint32_t g = group_of[i], slot = gstart[g] + fill[g]++;
@@ -99,12 +127,17 @@ extern "C" int r3d_cuda_raycast_fwd_noalloc(r3d_cuda_ctx *c, const r3d_frame_par
     d.img = (uchar4 *)rgba_out;
     d.stride = out_w;
     d.tile_begin = ntiles[g];
-    ntiles[g] += view_tiles(d, shape);
+    ntiles[g] += view_tiles(d, sc.tile_shape);
   }
-  // from pageable host memory the copy is staged before the call returns,
-  // so hv may go out of scope; the counters of this call start at zero
-  R3D_CUDA_TRY(c, cudaMemcpyAsync(table, hv, sizeof(DevView) * n, cudaMemcpyHostToDevice, st));
-  R3D_CUDA_TRY(c, cudaMemsetAsync(queue, 0, sizeof(uint32_t) * ngroups, st));
+  // the table and this call's zeroed counters, written on the stream ahead
+  // of the raycast launches (a call queued behind an earlier one on the
+  // same stream overwrites the scratch only once that one has finished)
+  for (uint32_t k = 0; k * kChunkViews < n; k++) {
+    const uint32_t m = std::min(kChunkViews, n - k * kChunkViews);
+    k_noalloc_table<<<1, 128, 0, st>>>(table + k * kChunkViews, m, queue, k ? 0u : ngroups,
+                                       chunk[k]);
+    R3D_CUDA_TRY(c, cudaGetLastError());
+  }
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
   const DevScene s = c->scene();
@@ -116,14 +149,16 @@ extern "C" int r3d_cuda_raycast_fwd_noalloc(r3d_cuda_ctx *c, const r3d_frame_par
     L.ntiles = ntiles[g];
     L.lut = c->lut;
     L.queue = queue + g;
-    L.refill_min = 16u;
-    L.shape = shape;
-    L.unroll = 1u;
+    L.refill_min = sc.refill_min;
+    L.shape = sc.tile_shape;
+    L.unroll = sc.unroll;
     L.mode = gkey[g] & 7u;
     L.fast = c->quality == R3D_QUALITY_FAST;
     L.path = (int)(gkey[g] >> 3);
-    uint32_t want =
-        (uint32_t)persist_blocks_per_sm(L.path, L.mode, L.fast, 1u) * (uint32_t)sms;
+    const int per_sm = sc.blocks_per_sm
+                           ? (int)sc.blocks_per_sm
+                           : persist_blocks_per_sm(L.path, L.mode, L.fast, L.unroll);
+    uint32_t want = (uint32_t)per_sm * (uint32_t)sms;
     uint32_t cap = (L.ntiles + 3u) / 4u;
     L.blocks = want < cap ? want : (cap ? cap : 1u);
     cudaError_t e = launch_persist(L, s, st);

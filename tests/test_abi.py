@@ -19,10 +19,11 @@ OFFSETS = {"cam_origin": 0, "step_voxels": 12, "cam_right": 16, "density": 28, "
            "view_org": 232, "view_flags": 236, "overlay_gain": 240, "overlay_flags": 244}
 
 
-def test_frame_params_layout(rb):
-    assert C.sizeof(rb.FrameParams) == 248
-    for name, off in OFFSETS.items():
-        assert getattr(rb.FrameParams, name).offset == off, name
+def test_frame_params_layout(rb, orc):
+    for fp in (rb.FrameParams, orc.FrameParams):  # the library's and the oracle's bindings
+        assert C.sizeof(fp) == 248
+        for name, off in OFFSETS.items():
+            assert getattr(fp, name).offset == off, name
 
 
 def test_c_header_layout_with_gcc(tmp_path):

@@ -1,8 +1,9 @@
-"""Parity at the benchmark sizes on sampled rays: the 1024^3 four-level
-brick cache at 1920x1080 (FULL, MIP, HEATMAP; cutoff 0.99) and a 2048^3
-sparse cache (bricks with maximum <= 40 left out) at 3840x2160 with LOD bias
-0 and 1.  Colours, step counts and MIP indices of every sampled ray must
-equal the oracle's; properties of whole frames are checked beside them."""
+"""Parity at the benchmark sizes: the 1024^3 four-level brick cache at
+1920x1080 (FULL, MIP, HEATMAP; cutoff 0.99) on sampled rays and on eight
+whole frames spread over the bench orbit, and a 2048^3 sparse cache (bricks
+with maximum <= 40 left out) at 3840x2160 with LOD bias 0 and 1 on sampled
+rays.  Colours (within 1/255), step counts and MIP indices must equal the
+oracle's; properties of whole frames are checked beside them."""
 import numpy as np
 import pytest
 
@@ -52,6 +53,35 @@ def test_1024_1080p(rb, orc, ctx, cache1024, scroll_tf, mode):
             img, steps = _check_frame(rb, orc, ctx, cache1024, scroll_tf, p, 1920, 1080, 0.99)
             assert np.all(img[..., 3] == 255)
             assert steps.max() <= (192 if mode == 0 else 256)  # bricks-LOD budgets
+    finally:
+        ctx.set_alpha_cutoff(0.98)
+
+
+@pytest.mark.parametrize("mode", [0, 1, 3])
+def test_1024_1080p_whole_frames(rb, orc, ctx, cache1024, scroll_tf, mode):
+    """Eight whole 1920x1080 frames spread over the 120-frame bench orbit
+    (phases 0, 15, ..., 105 of 120, frame_index = phase), cutoff 0.99: every
+    pixel within 1/255 of the oracle, every step count equal, and in MIP
+    mode every MIP index equal."""
+    ctx.set_transfer(scroll_tf)
+    ctx.set_alpha_cutoff(0.99)
+    ctx.set_quality(0)
+    w, h = 1920, 1080
+    try:
+        for i in range(0, 120, 15):
+            p = rb.orbit_view(i / 120.0, w, h, scroll_tf, step_voxels=0.5, mode=mode,
+                              frame_index=i)
+            p.brick_mode = ctx.brick_mode
+            steps = np.zeros((h, w), np.uint32)
+            mipi = np.zeros((h, w), np.uint32)
+            img = ctx.raycast(p, w, h, steps=steps, mip_index=mipi)
+            ref, rsteps, rmip, _, st = orc.render(p, cache1024, scroll_tf, w, h, cutoff=0.99)
+            assert st == 0
+            d = np.abs(img.astype(int) - ref.astype(int)).max()
+            assert d <= 1, f"phase {i}/120 mode {mode}: {d} LSB"
+            assert np.array_equal(steps, rsteps), f"phase {i}/120 mode {mode}: step counts"
+            if mode == rb.MODE_MIP:
+                assert np.array_equal(mipi, rmip), f"phase {i}/120: MIP indices"
     finally:
         ctx.set_alpha_cutoff(0.98)
 
