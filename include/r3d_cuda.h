@@ -399,16 +399,24 @@ int r3d_cuda_raycast_rows(r3d_cuda_ctx *ctx, const r3d_frame_params *view, uint8
                           uint32_t out_w, uint32_t out_h, uint32_t row0, uint32_t row1,
                           void *stream);
 
+/* Writes one RGBA8 colour into npix pixels of the device image img,
+ * stream-ordered.  The render layer's clear of the offscreen regions that no
+ * view covers when the pane layout changes (the vkCmdClearColorImage of
+ * src/vk/vkbackend.c:7079-7098). */
+int r3d_cuda_fill_rgba(r3d_cuda_ctx *ctx, uint8_t *img, size_t npix, const uint8_t rgba[4],
+                       void *stream);
+
 /* Forward raycast that allocates no device memory.  No counterpart in the
  * reference: it exists for callers that must not let the library allocate
  * while they render -- applications that give the renderer a fixed device-
  * memory budget at start-up, or real-time render threads for which an
  * allocation (which can synchronize the device) is a frame hitch.  Same
  * views, image rules and results as r3d_cuda_raycast_fwd with a device
- * rgba_out (required here), without the auxiliary outputs.  It runs the
- * persistent queue-draining kernel with the context's schedule (tile shape,
- * refill threshold, unroll, blocks per SM; r3d_cuda_set_schedule) whatever
- * its persistent flag.  Its per-call scratch (the view table and tile
+ * rgba_out (required here), without the auxiliary outputs.  It runs a
+ * persistent queue-draining kernel under the context's schedule
+ * (r3d_cuda_set_schedule): whole 8x4 tiles when its persistent field is 2,
+ * else lane refill with its tile shape, refill threshold and unroll; blocks
+ * per SM as set.  Its per-call scratch (the view table and tile
  * counters) lives in a 32 KiB array of device memory inside the library,
  * which every GPU that loads the library holds until the process exits; at
  * most 64 views fit, larger calls fail with R3D_E_INVALID.  The views reach
@@ -429,8 +437,12 @@ int r3d_cuda_raycast_fwd_noalloc(r3d_cuda_ctx *ctx, const r3d_frame_params *view
  * 32-ray tiles covering all views of the call, refilling lanes whose rays
  * have ended whenever at least refill_min lanes are idle; tile_shape 0/1/2
  * = 8x4 / 16x2 / 32x1 rays; unroll = march steps between refill checks
- * (1 or 2); blocks_per_sm = resident 128-thread blocks per SM (0: the
- * occupancy limit).  shade_group (FULL mode, one-thread-per-ray launches):
+ * (1 or 2).  persistent = 2: resident warps drain a queue of whole 8x4
+ * tiles covering all views of the call (one launch per sampling path and
+ * mode), each marching its 32 rays to the end before taking the next tile
+ * (refill_min, tile_shape and unroll unused).  blocks_per_sm = resident
+ * 128-thread blocks per SM of a persistent launch (0: the occupancy
+ * limit).  shade_group (FULL mode, one-thread-per-ray launches):
  * n > 0 lets lanes park a sample that needs gradient shading until n lanes
  * of the warp (or all its live lanes) wait, and shades them together (1:
  * each sample where its ray meets it); 0 picks the sampling path's default,
@@ -464,7 +476,27 @@ typedef struct r3d_cuda_request {
   uint8_t *rgba;
 } r3d_cuda_request;
 
+/* Raycasts n (1..64) requests, each into its own device image, on stream
+ * (NULL: the context's), under the context's schedule: one grid per request
+ * (persistent 0), or one queue-draining launch per sampling path and mode
+ * over all of them (persistent 1 or 2).  total_steps (nullable, device)
+ * += march iterations.  The batched form of the per-view dispatch loop of
+ * src/vk/vkbackend.c:7121-7173 for views of any size; nothing is kept
+ * between calls (r3d_cuda_batch_* plans a batch once for replay). */
+int r3d_cuda_raycast_batch(r3d_cuda_ctx *ctx, const r3d_cuda_request *reqs, uint32_t n,
+                           unsigned long long *total_steps, void *stream);
+
 typedef struct r3d_cuda_batch r3d_cuda_batch;
+
+/* One request of a batch whose views sample several scenes: a view, its
+ * image and the context whose scene it samples (volume or brick cache, TF,
+ * quality, cutoff; NULL: the batch's context).  No counterpart in the
+ * reference, which renders one scene per frame. */
+typedef struct r3d_cuda_scene_request {
+  r3d_frame_params view;
+  uint8_t *rgba;
+  r3d_cuda_ctx *scene;
+} r3d_cuda_scene_request;
 
 /* Plans a batch of 1..64 requests over the context's scene (all views use
  * it; requests may differ in size, projection and mode).  The plan keeps
@@ -472,24 +504,36 @@ typedef struct r3d_cuda_batch r3d_cuda_batch;
  * host data: it can be captured into a CUDA graph and replayed. */
 int r3d_cuda_batch_create(r3d_cuda_ctx *ctx, const r3d_cuda_request *reqs, uint32_t n,
                           r3d_cuda_batch **out);
+/* Plans a batch over up to 4 scenes (contexts on the batch context's
+ * device).  Under the whole-tile schedule (persistent 2, the default when
+ * there are several scenes) one launch per sampling path, mode and quality
+ * drains the tiles of every view of every scene; the lane-refill schedule
+ * needs a batch of one scene.  Launches read each scene as it is when they
+ * are enqueued, and a captured graph keeps the scenes as they were at
+ * capture: capture again after changing a scene. */
+int r3d_cuda_batch_create_scenes(r3d_cuda_ctx *ctx, const r3d_cuda_scene_request *reqs,
+                                 uint32_t n, r3d_cuda_batch **out);
 void r3d_cuda_batch_destroy(r3d_cuda_batch *batch);
-/* Schedule of the batch's launches (default: persistent, 8x4 tiles). */
+/* Schedule of the batch's launches (default: lane refill with 8x4 tiles
+ * for one scene, whole tiles for several). */
 int r3d_cuda_batch_set_schedule(r3d_cuda_batch *batch, const r3d_cuda_schedule *sched);
 int r3d_cuda_batch_get_schedule(const r3d_cuda_batch *batch, r3d_cuda_schedule *sched);
 /* Enqueues the batch on stream (NULL: the context's): one persistent
- * launch per mode present (one in the common single-mode batch) draining
- * the tiles of all its views, or one grid per view under a grid schedule.
+ * launch per sampling path and mode present (per path, mode and quality
+ * under whole tiles; one in the common single-mode batch) draining the
+ * tiles of all its views, or one grid per view under a grid schedule.
  * total_steps (nullable, device) += march iterations. */
 int r3d_cuda_batch_launch(r3d_cuda_batch *batch, unsigned long long *total_steps, void *stream);
 /* Captures r3d_cuda_batch_launch into a CUDA graph owned by the batch
  * (replacing an earlier one), and launches that graph. */
 int r3d_cuda_batch_capture(r3d_cuda_batch *batch, unsigned long long *total_steps, void *stream);
 int r3d_cuda_batch_replay(r3d_cuda_batch *batch, void *stream);
-/* Autotuner: times every candidate schedule (one thread per ray; persistent
- * with tile 8x4 / 16x2 / 32x1, refill threshold 8 / 16 / 24, 1 or 2 steps
- * between refills) over `reps` launches each after a warm-up, keeps the
- * fastest as the batch's schedule and returns it with its time per launch.
- * Results are identical under every candidate. */
+/* Autotuner: times every candidate schedule (one thread per ray with
+ * grouped shading off / 4 / 8 / 16; lane refill with tile 8x4 / 16x2 /
+ * 32x1, refill threshold 8 / 16 / 24, 1 or 2 steps between refills, for a
+ * batch of one scene; whole 8x4 tiles) over `reps` launches each after a
+ * warm-up, keeps the fastest as the batch's schedule and returns it with
+ * its time per launch.  Results are identical under every candidate. */
 int r3d_cuda_batch_autotune(r3d_cuda_batch *batch, uint32_t reps, r3d_cuda_schedule *best,
                             float *best_ms);
 

@@ -80,6 +80,10 @@ class Schedule(C.Structure):
                 ("blocks_per_sm", C.c_uint32), ("shade_group", C.c_uint32)]
 
 
+class SceneRequest(C.Structure):
+    _fields_ = [("view", FrameParams), ("rgba", C.c_void_p), ("scene", C.c_void_p)]
+
+
 class Request(C.Structure):
     _fields_ = [("view", FrameParams), ("rgba", C.c_void_p)]
 
@@ -264,9 +268,12 @@ def _load() -> C.CDLL:
         "r3d_cuda_last_kernel_ns": (I, [P, C.POINTER(C.c_uint64)]),
         "r3d_cuda_fmath_eval": (I, [P, P, P, P, U32]),
         "r3d_cuda_set_schedule": (I, [P, C.POINTER(Schedule)]),
+        "r3d_cuda_fill_rgba": (I, [P, P, C.c_size_t, P, P]),
         "r3d_cuda_raycast_fwd_noalloc": (I, [P, P, U32, P, U32, U32, P]),
         "r3d_cuda_diff_forward": (I, [P, C.POINTER(DiffScene), P, U32, P, P, P]),
         "r3d_cuda_diff_forward_tape": (I, [P, C.POINTER(DiffScene), P, U32, P, P, P]),
+        "r3d_cuda_batch_create_scenes": (I, [P, P, U32, C.POINTER(P)]),
+        "r3d_cuda_raycast_batch": (I, [P, P, U32, P, P]),
         "r3d_cuda_batch_create": (I, [P, P, U32, C.POINTER(P)]),
         "r3d_cuda_batch_destroy": (None, [P]),
         "r3d_cuda_batch_set_schedule": (I, [P, C.POINTER(Schedule)]),
@@ -938,6 +945,12 @@ class Context:
         self._check(lib.r3d_cuda_get_schedule(self.h, C.byref(sc)))
         return {f: getattr(sc, f) for f, _ in Schedule._fields_}
 
+    def raycast_batch(self, views, images, total=None, stream: int = 0) -> None:
+        """r3d_cuda_raycast_batch: each view into its own device image."""
+        arr = (Request * len(views))(*[Request(v, _ptr(im)) for v, im in zip(views, images)])
+        self._check(lib.r3d_cuda_raycast_batch(self.h, arr, len(views), _ptr(total) or None,
+                                               stream or None))
+
     def last_kernel_ns(self) -> int:
         ns = C.c_uint64()
         self._check(lib.r3d_cuda_last_kernel_ns(self.h, C.byref(ns)))
@@ -945,12 +958,20 @@ class Context:
 
 
 class Batch:
-    """r3d_cuda_batch: many views with their own device images (tensors)."""
+    """r3d_cuda_batch: many views with their own device images (tensors);
+    scenes (optional): per view the Context whose scene it samples (None:
+    ctx's)."""
 
-    def __init__(self, ctx: Context, views, images):
-        arr = (Request * len(views))(*[Request(v, _ptr(im)) for v, im in zip(views, images)])
+    def __init__(self, ctx: Context, views, images, scenes=None):
         h = C.c_void_p()
-        ctx._check(lib.r3d_cuda_batch_create(ctx.h, arr, len(views), C.byref(h)))
+        if scenes is None:
+            arr = (Request * len(views))(*[Request(v, _ptr(im)) for v, im in zip(views, images)])
+            ctx._check(lib.r3d_cuda_batch_create(ctx.h, arr, len(views), C.byref(h)))
+        else:
+            arr = (SceneRequest * len(views))(*[
+                SceneRequest(v, _ptr(im), sc.h if sc is not None else None)
+                for v, im, sc in zip(views, images, scenes)])
+            ctx._check(lib.r3d_cuda_batch_create_scenes(ctx.h, arr, len(views), C.byref(h)))
         self.ctx, self.h = ctx, h
 
     def close(self) -> None:

@@ -4,6 +4,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "r3d_internal.h"
@@ -233,7 +234,7 @@ int r3d_cuda_create(int device, r3d_cuda_ctx **out) {
           cudaSuccess ||
       cudaMalloc(&c->ring_dev, sizeof(DevView) * kMaxBatchViews * r3d_cuda_ctx::kRing) !=
           cudaSuccess ||
-      cudaMalloc(&c->ring_queue, sizeof(uint32_t) * kMaxBatchViews * r3d_cuda_ctx::kRing) !=
+      cudaMalloc(&c->ring_queue, sizeof(uint32_t) * 2 * kMaxBatchViews * r3d_cuda_ctx::kRing) !=
           cudaSuccess) {
     cudaGetLastError();
     r3d_cuda_destroy(c);
@@ -881,8 +882,8 @@ int prepare_view(r3d_cuda_ctx *c, const r3d_frame_params &in, uint32_t out_w,
 // sampling path and mode go into one launch (template parameters of the
 // kernel), in order of first appearance.
 static int launch_views_persistent(r3d_cuda_ctx *c, const r3d_frame_params *pcs,
-                                   const int *render, uint32_t nviews, uint8_t *img,
-                                   uint32_t out_w, uint32_t *steps, uint32_t *mip,
+                                   const int *render, uint32_t nviews, uint8_t *const *imgs,
+                                   const uint32_t *strides, uint32_t *steps, uint32_t *mip,
                                    unsigned long long *total, unsigned long long *counters,
                                    cudaStream_t st) {
   const int k = c->ring_next;
@@ -890,7 +891,7 @@ static int launch_views_persistent(r3d_cuda_ctx *c, const r3d_frame_params *pcs,
   if (c->ring_used[k]) R3D_CUDA_TRY(c, cudaEventSynchronize(c->ring_ev[k]));
   DevView *hv = c->ring_host + (size_t)k * kMaxBatchViews;
   DevView *dv = c->ring_dev + (size_t)k * kMaxBatchViews;
-  uint32_t *queue = c->ring_queue + (size_t)k * kMaxBatchViews;
+  uint32_t *queue = c->ring_queue + (size_t)k * 2 * kMaxBatchViews;  // two words per group
   const r3d_cuda_schedule &sc = c->sched;
   // group views by (path, mode)
   uint32_t order[64], group_of[64], ngroups = 0, gkey[64], gstart[65], gcount[64];
@@ -918,18 +919,42 @@ static int launch_views_persistent(r3d_cuda_ctx *c, const r3d_frame_params *pcs,
     DevView &d = hv[slot];
     memset(&d, 0, sizeof d);
     d.pc = pcs[order[i]];
-    d.img = (uchar4 *)img;
-    d.stride = out_w;
+    d.img = (uchar4 *)imgs[order[i]];
+    d.stride = strides[order[i]];
     d.tile_begin = ntiles[g];
-    ntiles[g] += view_tiles(d, sc.tile_shape);
+    ntiles[g] += view_tiles(d, sc.persistent == 2u ? 0u : sc.tile_shape);
   }
   R3D_CUDA_TRY(c, cudaMemcpyAsync(dv, hv, sizeof(DevView) * n, cudaMemcpyHostToDevice, st));
   R3D_CUDA_TRY(c, cudaEventRecord(c->ring_ev[k], st));
   c->ring_used[k] = true;
-  R3D_CUDA_TRY(c, cudaMemsetAsync(queue, 0, sizeof(uint32_t) * ngroups, st));
+  R3D_CUDA_TRY(c, cudaMemsetAsync(queue, 0, sizeof(uint32_t) * 2 * ngroups, st));
   int dev_sms = 148;
   cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device);
   const DevScene s = c->scene();
+  if (sc.persistent == 2u) {  // whole tiles, the views as launch parameters
+    for (uint32_t g = 0; g < ngroups; g++) {
+      TilesLaunch T;
+      memset(&T, 0, sizeof T);
+      T.views = hv + gstart[g];
+      T.nviews = gcount[g];
+      T.ntiles = ntiles[g];
+      T.scenes = &s;
+      T.luts = &c->lut;
+      T.nscenes = 1u;
+      T.queue = queue + 2 * g;
+      T.steps = steps;
+      T.mip = mip;
+      T.total = total;
+      T.counters = counters;
+      T.blocks = sc.blocks_per_sm * (uint32_t)dev_sms;
+      T.mode = gkey[g] & 7u;
+      T.fast = c->quality == R3D_QUALITY_FAST;
+      T.path = (int)(gkey[g] >> 3);
+      cudaError_t e = launch_tiles(T, st);
+      if (e != cudaSuccess) return cuda_fail(c, e, "raycast_fwd: whole-tile launch");
+    }
+    return R3D_OK;
+  }
   for (uint32_t g = 0; g < ngroups; g++) {
     PersistLaunch L;
     memset(&L, 0, sizeof L);
@@ -937,7 +962,7 @@ static int launch_views_persistent(r3d_cuda_ctx *c, const r3d_frame_params *pcs,
     L.nviews = gcount[g];
     L.ntiles = ntiles[g];
     L.lut = c->lut;
-    L.queue = queue + g;
+    L.queue = queue + 2 * g;
     L.refill_min = sc.refill_min;
     L.shape = sc.tile_shape;
     L.unroll = sc.unroll;
@@ -961,10 +986,17 @@ static int launch_views_persistent(r3d_cuda_ctx *c, const r3d_frame_params *pcs,
   return R3D_OK;
 }
 
+// One colour into every pixel of an RGBA8 image (grid-stride).
+__global__ void k_fill_rgba(uchar4 *__restrict__ img, size_t npix, uchar4 col) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < npix;
+       i += (size_t)gridDim.x * blockDim.x)
+    img[i] = col;
+}
+
 extern "C" {
 
 int r3d_cuda_set_schedule(r3d_cuda_ctx *c, const r3d_cuda_schedule *sc) {
-  if (!c || !sc || sc->persistent > 1u || sc->refill_min < 1u || sc->refill_min > 32u ||
+  if (!c || !sc || sc->persistent > 2u || sc->refill_min < 1u || sc->refill_min > 32u ||
       sc->tile_shape > 2u || (sc->unroll != 1u && sc->unroll != 2u) || sc->shade_group > 32u ||
       sc->blocks_per_sm > 32u)
     return fail(c, R3D_E_INVALID, "set_schedule: bad schedule");
@@ -1060,7 +1092,13 @@ int r3d_cuda_raycast_fwd(r3d_cuda_ctx *c, const r3d_frame_params *views, uint32_
     any_ovl = any_ovl || (render[v] && ((pcs[v].overlay_flags & kOvlAtlases) ||
                                         (pcs[v].view_flags & R3D_VIEW_SURF)));
   if (c->sched.persistent && !any_ovl) {
-    int rc = launch_views_persistent(c, pcs, render, nviews, img, out_w, steps, mip, total,
+    uint8_t *imgs[64];
+    uint32_t strides[64];
+    for (uint32_t v = 0; v < nviews; v++) {
+      imgs[v] = img;
+      strides[v] = out_w;
+    }
+    int rc = launch_views_persistent(c, pcs, render, nviews, imgs, strides, steps, mip, total,
                                      counters, st);
     if (rc != R3D_OK) return rc;
   } else {
@@ -1085,6 +1123,56 @@ int r3d_cuda_raycast_fwd(r3d_cuda_ctx *c, const r3d_frame_params *views, uint32_
     if (total) *aux->total_steps += tsum[0];
     if (counters)
       for (int k = 0; k < R3D_COUNTERS; k++) aux->counters[k] += tsum[1 + k];
+  }
+  return R3D_OK;
+}
+
+int r3d_cuda_fill_rgba(r3d_cuda_ctx *c, uint8_t *img, size_t npix, const uint8_t rgba[4],
+                       void *stream) {
+  if (!c || !img || !rgba) return fail(c, R3D_E_INVALID, "fill_rgba: bad arguments");
+  if (!npix) return R3D_OK;
+  R3D_CUDA_TRY(c, cudaSetDevice(c->device));
+  if (!is_device_ptr(img)) return fail(c, R3D_E_INVALID, "fill_rgba: the image must be device memory");
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  const uchar4 col = make_uchar4(rgba[0], rgba[1], rgba[2], rgba[3]);
+  const uint32_t blocks = (uint32_t)std::min<size_t>((npix + 255u) / 256u, 148u * 16u);
+  k_fill_rgba<<<blocks, 256, 0, st>>>((uchar4 *)img, npix, col);
+  R3D_CUDA_TRY(c, cudaGetLastError());
+  return R3D_OK;
+}
+
+int r3d_cuda_raycast_batch(r3d_cuda_ctx *c, const r3d_cuda_request *reqs, uint32_t n,
+                           unsigned long long *total_steps, void *stream) {
+  if (!c || !reqs || !n || n > kMaxBatchViews)
+    return fail(c, R3D_E_INVALID, "raycast_batch: 1..%u requests", kMaxBatchViews);
+  R3D_CUDA_TRY(c, cudaSetDevice(c->device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  r3d_frame_params pcs[kMaxBatchViews];
+  int render[kMaxBatchViews];
+  uint8_t *imgs[kMaxBatchViews];
+  uint32_t strides[kMaxBatchViews];
+  bool any_ovl = false;
+  for (uint32_t i = 0; i < n; i++) {
+    const r3d_frame_params &v = reqs[i].view;
+    if (!reqs[i].rgba || !v.viewport[0] || !v.viewport[1] || v.view_org)
+      return fail(c, R3D_E_INVALID, "raycast_batch: request %u needs an image, a viewport and "
+                                    "view_org 0", i);
+    if (!is_device_ptr(reqs[i].rgba))
+      return fail(c, R3D_E_INVALID, "raycast_batch: request %u image is not device memory", i);
+    render[i] = prepare_view(c, v, v.viewport[0], v.viewport[1], pcs[i]);
+    if (render[i] < 0) return render[i];
+    imgs[i] = reqs[i].rgba;
+    strides[i] = pcs[i].viewport[0];
+    any_ovl = any_ovl || (pcs[i].overlay_flags & kOvlAtlases) || (pcs[i].view_flags & R3D_VIEW_SURF);
+  }
+  if (c->sched.persistent && !any_ovl)
+    return launch_views_persistent(c, pcs, render, n, imgs, strides, nullptr, nullptr,
+                                   total_steps, nullptr, st);
+  for (uint32_t i = 0; i < n; i++) {
+    if (!render[i]) continue;
+    cudaError_t e = launch_view(c, pcs[i], imgs[i], strides[i], nullptr, nullptr, total_steps,
+                                nullptr, st);
+    if (e != cudaSuccess) return cuda_fail(c, e, "raycast_batch: launch");
   }
   return R3D_OK;
 }

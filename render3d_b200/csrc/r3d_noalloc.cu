@@ -20,12 +20,12 @@
 namespace {
 
 // Per-call scratch of every call on every device: up to kNoallocViews view
-// records followed by one tile counter per view.  Each GPU that loads the
+// records followed by two tile counters per view.  Each GPU that loads the
 // library holds these bytes until the process exits.
 constexpr uint32_t kNoallocViews = r3d::kMaxBatchViews;  // 64
 constexpr size_t kTableBytes = sizeof(r3d::DevView) * kNoallocViews;
 constexpr size_t kScratchBytes = 32768;  // 32 KiB
-static_assert(kTableBytes + kNoallocViews * sizeof(uint32_t) <= kScratchBytes,
+static_assert(kTableBytes + 2 * kNoallocViews * sizeof(uint32_t) <= kScratchBytes,
               "scratch too small for the view table");
 static_assert(sizeof(r3d::DevView) % 4u == 0u, "view records are copied as words");
 
@@ -127,14 +127,14 @@ extern "C" int r3d_cuda_raycast_fwd_noalloc(r3d_cuda_ctx *c, const r3d_frame_par
     d.img = (uchar4 *)rgba_out;
     d.stride = out_w;
     d.tile_begin = ntiles[g];
-    ntiles[g] += view_tiles(d, sc.tile_shape);
+    ntiles[g] += view_tiles(d, sc.persistent == 2u ? 0u : sc.tile_shape);
   }
   // the table and this call's zeroed counters, written on the stream ahead
   // of the raycast launches (a call queued behind an earlier one on the
   // same stream overwrites the scratch only once that one has finished)
   for (uint32_t k = 0; k * kChunkViews < n; k++) {
     const uint32_t m = std::min(kChunkViews, n - k * kChunkViews);
-    k_noalloc_table<<<1, 128, 0, st>>>(table + k * kChunkViews, m, queue, k ? 0u : ngroups,
+    k_noalloc_table<<<1, 128, 0, st>>>(table + k * kChunkViews, m, queue, k ? 0u : 2u * ngroups,
                                        chunk[k]);
     R3D_CUDA_TRY(c, cudaGetLastError());
   }
@@ -142,13 +142,32 @@ extern "C" int r3d_cuda_raycast_fwd_noalloc(r3d_cuda_ctx *c, const r3d_frame_par
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
   const DevScene s = c->scene();
   for (uint32_t g = 0; g < ngroups; g++) {
+    cudaError_t e;
+    if (sc.persistent == 2u) {  // whole tiles: the views travel as launch parameters
+      TilesLaunch T;
+      memset(&T, 0, sizeof T);
+      T.views = hv + gstart[g];
+      T.nviews = gcount[g];
+      T.ntiles = ntiles[g];
+      T.scenes = &s;
+      T.luts = &c->lut;
+      T.nscenes = 1u;
+      T.queue = queue + 2 * g;
+      T.blocks = sc.blocks_per_sm * (uint32_t)sms;
+      T.mode = gkey[g] & 7u;
+      T.fast = c->quality == R3D_QUALITY_FAST;
+      T.path = (int)(gkey[g] >> 3);
+      e = launch_tiles(T, st);
+      if (e != cudaSuccess) return cuda_fail(c, e, "raycast_fwd_noalloc: launch");
+      continue;
+    }
     PersistLaunch L;
     memset(&L, 0, sizeof L);
     L.views = table + gstart[g];
     L.nviews = gcount[g];
     L.ntiles = ntiles[g];
     L.lut = c->lut;
-    L.queue = queue + g;
+    L.queue = queue + 2 * g;
     L.refill_min = sc.refill_min;
     L.shape = sc.tile_shape;
     L.unroll = sc.unroll;
@@ -161,7 +180,7 @@ extern "C" int r3d_cuda_raycast_fwd_noalloc(r3d_cuda_ctx *c, const r3d_frame_par
     uint32_t want = (uint32_t)per_sm * (uint32_t)sms;
     uint32_t cap = (L.ntiles + 3u) / 4u;
     L.blocks = want < cap ? want : (cap ? cap : 1u);
-    cudaError_t e = launch_persist(L, s, st);
+    e = launch_persist(L, s, st);
     if (e != cudaSuccess) return cuda_fail(c, e, "raycast_fwd_noalloc: launch");
   }
   return R3D_OK;

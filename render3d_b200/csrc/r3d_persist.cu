@@ -13,8 +13,24 @@
 // Per-ray arithmetic is the same ray_begin / ray_step / ray_end as the
 // one-ray-per-thread kernel, so results are bit-identical to it and to the
 // CPU oracle; only the order in which rays are processed changes.
+#include <string.h>
+
 #include "r3d_internal.h"
 #include "r3d_persist.h"
+
+// Resident 128-thread blocks per SM the whole-tile kernel's registers are
+// bounded for: as the one-thread-per-ray kernels (8 for the plain LOD-brick
+// kernels, 9 for their MIP, 7 elsewhere), except the LOD-brick FULL kernel
+// (R3D_TILES_FULL_BLOCKS).
+#ifndef R3D_TILES_FULL_BLOCKS
+#define R3D_TILES_FULL_BLOCKS 8
+#endif
+#define R3D_TILES_BOUNDS                                                                   \
+  __launch_bounds__(128, (PATH == PATH_LOD_BRICKS && !COUNT && MODE != R3D_MODE_HEATMAP)    \
+                             ? (MODE == R3D_MODE_MIP     ? 9                                \
+                                : MODE == R3D_MODE_FULL ? R3D_TILES_FULL_BLOCKS            \
+                                                        : 8)                               \
+                             : 7)
 
 namespace r3d {
 
@@ -196,6 +212,146 @@ __global__ void __launch_bounds__(128) k_raycast_persist(
   }
 }
 
+// The views and scenes of a whole-tile launch, held in its launch
+// parameters (constant memory): N = 1 for a launch of one view, else up to
+// 64 views; NS scenes (1, or up to 4 when the views sample several).
+template <uint32_t N>
+struct TileViews {
+  DevView v[N];
+  uint32_t n;
+};
+template <uint32_t NS>
+struct TileScenes {
+  DevScene s[NS];
+  const uchar4 *lut[NS];
+  uint32_t n;
+};
+
+// Whole-tile queue: each warp takes an 8x4 ray tile from the queue, marches
+// its 32 rays to the end exactly as the one-thread-per-ray kernel does (no
+// per-step warp votes; the view's parameters and its scene in constant
+// memory), stores them and takes the next tile.  Warps never wait for each
+// other, so an SM slot freed by a warp whose rays ended early is refilled
+// at once, and the tail of a launch over many views is one tile long.
+template <int PATH, int MODE, bool FAST, bool COUNT, uint32_t N, uint32_t NS>
+__global__ void R3D_TILES_BOUNDS k_raycast_tiles(
+    const __grid_constant__ TileViews<N> tv, const __grid_constant__ TileScenes<NS> sc,
+    uint32_t *__restrict__ queue, uint32_t ntiles, uint32_t nwarps,
+    uint32_t *__restrict__ steps_out, uint32_t *__restrict__ mip_out,
+    unsigned long long *__restrict__ total, unsigned long long *__restrict__ counters) {
+  __shared__ float4 tf[NS][256];
+  for (uint32_t k = 0; k < (NS > 1 ? sc.n : 1u); k++)
+    for (uint32_t i = threadIdx.x; i < 256u; i += blockDim.x) {
+      const uchar4 u = sc.lut[k][i];
+      tf[k][i] = make_float4((float)u.x, (float)u.y, (float)u.z, (float)u.w);
+    }
+  __syncthreads();
+  uint32_t vi = 0;
+  while (true) {
+    uint32_t t = 0;
+    if ((threadIdx.x & 31u) == 0u) t = atomicAdd(queue, 1u);
+    t = __shfl_sync(kFull, t, 0);
+    if (t >= ntiles) break;
+    // tiles are taken in order, so the view index only moves forward
+    if (N > 1)
+      while (vi + 1u < tv.n && tv.v[vi + 1u].tile_begin <= t) vi++;
+    const DevView &v = tv.v[N > 1 ? vi : 0u];
+    const uint32_t si = NS > 1 ? v.scene : 0u;
+    const DevScene &s = sc.s[si];
+    uint32_t tx, ty;
+    tile_ray(v, t - v.tile_begin, threadIdx.x & 31u, 0u, tx, ty);
+    RayResult r;
+    r.steps = r.n_tf = r.n_grad = r.n_walk = 0u;
+    if (tx < v.grid_w && ty < v.grid_h) {
+      const bool half = (v.pc.view_flags & R3D_VIEW_HALF) != 0u;
+      const uint32_t px = half ? tx * 2u : tx, py = half ? ty * 2u : ty;
+      const ViewConst vc = view_const<PATH>(v.pc, s);
+      march<PATH, MODE, FAST, COUNT>(v.pc, s, vc, tf[si], px, py, r);
+      store_ray<MODE>(v, px, py, r, steps_out, mip_out);
+    }
+    // work counters per tile: one atomic per 32 rays, nothing kept live
+    // across the march
+    if (total) {
+      uint32_t sum = r.steps;
+      for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
+      if ((threadIdx.x & 31u) == 0u && sum) atomicAdd(total, (unsigned long long)sum);
+    }
+    if (COUNT) {
+      uint32_t v4[4] = {r.steps, r.n_tf, r.n_grad, r.n_walk};
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        uint32_t sum = v4[k];
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
+        if ((threadIdx.x & 31u) == 0u && sum) atomicAdd(counters + k, (unsigned long long)sum);
+      }
+    }
+  }
+  // the last warp to retire resets the counters for the next launch: every
+  // other warp took its last tile before it counted itself out
+  if ((threadIdx.x & 31u) == 0u) {
+    __threadfence();
+    if (atomicAdd(queue + 1, 1u) == nwarps - 1u) {
+      atomicExch(queue, 0u);
+      atomicExch(queue + 1, 0u);
+    }
+  }
+}
+
+template <int PATH, int MODE, bool FAST, bool COUNT, uint32_t N, uint32_t NS>
+static cudaError_t launch_tn(const TilesLaunch &L, cudaStream_t st) {
+  auto kern = k_raycast_tiles<PATH, MODE, FAST, COUNT, N, NS>;
+  uint32_t blocks = L.blocks;
+  if (!blocks) {
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 128, 0);
+    if (e != cudaSuccess) return e;
+    blocks = (uint32_t)(per > 0 ? per : 1) * (uint32_t)sms;
+  }
+  const uint32_t cap = (L.ntiles + 3u) / 4u;  // no more warps than tiles
+  blocks = blocks < cap ? blocks : (cap ? cap : 1u);
+  TileViews<N> tv;
+  memcpy(tv.v, L.views, sizeof(DevView) * L.nviews);
+  tv.n = L.nviews;
+  TileScenes<NS> sc;
+  for (uint32_t k = 0; k < L.nscenes; k++) {
+    sc.s[k] = L.scenes[k];
+    sc.lut[k] = L.luts[k];
+  }
+  sc.n = L.nscenes;
+  kern<<<blocks, 128, 0, st>>>(tv, sc, L.queue, L.ntiles, blocks * 4u, L.steps, L.mip, L.total,
+                               L.counters);
+  return cudaGetLastError();
+}
+
+template <int PATH, int MODE, bool FAST, bool COUNT>
+static cudaError_t launch_tt(const TilesLaunch &L, cudaStream_t st) {
+  if (L.nscenes > 1u) return launch_tn<PATH, MODE, FAST, COUNT, kMaxBatchViews, kMaxScenes>(L, st);
+  if (L.nviews == 1u) return launch_tn<PATH, MODE, FAST, COUNT, 1, 1>(L, st);
+  return launch_tn<PATH, MODE, FAST, COUNT, kMaxBatchViews, 1>(L, st);
+}
+
+template <int PATH, int MODE, bool FAST>
+static cudaError_t launch_tc(const TilesLaunch &L, cudaStream_t st) {
+  return L.counters ? launch_tt<PATH, MODE, FAST, true>(L, st)
+                    : launch_tt<PATH, MODE, FAST, false>(L, st);
+}
+
+template <int PATH>
+static cudaError_t launch_tm(const TilesLaunch &L, cudaStream_t st) {
+  switch (L.mode) {
+    case R3D_MODE_FULL:
+      return L.fast ? launch_tc<PATH, R3D_MODE_FULL, true>(L, st)
+                    : launch_tc<PATH, R3D_MODE_FULL, false>(L, st);
+    case R3D_MODE_MIP: return launch_tc<PATH, R3D_MODE_MIP, false>(L, st);
+    case R3D_MODE_DEPTH: return launch_tc<PATH, R3D_MODE_DEPTH, false>(L, st);
+    case R3D_MODE_HEATMAP: return launch_tc<PATH, R3D_MODE_HEATMAP, false>(L, st);
+    case R3D_MODE_RAYDIR: return launch_tc<PATH, R3D_MODE_RAYDIR, false>(L, st);
+    default: return launch_tc<PATH, R3D_MODE_FLAT, false>(L, st);
+  }
+}
+
 template <int PATH, int MODE, bool FAST, bool COUNT, int UNROLL>
 static cudaError_t launch_pt(const PersistLaunch &L, const DevScene &s, cudaStream_t st) {
   k_raycast_persist<PATH, MODE, FAST, COUNT, UNROLL><<<L.blocks, 128, 0, st>>>(
@@ -240,6 +396,11 @@ cudaError_t persist_path<R3D_FWD_PATH>(const PersistLaunch &L, const DevScene &s
 }
 
 template <>
+cudaError_t tiles_path<R3D_FWD_PATH>(const TilesLaunch &L, cudaStream_t st) {
+  return launch_tm<R3D_FWD_PATH>(L, st);
+}
+
+template <>
 int persist_occupancy<R3D_FWD_PATH>(uint32_t mode, bool fast, uint32_t unroll) {
   // occupancy of the instantiation that persist_path picks
   constexpr int P = R3D_FWD_PATH;
@@ -269,6 +430,17 @@ cudaError_t launch_persist(const PersistLaunch &L, const DevScene &s, cudaStream
     case PATH_LOD_BRICKS: return persist_path<PATH_LOD_BRICKS>(L, s, st);
     case PATH_SHARD: return persist_path<PATH_SHARD>(L, s, st);
     default: return persist_path<PATH_CUBE>(L, s, st);
+  }
+}
+
+cudaError_t launch_tiles(const TilesLaunch &L, cudaStream_t st) {
+  switch (L.path) {
+    case PATH_VSLAB: return tiles_path<PATH_VSLAB>(L, st);
+    case PATH_CLIP: return tiles_path<PATH_CLIP>(L, st);
+    case PATH_SLAB: return tiles_path<PATH_SLAB>(L, st);
+    case PATH_LOD_BRICKS: return tiles_path<PATH_LOD_BRICKS>(L, st);
+    case PATH_SHARD: return tiles_path<PATH_SHARD>(L, st);
+    default: return tiles_path<PATH_CUBE>(L, st);
   }
 }
 

@@ -15,7 +15,8 @@ struct DevView {
   uint32_t grid_w, grid_h;  // dispatch grid (half-resolution views: halved)
   uint32_t sup_x;       // 8x8-tile supertiles per grid row
   uint32_t tile_begin;  // index of the view's first tile in the launch
-  uint32_t pad[2];
+  uint32_t scene;       // whole-tile launches: index of the view's scene
+  uint32_t pad;
 };
 
 struct PersistLaunch {
@@ -23,7 +24,10 @@ struct PersistLaunch {
   uint32_t nviews;       // <= kMaxBatchViews
   uint32_t ntiles;
   const uchar4 *lut;
-  uint32_t *queue;  // tile counter, zero at launch
+  // lane refill (tiles false): one tile counter, zero at launch.  Whole
+  // tiles (tiles true): the tile counter and a counter of retired warps,
+  // zero at launch; the last warp to retire sets both back to zero.
+  uint32_t *queue;
   uint32_t refill_min, shape, unroll;
   uint32_t *steps, *mip;
   unsigned long long *total, *counters;
@@ -48,7 +52,32 @@ inline uint32_t view_tiles(DevView &v, uint32_t shape) {
   return v.sup_x * sup_y * 64u;
 }
 
+// A whole-tile launch: warps take whole 8x4 tiles (shape 0 numbering) of
+// views that may sample different scenes.  The views and scenes are host
+// copies passed to the kernel by value as its launch parameters.
+constexpr uint32_t kMaxScenes = 4;
+struct TilesLaunch {
+  const DevView *views;  // host array; DevView::scene indexes scenes
+  uint32_t nviews;       // <= kMaxBatchViews
+  uint32_t ntiles;
+  const DevScene *scenes;  // host array of nscenes (<= kMaxScenes)
+  const uchar4 *const *luts;  // per scene
+  uint32_t nscenes;
+  // the tile counter and a counter of retired warps, zero at launch; the
+  // last warp to retire sets both back to zero
+  uint32_t *queue;
+  uint32_t *steps, *mip;
+  unsigned long long *total, *counters;
+  uint32_t blocks;  // 0: the occupancy limit on every SM
+  uint32_t mode;
+  bool fast;
+  int path;
+};
+
 cudaError_t launch_persist(const PersistLaunch &L, const DevScene &s, cudaStream_t st);
+cudaError_t launch_tiles(const TilesLaunch &L, cudaStream_t st);
+template <int PATH>
+cudaError_t tiles_path(const TilesLaunch &L, cudaStream_t st);
 int persist_blocks_per_sm(int path, uint32_t mode, bool fast, uint32_t unroll);
 // Per-path halves of the two above (each defined in its own object).
 template <int PATH>

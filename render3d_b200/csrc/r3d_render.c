@@ -52,7 +52,22 @@ struct r3d_renderer {
   /* overlay atlases loaded (bit k: atlas k) and the flattened bake's pick */
   uint32_t ovl_loaded;
   int sv_use_overlay, sv_regtap, sv_pick;
+  /* pane cache (vkbackend.c:7066-7159): the layout hash of the last
+   * multi-view frame, each pane's input hash when it was last drawn, and
+   * the scene generation, bumped by every call that changes what a view
+   * samples; R3D_NO_PANE_CACHE=1 turns the cache off */
+  uint64_t layout_key, pane_key[R3D_MAX_VIEWS], scene_gen;
+  int pane_cache_off;
 };
+
+/* FNV-1a step over a 64-bit word, as the reference's pane hashes fold it */
+static uint64_t fnv(uint64_t k, uint64_t v) { return (k ^ v) * 1099511628211ull; }
+
+/* The scene (volume, caches, TF, quality, cutoff, sections, atlases) changed:
+ * cached panes must be drawn again. */
+static void touched(r3d_renderer *r) {
+  if (r) r->scene_gen++;
+}
 
 static uint64_t now_ns(void) {
   struct timespec ts;
@@ -92,6 +107,8 @@ int r3d_create(SDL_Window *win, const r3d_config *cfg, r3d_renderer **out) {
   if (!r) return -1;
   r->w = cfg->headless_w;
   r->h = cfg->headless_h;
+  const char *pc = getenv("R3D_NO_PANE_CACHE");
+  r->pane_cache_off = pc && *pc == '1';
   int dev = 0;
   cudaGetDevice(&dev);
   if (r3d_cuda_create(dev, &r->ctx) != R3D_OK) {
@@ -151,20 +168,24 @@ void r3d_destroy(r3d_renderer *r) {
 
 int r3d_upload_volume(r3d_renderer *r, const r3d_volume_desc *d, const uint8_t *voxels) {
   if (!r) return -1;
+  touched(r);
   return report(r, "upload_volume", r3d_cuda_upload_volume(r->ctx, d, voxels));
 }
 
 int r3d_set_transfer(r3d_renderer *r, const uint8_t rgba[256][4]) {
   if (!r) return -1;
+  touched(r);
   return report(r, "set_transfer", r3d_cuda_set_transfer(r->ctx, rgba));
 }
 
 void r3d_set_quality(r3d_renderer *r, uint32_t quality) {
+  touched(r);
   if (r) report(r, "set_quality", r3d_cuda_set_quality(r->ctx, quality));
 }
 
 int r3d_set_alpha_cutoff(r3d_renderer *r, float cutoff) {
   if (!r) return -1;
+  touched(r);
   return report(r, "set_alpha_cutoff", r3d_cuda_set_alpha_cutoff(r->ctx, cutoff));
 }
 
@@ -173,6 +194,7 @@ struct r3d_cuda_ctx *r3d_renderer_cuda(r3d_renderer *r) { return r ? r->ctx : NU
 int r3d_bricks_begin_volume(r3d_renderer *r, const r3d_volume_desc *d, const uint8_t *voxels,
                             uint32_t nlev, uint32_t min_max) {
   if (!r) return -1;
+  touched(r);
   int rc = r3d_cuda_bricks_build(r->ctx, d, voxels, nlev, min_max);
   if (rc != R3D_OK) return report(r, "bricks_begin_volume", rc);
   r->bricks = 1;
@@ -185,6 +207,7 @@ int r3d_bricks_begin_volume(r3d_renderer *r, const r3d_volume_desc *d, const uin
 int r3d_bricks_begin_shard(r3d_renderer *r, const uint8_t *voxels, uint32_t edge,
                            uint32_t pool_bpa) {
   if (!r) return -1;
+  touched(r);
   if (pool_bpa && pool_bpa < edge / 128u) {
     fprintf(stderr, "r3d: bricks_begin_shard: a single-level shard is resident whole; a pool "
                     "smaller than the volume streams as an LOD cache (r3d_bricks_begin_stream)\n");
@@ -201,6 +224,7 @@ int r3d_bricks_begin_shard(r3d_renderer *r, const uint8_t *voxels, uint32_t edge
 
 int r3d_bricks_end(r3d_renderer *r) {
   if (!r) return -1;
+  touched(r);
   r->bricks = 0;
   r->brick_mode = 0;
   r->ovl_loaded = 0;
@@ -257,6 +281,7 @@ int r3d_frame_views(r3d_renderer *r, const r3d_frame_params *views, uint32_t nvi
                     (v->viewport[0] == 0u || v->viewport[0] == r->w) &&
                     (v->viewport[1] == 0u || v->viewport[1] == r->h) && r->h >= 256u;
   r->nbands = 0;
+  uint32_t drawn = 0;
   if (whole) {
     /* row bands (multiples of 8 dispatch rows), band k > 0 on band stream
      * k - 1, which starts after this frame's begin event; the context's
@@ -278,15 +303,64 @@ int r3d_frame_views(r3d_renderer *r, const r3d_frame_params *views, uint32_t nvi
     for (uint32_t j = 1; j < k; j++)
       if (cudaStreamWaitEvent(stream, r->band_ev[j], 0) != cudaSuccess) return -1;
     r->nbands = k;
-  } else {
+    drawn = nviews;
+  } else if (nviews == 1u && v->view_org == 0u) {
+    /* one view at the origin draws every pixel of its region each frame
+     * (the reference's region-upscale path: no clear, no pane cache) */
     int rc = r3d_cuda_raycast_fwd(r->ctx, views, nviews, r->offscreen, r->w, r->h, NULL, stream);
     if (rc != R3D_OK) return report(r, "frame", rc);
+    drawn = 1;
+  } else {
+    /* pane cache (vkbackend.c:7066-7159): a frame of several views, or of
+     * one view away from the origin, keeps the offscreen between frames;
+     * the regions no view covers are cleared only when the layout changes,
+     * and a view is drawn only when its parameters (all but the jitter
+     * seed frame_index) or the scene changed since it was drawn; with
+     * R3D_NO_PANE_CACHE=1 every view is drawn and the offscreen cleared
+     * each frame */
+    const int cache = !r->pane_cache_off;
+    uint64_t lay = 1469598103934665603ull ^ nviews;
+    for (uint32_t k = 0; k < nviews; k++) {
+      lay = fnv(lay, views[k].view_org);
+      lay = fnv(lay, views[k].viewport[0]);
+      lay = fnv(lay, views[k].viewport[1]);
+    }
+    lay = fnv(fnv(lay, r->w), r->h);
+    if (lay != r->layout_key || !cache) {
+      static const uint8_t clear[4] = {13, 13, 15, 255}; /* (0.05, 0.05, 0.06, 1) */
+      int rc = r3d_cuda_fill_rgba(r->ctx, r->offscreen, (size_t)r->w * r->h, clear, stream);
+      if (rc != R3D_OK) return report(r, "frame", rc);
+      r->layout_key = lay;
+      memset(r->pane_key, 0, sizeof r->pane_key);
+    }
+    r3d_frame_params todo[R3D_MAX_VIEWS];
+    for (uint32_t k = 0; k < nviews; k++) {
+      if (cache) {
+        r3d_frame_params hp = views[k];
+        hp.frame_index = 0;
+        const uint8_t *hb = (const uint8_t *)&hp;
+        uint64_t key = 1469598103934665603ull;
+        for (size_t i = 0; i < sizeof hp; i++) key = fnv(key, hb[i]);
+        key = fnv(key, r->scene_gen);
+        if (key == 0) key = 1;
+        if (r->pane_key[k] == key) continue; /* unchanged: keep its pixels */
+        r->pane_key[k] = key;
+      }
+      todo[drawn++] = views[k];
+    }
+    if (drawn) {
+      int rc = r3d_cuda_raycast_fwd(r->ctx, todo, drawn, r->offscreen, r->w, r->h, NULL, stream);
+      if (rc != R3D_OK) {
+        memset(r->pane_key, 0, sizeof r->pane_key); /* nothing drawn is cached */
+        return report(r, "frame", rc);
+      }
+    }
   }
   if (cudaEventRecord(r->ev_end[slot], stream) != cudaSuccess) return -1;
   r->ev_used[slot] = 1;
   if (st) {
     st->cpu_record_ns = now_ns() - t0;
-    st->panes_drawn = nviews;
+    st->panes_drawn = drawn;
   }
   r->slot = (slot + 1u) % FRAMES_IN_FLIGHT;
   return 0;
@@ -328,6 +402,7 @@ int r3d_read_frame(r3d_renderer *r, uint8_t *rgba, uint32_t *w, uint32_t *h) {
 /* ---- tiled slab (render.h:22-33) ---- */
 
 int r3d_slab_init(r3d_renderer *r, const r3d_slab_desc *d) {
+  touched(r);
   if (!r || !d || !d->nx || !d->ny || !d->nz || d->wz < 4u || d->wz > d->nz) return -1;
   r->slab = *d;
   r->slab_src = NULL;
@@ -335,6 +410,7 @@ int r3d_slab_init(r3d_renderer *r, const r3d_slab_desc *d) {
 }
 
 int r3d_slab_window(r3d_renderer *r, const r3d_volume *src, uint32_t z0) {
+  touched(r);
   if (!r || !r->slab.wz || !src || !src->voxels || src->nx != r->slab.nx ||
       src->ny != r->slab.ny || src->nz != r->slab.nz)
     return -1;
@@ -357,12 +433,14 @@ void r3d_slab_params(const r3d_renderer *r, r3d_frame_params *p) {
 /* ---- clipmap (render.h:35-41) ---- */
 
 int r3d_clip_begin_volume(r3d_renderer *r, const r3d_volume *src, uint32_t depth_max) {
+  touched(r);
   if (!r || !src || !src->voxels) return -1;
   r3d_volume_desc d = {src->nx, src->ny, src->nz, 128u, 1.0f};
   return report(r, "clip_begin", r3d_cuda_clip_build(r->ctx, &d, src->voxels, depth_max));
 }
 
 int r3d_clip_frame(r3d_renderer *r, double fx, double fy, uint64_t z0, r3d_frame_params *p) {
+  touched(r);
   if (!r) return -1;
   return report(r, "clip_frame", r3d_cuda_clip_frame(r->ctx, fx, fy, z0, p));
 }
@@ -371,6 +449,7 @@ int r3d_clip_frame(r3d_renderer *r, double fx, double fy, uint64_t z0, r3d_frame
 
 int r3d_bricks_begin_stream(r3d_renderer *r, const r3d_volume_desc *d, const uint8_t *voxels,
                             uint32_t nlev, uint32_t nslots) {
+  touched(r);
   if (!r) return -1;
   int rc = r3d_cuda_stream_begin(r->ctx, d, voxels, nlev, nslots);
   if (rc != R3D_OK) return report(r, "bricks_begin_stream", rc);
@@ -401,6 +480,7 @@ void r3d_bricks_stream(r3d_renderer *r, const float eye[3], const float fwd[3], 
   if (report(r, "bricks_stream", r3d_cuda_stream_update(r->ctx, &v, &st)) == 0) {
     r->stream_last = st;
     r->stream_uploaded += st.uploaded;
+    if (st.uploaded) touched(r); /* views sample the new bricks */
   }
 }
 
@@ -429,6 +509,7 @@ void r3d_bricks_stream_submit(r3d_renderer *r, uint32_t budget) {
   if (report(r, "bricks_stream_submit", r3d_cuda_stream_submit(r->ctx, budget, &st)) == 0) {
     r->stream_last = st;
     r->stream_uploaded += st.uploaded;
+    if (st.uploaded) touched(r); /* views sample the new bricks */
   }
 }
 
@@ -468,14 +549,17 @@ static int atlas_attach(r3d_renderer *r, uint32_t which, const r3d_label_src *sr
 }
 
 int r3d_bricks_labels(r3d_renderer *r, const r3d_label_src *src) {
+  touched(r);
   return atlas_attach(r, 2u, src, "bricks_labels");
 }
 
 void r3d_bricks_labels_sync(r3d_renderer *r, uint32_t budget) {
+  touched(r);
   if (r) report(r, "bricks_labels_sync", r3d_cuda_bricks_atlas_sync(r->ctx, 2u, budget, NULL));
 }
 
 int r3d_bricks_regatlas(r3d_renderer *r, const r3d_label_src *src) {
+  touched(r);
   return atlas_attach(r, 3u, src, "bricks_regatlas");
 }
 
@@ -483,6 +567,7 @@ int r3d_bricks_regatlas(r3d_renderer *r, const r3d_label_src *src) {
  * call only observes it; here the round runs within the call (the
  * reference's own fallback when the worker is missing) */
 void r3d_bricks_regatlas_sync(r3d_renderer *r, uint32_t budget) {
+  touched(r);
   if (!r) return;
   uint32_t n = 0;
   if (report(r, "bricks_regatlas_sync", r3d_cuda_bricks_atlas_sync(r->ctx, 3u, budget, &n)) == 0 &&
@@ -491,20 +576,24 @@ void r3d_bricks_regatlas_sync(r3d_renderer *r, uint32_t budget) {
 }
 
 void r3d_bricks_regatlas_detach(r3d_renderer *r) {
+  touched(r);
   if (r) r3d_cuda_bricks_atlas_detach(r->ctx, 3u);
 }
 
 void r3d_bricks_postfilter(r3d_renderer *r, uint32_t mode, float amount, uint32_t targets) {
+  touched(r);
   if (r) report(r, "bricks_postfilter", r3d_cuda_bricks_postfilter(r->ctx, mode, amount, targets));
 }
 
 void r3d_bricks_refilter(r3d_renderer *r) {
+  touched(r);
   /* a no-op without a streamed LOD cache, as the reference's without one */
   if (r && r->streaming) report(r, "bricks_refilter", r3d_cuda_bricks_refilter(r->ctx));
 }
 
 int r3d_bricks_overlay_volume(r3d_renderer *r, uint32_t which, const r3d_volume_desc *d,
                               const uint8_t *voxels) {
+  touched(r);
   if (!r) return -1;
   int rc = r3d_cuda_bricks_overlay_build(r->ctx, which, d, voxels);
   if (rc != R3D_OK) return report(r, "bricks_overlay", rc);
@@ -516,6 +605,7 @@ int r3d_bricks_overlay_volume(r3d_renderer *r, uint32_t which, const r3d_volume_
 /* ---- virtual slab (render.h:161-184) ---- */
 
 int r3d_vslab_begin_volume(r3d_renderer *r, const r3d_vslab_desc *d, const uint8_t *voxels) {
+  touched(r);
   if (!r || !d || !voxels) return -1;
   r3d_volume_desc vd = {d->nx, d->ny, d->nz, 128u, 1.0f};
   return report(r, "vslab_begin",
@@ -524,6 +614,7 @@ int r3d_vslab_begin_volume(r3d_renderer *r, const r3d_vslab_desc *d, const uint8
 
 void r3d_vslab_frame(r3d_renderer *r, double fx, double fy, int64_t z0, uint32_t budget,
                      r3d_frame_params *p) {
+  touched(r);
   if (r) report(r, "vslab_frame", r3d_cuda_vslab_frame(r->ctx, fx, fy, z0, budget, p, NULL));
 }
 
@@ -556,12 +647,14 @@ uint32_t r3d_vslab_resident_pending(const r3d_renderer *r) {
 
 int r3d_surf_begin(r3d_renderer *r, uint32_t w, uint32_t h, const float *coords_rgba,
                    const float *normals_rgba) {
+  touched(r);
   if (!r) return -1;
   return report(r, "surf_begin", r3d_cuda_surf_begin(r->ctx, w, h, coords_rgba, normals_rgba));
 }
 
 int r3d_surf_swap(r3d_renderer *r, uint32_t w, uint32_t h, const float *coords_rgba,
                   const float *normals_rgba, float sx, float sy) {
+  touched(r);
   if (!r || !r->surf_w) return -1;
   /* new grids, the window re-made with the new scale: the next _window
    * call bakes everything, as in the reference */
@@ -574,6 +667,7 @@ int r3d_surf_swap(r3d_renderer *r, uint32_t w, uint32_t h, const float *coords_r
 
 int r3d_surfvol_begin(r3d_renderer *r, uint32_t w, uint32_t h, uint32_t layers,
                       uint32_t nback, float sx, float sy) {
+  touched(r);
   if (!r) return -1;
   int rc = r3d_cuda_surfvol_begin(r->ctx, w, h, layers, nback, sx, sy);
   if (rc != R3D_OK) return report(r, "surfvol_begin", rc);
@@ -588,6 +682,7 @@ void r3d_surfvol_window(r3d_renderer *r, double u0, double v0, float step, float
   if (!r || !r->surf_w) return;
   const float w[4] = {(float)u0, (float)v0, step, zoff0};
   if (r->surf_baked && !memcmp(w, r->surf_win, sizeof w)) return; /* unchanged */
+  touched(r); /* the flattened view samples fresh texels */
   if (report(r, "surfvol_window", r3d_cuda_surfvol_window(r->ctx, u0, v0, step, zoff0)) == 0) {
     memcpy(r->surf_win, w, sizeof w);
     r->surf_baked = 1;
@@ -600,16 +695,19 @@ void r3d_surfvol_visible(r3d_renderer *r, uint32_t x0, uint32_t y0, uint32_t z0,
 }
 
 void r3d_surfvol_mark(r3d_renderer *r) {
+  touched(r);
   if (r) report(r, "surfvol_mark", r3d_cuda_surfvol_mark(r->ctx));
 }
 
 void r3d_surfvol_overlay_enable(r3d_renderer *r, bool enable) {
+  touched(r);
   if (!r) return;
   r->sv_use_overlay = enable;
   surf_pick(r);
 }
 
 void r3d_surfvol_regtap(r3d_renderer *r, bool on) {
+  touched(r);
   /* vkbackend.c:5154-5169: a no-op without a surface volume, or to turn
    * the tap on without a registration atlas */
   if (!r || !r->surf_w || (on && !(r->ovl_loaded & 8u))) return;
@@ -619,12 +717,14 @@ void r3d_surfvol_regtap(r3d_renderer *r, bool on) {
 
 int r3d_surfvol_inkpred(r3d_renderer *r, const float *pred, uint32_t w, uint32_t h, float g0u,
                         float g0v, float px_per_grid) {
+  touched(r);
   if (!r || !r->surf_w || !pred || !w || !h) return -1;
   return report(r, "surfvol_inkpred",
                 r3d_cuda_surfvol_inkpred(r->ctx, pred, w, h, g0u, g0v, px_per_grid));
 }
 
 void r3d_surfvol_inkpred_clear(r3d_renderer *r) {
+  touched(r);
   if (r && r->surf_w)
     report(r, "surfvol_inkpred_clear", r3d_cuda_surfvol_inkpred(r->ctx, NULL, 0, 0, 0, 0, 0));
 }
@@ -634,11 +734,13 @@ void r3d_surfvol_params(const r3d_renderer *r, r3d_frame_params *p) {
 }
 
 int r3d_surfmask(r3d_renderer *r, const uint8_t *m, uint32_t w, uint32_t h) {
+  touched(r);
   if (!r || !m || !w || !h) return -1;
   return report(r, "surfmask", r3d_cuda_surfmask(r->ctx, m, w, h));
 }
 
 void r3d_surfmask_clear(r3d_renderer *r) {
+  touched(r);
   if (r) report(r, "surfmask_clear", r3d_cuda_surfmask(r->ctx, NULL, 0, 0));
 }
 
