@@ -48,6 +48,11 @@ WORKLOAD = "scroll phantom 1024^3 u8, 128^3 bricks x 4 LOD levels, 1920x1080 ful
 # `python bench.py --profile 6` (orbit phases 2/120 and 3/120).
 FWD_DRAM_TRAFFIC_BYTES = 240.9e6
 METRIC = "raycast Gsamples/s & fps @1024^3 1080p; fwd+bwd Gsamples/s vs plain, same GPU"
+# Issue of the same launches in that capture: smsp__inst_executed.sum over
+# (SMs x 4 schedulers x sm cycles elapsed), and smsp__thread_inst_executed.sum
+# over the launches' samples (None until captured)
+ISSUE_FRAC = None
+THREAD_INST_PER_SAMPLE = None
 
 
 def measured_peaks() -> tuple[float, str]:
@@ -332,7 +337,33 @@ def fwd_bwd_bench(rb, ctx, torch, local: int, steps: int, adam_steps: int) -> di
             lossN = loss
     torch.cuda.synchronize()
     adam_s = time.perf_counter() - t0
-    return {"workload": "256^3 FP32 density (phantom/255 + N(0,10/255)), 64 orbit views 256x256, "
+    # the plain forward on the same 64 views: the u8 phantom (the clean
+    # density's bytes) as a cube volume at level 0, FLAT compositing, the 64
+    # views as 256x256 panes of one 2048x2048 image in one call
+    pv = []
+    for i, v in enumerate(views):
+        q = v.copy()
+        q.mode = rb.MODE_FLAT
+        q.view_org = (w * (i % 8)) | ((w * (i // 8)) << 16)
+        pv.append(q)
+    ctx.upload_volume(rb.phantom(n, seed=SEED))
+    pimg = torch.zeros((8 * w, 8 * w, 4), dtype=torch.uint8, device=dev)
+    ptot = torch.zeros(1, dtype=torch.int64, device=dev)
+    for _ in range(3):
+        ctx.raycast(pv, 8 * w, 8 * w, out=pimg, stream=ctx.stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(steps):
+        ctx.raycast(pv, 8 * w, 8 * w, out=pimg, total=ptot, stream=ctx.stream)
+    e1.record(st)
+    torch.cuda.synchronize()
+    pms = e0.elapsed_time(e1) / steps
+    plain = {"ms_per_step": pms,
+             "gsamples_per_s": float(ptot.item()) / steps / (pms * 1e-3) / 1e9,
+             "workload": "the same 64 views, u8 phantom as a cube volume, level 0, FLAT"}
+    return {"plain_same_views": plain,
+            "workload": "256^3 FP32 density (phantom/255 + N(0,10/255)), 64 orbit views 256x256, "
                         "step 0.5, L2 loss, tape of 64 contributions per ray (checkpoints "
                         "every 64 samples beyond it), deterministic",
             "value": samples / (ms * 1e-3) / 1e9, "unit": "Gsamples/s", "ms_per_step": ms,
@@ -383,9 +414,11 @@ def batch_requests(rb, lut, rng, bm_scroll: int, bm_slab: int, slab_shape):
 
 
 def batch_bench(rb, torch, local: int, ctx, reps: int) -> dict:
-    """Batched heterogeneous views (64 requests) over two brick caches, each
-    planned as one batch, autotuned, captured into a CUDA graph and timed by
-    graph replay."""
+    """Batched heterogeneous views (64 requests) over two brick caches -- the
+    1024^3 scroll cache and a 3072x3072x96 slab cache -- planned as ONE batch
+    over both scenes, autotuned, captured into a CUDA graph and timed by
+    graph replay.  The whole-tile schedule drains every request of both
+    caches in one launch (one kernel node in the graph)."""
     dev = f"cuda:{local}"
     lut = rb.scroll_ramp_tf()
     slab_shape = (3072, 3072, 96)
@@ -398,38 +431,78 @@ def batch_bench(rb, torch, local: int, ctx, reps: int) -> dict:
     rng = np.random.default_rng(SEED)
     scroll_views, slab_views = batch_requests(rb, lut, rng, ctx.brick_mode, sctx.brick_mode,
                                               slab_shape)
-    out = {"requests": len(scroll_views) + len(slab_views), "batches": []}
-    total_ms, total_samples = 0.0, 0.0
-    for c, views, name in ((ctx, scroll_views, "1024^3 cache: 16 persp 1080p + 24 ortho panes"),
-                           (sctx, slab_views, "slab cache: 24 windows 3072x3072x32")):
-        imgs = [torch.zeros((v.viewport[1], v.viewport[0], 4), dtype=torch.uint8, device=dev)
-                for v in views]
-        b = rb.Batch(c, views, imgs)
-        sched, tune_ms = b.autotune(reps=2)
-        tot = torch.zeros(1, dtype=torch.int64, device=dev)
-        b.capture(total=tot, stream=c.stream)
-        torch.cuda.synchronize()
-        samples = float(tot.item())
-        st = torch.cuda.ExternalStream(c.stream, device=local)
+    views = scroll_views + slab_views
+    scenes = [ctx] * len(scroll_views) + [sctx] * len(slab_views)
+    imgs = [torch.zeros((v.viewport[1], v.viewport[0], 4), dtype=torch.uint8, device=dev)
+            for v in views]
+    b = rb.Batch(ctx, views, imgs, scenes=scenes)
+    sched, tune_ms = b.autotune(reps=2)
+    # every candidate's time per launch, for the record
+    cands = {}
+    for name, sc in (("grid", dict(persistent=0)), ("whole_tiles", dict(persistent=2))):
+        b.set_schedule(**sc)
+        b.launch(stream=ctx.stream)
+        st = torch.cuda.ExternalStream(ctx.stream, device=local)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(st)
         for _ in range(reps):
-            b.replay(stream=c.stream)
+            b.launch(stream=ctx.stream)
         e1.record(st)
         torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / reps
-        rays = sum(v.viewport[0] * v.viewport[1] for v in views)
-        out["batches"].append({"views": name, "schedule": sched, "autotune_ms": tune_ms,
-                               "ms_per_launch": ms, "samples": samples, "rays": rays,
-                               "gsamples_per_s": samples / (ms * 1e-3) / 1e9})
-        total_ms += ms
-        total_samples += samples
-        b.close()
-        del imgs
+        cands[name] = e0.elapsed_time(e1) / reps
+    b.set_schedule(**sched)
+    tot = torch.zeros(1, dtype=torch.int64, device=dev)
+    b.capture(total=tot, stream=ctx.stream)
+    torch.cuda.synchronize()
+    samples = float(tot.item())
+    st = torch.cuda.ExternalStream(ctx.stream, device=local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(reps):
+        b.replay(stream=ctx.stream)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    rays = sum(v.viewport[0] * v.viewport[1] for v in views)
+    out = {"requests": len(views),
+           "views": "16 persp 1080p + 24 ortho panes 960x540 over the 1024^3 cache, 24 slab "
+                    "windows 3072x3072x32 over the 3072x3072x96 cache, one batch",
+           "schedule": sched, "autotune_ms": tune_ms,
+           "kernel_launches_per_replay": 1 if sched["persistent"] == 2 else len(views),
+           "ms_per_launch_by_schedule": cands, "ms_per_batch": ms, "samples": samples,
+           "rays": rays, "value": samples / (ms * 1e-3) / 1e9, "unit": "Gsamples/s"}
+    b.close()
+    del imgs
     sctx.close()
-    out["ms_per_batch"] = total_ms
-    out["value"] = total_samples / (total_ms * 1e-3) / 1e9
-    out["unit"] = "Gsamples/s"
+    return out
+
+
+def noalloc_bench(rb, torch, ctx, lut, img, frames: int) -> dict:
+    """The orbit through r3d_cuda_raycast_fwd_noalloc (no allocation per
+    call; a persistent kernel with its scratch in a static device array)
+    beside r3d_cuda_raycast_fwd, per-frame CUDA events on the same stream."""
+    import ctypes as C
+    st = torch.cuda.ExternalStream(ctx.stream)
+    out = {}
+    for name, sched in (("lane_refill", dict()), ("whole_tiles", dict(persistent=2))):
+        ctx.set_schedule(**sched)
+
+        def frame(i):
+            arr = (rb.FrameParams * 1)(orbit_params(rb, lut, i, ctx.brick_mode))
+            rc = rb.lib.r3d_cuda_raycast_fwd_noalloc(ctx.h, arr, 1, img.data_ptr(), W, H,
+                                                     C.c_void_p(ctx.stream))
+            assert rc == 0, rb.lib.r3d_cuda_last_error(ctx.h)
+        for i in range(10):
+            frame(i)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for i in range(frames):
+            frame(i)
+        e1.record(st)
+        torch.cuda.synchronize()
+        out[name] = {"ms_per_frame": e0.elapsed_time(e1) / frames}
+    ctx.set_schedule()
     return out
 
 
@@ -567,12 +640,21 @@ def run_ours(args) -> None:
         ctx.raycast(orbit_params(rb, lut, i, bm), W, H, out=img, total=total,
                     counters=counters, stream=ctx.stream)
 
-    # untimed counting pass over the same frames: algorithmic work per frame
+    # untimed counting pass over the same frames: algorithmic work per frame,
+    # and the slots each frame reads (compulsory bytes)
     cnt = torch.zeros(4, dtype=torch.int64, device=f"cuda:{local}")
+    bits = torch.zeros((info["nslots"] + 31) // 32, dtype=torch.int32, device=f"cuda:{local}")
+    ctx.set_slot_trace(bits)
+    touched = []
     for i in range(Wm, Wm + K):
+        bits.zero_()
         frame(i, counters=cnt)
+        touched.append(int(np.unpackbits(bits.cpu().numpy().view(np.uint8)).sum()))
+    ctx.set_slot_trace(None)
     torch.cuda.synchronize()
     counts = cnt.cpu().numpy().astype(np.float64)
+    slots_read = float(np.mean(touched))
+    l2_gbs = ctx.l2_read_probe(48 << 20, 40)
 
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     # clocks are sampled across the warm-up and the timed frames
@@ -629,6 +711,8 @@ def run_ours(args) -> None:
     shard = shard_bench(rb, torch, local, vol, lut, ORBIT_FRAMES * 2)
     overlays = overlay_bench(rb, ctx, lut, torch, stream, total, img, ORBIT_FRAMES * 2)
 
+    noalloc = noalloc_bench(rb, torch, ctx, lut, img, ORBIT_FRAMES)
+
     bt = None
     if not args.no_batch:
         bt = batch_bench(rb, torch, local, ctx, reps=5)
@@ -637,6 +721,7 @@ def run_ours(args) -> None:
     if not args.no_fwd_bwd:
         fb = fwd_bwd_bench(rb, ctx, torch, local, steps=20, adam_steps=100)
         fb["ratio_vs_plain"] = fb["value"] / value
+        fb["ratio_vs_plain_same_views"] = fb["value"] / fb["plain_same_views"]["gsamples_per_s"]
 
     peak, peak_kind = measured_peaks()
     alg = algorithmic_bytes(counts, W * H * K)
@@ -671,12 +756,26 @@ def run_ours(args) -> None:
                             "unit": "GB/s", "frac": achieved / peak,
                             "traffic": FWD_DRAM_TRAFFIC_BYTES,
                             "peak_kind": peak_kind,
-                            "algorithmic_bytes_per_frame": alg / K},
+                            "algorithmic_bytes_per_frame": alg / K,
+                            # the same algorithmic bytes against the L2 read
+                            # bandwidth measured by this run's L2-resident probe
+                            "l2_peak_gbs": l2_gbs, "l2_frac": achieved / l2_gbs,
+                            # unique slots a frame reads (counting pass), as
+                            # 2 MiB u8 bricks and as this layout's bytes (8 MiB
+                            # quad words + 4 KiB block maxima per slot)
+                            "slots_read_per_frame": slots_read,
+                            "compulsory_hbm_bytes": slots_read * (2 << 20),
+                            "compulsory_frac": slots_read * (2 << 20) / (ms_max / K * 1e-3)
+                            / 1e9 / peak,
+                            "compulsory_layout_bytes": slots_read * ((8 << 20) + 4096),
+                            "issue_frac": ISSUE_FRAC,
+                            "thread_inst_per_sample": THREAD_INST_PER_SAMPLE},
                "modes": modes,
                "shard": shard,
                "overlays": overlays,
                "fwd_bwd": fb,
                "batch": bt,
+               "noalloc": noalloc,
                "gpu_launches": K,
                "clocks": clk.summary(),
                "cpu_baseline": cpu,

@@ -456,6 +456,12 @@ typedef struct r3d_cuda_schedule {
   uint32_t unroll;
   uint32_t blocks_per_sm;
   uint32_t shade_group;
+  /* 1: one-thread-per-ray launches of LOD-brick views in FULL or MIP mode
+   * without overlays, auxiliary outputs or row ranges run the TMA-staged
+   * kernel instead: blocks of 8x8 Morton ray tiles that copy the slot box
+   * their next samples fall in (32 x 17 x 17 u8 texels) into shared memory
+   * with cp.async.bulk.tensor, and sample it from there.  0: off. */
+  uint32_t staging;
 } r3d_cuda_schedule;
 
 int r3d_cuda_set_schedule(r3d_cuda_ctx *ctx, const r3d_cuda_schedule *sched);
@@ -596,6 +602,20 @@ int r3d_cuda_raycast_bwd(r3d_cuda_ctx *ctx, const r3d_cuda_diff_scene *scene,
                          void *stream);
 
 /* --- diagnostics ----------------------------------------------------------- */
+
+/* Slot trace of counting launches (those given aux->counters) of the LOD
+ * brick path: bit s of the device bitmap `bits` (nslots bits, zeroed by the
+ * caller) is set when a sample reads slot s's voxels; NULL turns it off.
+ * The benchmark's compulsory-bytes figure (unique bricks a frame reads);
+ * plain launches never test it.  No counterpart in the reference. */
+int r3d_cuda_set_slot_trace(r3d_cuda_ctx *ctx, uint32_t *bits);
+
+/* Read bandwidth of an L2-resident buffer of `bytes` (>= 1 MiB; pick it
+ * well inside the 126 MB L2) swept `passes` times through L2 by every SM,
+ * in GB/s from CUDA events: the L2 peak the raycast's algorithmic bytes are
+ * compared with (its footprint is reused through L1 and L2).  Allocates
+ * and frees its buffer; no counterpart in the reference. */
+int r3d_cuda_l2_read_probe(r3d_cuda_ctx *ctx, size_t bytes, uint32_t passes, float *gbs);
 
 /* Evaluates the raycast's log2, exp2, pow(x, y) and x^24 on the device for n
  * inputs (host pointers); out receives 4 floats per input in that order.

@@ -77,7 +77,8 @@ class Schedule(C.Structure):
     """r3d_cuda_schedule: forward launch scheduling (results never change)."""
     _fields_ = [("persistent", C.c_uint32), ("refill_min", C.c_uint32),
                 ("tile_shape", C.c_uint32), ("unroll", C.c_uint32),
-                ("blocks_per_sm", C.c_uint32), ("shade_group", C.c_uint32)]
+                ("blocks_per_sm", C.c_uint32), ("shade_group", C.c_uint32),
+                ("staging", C.c_uint32)]
 
 
 class SceneRequest(C.Structure):
@@ -268,6 +269,8 @@ def _load() -> C.CDLL:
         "r3d_cuda_last_kernel_ns": (I, [P, C.POINTER(C.c_uint64)]),
         "r3d_cuda_fmath_eval": (I, [P, P, P, P, U32]),
         "r3d_cuda_set_schedule": (I, [P, C.POINTER(Schedule)]),
+        "r3d_cuda_l2_read_probe": (I, [P, C.c_size_t, U32, C.POINTER(F)]),
+        "r3d_cuda_set_slot_trace": (I, [P, P]),
         "r3d_cuda_fill_rgba": (I, [P, P, C.c_size_t, P, P]),
         "r3d_cuda_raycast_fwd_noalloc": (I, [P, P, U32, P, U32, U32, P]),
         "r3d_cuda_diff_forward": (I, [P, C.POINTER(DiffScene), P, U32, P, P, P]),
@@ -935,10 +938,11 @@ class Context:
         return out
 
     def set_schedule(self, persistent: int = 0, refill_min: int = 16, tile_shape: int = 0,
-                     unroll: int = 1, blocks_per_sm: int = 0, shade_group: int = 0) -> None:
+                     unroll: int = 1, blocks_per_sm: int = 0, shade_group: int = 0,
+                     staging: int = 0) -> None:
         self._check(lib.r3d_cuda_set_schedule(
             self.h, C.byref(Schedule(persistent, refill_min, tile_shape, unroll, blocks_per_sm,
-                                     shade_group))))
+                                     shade_group, staging))))
 
     def schedule(self) -> dict:
         sc = Schedule()
@@ -950,6 +954,16 @@ class Context:
         arr = (Request * len(views))(*[Request(v, _ptr(im)) for v, im in zip(views, images)])
         self._check(lib.r3d_cuda_raycast_batch(self.h, arr, len(views), _ptr(total) or None,
                                                stream or None))
+
+    def set_slot_trace(self, bits=None) -> None:
+        """Counting launches mark the slots they read in bits (device u32)."""
+        self._check(lib.r3d_cuda_set_slot_trace(self.h, _ptr(bits) if bits is not None else None))
+
+    def l2_read_probe(self, nbytes: int = 48 << 20, passes: int = 40) -> float:
+        """GB/s of an L2-resident read sweep (r3d_cuda_l2_read_probe)."""
+        g = C.c_float()
+        self._check(lib.r3d_cuda_l2_read_probe(self.h, nbytes, passes, C.byref(g)))
+        return g.value
 
     def last_kernel_ns(self) -> int:
         ns = C.c_uint64()
@@ -987,7 +1001,8 @@ class Batch:
 
     def set_schedule(self, **kw) -> None:
         sc = Schedule(kw.get("persistent", 1), kw.get("refill_min", 16), kw.get("tile_shape", 0),
-                      kw.get("unroll", 1), kw.get("blocks_per_sm", 0), kw.get("shade_group", 0))
+                      kw.get("unroll", 1), kw.get("blocks_per_sm", 0), kw.get("shade_group", 0),
+                      kw.get("staging", 0))
         self.ctx._check(lib.r3d_cuda_batch_set_schedule(self.h, C.byref(sc)))
 
     def schedule(self) -> dict:

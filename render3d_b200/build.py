@@ -44,7 +44,7 @@ C_FLAGS = ["-O2", "-std=c2x", "-D_GNU_SOURCE", "-fPIC", "-ffp-contract=off", "-W
 CU_SOURCES = ["r3d_ctx.cu", "r3d_fwd.cu", "r3d_persist.cu", "r3d_noalloc.cu", "r3d_diff.cu",
               "r3d_batch.cu", "r3d_phantom.cu", "r3d_diag.cu", "r3d_shard.cu", "r3d_overlay.cu",
               "r3d_stream.cu", "r3d_slab.cu", "r3d_clip.cu", "r3d_vslab.cu", "r3d_surf.cu",
-              "r3d_postfilter.cu"]
+              "r3d_postfilter.cu", "r3d_staged.cu"]
 # sources compiled once more per sampling path (-DR3D_FWD_PATH=p), so the
 # paths' raycast kernels compile in parallel
 PER_PATH = {"r3d_fwd.cu", "r3d_persist.cu"}

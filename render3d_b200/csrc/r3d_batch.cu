@@ -19,7 +19,7 @@ struct r3d_cuda_batch {
   std::vector<uint32_t> scene_of;
   r3d_cuda_ctx *scenes[kMaxScenes] = {};
   uint32_t nscenes = 0;
-  r3d_cuda_schedule sched = {1u, 16u, 0u, 1u, 0u, 0u};
+  r3d_cuda_schedule sched = {1u, 16u, 0u, 1u, 0u, 0u, 0u};
   // lane refill (batches of one scene): per tile shape, device view tables
   // (views grouped by path and mode)
   DevView *dviews[3] = {nullptr, nullptr, nullptr};
@@ -192,7 +192,7 @@ extern "C" int r3d_cuda_batch_set_schedule(r3d_cuda_batch *b, const r3d_cuda_sch
   if (b && sc && sc->persistent == 1u && b->nscenes > 1u)
     return batch_fail(b, R3D_E_UNSUPPORTED, "batch_set_schedule: lane refill needs a batch of "
                                             "one scene");
-  if (!b || !sc || sc->persistent > 2u || sc->refill_min < 1u || sc->refill_min > 32u ||
+  if (!b || !sc || sc->persistent > 2u || sc->staging > 1u || sc->refill_min < 1u || sc->refill_min > 32u ||
       sc->tile_shape > 2u || (sc->unroll != 1u && sc->unroll != 2u) || sc->shade_group > 32u || sc->blocks_per_sm > 32u)
     return batch_fail(b, R3D_E_INVALID, "batch_set_schedule: bad schedule");
   b->sched = *sc;
@@ -328,12 +328,12 @@ extern "C" int r3d_cuda_batch_autotune(r3d_cuda_batch *b, uint32_t reps, r3d_cud
   cudaSetDevice(c->device);
   cudaStream_t st = c->stream;
   std::vector<r3d_cuda_schedule> cands;
-  for (uint32_t shade : {0u, 4u, 8u, 16u}) cands.push_back({0u, 16u, 0u, 1u, 0u, shade});
+  for (uint32_t shade : {0u, 4u, 8u, 16u}) cands.push_back({0u, 16u, 0u, 1u, 0u, shade, 0u});
   if (b->nscenes == 1u)  // lane refill drains one scene
     for (uint32_t shape = 0; shape < 3; shape++)
       for (uint32_t refill : {8u, 16u, 24u})
-        for (uint32_t unroll : {1u, 2u}) cands.push_back({1u, refill, shape, unroll, 0u, 0u});
-  cands.push_back({2u, 16u, 0u, 1u, 0u, 0u});  // whole 8x4 tiles from one queue
+        for (uint32_t unroll : {1u, 2u}) cands.push_back({1u, refill, shape, unroll, 0u, 0u, 0u});
+  cands.push_back({2u, 16u, 0u, 1u, 0u, 0u, 0u});  // whole 8x4 tiles from one queue
   const r3d_cuda_schedule keep = b->sched;
   float bms = 1e30f;
   r3d_cuda_schedule bsc = keep;

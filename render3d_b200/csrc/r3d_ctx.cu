@@ -208,6 +208,7 @@ r3d::DevScene r3d_cuda_ctx::scene() const {
   s.status = status;
   s.alpha_cutoff = alpha_cutoff;
   s.tf_zero_t = tf_zero_t;
+  s.slot_bits = slot_bits;
   return s;
 }
 
@@ -400,6 +401,13 @@ int r3d_cuda_set_transfer(r3d_cuda_ctx *c, const uint8_t rgba[256][4]) {
 int r3d_cuda_set_quality(r3d_cuda_ctx *c, uint32_t quality) {
   if (!c || quality >= R3D_QUALITY_COUNT) return fail(c, R3D_E_INVALID, "set_quality: %u", quality);
   c->quality = quality;
+  return R3D_OK;
+}
+
+int r3d_cuda_set_slot_trace(r3d_cuda_ctx *c, uint32_t *bits) {
+  if (!c) return R3D_E_INVALID;
+  if (bits && !is_device_ptr(bits)) return fail(c, R3D_E_INVALID, "set_slot_trace: not device");
+  c->slot_bits = bits;
   return R3D_OK;
 }
 
@@ -996,7 +1004,7 @@ __global__ void k_fill_rgba(uchar4 *__restrict__ img, size_t npix, uchar4 col) {
 extern "C" {
 
 int r3d_cuda_set_schedule(r3d_cuda_ctx *c, const r3d_cuda_schedule *sc) {
-  if (!c || !sc || sc->persistent > 2u || sc->refill_min < 1u || sc->refill_min > 32u ||
+  if (!c || !sc || sc->persistent > 2u || sc->staging > 1u || sc->refill_min < 1u || sc->refill_min > 32u ||
       sc->tile_shape > 2u || (sc->unroll != 1u && sc->unroll != 2u) || sc->shade_group > 32u ||
       sc->blocks_per_sm > 32u)
     return fail(c, R3D_E_INVALID, "set_schedule: bad schedule");

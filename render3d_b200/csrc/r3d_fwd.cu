@@ -98,8 +98,8 @@ __global__ void R3D_FWD_BOUNDS k_raycast(const __grid_constant__ r3d_frame_param
       }
     }
     if (marched) ray_end<MODE>(vc, st, r);
-  } else if (inside) {
-    march<PATH, MODE, FAST, COUNT, OVL>(pc, s, vc, tf, px, py, r);
+  } else {
+    march_warp<PATH, MODE, FAST, COUNT, OVL>(pc, s, vc, tf, px, py, inside, r);
   }
   if (inside) {
     my_tf = r.n_tf;
@@ -224,6 +224,9 @@ cudaError_t launch_view(const r3d_cuda_ctx *c, const r3d_frame_params &pc, uint8
                         cudaStream_t stream, const Rows &rows) {
   if (pc.view_flags & R3D_VIEW_SURF)
     return launch_surf(c, pc, img, out_w, steps, mip_index, stream);
+  if (c->sched.staging && !steps && !mip_index && !counters && rows.row0 == 0u &&
+      rows.row1 == 0xffffffffu && staged_supported(c, pc))
+    return launch_staged(c, pc, img, out_w, total, stream);
   const DevScene s = c->scene();
   const bool fast = c->quality == R3D_QUALITY_FAST;
   // shade_group 0 picks the path's default: grouped shading pays where a

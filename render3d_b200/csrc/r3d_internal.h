@@ -127,6 +127,7 @@ struct r3d_cuda_ctx {
   uint8_t lut_host[256][4];
   float tf_zero_t = -1.0f;
 
+  uint32_t *slot_bits = nullptr;  // r3d_cuda_set_slot_trace
   uint32_t quality = R3D_QUALITY_FULL;
   float alpha_cutoff = 0.98f;
   uint32_t *status = nullptr;
@@ -166,7 +167,7 @@ struct r3d_cuda_ctx {
   // forward scheduling and the view-table ring of persistent launches:
   // slot k holds one call's views (pinned host copy + device copy) and its
   // tile counters; ring_ev[k] completes once the slot's upload has run
-  r3d_cuda_schedule sched = {0u, 16u, 0u, 1u, 0u, 0u};
+  r3d_cuda_schedule sched = {0u, 16u, 0u, 1u, 0u, 0u, 0u};
   static constexpr int kRing = 4;
   r3d::DevView *ring_host = nullptr;
   r3d::DevView *ring_dev = nullptr;
@@ -209,6 +210,12 @@ cudaError_t launch_path(const r3d_frame_params &pc, const DevScene &s, bool fast
 // Flattened-segment view (view_flags R3D_VIEW_SURF) into a device image.
 cudaError_t launch_surf(const r3d_cuda_ctx *c, const r3d_frame_params &pc, uint8_t *img,
                         uint32_t out_w, uint32_t *steps, uint32_t *mip, cudaStream_t st);
+
+// The TMA-staged kernel (r3d_staged.cu): whether a view can use it, and its
+// launch into a device image.
+bool staged_supported(const r3d_cuda_ctx *c, const r3d_frame_params &pc);
+cudaError_t launch_staged(const r3d_cuda_ctx *c, const r3d_frame_params &pc, uint8_t *img,
+                          uint32_t out_w, unsigned long long *total, cudaStream_t st);
 
 // Forward launch of one sanitized view into a device image.
 cudaError_t launch_view(const r3d_cuda_ctx *c, const r3d_frame_params &pc, uint8_t *img,

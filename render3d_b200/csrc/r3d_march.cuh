@@ -166,6 +166,8 @@ struct DevScene {
   uint32_t *status;
   float alpha_cutoff;
   float tf_zero_t;  // TF coordinates below this have alpha exactly 0
+  // counting launches: bit s set when slot s's voxels are read (nullptr: off)
+  uint32_t *slot_bits;
 };
 
 struct RayResult {
@@ -424,6 +426,41 @@ __device__ __forceinline__ float tri_slot_q(const uint32_t *__restrict__ g, cons
 
 __device__ __forceinline__ float slot_sample(const DevScene &s, uint32_t slot, const SlotCoord &q) {
   return tri_slot_q(s.br.quad + (size_t)slot * (128u * 128u * 128u), q);
+}
+
+// A box of one slot's bytes staged in shared memory by TMA (the staged
+// kernel, r3d_staged.cu): kBoxX x kBoxY x kBoxZ texels from (bx, by, bz) of
+// slot `slot` (-1: nothing staged), x fastest.
+constexpr uint32_t kBoxX = 32, kBoxY = 17, kBoxZ = 17;
+constexpr uint32_t kBoxBytes = kBoxX * kBoxY * kBoxZ;
+struct StageBox {
+  const uint8_t *data;
+  int slot, bx, by, bz;
+};
+
+// Whether the 2x2x2 texels of a sample (base q, neighbours clamped to the
+// slot as in the quad pool) all lie in the staged box.
+__device__ __forceinline__ bool box_has(const StageBox &b, uint32_t slot, const SlotCoord &q) {
+  const int x1 = q.x0 < 127u ? (int)q.x0 + 1 : 127, y1 = q.y0 < 127u ? (int)q.y0 + 1 : 127,
+            z1 = q.z0 < 127u ? (int)q.z0 + 1 : 127;
+  return (int)slot == b.slot && (int)q.x0 >= b.bx && x1 < b.bx + (int)kBoxX &&
+         (int)q.y0 >= b.by && y1 < b.by + (int)kBoxY && (int)q.z0 >= b.bz &&
+         z1 < b.bz + (int)kBoxZ;
+}
+
+// tri_slot_q on the staged bytes: the same texels, the same lerps in the
+// same order, so the same bits.
+__device__ __forceinline__ float box_sample(const StageBox &b, const SlotCoord &q) {
+  const uint8_t *p =
+      b.data + (((int)q.z0 - b.bz) * (int)kBoxY + ((int)q.y0 - b.by)) * (int)kBoxX + ((int)q.x0 - b.bx);
+  const int dx = q.x0 < 127u ? 1 : 0, dy = q.y0 < 127u ? (int)kBoxX : 0,
+            dz = q.z0 < 127u ? (int)(kBoxX * kBoxY) : 0;
+  const float c00 = lerp_((float)p[0], (float)p[dx], q.fx);
+  const float c10 = lerp_((float)p[dy], (float)p[dy + dx], q.fx);
+  const float c01 = lerp_((float)p[dz], (float)p[dz + dx], q.fx);
+  const float c11 = lerp_((float)p[dz + dy], (float)p[dz + dy + dx], q.fx);
+  const float e0 = lerp_(c00, c10, q.fy), e1 = lerp_(c01, c11, q.fy);
+  return lerp_(e0, e1, q.fz) * kInv255;
 }
 
 // overlay_flags (raycast.slang:45-49): the four slot-parallel atlases
@@ -909,12 +946,11 @@ __device__ __forceinline__ float tap_sample(const DevScene &s, const DevCube &te
   return cube_sample(tex, p, lod);
 }
 
-// Gradient shading (FULL mode, raycast.slang:919-998) and front-to-back
-// compositing (:1015-1017) of a contributing sample, then the step advance
-// (:1020).  Returns false when the opacity cutoff ends the ray.
+// Colour of a contributing sample: the TF colour, gradient shading (FULL
+// mode, raycast.slang:919-998) and the overlay tints (:1000-1014).
 template <int PATH, int MODE, bool FAST, bool COUNT, bool OVL = false>
-__device__ __forceinline__ bool composite_sample(const DevScene &s, const ViewConst &vc,
-                                                 RayState &st, const Pending &q) {
+__device__ __forceinline__ float3 sample_color(const DevScene &s, const ViewConst &vc,
+                                               RayState &st, const Pending &q) {
   constexpr bool kLod = PATH == PATH_LOD_BRICKS;
   constexpr bool kShard = PATH == PATH_SHARD;
   constexpr bool kShaded = MODE == R3D_MODE_FULL;
@@ -1089,15 +1125,66 @@ __device__ __forceinline__ bool composite_sample(const DevScene &s, const ViewCo
       }
     }
   }
-  // front-to-back compositing (raycast.slang:1015-1017)
+  return make_float3(col_r, col_g, col_b);
+}
+
+// Gradient shading and front-to-back compositing (raycast.slang:1015-1017)
+// of a contributing sample, then the step advance (:1020).  Returns false
+// when the opacity cutoff ends the ray.
+template <int PATH, int MODE, bool FAST, bool COUNT, bool OVL = false>
+__device__ __forceinline__ bool composite_sample(const DevScene &s, const ViewConst &vc,
+                                                 RayState &st, const Pending &q) {
+  const float3 col = sample_color<PATH, MODE, FAST, COUNT, OVL>(s, vc, st, q);
   float wgt = (1.0f - st.acc_a) * q.a;
-  st.acc_r = fmaf(wgt, col_r, st.acc_r);
-  st.acc_g = fmaf(wgt, col_g, st.acc_g);
-  st.acc_b = fmaf(wgt, col_b, st.acc_b);
+  st.acc_r = fmaf(wgt, col.x, st.acc_r);
+  st.acc_g = fmaf(wgt, col.y, st.acc_g);
+  st.acc_b = fmaf(wgt, col.z, st.acc_b);
   st.acc_a = st.acc_a + wgt;
   if (st.acc_a >= s.alpha_cutoff) return false;
   st.t = fmaf(vc.dt, q.lod_step, st.t);
   return true;
+}
+
+// Shading later (LOD bricks, FULL mode).  The opacity a ray accumulates, and
+// so its termination and step positions, never depend on sample colours:
+// only the colour sums do, through rgb <- fma(w_i, c_i, rgb) in sample
+// order.  So the march can keep, for each contributing sample, its weight
+// w_i = (1 - A) a, its TF coordinate and its brick position, and leave the
+// shading (six brick taps, normal, lighting) for later.  A warp shades the
+// kept samples of all its rays together once every ray has ended, instead
+// of one or two lanes at a time inside divergent steps, and folds them into
+// the sums in the same order with the same operations: the image is
+// bit-identical.  A ray that keeps kShadeCap samples shades them at once.
+#ifndef R3D_SHADE_CAP
+#define R3D_SHADE_CAP 4
+#endif
+constexpr uint32_t kShadeCap = R3D_SHADE_CAP;
+struct ShadeEntry {
+  float wgt, tt, bx, by, bz, grad_vox;
+  uint32_t slot;
+};
+struct ShadeBuf {
+  ShadeEntry e[kShadeCap];
+  uint32_t n;
+};
+
+template <int PATH, int MODE, bool FAST, bool COUNT>
+__device__ __forceinline__ void shade_flush(const DevScene &s, const ViewConst &vc,
+                                            const float4 *tf, RayState &st, ShadeBuf &sb) {
+#pragma unroll 1
+  for (uint32_t k = 0; k < sb.n; k++) {
+    const ShadeEntry e = sb.e[k];
+    Pending q;
+    q.sm = tf_sample(tf, e.tt);
+    q.slot = e.slot;
+    q.bl = make_float3(e.bx, e.by, e.bz);
+    q.grad_vox = e.grad_vox;
+    const float3 col = sample_color<PATH, MODE, FAST, COUNT>(s, vc, st, q);
+    st.acc_r = fmaf(e.wgt, col.x, st.acc_r);
+    st.acc_g = fmaf(e.wgt, col.y, st.acc_g);
+    st.acc_b = fmaf(e.wgt, col.z, st.acc_b);
+  }
+  sb.n = 0;
 }
 
 // The footprint ratios y for which the step's LOD decisions are known
@@ -1124,9 +1211,11 @@ __device__ __forceinline__ void lod_range(RayState &st, const ViewConst &vc, int
 // opacity cutoff) and kStepCont otherwise.  With DEFER, a sample that needs
 // gradient shading stops before it: the sample is left in pend and
 // kStepShade returned; composite_sample(pend) completes the iteration.
-template <int PATH, int MODE, bool FAST, bool COUNT, bool DEFER = false, bool OVL = false>
+template <int PATH, int MODE, bool FAST, bool COUNT, bool DEFER = false, bool OVL = false,
+          bool LATER = false, bool STAGE = false>
 __device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, const float4 *tf,
-                                        RayState &st, Pending &pend) {
+                                        RayState &st, Pending &pend, ShadeBuf *sb = nullptr,
+                                        const StageBox *box = nullptr) {
   constexpr bool kLod = PATH == PATH_LOD_BRICKS;
   constexpr bool kShard = PATH == PATH_SHARD;
   constexpr bool kSlab = PATH == PATH_SLAB;
@@ -1201,7 +1290,11 @@ __device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, 
         st.t = fmaf(vc.dt, lod_step, t);
         return kStepCont;
       }
-      v = slot_sample(s, b.slot, q);
+      v = STAGE && box_has(*box, b.slot, q) ? box_sample(*box, q) : slot_sample(s, b.slot, q);
+      if (COUNT && s.slot_bits) {  // the unique slots a frame reads (test first: few atomics)
+        const uint32_t m = 1u << (b.slot & 31u);
+        if (!(__ldcg(s.slot_bits + (b.slot >> 5)) & m)) atomicOr(s.slot_bits + (b.slot >> 5), m);
+      }
     }
   } else if (kShard) {
     const DevShard &h = s.sh;
@@ -1312,6 +1405,15 @@ __device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, 
         sm.w = fmaxf(sm.w, rs.w * vc.reg_alpha);
       }
       float a = 1.0f - r3d_powf(1.0f - sm.w, vc.opac_k * lod_step);
+      if (LATER && a > 0.003f) {  // keep the sample; its colour comes later
+        const float wgt = (1.0f - st.acc_a) * a;
+        st.acc_a = st.acc_a + wgt;
+        sb->e[sb->n] = {wgt, tt, b.bl.x, b.bl.y, b.bl.z, b.grad_vox, b.slot};
+        if (++sb->n == kShadeCap) shade_flush<PATH, MODE, FAST, COUNT>(s, vc, tf, st, *sb);
+        if (st.acc_a >= s.alpha_cutoff) return kStepDone;
+        st.t = fmaf(vc.dt, lod_step, t);
+        return kStepCont;
+      }
       if (a > 0.003f) {
         const Pending q = {p, lod, lod_step, a, sm, b.slot, b.bl, b.grad_vox, rs, reg_live};
         if (DEFER && kShaded) {  // shading runs later, grouped across the warp
@@ -1397,6 +1499,41 @@ __device__ __forceinline__ void march(const r3d_frame_params &pc, const DevScene
   while (ray_step<PATH, MODE, FAST, COUNT, false, OVL>(s, vc, tf, st, pend) != kStepDone) {
   }
   ray_end<MODE, OVL>(vc, st, out);
+}
+
+// Whether a kernel instantiation shades later (see shade_flush).
+#ifndef R3D_SHADE_LATER
+#define R3D_SHADE_LATER 1
+#endif
+template <int PATH, int MODE, bool OVL>
+constexpr bool kShadesLater =
+    R3D_SHADE_LATER && PATH == PATH_LOD_BRICKS && MODE == R3D_MODE_FULL && !OVL;
+
+// march() for every lane of a warp (all 32 lanes call it; `inside` says
+// whether the lane has a ray): with shading later, the rays march, the warp
+// reconverges, and the kept samples of all its rays are shaded together.
+template <int PATH, int MODE, bool FAST, bool COUNT = false, bool OVL = false>
+__device__ __forceinline__ void march_warp(const r3d_frame_params &pc, const DevScene &s,
+                                           const ViewConst &vc, const float4 *tf, uint32_t px,
+                                           uint32_t py, bool inside, RayResult &out) {
+  if constexpr (kShadesLater<PATH, MODE, OVL>) {
+    RayState st;
+    Pending pend;
+    ShadeBuf sb;
+    sb.n = 0;
+    const bool marched = inside && ray_begin<PATH, MODE>(pc, s, vc, px, py, st, out);
+    if (marched)
+      while (ray_step<PATH, MODE, FAST, COUNT, false, false, true>(s, vc, tf, st, pend, &sb) !=
+             kStepDone) {
+      }
+    __syncwarp();
+    if (marched) {
+      shade_flush<PATH, MODE, FAST, COUNT>(s, vc, tf, st, sb);
+      ray_end<MODE>(vc, st, out);
+    }
+  } else {
+    if (inside) march<PATH, MODE, FAST, COUNT, OVL>(pc, s, vc, tf, px, py, out);
+  }
 }
 
 }  // namespace r3d

@@ -262,13 +262,12 @@ __global__ void R3D_TILES_BOUNDS k_raycast_tiles(
     tile_ray(v, t - v.tile_begin, threadIdx.x & 31u, 0u, tx, ty);
     RayResult r;
     r.steps = r.n_tf = r.n_grad = r.n_walk = 0u;
-    if (tx < v.grid_w && ty < v.grid_h) {
-      const bool half = (v.pc.view_flags & R3D_VIEW_HALF) != 0u;
-      const uint32_t px = half ? tx * 2u : tx, py = half ? ty * 2u : ty;
-      const ViewConst vc = view_const<PATH>(v.pc, s);
-      march<PATH, MODE, FAST, COUNT>(v.pc, s, vc, tf[si], px, py, r);
-      store_ray<MODE>(v, px, py, r, steps_out, mip_out);
-    }
+    const bool inside = tx < v.grid_w && ty < v.grid_h;
+    const bool half = (v.pc.view_flags & R3D_VIEW_HALF) != 0u;
+    const uint32_t px = half ? tx * 2u : tx, py = half ? ty * 2u : ty;
+    const ViewConst vc = view_const<PATH>(v.pc, s);
+    march_warp<PATH, MODE, FAST, COUNT>(v.pc, s, vc, tf[si], px, py, inside, r);
+    if (inside) store_ray<MODE>(v, px, py, r, steps_out, mip_out);
     // work counters per tile: one atomic per 32 rays, nothing kept live
     // across the march
     if (total) {
