@@ -884,6 +884,7 @@ def run_profile(args) -> None:
     ctx.set_alpha_cutoff(CUTOFF)
     ctx.bricks_build(vol, NLEV)
     img = torch.zeros((H, W, 4), dtype=torch.uint8, device="cuda")
+    ctx.set_schedule(persistent=args.profile_persistent, staging=args.profile_staging)
     for i in range(args.profile):
         ctx.raycast(orbit_params(rb, lut, i, ctx.brick_mode, args.profile_mode), W, H, out=img,
                     stream=ctx.stream)
@@ -992,14 +993,19 @@ def run_sparse(args) -> None:
     torch.cuda.empty_cache()
     out["stream"] = stream_bench(rb, torch, lut)
     out["stream_small_pool"] = stream_bench(rb, torch, lut, nslots=80)
+    # the cache at 35 % residency: 1638 of the pyramid's 4680 bricks resident,
+    # which ones chosen by the pump's view-cone request set (the reference's
+    # residency rule for a pool smaller than the volume), at 3840x2160
+    out["stream_35pct_4k"] = stream_bench(rb, torch, lut, nslots=1638, budget=64, frames=120,
+                                          w=3840, h=2160)
     print(json.dumps(out), flush=True)
 
 
 def stream_bench(rb, torch, lut, nslots: int = 1024, budget: int = 16,
-                 frames: int = 240) -> dict:
+                 frames: int = 240, w: int = W, h: int = H) -> dict:
     """The 2048^3 phantom as a streaming cache: the whole 4-level pyramid in
-    pinned host memory and 1024 device slots (2 GiB); every frame of a
-    1920x1080 orbit runs one pump update (at most 16 bricks copied in) and
+    pinned host memory and nslots device slots (1024: 2 GiB); every frame of
+    a w x h orbit runs one pump update (at most `budget` bricks copied in) and
     renders; wall-clock fps with one synchronize at the end."""
     ctx = rb.Context(0)
     try:
@@ -1011,14 +1017,16 @@ def stream_bench(rb, torch, lut, nslots: int = 1024, budget: int = 16,
         begin_s = time.perf_counter() - t0
         del vol
         torch.cuda.empty_cache()
-        img = torch.zeros((H, W, 4), dtype=torch.uint8, device="cuda")
+        img = torch.zeros((h, w, 4), dtype=torch.uint8, device="cuda")
 
         def frame(i, stats):
-            p = orbit_params(rb, lut, i, ctx.brick_mode)
+            p = rb.orbit_view((i % ORBIT_FRAMES) / ORBIT_FRAMES, w, h, lut,
+                              step_voxels=STEP_VOXELS, frame_index=i)
+            p.brick_mode = ctx.brick_mode
             st = ctx.stream_update(p, budget)
             for k in stats:
                 stats[k] += st[k]
-            ctx.raycast(p, W, H, out=img, stream=ctx.stream)
+            ctx.raycast(p, w, h, out=img, stream=ctx.stream)
         warm = {k: 0 for k in ("desired", "requested", "uploaded", "evicted")}
         for i in range(20):
             frame(i, warm)
@@ -1030,7 +1038,8 @@ def stream_bench(rb, torch, lut, nslots: int = 1024, budget: int = 16,
         torch.cuda.synchronize()
         s = time.perf_counter() - t0
         return {"workload": f"2048^3 streamed: 4680 bricks in pinned host memory, {nslots} device "
-                            f"slots, 1920x1080 orbit, pump budget {budget} bricks per frame",
+                            f"slots, {w}x{h} orbit, pump budget {budget} bricks per frame",
+                "resident_fraction": nslots / 4680,
                 "begin_s": begin_s, "fps": frames / s, "ms_per_frame": 1e3 * s / frames,
                 "bricks_copied_per_frame": stats["uploaded"] / frames,
                 "evicted_per_frame": stats["evicted"] / frames,
@@ -1267,6 +1276,10 @@ def main() -> None:
     ap.add_argument("--profile", type=int, default=0, metavar="N",
                     help="only build the workload and render N orbit frames (for ncu)")
     ap.add_argument("--profile-mode", type=int, default=0)
+    ap.add_argument("--profile-persistent", type=int, default=0,
+                    help="schedule of the --profile frames: 0 grid, 1 lane refill, 2 whole tiles")
+    ap.add_argument("--profile-staging", type=int, default=0,
+                    help="1: the --profile frames run the TMA-staged kernel")
     ap.add_argument("--profile-sections", type=int, default=0, metavar="N",
                     help="only render N frames of each section mode and of flattened views")
     ap.add_argument("--profile-diff", type=int, default=0, metavar="N",

@@ -22,7 +22,7 @@
 namespace r3d {
 
 constexpr uint32_t kStageThreads = 64;
-constexpr uint32_t kWaitLimit = 1u << 22;  // try_wait polls before giving up
+constexpr uint32_t kWaitLimit = 1u << 20;  // try_wait polls before giving up (well under a second)
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
