@@ -15,9 +15,13 @@
  * gradients with respect to every voxel, every LUT entry and the density
  * scale.  With decisions32 set, which samples contribute and where a ray
  * terminates are taken from the FP32 render (of dec_dens / dec_lut when
- * given, so finite differences can hold them fixed), so the FP64 gradient is
- * that of the same piecewise-smooth branch the FP32 kernel differentiates;
- * otherwise the FP64 render decides. */
+ * given, so finite differences can hold them fixed), and so is each sample's
+ * piece of the piecewise-smooth render: its trilinear cell, its TF texel and
+ * whether the TF coordinate and alpha lie inside their clamps.  The FP64
+ * gradient is then that of the same branch and piece the FP32 kernel
+ * differentiates: where a sample sits within rounding of a texel boundary,
+ * FP32 and FP64 arithmetic can pick neighbouring texels, whose slopes differ
+ * by the full LUT step; otherwise the FP64 render decides. */
 #include <math.h>
 #include <omp.h>
 #include <stdlib.h>
@@ -195,15 +199,18 @@ typedef struct samp64 {
   double w8[8];
 } samp64;
 
-static double tri64(const float *g, const uint32_t n[3], const double p[3], uint32_t *idx8,
-                    double *w8) {
+/* FP64 trilinear; cell0 (nullable) forces the base texel of each axis (the
+ * FP32 sample's cell, whose piece of the piecewise-trilinear function is
+ * then differentiated; the weights extend that piece linearly). */
+static double tri64(const float *g, const uint32_t n[3], const double p[3],
+                    const uint32_t *cell0, uint32_t *idx8, double *w8) {
   double t[3], f[3];
   uint32_t i0[3], i1[3];
   for (int a = 0; a < 3; a++) {
     t[a] = p[a] * (double)n[a] - 0.5;
     if (t[a] < 0.0) t[a] = 0.0;
     if (t[a] > (double)(n[a] - 1u)) t[a] = (double)(n[a] - 1u);
-    i0[a] = (uint32_t)t[a];
+    i0[a] = cell0 ? cell0[a] : (uint32_t)t[a];
     f[a] = t[a] - (double)i0[a];
     i1[a] = i0[a] + 1u < n[a] ? i0[a] + 1u : n[a] - 1u;
   }
@@ -221,11 +228,35 @@ static double tri64(const float *g, const uint32_t n[3], const double p[3], uint
   return v;
 }
 
-/* Builds the FP64 sample list of one ray.  decide32: the contributing steps
- * from the FP32 render (rec, nrec); else decided in FP64.  Returns count. */
+/* The FP32 render's pieces at one sample: the trilinear cell, the TF texel
+ * and whether the TF coordinate and alpha are inside their clamps (these
+ * choose the smooth piece of the FP32 function the kernel differentiates). */
+typedef struct piece32 {
+  uint32_t cell[3], texel;
+  int tt_free, alpha_free;
+} piece32;
+
+static void pieces32(const float *dens, const uint32_t n[3], const float *lut, const float p[3],
+                     piece32 *o) {
+  for (int a = 0; a < 3; a++)
+    o->cell[a] = (uint32_t)clampf_(fmaf(p[a], (float)n[a], -0.5f), 0.0f, (float)(n[a] - 1u));
+  const float v = tri32(dens, n, p, NULL, NULL);
+  const float tu = fmaf(v, 256.0f, -0.5f), tt = clampf_(tu, 0.0f, 255.0f);
+  o->texel = (uint32_t)tt;
+  o->tt_free = tu > 0.0f && tu < 255.0f;
+  const uint32_t i1 = o->texel + 1u < 256u ? o->texel + 1u : 255u;
+  const float s3 = lerpf_(lut[o->texel * 4 + 3], lut[i1 * 4 + 3], tt - (float)o->texel);
+  o->alpha_free = s3 > 0.0f && s3 < 1.0f;
+}
+
+/* Builds the FP64 sample list of one ray.  rec (decisions32): the
+ * contributing steps from the FP32 render of (pdens, plut), whose pieces
+ * (pieces32) the FP64 samples also keep; else everything is decided in FP64.
+ * Returns count. */
 static uint32_t ray_samples64(const r3d_frame_params *pc, const float *dens, const uint32_t n[3],
                               const float *lut, double density, float cutoff, uint32_t px,
-                              uint32_t py, const uint32_t *rec, uint32_t nrec, samp64 *out,
+                              uint32_t py, const uint32_t *rec, uint32_t nrec,
+                              const float *pdens, const float *plut, samp64 *out,
                               uint32_t cap, double rgb[3]) {
   uint32_t nmax = n[0] > n[1] ? n[0] : n[1];
   if (n[2] > nmax) nmax = n[2];
@@ -242,17 +273,20 @@ static uint32_t ray_samples64(const r3d_frame_params *pc, const float *dens, con
       steps++;
       int consider = rec ? (ri < nrec && rec[ri] == steps) : 1;
       if (consider) {
-        double p[3] = {(double)fmaf(t, r.dir[0], r.ro[0]), (double)fmaf(t, r.dir[1], r.ro[1]),
-                       (double)fmaf(t, r.dir[2], r.ro[2])};
+        const float p32[3] = {fmaf(t, r.dir[0], r.ro[0]), fmaf(t, r.dir[1], r.ro[1]),
+                              fmaf(t, r.dir[2], r.ro[2])};
+        double p[3] = {(double)p32[0], (double)p32[1], (double)p32[2]};
+        piece32 pc32;
+        if (rec) pieces32(pdens, n, plut, p32, &pc32);
         samp64 s;
-        double v = tri64(dens, n, p, s.idx8, s.w8);
+        double v = tri64(dens, n, p, rec ? pc32.cell : NULL, s.idx8, s.w8);
         int contrib = 0;
         if (rec || !(v < (double)pc->threshold)) {
           double tt = v * 256.0 - 0.5;
-          s.tt_free = tt > 0.0 && tt < 255.0;
+          s.tt_free = rec ? pc32.tt_free : (tt > 0.0 && tt < 255.0);
           if (tt < 0.0) tt = 0.0;
           if (tt > 255.0) tt = 255.0;
-          s.i0 = (uint32_t)tt;
+          s.i0 = rec ? pc32.texel : (uint32_t)tt;
           s.i1 = s.i0 + 1u < 256u ? s.i0 + 1u : 255u;
           s.f = tt - (double)s.i0;
           s.tt = tt;
@@ -261,7 +295,7 @@ static uint32_t ray_samples64(const r3d_frame_params *pc, const float *dens, con
             sv[c] = (double)lut[s.i0 * 4 + c] +
                     s.f * ((double)lut[s.i1 * 4 + c] - (double)lut[s.i0 * 4 + c]);
           double alpha = sv[3] < 0.0 ? 0.0 : (sv[3] > 1.0 ? 1.0 : sv[3]);
-          s.alpha_free = sv[3] > 0.0 && sv[3] < 1.0;
+          s.alpha_free = rec ? pc32.alpha_free : (sv[3] > 0.0 && sv[3] < 1.0);
           s.alpha = alpha;
           s.kk = kk;
           s.kstep = kstep;
@@ -320,7 +354,8 @@ int orc_diff_grad64(const r3d_frame_params *pc, const float *dens, const uint32_
         }
         double rgb[3];
         uint32_t ns = ray_samples64(pc, dens, n, lut, density, cutoff, x, y,
-                                    decisions32 ? rec : NULL, nrec, buf, 4096, rgb);
+                                    decisions32 ? rec : NULL, nrec, dec_dens ? dec_dens : dens,
+                                    dec_lut ? dec_lut : lut, buf, 4096, rgb);
         if (rgb64_out)
           for (int c = 0; c < 3; c++) rgb64_out[pix * 3 + c] = rgb[c];
         const float *g = dl_drgb + pix * 3;

@@ -1503,7 +1503,7 @@ __device__ __forceinline__ void march(const r3d_frame_params &pc, const DevScene
 
 // Whether a kernel instantiation shades later (see shade_flush).
 #ifndef R3D_SHADE_LATER
-#define R3D_SHADE_LATER 1
+#define R3D_SHADE_LATER 0
 #endif
 template <int PATH, int MODE, bool OVL>
 constexpr bool kShadesLater =

@@ -5,8 +5,8 @@
   the unperturbed phantom's render: GPU gradients (voxels, LUT, density
   scale) against the FP64 oracle over all 64 views for both accumulation
   modes, with and without the tape; central finite differences of the GPU
-  forward (h = 1e-2) on 512 seeded voxels, every LUT entry with a gradient
-  and the density scale, against the GPU gradient.
+  forward on 512 seeded voxels (h = 1e-2), every LUT entry with a gradient
+  and the density scale (h = 1e-3), against the GPU gradient.
 * 512^3 FP32 density, 16 orbit views of 512x512 at step 0.25: checkpoint
   intervals K = 32, 64, 128 in atomic and deterministic accumulation, each
   against the FP64 oracle, and deterministic against atomic.  Once with the
@@ -162,12 +162,19 @@ def test_256_64views_finite_differences(rb, ctx, cfg256):
             e.append((g[j], (lp - lm) / float(hi - lo)))
         e = np.array(e)
         assert _rel(e[:, 0], e[:, 1]) < 1e-2  # O(h^2) truncation at h = 1e-2
+        # LUT entries (and the density scale) with h = 1e-3: an entry is shared
+        # by every sample whose density falls in its texel, hundreds per ray in
+        # the air, and a step of 1e-2 moves an air-range alpha (~0.02) by half
+        # its value, far outside the range where the transmittance is
+        # near-linear in it (measured: 4.8 % relative L2 at 1e-2, 0.05 % at
+        # 1e-3)
         lflat = dlut.view(-1)
         gln = gl.view(-1).cpu().numpy()
         e = []
+        hl = 1e-3
         for j in np.nonzero(np.abs(gln) > 0)[0]:
             x = lflat[j].item()
-            hi, lo = np.float32(x + h), np.float32(x - h)
+            hi, lo = np.float32(x + hl), np.float32(x - hl)
             lflat[j] = float(hi)
             lp = loss(dens, dlut)
             lflat[j] = float(lo)
@@ -177,8 +184,8 @@ def test_256_64views_finite_differences(rb, ctx, cfg256):
         e = np.array(e)
         assert len(e) > 500
         assert _rel(e[:, 0], e[:, 1]) < 1e-2
-        s0 = vs[0].density
-        fd = (loss(dens, dlut, s0 + h) - loss(dens, dlut, s0 - h)) / (2 * h)
+        s0 = vs[0].density  # the scale multiplies every sample's opacity exponent
+        fd = (loss(dens, dlut, s0 + hl) - loss(dens, dlut, s0 - hl)) / (2 * hl)
         assert abs(gs.item() - fd) <= 1e-2 * abs(fd)
     finally:
         ctx.set_alpha_cutoff(0.98)
@@ -217,8 +224,9 @@ def test_512_16views_step025_checkpoints(rb, orc, ctx, faint):
                 else:
                     atomic = got
             # deterministic against atomic accumulation of the same interval
-            assert torch.allclose(dets[k][0], atomic[0], rtol=1e-4, atol=1e-7)
-            assert torch.allclose(dets[k][1], atomic[1], rtol=1e-4, atol=1e-6)
+            # (FP32 atomic sums: the same relative L2 bar as against FP64)
+            for x, y in zip(dets[k][:2], atomic[:2]):
+                assert _rel(y.cpu().numpy(), x.cpu().numpy().astype(np.float64)) < 1e-4
         # the interval changes where the backward re-marches, not the bits
         # of the deterministic sums
         assert torch.equal(dets[32][0], dets[128][0]) and torch.equal(dets[32][1], dets[128][1])
