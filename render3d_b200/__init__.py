@@ -1246,9 +1246,11 @@ class Renderer:
 
     def read_frame(self, out=None):
         w, h = C.c_uint32(), C.c_uint32()
-        lib.r3d_read_frame(self.r, None, C.byref(w), C.byref(h))
-        if out is None:
+        if out is None:  # the size first (rgba NULL queries it)
+            lib.r3d_read_frame(self.r, None, C.byref(w), C.byref(h))
             out = np.empty((h.value, w.value, 4), np.uint8)
+        elif out.nbytes < self.w * self.h * 4:
+            raise ValueError("read_frame: the buffer is smaller than the frame")
         self._ok(lib.r3d_read_frame(self.r, _ptr(out), C.byref(w), C.byref(h)),
                  "r3d_read_frame")
         return out
