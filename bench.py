@@ -43,16 +43,15 @@ CUTOFF = 0.99
 STEP_VOXELS = 0.5
 ORBIT_FRAMES = 120
 WORKLOAD = "scroll phantom 1024^3 u8, 128^3 bricks x 4 LOD levels, 1920x1080 full shading"
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_raycast
-# launch of this workload, mean of launches 3 and 4 of one ncu capture of
-# `python bench.py --profile 6` (orbit phases 2/120 and 3/120).
-FWD_DRAM_TRAFFIC_BYTES = 240.9e6
+# One ncu capture (--clock-control none, 1 pass) of `python bench.py
+# --profile 6`, launches 3 and 4 of k_raycast (orbit phases 2/120 and
+# 3/120), the mean per launch of: DRAM bytes (dram__bytes_read.sum +
+# dram__bytes_write.sum), warp instructions (smsp__inst_executed.sum) and
+# thread instructions (smsp__thread_inst_executed.sum).
+FWD_DRAM_TRAFFIC_BYTES = 238.7e6
+FWD_WARP_INST = 310.9e6
+FWD_THREAD_INST = 6.047e9
 METRIC = "raycast Gsamples/s & fps @1024^3 1080p; fwd+bwd Gsamples/s vs plain, same GPU"
-# Issue of the same launches in that capture: smsp__inst_executed.sum over
-# (SMs x 4 schedulers x sm cycles elapsed), and smsp__thread_inst_executed.sum
-# over the launches' samples (None until captured)
-ISSUE_FRAC = None
-THREAD_INST_PER_SAMPLE = None
 
 
 def measured_peaks() -> tuple[float, str]:
@@ -731,6 +730,9 @@ def run_ours(args) -> None:
 
     peak, peak_kind = measured_peaks()
     alg = algorithmic_bytes(counts, W * H * K)
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    clk_sum = clk.summary()
+    sm_hz = (clk_sum["sm_mhz"] or 1965.0) * 1e6
     achieved = alg / (ms * 1e-3) / 1e9
     out = None
     if rank == 0:
@@ -774,8 +776,13 @@ def run_ours(args) -> None:
                             "compulsory_frac": slots_read * (2 << 20) / (ms_max / K * 1e-3)
                             / 1e9 / peak,
                             "compulsory_layout_bytes": slots_read * ((8 << 20) + 4096),
-                            "issue_frac": ISSUE_FRAC,
-                            "thread_inst_per_sample": THREAD_INST_PER_SAMPLE},
+                            # the captured launches' warp instructions over
+                            # the issue slots of this run's frame time (148
+                            # SMs x 4 schedulers x the median SM clock), and
+                            # thread instructions per sample of this run
+                            "issue_frac": FWD_WARP_INST / (sms * 4 * sm_hz * ms_max / K * 1e-3),
+                            "thread_inst_per_sample": FWD_THREAD_INST / (counts[0] / K),
+                            "simt_lanes_per_inst": FWD_THREAD_INST / FWD_WARP_INST},
                "modes": modes,
                "shard": shard,
                "overlays": overlays,
@@ -783,7 +790,7 @@ def run_ours(args) -> None:
                "batch": bt,
                "noalloc": noalloc,
                "gpu_launches": K,
-               "clocks": clk.summary(),
+               "clocks": clk_sum,
                "cpu_baseline": cpu,
                "parity": parity}
         print(json.dumps(out), flush=True)
@@ -1004,15 +1011,20 @@ def run_sparse(args) -> None:
     # residency rule for a pool smaller than the volume), at 3840x2160
     out["stream_35pct_4k"] = stream_bench(rb, torch, lut, nslots=1638, budget=64, frames=120,
                                           w=3840, h=2160)
+    out["fixed_35pct_4k"] = stream_bench(rb, torch, lut, nslots=1638, budget=1638, frames=120,
+                                         w=3840, h=2160, pump_timed=False)
     print(json.dumps(out), flush=True)
 
 
 def stream_bench(rb, torch, lut, nslots: int = 1024, budget: int = 16,
-                 frames: int = 240, w: int = W, h: int = H) -> dict:
+                 frames: int = 240, w: int = W, h: int = H, pump_timed: bool = True) -> dict:
     """The 2048^3 phantom as a streaming cache: the whole 4-level pyramid in
     pinned host memory and nslots device slots (1024: 2 GiB); every frame of
     a w x h orbit runs one pump update (at most `budget` bricks copied in) and
-    renders; wall-clock fps with one synchronize at the end."""
+    renders; wall-clock fps with one synchronize at the end.  pump_timed
+    False: the pump runs over the warm-up frames only, and the timed frames
+    render the cache as it was left (a fixed partial residency, the absent
+    bricks drawn from coarser levels)."""
     ctx = rb.Context(0)
     try:
         ctx.set_transfer(lut)
@@ -1025,13 +1037,14 @@ def stream_bench(rb, torch, lut, nslots: int = 1024, budget: int = 16,
         torch.cuda.empty_cache()
         img = torch.zeros((h, w, 4), dtype=torch.uint8, device="cuda")
 
-        def frame(i, stats):
+        def frame(i, stats, pump=True):
             p = rb.orbit_view((i % ORBIT_FRAMES) / ORBIT_FRAMES, w, h, lut,
                               step_voxels=STEP_VOXELS, frame_index=i)
             p.brick_mode = ctx.brick_mode
-            st = ctx.stream_update(p, budget)
-            for k in stats:
-                stats[k] += st[k]
+            if pump:
+                st = ctx.stream_update(p, budget)
+                for k in stats:
+                    stats[k] += st[k]
             ctx.raycast(p, w, h, out=img, stream=ctx.stream)
         warm = {k: 0 for k in ("desired", "requested", "uploaded", "evicted")}
         for i in range(20):
@@ -1040,11 +1053,12 @@ def stream_bench(rb, torch, lut, nslots: int = 1024, budget: int = 16,
         stats = {k: 0 for k in ("desired", "requested", "uploaded", "evicted")}
         t0 = time.perf_counter()
         for i in range(20, 20 + frames):
-            frame(i, stats)
+            frame(i, stats, pump_timed)
         torch.cuda.synchronize()
         s = time.perf_counter() - t0
         return {"workload": f"2048^3 streamed: 4680 bricks in pinned host memory, {nslots} device "
-                            f"slots, {w}x{h} orbit, pump budget {budget} bricks per frame",
+                            f"slots, {w}x{h} orbit, pump budget {budget} bricks per frame"
+                            + ("" if pump_timed else " over the warm-up only (fixed residency)"),
                 "resident_fraction": nslots / 4680,
                 "begin_s": begin_s, "fps": frames / s, "ms_per_frame": 1e3 * s / frames,
                 "bricks_copied_per_frame": stats["uploaded"] / frames,
