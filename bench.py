@@ -508,6 +508,45 @@ def noalloc_bench(rb, torch, ctx, lut, img, frames: int) -> dict:
     return out
 
 
+def split_views_bench(rb, torch, ctx, lut, frames: int) -> dict:
+    """One 1920x1080 frame split into 4, 16 and 64 views of the same orbit
+    (one r3d_cuda_raycast_fwd call per frame), one thread per ray (a grid
+    launch per view) against the automatic schedule (whole tiles of every
+    view in one launch); per-frame CUDA events on the context's stream."""
+    st = torch.cuda.ExternalStream(ctx.stream)
+    img = torch.zeros((H, W, 4), dtype=torch.uint8, device="cuda")
+    out = {}
+    for cols, rows in ((2, 2), (4, 4), (8, 8)):
+        w, h = W // cols, H // rows
+        seq = []
+        for i in range(frames):
+            vs = []
+            for k in range(cols * rows):
+                p = rb.orbit_view(((i + 7 * k) % ORBIT_FRAMES) / ORBIT_FRAMES, w, h, lut,
+                                  step_voxels=STEP_VOXELS, frame_index=i)
+                p.brick_mode = ctx.brick_mode
+                p.view_org = (w * (k % cols)) | ((h * (k // cols)) << 16)
+                vs.append(p)
+            seq.append(vs)
+        r = {}
+        for name, sched in (("grid", dict(persistent=0)), ("auto", dict())):
+            ctx.set_schedule(**sched)
+            for i in range(5):
+                ctx.raycast(seq[i], W, H, out=img, stream=ctx.stream)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for vs in seq:
+                ctx.raycast(vs, W, H, out=img, stream=ctx.stream)
+            e1.record(st)
+            torch.cuda.synchronize()
+            r[f"{name}_ms_per_frame"] = e0.elapsed_time(e1) / frames
+        r["speedup"] = r["grid_ms_per_frame"] / r["auto_ms_per_frame"]
+        out[f"{cols * rows}x{w}x{h}"] = r
+    ctx.set_schedule()
+    return out
+
+
 def cpu_baseline(rb, orc, ctx, vol_pages, lut, frames: list[int], threads: int) -> dict:
     """The oracle (FP32 CPU restatement of the reference shader) on a bounded
     sample of the same workload: whole 1920x1080 frames of the orbit, timed.
@@ -717,6 +756,7 @@ def run_ours(args) -> None:
     overlays = overlay_bench(rb, ctx, lut, torch, stream, total, img, ORBIT_FRAMES * 2)
 
     noalloc = noalloc_bench(rb, torch, ctx, lut, img, ORBIT_FRAMES)
+    split = split_views_bench(rb, torch, ctx, lut, ORBIT_FRAMES)
 
     bt = None
     if not args.no_batch:
@@ -789,6 +829,7 @@ def run_ours(args) -> None:
                "fwd_bwd": fb,
                "batch": bt,
                "noalloc": noalloc,
+               "split_views": split,
                "gpu_launches": K,
                "clocks": clk_sum,
                "cpu_baseline": cpu,

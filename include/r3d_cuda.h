@@ -440,7 +440,10 @@ int r3d_cuda_raycast_fwd_noalloc(r3d_cuda_ctx *ctx, const r3d_frame_params *view
  * (1 or 2).  persistent = 2: resident warps drain a queue of whole 8x4
  * tiles covering all views of the call (one launch per sampling path and
  * mode), each marching its 32 rays to the end before taking the next tile
- * (refill_min, tile_shape and unroll unused).  blocks_per_sm = resident
+ * (refill_min, tile_shape and unroll unused).  persistent = 3 (automatic,
+ * a context's default): whole tiles for a call with two or more views to
+ * render, one thread per ray for one view (a batch resolves it once, from
+ * its view count).  blocks_per_sm = resident
  * 128-thread blocks per SM of a persistent launch (0: the occupancy
  * limit).  shade_group (FULL mode, one-thread-per-ray launches):
  * n > 0 lets lanes park a sample that needs gradient shading until n lanes

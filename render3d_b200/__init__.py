@@ -937,7 +937,7 @@ class Context:
         self._check(lib.r3d_cuda_fmath_eval(self.h, _ptr(x), _ptr(y), _ptr(out), x.size))
         return out
 
-    def set_schedule(self, persistent: int = 0, refill_min: int = 16, tile_shape: int = 0,
+    def set_schedule(self, persistent: int = 3, refill_min: int = 16, tile_shape: int = 0,
                      unroll: int = 1, blocks_per_sm: int = 0, shade_group: int = 0,
                      staging: int = 0) -> None:
         self._check(lib.r3d_cuda_set_schedule(

@@ -192,10 +192,11 @@ extern "C" int r3d_cuda_batch_set_schedule(r3d_cuda_batch *b, const r3d_cuda_sch
   if (b && sc && sc->persistent == 1u && b->nscenes > 1u)
     return batch_fail(b, R3D_E_UNSUPPORTED, "batch_set_schedule: lane refill needs a batch of "
                                             "one scene");
-  if (!b || !sc || sc->persistent > 2u || sc->staging > 1u || sc->refill_min < 1u || sc->refill_min > 32u ||
+  if (!b || !sc || sc->persistent > 3u || sc->staging > 1u || sc->refill_min < 1u || sc->refill_min > 32u ||
       sc->tile_shape > 2u || (sc->unroll != 1u && sc->unroll != 2u) || sc->shade_group > 32u || sc->blocks_per_sm > 32u)
     return batch_fail(b, R3D_E_INVALID, "batch_set_schedule: bad schedule");
   b->sched = *sc;
+  b->sched.persistent = resolved_persistent(*sc, b->n);  // a batch's view count is fixed
   return R3D_OK;
 }
 

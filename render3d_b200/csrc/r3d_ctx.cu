@@ -889,8 +889,9 @@ int prepare_view(r3d_cuda_ctx *c, const r3d_frame_params &in, uint32_t out_w,
 // Persistent launches for the renderable views of one call: views sharing a
 // sampling path and mode go into one launch (template parameters of the
 // kernel), in order of first appearance.
-static int launch_views_persistent(r3d_cuda_ctx *c, const r3d_frame_params *pcs,
-                                   const int *render, uint32_t nviews, uint8_t *const *imgs,
+static int launch_views_persistent(r3d_cuda_ctx *c, uint32_t persistent,
+                                   const r3d_frame_params *pcs, const int *render,
+                                   uint32_t nviews, uint8_t *const *imgs,
                                    const uint32_t *strides, uint32_t *steps, uint32_t *mip,
                                    unsigned long long *total, unsigned long long *counters,
                                    cudaStream_t st) {
@@ -930,7 +931,7 @@ static int launch_views_persistent(r3d_cuda_ctx *c, const r3d_frame_params *pcs,
     d.img = (uchar4 *)imgs[order[i]];
     d.stride = strides[order[i]];
     d.tile_begin = ntiles[g];
-    ntiles[g] += view_tiles(d, sc.persistent == 2u ? 0u : sc.tile_shape);
+    ntiles[g] += view_tiles(d, persistent == 2u ? 0u : sc.tile_shape);
   }
   R3D_CUDA_TRY(c, cudaMemcpyAsync(dv, hv, sizeof(DevView) * n, cudaMemcpyHostToDevice, st));
   R3D_CUDA_TRY(c, cudaEventRecord(c->ring_ev[k], st));
@@ -939,7 +940,7 @@ static int launch_views_persistent(r3d_cuda_ctx *c, const r3d_frame_params *pcs,
   int dev_sms = 148;
   cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device);
   const DevScene s = c->scene();
-  if (sc.persistent == 2u) {  // whole tiles, the views as launch parameters
+  if (persistent == 2u) {  // whole tiles, the views as launch parameters
     for (uint32_t g = 0; g < ngroups; g++) {
       TilesLaunch T;
       memset(&T, 0, sizeof T);
@@ -1004,7 +1005,7 @@ __global__ void k_fill_rgba(uchar4 *__restrict__ img, size_t npix, uchar4 col) {
 extern "C" {
 
 int r3d_cuda_set_schedule(r3d_cuda_ctx *c, const r3d_cuda_schedule *sc) {
-  if (!c || !sc || sc->persistent > 2u || sc->staging > 1u || sc->refill_min < 1u || sc->refill_min > 32u ||
+  if (!c || !sc || sc->persistent > 3u || sc->staging > 1u || sc->refill_min < 1u || sc->refill_min > 32u ||
       sc->tile_shape > 2u || (sc->unroll != 1u && sc->unroll != 2u) || sc->shade_group > 32u ||
       sc->blocks_per_sm > 32u)
     return fail(c, R3D_E_INVALID, "set_schedule: bad schedule");
@@ -1099,15 +1100,18 @@ int r3d_cuda_raycast_fwd(r3d_cuda_ctx *c, const r3d_frame_params *views, uint32_
   for (uint32_t v = 0; v < nviews; v++)
     any_ovl = any_ovl || (render[v] && ((pcs[v].overlay_flags & kOvlAtlases) ||
                                         (pcs[v].view_flags & R3D_VIEW_SURF)));
-  if (c->sched.persistent && !any_ovl) {
+  uint32_t nrender = 0;
+  for (uint32_t v = 0; v < nviews; v++) nrender += render[v] ? 1u : 0u;
+  const uint32_t persistent = resolved_persistent(c->sched, nrender);
+  if (persistent && !any_ovl) {
     uint8_t *imgs[64];
     uint32_t strides[64];
     for (uint32_t v = 0; v < nviews; v++) {
       imgs[v] = img;
       strides[v] = out_w;
     }
-    int rc = launch_views_persistent(c, pcs, render, nviews, imgs, strides, steps, mip, total,
-                                     counters, st);
+    int rc = launch_views_persistent(c, persistent, pcs, render, nviews, imgs, strides, steps,
+                                     mip, total, counters, st);
     if (rc != R3D_OK) return rc;
   } else {
     for (uint32_t v = 0; v < nviews; v++) {
@@ -1173,9 +1177,12 @@ int r3d_cuda_raycast_batch(r3d_cuda_ctx *c, const r3d_cuda_request *reqs, uint32
     strides[i] = pcs[i].viewport[0];
     any_ovl = any_ovl || (pcs[i].overlay_flags & kOvlAtlases) || (pcs[i].view_flags & R3D_VIEW_SURF);
   }
-  if (c->sched.persistent && !any_ovl)
-    return launch_views_persistent(c, pcs, render, n, imgs, strides, nullptr, nullptr,
-                                   total_steps, nullptr, st);
+  uint32_t nrender = 0;
+  for (uint32_t i = 0; i < n; i++) nrender += render[i] ? 1u : 0u;
+  const uint32_t persistent = resolved_persistent(c->sched, nrender);
+  if (persistent && !any_ovl)
+    return launch_views_persistent(c, persistent, pcs, render, n, imgs, strides, nullptr,
+                                   nullptr, total_steps, nullptr, st);
   for (uint32_t i = 0; i < n; i++) {
     if (!render[i]) continue;
     cudaError_t e = launch_view(c, pcs[i], imgs[i], strides[i], nullptr, nullptr, total_steps,

@@ -116,6 +116,7 @@ extern "C" int r3d_cuda_raycast_fwd_noalloc(r3d_cuda_ctx *c, const r3d_frame_par
     gcount[g]++;
   }
   if (!n) return R3D_OK;
+  const uint32_t persistent = resolved_persistent(sc, n);
   gstart[0] = 0;
   for (uint32_t g = 0; g < ngroups; g++) gstart[g + 1] = gstart[g] + gcount[g];
   uint32_t fill[kNoallocViews] = {0}, ntiles[kNoallocViews] = {0};
@@ -127,7 +128,7 @@ extern "C" int r3d_cuda_raycast_fwd_noalloc(r3d_cuda_ctx *c, const r3d_frame_par
     d.img = (uchar4 *)rgba_out;
     d.stride = out_w;
     d.tile_begin = ntiles[g];
-    ntiles[g] += view_tiles(d, sc.persistent == 2u ? 0u : sc.tile_shape);
+    ntiles[g] += view_tiles(d, persistent == 2u ? 0u : sc.tile_shape);
   }
   // the table and this call's zeroed counters, written on the stream ahead
   // of the raycast launches (a call queued behind an earlier one on the
@@ -143,7 +144,7 @@ extern "C" int r3d_cuda_raycast_fwd_noalloc(r3d_cuda_ctx *c, const r3d_frame_par
   const DevScene s = c->scene();
   for (uint32_t g = 0; g < ngroups; g++) {
     cudaError_t e;
-    if (sc.persistent == 2u) {  // whole tiles: the views travel as launch parameters
+    if (persistent == 2u) {  // whole tiles: the views travel as launch parameters
       TilesLaunch T;
       memset(&T, 0, sizeof T);
       T.views = hv + gstart[g];

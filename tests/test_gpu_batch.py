@@ -157,13 +157,25 @@ def test_whole_tile_schedule(rb, ctx, batch_scene):
         v.viewport[0], v.viewport[1] = 96, 64
         v.view_org = (100 * (i % 2)) | ((70 * (i // 2)) << 16)
     try:
+        ctx.set_schedule(persistent=0)
         want = ctx.raycast(vs, w, h)
         ctx.set_schedule(persistent=2)
         got = ctx.raycast(vs, w, h)
         got2 = ctx.raycast(vs, w, h)
+        # the automatic schedule (the default) takes whole tiles for these
+        # three views and one grid for a call with one
+        ctx.set_schedule()
+        assert ctx.schedule()["persistent"] == 3
+        auto = ctx.raycast(vs, w, h)
+        one = [vs[0].copy()]
+        one[0].view_org = 0
+        one_grid = ctx.raycast(one, w, h)
+        ctx.set_schedule(persistent=0)
+        one_want = ctx.raycast(one, w, h)
     finally:
         ctx.set_schedule()
     assert np.array_equal(got, want) and np.array_equal(got2, want)
+    assert np.array_equal(auto, want) and np.array_equal(one_grid, one_want)
 
 
 def test_raycast_batch(rb, ctx, batch_scene):
@@ -172,7 +184,7 @@ def test_raycast_batch(rb, ctx, batch_scene):
     import torch
     views, refs, steps = batch_scene
     try:
-        for sc in (dict(), dict(persistent=1), dict(persistent=2)):
+        for sc in (dict(), dict(persistent=0), dict(persistent=1), dict(persistent=2)):
             ctx.set_schedule(**sc)
             imgs = _images(views)
             tot = torch.zeros(1, dtype=torch.int64, device="cuda")
