@@ -47,10 +47,12 @@ WORKLOAD = "scroll phantom 1024^3 u8, 128^3 bricks x 4 LOD levels, 1920x1080 ful
 # --profile 6`, launches 3 and 4 of k_raycast (orbit phases 2/120 and
 # 3/120), the mean per launch of: DRAM bytes (dram__bytes_read.sum +
 # dram__bytes_write.sum), warp instructions (smsp__inst_executed.sum) and
-# thread instructions (smsp__thread_inst_executed.sum).
+# thread instructions (smsp__thread_inst_executed.sum); and the samples of
+# those two frames (the counters that `--profile` prints).
 FWD_DRAM_TRAFFIC_BYTES = 238.7e6
 FWD_WARP_INST = 310.9e6
 FWD_THREAD_INST = 6.047e9
+FWD_CAPTURED_SAMPLES = 28.31e6
 METRIC = "raycast Gsamples/s & fps @1024^3 1080p; fwd+bwd Gsamples/s vs plain, same GPU"
 
 
@@ -689,7 +691,9 @@ def run_ours(args) -> None:
     touched = []
     for i in range(Wm, Wm + K):
         bits.zero_()
+        torch.cuda.synchronize()  # the frame runs on the context's stream
         frame(i, counters=cnt)
+        torch.cuda.synchronize()
         touched.append(int(np.unpackbits(bits.cpu().numpy().view(np.uint8)).sum()))
     ctx.set_slot_trace(None)
     torch.cuda.synchronize()
@@ -816,12 +820,14 @@ def run_ours(args) -> None:
                             "compulsory_frac": slots_read * (2 << 20) / (ms_max / K * 1e-3)
                             / 1e9 / peak,
                             "compulsory_layout_bytes": slots_read * ((8 << 20) + 4096),
-                            # the captured launches' warp instructions over
-                            # the issue slots of this run's frame time (148
-                            # SMs x 4 schedulers x the median SM clock), and
-                            # thread instructions per sample of this run
-                            "issue_frac": FWD_WARP_INST / (sms * 4 * sm_hz * ms_max / K * 1e-3),
-                            "thread_inst_per_sample": FWD_THREAD_INST / (counts[0] / K),
+                            # the captured launches' warp instructions per
+                            # sample, times this run's samples per frame,
+                            # over the issue slots of its frame time (148
+                            # SMs x 4 schedulers x the median SM clock); and
+                            # the captured thread instructions per sample
+                            "issue_frac": FWD_WARP_INST / FWD_CAPTURED_SAMPLES * (counts[0] / K)
+                            / (sms * 4 * sm_hz * ms_max / K * 1e-3),
+                            "thread_inst_per_sample": FWD_THREAD_INST / FWD_CAPTURED_SAMPLES,
                             "simt_lanes_per_inst": FWD_THREAD_INST / FWD_WARP_INST},
                "modes": modes,
                "shard": shard,
@@ -943,7 +949,17 @@ def run_profile(args) -> None:
         ctx.raycast(orbit_params(rb, lut, i, ctx.brick_mode, args.profile_mode), W, H, out=img,
                     stream=ctx.stream)
     torch.cuda.synchronize()
-    print("profile frames done:", args.profile)
+    # the work counters of the same frames, from launches after the profiled
+    # ones (samples, TF lookups, shaded samples, page walks per frame)
+    counts = []
+    for i in range(args.profile):
+        cnt = torch.zeros(4, dtype=torch.int64, device="cuda")
+        ctx.raycast(orbit_params(rb, lut, i, ctx.brick_mode, args.profile_mode), W, H, out=img,
+                    counters=cnt, stream=ctx.stream)
+        torch.cuda.synchronize()
+        counts.append([int(x) for x in cnt.cpu()])
+    print(json.dumps({"profile_frames": args.profile, "mode": args.profile_mode,
+                      "counters_per_frame": counts}))
     ctx.close()
 
 

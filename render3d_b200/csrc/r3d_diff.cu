@@ -8,7 +8,9 @@
 // a = 1 - (1 - alpha)^(density * step * lod_step), samples with a <= 0.003
 // ignored, front-to-back compositing with termination at the cutoff, then
 // the background.  The forward kernel writes an FP32 RGB image per view;
-// its arithmetic equals the CPU oracle's bit for bit.
+// its arithmetic equals the CPU oracle's bit for bit.  A sample whose
+// density falls in the TF's leading run of zero-alpha texels (both texels
+// alpha 0) has opacity exactly 0; it is skipped before the TF lookup.
 //
 // The adjoint kernel (one thread per ray) returns the gradients of
 // L = sum(dL/drgb * rgb) with respect to every voxel, every LUT entry and the
@@ -27,8 +29,9 @@
 // atomics; LUT contributions go to a per-block shared-memory table flushed
 // once per block; the density-scale gradient is reduced per warp.  Atomic
 // mode adds FP32 (order-dependent rounding).  Deterministic mode adds
-// fixed-point integers (value * 2^32, rounded, in int64): integer addition
-// is associative, so the result is identical for any execution order.
+// fixed-point integers (value * 2^32, rounded, in int64; mod 2^64 as two
+// 32-bit words in the shared table): integer addition is associative, so
+// the result is identical for any execution order.
 #include <string.h>
 
 #include "r3d_internal.h"
@@ -49,6 +52,7 @@ struct DiffGrid {
   // of its z plane, x1 = min(x + 1, nx - 1) and y1 likewise, so that a
   // trilinear sample reads two float4 instead of eight floats
   const float4 *quad;
+  const uint32_t *zc;  // the TF's first texel with alpha not 0 (256: none)
   uint32_t n[3];
   uint32_t nmax;
   const float *lut;  // 256 x 4
@@ -107,6 +111,7 @@ __device__ __forceinline__ void diff_setup(const r3d_frame_params &pc, const Dif
   r.span = fmaxf((tf - tn) / (4096.0f * r.dt), 1.0f);
 }
 
+
 // One sample: density, TF, opacity.  Fills the trilinear cell for scatters.
 struct DiffSample {
   float v, tt, f, s[4], alpha, a;
@@ -115,8 +120,9 @@ struct DiffSample {
   float fx, fy, fz;
 };
 
-__device__ __forceinline__ void diff_sample(const DiffGrid &g, const DiffRay &r, float t,
-                                            DiffSample &o) {
+// The trilinear cell of the sample at t: corner, strides, fractions.
+__device__ __forceinline__ void diff_cell(const DiffGrid &g, const DiffRay &r, float t,
+                                          DiffSample &o) {
   float p[3] = {fmaf(t, r.dir[0], r.ro[0]), fmaf(t, r.dir[1], r.ro[1]),
                 fmaf(t, r.dir[2], r.ro[2])};
   uint32_t i0[3];
@@ -137,25 +143,43 @@ __device__ __forceinline__ void diff_sample(const DiffGrid &g, const DiffRay &r,
   o.fx = fr[0];
   o.fy = fr[1];
   o.fz = fr[2];
-  const float4 q0 = __ldg(g.quad + o.base), q1 = __ldg(g.quad + o.base + o.sz);
-  const float c00 = lerp_(q0.x, q0.y, fr[0]), c10 = lerp_(q0.z, q0.w, fr[0]);
-  const float c01 = lerp_(q1.x, q1.y, fr[0]), c11 = lerp_(q1.z, q1.w, fr[0]);
-  o.v = lerp_(lerp_(c00, c10, fr[1]), lerp_(c01, c11, fr[1]), fr[2]);
 }
 
-// TF and opacity of a sample (FP32, as the oracle)
-__device__ __forceinline__ void diff_tf(const DiffGrid &g, float k, DiffSample &o) {
+__device__ __forceinline__ void diff_sample(const DiffGrid &g, const DiffRay &r, float t,
+                                            DiffSample &o) {
+  diff_cell(g, r, t, o);
+  const float4 q0 = __ldg(g.quad + o.base), q1 = __ldg(g.quad + o.base + o.sz);
+  const float c00 = lerp_(q0.x, q0.y, o.fx), c10 = lerp_(q0.z, q0.w, o.fx);
+  const float c01 = lerp_(q1.x, q1.y, o.fx), c11 = lerp_(q1.z, q1.w, o.fx);
+  o.v = lerp_(lerp_(c00, c10, o.fy), lerp_(c01, c11, o.fy), o.fz);
+}
+
+// TF coordinate, texels and colour of a sample (FP32, as the oracle)
+__device__ __forceinline__ void diff_tf_color(const float4 *lut, DiffSample &o) {
   o.tt = clamp_(fmaf(o.v, 256.0f, -0.5f), 0.0f, 255.0f);
   o.i0 = (uint32_t)o.tt;
   o.i1 = min(o.i0 + 1u, 255u);
   o.f = o.tt - (float)o.i0;
-  const float4 l0 = __ldg((const float4 *)g.lut + o.i0), l1 = __ldg((const float4 *)g.lut + o.i1);
+  const float4 l0 = lut[o.i0], l1 = lut[o.i1];
   o.s[0] = lerp_(l0.x, l1.x, o.f);
   o.s[1] = lerp_(l0.y, l1.y, o.f);
   o.s[2] = lerp_(l0.z, l1.z, o.f);
   o.s[3] = lerp_(l0.w, l1.w, o.f);
   o.alpha = clamp_(o.s[3], 0.0f, 1.0f);
+}
+
+// TF and opacity of a sample
+__device__ __forceinline__ void diff_tf(const float4 *lut, float k, DiffSample &o) {
+  diff_tf_color(lut, o);
   o.a = 1.0f - r3d_powf(1.0f - o.alpha, k);
+}
+
+// True when both TF texels of density v have alpha 0 (z = the first texel
+// whose alpha is not 0): then alpha = lerp(0, 0, f) = 0, the opacity is
+// 1 - 1^k = 0 and the sample cannot contribute.
+__device__ __forceinline__ bool diff_clear(float v, uint32_t z) {
+  const uint32_t i0 = (uint32_t)clamp_(fmaf(v, 256.0f, -0.5f), 0.0f, 255.0f);
+  return min(i0 + 1u, 255u) < z;
 }
 
 // The quad grid of DiffGrid::quad from the density grid.
@@ -170,19 +194,36 @@ __global__ void k_diff_quads(const float *__restrict__ d, uint32_t nx, uint32_t 
   }
 }
 
+// DiffGrid::zc from the TF (one block).
+__global__ void k_diff_tf_clear(const float *__restrict__ lut, uint32_t *__restrict__ zc) {
+  __shared__ uint32_t z;
+  if (threadIdx.x == 0) z = 256u;
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < 256u; i += blockDim.x)
+    if (__ldg(lut + 4u * i + 3u) != 0.0f) atomicMin(&z, i);
+  __syncthreads();
+  if (threadIdx.x == 0) *zc = z;
+}
+
 // Tape of a training forward: per ray, the first kTape contributing samples
-// (t, accumulated opacity before the sample) and their count.  A backward
-// over the same views and scene walks these in reverse instead of marching
-// the ray again; rays with more contributions take the checkpoint path.
+// and their count.  An entry holds t, the accumulated opacity before the
+// sample, and the sample's density and opacity (x, y, z, w), so that the
+// backward needs neither the density fetch nor the opacity's power again.
+// A backward over the same views and scene walks these in reverse instead
+// of marching the ray again; rays with more contributions take the
+// checkpoint path.
 constexpr uint32_t kTape = 64;
+using TapeEntry = float4;
 
 template <bool TAPE>
 __global__ void __launch_bounds__(128) k_diff_fwd(const DiffView *__restrict__ views,
                                                   const __grid_constant__ DiffGrid g,
                                                   float *__restrict__ rgb,
                                                   unsigned long long *__restrict__ total,
-                                                  float2 *__restrict__ tape,
+                                                  TapeEntry *__restrict__ tape,
                                                   uint32_t *__restrict__ tape_n) {
+  const float4 *lut = (const float4 *)g.lut;
+  const uint32_t zc = __ldg(g.zc);
   const DiffView &vw = views[blockIdx.z];
   const r3d_frame_params &pc = vw.pc;
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
@@ -203,10 +244,10 @@ __global__ void __launch_bounds__(128) k_diff_fwd(const DiffView *__restrict__ v
         steps++;
         DiffSample s;
         diff_sample(g, r, t, s);
-        if (!(s.v < pc.threshold)) {
-          diff_tf(g, k, s);
+        if (!(s.v < pc.threshold) && !diff_clear(s.v, zc)) {
+          diff_tf(lut, k, s);
           if (s.a > 0.003f) {
-            if (TAPE && nc < kTape) tape[ray * kTape + nc] = make_float2(t, acc_a);
+            if (TAPE && nc < kTape) tape[ray * kTape + nc] = make_float4(t, acc_a, s.v, s.a);
             nc++;
             float w = (1.0f - acc_a) * s.a;
             acc_r = fmaf(w, s.s[0], acc_r);
@@ -233,14 +274,71 @@ __global__ void __launch_bounds__(128) k_diff_fwd(const DiffView *__restrict__ v
   }
 }
 
+// x * 2^32 rounded to the nearest int64: the product is exact in FP32 (a
+// power-of-two scale), so converting it directly equals converting
+// (double)x * 2^32
+__device__ __forceinline__ long long fix32(float x) {
+  return __float2ll_rn(x * 4294967296.0f);
+}
+
 // voxel gradient sink: FP32 atomics or 2^32 fixed point
 template <bool DET>
 __device__ __forceinline__ void vox_add(float *gf, unsigned long long *gq, uint32_t i, float x) {
   if (x == 0.0f) return;
   if (DET)
-    atomicAdd(gq + i, (unsigned long long)(long long)__double2ll_rn((double)x * kFix));
+    atomicAdd(gq + i, (unsigned long long)fix32(x));
   else
     atomicAdd(gf + i, x);
+}
+
+// The block's LUT-gradient table in shared memory.  Deterministic sums are
+// kept mod 2^64 as two 32-bit words per entry: the low word takes the low
+// half of each addend, and a carry out of it goes to the high word with the
+// high half, so that every update is two native 32-bit shared atomics.
+struct LutGrad {
+  union {
+    uint32_t w[2048];  // deterministic: low words w[i], high words w[1024 + i]
+    float f[1024];     // FP32 atomics
+  };
+};
+
+template <bool DET>
+__device__ __forceinline__ void lut_add(LutGrad &lg, uint32_t i, float x) {
+  if (DET) {
+    const long long q = fix32(x);
+    if (!q) return;
+    const uint32_t ql = (uint32_t)q, qh = (uint32_t)((unsigned long long)q >> 32);
+    const uint32_t old = atomicAdd(&lg.w[i], ql);
+    const uint32_t h = qh + (old + ql < old ? 1u : 0u);
+    if (h) atomicAdd(&lg.w[1024u + i], h);
+  } else {
+    atomicAdd(&lg.f[i], x);
+  }
+}
+
+template <bool DET>
+__device__ __forceinline__ void lut_clear(LutGrad &lg) {
+  for (uint32_t i = threadIdx.x; i < 1024u; i += blockDim.x) {
+    if (DET) {
+      lg.w[i] = 0u;
+      lg.w[1024u + i] = 0u;
+    } else {
+      lg.f[i] = 0.0f;
+    }
+  }
+}
+
+template <bool DET>
+__device__ __forceinline__ void lut_flush(const LutGrad &lg, float *g_lut,
+                                          unsigned long long *q_lut) {
+  for (uint32_t i = threadIdx.x; i < 1024u; i += blockDim.x) {
+    if (DET) {
+      const unsigned long long q = ((unsigned long long)lg.w[1024u + i] << 32) | lg.w[i];
+      if (q) atomicAdd(q_lut + i, q);
+    } else {
+      if (lg.f[i] != 0.0f) atomicAdd(g_lut + i, lg.f[i]);
+    }
+  }
 }
 
 constexpr int kRing = 64;  // contributing samples remembered by the forward sweep
@@ -267,16 +365,13 @@ __device__ __forceinline__ void bwd_flush(BwdRay &b, float *g_dens, unsigned lon
                  b.cw[c]);
 }
 
-// Adjoint of one contributing sample at t with accumulated opacity acc_a
-// before it, visited in reverse order (suffix colour S <- a c + (1 - a) S).
+// Adjoint of one contributing sample s (density, TF and opacity filled) with
+// accumulated opacity acc_a before it, visited in reverse order (suffix
+// colour S <- a c + (1 - a) S).
 template <bool DET>
-__device__ __forceinline__ void bwd_sample(const DiffGrid &g, const DiffRay &r, float t,
-                                           float acc_a, BwdRay &b, float *s_lut,
-                                           unsigned long long *s_qlut, float *g_dens,
-                                           unsigned long long *q_dens) {
-  DiffSample s;
-  diff_sample(g, r, t, s);
-  diff_tf(g, b.k, s);
+__device__ __forceinline__ void bwd_contrib(const float4 *lut, const DiffSample &s, float acc_a,
+                                            BwdRay &b, LutGrad &lg, float *g_dens,
+                                            unsigned long long *q_dens) {
   const float tprev = 1.0f - acc_a;
   const float dc_r = b.gr * tprev * s.a, dc_g = b.gg * tprev * s.a, dc_b = b.gb * tprev * s.a;
   const float da = b.gr * tprev * (s.s[0] - b.S_r) + b.gg * tprev * (s.s[1] - b.S_g) +
@@ -285,27 +380,25 @@ __device__ __forceinline__ void bwd_sample(const DiffGrid &g, const DiffRay &r, 
   b.S_g = fmaf(s.a, s.s[1] - b.S_g, b.S_g);
   b.S_b = fmaf(s.a, s.s[2] - b.S_b, b.S_b);
   float dalpha = 0.0f;
-  const bool alpha_free = s.s[3] > 0.0f && s.s[3] < 1.0f;
-  if (alpha_free) dalpha = da * b.k * r3d_powf(1.0f - s.alpha, b.k - 1.0f);
-  if (s.alpha < 1.0f)
-    b.g_density += da * (-(1.0f - s.a) * (r3d_log2f(1.0f - s.alpha) * 0.693147181f)) * b.kstep;
+  const bool alpha_free = s.s[3] > 0.0f && s.s[3] < 1.0f;  // implies alpha < 1
+  if (s.alpha < 1.0f) {
+    const float x = 1.0f - s.alpha, l2 = r3d_log2f(x);
+    if (alpha_free) {  // r3d_powf(x, k - 1) with the logarithm shared (x > 0 here)
+      const float y = b.k - 1.0f;
+      dalpha = da * b.k * (y == 0.0f || x == 1.0f ? 1.0f : r3d_exp2f(y * l2));
+    }
+    b.g_density += da * (-(1.0f - s.a) * (l2 * 0.693147181f)) * b.kstep;
+  }
   const float ds[4] = {dc_r, dc_g, dc_b, dalpha};
   const float lf0 = 1.0f - s.f;
-  const float4 l0 = __ldg((const float4 *)g.lut + s.i0);
-  const float4 l1 = __ldg((const float4 *)g.lut + s.i1);
+  const float4 l0 = lut[s.i0];
+  const float4 l1 = lut[s.i1];
   const float dl[4] = {l1.x - l0.x, l1.y - l0.y, l1.z - l0.z, l1.w - l0.w};
   float dvv = 0.0f;
 #pragma unroll
   for (int c = 0; c < 4; c++) {
-    if (DET) {
-      atomicAdd(&s_qlut[s.i0 * 4u + c],
-                (unsigned long long)__double2ll_rn((double)(ds[c] * lf0) * kFix));
-      atomicAdd(&s_qlut[s.i1 * 4u + c],
-                (unsigned long long)__double2ll_rn((double)(ds[c] * s.f) * kFix));
-    } else {
-      atomicAdd(&s_lut[s.i0 * 4u + c], ds[c] * lf0);
-      atomicAdd(&s_lut[s.i1 * 4u + c], ds[c] * s.f);
-    }
+    lut_add<DET>(lg, s.i0 * 4u + c, ds[c] * lf0);
+    lut_add<DET>(lg, s.i1 * 4u + c, ds[c] * s.f);
     dvv = fmaf(ds[c], dl[c], dvv);
   }
   const bool tt_free = s.tt > 0.0f && s.tt < 255.0f;
@@ -327,6 +420,17 @@ __device__ __forceinline__ void bwd_sample(const DiffGrid &g, const DiffRay &r, 
     b.cw[c] = fmaf(dv, (wx[c & 1] * wy[(c >> 1) & 1]) * wz[c >> 2], b.cw[c]);
 }
 
+// The adjoint of the contributing sample at t, recomputed from the grid.
+template <bool DET>
+__device__ __forceinline__ void bwd_sample(const DiffGrid &g, const float4 *lut, const DiffRay &r,
+                                           float t, float acc_a, BwdRay &b, LutGrad &lg,
+                                           float *g_dens, unsigned long long *q_dens) {
+  DiffSample s;
+  diff_sample(g, r, t, s);
+  diff_tf(lut, b.k, s);
+  bwd_contrib<DET>(lut, s, acc_a, b, lg, g_dens, q_dens);
+}
+
 template <int K, bool DET>
 __global__ void __launch_bounds__(128) k_diff_bwd(const DiffView *__restrict__ views,
                                                   const __grid_constant__ DiffGrid g,
@@ -337,18 +441,14 @@ __global__ void __launch_bounds__(128) k_diff_bwd(const DiffView *__restrict__ v
                                                   unsigned long long *__restrict__ q_lut,
                                                   float *__restrict__ g_scale,
                                                   unsigned long long *__restrict__ q_scale,
-                                                  const float2 *__restrict__ tape,
+                                                  const TapeEntry *__restrict__ tape,
                                                   const uint32_t *__restrict__ tape_n) {
   constexpr int kMaxCk = (4096 + K - 1) / K;
-  __shared__ float s_lut[DET ? 1 : 1024];
-  __shared__ unsigned long long s_qlut[DET ? 1024 : 1];
-  for (uint32_t i = threadIdx.x; i < 1024u; i += blockDim.x) {
-    if (DET)
-      s_qlut[i] = 0ull;
-    else
-      s_lut[i] = 0.0f;
-  }
+  __shared__ LutGrad lg;
+  lut_clear<DET>(lg);
   __syncthreads();
+  const float4 *lut = (const float4 *)g.lut;
+  const uint32_t zc = __ldg(g.zc);
 
   const DiffView &vw = views[blockIdx.z];
   const r3d_frame_params &pc = vw.pc;
@@ -379,8 +479,13 @@ __global__ void __launch_bounds__(128) k_diff_bwd(const DiffView *__restrict__ v
     if (r.hit && (b.gr != 0.0f || b.gg != 0.0f || b.gb != 0.0f)) {
       if (ntape <= kTape) {  // every contribution is on the tape
         for (int i = (int)ntape - 1; i >= 0; i--) {
-          const float2 e = __ldg(tape + ray * kTape + i);
-          bwd_sample<DET>(g, r, e.x, e.y, b, s_lut, s_qlut, g_dens, q_dens);
+          const float4 e = __ldg(tape + ray * kTape + i);
+          DiffSample s;
+          diff_cell(g, r, e.x, s);
+          s.v = e.z;
+          diff_tf_color(lut, s);
+          s.a = e.w;
+          bwd_contrib<DET>(lut, s, e.y, b, lg, g_dens, q_dens);
         }
       } else {
         // forward sweep: checkpoints (t, accumulated opacity) before steps
@@ -400,10 +505,12 @@ __global__ void __launch_bounds__(128) k_diff_bwd(const DiffView *__restrict__ v
             }
             nsteps++;
             DiffSample s;
-            diff_sample(g, r, t, s);
             bool stop = false;
-            if (!(s.v < pc.threshold)) {
-              diff_tf(g, b.k, s);
+            bool live;
+            diff_sample(g, r, t, s);
+            live = !(s.v < pc.threshold) && !diff_clear(s.v, zc);
+            if (live) {
+              diff_tf(lut, b.k, s);
               if (s.a > 0.003f) {
                 ring_t[ncontrib % kRing] = t;
                 ring_a[ncontrib % kRing] = acc_a;
@@ -438,9 +545,11 @@ __global__ void __launch_bounds__(128) k_diff_bwd(const DiffView *__restrict__ v
             const uint32_t s_end = min(nsteps, (uint32_t)(j + 1) * K);
             for (uint32_t st = (uint32_t)j * K; st < s_end; st++) {
               DiffSample s;
+              bool live;
               diff_sample(g, r, t, s);
-              if (!(s.v < pc.threshold)) {
-                diff_tf(g, b.k, s);
+              live = !(s.v < pc.threshold) && !diff_clear(s.v, zc);
+              if (live) {
+                diff_tf(lut, b.k, s);
                 if (s.a > 0.003f) {
                   seg_t[nseg] = t;
                   seg_a[nseg] = acc_a;
@@ -453,7 +562,7 @@ __global__ void __launch_bounds__(128) k_diff_bwd(const DiffView *__restrict__ v
           }
           end = start;
           for (int i = nseg - 1; i >= 0; i--)
-            bwd_sample<DET>(g, r, seg_t[i], seg_a[i], b, s_lut, s_qlut, g_dens, q_dens);
+            bwd_sample<DET>(g, lut, r, seg_t[i], seg_a[i], b, lg, g_dens, q_dens);
         }
       }
       bwd_flush<DET>(b, g_dens, q_dens);
@@ -462,7 +571,7 @@ __global__ void __launch_bounds__(128) k_diff_bwd(const DiffView *__restrict__ v
   // density scale: warp reduction, one global add per warp
   float gs = b.g_density;
   if (DET) {
-    long long q = __double2ll_rn((double)gs * kFix);
+    long long q = fix32(gs);
     for (int off = 16; off > 0; off >>= 1) q += __shfl_xor_sync(0xffffffffu, q, off);
     if (lane == 0 && q) atomicAdd(q_scale, (unsigned long long)q);
   } else {
@@ -470,13 +579,7 @@ __global__ void __launch_bounds__(128) k_diff_bwd(const DiffView *__restrict__ v
     if (lane == 0 && gs != 0.0f) atomicAdd(g_scale, gs);
   }
   __syncthreads();
-  for (uint32_t i = threadIdx.x; i < 1024u; i += blockDim.x) {
-    if (DET) {
-      if (s_qlut[i]) atomicAdd(q_lut + i, s_qlut[i]);
-    } else {
-      if (s_lut[i] != 0.0f) atomicAdd(g_lut + i, s_lut[i]);
-    }
-  }
+  lut_flush<DET>(lg, g_lut, q_lut);
 }
 
 static unsigned grid_blocks(size_t n) {
@@ -550,7 +653,7 @@ static int diff_prepare(r3d_cuda_ctx *c, const r3d_cuda_diff_scene *sc,
 static int diff_quads(r3d_cuda_ctx *c, const r3d_cuda_diff_scene *sc, DiffGrid &g, bool reuse,
                       cudaStream_t st) {
   const size_t nvox = (size_t)sc->nx * sc->ny * sc->nz;
-  const size_t need = nvox * sizeof(float4);
+  const size_t need = nvox * sizeof(float4) + 256u;  // the quads, then DiffGrid::zc
   if (c->diff_quad_bytes < need) {  // grow; earlier work on the old buffer must finish first
     R3D_CUDA_TRY(c, cudaDeviceSynchronize());
     cudaFree(c->diff_quad);
@@ -561,6 +664,11 @@ static int diff_quads(r3d_cuda_ctx *c, const r3d_cuda_diff_scene *sc, DiffGrid &
     c->diff_quad_bytes = need;
   }
   g.quad = (const float4 *)c->diff_quad;
+  uint32_t *zc = (uint32_t *)((char *)c->diff_quad + nvox * sizeof(float4));
+  g.zc = zc;
+  // the TF may change between calls that share the density
+  k_diff_tf_clear<<<1, 256, 0, st>>>(sc->lut, zc);
+  R3D_CUDA_TRY(c, cudaGetLastError());
   if (reuse && c->quad_src == sc->density) return R3D_OK;
   k_diff_quads<<<grid_blocks(nvox), 256, 0, st>>>(sc->density, sc->nx, sc->ny, sc->nz,
                                                   (float4 *)c->diff_quad);
@@ -594,7 +702,7 @@ static int diff_forward(r3d_cuda_ctx *c, const r3d_cuda_diff_scene *sc,
   if (rc != R3D_OK) return rc;
   rc = diff_quads(c, sc, g, false, st);
   if (rc != R3D_OK) return rc;
-  float2 *tp = nullptr;
+  TapeEntry *tp = nullptr;
   uint32_t *tn = nullptr;
   if (tape) {
     const size_t rays = nf / 3u;
@@ -606,11 +714,11 @@ static int diff_forward(r3d_cuda_ctx *c, const r3d_cuda_diff_scene *sc,
       c->tape = nullptr;
       c->tape_n = nullptr;
       c->tape_rays = 0;
-      R3D_CUDA_TRY(c, cudaMalloc(&c->tape, rays * kTape * sizeof(float2)));
+      R3D_CUDA_TRY(c, cudaMalloc(&c->tape, rays * kTape * sizeof(TapeEntry)));
       R3D_CUDA_TRY(c, cudaMalloc(&c->tape_n, rays * sizeof(uint32_t)));
       c->tape_rays = rays;
     }
-    tp = (float2 *)c->tape;
+    tp = (TapeEntry *)c->tape;
     tn = c->tape_n;
   }
   R3D_CUDA_TRY(c, cudaEventRecord(c->ev0, st));
@@ -654,7 +762,7 @@ template <int K, bool DET>
 static cudaError_t launch_bwd(dim3 grid, cudaStream_t st, const DiffView *dv, const DiffGrid &g,
                               const float *dl, float *gd, unsigned long long *qd, float *gl,
                               unsigned long long *ql, float *gs, unsigned long long *qs,
-                              const float2 *tp, const uint32_t *tn) {
+                              const TapeEntry *tp, const uint32_t *tn) {
   k_diff_bwd<K, DET><<<grid, 128, 0, st>>>(dv, g, dl, gd, qd, gl, ql, gs, qs, tp, tn);
   return cudaGetLastError();
 }
@@ -704,7 +812,7 @@ extern "C" int r3d_cuda_raycast_bwd(r3d_cuda_ctx *c, const r3d_cuda_diff_scene *
   if (use_tape && !tape_matches(c, sc, views, nviews))
     return fail(c, R3D_E_STATE, "raycast_bwd: no tape of a training forward over these views "
                                 "and this scene");
-  const float2 *tp = use_tape ? (const float2 *)c->tape : nullptr;
+  const TapeEntry *tp = use_tape ? (const TapeEntry *)c->tape : nullptr;
   const uint32_t *tn = use_tape ? c->tape_n : nullptr;
   // the tape's forward built the quads from this (unchanged) density
   rc = diff_quads(c, sc, g, use_tape, st);
