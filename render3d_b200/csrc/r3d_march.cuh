@@ -412,16 +412,20 @@ __device__ __forceinline__ float qbyte(uint32_t w, uint32_t k) {
 // (x, y1), (x1, y1) of its z plane (x1, y1 clamped to the slot), so a
 // sample is two 4-byte loads; z1 is clamped the same way.  The lerps run
 // in 0..255 space, x then y then z, as on the byte grid.
-__device__ __forceinline__ float tri_slot_q(const uint32_t *__restrict__ g, const SlotCoord &q) {
-  const uint32_t dz1 = q.z0 < 127u ? 16384u : 0u;
-  const uint32_t *r = g + ((q.z0 << 14) | (q.y0 << 7) | q.x0);
-  const uint32_t w0 = __ldg(r), w1 = __ldg(r + dz1);
+// The trilinear value of the quad words w0 (plane z0) and w1 (plane z1).
+__device__ __forceinline__ float tri_words(uint32_t w0, uint32_t w1, const SlotCoord &q) {
   const float c00 = lerp_(qbyte(w0, 0), qbyte(w0, 1), q.fx);
   const float c10 = lerp_(qbyte(w0, 2), qbyte(w0, 3), q.fx);
   const float c01 = lerp_(qbyte(w1, 0), qbyte(w1, 1), q.fx);
   const float c11 = lerp_(qbyte(w1, 2), qbyte(w1, 3), q.fx);
   const float e0 = lerp_(c00, c10, q.fy), e1 = lerp_(c01, c11, q.fy);
   return lerp_(e0, e1, q.fz) * kInv255;
+}
+
+__device__ __forceinline__ float tri_slot_q(const uint32_t *__restrict__ g, const SlotCoord &q) {
+  const uint32_t dz1 = q.z0 < 127u ? 16384u : 0u;
+  const uint32_t *r = g + ((q.z0 << 14) | (q.y0 << 7) | q.x0);
+  return tri_words(__ldg(r), __ldg(r + dz1), q);
 }
 
 __device__ __forceinline__ float slot_sample(const DevScene &s, uint32_t slot, const SlotCoord &q) {
@@ -977,13 +981,25 @@ __device__ __forceinline__ float3 sample_color(const DevScene &s, const ViewCons
     if (FAST) {  // raycast.slang:919-955
       const float ir3 = 0.57735026919f, renorm = 0.86602540378f;
       float q0, q1, q2, q3;
-      if (kLod) {
+      if (kLod) {  // the eight quad words are loaded before any is used
         float ev = q.grad_vox * ir3;
         float3 u = q.bl;
-        q0 = brick_fetch(s, q.slot, make_float3(u.x + ev, u.y - ev, u.z - ev));
-        q1 = brick_fetch(s, q.slot, make_float3(u.x - ev, u.y - ev, u.z + ev));
-        q2 = brick_fetch(s, q.slot, make_float3(u.x - ev, u.y + ev, u.z - ev));
-        q3 = brick_fetch(s, q.slot, make_float3(u.x + ev, u.y + ev, u.z + ev));
+        const SlotCoord t[4] = {slot_coord(make_float3(u.x + ev, u.y - ev, u.z - ev)),
+                                slot_coord(make_float3(u.x - ev, u.y - ev, u.z + ev)),
+                                slot_coord(make_float3(u.x - ev, u.y + ev, u.z - ev)),
+                                slot_coord(make_float3(u.x + ev, u.y + ev, u.z + ev))};
+        const uint32_t *g = s.br.quad + (size_t)q.slot * (128u * 128u * 128u);
+        uint32_t w[8];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          const uint32_t *r = g + ((t[k].z0 << 14) | (t[k].y0 << 7) | t[k].x0);
+          w[2 * k] = __ldg(r);
+          w[2 * k + 1] = __ldg(r + (t[k].z0 < 127u ? 16384u : 0u));
+        }
+        q0 = tri_words(w[0], w[1], t[0]);
+        q1 = tri_words(w[2], w[3], t[1]);
+        q2 = tri_words(w[4], w[5], t[2]);
+        q3 = tri_words(w[6], w[7], t[3]);
       } else if (slot_taps) {
         const float ev = q.lod_step * ir3;
         const float3 u = q.bl, org = shard_slot_org(s.sh, q.slot);
@@ -1021,24 +1037,34 @@ __device__ __forceinline__ float3 sample_color(const DevScene &s, const ViewCons
     } else {  // raycast.slang:957-986
       if (kLod) {
         // each tap moves one axis; the other two keep the sample's own
-        // clamped coordinates, so only the moved axis is recomputed
+        // clamped coordinates.  The twelve quad words of the six taps are
+        // loaded before any of them is used, so their latencies overlap.
         const float ev = q.grad_vox;
         const float3 u = q.bl;
         const SlotCoord c = slot_coord(u);
-        SlotCoord a = c, b = c;
-        a.x0 = slot_axis(u.x + ev, a.fx);
-        b.x0 = slot_axis(u.x - ev, b.fx);
-        g0 = slot_sample(s, q.slot, a) - slot_sample(s, q.slot, b);
-        a = c;
-        b = c;
-        a.y0 = slot_axis(u.y + ev, a.fy);
-        b.y0 = slot_axis(u.y - ev, b.fy);
-        g1 = slot_sample(s, q.slot, a) - slot_sample(s, q.slot, b);
-        a = c;
-        b = c;
-        a.z0 = slot_axis(u.z + ev, a.fz);
-        b.z0 = slot_axis(u.z - ev, b.fz);
-        g2 = slot_sample(s, q.slot, a) - slot_sample(s, q.slot, b);
+        SlotCoord t[6];
+#pragma unroll
+        for (int k = 0; k < 6; k++) t[k] = c;
+        t[0].x0 = slot_axis(u.x + ev, t[0].fx);
+        t[1].x0 = slot_axis(u.x - ev, t[1].fx);
+        t[2].y0 = slot_axis(u.y + ev, t[2].fy);
+        t[3].y0 = slot_axis(u.y - ev, t[3].fy);
+        t[4].z0 = slot_axis(u.z + ev, t[4].fz);
+        t[5].z0 = slot_axis(u.z - ev, t[5].fz);
+        const uint32_t *g = s.br.quad + (size_t)q.slot * (128u * 128u * 128u);
+        uint32_t w[12];
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+          const uint32_t *r = g + ((t[k].z0 << 14) | (t[k].y0 << 7) | t[k].x0);
+          w[2 * k] = __ldg(r);
+          w[2 * k + 1] = __ldg(r + (t[k].z0 < 127u ? 16384u : 0u));
+        }
+        float v[6];
+#pragma unroll
+        for (int k = 0; k < 6; k++) v[k] = tri_words(w[2 * k], w[2 * k + 1], t[k]);
+        g0 = v[0] - v[1];
+        g1 = v[2] - v[3];
+        g2 = v[4] - v[5];
       } else if (slot_taps) {
         const float ev = q.lod_step;
         const float3 u = q.bl, org = shard_slot_org(s.sh, q.slot);
