@@ -227,7 +227,8 @@ cudaError_t launch_view(const r3d_cuda_ctx *c, const r3d_frame_params &pc, uint8
   if (c->sched.staging && !steps && !mip_index && !counters && rows.row0 == 0u &&
       rows.row1 == 0xffffffffu && staged_supported(c, pc))
     return launch_staged(c, pc, img, out_w, total, stream);
-  const DevScene s = c->scene();
+  DevScene s = c->scene();
+  s.el = elide_counts(pc, s.tf_zero_t);
   const bool fast = c->quality == R3D_QUALITY_FAST;
   // shade_group 0 picks the path's default: grouped shading pays where a
   // gradient tap is a whole section lookup (tiled slab, clipmap, virtual

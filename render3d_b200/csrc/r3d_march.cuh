@@ -156,6 +156,55 @@ struct DevVslab {
   float x0, y0, z0, nx;  // the frame parameters slab_x0/y0/z0 and slab_nx (= W)
 };
 
+// Byte-valued thresholds of the fetch elision.  A block maximum m (a byte)
+// bounds a sample by vub = (float)m * kInv255.  Every decision the elision
+// takes on vub -- below the threshold, below the skip gate, inside the TF's
+// clear prefix, at most the depth mode's hit level -- is monotone in m, so
+// it holds exactly for the m below a count n.  The counts of a view are
+// found on the host for each launch (a guess from the inverse, settled by
+// the same float expressions the device evaluates) and reach the kernels
+// as launch parameters.
+struct ElideCounts {
+  // m < n_void: known void (below the threshold or the skip gate); m <
+  // n_dec: the mode's outcome is known (FULL/FLAT: below the threshold or
+  // TF-clear; DEPTH: below the threshold or at most the hit level; MIP:
+  // below the threshold); k2_dec: n_dec in the form bytes_below takes
+  uint32_t n_void, n_dec, k2_dec;
+};
+__host__ __device__ inline float vub_of(uint32_t m) { return (float)m * kInv255; }
+// The number of m in 0..255 whose vub satisfies pred, for a pred that holds
+// on a prefix of 0..255, from a guess g: kind 0: vub < x, 1: vub <= x, 2:
+// the TF coordinate of vub lies below x (the TF's clear prefix).
+__host__ __device__ inline bool vub_pred(int kind, float v, float x) {
+  if (kind == 0) return v < x;
+  if (kind == 1) return v <= x;
+  return fminf(fmaxf(fmaf(v, 256.0f, -0.5f), 0.0f), 255.0f) < x;
+}
+__host__ __device__ inline uint32_t vub_prefix(int kind, float x, float g) {
+  int n = g >= 256.0f ? 256 : (g > 0.0f ? (int)g : 0);  // NaN: 0
+  while (n > 0 && !vub_pred(kind, vub_of((uint32_t)n - 1u), x)) n--;
+  while (n < 256 && vub_pred(kind, vub_of((uint32_t)n), x)) n++;
+  return (uint32_t)n;
+}
+// The counts of a LOD-brick view (threshold, skip gate and mode from pc; the
+// scene's TF-clear coordinate tf_zero_t).  The gates follow view_const.
+__host__ __device__ inline ElideCounts elide_counts(const r3d_frame_params &pc, float tf_zero_t) {
+  const float bgate = fmaxf(fmaxf(pc.skip_gate, 0.5f / 255.0f), 4.5f / 255.0f);
+  const uint32_t n_cut = vub_prefix(0, pc.threshold, ceilf(pc.threshold * 255.0f));
+  const uint32_t n_bg = vub_prefix(0, bgate, ceilf(bgate * 255.0f));
+  ElideCounts e;
+  e.n_void = n_cut > n_bg ? n_cut : n_bg;
+  e.n_dec = n_cut;
+  uint32_t n2 = 0;
+  if (pc.mode == R3D_MODE_FULL || pc.mode == R3D_MODE_FLAT)
+    n2 = vub_prefix(2, tf_zero_t, ceilf((tf_zero_t + 0.5f) * (255.0f / 256.0f)));
+  else if (pc.mode == R3D_MODE_DEPTH)
+    n2 = vub_prefix(1, 0.05f, floorf(0.05f * 255.0f) + 1.0f);
+  if (n2 > e.n_dec) e.n_dec = n2;
+  e.k2_dec = (256u - e.n_dec) * 0x00010001u;
+  return e;
+}
+
 struct DevScene {
   DevCube cube;
   DevBricks br;
@@ -168,6 +217,8 @@ struct DevScene {
   float tf_zero_t;  // TF coordinates below this have alpha exactly 0
   // counting launches: bit s set when slot s's voxels are read (nullptr: off)
   uint32_t *slot_bits;
+  // one-view launches (grid, staged): the view's elision counts
+  ElideCounts el;
 };
 
 struct RayResult {
@@ -272,10 +323,12 @@ struct BrickCtx {  // raycast.slang:144-152
 
 struct LodCache {  // raycast.slang:190-196 (the cached brick is kept as the
                    // float origin lo = 128 * bc of its coordinates)
-  bool valid;
   int desired;
   float inv_scale;
-  float lo[3];  // (uint)lv >> 7 == bc  <=>  lo <= lv < lo + 128, for lv >= 0
+  // (uint)lv >> 7 == bc  <=>  lo <= lv < lo + 128, for lv >= 0; an empty
+  // cache (no brick found, or none looked up yet) holds lo = +inf, which no
+  // coordinate reaches
+  float lo[3];
   BrickCtx c;
 };
 
@@ -335,36 +388,37 @@ __device__ __forceinline__ BrickCtx lod_locate_ex(const DevScene &s, float3 p, f
     bco[2] = bc[2];
     break;
   }
-  lc.valid = c.ok;
   lc.desired = desired;
   lc.inv_scale = inv_out;
-  lc.lo[0] = (float)(bco[0] << 7);
-  lc.lo[1] = (float)(bco[1] << 7);
-  lc.lo[2] = (float)(bco[2] << 7);
+  lc.lo[0] = c.ok ? (float)(bco[0] << 7) : R3D_FM_INF;
+  lc.lo[1] = c.ok ? (float)(bco[1] << 7) : R3D_FM_INF;
+  lc.lo[2] = c.ok ? (float)(bco[2] << 7) : R3D_FM_INF;
   lc.c = c;
   return c;
 }
 
 // The hit test of bricks_lod_locate_cached (raycast.slang:255-279): true,
 // with the brick context in out, when the desired level and the brick under
-// p are the cached ones.
+// p are the cached ones.  The test runs on bl = lv - lo: rounding keeps the
+// sign of a difference, and for lo <= lv < lo + 128 the difference is exact
+// (lo = 0, or lv <= 2 lo), so bl >= 0 && bl < 128 decides exactly what
+// lo <= lv < lo + 128 does, and an empty cache (lo = +inf) never hits.
 __device__ __forceinline__ bool lod_cache_hit(const DevScene &s, float3 p, int desired,
                                               const LodCache &lc, BrickCtx &out) {
   const DevBricks &b = s.br;
-  if (lc.valid && lc.desired == desired) {
-    float lv[3];
+  if (lc.desired == desired) {
+    float bl[3];
     bool same = true;
     float pv[3] = {p.x, p.y, p.z};
 #pragma unroll
     for (int a = 0; a < 3; a++) {
       float base_v = clamp_(pv[a] * b.md, 0.0f, b.bs_hi[a]);
-      lv[a] = base_v * lc.inv_scale;
-      // lv >= 0, so floor(lv) >> 7 == bc exactly when lo <= lv < lo + 128
-      same = same && lv[a] >= lc.lo[a] && lv[a] < lc.lo[a] + 128.0f;
+      bl[a] = base_v * lc.inv_scale - lc.lo[a];
+      same = same && bl[a] >= 0.0f && bl[a] < 128.0f;
     }
     if (same) {
       out = lc.c;
-      out.bl = make_float3(lv[0] - lc.lo[0], lv[1] - lc.lo[1], lv[2] - lc.lo[2]);
+      out.bl = make_float3(bl[0], bl[1], bl[2]);
       return true;
     }
   }
@@ -388,9 +442,16 @@ __device__ __forceinline__ uint32_t floor_frac(float t, float &frac) {
 }
 
 // One axis of bricks_fetch's coordinate: clamp to [0.5, 127.5] inside the
-// brick, texel-centre shift, floor and fraction.
+// brick, texel-centre shift, floor and fraction.  The shift rides on the
+// truncating add: c + (2^23 - 0.5) is 2^23 + (c - 0.5) exactly before the
+// truncation, so r holds 2^23 + floor(c - 0.5); r - (2^23 - 0.5) =
+// floor + 0.5 and c - (floor + 0.5) are exact, so the floor and the
+// fraction are the bits of floor_frac(c - 0.5).
 __device__ __forceinline__ uint32_t slot_axis(float b, float &frac) {
-  return floor_frac(clamp_(b, 0.5f, 127.5f) - 0.5f, frac);
+  const float c = clamp_(b, 0.5f, 127.5f);
+  const float r = __fadd_rz(c, 8388607.5f);
+  frac = c - (r - 8388607.5f);
+  return __float_as_uint(r) & 0x7fffffu;
 }
 
 __device__ __forceinline__ SlotCoord slot_coord(float3 bl) {
@@ -686,6 +747,24 @@ __device__ __forceinline__ float4 tf_sample(const float4 *tf, float t) {
                      lerp_(a.z, b.z, f) * kInv255, lerp_(a.w, b.w, f) * kInv255);
 }
 
+// (float)m for a byte m without the conversion unit (exact: the byte
+// permute assembles the bits of 2^23 + m)
+__device__ __forceinline__ float byte_float(uint32_t m) {
+  return __uint_as_float(__byte_perm(m, 0x4B000000u, 0x7650u)) - 8388608.0f;
+}
+// Whether all eight bytes of two quad words are below k, with
+// k2 = (256 - k) * 0x00010001: each byte goes into a 16-bit lane of its own,
+// and adding 256 - k sets bit 8 of the lane exactly when the byte is >= k.
+__device__ __forceinline__ bool bytes_below(uint32_t w0, uint32_t w1, uint32_t k2) {
+  const uint32_t a = __byte_perm(w0, 0u, 0x4240u), b = __byte_perm(w0, 0u, 0x4341u);
+  const uint32_t c = __byte_perm(w1, 0u, 0x4240u), d = __byte_perm(w1, 0u, 0x4341u);
+  return (((a + k2) | (b + k2) | (c + k2) | (d + k2)) & 0x01000100u) == 0u;
+}
+
+#ifndef R3D_BYTE_ELIDE
+#define R3D_BYTE_ELIDE 1
+#endif
+
 // Per-view constants of the march (raycast.slang:647-683,722-762).
 struct ViewConst {
   float voxel, vox_inv, max_lod, cone, dt, bs, occ_gate, bgate, opac_k;
@@ -697,11 +776,14 @@ struct ViewConst {
   uint32_t ovl;
   float ovl_gain, reg_alpha;
   float3 ovl_col;
+  ElideCounts el;  // LOD bricks: the fetch elision's counts
 };
 
 template <int PATH>
-__device__ __forceinline__ ViewConst view_const(const r3d_frame_params &pc, const DevScene &s) {
+__device__ __forceinline__ ViewConst view_const(const r3d_frame_params &pc, const DevScene &s,
+                                                const ElideCounts &el) {
   ViewConst v;
+  v.el = el;
   if (PATH == PATH_LOD_BRICKS) {
     v.voxel = 1.0f / s.br.md;
     v.vox_inv = s.br.md;
@@ -757,6 +839,11 @@ __device__ __forceinline__ ViewConst view_const(const r3d_frame_params &pc, cons
   v.ovl_col = ((pc.overlay_flags >> 8) & 0xffu) == 1u ? make_float3(0.3f, 0.72f, 1.0f)
                                                       : make_float3(0.25f, 1.0f, 0.55f);
   return v;
+}
+// A one-view launch: the counts travel in the scene parameter.
+template <int PATH>
+__device__ __forceinline__ ViewConst view_const(const r3d_frame_params &pc, const DevScene &s) {
+  return view_const<PATH>(pc, s, s.el);
 }
 
 enum { kStepDone = 0, kStepCont = 1, kStepShade = 2 };
@@ -911,10 +998,9 @@ __device__ __forceinline__ bool ray_begin(const r3d_frame_params &pc, const DevS
   st.first_hit = -1.0f;
   st.acc_r = st.acc_g = st.acc_b = st.acc_a = 0.0f;
   st.ink_max = st.ink2_max = st.lbl_max = st.reg_max = 0.0f;
-  st.lc.valid = false;
   st.lc.desired = -1;
   st.lc.inv_scale = 1.0f;
-  st.lc.lo[0] = st.lc.lo[1] = st.lc.lo[2] = 0.0f;
+  st.lc.lo[0] = st.lc.lo[1] = st.lc.lo[2] = R3D_FM_INF;
   st.lc.c.ok = false;
   st.lc.c.maxv = 0.0f;
   st.lc.c.slot = 0;
@@ -1290,23 +1376,23 @@ __device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, 
       // Exact fetch elision: vub bounds the trilinear value from above
       // (every tap lies in the dilated block and rounding is monotone).
       // When vub already fixes every decision the sample feeds, the outcome
-      // equals the fetched one and the 8 loads are skipped.
+      // equals the fetched one and the 8 loads are skipped.  The decisions
+      // on vub are taken on its byte m against the view's counts.
       const SlotCoord q = slot_coord(b.bl);
       const uint32_t m = __ldg(s.br.bmax + (size_t)b.slot * 4096u +
                                (((q.z0 >> 3) << 8) | ((q.y0 >> 3) << 4) | (q.x0 >> 3)));
-      const float vub = (float)m * kInv255;
-      const bool cut_known = vub < vc.threshold;
-      const bool void_known = b.maxv >= vc.bgate || vub < vc.bgate || cut_known;
+      const bool brick_lit = b.maxv >= vc.bgate;
+      const bool void_known = brick_lit || m < vc.el.n_void;
       bool elide;
       if (MODE == R3D_MODE_MIP)
-        elide = b.maxv <= st.mip_max || (void_known && (cut_known || vub <= st.mip_max));
+        elide = b.maxv <= st.mip_max ||
+                (void_known && (m < vc.el.n_dec || byte_float(m) * kInv255 <= st.mip_max));
       else if (MODE == R3D_MODE_DEPTH)
-        elide = void_known && (cut_known || st.first_hit >= 0.0f || vub <= 0.05f);
+        elide = void_known && (st.first_hit >= 0.0f || m < vc.el.n_dec);
       else if (MODE == R3D_MODE_HEATMAP)
         elide = void_known;
       else
-        elide = void_known &&
-                (cut_known || clamp_(fmaf(vub, 256.0f, -0.5f), 0.0f, 255.0f) < s.tf_zero_t);
+        elide = void_known && m < vc.el.n_dec;
       // overlays read every sample (MIP maxima, registration opacity)
       if (!OVL && elide) {  // the sample changes nothing but the march position
         if ((MODE == R3D_MODE_MIP && b.maxv <= st.mip_max) || b.maxv < vc.bgate) {
@@ -1316,10 +1402,26 @@ __device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, 
         st.t = fmaf(vc.dt, lod_step, t);
         return kStepCont;
       }
-      v = STAGE && box_has(*box, b.slot, q) ? box_sample(*box, q) : slot_sample(s, b.slot, q);
       if (COUNT && s.slot_bits) {  // the unique slots a frame reads (test first: few atomics)
         const uint32_t m = 1u << (b.slot & 31u);
         if (!(__ldcg(s.slot_bits + (b.slot >> 5)) & m)) atomicOr(s.slot_bits + (b.slot >> 5), m);
+      }
+      if (STAGE && box_has(*box, b.slot, q)) {
+        v = box_sample(*box, q);
+      } else {
+        const uint32_t *g = s.br.quad + (size_t)b.slot * (128u * 128u * 128u) +
+                            ((q.z0 << 14) | (q.y0 << 7) | q.x0);
+        const uint32_t w0 = __ldg(g), w1 = __ldg(g + (q.z0 < 127u ? 16384u : 0u));
+        // The same elision on the sample's own eight bytes: their maximum
+        // bounds the trilinear value too, so in a lit brick (known void) the
+        // outcome is fixed when every byte is below n_dec.
+        constexpr bool kByteElide = R3D_BYTE_ELIDE && !OVL &&
+            (MODE == R3D_MODE_FULL || MODE == R3D_MODE_FLAT || MODE == R3D_MODE_DEPTH);
+        if (kByteElide && brick_lit && bytes_below(w0, w1, vc.el.k2_dec)) {
+          st.t = fmaf(vc.dt, lod_step, t);
+          return kStepCont;
+        }
+        v = tri_words(w0, w1, q);
       }
     }
   } else if (kShard) {

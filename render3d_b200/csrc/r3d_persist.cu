@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(128) k_raycast_persist(
     tf[i] = make_float4((float)u.x, (float)u.y, (float)u.z, (float)u.w);
   }
   for (uint32_t i = threadIdx.x; i < nviews; i += blockDim.x)
-    vcs[i] = view_const<PATH>(views[i].pc, s);
+    vcs[i] = view_const<PATH>(views[i].pc, s, elide_counts(views[i].pc, s.tf_zero_t));
   __syncthreads();
 
   const uint32_t lane = threadIdx.x & 31u;
@@ -265,7 +265,7 @@ __global__ void R3D_TILES_BOUNDS k_raycast_tiles(
     const bool inside = tx < v.grid_w && ty < v.grid_h;
     const bool half = (v.pc.view_flags & R3D_VIEW_HALF) != 0u;
     const uint32_t px = half ? tx * 2u : tx, py = half ? ty * 2u : ty;
-    const ViewConst vc = view_const<PATH>(v.pc, s);
+    const ViewConst vc = view_const<PATH>(v.pc, s, v.el);
     march_warp<PATH, MODE, FAST, COUNT>(v.pc, s, vc, tf[si], px, py, inside, r);
     if (inside) store_ray<MODE>(v, px, py, r, steps_out, mip_out);
     // work counters per tile: one atomic per 32 rays, nothing kept live
@@ -313,6 +313,8 @@ static cudaError_t launch_tn(const TilesLaunch &L, cudaStream_t st) {
   TileViews<N> tv;
   memcpy(tv.v, L.views, sizeof(DevView) * L.nviews);
   tv.n = L.nviews;
+  for (uint32_t i = 0; i < L.nviews; i++)
+    tv.v[i].el = elide_counts(tv.v[i].pc, L.scenes[L.nscenes > 1u ? tv.v[i].scene : 0u].tf_zero_t);
   TileScenes<NS> sc;
   for (uint32_t k = 0; k < L.nscenes; k++) {
     sc.s[k] = L.scenes[k];

@@ -16,7 +16,7 @@ struct DevView {
   uint32_t sup_x;       // 8x8-tile supertiles per grid row
   uint32_t tile_begin;  // index of the view's first tile in the launch
   uint32_t scene;       // whole-tile launches: index of the view's scene
-  uint32_t pad;
+  ElideCounts el;       // whole-tile launches: the view's elision counts
 };
 
 struct PersistLaunch {

@@ -249,7 +249,8 @@ cudaError_t launch_staged(const r3d_cuda_ctx *c, const r3d_frame_params &pc, uin
   const uint32_t gw = half ? (pc.viewport[0] + 1u) / 2u : pc.viewport[0];
   const uint32_t gh = half ? (pc.viewport[1] + 1u) / 2u : pc.viewport[1];
   const dim3 grid((gw + 7u) / 8u, (gh + 7u) / 8u);
-  const DevScene s = c->scene();
+  DevScene s = c->scene();
+  s.el = elide_counts(pc, s.tf_zero_t);
   const bool fast = c->quality == R3D_QUALITY_FAST;
   if (pc.mode == R3D_MODE_MIP)
     k_raycast_staged<R3D_MODE_MIP, false><<<grid, kStageThreads, 0, st>>>(
