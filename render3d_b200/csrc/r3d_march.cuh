@@ -865,9 +865,9 @@ struct RayState {
   float3 ro, dir;  // volume space
   float t, tf_, span_step;
   bool span_dom;  // span_step >= every exp2(lod): lod_step is span_step
-  // LOD bricks: for a footprint ratio y in [lod_ylo, lod_yhi) the desired
-  // level is lc.desired and lod_step is span_step (empty range: unknown)
-  float lod_ylo, lod_yhi;
+  // LOD bricks: for t in [lod_tlo, lod_thi) the desired level is
+  // lc.desired and lod_step is span_step (empty range: unknown)
+  float lod_tlo, lod_thi;
   float slab_cap;  // tiled slab: at least 4 samples across the box (raycast.slang:778-779)
   uint32_t steps, mip_index;
   float mip_max, first_hit;
@@ -990,8 +990,8 @@ __device__ __forceinline__ bool ray_begin(const r3d_frame_params &pc, const DevS
   // two are exact and the margin covers the approximation), so beyond this
   // bound max(exp2(lod), span_step) is span_step without evaluating exp2
   st.span_dom = st.span_step >= r3d_exp2f(ceilf(vc.max_lod)) * 1.001f;
-  st.lod_ylo = R3D_FM_INF;
-  st.lod_yhi = 0.0f;
+  st.lod_tlo = R3D_FM_INF;
+  st.lod_thi = 0.0f;
   st.steps = 0;
   st.mip_index = 0;
   st.mip_max = 0.0f;
@@ -1299,23 +1299,45 @@ __device__ __forceinline__ void shade_flush(const DevScene &s, const ViewConst &
   sb.n = 0;
 }
 
-// The footprint ratios y for which the step's LOD decisions are known
-// without log2 / exp2, after the exact lod at some y gave desired level d:
-// lod = clamp(log2(y) + bias, 0, max_lod) has floor d for every y in
-// [2^(d - bias), 2^(d + 1 - bias)) (open at the ends for d = 0 and the top
-// level), narrowed by 2^-12 relative at each end -- 3.5e-4 in log2, far
-// above the error of r3d_log2f plus the rounding of the bias add -- and
-// when span_step >= 1.001 * 2^(d + 1) (2^max_lod at the top), lod_step is
-// span_step for every lod of the level.  Otherwise the range is empty.
+// The footprint ratio of a sample at t (raycast.slang:772-774).
+__device__ __forceinline__ float lod_y(const ViewConst &vc, float t) {
+  const float foot = vc.ortho ? vc.cone : t * vc.cone;
+  return fmaxf(foot * vc.vox_inv, 1.0f);
+}
+
+// The samples whose LOD decisions are known without log2 / exp2, after the
+// exact lod at some t gave desired level d.  lod = clamp(log2(y) + bias, 0,
+// max_lod) has floor d for every footprint ratio y in [2^(d - bias),
+// 2^(d + 1 - bias)) (open at the ends for d = 0 and the top level), narrowed
+// by 2^-12 relative at each end -- 3.5e-4 in log2, far above the error of
+// r3d_log2f plus the rounding of the bias add -- and when span_step >=
+// 1.001 * 2^(d + 1) (2^max_lod at the top), lod_step is span_step for every
+// lod of the level.  Otherwise the range is empty.  The range is kept as an
+// interval of t: y(t) = max(fl(fl(t cone) vox_inv), 1) lies within a
+// factor (1 +- 2^-24)^2 of t * cone * vox_inv, so the ends divided by that
+// product and moved inwards by 2^-20 relative (far above those roundings
+// and the ones of the division) bound t values whose y is certainly inside.
+// A sample between the certain interval and the range's true ends takes the
+// exact path (log2), which decides the same level and step.
 __device__ __forceinline__ void lod_range(RayState &st, const ViewConst &vc, int d, int top) {
   const float hi_lod = d >= top ? vc.max_lod : (float)(d + 1);
-  if (!(st.span_step >= r3d_exp2f(hi_lod) * 1.001f)) {
-    st.lod_ylo = R3D_FM_INF;
-    st.lod_yhi = 0.0f;
+  st.lod_tlo = R3D_FM_INF;
+  st.lod_thi = 0.0f;
+  if (!(st.span_step >= r3d_exp2f(hi_lod) * 1.001f)) return;
+  const float ylo = d == 0 ? 0.0f : r3d_exp2f((float)d - vc.lod_bias) * (1.0f + 0x1p-12f);
+  const float yhi = d >= top ? R3D_FM_INF : r3d_exp2f((float)(d + 1) - vc.lod_bias) * (1.0f - 0x1p-12f);
+  if (vc.ortho) {  // y does not depend on t
+    const float y = lod_y(vc, 0.0f);
+    if (y >= ylo && y < yhi) {
+      st.lod_tlo = -R3D_FM_INF;
+      st.lod_thi = R3D_FM_INF;
+    }
     return;
   }
-  st.lod_ylo = d == 0 ? 0.0f : r3d_exp2f((float)d - vc.lod_bias) * (1.0f + 0x1p-12f);
-  st.lod_yhi = d >= top ? R3D_FM_INF : r3d_exp2f((float)(d + 1) - vc.lod_bias) * (1.0f - 0x1p-12f);
+  const float k = vc.cone * vc.vox_inv;
+  if (!(k >= 0x1p-60f && k <= 0x1p60f) || !(yhi > 1.0f)) return;  // y >= 1: never below yhi <= 1
+  st.lod_tlo = ylo <= 1.0f ? -R3D_FM_INF : (ylo / k) * (1.0f + 0x1p-20f);
+  st.lod_thi = yhi == R3D_FM_INF ? R3D_FM_INF : (yhi / k) * (1.0f - 0x1p-20f);
 }
 
 // One iteration of the hot loop (raycast.slang:767-1021).  Returns
@@ -1340,15 +1362,13 @@ __device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, 
   st.steps++;
   const float t = st.t;
   // LOD and step (raycast.slang:772-779)
-  float lod = 0.0f, y = 1.0f;
+  float lod = 0.0f;
   bool lod_known = true;
   if (vc.lod_on) {
-    float foot = vc.ortho ? vc.cone : t * vc.cone;
-    y = fmaxf(foot * vc.vox_inv, 1.0f);
-    if (kLod && y >= st.lod_ylo && y < st.lod_yhi)
+    if (kLod && t >= st.lod_tlo && t < st.lod_thi)
       lod_known = false;  // level and lod_step known (lod_range)
     else
-      lod = clamp_(r3d_log2f(y) + vc.lod_bias, 0.0f, vc.max_lod);
+      lod = clamp_(r3d_log2f(lod_y(vc, t)) + vc.lod_bias, 0.0f, vc.max_lod);
   }
   float lod_step =
       !lod_known || st.span_dom ? st.span_step
@@ -1368,7 +1388,7 @@ __device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, 
       if (desired != st.lc.desired) lod_range(st, vc, desired, top);
     }
     if (!lod_cache_hit(s, p, desired, st.lc, b)) {  // walk the page table
-      if (!lod_known) lod = clamp_(r3d_log2f(y) + vc.lod_bias, 0.0f, vc.max_lod);
+      if (!lod_known) lod = clamp_(r3d_log2f(lod_y(vc, t)) + vc.lod_bias, 0.0f, vc.max_lod);
       if (COUNT) st.n_walk++;
       b = lod_locate_ex(s, p, lod, st.lc, desired);
     }

@@ -78,10 +78,8 @@ __device__ __forceinline__ bool peek_fetch(const DevScene &s, const ViewConst &v
   const float t = st.t;
   int desired = st.lc.desired;
   if (vc.lod_on) {
-    const float foot = vc.ortho ? vc.cone : t * vc.cone;
-    const float y = fmaxf(foot * vc.vox_inv, 1.0f);
-    if (!(y >= st.lod_ylo && y < st.lod_yhi)) {
-      const float lod = clamp_(r3d_log2f(y) + vc.lod_bias, 0.0f, vc.max_lod);
+    if (!(t >= st.lod_tlo && t < st.lod_thi)) {
+      const float lod = clamp_(r3d_log2f(lod_y(vc, t)) + vc.lod_bias, 0.0f, vc.max_lod);
       desired = (int)clamp_(floorf(lod), 0.0f, (float)((int)s.br.nlev - 1));
     }
   } else {
