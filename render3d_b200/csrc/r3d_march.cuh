@@ -168,8 +168,10 @@ struct ElideCounts {
   // m < n_void: known void (below the threshold or the skip gate); m <
   // n_dec: the mode's outcome is known (FULL/FLAT: below the threshold or
   // TF-clear; DEPTH: below the threshold or at most the hit level; MIP:
-  // below the threshold); k2_dec: n_dec in the form bytes_below takes
-  uint32_t n_void, n_dec, k2_dec;
+  // below the threshold); raw_dec: 2^23 + n_dec, for bytes taken as
+  // 2^23 + byte (qraw)
+  uint32_t n_void, n_dec;
+  float raw_dec;
 };
 __host__ __device__ inline float vub_of(uint32_t m) { return (float)m * kInv255; }
 // The number of m in 0..255 whose vub satisfies pred, for a pred that holds
@@ -201,7 +203,7 @@ __host__ __device__ inline ElideCounts elide_counts(const r3d_frame_params &pc, 
   else if (pc.mode == R3D_MODE_DEPTH)
     n2 = vub_prefix(1, 0.05f, floorf(0.05f * 255.0f) + 1.0f);
   if (n2 > e.n_dec) e.n_dec = n2;
-  e.k2_dec = (256u - e.n_dec) * 0x00010001u;
+  e.raw_dec = 8388608.0f + (float)e.n_dec;
   return e;
 }
 
@@ -254,6 +256,27 @@ __device__ __forceinline__ uint8_t unorm8(float x) {
   return (uint8_t)(int)fmaf(sat_(x), 255.0f, 0.5f);
 }
 
+// floor of t in [0, 2^23) as an integer and its fraction, without the
+// conversion unit: adding 2^23 with truncation leaves floor(t) in the
+// mantissa.  Equal to (uint32_t)t and t - (float)(uint32_t)t.
+__device__ __forceinline__ uint32_t floor_frac(float t, float &frac) {
+  float r = __fadd_rz(t, 8388608.0f);
+  frac = t - (r - 8388608.0f);
+  return __float_as_uint(r) & 0x7fffffu;
+}
+
+// Bytes taken as the float 2^23 + byte (bits assembled, no conversion
+// unit).  The difference of two such floats is the bytes' difference
+// exactly, and one subtraction of 2^23 gives the first byte, so
+// lerp_raw(2^23 + a, 2^23 + b, t) is lerp_(a, b, t) = fmaf(t, b - a, a) in
+// the same bits, with one instruction fewer.
+__device__ __forceinline__ float raw_u8(const uint8_t *p) {
+  return __uint_as_float(0x4B000000u | (uint32_t)__ldg(p));
+}
+__device__ __forceinline__ float lerp_raw(float ra, float rb, float t) {
+  return fmaf(t, rb - ra, ra - 8388608.0f);
+}
+
 // Clamp-to-edge trilinear at texel centres on a u8 grid: x, then y, then z
 // lerps in 0..255 space, scaled by 1/255 at the end.
 __device__ __forceinline__ float tri_u8(const uint8_t *__restrict__ g, uint32_t dx, uint32_t dy,
@@ -261,20 +284,18 @@ __device__ __forceinline__ float tri_u8(const uint8_t *__restrict__ g, uint32_t 
   tx = clamp_(tx, 0.0f, (float)(dx - 1u));
   ty = clamp_(ty, 0.0f, (float)(dy - 1u));
   tz = clamp_(tz, 0.0f, (float)(dz - 1u));
-  uint32_t x0 = (uint32_t)tx, y0 = (uint32_t)ty, z0 = (uint32_t)tz;
-  float fx = tx - (float)x0, fy = ty - (float)y0, fz = tz - (float)z0;
+  float fx, fy, fz;
+  const uint32_t x0 = floor_frac(tx, fx), y0 = floor_frac(ty, fy), z0 = floor_frac(tz, fz);
   uint32_t x1 = min(x0 + 1u, dx - 1u), y1 = min(y0 + 1u, dy - 1u), z1 = min(z0 + 1u, dz - 1u);
   size_t sy = dx, sz = (size_t)dx * dy;
   const uint8_t *r00 = g + (size_t)y0 * sy + (size_t)z0 * sz;
   const uint8_t *r10 = g + (size_t)y1 * sy + (size_t)z0 * sz;
   const uint8_t *r01 = g + (size_t)y0 * sy + (size_t)z1 * sz;
   const uint8_t *r11 = g + (size_t)y1 * sy + (size_t)z1 * sz;
-  float a0 = __ldg(r00 + x0), a1 = __ldg(r00 + x1);
-  float b0 = __ldg(r10 + x0), b1 = __ldg(r10 + x1);
-  float c0 = __ldg(r01 + x0), c1 = __ldg(r01 + x1);
-  float d0 = __ldg(r11 + x0), d1 = __ldg(r11 + x1);
-  float c00 = lerp_(a0, a1, fx), c10 = lerp_(b0, b1, fx);
-  float c01 = lerp_(c0, c1, fx), c11 = lerp_(d0, d1, fx);
+  float c00 = lerp_raw(raw_u8(r00 + x0), raw_u8(r00 + x1), fx);
+  float c10 = lerp_raw(raw_u8(r10 + x0), raw_u8(r10 + x1), fx);
+  float c01 = lerp_raw(raw_u8(r01 + x0), raw_u8(r01 + x1), fx);
+  float c11 = lerp_raw(raw_u8(r11 + x0), raw_u8(r11 + x1), fx);
   float e0 = lerp_(c00, c10, fy), e1 = lerp_(c01, c11, fy);
   return lerp_(e0, e1, fz) * kInv255;
 }
@@ -432,15 +453,6 @@ struct SlotCoord {
   uint32_t x0, y0, z0;
 };
 
-// floor of t in [0, 2^23) as an integer and its fraction, without the
-// conversion unit: adding 2^23 with truncation leaves floor(t) in the
-// mantissa.  Equal to (uint32_t)t and t - (float)(uint32_t)t.
-__device__ __forceinline__ uint32_t floor_frac(float t, float &frac) {
-  float r = __fadd_rz(t, 8388608.0f);
-  frac = t - (r - 8388608.0f);
-  return __float_as_uint(r) & 0x7fffffu;
-}
-
 // One axis of bricks_fetch's coordinate: clamp to [0.5, 127.5] inside the
 // brick, texel-centre shift, floor and fraction.  The shift rides on the
 // truncating add: c + (2^23 - 0.5) is 2^23 + (c - 0.5) exactly before the
@@ -474,13 +486,33 @@ __device__ __forceinline__ float qbyte(uint32_t w, uint32_t k) {
 // sample is two 4-byte loads; z1 is clamped the same way.  The lerps run
 // in 0..255 space, x then y then z, as on the byte grid.
 // The trilinear value of the quad words w0 (plane z0) and w1 (plane z1).
-__device__ __forceinline__ float tri_words(uint32_t w0, uint32_t w1, const SlotCoord &q) {
-  const float c00 = lerp_(qbyte(w0, 0), qbyte(w0, 1), q.fx);
-  const float c10 = lerp_(qbyte(w0, 2), qbyte(w0, 3), q.fx);
-  const float c01 = lerp_(qbyte(w1, 0), qbyte(w1, 1), q.fx);
-  const float c11 = lerp_(qbyte(w1, 2), qbyte(w1, 3), q.fx);
+// The x lerps take the bytes as 2^23 + byte (the permute alone; lerp_raw).
+__device__ __forceinline__ float qraw(uint32_t w, uint32_t k) {
+  return __uint_as_float(__byte_perm(w, 0x4B000000u, k | 0x7540u));
+}
+// The eight bytes of two quad words, as 2^23 + byte.
+struct RawBytes {
+  float r[8];
+};
+__device__ __forceinline__ RawBytes raw_bytes(uint32_t w0, uint32_t w1) {
+  return {{qraw(w0, 0), qraw(w0, 1), qraw(w0, 2), qraw(w0, 3), qraw(w1, 0), qraw(w1, 1),
+           qraw(w1, 2), qraw(w1, 3)}};
+}
+// 2^23 + the largest of the eight bytes
+__device__ __forceinline__ float raw_max(const RawBytes &b) {
+  return fmaxf(fmaxf(fmaxf(b.r[0], b.r[1]), fmaxf(b.r[2], b.r[3])),
+               fmaxf(fmaxf(b.r[4], b.r[5]), fmaxf(b.r[6], b.r[7])));
+}
+__device__ __forceinline__ float tri_raw(const RawBytes &b, const SlotCoord &q) {
+  const float c00 = lerp_raw(b.r[0], b.r[1], q.fx);
+  const float c10 = lerp_raw(b.r[2], b.r[3], q.fx);
+  const float c01 = lerp_raw(b.r[4], b.r[5], q.fx);
+  const float c11 = lerp_raw(b.r[6], b.r[7], q.fx);
   const float e0 = lerp_(c00, c10, q.fy), e1 = lerp_(c01, c11, q.fy);
   return lerp_(e0, e1, q.fz) * kInv255;
+}
+__device__ __forceinline__ float tri_words(uint32_t w0, uint32_t w1, const SlotCoord &q) {
+  return tri_raw(raw_bytes(w0, w1), q);
 }
 
 __device__ __forceinline__ float tri_slot_q(const uint32_t *__restrict__ g, const SlotCoord &q) {
@@ -595,8 +627,8 @@ __device__ __forceinline__ float tex_wrapz(const uint8_t *__restrict__ g, uint32
   const float tx = clamp_(fmaf(u, (float)tw, -0.5f), 0.0f, (float)(tw - 1u));
   const float ty = clamp_(fmaf(v, (float)th, -0.5f), 0.0f, (float)(th - 1u));
   const float tz = fmaf(w, (float)wz, -0.5f);
-  const uint32_t x0 = (uint32_t)tx, y0 = (uint32_t)ty;
-  const float fx = tx - (float)x0, fy = ty - (float)y0;
+  float fx, fy;
+  const uint32_t x0 = floor_frac(tx, fx), y0 = floor_frac(ty, fy);
   const float zf = floorf(tz), fz = tz - zf;
   // w is a fraction in [0, 1), so floor(tz) lies in [-1, wz - 1] and its
   // ring layer is one conditional away (the modulo of the restatement)
@@ -607,10 +639,10 @@ __device__ __forceinline__ float tex_wrapz(const uint8_t *__restrict__ g, uint32
   const size_t sy = tw, sz = (size_t)tw * th;
   const uint8_t *r00 = g + y0 * sy + z0 * sz, *r10 = g + y1 * sy + z0 * sz;
   const uint8_t *r01 = g + y0 * sy + z1 * sz, *r11 = g + y1 * sy + z1 * sz;
-  const float c00 = lerp_((float)__ldg(r00 + x0), (float)__ldg(r00 + x1), fx);
-  const float c10 = lerp_((float)__ldg(r10 + x0), (float)__ldg(r10 + x1), fx);
-  const float c01 = lerp_((float)__ldg(r01 + x0), (float)__ldg(r01 + x1), fx);
-  const float c11 = lerp_((float)__ldg(r11 + x0), (float)__ldg(r11 + x1), fx);
+  const float c00 = lerp_raw(raw_u8(r00 + x0), raw_u8(r00 + x1), fx);
+  const float c10 = lerp_raw(raw_u8(r10 + x0), raw_u8(r10 + x1), fx);
+  const float c01 = lerp_raw(raw_u8(r01 + x0), raw_u8(r01 + x1), fx);
+  const float c11 = lerp_raw(raw_u8(r11 + x0), raw_u8(r11 + x1), fx);
   return lerp_(lerp_(c00, c10, fy), lerp_(c01, c11, fy), fz) * kInv255;
 }
 
@@ -751,14 +783,6 @@ __device__ __forceinline__ float4 tf_sample(const float4 *tf, float t) {
 // permute assembles the bits of 2^23 + m)
 __device__ __forceinline__ float byte_float(uint32_t m) {
   return __uint_as_float(__byte_perm(m, 0x4B000000u, 0x7650u)) - 8388608.0f;
-}
-// Whether all eight bytes of two quad words are below k, with
-// k2 = (256 - k) * 0x00010001: each byte goes into a 16-bit lane of its own,
-// and adding 256 - k sets bit 8 of the lane exactly when the byte is >= k.
-__device__ __forceinline__ bool bytes_below(uint32_t w0, uint32_t w1, uint32_t k2) {
-  const uint32_t a = __byte_perm(w0, 0u, 0x4240u), b = __byte_perm(w0, 0u, 0x4341u);
-  const uint32_t c = __byte_perm(w1, 0u, 0x4240u), d = __byte_perm(w1, 0u, 0x4341u);
-  return (((a + k2) | (b + k2) | (c + k2) | (d + k2)) & 0x01000100u) == 0u;
 }
 
 #ifndef R3D_BYTE_ELIDE
@@ -1437,11 +1461,12 @@ __device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, 
         // outcome is fixed when every byte is below n_dec.
         constexpr bool kByteElide = R3D_BYTE_ELIDE && !OVL &&
             (MODE == R3D_MODE_FULL || MODE == R3D_MODE_FLAT || MODE == R3D_MODE_DEPTH);
-        if (kByteElide && brick_lit && bytes_below(w0, w1, vc.el.k2_dec)) {
+        const RawBytes rb = raw_bytes(w0, w1);
+        if (kByteElide && brick_lit && raw_max(rb) < vc.el.raw_dec) {
           st.t = fmaf(vc.dt, lod_step, t);
           return kStepCont;
         }
-        v = tri_words(w0, w1, q);
+        v = tri_raw(rb, q);
       }
     }
   } else if (kShard) {
