@@ -368,7 +368,8 @@ int r3d_cuda_shard_read(r3d_cuda_ctx *ctx, int level, uint32_t *page, uint8_t *o
  * (device or host) as the image. */
 typedef struct r3d_cuda_aux {
   uint32_t *steps;     /* out_w*out_h: march iterations of the ray */
-  uint32_t *mip_index; /* out_w*out_h: step at which the MIP max last rose (MIP views) */
+  uint32_t *mip_index; /* out_w*out_h: step at which the MIP max last rose; defined for
+                        MIP views (LOD-brick views of other modes leave 0) */
   unsigned long long *total_steps; /* one counter: += sum of steps */
   /* R3D_COUNTERS counters, += per frame: samples (= steps), composited TF
    * lookups, gradient-shaded samples, page-table walks.  Counting runs a

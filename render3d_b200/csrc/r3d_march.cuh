@@ -1534,7 +1534,10 @@ __device__ __forceinline__ int ray_step(const DevScene &s, const ViewConst &vc, 
     return kStepCont;
   }
 
-  if (v > st.mip_max) {
+  // the running maximum and its step, for MIP views (their MIP index aux
+  // output); LOD-brick views of other modes without overlays skip it
+  constexpr bool kTrackMip = MODE == R3D_MODE_MIP || !kLod || OVL;
+  if (kTrackMip && v > st.mip_max) {
     st.mip_max = v;
     st.mip_index = st.steps;
   }

@@ -258,16 +258,25 @@ __global__ void R3D_TILES_BOUNDS k_raycast_tiles(
     const DevView &v = tv.v[N > 1 ? vi : 0u];
     const uint32_t si = NS > 1 ? v.scene : 0u;
     const DevScene &s = sc.s[si];
-    uint32_t tx, ty;
-    tile_ray(v, t - v.tile_begin, threadIdx.x & 31u, 0u, tx, ty);
+    const bool half = (v.pc.view_flags & R3D_VIEW_HALF) != 0u;
     RayResult r;
     r.steps = r.n_tf = r.n_grad = r.n_walk = 0u;
-    const bool inside = tx < v.grid_w && ty < v.grid_h;
-    const bool half = (v.pc.view_flags & R3D_VIEW_HALF) != 0u;
-    const uint32_t px = half ? tx * 2u : tx, py = half ? ty * 2u : ty;
-    const ViewConst vc = view_const<PATH>(v.pc, s, v.el);
-    march_warp<PATH, MODE, FAST, COUNT>(v.pc, s, vc, tf[si], px, py, inside, r);
-    if (inside) store_ray<MODE>(v, px, py, r, steps_out, mip_out);
+    {
+      uint32_t tx, ty;
+      tile_ray(v, t - v.tile_begin, threadIdx.x & 31u, 0u, tx, ty);
+      const bool inside = tx < v.grid_w && ty < v.grid_h;
+      const uint32_t px = half ? tx * 2u : tx, py = half ? ty * 2u : ty;
+      const ViewConst vc = view_const<PATH>(v.pc, s, v.el);
+      march_warp<PATH, MODE, FAST, COUNT>(v.pc, s, vc, tf[si], px, py, inside, r);
+    }
+    // the ray's pixel again, from the tile index: recomputed after the march
+    // (an opaque copy of t stops the compiler from keeping it live across)
+    uint32_t t2;
+    asm volatile("mov.u32 %0, %1;" : "=r"(t2) : "r"(t));
+    uint32_t tx, ty;
+    tile_ray(v, t2 - v.tile_begin, threadIdx.x & 31u, 0u, tx, ty);
+    if (tx < v.grid_w && ty < v.grid_h)
+      store_ray<MODE>(v, half ? tx * 2u : tx, half ? ty * 2u : ty, r, steps_out, mip_out);
     // work counters per tile: one atomic per 32 rays, nothing kept live
     // across the march
     if (total) {
