@@ -627,6 +627,15 @@ int r3d_cuda_l2_read_probe(r3d_cuda_ctx *ctx, size_t bytes, uint32_t passes, flo
 int r3d_cuda_fmath_eval(r3d_cuda_ctx *ctx, const float *x, const float *y, float *out,
                         uint32_t n);
 
+/* The byte counts the LOD-brick kernels' fetch elision compares a block
+ * maximum m (and a fetched sample's bytes) with, for view p in a scene whose
+ * TF is clear below tf_zero_t: out[0] = n_void (m < n_void: the sample is
+ * below the threshold or the skip gate), out[1] = n_dec (m < n_dec: the
+ * view's mode decides nothing on the sample).  Host code, the same function
+ * the launches use; no device work.  Used to check the counts against all
+ * 256 byte values; no counterpart in the reference. */
+void r3d_cuda_elide_counts(const r3d_frame_params *p, float tf_zero_t, uint32_t out[2]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -268,6 +268,7 @@ def _load() -> C.CDLL:
         "r3d_cuda_raycast_rows": (I, [P, P, P, U32, U32, U32, U32, P]),
         "r3d_cuda_last_kernel_ns": (I, [P, C.POINTER(C.c_uint64)]),
         "r3d_cuda_fmath_eval": (I, [P, P, P, P, U32]),
+        "r3d_cuda_elide_counts": (None, [P, F, P]),
         "r3d_cuda_set_schedule": (I, [P, C.POINTER(Schedule)]),
         "r3d_cuda_l2_read_probe": (I, [P, C.c_size_t, U32, C.POINTER(F)]),
         "r3d_cuda_set_slot_trace": (I, [P, P]),

@@ -218,6 +218,17 @@ cudaError_t launch_path<R3D_FWD_PATH>(const r3d_frame_params &pc, const DevScene
                                 st);
 }
 #else
+}  // namespace r3d
+
+extern "C" void r3d_cuda_elide_counts(const r3d_frame_params *p, float tf_zero_t,
+                                      uint32_t out[2]) {
+  const r3d::ElideCounts e = r3d::elide_counts(*p, tf_zero_t);
+  out[0] = e.n_void;
+  out[1] = e.n_dec;
+}
+
+namespace r3d {
+
 cudaError_t launch_view(const r3d_cuda_ctx *c, const r3d_frame_params &pc, uint8_t *img,
                         uint32_t out_w, uint32_t *steps, uint32_t *mip_index,
                         unsigned long long *total, unsigned long long *counters,

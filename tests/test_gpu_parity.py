@@ -236,6 +236,46 @@ def test_bricks_clips(rb, orc, ctx, bricks256, scroll_tf, case, sched):
         ctx.set_alpha_cutoff(0.98)
 
 
+# TFs and gates that move the fetch elision's byte counts to their edges:
+# a TF with opacity from 0 (no clear prefix), one clear up to 250, a low
+# cut (threshold) and a high skip gate
+ELIDE_EDGES = {
+    "opaque_from_0": ([(0, (10, 10, 10, 20)), (255, (255, 255, 255, 230))], 0.0, None),
+    "clear_to_250": ([(0, (0, 0, 0, 0)), (250, (250, 250, 250, 0)), (255, (255, 255, 255, 255))],
+                     0.0, None),
+    "low_cut": (None, 90.0, None),
+    "high_gate": (None, 0.0, 0.25),
+}
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2, 3, 5])
+@pytest.mark.parametrize("case", list(ELIDE_EDGES))
+def test_bricks_elision_edges(rb, orc, ctx, bricks256, scroll_tf, case, mode):
+    """The elision decides on the byte of a block maximum (and on a fetched
+    sample's own eight bytes) against per-view counts; at the counts' edges
+    the images, step counts and MIP indices still equal the oracle's."""
+    pts, low_cut, gate = ELIDE_EDGES[case]
+    lut = rb.tf_build(pts) if pts else scroll_tf
+    w, h = 256, 192
+    p = rb.camera_view(1.3, -0.4, 1.5, w, h, lut, step_voxels=0.5, mode=mode, low_cut=low_cut)
+    p.brick_mode = ctx.brick_mode
+    if gate is not None:
+        p.skip_gate = gate
+    ctx.set_transfer(lut)
+    try:
+        steps = np.zeros((h, w), np.uint32)
+        mipi = np.zeros((h, w), np.uint32)
+        got = ctx.raycast(p, w, h, steps=steps, mip_index=mipi)
+        ref, rsteps, rmip, _, st = orc.render(p, bricks256, lut, w, h)
+        assert st == 0
+        _cmp(got, ref, f"{case} mode {mode}")
+        assert np.array_equal(steps, rsteps), f"{case} mode {mode}: step counts"
+        if mode == 1:
+            assert np.array_equal(mipi, rmip), f"{case}: MIP indices"
+    finally:
+        ctx.set_transfer(scroll_tf)
+
+
 def test_bad_page_entries_report_status(rb, orc, ctx, scroll_tf):
     """A page table whose entries point past the slot pool must not fault:
     the kernel treats them as absent and raises a status bit, like the
