@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(kStageThreads, 16)
   if (waited_out) mbar_wait(&bar, phase ^ 1u);
 }
 
-// The driver's tensor-map encoder, looked up once through the runtime.
+// The CUDA driver API's tensor-map encoder, looked up once through the runtime.
 static PFN_cuTensorMapEncodeTiled_v12000 encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   if (!fn) {

@@ -1,6 +1,6 @@
 """Parity of the sm_100a kernels with the CPU oracle.
 
-Images must agree within 1/255 per channel (
+Images must agree within 1/255 per channel (the parity tolerance;
 in practice they are identical), heatmap step counts and MIP indices must be
 identical, and the device-side builders (mip chain, occupancy grid, LOD
 brick pyramid and page table) must be bit-exact."""
