@@ -49,9 +49,9 @@ WORKLOAD = "scroll phantom 1024^3 u8, 128^3 bricks x 4 LOD levels, 1920x1080 ful
 # dram__bytes_write.sum), warp instructions (smsp__inst_executed.sum) and
 # thread instructions (smsp__thread_inst_executed.sum); and the samples of
 # those two frames (the counters that `--profile` prints).
-FWD_DRAM_TRAFFIC_BYTES = 238.3e6
-FWD_WARP_INST = 282.1e6
-FWD_THREAD_INST = 5.380e9
+FWD_DRAM_TRAFFIC_BYTES = 238.8e6
+FWD_WARP_INST = 282.6e6
+FWD_THREAD_INST = 5.389e9
 FWD_CAPTURED_SAMPLES = 28.31e6
 METRIC = "raycast Gsamples/s & fps @1024^3 1080p; fwd+bwd Gsamples/s vs plain, same GPU"
 
