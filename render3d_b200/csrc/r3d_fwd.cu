@@ -82,12 +82,22 @@ __global__ void R3D_FWD_BOUNDS k_raycast(const __grid_constant__ r3d_frame_param
     bx = strip * kStrip + within % sw;
     by = within / sw;
   } else if (kTall) {
-    // block rows from the middle outwards (mid, mid - 1, mid + 1, ...): the
-    // long rays through the volume start first and the frame's tail holds
-    // the short ones (1080p FULL and FLAT 3.5 % faster than row order);
-    // mid - d >= 0 and mid + d < gridDim.y for every row i
-    const uint32_t mid = gridDim.y / 2u, i = blockIdx.y, d = (i + 1u) / 2u;
-    by = (i & 1u) ? mid - d : mid + d;
+    // block rows by their distance from the view's middle row c (c, c - 1,
+    // c + 1, ..., then the longer side's rest; a band of rows off the
+    // middle runs from its edge nearest it): the long rays through the
+    // volume start first and the frame's tail holds the short ones (1080p
+    // FULL and FLAT 3.5 % faster than row order).  Every index stays in
+    // [0, gridDim.y) and each row is taken once.
+    const uint32_t nby = gridDim.y, i = blockIdx.y;
+    const uint32_t gh = (pc.view_flags & R3D_VIEW_HALF) ? (pc.viewport[1] + 1u) / 2u
+                                                         : pc.viewport[1];
+    const int c0 = (int)(gh / 2u / kBlockH) - (int)(row0 / kBlockH);
+    const uint32_t c = (uint32_t)min(max(c0, 0), (int)nby - 1);
+    const uint32_t below = c, above = nby - 1u - c, m = min(below, above);
+    if (i <= 2u * m)
+      by = (i & 1u) ? c - (i + 1u) / 2u : c + i / 2u;
+    else
+      by = below > above ? c - (i - m) : c + (i - m);
   }
   const uint32_t tx = bx * kBlockW + (kTall ? warp * 4u : (warp & 1u) * 8u) + lx;
   const uint32_t ty = row0 + by * kBlockH + (kTall ? 0u : (warp >> 1) * 4u) + ly;

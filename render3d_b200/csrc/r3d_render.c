@@ -35,11 +35,11 @@ struct r3d_renderer {
   int ev_used[FRAMES_IN_FLIGHT];
   /* banded frames: the render streams of bands 1.. (band 0 runs on the
    * context's stream), the copy stream, one event per band and the image
-   * rows of band k, [band_row[k], band_row[k + 1]) */
+   * image rows of band k, [band_row[k], band_end[k]) */
   cudaStream_t band_stream[BANDS - 1], copy_stream;
   cudaEvent_t band_ev[BANDS];
   uint32_t nbands; /* bands of the last frame; 0: drawn whole */
-  uint32_t band_row[BANDS + 1];
+  uint32_t band_row[BANDS], band_end[BANDS];
   /* section modes and flattened views driven through this interface */
   r3d_slab_desc slab;        /* from r3d_slab_init (wz 0: none) */
   const uint8_t *slab_src;   /* the volume the tiles were built from */
@@ -289,16 +289,29 @@ int r3d_frame_views(r3d_renderer *r, const r3d_frame_params *views, uint32_t nvi
     const int half = (v->view_flags & R3D_VIEW_HALF) != 0u;
     const uint32_t gh = half ? (r->h + 1u) / 2u : r->h;
     const uint32_t rb = ((gh + BANDS - 1u) / BANDS + 7u) / 8u * 8u;
+    /* the band holding the middle row is drawn first, then the others in
+     * row order: the kernels take a band's rows by their distance from the
+     * view's middle row, so the frame's long rays start first and its last
+     * band (and last copy) holds short ones */
+    uint32_t lo[BANDS], hi[BANDS], order[BANDS], nb = 0, mid = 0, n = 0;
+    for (uint32_t r0 = 0; r0 < gh && nb < BANDS; r0 += rb, nb++) {
+      lo[nb] = r0;
+      hi[nb] = r0 + rb < gh ? r0 + rb : gh;
+      if (lo[nb] <= gh / 2u && gh / 2u < hi[nb]) mid = nb;
+    }
+    order[n++] = mid;
+    for (uint32_t b = 0; b < nb; b++)
+      if (b != mid) order[n++] = b;
     uint32_t k = 0;
-    for (uint32_t r0 = 0; r0 < gh && k < BANDS; r0 += rb, k++) {
-      const uint32_t r1 = r0 + rb < gh ? r0 + rb : gh;
+    for (; k < nb; k++) {
+      const uint32_t r0 = lo[order[k]], r1 = hi[order[k]];
       cudaStream_t s = k ? r->band_stream[k - 1] : stream;
       if (k && cudaStreamWaitEvent(s, r->ev_begin[slot], 0) != cudaSuccess) return -1;
       int rc = r3d_cuda_raycast_rows(r->ctx, v, r->offscreen, r->w, r->h, r0, r1, s);
       if (rc != R3D_OK) return report(r, "frame", rc);
       if (cudaEventRecord(r->band_ev[k], s) != cudaSuccess) return -1;
       r->band_row[k] = half ? 2u * r0 : r0;
-      r->band_row[k + 1] = half ? (2u * r1 < r->h ? 2u * r1 : r->h) : r1;
+      r->band_end[k] = half ? (2u * r1 < r->h ? 2u * r1 : r->h) : r1;
     }
     for (uint32_t j = 1; j < k; j++)
       if (cudaStreamWaitEvent(stream, r->band_ev[j], 0) != cudaSuccess) return -1;
@@ -376,7 +389,7 @@ int r3d_read_frame(r3d_renderer *r, uint8_t *rgba, uint32_t *w, uint32_t *h) {
     /* each band as soon as it is drawn, on the copy stream */
     const size_t row = (size_t)r->w * 4u;
     for (uint32_t k = 0; k < r->nbands; k++) {
-      const size_t off = r->band_row[k] * row, n = (r->band_row[k + 1] - r->band_row[k]) * row;
+      const size_t off = r->band_row[k] * row, n = (r->band_end[k] - r->band_row[k]) * row;
       if (cudaStreamWaitEvent(r->copy_stream, r->band_ev[k], 0) != cudaSuccess ||
           (n && cudaMemcpyAsync(rgba + off, r->offscreen + off, n, cudaMemcpyDeviceToHost,
                                 r->copy_stream) != cudaSuccess)) {
